@@ -1,0 +1,71 @@
+#!/usr/bin/env bash
+# Build recipe for oracle/_ref/libv2rdm_ref.so: hilbert's OWN constraint-map,
+# index-table, sizing, b/c and guess code compiled where it lies in the
+# reference tree, against the test-only Psi4 stand-ins in oracle/ref_shim/.
+#
+# The library is test infrastructure (the bit-exact checker for the B200 maps
+# and the timed CPU baseline of the reference path); the product never links it.
+#
+# Inputs : $V2B_REFERENCE (default /root/reference), read-only.
+# Outputs: oracle/_ref/ only (git-ignored; travels with the working tree).
+set -euo pipefail
+here="$(cd "$(dirname "$0")" && pwd)"
+ref="${V2B_REFERENCE:-/root/reference}"
+src="$ref/src/v2rdm_casscf"
+out="$here/_ref"
+if [ ! -f "$src/v2rdm_solver.cc" ]; then
+  echo "build_ref.sh: reference sources not found under $ref" >&2
+  exit 2
+fi
+mkdir -p "$out"
+
+# v2rdm_solver.cc as a whole needs most of Psi4; the functions the map path
+# needs only touch plain members.  Pull those definitions out by name (start:
+# the definition line at column 0, end: the first closing brace at column 0)
+# into a generated translation unit under _ref/.
+extract() {  # $1 = file, $2... = member function names
+  local f="$1"; shift
+  for name in "$@"; do
+    awk -v pat="v2RDMSolver::${name}\\\\(" '
+      !on && $0 ~ /^[A-Za-z]/ && $0 ~ pat { on = 1 }
+      on { print }
+      on && $0 ~ /^}/ { on = 0; print "" }
+    ' "$f"
+  done
+}
+gen="$out/v2rdm_solver_extract.cc"
+{
+  echo '// generated by oracle/build_ref.sh from the reference tree; do not edit'
+  echo '#include <psi4/psi4-dec.h>'
+  echo '#include <psi4/libqt/qt.h>'
+  echo '#include "v2rdm_solver.h"'
+  echo 'using namespace psi;'
+  echo 'namespace hilbert {'
+  extract "$src/v2rdm_solver.cc" SymmetryPair TotalSym set_constraints \
+      determine_n_primal determine_n_dual set_primal_offsets BuildConstraints \
+      Guess bpsdp_Au bpsdp_ATu
+  extract "$src/oei.cc" GetOEI_external GetOEI_hubbard
+  echo '}'
+} > "$gen"
+
+for name in SymmetryPair TotalSym set_constraints determine_n_primal determine_n_dual \
+            set_primal_offsets BuildConstraints Guess bpsdp_Au bpsdp_ATu GetOEI_external \
+            GetOEI_hubbard; do
+  grep -q "v2RDMSolver::${name}(" "$gen" || { echo "build_ref.sh: could not extract ${name}" >&2; exit 3; }
+done
+
+# -ffp-contract=off keeps a*b+c as two roundings, as in a plain x86-64 build
+CXX="${CXX:-g++}"
+FLAGS=(-std=c++17 -O2 -fPIC -ffp-contract=off -w
+       -I"$here/ref_shim" -I"$src" -I"$ref/src")
+units=(basis d2 spin q2 g2 t1 t2 d3 d4 e3 f3 q3 tei)
+objs=()
+for u in "${units[@]}"; do
+  "$CXX" "${FLAGS[@]}" -c "$src/$u.cc" -o "$out/$u.o"
+  objs+=("$out/$u.o")
+done
+"$CXX" "${FLAGS[@]}" -c "$gen" -o "$out/v2rdm_solver_extract.o"
+"$CXX" "${FLAGS[@]}" -c "$here/ref_harness.cc" -o "$out/ref_harness.o"
+"$CXX" -shared -Wl,--no-undefined -o "$out/libv2rdm_ref.so" "${objs[@]}" \
+    "$out/v2rdm_solver_extract.o" "$out/ref_harness.o"
+echo "built $out/libv2rdm_ref.so"

@@ -1,0 +1,1071 @@
+/*
+ * ORACLE -- TEST INFRASTRUCTURE ONLY.  Not part of the product: only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it.
+ *
+ * Plain-C restatement of hilbert's v2RDM constraint maps for C1 symmetry
+ * (one irrep, no frozen/restricted orbitals), written to follow the
+ * reference's loop and accumulation order so that A.x and A^T.y agree with
+ * the reference bit for bit.  Each function cites the reference code it
+ * restates (paths relative to the hilbert source tree).
+ *
+ * Supported constraint sets: POSITIVITY D / DQ / DG / DQG with
+ * CONSTRAIN_SPIN and CONSTRAIN_SZ on or off, singlet and non-singlet.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct {
+    int n;            /* active orbitals (amo_) */
+    int na, nb;       /* alpha / beta electrons */
+    int q2, g2, spin, sz;
+    int mult;         /* 2S+1 as the reference stores it */
+    int gab, gaa;
+    int *bas_ab, *ibas_ab, *bas_aa, *ibas_aa;
+    long d2ab, d2aa, d2bb, d200, d1a, d1b, q1a, q1b, q2ab, q2aa, q2bb, g2ab, g2ba, g2aa;
+    long n_primal, n_dual;
+    int nblocks;
+    int dims[32];
+} v2o_problem;
+
+/* basis.cc:426-533 (C1): geminal (j,i) is pushed for i outer, j inner, so
+ * geminal n = i*amo + j holds (first, second) = (j, i); aa geminals keep
+ * first < second and are numbered in the same sweep. */
+static void build_tables(v2o_problem *p) {
+    int n = p->n;
+    p->gab = n * n;
+    p->gaa = n * (n - 1) / 2;
+    p->bas_ab = (int *)malloc(sizeof(int) * 2 * (p->gab > 0 ? p->gab : 1));
+    p->ibas_ab = (int *)malloc(sizeof(int) * (n * n > 0 ? n * n : 1));
+    p->bas_aa = (int *)malloc(sizeof(int) * 2 * (p->gaa > 0 ? p->gaa : 1));
+    p->ibas_aa = (int *)malloc(sizeof(int) * (n * n > 0 ? n * n : 1));
+    for (int i = 0; i < n * n; i++) { p->ibas_ab[i] = -999; p->ibas_aa[i] = -999; }
+    int count_ab = 0, count_aa = 0;
+    for (int i = 0; i < n; i++) {
+        for (int j = 0; j < n; j++) {
+            int first = j, second = i;
+            p->ibas_ab[first * n + second] = count_ab;
+            p->bas_ab[2 * count_ab] = first;
+            p->bas_ab[2 * count_ab + 1] = second;
+            count_ab++;
+            if (first >= second) continue;
+            p->ibas_aa[first * n + second] = count_aa;
+            p->ibas_aa[second * n + first] = count_aa;
+            p->bas_aa[2 * count_aa] = first;
+            p->bas_aa[2 * count_aa + 1] = second;
+            count_aa++;
+        }
+    }
+}
+
+#define IAB(p, i, j) ((p)->ibas_ab[(i) * (p)->n + (j)])
+#define IAA(p, i, j) ((p)->ibas_aa[(i) * (p)->n + (j)])
+
+/* v2rdm_solver.cc:3729-4079 (set_primal_offsets) and 3294-3727 (sizes) */
+static void set_offsets(v2o_problem *p) {
+    long off = 0;
+    int gab = p->gab, gaa = p->gaa, n = p->n, nb = 0;
+    p->d2ab = off; off += (long)gab * gab; p->dims[nb++] = gab;
+    p->d2aa = off; off += (long)gaa * gaa; p->dims[nb++] = gaa;
+    p->d2bb = off; off += (long)gaa * gaa; p->dims[nb++] = gaa;
+    p->d200 = -1;
+    if (p->spin && p->na == p->nb) {
+        p->d200 = off; off += (long)gab * gab; p->dims[nb++] = gab;
+    } else if (p->spin) {
+        p->d200 = off; off += 4L * gab * gab; p->dims[nb++] = 2 * gab;
+    }
+    p->d1a = off; off += (long)n * n; p->dims[nb++] = n;
+    p->d1b = off; off += (long)n * n; p->dims[nb++] = n;
+    p->q1a = off; off += (long)n * n; p->dims[nb++] = n;
+    p->q1b = off; off += (long)n * n; p->dims[nb++] = n;
+    p->q2ab = p->q2aa = p->q2bb = -1;
+    if (p->q2) {
+        p->q2ab = off; off += (long)gab * gab; p->dims[nb++] = gab;
+        p->q2aa = off; off += (long)gaa * gaa; p->dims[nb++] = gaa;
+        p->q2bb = off; off += (long)gaa * gaa; p->dims[nb++] = gaa;
+    }
+    p->g2ab = p->g2ba = p->g2aa = -1;
+    if (p->g2) {
+        p->g2ab = off; off += (long)gab * gab; p->dims[nb++] = gab;
+        p->g2ba = off; off += (long)gab * gab; p->dims[nb++] = gab;
+        p->g2aa = off; off += 4L * gab * gab; p->dims[nb++] = 2 * gab;
+    }
+    p->n_primal = off;
+    p->nblocks = nb;
+
+    long d = 0;
+    d += p->sz ? 3 : 1;
+    d += 2L * gaa * gaa + (long)gab * gab;          /* hermiticity */
+    d += 2L * n * n;                                 /* D1 + Q1 = I */
+    d += (p->sz ? 4L : 2L) * n * n;                  /* partial traces */
+    if (p->spin) {
+        d += 1;
+        if (p->na == p->nb) d += (long)n * n + 3L * gaa * gaa + 2L * gab * gab;
+        else d += 4L * gab * gab;
+        if (p->g2) d += 2L * gab;
+    }
+    if (p->q2) d += (long)gab * gab + 2L * gaa * gaa;
+    if (p->g2) d += 6L * gab * gab;
+    p->n_dual = d;
+}
+
+/* positivity: 0 D, 1 DQ, 2 DG, 3 DQG (v2rdm_solver.cc:4081-4118).
+ * hubbard selects the multiplicity convention of
+ * v2rdm_solver.cc:862-863 (Hubbard) versus :983-984 (external). */
+v2o_problem *v2o_create(int n, int na, int nb, int positivity, int spin, int sz, int hubbard) {
+    if (n < 1 || na < 0 || nb < 0 || na > n || nb > n) return NULL;
+    v2o_problem *p = (v2o_problem *)calloc(1, sizeof(v2o_problem));
+    p->n = n; p->na = na; p->nb = nb;
+    p->q2 = (positivity == 1 || positivity == 3);
+    p->g2 = (positivity == 2 || positivity == 3);
+    p->spin = spin != 0; p->sz = sz != 0;
+    p->mult = hubbard ? 2 * (na - nb) + 1 : (na - nb) + 1;
+    build_tables(p);
+    set_offsets(p);
+    return p;
+}
+
+void v2o_destroy(v2o_problem *p) {
+    if (!p) return;
+    free(p->bas_ab); free(p->ibas_ab); free(p->bas_aa); free(p->ibas_aa);
+    free(p);
+}
+
+long v2o_n_primal(const v2o_problem *p) { return p->n_primal; }
+long v2o_n_dual(const v2o_problem *p) { return p->n_dual; }
+int v2o_n_blocks(const v2o_problem *p) { return p->nblocks; }
+void v2o_block_dims(const v2o_problem *p, int *out) { memcpy(out, p->dims, sizeof(int) * p->nblocks); }
+void v2o_gems(const v2o_problem *p, int *gab, int *gaa) { *gab = p->gab; *gaa = p->gaa; }
+void v2o_tables(const v2o_problem *p, int *bas_ab, int *ibas_ab, int *bas_aa, int *ibas_aa) {
+    memcpy(bas_ab, p->bas_ab, sizeof(int) * 2 * p->gab);
+    memcpy(bas_aa, p->bas_aa, sizeof(int) * 2 * p->gaa);
+    memcpy(ibas_ab, p->ibas_ab, sizeof(int) * p->n * p->n);
+    memcpy(ibas_aa, p->ibas_aa, sizeof(int) * p->n * p->n);
+}
+/* block offsets in the order d2ab d2aa d2bb d200 d1a d1b q1a q1b q2ab q2aa q2bb g2ab g2ba g2aa */
+void v2o_offsets(const v2o_problem *p, long *o) {
+    long v[14] = {p->d2ab, p->d2aa, p->d2bb, p->d200, p->d1a, p->d1b, p->q1a,
+                  p->q1b,  p->q2ab, p->q2aa, p->q2bb, p->g2ab, p->g2ba, p->g2aa};
+    memcpy(o, v, sizeof(v));
+}
+
+/* ---------------------------------------------------------------- b ---- */
+/* v2rdm_solver.cc:1826-2070 (BuildConstraints) */
+void v2o_build_b(const v2o_problem *p, double *b) {
+    int n = p->n, gab = p->gab, gaa = p->gaa;
+    double na = p->na, nb = p->nb;
+    memset(b, 0, sizeof(double) * p->n_dual);
+    long off = 0;
+    if (p->sz) {
+        b[off++] = na * nb;
+        b[off++] = na * (na - 1.0);
+        b[off++] = nb * (nb - 1.0);
+    } else {
+        double nt = na + nb;
+        b[off++] = nt * (nt - 1.0);
+    }
+    off += 2L * gaa * gaa + (long)gab * gab;
+    for (int s = 0; s < 2; s++) {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) b[off + i * n + j] = (double)(i == j);
+        off += (long)n * n;
+    }
+    off += (p->sz ? 4L : 2L) * n * n;
+    if (p->spin) {
+        double ms = (p->mult - 1.0) / 2.0;
+        b[off++] = 0.5 * (na + nb) + ms * ms - ms * (ms + 1.0);
+        if (p->na == p->nb) off += (long)n * n + 3L * gaa * gaa + 2L * gab * gab;
+        else off += 4L * gab * gab;
+        if (p->g2) off += 2L * gab;
+    }
+    if (p->q2) {
+        for (int ij = 0; ij < gab; ij++) {
+            int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                b[off + (long)ij * gab + kl] = -(i == k) * (j == l);
+            }
+        }
+        off += (long)gab * gab;
+        for (int s = 0; s < 2; s++) {
+            for (int ij = 0; ij < gaa; ij++) {
+                int i = p->bas_aa[2 * ij], j = p->bas_aa[2 * ij + 1];
+                for (int kl = 0; kl < gaa; kl++) {
+                    int k = p->bas_aa[2 * kl], l = p->bas_aa[2 * kl + 1];
+                    b[off + (long)ij * gaa + kl] = -(i == k) * (j == l) + (i == l) * (j == k);
+                }
+            }
+            off += (long)gaa * gaa;
+        }
+    }
+}
+
+/* ---------------------------------------------------------------- c ---- */
+/* Hubbard ring: oei.cc:76-95 (h), tei.cc:285-292 ((ii|ii) = U), repacked
+ * through tei.cc:139-199 / 201-275 (RepackIntegrals, FrozenCoreEnergy). */
+void v2o_build_c_hubbard(const v2o_problem *p, double t, double U, double *c) {
+    int n = p->n, gab = p->gab, gaa = p->gaa;
+    memset(c, 0, sizeof(double) * p->n_primal);
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) {
+            /* only the upper triangle survives the packed oei buffer */
+            int lo = i < j ? i : j, hi = i < j ? j : i;
+            double h = 0.0;
+            if (abs(lo - hi) == 1) h = -t;
+            else if (abs(lo - hi) == n - 1) h = -t;
+            c[p->d1a + i * n + j] = h;
+            c[p->d1b + i * n + j] = h;
+            c[p->d1a + i * n + j] += 0.0;
+            c[p->d1b + i * n + j] += 0.0;
+        }
+    for (int ij = 0; ij < gab; ij++) {
+        int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+        for (int kl = 0; kl < gab; kl++) {
+            int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+            /* TEI(i,k,j,l) */
+            c[p->d2ab + (long)ij * gab + kl] = (i == k && j == l && i == j) ? U : 0.0;
+        }
+    }
+    for (int ij = 0; ij < gaa; ij++) {
+        int i = p->bas_aa[2 * ij], j = p->bas_aa[2 * ij + 1];
+        for (int kl = 0; kl < gaa; kl++) {
+            int k = p->bas_aa[2 * kl], l = p->bas_aa[2 * kl + 1];
+            double d1 = (i == k && j == l && i == j) ? U : 0.0;
+            double d2 = (i == l && j == k && i == j) ? U : 0.0;
+            c[p->d2aa + (long)ij * gaa + kl] = d1 - d2;
+            c[p->d2bb + (long)ij * gaa + kl] = d1 - d2;
+        }
+    }
+}
+
+/* external Hamiltonian: v2rdm_solver.cc:164-193 (h -> D1, (ik|jl) -> D2ab,
+ * (ik|jl)-(il|jk) -> D2aa/bb), then GetOEI_external (oei.cc:59-74) and
+ * RepackIntegrals: D1 is rebuilt from the upper triangle of h. */
+void v2o_build_c_external(const v2o_problem *p, const double *h, const double *g, double *c) {
+    long n = p->n;
+    int gab = p->gab, gaa = p->gaa;
+    memset(c, 0, sizeof(double) * p->n_primal);
+    for (long i = 0; i < n; i++)
+        for (long j = 0; j < n; j++) {
+            long lo = i < j ? i : j, hi = i < j ? j : i;
+            double v = h[lo * n + hi];
+            c[p->d1a + i * n + j] = v;
+            c[p->d1b + i * n + j] = v;
+            c[p->d1a + i * n + j] += 0.0;
+            c[p->d1b + i * n + j] += 0.0;
+        }
+    for (int ij = 0; ij < gab; ij++) {
+        long i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+        for (int kl = 0; kl < gab; kl++) {
+            long k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+            c[p->d2ab + (long)ij * gab + kl] = g[i * n * n * n + k * n * n + j * n + l];
+        }
+    }
+    for (int ij = 0; ij < gaa; ij++) {
+        long i = p->bas_aa[2 * ij], j = p->bas_aa[2 * ij + 1];
+        for (int kl = 0; kl < gaa; kl++) {
+            long k = p->bas_aa[2 * kl], l = p->bas_aa[2 * kl + 1];
+            double v = g[i * n * n * n + k * n * n + j * n + l] - g[i * n * n * n + l * n * n + j * n + k];
+            c[p->d2aa + (long)ij * gaa + kl] = v;
+            c[p->d2bb + (long)ij * gaa + kl] = v;
+        }
+    }
+}
+
+/* ------------------------------------------------------------ guess ---- */
+/* v2rdm_solver.cc:1799-1806: srand(0); x = (rand()/RAND_MAX - 1) * 2 */
+void v2o_guess_random(const v2o_problem *p, double *x) {
+    srand(0);
+    for (long i = 0; i < p->n_primal; i++) x[i] = ((double)rand() / RAND_MAX - 1.0) * 2.0;
+}
+
+/* q2.cc:45-167 (Q2 guess) */
+static void q2_guess(const v2o_problem *p, double *u) {
+    int n = p->n, gab = p->gab, gaa = p->gaa;
+    for (int ij = 0; ij < gab; ij++) {
+        int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+        for (int kl = 0; kl < gab; kl++) {
+            int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+            double dum = 0.0;
+            dum += u[p->d2ab + (long)kl * gab + ij];
+            if (j == l) dum += u[p->q1a + i * n + k];
+            if (i == k) dum -= u[p->d1b + l * n + j];
+            u[p->q2ab + (long)ij * gab + kl] = dum;
+        }
+    }
+    for (int s = 0; s < 2; s++) {
+        long d2 = s ? p->d2bb : p->d2aa, q2 = s ? p->q2bb : p->q2aa;
+        long q1 = s ? p->q1b : p->q1a, d1 = s ? p->d1b : p->d1a;
+        for (int ij = 0; ij < gaa; ij++) {
+            int i = p->bas_aa[2 * ij], j = p->bas_aa[2 * ij + 1];
+            for (int kl = 0; kl < gaa; kl++) {
+                int k = p->bas_aa[2 * kl], l = p->bas_aa[2 * kl + 1];
+                double dum = 0.0;
+                dum += u[d2 + (long)kl * gaa + ij];
+                if (j == l) dum += u[q1 + i * n + k];
+                if (j == k) dum += u[d1 + l * n + i];
+                if (i == l) dum -= u[q1 + j * n + k];
+                if (i == k) dum -= u[d1 + l * n + j];
+                u[q2 + (long)ij * gaa + kl] = dum;
+            }
+        }
+    }
+}
+
+/* g2.cc:44-242 (G2 guess) */
+static void g2_guess(const v2o_problem *p, double *u) {
+    int n = p->n, gab = p->gab, gaa = p->gaa;
+    for (int s = 0; s < 2; s++) {
+        long g2 = s ? p->g2ba : p->g2ab, d1 = s ? p->d1b : p->d1a;
+        for (int ij = 0; ij < gab; ij++) {
+            int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                double dum = 0.0;
+                if (j == l) dum += u[d1 + i * n + k];
+                if (s == 0) dum -= u[p->d2ab + (long)IAB(p, i, l) * gab + IAB(p, k, j)];
+                else dum -= u[p->d2ab + (long)IAB(p, l, i) * gab + IAB(p, j, k)];
+                u[g2 + (long)ij * gab + kl] = dum;
+            }
+        }
+    }
+    long g = p->g2aa;
+    long w = 2L * gab;
+    for (int s = 0; s < 2; s++) {
+        long d1 = s ? p->d1b : p->d1a, d2 = s ? p->d2bb : p->d2aa, sh = s ? gab : 0;
+        for (int ij = 0; ij < gab; ij++) {
+            int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                double dum = 0.0;
+                if (j == l) dum += u[d1 + i * n + k];
+                if (i != l && k != j) {
+                    int sil = i < l ? 1 : -1, skj = k < j ? 1 : -1;
+                    dum -= u[d2 + (long)IAA(p, i, l) * gaa + IAA(p, k, j)] * sil * skj;
+                }
+                u[g + (sh + ij) * w + (sh + kl)] = dum;
+            }
+        }
+    }
+    for (int ij = 0; ij < gab; ij++) {
+        int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+        for (int kl = 0; kl < gab; kl++) {
+            int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+            double dum = 0.0;
+            dum += u[p->d2ab + (long)IAB(p, i, l) * gab + IAB(p, j, k)];
+            u[g + (long)ij * w + (gab + kl)] = dum;
+        }
+    }
+    for (int ij = 0; ij < gab; ij++) {
+        int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+        for (int kl = 0; kl < gab; kl++) {
+            int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+            double dum = 0.0;
+            dum += u[p->d2ab + (long)IAB(p, l, i) * gab + IAB(p, k, j)];
+            u[g + (gab + ij) * w + kl] = dum;
+        }
+    }
+}
+
+/* v2rdm_solver.cc:1713-1823 (TPDM_GUESS HF).  The reference stores
+ * doccpi = nalpha and soccpi = 0 for Hubbard/external problems
+ * (v2rdm_solver.cc:881-882, 1003-1004), so both spins occupy nalpha orbitals. */
+void v2o_guess_hf(const v2o_problem *p, double *x) {
+    int n = p->n, gab = p->gab, gaa = p->gaa;
+    int occ = p->na;
+    memset(x, 0, sizeof(double) * p->n_primal);
+    for (int i = 0; i < occ; i++)
+        for (int j = 0; j < occ; j++) {
+            int ij = IAB(p, i, j);
+            x[p->d2ab + (long)ij * gab + ij] = 1.0;
+        }
+    for (int i = 0; i < occ; i++)
+        for (int j = 0; j < i; j++) {
+            int ij = IAA(p, i, j);
+            x[p->d2aa + (long)ij * gaa + ij] = 1.0;
+        }
+    for (int i = 0; i < occ; i++)
+        for (int j = 0; j < i; j++) {
+            int ij = IAA(p, i, j);
+            x[p->d2bb + (long)ij * gaa + ij] = 1.0;
+        }
+    for (int i = 0; i < occ; i++) x[p->d1a + i * n + i] = 1.0;
+    for (int i = 0; i < occ; i++) x[p->d1b + i * n + i] = 1.0;
+    for (int i = occ; i < n; i++) x[p->q1a + i * n + i] = 1.0;
+    for (int i = occ; i < n; i++) x[p->q1b + i * n + i] = 1.0;
+    if (p->q2) q2_guess(p, x);
+    if (p->g2) g2_guess(p, x);
+}
+
+/* ------------------------------------------------------------- A.x ---- */
+/* v2rdm_solver.cc:2995-3050 (bpsdp_Au) -> d2.cc:314-594, spin.cc:276-508,
+ * q2.cc:170-318, g2.cc:245-442 */
+void v2o_Au(const v2o_problem *p, const double *u, double *A) {
+    int n = p->n, gab = p->gab, gaa = p->gaa;
+    double na = p->na, nb = p->nb;
+    long off = 0;
+    memset(A, 0, sizeof(double) * p->n_dual);
+
+    /* d2.cc:314-378 traces */
+    if (p->sz) {
+        double s = 0.0;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) { int ij = IAB(p, i, j); s += u[p->d2ab + (long)ij * gab + ij]; }
+        A[off++] = s;
+        s = 0.0;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                if (i == j || gaa == 0) continue;
+                int ij = IAA(p, i, j); s += u[p->d2aa + (long)ij * gaa + ij];
+            }
+        A[off++] = s;
+        s = 0.0;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                if (i == j || gaa == 0) continue;
+                int ij = IAA(p, i, j); s += u[p->d2bb + (long)ij * gaa + ij];
+            }
+        A[off++] = s;
+    } else {
+        double s = 0.0;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                int ij = IAB(p, i, j);
+                s += 2.0 * u[p->d2ab + (long)ij * gab + ij];
+                if (i == j || gaa == 0) continue;
+                ij = IAA(p, i, j);
+                s += u[p->d2aa + (long)ij * gaa + ij];
+                s += u[p->d2bb + (long)ij * gaa + ij];
+            }
+        A[off++] = s;
+    }
+    /* d2.cc:380-414 hermiticity */
+    const long hb[3] = {p->d2aa, p->d2bb, p->d2ab};
+    const int hg[3] = {gaa, gaa, gab};
+    for (int s = 0; s < 3; s++)
+        for (long ij = 0; ij < hg[s]; ij++)
+            for (long kl = 0; kl < hg[s]; kl++) {
+                double dum = u[hb[s] + ij * hg[s] + kl];
+                dum -= u[hb[s] + kl * hg[s] + ij];
+                A[off++] = dum;
+            }
+    /* d2.cc:416-435 D1 + Q1 */
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) A[off + i * n + j] = u[p->d1a + j * n + i] + u[p->q1a + i * n + j];
+    off += (long)n * n;
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) A[off + i * n + j] = u[p->d1b + j * n + i] + u[p->q1b + i * n + j];
+    off += (long)n * n;
+    /* d2.cc:441-591 partial traces */
+    if (!p->sz) {
+        double nt = na + nb;
+        for (int s = 0; s < 2; s++) {
+            long d1 = s ? p->d1b : p->d1a, d2 = s ? p->d2bb : p->d2aa;
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j < n; j++) {
+                    double sum = (nt - 1.0) * u[d1 + i * n + j];
+                    for (int k = 0; k < n; k++) {
+                        int ik = s ? IAB(p, k, i) : IAB(p, i, k);
+                        int jk = s ? IAB(p, k, j) : IAB(p, j, k);
+                        sum -= u[p->d2ab + (long)ik * gab + jk];
+                    }
+                    for (int k = 0; k < n; k++) {
+                        if (i == k || j == k) continue;
+                        int ik = IAA(p, i, k), jk = IAA(p, j, k);
+                        int sik = i < k ? 1 : -1, sjk = j < k ? 1 : -1;
+                        sum -= sik * sjk * u[d2 + (long)ik * gaa + jk];
+                    }
+                    A[off + i * n + j] = sum;
+                }
+            off += (long)n * n;
+        }
+    } else {
+        for (int s = 0; s < 2; s++) {
+            long d1 = s ? p->d1b : p->d1a;
+            double f = s ? na : nb;
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j < n; j++) {
+                    double sum = f * u[d1 + i * n + j];
+                    for (int k = 0; k < n; k++) {
+                        int ik = s ? IAB(p, k, i) : IAB(p, i, k);
+                        int jk = s ? IAB(p, k, j) : IAB(p, j, k);
+                        sum -= u[p->d2ab + (long)ik * gab + jk];
+                    }
+                    A[off + i * n + j] = sum;
+                }
+            off += (long)n * n;
+        }
+        for (int s = 0; s < 2; s++) {
+            long d1 = s ? p->d1b : p->d1a, d2 = s ? p->d2bb : p->d2aa;
+            double f = s ? (nb - 1.0) : (na - 1.0);
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j < n; j++) {
+                    double sum = f * u[d1 + i * n + j];
+                    for (int k = 0; k < n; k++) {
+                        if (i == k || j == k) continue;
+                        int ik = IAA(p, i, k), jk = IAA(p, j, k);
+                        int sik = i < k ? 1 : -1, sjk = j < k ? 1 : -1;
+                        sum -= sik * sjk * u[d2 + (long)ik * gaa + jk];
+                    }
+                    A[off + i * n + j] = sum;
+                }
+            off += (long)n * n;
+        }
+    }
+
+    if (p->spin) {
+        /* spin.cc:279-290  <S^2> row */
+        double s2 = 0.0;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) s2 += u[p->d2ab + (long)IAB(p, i, j) * gab + IAB(p, j, i)];
+        A[off++] = s2;
+        if (p->na == p->nb) {
+            /* spin.cc:320-393 singlet rows */
+            for (long r = 0; r < (long)n * n; r++) { A[off + r] = u[p->d1a + r]; A[off + r] += -1.0 * u[p->d1b + r]; }
+            off += (long)n * n;
+            for (long r = 0; r < (long)gaa * gaa; r++) { A[off + r] = u[p->d2aa + r]; A[off + r] += -1.0 * u[p->d2bb + r]; }
+            off += (long)gaa * gaa;
+            for (int s = 0; s < 2; s++) {
+                long d2 = s ? p->d2bb : p->d2aa;
+                for (long r = 0; r < (long)gaa * gaa; r++) A[off + r] = u[d2 + r];
+                for (int ij = 0; ij < gaa; ij++) {
+                    int i = p->bas_aa[2 * ij], j = p->bas_aa[2 * ij + 1];
+                    long ijb = IAB(p, i, j), jib = IAB(p, j, i);
+                    for (int kl = 0; kl < gaa; kl++) {
+                        int k = p->bas_aa[2 * kl], l = p->bas_aa[2 * kl + 1];
+                        long klb = IAB(p, k, l), lkb = IAB(p, l, k);
+                        double *a = &A[off + (long)ij * gaa + kl];
+                        *a -= 0.5 * u[p->d2ab + ijb * gab + klb];
+                        *a += 0.5 * u[p->d2ab + jib * gab + klb];
+                        *a += 0.5 * u[p->d2ab + ijb * gab + lkb];
+                        *a -= 0.5 * u[p->d2ab + jib * gab + lkb];
+                    }
+                }
+                off += (long)gaa * gaa;
+            }
+            for (long r = 0; r < (long)gab * gab; r++) A[off + r] = u[p->d200 + r];
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                long ji = IAB(p, j, i);
+                double dij = (i == j) ? sqrt(2.0) : 1.0;
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    long lk = IAB(p, l, k);
+                    double dkl = (k == l) ? sqrt(2.0) : 1.0;
+                    double *a = &A[off + (long)ij * gab + kl];
+                    *a -= 0.5 / (dij * dkl) * u[p->d2ab + (long)ij * gab + kl];
+                    *a -= 0.5 / (dij * dkl) * u[p->d2ab + ji * gab + kl];
+                    *a -= 0.5 / (dij * dkl) * u[p->d2ab + (long)ij * gab + lk];
+                    *a -= 0.5 / (dij * dkl) * u[p->d2ab + ji * gab + lk];
+                }
+            }
+            off += (long)gab * gab;
+            for (long r = 0; r < (long)gab * gab; r++) A[off + r] += 1.0 * u[p->d2ab + r];
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                long ji = IAB(p, j, i);
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    long lk = IAB(p, l, k);
+                    A[off + (long)ij * gab + kl] -= u[p->d2ab + ji * gab + lk];
+                }
+            }
+            off += (long)gab * gab;
+        } else {
+            /* spin.cc:411-485 non-singlet 2gab x 2gab block */
+            long w = 2L * gab;
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                long ji = IAB(p, j, i);
+                double dij = (i == j) ? sqrt(2.0) : 1.0;
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    long lk = IAB(p, l, k);
+                    double dkl = (k == l) ? sqrt(2.0) : 1.0;
+                    double *a = &A[off + (long)ij * w + kl];
+                    *a += u[p->d200 + (long)ij * w + kl];
+                    *a -= 0.5 / (dij * dkl) * u[p->d2ab + (long)ij * gab + kl];
+                    *a -= 0.5 / (dij * dkl) * u[p->d2ab + ji * gab + kl];
+                    *a -= 0.5 / (dij * dkl) * u[p->d2ab + (long)ij * gab + lk];
+                    *a -= 0.5 / (dij * dkl) * u[p->d2ab + ji * gab + lk];
+                }
+            }
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                long ji = IAB(p, j, i);
+                double dij = (i == j) ? sqrt(2.0) : 1.0;
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    long lk = IAB(p, l, k);
+                    double *a = &A[off + (long)ij * w + (kl + gab)];
+                    *a += u[p->d200 + (long)ij * w + (kl + gab)];
+                    *a -= 0.5 / dij * u[p->d2ab + (long)ij * gab + kl];
+                    *a += 0.5 / dij * u[p->d2ab + (long)ij * gab + lk];
+                    *a -= 0.5 / dij * u[p->d2ab + ji * gab + kl];
+                    *a += 0.5 / dij * u[p->d2ab + ji * gab + lk];
+                }
+            }
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                long ji = IAB(p, j, i);
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    long lk = IAB(p, l, k);
+                    double dkl = (k == l) ? sqrt(2.0) : 1.0;
+                    double *a = &A[off + (ij + gab) * w + kl];
+                    *a += u[p->d200 + (ij + gab) * w + kl];
+                    *a -= 0.5 / dkl * u[p->d2ab + (long)ij * gab + kl];
+                    *a -= 0.5 / dkl * u[p->d2ab + (long)ij * gab + lk];
+                    *a += 0.5 / dkl * u[p->d2ab + ji * gab + kl];
+                    *a += 0.5 / dkl * u[p->d2ab + ji * gab + lk];
+                }
+            }
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                long ji = IAB(p, j, i);
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    long lk = IAB(p, l, k);
+                    double *a = &A[off + (ij + gab) * w + (kl + gab)];
+                    *a += u[p->d200 + (ij + gab) * w + (kl + gab)];
+                    *a -= 0.5 * u[p->d2ab + (long)ij * gab + kl];
+                    *a += 0.5 * u[p->d2ab + ji * gab + kl];
+                    *a += 0.5 * u[p->d2ab + (long)ij * gab + lk];
+                    *a -= 0.5 * u[p->d2ab + ji * gab + lk];
+                }
+            }
+            off += 4L * gab * gab;
+        }
+        if (p->g2) {
+            /* spin.cc:487-507 maximal-spin rows on G2ba */
+            for (int kl = 0; kl < gab; kl++) {
+                double dum = 0.0;
+                for (int i = 0; i < n; i++) dum += u[p->g2ba + (long)kl * gab + IAB(p, i, i)];
+                A[off + kl] = dum;
+            }
+            off += gab;
+            for (int kl = 0; kl < gab; kl++) {
+                double dum = 0.0;
+                for (int i = 0; i < n; i++) dum += u[p->g2ba + (long)IAB(p, i, i) * gab + kl];
+                A[off + kl] = dum;
+            }
+            off += gab;
+        }
+    }
+
+    if (p->q2) {
+        /* q2.cc:170-216 Q2ab */
+        for (long r = 0; r < (long)gab * gab; r++) { A[off + r] = u[p->d2ab + r]; A[off + r] += -1.0 * u[p->q2ab + r]; }
+        for (int ij = 0; ij < gab; ij++) {
+            int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+            for (int k = 0; k < n; k++) A[off + (long)ij * gab + IAB(p, k, j)] -= u[p->d1a + k * n + i];
+            for (int l = 0; l < n; l++) A[off + (long)ij * gab + IAB(p, i, l)] -= u[p->d1b + l * n + j];
+        }
+        off += (long)gab * gab;
+        /* q2.cc:218-318 Q2aa / Q2bb */
+        for (int s = 0; s < 2; s++) {
+            long d2 = s ? p->d2bb : p->d2aa, q2 = s ? p->q2bb : p->q2aa, d1 = s ? p->d1b : p->d1a;
+            for (long r = 0; r < (long)gaa * gaa; r++) { A[off + r] = u[d2 + r]; A[off + r] += -1.0 * u[q2 + r]; }
+            for (int ij = 0; ij < gaa; ij++) {
+                int i = p->bas_aa[2 * ij], j = p->bas_aa[2 * ij + 1];
+                for (int kl = 0; kl < gaa; kl++) {
+                    int k = p->bas_aa[2 * kl], l = p->bas_aa[2 * kl + 1];
+                    double dum = 0.0;
+                    if (j == l) dum -= u[d1 + k * n + i];
+                    if (j == k) dum += u[d1 + l * n + i];
+                    if (i == l) dum += u[d1 + k * n + j];
+                    if (i == k) dum -= u[d1 + l * n + j];
+                    A[off + (long)ij * gaa + kl] += dum;
+                }
+            }
+            off += (long)gaa * gaa;
+        }
+    }
+
+    if (p->g2) {
+        /* g2.cc:245-312 G2ab / G2ba */
+        for (int s = 0; s < 2; s++) {
+            long g = s ? p->g2ba : p->g2ab, d1 = s ? p->d1b : p->d1a;
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    double dum = -u[g + (long)ij * gab + kl];
+                    if (j == l) dum += u[d1 + i * n + k];
+                    if (s == 0) dum -= u[p->d2ab + (long)IAB(p, i, l) * gab + IAB(p, k, j)];
+                    else dum -= u[p->d2ab + (long)IAB(p, l, i) * gab + IAB(p, j, k)];
+                    A[off + (long)ij * gab + kl] = dum;
+                }
+            }
+            off += (long)gab * gab;
+        }
+        /* g2.cc:313-440 G2 aaaa / bbbb / aabb / bbaa */
+        long g = p->g2aa, w = 2L * gab;
+        for (int s = 0; s < 2; s++) {
+            long d1 = s ? p->d1b : p->d1a, d2 = s ? p->d2bb : p->d2aa, sh = s ? gab : 0;
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    double dum = -u[g + (sh + ij) * w + (sh + kl)];
+                    if (j == l) dum += u[d1 + i * n + k];
+                    if (i != l && k != j) {
+                        int sil = i < l ? 1 : -1, skj = k < j ? 1 : -1;
+                        dum -= u[d2 + (long)IAA(p, i, l) * gaa + IAA(p, k, j)] * sil * skj;
+                    }
+                    A[off + (sh + ij) * w + (sh + kl)] = dum;
+                }
+            }
+        }
+        for (int ij = 0; ij < gab; ij++) {
+            int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                double dum = -u[g + (long)ij * w + (gab + kl)];
+                dum += u[p->d2ab + (long)IAB(p, i, l) * gab + IAB(p, j, k)];
+                A[off + (long)ij * w + (gab + kl)] = dum;
+            }
+        }
+        for (int ij = 0; ij < gab; ij++) {
+            int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                double dum = -u[g + (gab + ij) * w + kl];
+                dum += u[p->d2ab + (long)IAB(p, l, i) * gab + IAB(p, k, j)];
+                A[off + (gab + ij) * w + kl] = dum;
+            }
+        }
+        off += 4L * gab * gab;
+    }
+}
+
+/* ----------------------------------------------------------- A^T.y ---- */
+/* v2rdm_solver.cc:3054-3108 (bpsdp_ATu) -> d2.cc:46-311, spin.cc:46-273,
+ * q2.cc:320-438, g2.cc:444-634; same scatter order as the reference */
+void v2o_ATu(const v2o_problem *p, const double *u, double *A) {
+    int n = p->n, gab = p->gab, gaa = p->gaa;
+    double na = p->na, nb = p->nb;
+    long off = 0;
+    memset(A, 0, sizeof(double) * p->n_primal);
+
+    if (p->sz) {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) { int ij = IAB(p, i, j); A[p->d2ab + (long)ij * gab + ij] += u[off]; }
+        off++;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                if (i == j || gaa == 0) continue;
+                int ij = IAA(p, i, j); A[p->d2aa + (long)ij * gaa + ij] += u[off];
+            }
+        off++;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                if (i == j || gaa == 0) continue;
+                int ij = IAA(p, i, j); A[p->d2bb + (long)ij * gaa + ij] += u[off];
+            }
+        off++;
+    } else {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                int ij = IAB(p, i, j);
+                A[p->d2ab + (long)ij * gab + ij] += 2.0 * u[off];
+                if (i == j || gaa == 0) continue;
+                ij = IAA(p, i, j);
+                A[p->d2aa + (long)ij * gaa + ij] += u[off];
+                A[p->d2bb + (long)ij * gaa + ij] += u[off];
+            }
+        off++;
+    }
+    const long hb[3] = {p->d2aa, p->d2bb, p->d2ab};
+    const int hg[3] = {gaa, gaa, gab};
+    for (int s = 0; s < 3; s++)
+        for (long ij = 0; ij < hg[s]; ij++)
+            for (long kl = 0; kl < hg[s]; kl++) {
+                double dum = u[off];
+                A[hb[s] + ij * hg[s] + kl] += dum;
+                A[hb[s] + kl * hg[s] + ij] -= dum;
+                off++;
+            }
+    for (int s = 0; s < 2; s++) {
+        long d1 = s ? p->d1b : p->d1a, q1 = s ? p->q1b : p->q1a;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                double dum = u[off + i * n + j];
+                A[d1 + j * n + i] += dum;
+                A[q1 + i * n + j] += dum;
+            }
+        off += (long)n * n;
+    }
+    if (!p->sz) {
+        for (int s = 0; s < 2; s++) {
+            long d1 = s ? p->d1b : p->d1a, d2 = s ? p->d2bb : p->d2aa;
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j < n; j++) {
+                    A[d1 + i * n + j] += (na + nb - 1.0) * u[off + i * n + j];
+                    for (int k = 0; k < n; k++) {
+                        int ik = s ? IAB(p, k, i) : IAB(p, i, k);
+                        int jk = s ? IAB(p, k, j) : IAB(p, j, k);
+                        A[p->d2ab + (long)ik * gab + jk] -= u[off + i * n + j];
+                    }
+                    for (int k = 0; k < n; k++) {
+                        if (i == k || j == k) continue;
+                        int ik = IAA(p, i, k), jk = IAA(p, j, k);
+                        int sik = i < k ? 1 : -1, sjk = j < k ? 1 : -1;
+                        A[d2 + (long)ik * gaa + jk] -= sik * sjk * u[off + i * n + j];
+                    }
+                }
+            off += (long)n * n;
+        }
+    } else {
+        for (int s = 0; s < 2; s++) {
+            long d1 = s ? p->d1b : p->d1a;
+            double f = s ? na : nb;
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j < n; j++) {
+                    A[d1 + i * n + j] += f * u[off + i * n + j];
+                    for (int k = 0; k < n; k++) {
+                        int ik = s ? IAB(p, k, i) : IAB(p, i, k);
+                        int jk = s ? IAB(p, k, j) : IAB(p, j, k);
+                        A[p->d2ab + (long)ik * gab + jk] -= u[off + i * n + j];
+                    }
+                }
+            off += (long)n * n;
+        }
+        for (int s = 0; s < 2; s++) {
+            long d1 = s ? p->d1b : p->d1a, d2 = s ? p->d2bb : p->d2aa;
+            double f = s ? (nb - 1.0) : (na - 1.0);
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j < n; j++) {
+                    A[d1 + i * n + j] += f * u[off + i * n + j];
+                    for (int k = 0; k < n; k++) {
+                        if (i == k || j == k) continue;
+                        int ik = IAA(p, i, k), jk = IAA(p, j, k);
+                        int sik = i < k ? 1 : -1, sjk = j < k ? 1 : -1;
+                        A[d2 + (long)ik * gaa + jk] -= sik * sjk * u[off + i * n + j];
+                    }
+                }
+            off += (long)n * n;
+        }
+    }
+
+    if (p->spin) {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) A[p->d2ab + (long)IAB(p, i, j) * gab + IAB(p, j, i)] += u[off];
+        off++;
+        if (p->na == p->nb) {
+            for (long r = 0; r < (long)n * n; r++) A[p->d1a + r] += 1.0 * u[off + r];
+            for (long r = 0; r < (long)n * n; r++) A[p->d1b + r] += -1.0 * u[off + r];
+            off += (long)n * n;
+            for (long r = 0; r < (long)gaa * gaa; r++) A[p->d2aa + r] += 1.0 * u[off + r];
+            for (long r = 0; r < (long)gaa * gaa; r++) A[p->d2bb + r] += -1.0 * u[off + r];
+            off += (long)gaa * gaa;
+            for (int s = 0; s < 2; s++) {
+                long d2 = s ? p->d2bb : p->d2aa;
+                for (long r = 0; r < (long)gaa * gaa; r++) A[d2 + r] += 1.0 * u[off + r];
+                for (int ij = 0; ij < gaa; ij++) {
+                    int i = p->bas_aa[2 * ij], j = p->bas_aa[2 * ij + 1];
+                    long ijb = IAB(p, i, j), jib = IAB(p, j, i);
+                    for (int kl = 0; kl < gaa; kl++) {
+                        int k = p->bas_aa[2 * kl], l = p->bas_aa[2 * kl + 1];
+                        long klb = IAB(p, k, l), lkb = IAB(p, l, k);
+                        double v = u[off + (long)ij * gaa + kl];
+                        A[p->d2ab + ijb * gab + klb] -= 0.5 * v;
+                        A[p->d2ab + jib * gab + klb] += 0.5 * v;
+                        A[p->d2ab + ijb * gab + lkb] += 0.5 * v;
+                        A[p->d2ab + jib * gab + lkb] -= 0.5 * v;
+                    }
+                }
+                off += (long)gaa * gaa;
+            }
+            for (long r = 0; r < (long)gab * gab; r++) A[p->d200 + r] += 1.0 * u[off + r];
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                long ji = IAB(p, j, i);
+                double dij = (i == j) ? sqrt(2.0) : 1.0;
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    long lk = IAB(p, l, k);
+                    double dkl = (k == l) ? sqrt(2.0) : 1.0;
+                    double v = u[off + (long)ij * gab + kl];
+                    A[p->d2ab + (long)ij * gab + kl] -= 0.5 / (dij * dkl) * v;
+                    A[p->d2ab + ji * gab + kl] -= 0.5 / (dij * dkl) * v;
+                    A[p->d2ab + (long)ij * gab + lk] -= 0.5 / (dij * dkl) * v;
+                    A[p->d2ab + ji * gab + lk] -= 0.5 / (dij * dkl) * v;
+                }
+            }
+            off += (long)gab * gab;
+            for (long r = 0; r < (long)gab * gab; r++) A[p->d2ab + r] += 1.0 * u[off + r];
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                long ji = IAB(p, j, i);
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    long lk = IAB(p, l, k);
+                    A[p->d2ab + ji * gab + lk] -= u[off + (long)ij * gab + kl];
+                }
+            }
+            off += (long)gab * gab;
+        } else {
+            long w = 2L * gab;
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                long ji = IAB(p, j, i);
+                double dij = (i == j) ? sqrt(2.0) : 1.0;
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    long lk = IAB(p, l, k);
+                    double dkl = (k == l) ? sqrt(2.0) : 1.0;
+                    double v = u[off + (long)ij * w + kl];
+                    A[p->d200 + (long)ij * w + kl] += v;
+                    A[p->d2ab + (long)ij * gab + kl] -= 0.5 / (dij * dkl) * v;
+                    A[p->d2ab + ji * gab + kl] -= 0.5 / (dij * dkl) * v;
+                    A[p->d2ab + (long)ij * gab + lk] -= 0.5 / (dij * dkl) * v;
+                    A[p->d2ab + ji * gab + lk] -= 0.5 / (dij * dkl) * v;
+                }
+            }
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                long ji = IAB(p, j, i);
+                double dij = (i == j) ? sqrt(2.0) : 1.0;
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    long lk = IAB(p, l, k);
+                    double v = u[off + (long)ij * w + (kl + gab)];
+                    A[p->d200 + (long)ij * w + (kl + gab)] += v;
+                    A[p->d2ab + (long)ij * gab + kl] -= 0.5 / dij * v;
+                    A[p->d2ab + (long)ij * gab + lk] += 0.5 / dij * v;
+                    A[p->d2ab + ji * gab + kl] -= 0.5 / dij * v;
+                    A[p->d2ab + ji * gab + lk] += 0.5 / dij * v;
+                }
+            }
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                long ji = IAB(p, j, i);
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    long lk = IAB(p, l, k);
+                    double dkl = (k == l) ? sqrt(2.0) : 1.0;
+                    double v = u[off + (ij + gab) * w + kl];
+                    A[p->d200 + (ij + gab) * w + kl] += v;
+                    A[p->d2ab + (long)ij * gab + kl] -= 0.5 / dkl * v;
+                    A[p->d2ab + (long)ij * gab + lk] -= 0.5 / dkl * v;
+                    A[p->d2ab + ji * gab + kl] += 0.5 / dkl * v;
+                    A[p->d2ab + ji * gab + lk] += 0.5 / dkl * v;
+                }
+            }
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                long ji = IAB(p, j, i);
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    long lk = IAB(p, l, k);
+                    double v = u[off + (ij + gab) * w + (kl + gab)];
+                    A[p->d200 + (ij + gab) * w + (kl + gab)] += v;
+                    A[p->d2ab + (long)ij * gab + kl] -= 0.5 * v;
+                    A[p->d2ab + ji * gab + kl] += 0.5 * v;
+                    A[p->d2ab + (long)ij * gab + lk] += 0.5 * v;
+                    A[p->d2ab + ji * gab + lk] -= 0.5 * v;
+                }
+            }
+            off += 4L * gab * gab;
+        }
+        if (p->g2) {
+            for (int kl = 0; kl < gab; kl++) {
+                double dum = u[off + kl];
+                for (int i = 0; i < n; i++) A[p->g2ba + (long)kl * gab + IAB(p, i, i)] += dum;
+            }
+            off += gab;
+            for (int kl = 0; kl < gab; kl++) {
+                double dum = u[off + kl];
+                for (int i = 0; i < n; i++) A[p->g2ba + (long)IAB(p, i, i) * gab + kl] += dum;
+            }
+            off += gab;
+        }
+    }
+
+    if (p->q2) {
+        for (long r = 0; r < (long)gab * gab; r++) A[p->d2ab + r] += 1.0 * u[off + r];
+        for (long r = 0; r < (long)gab * gab; r++) A[p->q2ab + r] += -1.0 * u[off + r];
+        for (int ij = 0; ij < gab; ij++) {
+            int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                double v = u[off + (long)ij * gab + kl];
+                if (j == l) A[p->d1a + k * n + i] -= v;
+                if (i == k) A[p->d1b + l * n + j] -= v;
+            }
+        }
+        off += (long)gab * gab;
+        for (int s = 0; s < 2; s++) {
+            long d2 = s ? p->d2bb : p->d2aa, q2 = s ? p->q2bb : p->q2aa, d1 = s ? p->d1b : p->d1a;
+            for (long r = 0; r < (long)gaa * gaa; r++) A[d2 + r] += 1.0 * u[off + r];
+            for (long r = 0; r < (long)gaa * gaa; r++) A[q2 + r] += -1.0 * u[off + r];
+            for (int ij = 0; ij < gaa; ij++) {
+                int i = p->bas_aa[2 * ij], j = p->bas_aa[2 * ij + 1];
+                for (int kl = 0; kl < gaa; kl++) {
+                    int k = p->bas_aa[2 * kl], l = p->bas_aa[2 * kl + 1];
+                    double v = u[off + (long)ij * gaa + kl];
+                    if (j == l) A[d1 + k * n + i] -= v;
+                    if (j == k) A[d1 + l * n + i] += v;
+                    if (i == l) A[d1 + k * n + j] += v;
+                    if (i == k) A[d1 + l * n + j] -= v;
+                }
+            }
+            off += (long)gaa * gaa;
+        }
+    }
+
+    if (p->g2) {
+        for (int s = 0; s < 2; s++) {
+            long g = s ? p->g2ba : p->g2ab, d1 = s ? p->d1b : p->d1a;
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    double dum = u[off + (long)ij * gab + kl];
+                    A[g + (long)ij * gab + kl] -= dum;
+                    if (j == l) A[d1 + i * n + k] += dum;
+                    if (s == 0) A[p->d2ab + (long)IAB(p, i, l) * gab + IAB(p, k, j)] -= dum;
+                    else A[p->d2ab + (long)IAB(p, l, i) * gab + IAB(p, j, k)] -= dum;
+                }
+            }
+            off += (long)gab * gab;
+        }
+        long g = p->g2aa, w = 2L * gab;
+        for (int s = 0; s < 2; s++) {
+            long d1 = s ? p->d1b : p->d1a, d2 = s ? p->d2bb : p->d2aa, sh = s ? gab : 0;
+            for (int ij = 0; ij < gab; ij++) {
+                int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+                for (int kl = 0; kl < gab; kl++) {
+                    int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                    double dum = u[off + (sh + ij) * w + (sh + kl)];
+                    A[g + (sh + ij) * w + (sh + kl)] -= dum;
+                    if (j == l) A[d1 + i * n + k] += dum;
+                    if (i != l && k != j) {
+                        int sil = i < l ? 1 : -1, skj = k < j ? 1 : -1;
+                        A[d2 + (long)IAA(p, i, l) * gaa + IAA(p, k, j)] -= dum * sil * skj;
+                    }
+                }
+            }
+        }
+        for (int ij = 0; ij < gab; ij++) {
+            int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                double dum = u[off + (long)ij * w + (kl + gab)];
+                A[g + (long)ij * w + (kl + gab)] -= dum;
+                A[p->d2ab + (long)IAB(p, i, l) * gab + IAB(p, j, k)] += dum;
+            }
+        }
+        for (int ij = 0; ij < gab; ij++) {
+            int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                double dum = u[off + (gab + ij) * w + kl];
+                A[g + (gab + ij) * w + kl] -= dum;
+                A[p->d2ab + (long)IAB(p, l, i) * gab + IAB(p, k, j)] += dum;
+            }
+        }
+        off += 4L * gab * gab;
+    }
+}
