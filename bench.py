@@ -1,0 +1,365 @@
+"""Benchmark: time to 1e-6 boundary-point SDP convergence of a v2RDM problem on B200.
+
+Workload (default ``hubbard8``): plain v2RDM, POSITIVITY DQG, fixed orbitals,
+FP64, C1, on the 1D periodic Hubbard ring with 8 sites, 8 electrons, t = 1,
+U = 4 (hilbert's own Hubbard path: h = -t on ring neighbours, (ii|ii) = U),
+converged to primal and dual error < 1e-6 and |E_p - E_d| < 1e-6, from the
+reference's random guess (srand(0)), MU_UPDATE_FREQUENCY 500, CG_CONVERGENCE
+1e-9.  Data are synthetic by construction (the Hamiltonian is the model).
+
+One step = one full solve to convergence.  ``value`` is the device solve
+time with b, c, x already in HBM (CUDA events on the library's stream);
+``e2e`` is the same solve through the public API with host arrays (pinned
+H2D of x0, b, c and D2H of x inside the timed region).  L2 is flushed between
+steps (a 256 MiB write); inside one solve the working set stays L2-resident.
+
+Multi-GPU: replicas only.  Each rank solves its own copy of the workload;
+the reported time is the max over ranks; nothing crosses NVLink in the data
+path.
+
+``--impl reference`` times the reference's own CPU implementation of the path
+(hilbert's compiled constraint maps from oracle/_ref, else the C restatement,
+driven by the numpy boundary-point restatement), each step a bounded sample
+of outer iterations extrapolated to the workload's iteration count.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "hubbard8": dict(nmo=8, nalpha=4, nbeta=4, positivity="DQG", hubbard=(1.0, 4.0),
+                     r_conv=1e-6, e_conv=1e-6, cg_conv=1e-9, muf=500, maxiter=400000),
+}
+# (outer, CG) iterations the FP64 oracle needed to converge this workload,
+# recorded from a full oracle run; the reference arm scales its sample by them
+ORACLE_ITERS = {"hubbard8": (None, None)}
+
+METRIC = "time to 1e-6 SDP convergence, mixed/batched vs plain FP64 on B200; |dE| vs FP64"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="hubbard8", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}",
+                                      f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits"],
+                                     capture_output=True, text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([v.strip() for v in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 5 + k and r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dist_setup():
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_threads():
+    try:
+        from threadpoolctl import threadpool_info
+        n = [i.get("num_threads", 1) for i in threadpool_info() if i.get("user_api") == "blas"]
+        return max(n) if n else 1
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_sample(w, seconds):
+    """Time the CPU path on a bounded sample.
+
+    The boundary-point iteration's cost is (cost of one CG iteration: A^T.p,
+    A.t, two dots, three axpys) x CG iterations + (fixed cost of one outer
+    iteration: A.x, A.(c-z), A^T.y, the block eigendecompositions, norms) x
+    outer iterations.  Both unit costs are timed here on the host, each for
+    about seconds/2, from the reference's random guess.
+    Returns (seconds per CG iteration, seconds per outer iteration, kind, repeats).
+    """
+    import numpy as np
+    from oracle import maps
+    from oracle.bpsdp import project_blocks
+    kind = "reference" if maps.ref_available() else "port"
+    P = maps.RefProblem if kind == "reference" else maps.OracleProblem
+    prob = P(w["nmo"], w["nalpha"], w["nbeta"], w["positivity"], True, True, hubbard=w["hubbard"])
+    o = maps.OracleProblem(w["nmo"], w["nalpha"], w["nbeta"], w["positivity"], True, True,
+                           hubbard=w["hubbard"])
+    x = o.guess("random")
+    z = np.zeros(prob.n_primal)
+    y = np.random.default_rng(0).standard_normal(prob.n_dual)
+    r = y.copy()
+    pv = y.copy()
+    mu = 0.1
+    reps = [0, 0]
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds / 2 or reps[0] < 3:
+        q = prob.Au(prob.ATu(pv))
+        a = float(r @ r) / float(pv @ q)
+        y += a * pv
+        r -= a * q
+        pv = r + 0.5 * pv
+        reps[0] += 1
+    t_cg = (time.perf_counter() - t0) / reps[0]
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds / 2 or reps[1] < 3:
+        ax = prob.Au(x)
+        acz = prob.Au(prob.c - z)
+        rhs = acz + mu * (prob.b - ax)
+        aty = prob.ATu(y)
+        U = mu * x + aty - prob.c
+        xn, z = project_blocks(U, prob.dims, mu)
+        ep = np.linalg.norm(prob.Au(xn) - prob.b)
+        ed = np.linalg.norm(aty + z - prob.c)
+        _ = float(prob.c @ xn) + float(prob.b @ y) + ep + ed + float(rhs[0])
+        reps[1] += 1
+    t_outer = (time.perf_counter() - t0) / reps[1]
+    return t_cg, t_outer, kind, reps
+
+
+def run_reference(args, w):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    oiter, iiter = ORACLE_ITERS.get(args.workload, (None, None))
+    vals = []
+    for k in range(args.warmup + args.steps):
+        t_cg, t_out, kind, reps = cpu_sample(w, max(2.0, args.cpu_sample_seconds / 3))
+        if k >= args.warmup:
+            vals.append(t_cg * iiter + t_out * oiter if oiter else None)
+    total = statistics.mean(vals) if oiter else None
+    line = {"impl": "reference", "metric": METRIC, "value": total, "unit": "s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, **{k: v for k, v in w.items()},
+                       "oracle_outer_iterations": oiter, "oracle_cg_iterations": iiter,
+                       "parallelism": "replicas"},
+            "cpu_baseline": {"value": total, "unit": "s", "cores": cpu_threads(), "kind": kind,
+                             "sample": f"per step: {reps[0]} CG iterations ({t_cg*1e3:.2f} ms each) and "
+                                       f"{reps[1]} outer-iteration bodies ({t_out*1e3:.2f} ms each) timed, "
+                                       f"scaled to {iiter} CG + {oiter} outer iterations to convergence"},
+            "e2e": {"value": total, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, w):
+    import numpy as np
+    import torch
+
+    import hilbert_b200 as hb
+    world, rank, local = dist_setup()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    opts = hb.Options({"R_CONVERGENCE": w["r_conv"], "E_CONVERGENCE": w["e_conv"],
+                       "CG_CONVERGENCE": w["cg_conv"], "MAXITER": w["maxiter"],
+                       "MU_UPDATE_FREQUENCY": w["muf"]})
+    p = hb.V2RDMProblem(w["nmo"], w["nalpha"], w["nbeta"], w["positivity"], True, True,
+                        hubbard_multiplicity=True)
+    b = p.b()
+    c = p.c_hubbard(*w["hubbard"])
+    x0 = p.guess("RANDOM")
+    db = torch.from_numpy(b).to(dev)
+    dc = torch.from_numpy(c).to(dev)
+    dx0 = torch.from_numpy(x0).to(dev)
+    dx = torch.empty_like(dx0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def one(profile=False):
+        dx.copy_(dx0)
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        barrier(world)
+        st = p.solve_device(dx, db, dc, opts)
+        return st
+
+    for _ in range(args.warmup):
+        one()
+    times, stats = [], None
+    launches0 = p.kernel_launches()
+    p.set_profiling(True)
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            dx.copy_(dx0)
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            barrier(world)
+            s = torch.cuda.Stream(device=dev)
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(s)
+            stats = p.solve_device(dx, db, dc, opts)
+            ev1.record(s)
+            torch.cuda.synchronize()
+            times.append(ev0.elapsed_time(ev1) / 1e3)
+    prof = p.profile()
+    p.set_profiling(False)
+    launches = p.kernel_launches() - launches0
+    t = max_over_ranks(max(times), world)
+    energy = float(c @ dx.cpu().numpy())
+
+    # end to end through the public API (host arrays in and out)
+    e2e_times = []
+    for _ in range(max(1, args.steps // 2)):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        xh, st2 = p.solve(x0, b, c, opts)
+        e2e_times.append(time.perf_counter() - t0)
+    te2e = max_over_ranks(max(e2e_times), world)
+
+    # roofline of the dominant kernel class
+    dom = max(prof, key=lambda k: prof[k][0])
+    ms, n = prof[dom]
+    oiter, iiter = stats["oiter"], stats["iiter"]
+    npr, ndu = p.n_primal, p.n_dual
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    bf16 = peaks.get("bf16_tflops", 1590.0)
+    if dom == "jacobi_project_kernel":
+        flops = sum((16.0 / 3.0) * float(d) ** 3 for d in p.dims)
+        ach = flops / (ms / n / 1e3) / 1e12
+        roof = {"kernel": dom, "bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s",
+                "frac": ach / bf16, "traffic": None,
+                "note": "FP64 SIMT Jacobi; algorithmic flops sum (16/3) n_b^3 per launch; peak is "
+                        "the measured dense bf16 figure (no FP64 peak is measured)"}
+    else:
+        cg_iters_per_launch = iiter / max(oiter, 1)
+        if dom == "cg_kernel":
+            bytes_ = 8.0 * (cg_iters_per_launch * (2 * npr + 7 * ndu) + 2 * npr + 5 * ndu)
+        elif dom == "spmv_AT_U_kernel":
+            bytes_ = 8.0 * (4 * npr + ndu)
+        elif dom == "spmv_A2_kernel":
+            bytes_ = 8.0 * (3 * npr + 2 * ndu)
+        else:
+            bytes_ = 8.0 * (5 * npr + 3 * ndu)
+        ach = bytes_ / (ms / n / 1e3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": ach / hbm, "traffic": None}
+    roof["peak_source"] = "MEASURED_PEAKS.json" if peaks else "fallback"
+    roof["kernel_ms_share"] = {k: round(v[0] / sum(x[0] for x in prof.values()), 4)
+                               for k, v in prof.items()}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        t_cg, t_out, kind, reps = cpu_sample(w, args.cpu_sample_seconds)
+        cpu = {"value": t_cg * iiter + t_out * oiter, "unit": "s", "cores": cpu_threads(),
+               "kind": kind,
+               "sample": f"{reps[0]} CG iterations ({t_cg*1e3:.2f} ms each) and {reps[1]} "
+                         f"outer-iteration bodies ({t_out*1e3:.2f} ms each) timed on the host, "
+                         f"scaled to the {iiter} CG + {oiter} outer iterations of the device solve"}
+    clocks = clk.summary()
+    if rank == 0:
+        line = {"metric": METRIC, "value": t, "unit": "s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": args.workload, "nmo": w["nmo"], "nalpha": w["nalpha"],
+                           "nbeta": w["nbeta"], "positivity": w["positivity"],
+                           "hubbard_t_U": list(w["hubbard"]), "r_convergence": w["r_conv"],
+                           "e_convergence": w["e_conv"], "cg_convergence": w["cg_conv"],
+                           "mu_update_frequency": w["muf"], "n_primal": npr, "n_dual": ndu,
+                           "parallelism": "replicas" if world > 1 else "single",
+                           "l2": "flushed between steps (256 MiB write)",
+                           "outer_iterations": oiter, "cg_iterations": iiter,
+                           "energy": energy, "converged": stats["converged"]},
+                "e2e": {"value": te2e, "unit": "s", "h2d_bytes_per_step": 8 * (2 * npr + ndu),
+                        "d2h_bytes_per_step": 8 * npr},
+                "gpu_launches": int(launches),
+                "roofline": roof, "cpu_baseline": cpu, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, w)
+    else:
+        run_b200(args, w)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,367 @@
+// CUDA kernels of the B200 boundary-point iteration (sm_100a).
+//
+//   spmv_kernel          y = A.x or A^T.y over packed rows (bit-exact to hilbert's maps)
+//   spmv_A2_kernel       A.x and A.(c - z) in one pass over A's rows
+//   spmv_AT_U_kernel     A^T.y and U = mu x + A^T y - c in one pass over A^T's rows
+//   cg_kernel            persistent conjugate-gradient solve of (A A^T) y = rhs
+//   stats_kernel         eps_p^2, eps_d^2, c.x, b.y (deterministic reductions)
+//   jacobi_project_kernel  per-block symmetric eigensolve (parallel cyclic
+//                        Jacobi in shared memory) and PSD split x = U+/mu, z = U+ - U
+#include "v2b_kernels.cuh"
+
+namespace v2b {
+
+__global__ void spmv_kernel(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ent,
+                            int64_t nrows, const double *__restrict__ x, double *__restrict__ y,
+                            Palette pal) {
+    __shared__ double spal[16];
+    if (threadIdx.x < 16) spal[threadIdx.x] = pal.v[threadIdx.x];
+    __syncthreads();
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows;
+         r += (int64_t)gridDim.x * blockDim.x)
+        y[r] = packed_row(ent, __ldg(rp + r), __ldg(rp + r + 1), x, spal);
+}
+
+__global__ void spmv_A2_kernel(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ent,
+                               int64_t nrows, const double *__restrict__ x,
+                               const double *__restrict__ c, const double *__restrict__ z,
+                               double *__restrict__ Ax, double *__restrict__ Acz, Palette pal) {
+    __shared__ double spal[16];
+    if (threadIdx.x < 16) spal[threadIdx.x] = pal.v[threadIdx.x];
+    __syncthreads();
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t b = __ldg(rp + r), e = __ldg(rp + r + 1);
+        double a0 = 0.0, a1 = 0.0, w0 = 0.0, w1 = 0.0;
+        bool grp = false;
+        for (uint32_t k = b; k < e; k++) {
+            const uint32_t w = __ldg(ent + k);
+            const uint32_t col = w & kDevColMask;
+            const double cf = spal[(w >> 27) & 15u];
+            const double vx = __dmul_rn(cf, __ldg(x + col));
+            const double vw = __dmul_rn(cf, __dsub_rn(__ldg(c + col), __ldg(z + col)));
+            grp = grp || (w >> 31);
+            if (grp) { a1 = __dadd_rn(a1, vx); w1 = __dadd_rn(w1, vw); }
+            else { a0 = __dadd_rn(a0, vx); w0 = __dadd_rn(w0, vw); }
+        }
+        Ax[r] = grp ? __dadd_rn(a0, a1) : a0;
+        Acz[r] = grp ? __dadd_rn(w0, w1) : w0;
+    }
+}
+
+__global__ void spmv_AT_U_kernel(const uint32_t *__restrict__ rp,
+                                 const uint32_t *__restrict__ ent, int64_t nrows,
+                                 const double *__restrict__ y, const double *__restrict__ x,
+                                 const double *__restrict__ c, double mu,
+                                 double *__restrict__ ATy, double *__restrict__ U, Palette pal) {
+    __shared__ double spal[16];
+    if (threadIdx.x < 16) spal[threadIdx.x] = pal.v[threadIdx.x];
+    __syncthreads();
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const double a = packed_row(ent, __ldg(rp + r), __ldg(rp + r + 1), y, spal);
+        ATy[r] = a;
+        U[r] = mu * x[r] + a - c[r];
+    }
+}
+
+// ------------------------------------------------------------------ CG
+// Solves (A A^T) y = rhs with rhs = A(c - z) + mu (b - A x), warm-started from
+// y.  Three grid barriers per iteration:
+//   1. t = A^T (r + beta p_old), p_new = r + beta p_old
+//   2. q = A t,  partial p_new.q
+//   3. y += alpha p_new, r -= alpha q, partial r.r
+__global__ void __launch_bounds__(kCgThreads) cg_kernel(CgParams P) {
+    __shared__ double palA[16], palT[16];
+    __shared__ double red[32];
+    __shared__ double bcast;
+    __shared__ int flag;
+    if (threadIdx.x < 16) {
+        palA[threadIdx.x] = P.palA.v[threadIdx.x];
+        palT[threadIdx.x] = P.palT.v[threadIdx.x];
+    }
+    __syncthreads();
+    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int nb = gridDim.x;
+
+    // r = rhs - A A^T y
+    for (int64_t i = gtid; i < P.np; i += stride)
+        P.t[i] = packed_row(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), P.y, palT);
+    if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
+    double loc = 0.0;
+    for (int64_t j = gtid; j < P.nd; j += stride) {
+        const double rhs = P.Acz[j] + P.mu * (P.b[j] - P.Ax[j]);
+        const double v = rhs - packed_row(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), P.t, palA);
+        P.r[j] = v;
+        loc += v * v;
+    }
+    double s = block_sum(loc, red);
+    if (threadIdx.x == 0) P.partials[blockIdx.x] = s;
+    if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
+    double rs = sum_partials(P.partials, nb, &bcast);
+
+    int it = 0;
+    double beta = 0.0;
+    const double *pold = P.r;   // first direction p = r (beta = 0)
+    double *pnew = P.p0;
+    bool done = !(sqrt(rs) >= P.tol);
+    while (!done && it < P.maxit) {
+        for (int64_t i = gtid; i < P.np; i += stride)
+            P.t[i] = packed_row_rbp(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), P.r, pold,
+                                    beta, palT);
+        for (int64_t j = gtid; j < P.nd; j += stride)
+            pnew[j] = __dadd_rn(P.r[j], __dmul_rn(beta, pold[j]));
+        if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
+
+        loc = 0.0;
+        for (int64_t j = gtid; j < P.nd; j += stride) {
+            const double q = packed_row(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), P.t, palA);
+            P.q[j] = q;
+            loc += pnew[j] * q;
+        }
+        s = block_sum(loc, red);
+        if (threadIdx.x == 0) P.partials[blockIdx.x] = s;
+        if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
+        const double pq = sum_partials(P.partials, nb, &bcast);
+        if (!(pq > 0.0)) break;   // range of A A^T exhausted (or non-finite)
+        const double alpha = rs / pq;
+
+        loc = 0.0;
+        for (int64_t j = gtid; j < P.nd; j += stride) {
+            P.y[j] += alpha * pnew[j];
+            const double rv = P.r[j] - alpha * P.q[j];
+            P.r[j] = rv;
+            loc += rv * rv;
+        }
+        s = block_sum(loc, red);
+        if (threadIdx.x == 0) P.partials[blockIdx.x] = s;
+        if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
+        const double rs_new = sum_partials(P.partials, nb, &bcast);
+        it++;
+        if (!(rs_new == rs_new)) {   // NaN
+            if (gtid == 0) atomicExch(P.status, kStatusNan);
+            break;
+        }
+        done = sqrt(rs_new) < P.tol;
+        beta = rs_new / rs;
+        rs = rs_new;
+        // the next direction is built from r and the current one
+        double *tmp = (pnew == P.p0) ? P.p1 : P.p0;
+        pold = pnew;
+        pnew = tmp;
+    }
+    if (gtid == 0) {
+        P.out[0] = (double)it;
+        P.out[1] = sqrt(rs);
+    }
+}
+
+// --------------------------------------------------------------- stats
+// out[0] = ||A x - b||^2, out[1] = ||A^T y + z - c||^2, out[2] = c.x, out[3] = b.y
+__global__ void stats_kernel(const double *__restrict__ Ax, const double *__restrict__ b,
+                             const double *__restrict__ ATy, const double *__restrict__ z,
+                             const double *__restrict__ c, const double *__restrict__ x,
+                             const double *__restrict__ y, int64_t np, int64_t nd,
+                             double *__restrict__ partials, unsigned int *counter,
+                             double *__restrict__ out, int *status) {
+    __shared__ double red[32];
+    __shared__ bool last;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t j = gtid; j < nd; j += stride) {
+        const double d = Ax[j] - b[j];
+        s[0] += d * d;
+        s[3] += b[j] * y[j];
+    }
+    for (int64_t i = gtid; i < np; i += stride) {
+        const double d = ATy[i] + z[i] - c[i];
+        s[1] += d * d;
+        s[2] += c[i] * x[i];
+    }
+    for (int k = 0; k < 4; k++) {
+        const double v = block_sum(s[k], red);
+        if (threadIdx.x == 0) partials[k * gridDim.x + blockIdx.x] = v;
+    }
+    __threadfence();
+    if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int k = 0; k < 4; k++) {
+        double v = 0.0;
+        if (threadIdx.x < 32) {
+            for (int i = threadIdx.x; i < (int)gridDim.x; i += 32)
+                v += *((volatile double *)(partials + k * gridDim.x + i));
+            v = warp_sum(v);
+        }
+        if (threadIdx.x == 0) {
+            out[k] = v;
+            if (!(v == v) || v - v != 0.0) atomicExch(status, kStatusNan);
+        }
+    }
+    if (threadIdx.x == 0) *counter = 0u;
+}
+
+// --------------------------------------------------------- projection
+// Round-robin ("circle method") pairing of np (even) indices: in step s the
+// fixed index np-1 meets s and, for k >= 1, (s+k) meets (s-k) mod (np-1).
+__device__ __forceinline__ void rr_pair(int s, int k, int np, int &p, int &q) {
+    const int m1 = np - 1;
+    int a, b;
+    if (k == 0) {
+        a = m1;
+        b = s;
+    } else {
+        a = (s + k) % m1;
+        b = (s - k + m1) % m1;
+    }
+    p = a < b ? a : b;
+    q = a < b ? b : a;
+}
+
+// One CTA per PSD block (n <= kJacobiMaxDim).  The symmetrised block is
+// diagonalised in shared memory by parallel cyclic Jacobi (sym.schur2
+// rotations, Golub & Van Loan sec. 8.5); the rotations of every sweep are
+// recorded in global scratch and replayed afterwards on V^T held in the same
+// shared buffer, so only one n x n matrix is resident at a time.
+__global__ void __launch_bounds__(kJacobiThreads)
+    jacobi_project_kernel(const double *__restrict__ U, double *__restrict__ xo,
+                          double *__restrict__ zo, double mu, const int64_t *__restrict__ boff,
+                          const int *__restrict__ bdim, double2 *__restrict__ rot,
+                          const int64_t *__restrict__ rot_off, int max_sweeps, double rel_tol,
+                          int *status, int *sweeps_out) {
+    extern __shared__ double sm[];
+    const int blk = blockIdx.x;
+    const int n = bdim[blk];
+    if (n <= 0) return;
+    const int64_t off = boff[blk];
+    const int np = n + (n & 1);
+    const int m = np / 2;
+    double *T = sm;                              // np*np
+    double2 *cs = (double2 *)(T + (size_t)np * np);  // m
+    double *lam = (double *)(cs + m);            // np
+    __shared__ double red[32];
+    __shared__ int nrot;
+    __shared__ double s_tol;
+
+    const double *Ub = U + off;
+    double fro = 0.0;
+    for (int e = threadIdx.x; e < np * np; e += blockDim.x) {
+        const int i = e / np, j = e % np;
+        double v = 0.0;
+        if (i < n && j < n) v = 0.5 * (Ub[(int64_t)i * n + j] + Ub[(int64_t)j * n + i]);
+        T[e] = v;
+        fro += v * v;
+    }
+    fro = block_sum(fro, red);
+    if (threadIdx.x == 0) s_tol = rel_tol * sqrt(fro) + 1e-300;
+    __syncthreads();
+    const double tol = s_tol;
+
+    double2 *rb = rot + rot_off[blk];
+    int sweep = 0;
+    for (; sweep < max_sweeps; sweep++) {
+        if (threadIdx.x == 0) nrot = 0;
+        __syncthreads();
+        for (int st = 0; st < np - 1; st++) {
+            for (int k = threadIdx.x; k < m; k += blockDim.x) {
+                int p, q;
+                rr_pair(st, k, np, p, q);
+                double c = 1.0, s = 0.0;
+                if (q < n) {
+                    const double apq = T[p * np + q];
+                    if (fabs(apq) > tol) {
+                        const double app = T[p * np + p], aqq = T[q * np + q];
+                        const double tau = (aqq - app) / (2.0 * apq);
+                        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + hypot(1.0, tau));
+                        c = 1.0 / sqrt(1.0 + t * t);
+                        s = t * c;
+                        atomicAdd(&nrot, 1);
+                    }
+                }
+                cs[k] = make_double2(c, s);
+                rb[((int64_t)sweep * (np - 1) + st) * m + k] = make_double2(c, s);
+            }
+            __syncthreads();
+            // every element belongs to exactly one 2x2 block (P, Q), P <= Q
+            for (int it = threadIdx.x; it < m * m; it += blockDim.x) {
+                const int P = it / m, Q = it % m;
+                if (P > Q) continue;
+                const double2 cp = cs[P], cq = cs[Q];
+                int pP, qP, pQ, qQ;
+                rr_pair(st, P, np, pP, qP);
+                rr_pair(st, Q, np, pQ, qQ);
+                const double b11 = T[pP * np + pQ], b12 = T[pP * np + qQ];
+                const double b21 = T[qP * np + pQ], b22 = T[qP * np + qQ];
+                const double m11 = b11 * cq.x - b12 * cq.y, m12 = b11 * cq.y + b12 * cq.x;
+                const double m21 = b21 * cq.x - b22 * cq.y, m22 = b21 * cq.y + b22 * cq.x;
+                double n11 = cp.x * m11 - cp.y * m21, n12 = cp.x * m12 - cp.y * m22;
+                double n21 = cp.y * m11 + cp.x * m21, n22 = cp.y * m12 + cp.x * m22;
+                if (P == Q) {
+                    if (cp.y != 0.0) { n12 = 0.0; n21 = 0.0; }
+                    T[pP * np + pP] = n11;
+                    T[pP * np + qP] = n12;
+                    T[qP * np + pP] = n21;
+                    T[qP * np + qP] = n22;
+                } else {
+                    T[pP * np + pQ] = n11; T[pQ * np + pP] = n11;
+                    T[pP * np + qQ] = n12; T[qQ * np + pP] = n12;
+                    T[qP * np + pQ] = n21; T[pQ * np + qP] = n21;
+                    T[qP * np + qQ] = n22; T[qQ * np + qP] = n22;
+                }
+            }
+            __syncthreads();
+        }
+        const int done = (nrot == 0);
+        __syncthreads();
+        if (done) {
+            sweep++;
+            break;
+        }
+    }
+    if (threadIdx.x == 0) {
+        if (sweeps_out) sweeps_out[blk] = sweep;
+        if (sweep >= max_sweeps && nrot != 0) atomicMax(status, 1);   // not converged: flag only
+    }
+    for (int i = threadIdx.x; i < np; i += blockDim.x) lam[i] = T[i * np + i];
+    __syncthreads();
+
+    // replay: V^T (rows = eigenvectors) starts as the identity
+    double *Vt = T;
+    for (int e = threadIdx.x; e < np * np; e += blockDim.x) Vt[e] = (e / np == e % np) ? 1.0 : 0.0;
+    __syncthreads();
+    for (int sw = 0; sw < sweep; sw++) {
+        for (int st = 0; st < np - 1; st++) {
+            const double2 *rs = rb + ((int64_t)sw * (np - 1) + st) * m;
+            for (int it = threadIdx.x; it < m * np; it += blockDim.x) {
+                const int k = it / np, j = it % np;
+                const double2 r = __ldg(rs + k);
+                if (r.y == 0.0) continue;
+                int p, q;
+                rr_pair(st, k, np, p, q);
+                const double vp = Vt[p * np + j], vq = Vt[q * np + j];
+                Vt[p * np + j] = r.x * vp - r.y * vq;
+                Vt[q * np + j] = r.y * vp + r.x * vq;
+            }
+            __syncthreads();
+        }
+    }
+
+    // U+ = sum_k lam_k^+ v_k v_k^T; x = U+ / mu; z = U+ - sym(U)
+    const double inv_mu = 1.0 / mu;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int i = e / n, j = e % n;
+        double acc = 0.0;
+        for (int k = 0; k < n; k++) {
+            const double l = lam[k];
+            if (l > 0.0) acc += l * Vt[k * np + i] * Vt[k * np + j];
+        }
+        const double us = 0.5 * (Ub[(int64_t)i * n + j] + Ub[(int64_t)j * n + i]);
+        xo[off + e] = acc * inv_mu;
+        zo[off + e] = acc - us;
+    }
+}
+
+}  // namespace v2b

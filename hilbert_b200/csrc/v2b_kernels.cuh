@@ -1,0 +1,70 @@
+// Kernel declarations and launch parameters for the B200 v2RDM path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "v2b_device.cuh"
+
+namespace v2b {
+
+constexpr int kSpmvThreads = 256;
+constexpr int kCgThreads = 512;
+constexpr int kJacobiThreads = 512;
+constexpr int kJacobiMaxDim = 160;     // np*np doubles + rotations must fit in 227 KB
+constexpr int kStatsBlocks = 256;
+
+struct Palette {
+    double v[16];
+};
+
+struct CgParams {
+    const uint32_t *a_rp, *a_ent;   // A   (rows = dual constraints)
+    const uint32_t *t_rp, *t_ent;   // A^T (rows = primal variables)
+    Palette palA, palT;
+    int64_t np, nd;
+    const double *Ax, *Acz, *b;     // rhs = Acz + mu (b - Ax)
+    double mu;
+    double *y, *r, *p0, *p1, *t, *q;
+    double *partials;               // >= gridDim.x
+    GridBarrier *bar;
+    int *status;
+    long long spin_limit;
+    double tol;
+    int maxit;
+    double *out;                    // out[0] = iterations, out[1] = final ||r||
+};
+
+__global__ void spmv_kernel(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ent,
+                            int64_t nrows, const double *__restrict__ x, double *__restrict__ y,
+                            Palette pal);
+__global__ void spmv_A2_kernel(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ent,
+                               int64_t nrows, const double *__restrict__ x,
+                               const double *__restrict__ c, const double *__restrict__ z,
+                               double *__restrict__ Ax, double *__restrict__ Acz, Palette pal);
+__global__ void spmv_AT_U_kernel(const uint32_t *__restrict__ rp,
+                                 const uint32_t *__restrict__ ent, int64_t nrows,
+                                 const double *__restrict__ y, const double *__restrict__ x,
+                                 const double *__restrict__ c, double mu,
+                                 double *__restrict__ ATy, double *__restrict__ U, Palette pal);
+__global__ void cg_kernel(CgParams P);
+__global__ void stats_kernel(const double *__restrict__ Ax, const double *__restrict__ b,
+                             const double *__restrict__ ATy, const double *__restrict__ z,
+                             const double *__restrict__ c, const double *__restrict__ x,
+                             const double *__restrict__ y, int64_t np, int64_t nd,
+                             double *__restrict__ partials, unsigned int *counter,
+                             double *__restrict__ out, int *status);
+__global__ void jacobi_project_kernel(const double *__restrict__ U, double *__restrict__ xo,
+                                      double *__restrict__ zo, double mu,
+                                      const int64_t *__restrict__ boff,
+                                      const int *__restrict__ bdim, double2 *__restrict__ rot,
+                                      const int64_t *__restrict__ rot_off, int max_sweeps,
+                                      double rel_tol, int *status, int *sweeps_out);
+
+inline size_t jacobi_smem_bytes(int n) {
+    const int np = n + (n & 1);
+    return (size_t)np * np * sizeof(double) + (size_t)(np / 2) * sizeof(double2) +
+           (size_t)np * sizeof(double);
+}
+
+}  // namespace v2b

@@ -1,0 +1,719 @@
+// Host orchestration of the B200 boundary-point iteration and the C ABI
+// declared in include/v2rdm_b200.h.
+//
+// Outer protocol (hilbert v2rdm_solver.cc:1296-1361 with libsdp's BPSDP):
+//   mu0 = 0.1; each solve() call runs up to MU_UPDATE_FREQUENCY iterations
+//   with mu fixed, then mu <- mu * eps_p / eps_d.
+// One iteration on the device:
+//   cg_kernel          (A A^T) y = A(c - z) + mu (b - A x)       [cooperative]
+//   spmv_AT_U_kernel   A^T y, U = mu x + A^T y - c
+//   jacobi_project     x = U+ / mu, z = U+ - U   per PSD block
+//   spmv_A2_kernel     A x, A (c - z)  (reused by the next iteration's rhs)
+//   stats_kernel       eps_p, eps_d, c.x, b.y  -> pinned host readback
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "v2b_kernels.cuh"
+#include "v2rdm_b200.h"
+#include "v2rdm_problem.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Failure : std::runtime_error {
+    int code;
+    Failure(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define V2B_CK(call)                                                                      \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            throw Failure(V2B_CUDA_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class F>
+int guarded(F &&f) {
+    try {
+        return f();
+    } catch (const Failure &e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::invalid_argument &e) {
+        g_last_error = e.what();
+        return V2B_BAD_ARG;
+    } catch (const std::exception &e) {
+        g_last_error = e.what();
+        return V2B_INTERNAL;
+    }
+}
+
+template <class T>
+T *dalloc(size_t n) {
+    void *p = nullptr;
+    V2B_CK(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+    return (T *)p;
+}
+
+void ensure_device() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+        throw Failure(V2B_NO_DEVICE, "no CUDA device available");
+}
+
+struct DeviceOp {
+    uint32_t *rp = nullptr, *ent = nullptr;
+    int64_t nrows = 0;
+    size_t nnz = 0;
+    v2b::Palette pal{};
+    void upload(const v2b::PackedOperator &op) {
+        nrows = op.nrows;
+        nnz = op.entries.size();
+        rp = dalloc<uint32_t>(op.row_ptr.size());
+        ent = dalloc<uint32_t>(nnz);
+        V2B_CK(cudaMemcpy(rp, op.row_ptr.data(), op.row_ptr.size() * 4, cudaMemcpyHostToDevice));
+        V2B_CK(cudaMemcpy(ent, op.entries.data(), nnz * 4, cudaMemcpyHostToDevice));
+        for (int i = 0; i < 16; i++) pal.v[i] = i < (int)op.palette.size() ? op.palette[i] : 0.0;
+    }
+    void release() {
+        cudaFree(rp);
+        cudaFree(ent);
+        rp = ent = nullptr;
+    }
+};
+
+// Per-block projection resources for a fixed list of block sizes.
+struct ProjectPlan {
+    std::vector<int> dims;
+    int nblk = 0;
+    int64_t total = 0;
+    int64_t *boff = nullptr;
+    int *bdim = nullptr;
+    double2 *rot = nullptr;
+    int64_t *rot_off = nullptr;
+    int *sweeps = nullptr;
+    size_t smem = 0;
+    int max_sweeps = 30;
+
+    void build(const std::vector<int> &d) {
+        dims = d;
+        nblk = (int)d.size();
+        std::vector<int64_t> off(nblk), roff(nblk);
+        int64_t o = 0, ro = 0;
+        smem = 0;
+        for (int i = 0; i < nblk; i++) {
+            if (d[i] < 0) throw std::invalid_argument("negative block dimension");
+            if (d[i] > v2b::kJacobiMaxDim)
+                throw std::invalid_argument("PSD block of dimension " + std::to_string(d[i]) +
+                                            " exceeds the shared-memory eigensolver limit " +
+                                            std::to_string(v2b::kJacobiMaxDim));
+            off[i] = o;
+            o += (int64_t)d[i] * d[i];
+            const int np = d[i] + (d[i] & 1);
+            roff[i] = ro;
+            ro += (int64_t)max_sweeps * std::max(np - 1, 0) * (np / 2);
+            smem = std::max(smem, v2b::jacobi_smem_bytes(d[i]));
+        }
+        total = o;
+        boff = dalloc<int64_t>(nblk);
+        bdim = dalloc<int>(nblk);
+        rot_off = dalloc<int64_t>(nblk);
+        rot = dalloc<double2>(ro);
+        sweeps = dalloc<int>(nblk);
+        V2B_CK(cudaMemcpy(boff, off.data(), nblk * 8, cudaMemcpyHostToDevice));
+        V2B_CK(cudaMemcpy(bdim, d.data(), nblk * 4, cudaMemcpyHostToDevice));
+        V2B_CK(cudaMemcpy(rot_off, roff.data(), nblk * 8, cudaMemcpyHostToDevice));
+        V2B_CK(cudaFuncSetAttribute(v2b::jacobi_project_kernel,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    void release() {
+        cudaFree(boff); cudaFree(bdim); cudaFree(rot); cudaFree(rot_off); cudaFree(sweeps);
+        boff = nullptr; bdim = nullptr; rot = nullptr; rot_off = nullptr; sweeps = nullptr;
+    }
+    void launch(const double *U, double mu, double *x, double *z, int *status, cudaStream_t s,
+                long &launches) {
+        if (nblk == 0) return;
+        v2b::jacobi_project_kernel<<<nblk, v2b::kJacobiThreads, smem, s>>>(
+            U, x, z, mu, boff, bdim, rot, rot_off, max_sweeps, 1e-14, status, sweeps);
+        V2B_CK(cudaGetLastError());
+        launches++;
+    }
+};
+
+int sm_count() {
+    int dev = 0, n = 0;
+    V2B_CK(cudaGetDevice(&dev));
+    V2B_CK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    return n;
+}
+
+}  // namespace
+
+// ====================================================================
+// device-map problem
+// ====================================================================
+struct v2b_problem {
+    v2b::Problem prob;
+    DeviceOp A, AT;
+    ProjectPlan plan;
+    cudaStream_t stream = nullptr;
+    double *x = nullptr, *b = nullptr, *c = nullptr, *y = nullptr, *z = nullptr;
+    double *Ax = nullptr, *Acz = nullptr, *ATy = nullptr, *U = nullptr;
+    double *r = nullptr, *p0 = nullptr, *p1 = nullptr, *t = nullptr, *q = nullptr;
+    double *partials = nullptr, *cg_out = nullptr, *stats = nullptr, *stats_partials = nullptr;
+    unsigned int *stats_counter = nullptr;
+    v2b::GridBarrier *bar = nullptr;
+    int *status = nullptr;   // [0] fatal device status, [1] projection sweeps exhausted
+    double *h_readback = nullptr;   // pinned: stats[4], cg_out[2], status[2]
+    int cg_grid = 0;
+    double mu = 0.1;
+    long launches = 0;
+
+    // optional per-kernel-class CUDA-event timing on the launching stream
+    // classes: 0 cg_kernel, 1 spmv_AT_U, 2 jacobi_project, 3 spmv_A2, 4 stats
+    static constexpr int kClasses = 5;
+    bool profiling = false;
+    cudaEvent_t ev[2 * kClasses] = {};
+    double prof_ms[kClasses] = {};
+    long prof_n[kClasses] = {};
+    void mark(int cls, int edge) {
+        if (profiling) V2B_CK(cudaEventRecord(ev[2 * cls + edge], stream));
+    }
+    void collect() {
+        if (!profiling) return;
+        for (int k = 0; k < kClasses; k++) {
+            float ms = 0.f;
+            V2B_CK(cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]));
+            prof_ms[k] += ms;
+            prof_n[k] += 1;
+        }
+    }
+    void set_profiling(bool on) {
+        if (on && !ev[0])
+            for (auto &e : ev) V2B_CK(cudaEventCreate(&e));
+        profiling = on;
+        for (int k = 0; k < kClasses; k++) { prof_ms[k] = 0.0; prof_n[k] = 0; }
+    }
+
+    ~v2b_problem() {
+        if (!on_device) return;
+        A.release();
+        AT.release();
+        plan.release();
+        for (double *p : {x, b, c, y, z, Ax, Acz, ATy, U, r, p0, p1, t, q, partials, cg_out, stats,
+                          stats_partials})
+            cudaFree(p);
+        cudaFree(stats_counter);
+        cudaFree(bar);
+        cudaFree(status);
+        if (h_readback) cudaFreeHost(h_readback);
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    // host operator tables, built once at creation
+    v2b::PackedOperator hostA, hostAT;
+    bool on_device = false;
+
+    // device resources are created on first device use, so that the host-side
+    // problem (sizes, b, c, guesses, operator tables) needs no GPU
+    void setup() {
+        if (on_device) return;
+        ensure_device();
+        V2B_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        A.upload(hostA);
+        AT.upload(hostAT);
+        plan.build(prob.dims);
+        const int64_t np = prob.n_primal, nd = prob.n_dual;
+        x = dalloc<double>(np); c = dalloc<double>(np); z = dalloc<double>(np);
+        ATy = dalloc<double>(np); U = dalloc<double>(np); t = dalloc<double>(np);
+        b = dalloc<double>(nd); y = dalloc<double>(nd); Ax = dalloc<double>(nd);
+        Acz = dalloc<double>(nd); r = dalloc<double>(nd); p0 = dalloc<double>(nd);
+        p1 = dalloc<double>(nd); q = dalloc<double>(nd);
+        int per_sm = 0;
+        V2B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v2b::cg_kernel,
+                                                             v2b::kCgThreads, 0));
+        if (per_sm < 1) throw Failure(V2B_INTERNAL, "cg_kernel cannot be resident");
+        cg_grid = sm_count() * std::min(per_sm, 2);
+        partials = dalloc<double>(std::max(cg_grid, 4 * v2b::kStatsBlocks));
+        stats_partials = dalloc<double>(4 * v2b::kStatsBlocks);
+        cg_out = dalloc<double>(2);
+        stats = dalloc<double>(4);
+        stats_counter = dalloc<unsigned int>(1);
+        bar = dalloc<v2b::GridBarrier>(1);
+        status = dalloc<int>(2);
+        V2B_CK(cudaMemset(stats_counter, 0, 4));
+        V2B_CK(cudaMemset(status, 0, 8));
+        V2B_CK(cudaMallocHost(&h_readback, 8 * sizeof(double)));
+        on_device = true;
+    }
+
+    int grid_for(int64_t rows, int threads) const {
+        const int64_t g = (rows + threads - 1) / threads;
+        return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 16));
+    }
+
+    void Au(const double *in, double *out, cudaStream_t s) {
+        v2b::spmv_kernel<<<grid_for(A.nrows, v2b::kSpmvThreads), v2b::kSpmvThreads, 0, s>>>(
+            A.rp, A.ent, A.nrows, in, out, A.pal);
+        V2B_CK(cudaGetLastError());
+        launches++;
+    }
+    void ATu(const double *in, double *out, cudaStream_t s) {
+        v2b::spmv_kernel<<<grid_for(AT.nrows, v2b::kSpmvThreads), v2b::kSpmvThreads, 0, s>>>(
+            AT.rp, AT.ent, AT.nrows, in, out, AT.pal);
+        V2B_CK(cudaGetLastError());
+        launches++;
+    }
+
+    void launch_cg(double tol, int maxit) {
+        V2B_CK(cudaMemsetAsync(bar, 0, sizeof(v2b::GridBarrier), stream));
+        v2b::CgParams P;
+        P.a_rp = A.rp; P.a_ent = A.ent; P.t_rp = AT.rp; P.t_ent = AT.ent;
+        P.palA = A.pal; P.palT = AT.pal;
+        P.np = prob.n_primal; P.nd = prob.n_dual;
+        P.Ax = Ax; P.Acz = Acz; P.b = b; P.mu = mu;
+        P.y = y; P.r = r; P.p0 = p0; P.p1 = p1; P.t = t; P.q = q;
+        P.partials = partials; P.bar = bar; P.status = status;
+        P.spin_limit = 20000000LL;   // ~2.5 s of 128 ns polls
+        P.tol = tol; P.maxit = maxit; P.out = cg_out;
+        void *args[] = {&P};
+        V2B_CK(cudaLaunchCooperativeKernel((const void *)v2b::cg_kernel, dim3(cg_grid),
+                                           dim3(v2b::kCgThreads), args, 0, stream));
+        launches++;
+    }
+
+    // one boundary-point iteration; returns {iters, eps_p, eps_d, E_p, E_d}
+    void iterate(const v2b_sdp_options &o, double out[5]) {
+        const int64_t np = prob.n_primal, nd = prob.n_dual;
+        mark(0, 0);
+        launch_cg(o.cg_convergence, o.cg_maxiter);
+        mark(0, 1);
+        mark(1, 0);
+        v2b::spmv_AT_U_kernel<<<grid_for(np, v2b::kSpmvThreads), v2b::kSpmvThreads, 0, stream>>>(
+            AT.rp, AT.ent, np, y, x, c, mu, ATy, U, AT.pal);
+        V2B_CK(cudaGetLastError());
+        launches++;
+        mark(1, 1);
+        mark(2, 0);
+        plan.launch(U, mu, x, z, status + 1, stream, launches);
+        mark(2, 1);
+        mark(3, 0);
+        v2b::spmv_A2_kernel<<<grid_for(nd, v2b::kSpmvThreads), v2b::kSpmvThreads, 0, stream>>>(
+            A.rp, A.ent, nd, x, c, z, Ax, Acz, A.pal);
+        V2B_CK(cudaGetLastError());
+        launches++;
+        mark(3, 1);
+        mark(4, 0);
+        v2b::stats_kernel<<<v2b::kStatsBlocks, 256, 0, stream>>>(Ax, b, ATy, z, c, x, y, np, nd,
+                                                                 stats_partials, stats_counter,
+                                                                 stats, status);
+        V2B_CK(cudaGetLastError());
+        launches++;
+        mark(4, 1);
+        V2B_CK(cudaMemcpyAsync(h_readback, stats, 4 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        V2B_CK(cudaMemcpyAsync(h_readback + 4, cg_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        V2B_CK(cudaMemcpyAsync(h_readback + 6, status, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        V2B_CK(cudaStreamSynchronize(stream));
+        collect();
+        const int *st = (const int *)(h_readback + 6);
+        if (st[0] == V2B_DEVICE_TIMEOUT)
+            throw Failure(V2B_DEVICE_TIMEOUT, "grid barrier wait gave up in cg_kernel");
+        if (st[0] == V2B_NAN) throw Failure(V2B_NAN, "non-finite value in the iteration");
+        out[0] = h_readback[4];
+        out[1] = std::sqrt(h_readback[0]);
+        out[2] = std::sqrt(h_readback[1]);
+        out[3] = h_readback[2];
+        out[4] = h_readback[3];
+    }
+
+    int solve_device(const v2b_sdp_options &o, int muf, v2b_sdp_monitor monitor, int print_level,
+                     void *data, long *oiter_out, long *iiter_out, double *energy) {
+        if (muf < 1) throw std::invalid_argument("mu_update_frequency must be >= 1");
+        const int64_t np = prob.n_primal, nd = prob.n_dual;
+        mu = 0.1;
+        V2B_CK(cudaMemsetAsync(y, 0, nd * 8, stream));
+        V2B_CK(cudaMemsetAsync(z, 0, np * 8, stream));
+        V2B_CK(cudaMemsetAsync(status, 0, 8, stream));
+        v2b::spmv_A2_kernel<<<grid_for(nd, v2b::kSpmvThreads), v2b::kSpmvThreads, 0, stream>>>(
+            A.rp, A.ent, nd, x, c, z, Ax, Acz, A.pal);
+        V2B_CK(cudaGetLastError());
+        launches++;
+        long oiter = 0, iiter = 0;
+        bool converged = false;
+        double res[5] = {0, 0, 0, 0, 0};
+        while (!converged && oiter < o.maxiter) {
+            const long budget = std::min<long>(muf, o.maxiter - oiter);
+            for (long k = 0; k < budget; k++) {
+                iterate(o, res);
+                const int it = (int)res[0];
+                if (monitor) monitor(print_level, (int)oiter, it, res[3], res[4], mu, res[1], res[2], data);
+                oiter++;
+                iiter += it;
+                converged = res[1] < o.sdp_error_convergence && res[2] < o.sdp_error_convergence &&
+                            std::fabs(res[3] - res[4]) < o.sdp_objective_convergence;
+                if (converged) break;
+            }
+            if (!converged && res[2] > 0.0) mu = mu * res[1] / res[2];
+        }
+        if (oiter_out) *oiter_out = oiter;
+        if (iiter_out) *iiter_out = iiter;
+        if (energy) *energy = res[3];
+        return converged ? V2B_OK : V2B_NOT_CONVERGED;
+    }
+};
+
+// ====================================================================
+// libsdp-shaped solver with host callbacks
+// ====================================================================
+struct v2b_bpsdp {
+    long np = 0, nd = 0;
+    v2b_sdp_options opt{};
+    double mu = 0.1;
+    std::vector<double> y, z;
+    long iiter = 0, oiter = 0;
+    bool converged = false;
+    ProjectPlan plan;
+    cudaStream_t stream = nullptr;
+    double *dU = nullptr, *dx = nullptr, *dz = nullptr;
+    int *status = nullptr;
+    long launches = 0;
+
+    ~v2b_bpsdp() {
+        if (!stream) return;
+        plan.release();
+        cudaFree(dU); cudaFree(dx); cudaFree(dz); cudaFree(status);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    void ensure_plan(const std::vector<int> &dims) {
+        if (dims == plan.dims && dU) return;
+        int64_t tot = 0;
+        for (int d : dims) tot += (int64_t)d * d;
+        if (tot != np) throw std::invalid_argument("sum of squared block dimensions != n_primal");
+        plan.release();
+        plan.build(dims);
+        if (!dU) {
+            dU = dalloc<double>(np); dx = dalloc<double>(np); dz = dalloc<double>(np);
+            status = dalloc<int>(2);
+            V2B_CK(cudaMemset(status, 0, 8));
+        }
+    }
+
+    int solve(double *x, const double *b, const double *c, const std::vector<int> &dims, int maxiter,
+              v2b_sdp_callback Au, v2b_sdp_callback ATu, v2b_sdp_monitor monitor, int print_level,
+              void *data) {
+        ensure_plan(dims);
+        std::vector<double> Ax(nd), Acz(nd), rhs(nd), r(nd), p(nd), Ap(nd), tmp_p(np), w(np);
+        std::vector<double> ATy(np), U(np);
+        auto dot = [](const std::vector<double> &a, const std::vector<double> &bb) {
+            double s = 0.0;
+            for (size_t i = 0; i < a.size(); i++) s += a[i] * bb[i];
+            return s;
+        };
+        auto AAT = [&](std::vector<double> &in, std::vector<double> &out) {
+            ATu(tmp_p.data(), in.data(), data);
+            Au(out.data(), tmp_p.data(), data);
+        };
+        double ep = 0, ed = 0;
+        converged = false;
+        for (int it = 0; it < maxiter; it++) {
+            Au(Ax.data(), x, data);
+            for (long i = 0; i < np; i++) w[i] = c[i] - z[i];
+            Au(Acz.data(), w.data(), data);
+            for (long j = 0; j < nd; j++) rhs[j] = Acz[j] + mu * (b[j] - Ax[j]);
+            // conjugate gradients on A A^T, warm start from y
+            AAT(y, Ap);
+            for (long j = 0; j < nd; j++) { r[j] = rhs[j] - Ap[j]; p[j] = r[j]; }
+            double rs = dot(r, r);
+            int cg_it = 0;
+            while (std::sqrt(rs) >= opt.cg_convergence && cg_it < opt.cg_maxiter) {
+                AAT(p, Ap);
+                const double pAp = dot(p, Ap);
+                if (!(pAp > 0.0)) break;
+                const double alpha = rs / pAp;
+                for (long j = 0; j < nd; j++) { y[j] += alpha * p[j]; r[j] -= alpha * Ap[j]; }
+                const double rs_new = dot(r, r);
+                cg_it++;
+                if (std::sqrt(rs_new) < opt.cg_convergence) { rs = rs_new; break; }
+                const double beta = rs_new / rs;
+                for (long j = 0; j < nd; j++) p[j] = r[j] + beta * p[j];
+                rs = rs_new;
+            }
+            ATu(ATy.data(), y.data(), data);
+            for (long i = 0; i < np; i++) U[i] = mu * x[i] + ATy[i] - c[i];
+            V2B_CK(cudaMemcpyAsync(dU, U.data(), np * 8, cudaMemcpyHostToDevice, stream));
+            plan.launch(dU, mu, dx, dz, status + 1, stream, launches);
+            V2B_CK(cudaMemcpyAsync(x, dx, np * 8, cudaMemcpyDeviceToHost, stream));
+            V2B_CK(cudaMemcpyAsync(z.data(), dz, np * 8, cudaMemcpyDeviceToHost, stream));
+            V2B_CK(cudaStreamSynchronize(stream));
+            Au(Ax.data(), x, data);
+            double s0 = 0.0, s1 = 0.0, Ep = 0.0, Ed = 0.0;
+            for (long j = 0; j < nd; j++) { const double d = Ax[j] - b[j]; s0 += d * d; Ed += b[j] * y[j]; }
+            for (long i = 0; i < np; i++) { const double d = ATy[i] + z[i] - c[i]; s1 += d * d; Ep += c[i] * x[i]; }
+            ep = std::sqrt(s0);
+            ed = std::sqrt(s1);
+            if (!std::isfinite(ep) || !std::isfinite(ed)) throw Failure(V2B_NAN, "non-finite error norm");
+            iiter += cg_it;
+            if (monitor) monitor(print_level, (int)oiter, cg_it, Ep, Ed, mu, ep, ed, data);
+            oiter++;
+            converged = ep < opt.sdp_error_convergence && ed < opt.sdp_error_convergence &&
+                        std::fabs(Ep - Ed) < opt.sdp_objective_convergence;
+            if (converged) break;
+        }
+        if (!converged && ed > 0.0) mu = mu * ep / ed;
+        return converged ? V2B_OK : V2B_NOT_CONVERGED;
+    }
+};
+
+// ====================================================================
+// C ABI
+// ====================================================================
+extern "C" {
+
+const char *v2b_last_error(void) { return g_last_error.c_str(); }
+int v2b_version(void) { return 1; }
+
+int v2b_bpsdp_create(long n_primal, long n_dual, const v2b_sdp_options *options, v2b_bpsdp **out) {
+    return guarded([&] {
+        if (!out || !options || n_primal <= 0 || n_dual <= 0)
+            throw std::invalid_argument("v2b_bpsdp_create: bad arguments");
+        ensure_device();
+        std::unique_ptr<v2b_bpsdp> s(new v2b_bpsdp());
+        s->np = n_primal;
+        s->nd = n_dual;
+        s->opt = *options;
+        s->y.assign(n_dual, 0.0);
+        s->z.assign(n_primal, 0.0);
+        V2B_CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+        *out = s.release();
+        return V2B_OK;
+    });
+}
+
+int v2b_bpsdp_solve(v2b_bpsdp *s, double *x, const double *b, const double *c,
+                    const int *primal_block_dims, int n_blocks, int maxiter, v2b_sdp_callback Au,
+                    v2b_sdp_callback ATu, v2b_sdp_monitor monitor, int print_level, void *data) {
+    return guarded([&] {
+        if (!s || !x || !b || !c || !primal_block_dims || n_blocks <= 0 || !Au || !ATu || maxiter < 0)
+            throw std::invalid_argument("v2b_bpsdp_solve: bad arguments");
+        std::vector<int> dims(primal_block_dims, primal_block_dims + n_blocks);
+        return s->solve(x, b, c, dims, maxiter, Au, ATu, monitor, print_level, data);
+    });
+}
+
+int v2b_bpsdp_is_converged(const v2b_bpsdp *s) { return s && s->converged ? 1 : 0; }
+double v2b_bpsdp_get_mu(const v2b_bpsdp *s) { return s ? s->mu : NAN; }
+int v2b_bpsdp_set_mu(v2b_bpsdp *s, double mu) {
+    if (!s || !(mu > 0.0)) { g_last_error = "set_mu: mu must be positive"; return V2B_BAD_ARG; }
+    s->mu = mu;
+    return V2B_OK;
+}
+int v2b_bpsdp_get_y(const v2b_bpsdp *s, double *y) {
+    if (!s || !y) return V2B_BAD_ARG;
+    std::memcpy(y, s->y.data(), s->nd * 8);
+    return V2B_OK;
+}
+int v2b_bpsdp_get_z(const v2b_bpsdp *s, double *z) {
+    if (!s || !z) return V2B_BAD_ARG;
+    std::memcpy(z, s->z.data(), s->np * 8);
+    return V2B_OK;
+}
+int v2b_bpsdp_set_y(v2b_bpsdp *s, const double *y) {
+    if (!s || !y) return V2B_BAD_ARG;
+    std::memcpy(s->y.data(), y, s->nd * 8);
+    return V2B_OK;
+}
+int v2b_bpsdp_set_z(v2b_bpsdp *s, const double *z) {
+    if (!s || !z) return V2B_BAD_ARG;
+    std::memcpy(s->z.data(), z, s->np * 8);
+    return V2B_OK;
+}
+long v2b_bpsdp_iiter_total(const v2b_bpsdp *s) { return s ? s->iiter : -1; }
+long v2b_bpsdp_oiter_total(const v2b_bpsdp *s) { return s ? s->oiter : -1; }
+void v2b_bpsdp_destroy(v2b_bpsdp *s) { delete s; }
+
+int v2b_problem_create(int nmo, int nalpha, int nbeta, int positivity, int constrain_spin,
+                       int constrain_sz, int hubbard_multiplicity, v2b_problem **out) {
+    return guarded([&] {
+        if (!out) throw std::invalid_argument("v2b_problem_create: out is NULL");
+        v2b::ProblemSpec spec;
+        spec.nmo = nmo;
+        spec.nalpha = nalpha;
+        spec.nbeta = nbeta;
+        spec.positivity = positivity;
+        spec.constrain_spin = constrain_spin != 0;
+        spec.constrain_sz = constrain_sz != 0;
+        spec.hubbard_multiplicity = hubbard_multiplicity != 0;
+        std::unique_ptr<v2b_problem> p(new v2b_problem());
+        p->prob = v2b::make_problem(spec);
+        p->hostA = v2b::build_A(p->prob);
+        p->hostAT = v2b::build_AT(p->prob);
+        *out = p.release();
+        return V2B_OK;
+    });
+}
+
+void v2b_problem_destroy(v2b_problem *p) { delete p; }
+long v2b_problem_n_primal(const v2b_problem *p) { return p ? p->prob.n_primal : -1; }
+long v2b_problem_n_dual(const v2b_problem *p) { return p ? p->prob.n_dual : -1; }
+int v2b_problem_n_blocks(const v2b_problem *p) { return p ? (int)p->prob.dims.size() : -1; }
+int v2b_problem_block_dims(const v2b_problem *p, int *dims) {
+    if (!p || !dims) return V2B_BAD_ARG;
+    std::copy(p->prob.dims.begin(), p->prob.dims.end(), dims);
+    return V2B_OK;
+}
+int v2b_problem_build_b(const v2b_problem *p, double *b) {
+    return guarded([&] {
+        if (!p || !b) throw std::invalid_argument("build_b: NULL argument");
+        v2b::build_b(p->prob, b);
+        return V2B_OK;
+    });
+}
+int v2b_problem_build_c_hubbard(const v2b_problem *p, double t, double U, double *c) {
+    return guarded([&] {
+        if (!p || !c) throw std::invalid_argument("build_c_hubbard: NULL argument");
+        v2b::build_c_hubbard(p->prob, t, U, c);
+        return V2B_OK;
+    });
+}
+int v2b_problem_build_c_external(const v2b_problem *p, const double *h, const double *g, double *c) {
+    return guarded([&] {
+        if (!p || !h || !g || !c) throw std::invalid_argument("build_c_external: NULL argument");
+        v2b::build_c_external(p->prob, h, g, c);
+        return V2B_OK;
+    });
+}
+int v2b_problem_guess(const v2b_problem *p, int hf, double *x) {
+    return guarded([&] {
+        if (!p || !x) throw std::invalid_argument("guess: NULL argument");
+        if (hf) v2b::guess_hf(p->prob, x);
+        else v2b::guess_random(p->prob, x);
+        return V2B_OK;
+    });
+}
+int v2b_problem_Au(v2b_problem *p, const double *d_in, double *d_out, void *stream) {
+    return guarded([&] {
+        if (!p || !d_in || !d_out) throw std::invalid_argument("Au: NULL argument");
+        p->setup();
+        p->Au(d_in, d_out, (cudaStream_t)stream);
+        return V2B_OK;
+    });
+}
+int v2b_problem_ATu(v2b_problem *p, const double *d_in, double *d_out, void *stream) {
+    return guarded([&] {
+        if (!p || !d_in || !d_out) throw std::invalid_argument("ATu: NULL argument");
+        p->setup();
+        p->ATu(d_in, d_out, (cudaStream_t)stream);
+        return V2B_OK;
+    });
+}
+int v2b_problem_project(v2b_problem *p, const double *d_U, double mu, double *d_x, double *d_z,
+                        void *stream) {
+    return guarded([&] {
+        if (!p || !d_U || !d_x || !d_z || !(mu > 0.0)) throw std::invalid_argument("project: bad argument");
+        p->setup();
+        p->plan.launch(d_U, mu, d_x, d_z, p->status + 1, (cudaStream_t)stream, p->launches);
+        return V2B_OK;
+    });
+}
+int v2b_problem_solve_device(v2b_problem *p, double *d_x, const double *d_b, const double *d_c,
+                             const v2b_sdp_options *options, int mu_update_frequency,
+                             v2b_sdp_monitor monitor, int print_level, void *data, long *oiter,
+                             long *iiter, double *energy) {
+    return guarded([&] {
+        if (!p || !d_x || !d_b || !d_c || !options) throw std::invalid_argument("solve_device: NULL argument");
+        p->setup();
+        const int64_t np = p->prob.n_primal, nd = p->prob.n_dual;
+        V2B_CK(cudaMemcpyAsync(p->x, d_x, np * 8, cudaMemcpyDeviceToDevice, p->stream));
+        V2B_CK(cudaMemcpyAsync(p->b, d_b, nd * 8, cudaMemcpyDeviceToDevice, p->stream));
+        V2B_CK(cudaMemcpyAsync(p->c, d_c, np * 8, cudaMemcpyDeviceToDevice, p->stream));
+        const int rc = p->solve_device(*options, mu_update_frequency, monitor, print_level, data, oiter,
+                                       iiter, energy);
+        V2B_CK(cudaMemcpyAsync(d_x, p->x, np * 8, cudaMemcpyDeviceToDevice, p->stream));
+        V2B_CK(cudaStreamSynchronize(p->stream));
+        return rc;
+    });
+}
+int v2b_problem_solve(v2b_problem *p, double *x, const double *b, const double *c,
+                      const v2b_sdp_options *options, int mu_update_frequency,
+                      v2b_sdp_monitor monitor, int print_level, void *data, long *oiter, long *iiter,
+                      double *energy) {
+    return guarded([&] {
+        if (!p || !x || !b || !c || !options) throw std::invalid_argument("solve: NULL argument");
+        p->setup();
+        const int64_t np = p->prob.n_primal, nd = p->prob.n_dual;
+        V2B_CK(cudaMemcpyAsync(p->x, x, np * 8, cudaMemcpyHostToDevice, p->stream));
+        V2B_CK(cudaMemcpyAsync(p->b, b, nd * 8, cudaMemcpyHostToDevice, p->stream));
+        V2B_CK(cudaMemcpyAsync(p->c, c, np * 8, cudaMemcpyHostToDevice, p->stream));
+        const int rc = p->solve_device(*options, mu_update_frequency, monitor, print_level, data, oiter,
+                                       iiter, energy);
+        V2B_CK(cudaMemcpyAsync(x, p->x, np * 8, cudaMemcpyDeviceToHost, p->stream));
+        V2B_CK(cudaStreamSynchronize(p->stream));
+        return rc;
+    });
+}
+int v2b_problem_get_y(const v2b_problem *p, double *y) {
+    return guarded([&] {
+        if (!p || !y) throw std::invalid_argument("get_y: NULL argument");
+        if (!p->on_device) throw std::invalid_argument("get_y: no device solve has run");
+        V2B_CK(cudaMemcpy(y, p->y, p->prob.n_dual * 8, cudaMemcpyDeviceToHost));
+        return V2B_OK;
+    });
+}
+int v2b_problem_get_z(const v2b_problem *p, double *z) {
+    return guarded([&] {
+        if (!p || !z) throw std::invalid_argument("get_z: NULL argument");
+        if (!p->on_device) throw std::invalid_argument("get_z: no device solve has run");
+        V2B_CK(cudaMemcpy(z, p->z, p->prob.n_primal * 8, cudaMemcpyDeviceToHost));
+        return V2B_OK;
+    });
+}
+int v2b_problem_operator_size(const v2b_problem *p, int transposed, long *nrows, long *nnz,
+                              int *npalette) {
+    if (!p || !nrows || !nnz || !npalette) return V2B_BAD_ARG;
+    const v2b::PackedOperator &op = transposed ? p->hostAT : p->hostA;
+    *nrows = op.nrows;
+    *nnz = (long)op.entries.size();
+    *npalette = (int)op.palette.size();
+    return V2B_OK;
+}
+int v2b_problem_operator(const v2b_problem *p, int transposed, uint32_t *row_ptr, uint32_t *entries,
+                         double *palette) {
+    if (!p || !row_ptr || !entries || !palette) return V2B_BAD_ARG;
+    const v2b::PackedOperator &op = transposed ? p->hostAT : p->hostA;
+    std::copy(op.row_ptr.begin(), op.row_ptr.end(), row_ptr);
+    std::copy(op.entries.begin(), op.entries.end(), entries);
+    std::copy(op.palette.begin(), op.palette.end(), palette);
+    return V2B_OK;
+}
+double v2b_problem_get_mu(const v2b_problem *p) { return p ? p->mu : NAN; }
+long v2b_problem_kernel_launches(const v2b_problem *p) { return p ? p->launches : -1; }
+int v2b_problem_set_profiling(v2b_problem *p, int on) {
+    return guarded([&] {
+        if (!p) throw std::invalid_argument("set_profiling: NULL problem");
+        p->setup();
+        p->set_profiling(on != 0);
+        return V2B_OK;
+    });
+}
+int v2b_problem_profile(const v2b_problem *p, double *ms, long *launches) {
+    if (!p || !ms || !launches) return V2B_BAD_ARG;
+    for (int k = 0; k < v2b_problem::kClasses; k++) {
+        ms[k] = p->prof_ms[k];
+        launches[k] = p->prof_n[k];
+    }
+    return V2B_OK;
+}
+void *v2b_problem_stream(const v2b_problem *p) { return p ? (void *)p->stream : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,952 @@
+// Host problem builder for the B200 v2RDM path (see v2rdm_problem.h).
+//
+// The operator emitters walk the constraint families in the order of
+// hilbert's bpsdp_Au / bpsdp_ATu and record, for every dual row (A) or
+// primal element (A^T), its terms in the order the reference accumulates
+// them.  A gather that sums each row left to right with separate multiply
+// and add roundings therefore reproduces the reference's A.x and A^T.y.
+#include "v2rdm_problem.h"
+
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <stdexcept>
+
+namespace v2b {
+
+Problem make_problem(const ProblemSpec &spec) {
+    if (spec.nmo < 1 || spec.nalpha < 0 || spec.nbeta < 0 || spec.nalpha > spec.nmo ||
+        spec.nbeta > spec.nmo)
+        throw std::invalid_argument("invalid orbital / electron counts");
+    if (spec.positivity < POS_D || spec.positivity > POS_DQG)
+        throw std::invalid_argument("unsupported POSITIVITY");
+    Problem p;
+    p.spec = spec;
+    const int n = spec.nmo;
+    p.n = n;
+    p.gab = n * n;
+    p.gaa = n * (n - 1) / 2;
+    p.q2 = spec.positivity == POS_DQ || spec.positivity == POS_DQG;
+    p.g2 = spec.positivity == POS_DG || spec.positivity == POS_DQG;
+    p.mult = spec.hubbard_multiplicity ? 2 * (spec.nalpha - spec.nbeta) + 1
+                                       : (spec.nalpha - spec.nbeta) + 1;
+
+    // basis.cc:426-533 for one irrep: geminal number i*n + j holds the
+    // ordered pair (j, i); aa geminals are the pairs with first < second,
+    // numbered in the same sweep.
+    p.bas_ab.assign(2 * p.gab, -999);
+    p.bas_aa.assign(2 * (p.gaa > 0 ? p.gaa : 1), -999);
+    p.ibas_ab.assign(n * n, -999);
+    p.ibas_aa.assign(n * n, -999);
+    int count_aa = 0;
+    for (int second = 0; second < n; second++) {
+        for (int first = 0; first < n; first++) {
+            const int g = second * n + first;
+            p.ibas_ab[first * n + second] = g;
+            p.bas_ab[2 * g] = first;
+            p.bas_ab[2 * g + 1] = second;
+            if (first < second) {
+                p.ibas_aa[first * n + second] = count_aa;
+                p.ibas_aa[second * n + first] = count_aa;
+                p.bas_aa[2 * count_aa] = first;
+                p.bas_aa[2 * count_aa + 1] = second;
+                count_aa++;
+            }
+        }
+    }
+
+    int64_t off = 0;
+    auto add_block = [&](int64_t &where, int dim) {
+        where = off;
+        off += (int64_t)dim * dim;
+        p.dims.push_back(dim);
+        p.block_off.push_back(where);
+    };
+    const bool singlet = spec.nalpha == spec.nbeta;
+    add_block(p.d2ab, p.gab);
+    add_block(p.d2aa, p.gaa);
+    add_block(p.d2bb, p.gaa);
+    if (spec.constrain_spin) add_block(p.d200, singlet ? p.gab : 2 * p.gab);
+    add_block(p.d1a, n);
+    add_block(p.d1b, n);
+    add_block(p.q1a, n);
+    add_block(p.q1b, n);
+    if (p.q2) {
+        add_block(p.q2ab, p.gab);
+        add_block(p.q2aa, p.gaa);
+        add_block(p.q2bb, p.gaa);
+    }
+    if (p.g2) {
+        add_block(p.g2ab, p.gab);
+        add_block(p.g2ba, p.gab);
+        add_block(p.g2aa, 2 * p.gab);
+    }
+    p.n_primal = off;
+
+    const int64_t gab2 = (int64_t)p.gab * p.gab, gaa2 = (int64_t)p.gaa * p.gaa, n2 = (int64_t)n * n;
+    int64_t d = spec.constrain_sz ? 3 : 1;
+    d += 2 * gaa2 + gab2 + 2 * n2 + (spec.constrain_sz ? 4 : 2) * n2;
+    if (spec.constrain_spin) {
+        d += 1 + (singlet ? n2 + 3 * gaa2 + 2 * gab2 : 4 * gab2);
+        if (p.g2) d += 2 * (int64_t)p.gab;
+    }
+    if (p.q2) d += gab2 + 2 * gaa2;
+    if (p.g2) d += 6 * gab2;
+    p.n_dual = d;
+    if (p.n_primal > (int64_t)kColMask || p.n_dual > (int64_t)kColMask)
+        throw std::invalid_argument("problem too large for 27-bit packed column indices");
+    return p;
+}
+
+// ------------------------------------------------------------------ b, c, x
+void build_b(const Problem &p, double *b) {
+    const int n = p.n, gab = p.gab, gaa = p.gaa;
+    const double na = p.spec.nalpha, nb = p.spec.nbeta;
+    std::memset(b, 0, sizeof(double) * p.n_dual);
+    int64_t off = 0;
+    if (p.spec.constrain_sz) {
+        b[off++] = na * nb;
+        b[off++] = na * (na - 1.0);
+        b[off++] = nb * (nb - 1.0);
+    } else {
+        const double nt = na + nb;
+        b[off++] = nt * (nt - 1.0);
+    }
+    off += 2 * (int64_t)gaa * gaa + (int64_t)gab * gab;
+    for (int s = 0; s < 2; s++) {
+        for (int i = 0; i < n; i++) b[off + i * n + i] = 1.0;
+        off += (int64_t)n * n;
+    }
+    off += (p.spec.constrain_sz ? 4 : 2) * (int64_t)n * n;
+    if (p.spec.constrain_spin) {
+        const double ms = (p.mult - 1.0) / 2.0;
+        b[off++] = 0.5 * (na + nb) + ms * ms - ms * (ms + 1.0);
+        if (p.spec.nalpha == p.spec.nbeta)
+            off += (int64_t)n * n + 3 * (int64_t)gaa * gaa + 2 * (int64_t)gab * gab;
+        else
+            off += 4 * (int64_t)gab * gab;
+        if (p.g2) off += 2 * (int64_t)gab;
+    }
+    if (p.q2) {
+        for (int ij = 0; ij < gab; ij++) {
+            const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+            b[off + (int64_t)ij * gab + p.iab(i, j)] = -1.0;  // -d_ik d_jl
+        }
+        off += (int64_t)gab * gab;
+        for (int s = 0; s < 2; s++) {
+            for (int ij = 0; ij < gaa; ij++) {
+                const int i = p.bas_aa[2 * ij], j = p.bas_aa[2 * ij + 1];
+                for (int kl = 0; kl < gaa; kl++) {
+                    const int k = p.bas_aa[2 * kl], l = p.bas_aa[2 * kl + 1];
+                    b[off + (int64_t)ij * gaa + kl] = -(double)((i == k) && (j == l)) + (double)((i == l) && (j == k));
+                }
+            }
+            off += (int64_t)gaa * gaa;
+        }
+    }
+}
+
+namespace {
+// D1 from the upper triangle of h, as the packed one-electron buffer of
+// tei.cc:96-120 leaves it, plus the (zero) core contribution of tei.cc:236-270.
+void fill_d1(const Problem &p, const double *hsym, double *c) {
+    const int n = p.n;
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) {
+            const double v = hsym[(i < j ? i : j) * n + (i < j ? j : i)];
+            c[p.d1a + i * n + j] = v + 0.0;
+            c[p.d1b + i * n + j] = v + 0.0;
+        }
+}
+}  // namespace
+
+void build_c_hubbard(const Problem &p, double t, double U, double *c) {
+    const int n = p.n, gab = p.gab;
+    std::memset(c, 0, sizeof(double) * p.n_primal);
+    std::vector<double> h((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) {
+            const int d = std::abs(i - j);
+            if (d == 1 || d == n - 1) h[i * n + j] = -t;   // oei.cc:83-88
+        }
+    fill_d1(p, h.data(), c);
+    for (int i = 0; i < n; i++) {
+        const int ii = p.iab(i, i);
+        c[p.d2ab + (int64_t)ii * gab + ii] = U;             // tei.cc:285-292
+    }
+}
+
+void build_c_external(const Problem &p, const double *h, const double *g, double *c) {
+    const int64_t n = p.n;
+    const int gab = p.gab, gaa = p.gaa;
+    std::memset(c, 0, sizeof(double) * p.n_primal);
+    fill_d1(p, h, c);
+    for (int ij = 0; ij < gab; ij++) {
+        const int64_t i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+        for (int kl = 0; kl < gab; kl++) {
+            const int64_t k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+            c[p.d2ab + (int64_t)ij * gab + kl] = g[((i * n + k) * n + j) * n + l];
+        }
+    }
+    for (int ij = 0; ij < gaa; ij++) {
+        const int64_t i = p.bas_aa[2 * ij], j = p.bas_aa[2 * ij + 1];
+        for (int kl = 0; kl < gaa; kl++) {
+            const int64_t k = p.bas_aa[2 * kl], l = p.bas_aa[2 * kl + 1];
+            const double v = g[((i * n + k) * n + j) * n + l] - g[((i * n + l) * n + j) * n + k];
+            c[p.d2aa + (int64_t)ij * gaa + kl] = v;
+            c[p.d2bb + (int64_t)ij * gaa + kl] = v;
+        }
+    }
+}
+
+void guess_random(const Problem &p, double *x) {
+    // v2rdm_solver.cc:1799-1806 (C library rand() seeded with 0)
+    srand(0);
+    for (int64_t i = 0; i < p.n_primal; i++) x[i] = ((double)rand() / RAND_MAX - 1.0) * 2.0;
+}
+
+void guess_hf(const Problem &p, double *x) {
+    // v2rdm_solver.cc:1713-1823; the reference stores doccpi = nalpha for
+    // Hubbard / external problems, so both spins fill nalpha orbitals.
+    const int n = p.n, gab = p.gab, gaa = p.gaa, occ = p.spec.nalpha;
+    std::memset(x, 0, sizeof(double) * p.n_primal);
+    for (int i = 0; i < occ; i++)
+        for (int j = 0; j < occ; j++) {
+            const int ij = p.iab(i, j);
+            x[p.d2ab + (int64_t)ij * gab + ij] = 1.0;
+        }
+    for (int i = 0; i < occ; i++)
+        for (int j = 0; j < i; j++) {
+            const int ij = p.iaa(i, j);
+            x[p.d2aa + (int64_t)ij * gaa + ij] = 1.0;
+            x[p.d2bb + (int64_t)ij * gaa + ij] = 1.0;
+        }
+    for (int i = 0; i < occ; i++) {
+        x[p.d1a + i * n + i] = 1.0;
+        x[p.d1b + i * n + i] = 1.0;
+    }
+    for (int i = occ; i < n; i++) {
+        x[p.q1a + i * n + i] = 1.0;
+        x[p.q1b + i * n + i] = 1.0;
+    }
+    if (p.q2) {  // q2.cc:45-167
+        for (int ij = 0; ij < gab; ij++) {
+            const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                double dum = 0.0;
+                dum += x[p.d2ab + (int64_t)kl * gab + ij];
+                if (j == l) dum += x[p.q1a + i * n + k];
+                if (i == k) dum -= x[p.d1b + l * n + j];
+                x[p.q2ab + (int64_t)ij * gab + kl] = dum;
+            }
+        }
+        for (int s = 0; s < 2; s++) {
+            const int64_t d2 = s ? p.d2bb : p.d2aa, q2 = s ? p.q2bb : p.q2aa;
+            const int64_t q1 = s ? p.q1b : p.q1a, d1 = s ? p.d1b : p.d1a;
+            for (int ij = 0; ij < gaa; ij++) {
+                const int i = p.bas_aa[2 * ij], j = p.bas_aa[2 * ij + 1];
+                for (int kl = 0; kl < gaa; kl++) {
+                    const int k = p.bas_aa[2 * kl], l = p.bas_aa[2 * kl + 1];
+                    double dum = 0.0;
+                    dum += x[d2 + (int64_t)kl * gaa + ij];
+                    if (j == l) dum += x[q1 + i * n + k];
+                    if (j == k) dum += x[d1 + l * n + i];
+                    if (i == l) dum -= x[q1 + j * n + k];
+                    if (i == k) dum -= x[d1 + l * n + j];
+                    x[q2 + (int64_t)ij * gaa + kl] = dum;
+                }
+            }
+        }
+    }
+    if (p.g2) {  // g2.cc:44-242
+        for (int s = 0; s < 2; s++) {
+            const int64_t g = s ? p.g2ba : p.g2ab, d1 = s ? p.d1b : p.d1a;
+            for (int ij = 0; ij < gab; ij++) {
+                const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+                for (int kl = 0; kl < gab; kl++) {
+                    const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                    double dum = 0.0;
+                    if (j == l) dum += x[d1 + i * n + k];
+                    dum -= s ? x[p.d2ab + (int64_t)p.iab(l, i) * gab + p.iab(j, k)]
+                             : x[p.d2ab + (int64_t)p.iab(i, l) * gab + p.iab(k, j)];
+                    x[g + (int64_t)ij * gab + kl] = dum;
+                }
+            }
+        }
+        const int64_t w = 2 * (int64_t)gab;
+        for (int s = 0; s < 2; s++) {
+            const int64_t d1 = s ? p.d1b : p.d1a, d2 = s ? p.d2bb : p.d2aa, sh = s ? gab : 0;
+            for (int ij = 0; ij < gab; ij++) {
+                const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+                for (int kl = 0; kl < gab; kl++) {
+                    const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                    double dum = 0.0;
+                    if (j == l) dum += x[d1 + i * n + k];
+                    if (i != l && k != j) {
+                        const int sil = i < l ? 1 : -1, skj = k < j ? 1 : -1;
+                        dum -= x[d2 + (int64_t)p.iaa(i, l) * gaa + p.iaa(k, j)] * sil * skj;
+                    }
+                    x[p.g2aa + (sh + ij) * w + (sh + kl)] = dum;
+                }
+            }
+        }
+        for (int ij = 0; ij < gab; ij++) {
+            const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                x[p.g2aa + (int64_t)ij * w + (gab + kl)] = 0.0 + x[p.d2ab + (int64_t)p.iab(i, l) * gab + p.iab(j, k)];
+                x[p.g2aa + (gab + ij) * w + kl] = 0.0 + x[p.d2ab + (int64_t)p.iab(l, i) * gab + p.iab(k, j)];
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ emitters
+namespace {
+
+const double kSqrt2 = std::sqrt(2.0);
+
+// A (rows = dual constraints).  S::t(row, col, coef) appends a term to row's
+// running sum; S::g(row, col, coef) appends to the row's second partial sum
+// (rows the reference assembles as "first part + separately summed tail").
+template <class S>
+void visit_A(const Problem &p, S &s) {
+    const int n = p.n, gab = p.gab, gaa = p.gaa;
+    const double na = p.spec.nalpha, nb = p.spec.nbeta;
+    int64_t off = 0;
+    // d2.cc:316-378 traces
+    if (p.spec.constrain_sz) {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) { const int ij = p.iab(i, j); s.t(off, p.d2ab + (int64_t)ij * gab + ij, 1.0); }
+        off++;
+        for (int sp = 0; sp < 2; sp++) {
+            const int64_t d2 = sp ? p.d2bb : p.d2aa;
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j < n; j++) {
+                    if (i == j || gaa == 0) continue;
+                    const int ij = p.iaa(i, j);
+                    s.t(off, d2 + (int64_t)ij * gaa + ij, 1.0);
+                }
+            off++;
+        }
+    } else {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                int ij = p.iab(i, j);
+                s.t(off, p.d2ab + (int64_t)ij * gab + ij, 2.0);
+                if (i == j || gaa == 0) continue;
+                ij = p.iaa(i, j);
+                s.t(off, p.d2aa + (int64_t)ij * gaa + ij, 1.0);
+                s.t(off, p.d2bb + (int64_t)ij * gaa + ij, 1.0);
+            }
+        off++;
+    }
+    // d2.cc:380-414 hermiticity
+    const int64_t hb[3] = {p.d2aa, p.d2bb, p.d2ab};
+    const int hg[3] = {gaa, gaa, gab};
+    for (int sp = 0; sp < 3; sp++)
+        for (int64_t ij = 0; ij < hg[sp]; ij++)
+            for (int64_t kl = 0; kl < hg[sp]; kl++) {
+                s.t(off, hb[sp] + ij * hg[sp] + kl, 1.0);
+                s.t(off, hb[sp] + kl * hg[sp] + ij, -1.0);
+                off++;
+            }
+    // d2.cc:416-435 D1^T + Q1 = I
+    for (int sp = 0; sp < 2; sp++) {
+        const int64_t d1 = sp ? p.d1b : p.d1a, q1 = sp ? p.q1b : p.q1a;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                s.t(off + i * n + j, d1 + j * n + i, 1.0);
+                s.t(off + i * n + j, q1 + i * n + j, 1.0);
+            }
+        off += (int64_t)n * n;
+    }
+    // d2.cc:441-591 partial traces
+    auto contract_ab = [&](int sp, double f, int64_t d1) {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                const int64_t row = off + i * n + j;
+                s.t(row, d1 + i * n + j, f);
+                for (int k = 0; k < n; k++) {
+                    const int ik = sp ? p.iab(k, i) : p.iab(i, k);
+                    const int jk = sp ? p.iab(k, j) : p.iab(j, k);
+                    s.t(row, p.d2ab + (int64_t)ik * gab + jk, -1.0);
+                }
+            }
+    };
+    auto contract_aa = [&](int64_t d2, bool with_ab, int sp, double f, int64_t d1) {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                const int64_t row = off + i * n + j;
+                s.t(row, d1 + i * n + j, f);
+                if (with_ab)
+                    for (int k = 0; k < n; k++) {
+                        const int ik = sp ? p.iab(k, i) : p.iab(i, k);
+                        const int jk = sp ? p.iab(k, j) : p.iab(j, k);
+                        s.t(row, p.d2ab + (int64_t)ik * gab + jk, -1.0);
+                    }
+                for (int k = 0; k < n; k++) {
+                    if (i == k || j == k) continue;
+                    const int sik = i < k ? 1 : -1, sjk = j < k ? 1 : -1;
+                    s.t(row, d2 + (int64_t)p.iaa(i, k) * gaa + p.iaa(j, k), -(double)(sik * sjk));
+                }
+            }
+    };
+    if (!p.spec.constrain_sz) {
+        contract_aa(p.d2aa, true, 0, na + nb - 1.0, p.d1a); off += (int64_t)n * n;
+        contract_aa(p.d2bb, true, 1, na + nb - 1.0, p.d1b); off += (int64_t)n * n;
+    } else {
+        contract_ab(0, nb, p.d1a); off += (int64_t)n * n;
+        contract_ab(1, na, p.d1b); off += (int64_t)n * n;
+        contract_aa(p.d2aa, false, 0, na - 1.0, p.d1a); off += (int64_t)n * n;
+        contract_aa(p.d2bb, false, 1, nb - 1.0, p.d1b); off += (int64_t)n * n;
+    }
+
+    if (p.spec.constrain_spin) {
+        // spin.cc:279-290 <S^2>
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) s.t(off, p.d2ab + (int64_t)p.iab(i, j) * gab + p.iab(j, i), 1.0);
+        off++;
+        if (p.spec.nalpha == p.spec.nbeta) {
+            // spin.cc:320-393
+            for (int64_t r = 0; r < (int64_t)n * n; r++) { s.t(off + r, p.d1a + r, 1.0); s.t(off + r, p.d1b + r, -1.0); }
+            off += (int64_t)n * n;
+            for (int64_t r = 0; r < (int64_t)gaa * gaa; r++) { s.t(off + r, p.d2aa + r, 1.0); s.t(off + r, p.d2bb + r, -1.0); }
+            off += (int64_t)gaa * gaa;
+            for (int sp = 0; sp < 2; sp++) {
+                const int64_t d2 = sp ? p.d2bb : p.d2aa;
+                for (int ij = 0; ij < gaa; ij++) {
+                    const int i = p.bas_aa[2 * ij], j = p.bas_aa[2 * ij + 1];
+                    const int64_t ijb = p.iab(i, j), jib = p.iab(j, i);
+                    for (int kl = 0; kl < gaa; kl++) {
+                        const int k = p.bas_aa[2 * kl], l = p.bas_aa[2 * kl + 1];
+                        const int64_t klb = p.iab(k, l), lkb = p.iab(l, k);
+                        const int64_t row = off + (int64_t)ij * gaa + kl;
+                        s.t(row, d2 + (int64_t)ij * gaa + kl, 1.0);
+                        s.t(row, p.d2ab + ijb * gab + klb, -0.5);
+                        s.t(row, p.d2ab + jib * gab + klb, 0.5);
+                        s.t(row, p.d2ab + ijb * gab + lkb, 0.5);
+                        s.t(row, p.d2ab + jib * gab + lkb, -0.5);
+                    }
+                }
+                off += (int64_t)gaa * gaa;
+            }
+            for (int ij = 0; ij < gab; ij++) {
+                const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+                const int64_t ji = p.iab(j, i);
+                const double dij = (i == j) ? kSqrt2 : 1.0;
+                for (int kl = 0; kl < gab; kl++) {
+                    const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                    const int64_t lk = p.iab(l, k);
+                    const double dkl = (k == l) ? kSqrt2 : 1.0;
+                    const double f = -(0.5 / (dij * dkl));
+                    const int64_t row = off + (int64_t)ij * gab + kl;
+                    s.t(row, p.d200 + (int64_t)ij * gab + kl, 1.0);
+                    s.t(row, p.d2ab + (int64_t)ij * gab + kl, f);
+                    s.t(row, p.d2ab + ji * gab + kl, f);
+                    s.t(row, p.d2ab + (int64_t)ij * gab + lk, f);
+                    s.t(row, p.d2ab + ji * gab + lk, f);
+                }
+            }
+            off += (int64_t)gab * gab;
+            for (int ij = 0; ij < gab; ij++) {
+                const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+                const int64_t ji = p.iab(j, i);
+                for (int kl = 0; kl < gab; kl++) {
+                    const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                    const int64_t row = off + (int64_t)ij * gab + kl;
+                    s.t(row, p.d2ab + (int64_t)ij * gab + kl, 1.0);
+                    s.t(row, p.d2ab + ji * gab + p.iab(l, k), -1.0);
+                }
+            }
+            off += (int64_t)gab * gab;
+        } else {
+            // spin.cc:411-485 (non-singlet 2gab x 2gab block)
+            const int64_t w = 2 * (int64_t)gab;
+            for (int q = 0; q < 4; q++) {
+                const int rs = q >> 1, cs = q & 1;   // (row half, column half)
+                for (int ij = 0; ij < gab; ij++) {
+                    const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+                    const int64_t ji = p.iab(j, i);
+                    const double dij = (i == j) ? kSqrt2 : 1.0;
+                    for (int kl = 0; kl < gab; kl++) {
+                        const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                        const int64_t lk = p.iab(l, k);
+                        const double dkl = (k == l) ? kSqrt2 : 1.0;
+                        const int64_t e = (ij + rs * gab) * w + (kl + cs * gab);
+                        const int64_t row = off + e;
+                        const int64_t ab_ijkl = (int64_t)ij * gab + kl, ab_jikl = ji * gab + kl;
+                        const int64_t ab_ijlk = (int64_t)ij * gab + lk, ab_jilk = ji * gab + lk;
+                        s.t(row, p.d200 + e, 1.0);
+                        if (q == 0) {
+                            const double f = -(0.5 / (dij * dkl));
+                            s.t(row, p.d2ab + ab_ijkl, f); s.t(row, p.d2ab + ab_jikl, f);
+                            s.t(row, p.d2ab + ab_ijlk, f); s.t(row, p.d2ab + ab_jilk, f);
+                        } else if (q == 1) {
+                            const double f = 0.5 / dij;
+                            s.t(row, p.d2ab + ab_ijkl, -f); s.t(row, p.d2ab + ab_ijlk, f);
+                            s.t(row, p.d2ab + ab_jikl, -f); s.t(row, p.d2ab + ab_jilk, f);
+                        } else if (q == 2) {
+                            const double f = 0.5 / dkl;
+                            s.t(row, p.d2ab + ab_ijkl, -f); s.t(row, p.d2ab + ab_ijlk, -f);
+                            s.t(row, p.d2ab + ab_jikl, f); s.t(row, p.d2ab + ab_jilk, f);
+                        } else {
+                            s.t(row, p.d2ab + ab_ijkl, -0.5); s.t(row, p.d2ab + ab_jikl, 0.5);
+                            s.t(row, p.d2ab + ab_ijlk, 0.5); s.t(row, p.d2ab + ab_jilk, -0.5);
+                        }
+                    }
+                }
+            }
+            off += 4 * (int64_t)gab * gab;
+        }
+        if (p.g2) {
+            // spin.cc:487-507
+            for (int kl = 0; kl < gab; kl++)
+                for (int i = 0; i < n; i++) s.t(off + kl, p.g2ba + (int64_t)kl * gab + p.iab(i, i), 1.0);
+            off += gab;
+            for (int kl = 0; kl < gab; kl++)
+                for (int i = 0; i < n; i++) s.t(off + kl, p.g2ba + (int64_t)p.iab(i, i) * gab + kl, 1.0);
+            off += gab;
+        }
+    }
+
+    if (p.q2) {
+        // q2.cc:170-216
+        for (int ij = 0; ij < gab; ij++) {
+            const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                const int64_t row = off + (int64_t)ij * gab + kl;
+                s.t(row, p.d2ab + (int64_t)ij * gab + kl, 1.0);
+                s.t(row, p.q2ab + (int64_t)ij * gab + kl, -1.0);
+                if (j == l) s.t(row, p.d1a + k * n + i, -1.0);
+                if (i == k) s.t(row, p.d1b + l * n + j, -1.0);
+            }
+        }
+        off += (int64_t)gab * gab;
+        // q2.cc:218-318: (D2 - Q2) + (separately summed delta terms)
+        for (int sp = 0; sp < 2; sp++) {
+            const int64_t d2 = sp ? p.d2bb : p.d2aa, q2 = sp ? p.q2bb : p.q2aa, d1 = sp ? p.d1b : p.d1a;
+            for (int ij = 0; ij < gaa; ij++) {
+                const int i = p.bas_aa[2 * ij], j = p.bas_aa[2 * ij + 1];
+                for (int kl = 0; kl < gaa; kl++) {
+                    const int k = p.bas_aa[2 * kl], l = p.bas_aa[2 * kl + 1];
+                    const int64_t row = off + (int64_t)ij * gaa + kl;
+                    s.t(row, d2 + (int64_t)ij * gaa + kl, 1.0);
+                    s.t(row, q2 + (int64_t)ij * gaa + kl, -1.0);
+                    if (j == l) s.g(row, d1 + k * n + i, -1.0);
+                    if (j == k) s.g(row, d1 + l * n + i, 1.0);
+                    if (i == l) s.g(row, d1 + k * n + j, 1.0);
+                    if (i == k) s.g(row, d1 + l * n + j, -1.0);
+                }
+            }
+            off += (int64_t)gaa * gaa;
+        }
+    }
+
+    if (p.g2) {
+        // g2.cc:245-312
+        for (int sp = 0; sp < 2; sp++) {
+            const int64_t g = sp ? p.g2ba : p.g2ab, d1 = sp ? p.d1b : p.d1a;
+            for (int ij = 0; ij < gab; ij++) {
+                const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+                for (int kl = 0; kl < gab; kl++) {
+                    const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                    const int64_t row = off + (int64_t)ij * gab + kl;
+                    s.t(row, g + (int64_t)ij * gab + kl, -1.0);
+                    if (j == l) s.t(row, d1 + i * n + k, 1.0);
+                    const int64_t col = sp ? p.d2ab + (int64_t)p.iab(l, i) * gab + p.iab(j, k)
+                                           : p.d2ab + (int64_t)p.iab(i, l) * gab + p.iab(k, j);
+                    s.t(row, col, -1.0);
+                }
+            }
+            off += (int64_t)gab * gab;
+        }
+        // g2.cc:313-440
+        const int64_t w = 2 * (int64_t)gab;
+        for (int sp = 0; sp < 2; sp++) {
+            const int64_t d1 = sp ? p.d1b : p.d1a, d2 = sp ? p.d2bb : p.d2aa, sh = sp ? gab : 0;
+            for (int ij = 0; ij < gab; ij++) {
+                const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+                for (int kl = 0; kl < gab; kl++) {
+                    const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                    const int64_t e = (sh + ij) * w + (sh + kl);
+                    s.t(off + e, p.g2aa + e, -1.0);
+                    if (j == l) s.t(off + e, d1 + i * n + k, 1.0);
+                    if (i != l && k != j) {
+                        const int sil = i < l ? 1 : -1, skj = k < j ? 1 : -1;
+                        s.t(off + e, d2 + (int64_t)p.iaa(i, l) * gaa + p.iaa(k, j), -(double)(sil * skj));
+                    }
+                }
+            }
+        }
+        for (int ij = 0; ij < gab; ij++) {
+            const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                const int64_t e = (int64_t)ij * w + (gab + kl);
+                s.t(off + e, p.g2aa + e, -1.0);
+                s.t(off + e, p.d2ab + (int64_t)p.iab(i, l) * gab + p.iab(j, k), 1.0);
+            }
+        }
+        for (int ij = 0; ij < gab; ij++) {
+            const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                const int64_t e = (gab + ij) * w + kl;
+                s.t(off + e, p.g2aa + e, -1.0);
+                s.t(off + e, p.d2ab + (int64_t)p.iab(l, i) * gab + p.iab(k, j), 1.0);
+            }
+        }
+        off += 4 * (int64_t)gab * gab;
+    }
+    if (off != p.n_dual) throw std::logic_error("A emitter row count mismatch");
+}
+
+// A^T (rows = primal elements).  S::t(primal, dual_row, coef) appends one
+// contribution in the order hilbert's bpsdp_ATu scatters it.
+template <class S>
+void visit_AT(const Problem &p, S &s) {
+    const int n = p.n, gab = p.gab, gaa = p.gaa;
+    const double na = p.spec.nalpha, nb = p.spec.nbeta;
+    int64_t off = 0;
+    // d2.cc:48-100
+    if (p.spec.constrain_sz) {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) { const int ij = p.iab(i, j); s.t(p.d2ab + (int64_t)ij * gab + ij, off, 1.0); }
+        off++;
+        for (int sp = 0; sp < 2; sp++) {
+            const int64_t d2 = sp ? p.d2bb : p.d2aa;
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j < n; j++) {
+                    if (i == j || gaa == 0) continue;
+                    const int ij = p.iaa(i, j);
+                    s.t(d2 + (int64_t)ij * gaa + ij, off, 1.0);
+                }
+            off++;
+        }
+    } else {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                int ij = p.iab(i, j);
+                s.t(p.d2ab + (int64_t)ij * gab + ij, off, 2.0);
+                if (i == j || gaa == 0) continue;
+                ij = p.iaa(i, j);
+                s.t(p.d2aa + (int64_t)ij * gaa + ij, off, 1.0);
+                s.t(p.d2bb + (int64_t)ij * gaa + ij, off, 1.0);
+            }
+        off++;
+    }
+    // d2.cc:102-134
+    const int64_t hb[3] = {p.d2aa, p.d2bb, p.d2ab};
+    const int hg[3] = {gaa, gaa, gab};
+    for (int sp = 0; sp < 3; sp++)
+        for (int64_t ij = 0; ij < hg[sp]; ij++)
+            for (int64_t kl = 0; kl < hg[sp]; kl++) {
+                s.t(hb[sp] + ij * hg[sp] + kl, off, 1.0);
+                s.t(hb[sp] + kl * hg[sp] + ij, off, -1.0);
+                off++;
+            }
+    // d2.cc:136-158
+    for (int sp = 0; sp < 2; sp++) {
+        const int64_t d1 = sp ? p.d1b : p.d1a, q1 = sp ? p.q1b : p.q1a;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                s.t(d1 + j * n + i, off + i * n + j, 1.0);
+                s.t(q1 + i * n + j, off + i * n + j, 1.0);
+            }
+        off += (int64_t)n * n;
+    }
+    // d2.cc:160-309
+    auto contract = [&](int sp, double f, int64_t d1, bool with_ab, bool with_aa, int64_t d2) {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                const int64_t row = off + i * n + j;
+                s.t(d1 + i * n + j, row, f);
+                if (with_ab)
+                    for (int k = 0; k < n; k++) {
+                        const int ik = sp ? p.iab(k, i) : p.iab(i, k);
+                        const int jk = sp ? p.iab(k, j) : p.iab(j, k);
+                        s.t(p.d2ab + (int64_t)ik * gab + jk, row, -1.0);
+                    }
+                if (with_aa)
+                    for (int k = 0; k < n; k++) {
+                        if (i == k || j == k) continue;
+                        const int sik = i < k ? 1 : -1, sjk = j < k ? 1 : -1;
+                        s.t(d2 + (int64_t)p.iaa(i, k) * gaa + p.iaa(j, k), row, -(double)(sik * sjk));
+                    }
+            }
+        off += (int64_t)n * n;
+    };
+    if (!p.spec.constrain_sz) {
+        contract(0, na + nb - 1.0, p.d1a, true, true, p.d2aa);
+        contract(1, na + nb - 1.0, p.d1b, true, true, p.d2bb);
+    } else {
+        contract(0, nb, p.d1a, true, false, p.d2aa);
+        contract(1, na, p.d1b, true, false, p.d2bb);
+        contract(0, na - 1.0, p.d1a, false, true, p.d2aa);
+        contract(1, nb - 1.0, p.d1b, false, true, p.d2bb);
+    }
+
+    if (p.spec.constrain_spin) {
+        // spin.cc:48-60
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) s.t(p.d2ab + (int64_t)p.iab(i, j) * gab + p.iab(j, i), off, 1.0);
+        off++;
+        if (p.spec.nalpha == p.spec.nbeta) {
+            // spin.cc:88-170
+            for (int64_t r = 0; r < (int64_t)n * n; r++) s.t(p.d1a + r, off + r, 1.0);
+            for (int64_t r = 0; r < (int64_t)n * n; r++) s.t(p.d1b + r, off + r, -1.0);
+            off += (int64_t)n * n;
+            for (int64_t r = 0; r < (int64_t)gaa * gaa; r++) s.t(p.d2aa + r, off + r, 1.0);
+            for (int64_t r = 0; r < (int64_t)gaa * gaa; r++) s.t(p.d2bb + r, off + r, -1.0);
+            off += (int64_t)gaa * gaa;
+            for (int sp = 0; sp < 2; sp++) {
+                const int64_t d2 = sp ? p.d2bb : p.d2aa;
+                for (int64_t r = 0; r < (int64_t)gaa * gaa; r++) s.t(d2 + r, off + r, 1.0);
+                for (int ij = 0; ij < gaa; ij++) {
+                    const int i = p.bas_aa[2 * ij], j = p.bas_aa[2 * ij + 1];
+                    const int64_t ijb = p.iab(i, j), jib = p.iab(j, i);
+                    for (int kl = 0; kl < gaa; kl++) {
+                        const int k = p.bas_aa[2 * kl], l = p.bas_aa[2 * kl + 1];
+                        const int64_t klb = p.iab(k, l), lkb = p.iab(l, k);
+                        const int64_t row = off + (int64_t)ij * gaa + kl;
+                        s.t(p.d2ab + ijb * gab + klb, row, -0.5);
+                        s.t(p.d2ab + jib * gab + klb, row, 0.5);
+                        s.t(p.d2ab + ijb * gab + lkb, row, 0.5);
+                        s.t(p.d2ab + jib * gab + lkb, row, -0.5);
+                    }
+                }
+                off += (int64_t)gaa * gaa;
+            }
+            for (int64_t r = 0; r < (int64_t)gab * gab; r++) s.t(p.d200 + r, off + r, 1.0);
+            for (int ij = 0; ij < gab; ij++) {
+                const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+                const int64_t ji = p.iab(j, i);
+                const double dij = (i == j) ? kSqrt2 : 1.0;
+                for (int kl = 0; kl < gab; kl++) {
+                    const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                    const int64_t lk = p.iab(l, k);
+                    const double dkl = (k == l) ? kSqrt2 : 1.0;
+                    const double f = -(0.5 / (dij * dkl));
+                    const int64_t row = off + (int64_t)ij * gab + kl;
+                    s.t(p.d2ab + (int64_t)ij * gab + kl, row, f);
+                    s.t(p.d2ab + ji * gab + kl, row, f);
+                    s.t(p.d2ab + (int64_t)ij * gab + lk, row, f);
+                    s.t(p.d2ab + ji * gab + lk, row, f);
+                }
+            }
+            off += (int64_t)gab * gab;
+            for (int64_t r = 0; r < (int64_t)gab * gab; r++) s.t(p.d2ab + r, off + r, 1.0);
+            for (int ij = 0; ij < gab; ij++) {
+                const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+                const int64_t ji = p.iab(j, i);
+                for (int kl = 0; kl < gab; kl++) {
+                    const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                    s.t(p.d2ab + ji * gab + p.iab(l, k), off + (int64_t)ij * gab + kl, -1.0);
+                }
+            }
+            off += (int64_t)gab * gab;
+        } else {
+            // spin.cc:171-251
+            const int64_t w = 2 * (int64_t)gab;
+            for (int q = 0; q < 4; q++) {
+                const int rs = q >> 1, cs = q & 1;
+                for (int ij = 0; ij < gab; ij++) {
+                    const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+                    const int64_t ji = p.iab(j, i);
+                    const double dij = (i == j) ? kSqrt2 : 1.0;
+                    for (int kl = 0; kl < gab; kl++) {
+                        const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                        const int64_t lk = p.iab(l, k);
+                        const double dkl = (k == l) ? kSqrt2 : 1.0;
+                        const int64_t e = (ij + rs * gab) * w + (kl + cs * gab);
+                        const int64_t row = off + e;
+                        const int64_t ab_ijkl = (int64_t)ij * gab + kl, ab_jikl = ji * gab + kl;
+                        const int64_t ab_ijlk = (int64_t)ij * gab + lk, ab_jilk = ji * gab + lk;
+                        s.t(p.d200 + e, row, 1.0);
+                        if (q == 0) {
+                            const double f = -(0.5 / (dij * dkl));
+                            s.t(p.d2ab + ab_ijkl, row, f); s.t(p.d2ab + ab_jikl, row, f);
+                            s.t(p.d2ab + ab_ijlk, row, f); s.t(p.d2ab + ab_jilk, row, f);
+                        } else if (q == 1) {
+                            const double f = 0.5 / dij;
+                            s.t(p.d2ab + ab_ijkl, row, -f); s.t(p.d2ab + ab_ijlk, row, f);
+                            s.t(p.d2ab + ab_jikl, row, -f); s.t(p.d2ab + ab_jilk, row, f);
+                        } else if (q == 2) {
+                            const double f = 0.5 / dkl;
+                            s.t(p.d2ab + ab_ijkl, row, -f); s.t(p.d2ab + ab_ijlk, row, -f);
+                            s.t(p.d2ab + ab_jikl, row, f); s.t(p.d2ab + ab_jilk, row, f);
+                        } else {
+                            s.t(p.d2ab + ab_ijkl, row, -0.5); s.t(p.d2ab + ab_jikl, row, 0.5);
+                            s.t(p.d2ab + ab_ijlk, row, 0.5); s.t(p.d2ab + ab_jilk, row, -0.5);
+                        }
+                    }
+                }
+            }
+            off += 4 * (int64_t)gab * gab;
+        }
+        if (p.g2) {
+            // spin.cc:253-271
+            for (int kl = 0; kl < gab; kl++)
+                for (int i = 0; i < n; i++) s.t(p.g2ba + (int64_t)kl * gab + p.iab(i, i), off + kl, 1.0);
+            off += gab;
+            for (int kl = 0; kl < gab; kl++)
+                for (int i = 0; i < n; i++) s.t(p.g2ba + (int64_t)p.iab(i, i) * gab + kl, off + kl, 1.0);
+            off += gab;
+        }
+    }
+
+    if (p.q2) {
+        // q2.cc:320-354
+        for (int64_t r = 0; r < (int64_t)gab * gab; r++) s.t(p.d2ab + r, off + r, 1.0);
+        for (int64_t r = 0; r < (int64_t)gab * gab; r++) s.t(p.q2ab + r, off + r, -1.0);
+        for (int ij = 0; ij < gab; ij++) {
+            const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                const int64_t row = off + (int64_t)ij * gab + kl;
+                if (j == l) s.t(p.d1a + k * n + i, row, -1.0);
+                if (i == k) s.t(p.d1b + l * n + j, row, -1.0);
+            }
+        }
+        off += (int64_t)gab * gab;
+        // q2.cc:356-436
+        for (int sp = 0; sp < 2; sp++) {
+            const int64_t d2 = sp ? p.d2bb : p.d2aa, q2 = sp ? p.q2bb : p.q2aa, d1 = sp ? p.d1b : p.d1a;
+            for (int64_t r = 0; r < (int64_t)gaa * gaa; r++) s.t(d2 + r, off + r, 1.0);
+            for (int64_t r = 0; r < (int64_t)gaa * gaa; r++) s.t(q2 + r, off + r, -1.0);
+            for (int ij = 0; ij < gaa; ij++) {
+                const int i = p.bas_aa[2 * ij], j = p.bas_aa[2 * ij + 1];
+                for (int kl = 0; kl < gaa; kl++) {
+                    const int k = p.bas_aa[2 * kl], l = p.bas_aa[2 * kl + 1];
+                    const int64_t row = off + (int64_t)ij * gaa + kl;
+                    if (j == l) s.t(d1 + k * n + i, row, -1.0);
+                    if (j == k) s.t(d1 + l * n + i, row, 1.0);
+                    if (i == l) s.t(d1 + k * n + j, row, 1.0);
+                    if (i == k) s.t(d1 + l * n + j, row, -1.0);
+                }
+            }
+            off += (int64_t)gaa * gaa;
+        }
+    }
+
+    if (p.g2) {
+        // g2.cc:445-510
+        for (int sp = 0; sp < 2; sp++) {
+            const int64_t g = sp ? p.g2ba : p.g2ab, d1 = sp ? p.d1b : p.d1a;
+            for (int ij = 0; ij < gab; ij++) {
+                const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+                for (int kl = 0; kl < gab; kl++) {
+                    const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                    const int64_t row = off + (int64_t)ij * gab + kl;
+                    s.t(g + (int64_t)ij * gab + kl, row, -1.0);
+                    if (j == l) s.t(d1 + i * n + k, row, 1.0);
+                    const int64_t col = sp ? p.d2ab + (int64_t)p.iab(l, i) * gab + p.iab(j, k)
+                                           : p.d2ab + (int64_t)p.iab(i, l) * gab + p.iab(k, j);
+                    s.t(col, row, -1.0);
+                }
+            }
+            off += (int64_t)gab * gab;
+        }
+        // g2.cc:511-631
+        const int64_t w = 2 * (int64_t)gab;
+        for (int sp = 0; sp < 2; sp++) {
+            const int64_t d1 = sp ? p.d1b : p.d1a, d2 = sp ? p.d2bb : p.d2aa, sh = sp ? gab : 0;
+            for (int ij = 0; ij < gab; ij++) {
+                const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+                for (int kl = 0; kl < gab; kl++) {
+                    const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                    const int64_t e = (sh + ij) * w + (sh + kl);
+                    s.t(p.g2aa + e, off + e, -1.0);
+                    if (j == l) s.t(d1 + i * n + k, off + e, 1.0);
+                    if (i != l && k != j) {
+                        const int sil = i < l ? 1 : -1, skj = k < j ? 1 : -1;
+                        s.t(d2 + (int64_t)p.iaa(i, l) * gaa + p.iaa(k, j), off + e, -(double)(sil * skj));
+                    }
+                }
+            }
+        }
+        for (int ij = 0; ij < gab; ij++) {
+            const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                const int64_t e = (int64_t)ij * w + (gab + kl);
+                s.t(p.g2aa + e, off + e, -1.0);
+                s.t(p.d2ab + (int64_t)p.iab(i, l) * gab + p.iab(j, k), off + e, 1.0);
+            }
+        }
+        for (int ij = 0; ij < gab; ij++) {
+            const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                const int64_t e = (gab + ij) * w + kl;
+                s.t(p.g2aa + e, off + e, -1.0);
+                s.t(p.d2ab + (int64_t)p.iab(l, i) * gab + p.iab(k, j), off + e, 1.0);
+            }
+        }
+        off += 4 * (int64_t)gab * gab;
+    }
+    if (off != p.n_dual) throw std::logic_error("A^T emitter row count mismatch");
+}
+
+struct Palette {
+    std::vector<double> v;
+    uint32_t code(double c) {
+        for (size_t i = 0; i < v.size(); i++)
+            if (std::memcmp(&v[i], &c, sizeof(double)) == 0) return (uint32_t)i;
+        if (v.size() >= 16) throw std::logic_error("more than 16 distinct coefficients");
+        v.push_back(c);
+        return (uint32_t)(v.size() - 1);
+    }
+};
+
+struct CountSink {
+    std::vector<uint64_t> &cnt;
+    Palette &pal;
+    void t(int64_t row, int64_t, double c) { cnt[row]++; pal.code(c); }
+    void g(int64_t row, int64_t, double c) { cnt[row]++; pal.code(c); }
+};
+
+struct FillSink {
+    std::vector<uint64_t> &cursor;
+    std::vector<uint32_t> &ent;
+    Palette &pal;
+    void t(int64_t row, int64_t col, double c) {
+        ent[cursor[row]++] = (uint32_t)col | (pal.code(c) << kColBits);
+    }
+    void g(int64_t row, int64_t col, double c) {
+        ent[cursor[row]++] = (uint32_t)col | (pal.code(c) << kColBits) | kGroupFlag;
+    }
+};
+
+template <bool Transposed>
+PackedOperator build_op(const Problem &p) {
+    PackedOperator op;
+    op.nrows = Transposed ? p.n_primal : p.n_dual;
+    op.ncols = Transposed ? p.n_dual : p.n_primal;
+    std::vector<uint64_t> cnt(op.nrows + 1, 0);
+    Palette pal;
+    CountSink cs{cnt, pal};
+    if (Transposed) visit_AT(p, cs); else visit_A(p, cs);
+    std::vector<uint64_t> cursor(op.nrows + 1, 0);
+    uint64_t nnz = 0;
+    for (int64_t r = 0; r < op.nrows; r++) { cursor[r] = nnz; nnz += cnt[r]; }
+    if (nnz >= (1ull << 32)) throw std::invalid_argument("operator has more than 2^32 entries");
+    op.row_ptr.resize(op.nrows + 1);
+    for (int64_t r = 0; r < op.nrows; r++) op.row_ptr[r] = (uint32_t)cursor[r];
+    op.row_ptr[op.nrows] = (uint32_t)nnz;
+    op.entries.resize(nnz);
+    FillSink fs{cursor, op.entries, pal};
+    if (Transposed) visit_AT(p, fs); else visit_A(p, fs);
+    op.palette = pal.v;
+    return op;
+}
+
+}  // namespace
+
+PackedOperator build_A(const Problem &p) { return build_op<false>(p); }
+PackedOperator build_AT(const Problem &p) { return build_op<true>(p); }
+
+}  // namespace v2b

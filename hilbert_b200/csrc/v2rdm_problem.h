@@ -1,0 +1,73 @@
+// Host-side description of one C1 v2RDM boundary-point problem: geminal
+// tables, primal block layout, b, c, guesses, and the constraint operator A
+// emitted as packed sparse rows (A) and packed sparse columns (A^T).
+//
+// Layout and ordering follow hilbert's v2RDMSolver:
+//   tables         src/v2rdm_casscf/basis.cc:426-533
+//   primal blocks  src/v2rdm_casscf/v2rdm_solver.cc:3729-4079 (set_primal_offsets)
+//   dual rows      src/v2rdm_casscf/v2rdm_solver.cc:2995-3050 (bpsdp_Au call order)
+//   b              src/v2rdm_casscf/v2rdm_solver.cc:1826-2070 (BuildConstraints)
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace v2b {
+
+enum Positivity { POS_D = 0, POS_DQ = 1, POS_DG = 2, POS_DQG = 3 };
+
+struct ProblemSpec {
+    int nmo = 0;          // active orbitals (C1, no frozen/restricted orbitals)
+    int nalpha = 0;
+    int nbeta = 0;
+    int positivity = POS_DQG;
+    bool constrain_spin = true;
+    bool constrain_sz = true;
+    bool hubbard_multiplicity = false;  // 2*(na-nb)+1 (Hubbard) vs (na-nb)+1 (external)
+};
+
+// Packed sparse operator: entry = col (bits 0..26) | coef code (27..30) | group flag (31).
+// Within a row the entries are stored in the order the reference accumulates them.
+struct PackedOperator {
+    int64_t nrows = 0;
+    int64_t ncols = 0;
+    std::vector<uint32_t> row_ptr;   // nrows + 1 (host check: nnz < 2^32)
+    std::vector<uint32_t> entries;
+    std::vector<double> palette;     // <= 16 distinct coefficients
+};
+
+constexpr uint32_t kColBits = 27;
+constexpr uint32_t kColMask = (1u << kColBits) - 1u;
+constexpr uint32_t kGroupFlag = 1u << 31;
+
+struct Problem {
+    ProblemSpec spec;
+    int n = 0, gab = 0, gaa = 0, mult = 1;
+    bool q2 = false, g2 = false;
+    std::vector<int> bas_ab, ibas_ab, bas_aa, ibas_aa;
+    int64_t d2ab = -1, d2aa = -1, d2bb = -1, d200 = -1, d1a = -1, d1b = -1, q1a = -1, q1b = -1;
+    int64_t q2ab = -1, q2aa = -1, q2bb = -1, g2ab = -1, g2ba = -1, g2aa = -1;
+    int64_t n_primal = 0, n_dual = 0;
+    std::vector<int> dims;           // PSD block sizes, in primal order
+    std::vector<int64_t> block_off;  // offset of each block in x
+
+    int iab(int i, int j) const { return ibas_ab[i * n + j]; }
+    int iaa(int i, int j) const { return ibas_aa[i * n + j]; }
+};
+
+// Throws std::invalid_argument on bad sizes.
+Problem make_problem(const ProblemSpec &spec);
+
+void build_b(const Problem &p, double *b);
+// 1D periodic Hubbard ring: h_{i,i+-1 mod n} = -t, (ii|ii) = U
+void build_c_hubbard(const Problem &p, double t, double U, double *c);
+// external Hamiltonian: h[i*n+j], g[i*n^3+j*n^2+k*n+l] = (ij|kl)
+void build_c_external(const Problem &p, const double *h, const double *g, double *c);
+void guess_random(const Problem &p, double *x);
+void guess_hf(const Problem &p, double *x);
+
+PackedOperator build_A(const Problem &p);    // rows = dual constraints
+PackedOperator build_AT(const Problem &p);   // rows = primal variables
+
+}  // namespace v2b

@@ -1,0 +1,403 @@
+"""Host-side mirror of hilbert's v2RDM-CASSCF interface for the B200 path.
+
+* ``Options``        -- the HILBERT option names and defaults that the v2RDM
+                         path reads (src/plugin.cc:80-463).
+* ``v2RDMHelper``    -- the pybind class of src/python_api/python_helpers.cc:104-113
+                         (external-Hamiltonian constructor and the Hubbard path).
+* ``V2RDMProblem``   -- the device-map problem: A.x, A^T.y, projection and the
+                         full solve on CUDA tensors through the C ABI.
+* ``BPSDPSolver``    -- libsdp::BPSDPSolver-shaped solver with host callbacks
+                         (src/v2rdm_casscf/v2rdm_solver.cc:424-447, 1340).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _capi
+from ._capi import SDP_CALLBACK, SDP_MONITOR, SDPOptions, check
+
+# option name -> default (src/plugin.cc line of the add_* call in comments)
+DEFAULTS = {
+    "E_CONVERGENCE": 1e-6,          # :94
+    "R_CONVERGENCE": 1e-5,          # :97
+    "MAXITER": 50,                  # :100
+    "CG_CONVERGENCE": 1e-9,         # :238
+    "CG_MAXITER": 10000,            # :241
+    "MU_UPDATE_FREQUENCY": 1000,    # :217
+    "POSITIVITY": "DQG",            # :220
+    "CONSTRAIN_SPIN": True,         # :306
+    "CONSTRAIN_SZ": True,           # :309
+    "TPDM_GUESS": "RANDOM",         # :205
+    "SDP_SOLVER": "BPSDP",          # :246
+    "HUBBARD_HAMILTONIAN": False,   # :249
+    "HUBBARD_T": 1.0,               # :252
+    "HUBBARD_U": 1.0,               # :255
+    "N_HUBBARD_SITES": 4,           # :258
+    "N_HUBBARD_SPINS": 4,           # :261
+    "OPTIMIZE_ORBITALS": True,      # :138
+    "ORBOPT_FREQUENCY": 500,        # :150
+    "ORBOPT_MAXITER": 10,           # :168
+    "ORBOPT_GRADIENT_CONVERGENCE": 1e-4,   # :153
+    "ORBOPT_ENERGY_CONVERGENCE": 1e-8,     # :156
+}
+
+
+class Options:
+    """Case-insensitive option store with Psi4-style accessors."""
+
+    def __init__(self, values=None, **kw):
+        self._v = dict(DEFAULTS)
+        for src in (values or {}), kw:
+            for k, v in src.items():
+                self.set(k, v)
+
+    def set(self, key, value):
+        key = key.upper()
+        if isinstance(value, str):
+            value = value.upper()
+        self._v[key] = value
+
+    def get(self, key):
+        return self._v[key.upper()]
+
+    get_str = get_double = get_int = get_bool = get
+
+    def __getitem__(self, key):
+        return self.get(key)
+
+    def sdp_options(self):
+        return SDPOptions(float(self.get("E_CONVERGENCE")), float(self.get("R_CONVERGENCE")),
+                          float(self.get("CG_CONVERGENCE")), int(self.get("CG_MAXITER")),
+                          int(self.get("MAXITER")))
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _tptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class V2RDMProblem:
+    """One C1 v2RDM problem whose constraint maps live on the GPU."""
+
+    def __init__(self, nmo, nalpha, nbeta, positivity="DQG", constrain_spin=True,
+                 constrain_sz=True, hubbard_multiplicity=False):
+        lib = _capi.load()
+        self._lib = lib
+        h = ctypes.c_void_p()
+        pos = positivity.upper()
+        if pos not in _capi.POSITIVITY:
+            raise ValueError(f"POSITIVITY {positivity} is not on the device path "
+                             f"(supported: {sorted(_capi.POSITIVITY)})")
+        check(lib.v2b_problem_create(int(nmo), int(nalpha), int(nbeta), _capi.POSITIVITY[pos],
+                                     int(bool(constrain_spin)), int(bool(constrain_sz)),
+                                     int(bool(hubbard_multiplicity)), ctypes.byref(h)))
+        self._h = h
+        self.nmo, self.nalpha, self.nbeta = nmo, nalpha, nbeta
+        self.n_primal = lib.v2b_problem_n_primal(h)
+        self.n_dual = lib.v2b_problem_n_dual(h)
+        nb = lib.v2b_problem_n_blocks(h)
+        dims = (ctypes.c_int * nb)()
+        check(lib.v2b_problem_block_dims(h, dims))
+        self.dims = np.array(dims[:], dtype=np.int32)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.v2b_problem_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # host-side problem data
+    def b(self):
+        out = np.zeros(self.n_dual)
+        check(self._lib.v2b_problem_build_b(self._h, _dptr(out)))
+        return out
+
+    def c_hubbard(self, t, U):
+        out = np.zeros(self.n_primal)
+        check(self._lib.v2b_problem_build_c_hubbard(self._h, float(t), float(U), _dptr(out)))
+        return out
+
+    def c_external(self, h, g):
+        h = np.ascontiguousarray(h, dtype=np.float64).ravel()
+        g = np.ascontiguousarray(g, dtype=np.float64).ravel()
+        if h.size != self.nmo ** 2 or g.size != self.nmo ** 4:
+            raise ValueError("h must hold nmo^2 and g nmo^4 elements")
+        out = np.zeros(self.n_primal)
+        check(self._lib.v2b_problem_build_c_external(self._h, _dptr(h), _dptr(g), _dptr(out)))
+        return out
+
+    def guess(self, kind="RANDOM"):
+        out = np.zeros(self.n_primal)
+        check(self._lib.v2b_problem_guess(self._h, int(kind.upper() == "HF"), _dptr(out)))
+        return out
+
+    # device maps on torch CUDA tensors (float64, contiguous)
+    def _stream(self):
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    @staticmethod
+    def _check_tensor(t, n):
+        if not (t.is_cuda and t.dtype.__repr__() == "torch.float64" and t.is_contiguous()
+                and t.numel() == n):
+            raise ValueError(f"expected a contiguous float64 CUDA tensor of {n} elements")
+
+    def Au(self, x, out=None):
+        import torch
+        self._check_tensor(x, self.n_primal)
+        out = torch.empty(self.n_dual, dtype=torch.float64, device=x.device) if out is None else out
+        self._check_tensor(out, self.n_dual)
+        check(self._lib.v2b_problem_Au(self._h, _tptr(x), _tptr(out), self._stream()))
+        return out
+
+    def ATu(self, y, out=None):
+        import torch
+        self._check_tensor(y, self.n_dual)
+        out = torch.empty(self.n_primal, dtype=torch.float64, device=y.device) if out is None else out
+        self._check_tensor(out, self.n_primal)
+        check(self._lib.v2b_problem_ATu(self._h, _tptr(y), _tptr(out), self._stream()))
+        return out
+
+    def project(self, U, mu):
+        import torch
+        self._check_tensor(U, self.n_primal)
+        x = torch.empty_like(U)
+        z = torch.empty_like(U)
+        check(self._lib.v2b_problem_project(self._h, _tptr(U), float(mu), _tptr(x), _tptr(z),
+                                            self._stream()))
+        return x, z
+
+    def solve(self, x0, b, c, options, monitor=None):
+        """Host arrays in, converged x out (hilbert's compute_energy outer loop)."""
+        x = np.array(x0, dtype=np.float64, copy=True)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        o = options.sdp_options() if isinstance(options, Options) else options
+        muf = int(options.get("MU_UPDATE_FREQUENCY")) if isinstance(options, Options) else 1000
+        cb = SDP_MONITOR(monitor) if monitor is not None else SDP_MONITOR()
+        oi, ii, e = ctypes.c_long(), ctypes.c_long(), ctypes.c_double()
+        rc = check(self._lib.v2b_problem_solve(self._h, _dptr(x), _dptr(b), _dptr(c), ctypes.byref(o),
+                                               muf, cb, 1, None, ctypes.byref(oi), ctypes.byref(ii),
+                                               ctypes.byref(e)),
+                   allow=(_capi.V2B_OK, _capi.V2B_NOT_CONVERGED))
+        return x, {"converged": rc == _capi.V2B_OK, "oiter": oi.value, "iiter": ii.value,
+                   "energy": e.value, "mu": self._lib.v2b_problem_get_mu(self._h)}
+
+    def solve_device(self, x, b, c, options, monitor=None):
+        """x, b, c are CUDA float64 tensors; x is updated in place."""
+        self._check_tensor(x, self.n_primal)
+        self._check_tensor(b, self.n_dual)
+        self._check_tensor(c, self.n_primal)
+        o = options.sdp_options() if isinstance(options, Options) else options
+        muf = int(options.get("MU_UPDATE_FREQUENCY")) if isinstance(options, Options) else 1000
+        cb = SDP_MONITOR(monitor) if monitor is not None else SDP_MONITOR()
+        oi, ii, e = ctypes.c_long(), ctypes.c_long(), ctypes.c_double()
+        import torch
+        torch.cuda.current_stream().synchronize()
+        rc = check(self._lib.v2b_problem_solve_device(self._h, _tptr(x), _tptr(b), _tptr(c),
+                                                      ctypes.byref(o), muf, cb, 1, None,
+                                                      ctypes.byref(oi), ctypes.byref(ii),
+                                                      ctypes.byref(e)),
+                   allow=(_capi.V2B_OK, _capi.V2B_NOT_CONVERGED))
+        return {"converged": rc == _capi.V2B_OK, "oiter": oi.value, "iiter": ii.value,
+                "energy": e.value, "mu": self._lib.v2b_problem_get_mu(self._h)}
+
+    def get_y(self):
+        out = np.zeros(self.n_dual)
+        check(self._lib.v2b_problem_get_y(self._h, _dptr(out)))
+        return out
+
+    def get_z(self):
+        out = np.zeros(self.n_primal)
+        check(self._lib.v2b_problem_get_z(self._h, _dptr(out)))
+        return out
+
+    def kernel_launches(self):
+        return self._lib.v2b_problem_kernel_launches(self._h)
+
+    KERNEL_CLASSES = ("cg_kernel", "spmv_AT_U_kernel", "jacobi_project_kernel", "spmv_A2_kernel",
+                      "stats_kernel")
+
+    def set_profiling(self, on=True):
+        check(self._lib.v2b_problem_set_profiling(self._h, int(bool(on))))
+
+    def profile(self):
+        """{kernel: (total_ms, launches)} from CUDA events on the library's stream"""
+        ms = (ctypes.c_double * 5)()
+        n = (ctypes.c_long * 5)()
+        check(self._lib.v2b_problem_profile(self._h, ms, n))
+        return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNEL_CLASSES)}
+
+    def stream_handle(self):
+        return self._lib.v2b_problem_stream(self._h)
+
+
+class BPSDPSolver:
+    """libsdp::BPSDPSolver with host callbacks (evaluate_Au / evaluate_ATu)."""
+
+    def __init__(self, n_primal, n_dual, options):
+        self._lib = _capi.load()
+        self.n_primal, self.n_dual = int(n_primal), int(n_dual)
+        o = options.sdp_options() if isinstance(options, Options) else options
+        h = ctypes.c_void_p()
+        check(self._lib.v2b_bpsdp_create(self.n_primal, self.n_dual, ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        try:
+            if self._h:
+                self._lib.v2b_bpsdp_destroy(self._h)
+        except Exception:
+            pass
+
+    def solve(self, x, b, c, primal_block_dims, maxiter, Au, ATu, monitor=None, print_level=1):
+        """x (float64 numpy, updated in place); Au(in) / ATu(in) return numpy arrays."""
+        nd, np_ = self.n_dual, self.n_primal
+
+        def wrap(fn, n_in, n_out):
+            def cb(out, inp, _data):
+                vin = np.ctypeslib.as_array(inp, shape=(n_in,))
+                vout = np.ctypeslib.as_array(out, shape=(n_out,))
+                vout[:] = fn(vin)
+            return SDP_CALLBACK(cb)
+
+        cau = wrap(Au, np_, nd)
+        catu = wrap(ATu, nd, np_)
+        cmon = SDP_MONITOR(monitor) if monitor is not None else SDP_MONITOR()
+        dims = np.ascontiguousarray(primal_block_dims, dtype=np.int32)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        rc = check(self._lib.v2b_bpsdp_solve(self._h, _dptr(x), _dptr(b), _dptr(c),
+                                             dims.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                             len(dims), int(maxiter), cau, catu, cmon,
+                                             int(print_level), None),
+                   allow=(_capi.V2B_OK, _capi.V2B_NOT_CONVERGED))
+        return rc == _capi.V2B_OK
+
+    def is_converged(self):
+        return bool(self._lib.v2b_bpsdp_is_converged(self._h))
+
+    def get_mu(self):
+        return self._lib.v2b_bpsdp_get_mu(self._h)
+
+    def set_mu(self, mu):
+        check(self._lib.v2b_bpsdp_set_mu(self._h, float(mu)))
+
+    def get_y(self):
+        out = np.zeros(self.n_dual)
+        check(self._lib.v2b_bpsdp_get_y(self._h, _dptr(out)))
+        return out
+
+    def get_z(self):
+        out = np.zeros(self.n_primal)
+        check(self._lib.v2b_bpsdp_get_z(self._h, _dptr(out)))
+        return out
+
+    def set_y(self, y):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        check(self._lib.v2b_bpsdp_set_y(self._h, _dptr(y)))
+
+    def set_z(self, z):
+        z = np.ascontiguousarray(z, dtype=np.float64)
+        check(self._lib.v2b_bpsdp_set_z(self._h, _dptr(z)))
+
+    def iiter_total(self):
+        return self._lib.v2b_bpsdp_iiter_total(self._h)
+
+    def oiter_total(self):
+        return self._lib.v2b_bpsdp_oiter_total(self._h)
+
+
+class v2RDMHelper:
+    """hilbert.v2RDMHelper (src/python_api/python_helpers.cc:104-113, 357-371).
+
+    ``v2RDMHelper(nalpha, nbeta, nmo, h, g, options)`` builds the
+    external-Hamiltonian problem (v2rdm_solver.cc:147-195);
+    ``v2RDMHelper(None, options)`` with HUBBARD_HAMILTONIAN builds the 1D
+    Hubbard ring (v2rdm_solver.cc:839-962).  Molecular wavefunctions need Psi4
+    and are outside this package.
+    """
+
+    def __init__(self, *args):
+        if len(args) == 6:
+            nalpha, nbeta, nmo, h, g, options = args
+            self.options = options if isinstance(options, Options) else Options(options)
+            self._hubbard = False
+        elif len(args) == 2:
+            _ref_wfn, options = args
+            self.options = options if isinstance(options, Options) else Options(options)
+            if not self.options.get("HUBBARD_HAMILTONIAN"):
+                raise NotImplementedError("molecular Hamiltonians need Psi4; use the external-"
+                                          "Hamiltonian constructor or HUBBARD_HAMILTONIAN")
+            nspins = int(self.options.get("N_HUBBARD_SPINS"))
+            if nspins % 2:
+                raise ValueError("Hubbard model only works for even numbers of electrons currently.")
+            nmo = int(self.options.get("N_HUBBARD_SITES"))
+            nalpha = nbeta = nspins // 2
+            self._hubbard = True
+        else:
+            raise TypeError("v2RDMHelper(nalpha, nbeta, nmo, h, g, options) or v2RDMHelper(ref_wfn, options)")
+        o = self.options
+        self.problem = V2RDMProblem(nmo, nalpha, nbeta, o.get("POSITIVITY"), o.get("CONSTRAIN_SPIN"),
+                                    o.get("CONSTRAIN_SZ"), hubbard_multiplicity=self._hubbard)
+        p = self.problem
+        if self._hubbard:
+            self.c = p.c_hubbard(o.get("HUBBARD_T"), o.get("HUBBARD_U"))
+        else:
+            self.c = p.c_external(h, g)
+        self.b = p.b()
+        self.x = None
+        self.stats = None
+        self.variables = {}
+
+    def compute_energy(self, monitor=None):
+        p = self.problem
+        x0 = p.guess(self.options.get("TPDM_GUESS"))
+        self.x, self.stats = p.solve(x0, self.b, self.c, self.options, monitor)
+        e = float(self.c @ self.x)
+        # enuc = efzc = 0 for Hubbard / external Hamiltonians (v2rdm_solver.cc:851-853, 972-974)
+        self.variables["CURRENT ENERGY"] = e
+        self.variables["v2RDM TOTAL ENERGY"] = e
+        return e
+
+    def get_opdm(self):
+        """Spin-summed active 1-RDM D1a + D1b (python_api.cc:374-394, C1 active block)."""
+        n = self.problem.nmo
+        o = self.options
+        off = block_offsets(n, self.problem.nalpha, self.problem.nbeta, o.get("POSITIVITY"),
+                            o.get("CONSTRAIN_SPIN"))
+        d1a = self.x[off["d1a"]:off["d1a"] + n * n].reshape(n, n)
+        d1b = self.x[off["d1b"]:off["d1b"] + n * n].reshape(n, n)
+        return d1a + d1b
+
+
+def block_layout(nmo, nalpha, nbeta, positivity="DQG", constrain_spin=True):
+    """[(name, dim)] in the primal order of set_primal_offsets (v2rdm_solver.cc:3729-4079)."""
+    n = int(nmo)
+    gab, gaa = n * n, n * (n - 1) // 2
+    pos = positivity.upper()
+    blocks = [("d2ab", gab), ("d2aa", gaa), ("d2bb", gaa)]
+    if constrain_spin:
+        blocks.append(("d200", gab if nalpha == nbeta else 2 * gab))
+    blocks += [("d1a", n), ("d1b", n), ("q1a", n), ("q1b", n)]
+    if pos in ("DQ", "DQG"):
+        blocks += [("q2ab", gab), ("q2aa", gaa), ("q2bb", gaa)]
+    if pos in ("DG", "DQG"):
+        blocks += [("g2ab", gab), ("g2ba", gab), ("g2aa", 2 * gab)]
+    return blocks
+
+
+def block_offsets(nmo, nalpha, nbeta, positivity="DQG", constrain_spin=True):
+    off, o = {}, 0
+    for name, d in block_layout(nmo, nalpha, nbeta, positivity, constrain_spin):
+        off[name] = o
+        o += d * d
+    return off

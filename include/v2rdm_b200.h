@@ -1,0 +1,171 @@
+/*
+ * v2rdm_b200 -- C ABI of the B200 boundary-point SDP path for hilbert's
+ * v2RDM-CASSCF solver.  Plain pointers and sizes only; every entry point
+ * returns a status code (never throws) and v2b_last_error() describes the
+ * last failure on the calling thread.
+ *
+ * Two families of entry points:
+ *
+ *  1. libsdp-shaped solver (drop-in for libsdp::BPSDPSolver as hilbert calls
+ *     it).  The caller supplies A.x / A^T.y as host callbacks exactly like
+ *     evaluate_Au / evaluate_ATu (src/v2rdm_casscf/v2rdm_solver.cc:97-112);
+ *     vectors stay on the host, the per-block PSD projection runs on the GPU.
+ *
+ *  2. Device-map problems: the constraint operator of a C1 v2RDM problem is
+ *     built in the library (bit-exact to hilbert's maps) and every step of the
+ *     iteration -- A.x, A^T.y, conjugate gradients, projection, norms -- runs
+ *     on the GPU.  x, b, c passed to v2b_problem_solve are host arrays.
+ */
+#ifndef V2RDM_B200_H
+#define V2RDM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define V2B_OK             0
+#define V2B_NOT_CONVERGED  1   /* iteration cap reached (not an error for solve) */
+#define V2B_BAD_ARG        2
+#define V2B_NAN            3   /* non-finite value met in a reduction */
+#define V2B_DEVICE_TIMEOUT 4   /* a bounded device-side wait gave up */
+#define V2B_CUDA_ERROR     5
+#define V2B_NO_DEVICE      6
+#define V2B_INTERNAL       7
+
+/* POSITIVITY option values (src/plugin.cc:220) supported on the device path */
+#define V2B_POSITIVITY_D   0
+#define V2B_POSITIVITY_DQ  1
+#define V2B_POSITIVITY_DG  2
+#define V2B_POSITIVITY_DQG 3
+
+/* libsdp::SDPOptions as hilbert fills it (src/v2rdm_casscf/v2rdm_solver.cc:426-431) */
+typedef struct {
+    double sdp_objective_convergence; /* E_CONVERGENCE  (src/plugin.cc:94)  */
+    double sdp_error_convergence;     /* R_CONVERGENCE  (src/plugin.cc:97)  */
+    double cg_convergence;            /* CG_CONVERGENCE (src/plugin.cc:238) */
+    int cg_maxiter;                   /* CG_MAXITER     (src/plugin.cc:241) */
+    int maxiter;                      /* MAXITER        (src/plugin.cc:100) */
+} v2b_sdp_options;
+
+/* libsdp::SDPCallbackFunction: out = A.in or A^T.in; the callee overwrites out */
+typedef void (*v2b_sdp_callback)(double *out, double *in, void *data);
+/* libsdp::SDPProgressMonitorFunction (src/v2rdm_casscf/v2rdm_solver.cc:115-124) */
+typedef void (*v2b_sdp_monitor)(int print_level, int oiter, int iiter, double energy_primal,
+                                double energy_dual, double mu, double primal_error,
+                                double dual_error, void *data);
+
+typedef struct v2b_bpsdp v2b_bpsdp;
+typedef struct v2b_problem v2b_problem;
+
+const char *v2b_last_error(void);
+int v2b_version(void);
+
+/* ---- 1. libsdp-shaped solver ------------------------------------------------ */
+
+/* replaces libsdp::BPSDPSolver(long n_primal, long n_dual, SDPOptions)
+ * (src/v2rdm_casscf/v2rdm_solver.cc:433) */
+int v2b_bpsdp_create(long n_primal, long n_dual, const v2b_sdp_options *options,
+                     v2b_bpsdp **out);
+/* replaces BPSDPSolver::solve(x, b, c, primal_block_dims, maxiter, Au, ATu,
+ * monitor, print_level, data) (src/v2rdm_casscf/v2rdm_solver.cc:1340).
+ * x is updated in place; mu, y, z persist across calls.  Returns V2B_OK when
+ * converged, V2B_NOT_CONVERGED when maxiter iterations ran without converging. */
+int v2b_bpsdp_solve(v2b_bpsdp *s, double *x, const double *b, const double *c,
+                    const int *primal_block_dims, int n_blocks, int maxiter,
+                    v2b_sdp_callback Au, v2b_sdp_callback ATu, v2b_sdp_monitor monitor,
+                    int print_level, void *data);
+/* SDPSolver::is_converged() (src/v2rdm_casscf/v2rdm_solver.cc:1361) */
+int v2b_bpsdp_is_converged(const v2b_bpsdp *s);
+/* SDPSolver::get_mu / set_mu (src/v2rdm_casscf/v2rdm_solver.cc:1323) */
+double v2b_bpsdp_get_mu(const v2b_bpsdp *s);
+int v2b_bpsdp_set_mu(v2b_bpsdp *s, double mu);
+/* SDPSolver::get_y / get_z copy out; set_y / set_z copy in
+ * (src/v2rdm_casscf/checkpoint.cc:58-120) */
+int v2b_bpsdp_get_y(const v2b_bpsdp *s, double *y);
+int v2b_bpsdp_get_z(const v2b_bpsdp *s, double *z);
+int v2b_bpsdp_set_y(v2b_bpsdp *s, const double *y);
+int v2b_bpsdp_set_z(v2b_bpsdp *s, const double *z);
+/* SDPSolver::iiter_total / oiter_total (src/v2rdm_casscf/v2rdm_solver.cc:1546-1547) */
+long v2b_bpsdp_iiter_total(const v2b_bpsdp *s);
+long v2b_bpsdp_oiter_total(const v2b_bpsdp *s);
+void v2b_bpsdp_destroy(v2b_bpsdp *s);
+
+/* ---- 2. device-map problems -------------------------------------------------- */
+
+/* Sets up the C1 problem that v2RDMSolver::initialize_common_elements builds
+ * (src/v2rdm_casscf/v2rdm_solver.cc:1087-1107: set_constraints,
+ * build_mapping_arrays, determine_n_primal/dual, set_primal_offsets) for nmo
+ * active orbitals, nalpha/nbeta electrons and the POSITIVITY / CONSTRAIN_SPIN /
+ * CONSTRAIN_SZ options; hubbard_multiplicity selects the 2S+1 convention of
+ * the Hubbard initialiser (v2rdm_solver.cc:862) over the external one (:983). */
+int v2b_problem_create(int nmo, int nalpha, int nbeta, int positivity, int constrain_spin,
+                       int constrain_sz, int hubbard_multiplicity, v2b_problem **out);
+void v2b_problem_destroy(v2b_problem *p);
+long v2b_problem_n_primal(const v2b_problem *p);
+long v2b_problem_n_dual(const v2b_problem *p);
+int v2b_problem_n_blocks(const v2b_problem *p);
+/* dimensions_ (v2rdm_solver.cc:3729-4079) */
+int v2b_problem_block_dims(const v2b_problem *p, int *dims);
+/* BuildConstraints (v2rdm_solver.cc:1826-2992) */
+int v2b_problem_build_b(const v2b_problem *p, double *b);
+/* c for the 1D Hubbard ring (oei.cc:76-95, tei.cc:285-292) */
+int v2b_problem_build_c_hubbard(const v2b_problem *p, double t, double U, double *c);
+/* c for an external Hamiltonian (v2rdm_solver.cc:147-195): h[nmo^2], g[nmo^4] = (ij|kl) */
+int v2b_problem_build_c_external(const v2b_problem *p, const double *h, const double *g,
+                                 double *c);
+/* Guess (v2rdm_solver.cc:1711-1824): hf = 0 random (srand(0)), hf = 1 HF determinant */
+int v2b_problem_guess(const v2b_problem *p, int hf, double *x);
+/* bpsdp_Au / bpsdp_ATu (v2rdm_solver.cc:2995-3108) on DEVICE pointers, on
+ * the given cudaStream_t (0 = legacy default stream) */
+int v2b_problem_Au(v2b_problem *p, const double *d_in, double *d_out, void *stream);
+int v2b_problem_ATu(v2b_problem *p, const double *d_in, double *d_out, void *stream);
+/* Per-block PSD projection on DEVICE pointers: x = U+ / mu, z = U+ - sym(U),
+ * one block per entry of the problem's block_dims. */
+int v2b_problem_project(v2b_problem *p, const double *d_U, double mu, double *d_x, double *d_z,
+                        void *stream);
+/* Runs the outer protocol of v2RDMSolver::compute_energy for Hubbard /
+ * external Hamiltonians (v2rdm_solver.cc:1296-1361): repeated solve() calls
+ * of mu_update_frequency iterations, mu <- mu*eps_p/eps_d between calls,
+ * until converged or options->maxiter outer iterations.  x (in/out), b, c are
+ * host arrays.  On return *oiter / *iiter hold the iteration totals and
+ * *energy the primal energy c.x. */
+int v2b_problem_solve(v2b_problem *p, double *x, const double *b, const double *c,
+                      const v2b_sdp_options *options, int mu_update_frequency,
+                      v2b_sdp_monitor monitor, int print_level, void *data, long *oiter,
+                      long *iiter, double *energy);
+/* Same iteration with x, b, c already in device memory (x updated in place). */
+int v2b_problem_solve_device(v2b_problem *p, double *d_x, const double *d_b, const double *d_c,
+                             const v2b_sdp_options *options, int mu_update_frequency,
+                             v2b_sdp_monitor monitor, int print_level, void *data, long *oiter,
+                             long *iiter, double *energy);
+/* dual variables and penalty of the last device solve (host copies) */
+int v2b_problem_get_y(const v2b_problem *p, double *y);
+int v2b_problem_get_z(const v2b_problem *p, double *z);
+double v2b_problem_get_mu(const v2b_problem *p);
+/* The packed constraint operator the device maps read: A (transposed = 0,
+ * rows = dual constraints) or A^T (transposed = 1, rows = primal elements).
+ * Entry bits 0..26 hold the column, 27..30 an index into the palette of
+ * coefficients, bit 31 marks terms summed into the row's second partial sum
+ * (q2.cc:218-318).  Terms are stored in hilbert's accumulation order. */
+int v2b_problem_operator_size(const v2b_problem *p, int transposed, long *nrows, long *nnz,
+                              int *npalette);
+int v2b_problem_operator(const v2b_problem *p, int transposed, uint32_t *row_ptr,
+                         uint32_t *entries, double *palette);
+/* number of kernels the library launched since the problem was created */
+long v2b_problem_kernel_launches(const v2b_problem *p);
+/* CUDA-event timing of each kernel class of the device iteration, recorded on
+ * the library's stream: 0 cg_kernel, 1 spmv_AT_U_kernel, 2 jacobi_project_kernel,
+ * 3 spmv_A2_kernel, 4 stats_kernel.  set_profiling resets the totals. */
+int v2b_problem_set_profiling(v2b_problem *p, int on);
+int v2b_problem_profile(const v2b_problem *p, double *ms /* [5] */, long *launches /* [5] */);
+/* the cudaStream_t the device solve runs on (after the first device call) */
+void *v2b_problem_stream(const v2b_problem *p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* V2RDM_B200_H */

@@ -1,0 +1,45 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+
+
+@pytest.fixture(scope="session")
+def golden():
+    path = os.path.join(ROOT, "tests", "golden", "v2rdm_maps.npz")
+    data = np.load(path)
+    cases = {}
+    for key in data.files:
+        name, field = key.split("/", 1)
+        cases.setdefault(name, {})[field] = data[key]
+    return cases
+
+
+def case_kwargs(case):
+    """keyword arguments that rebuild a golden case's problem"""
+    n, na, nb, spin, sz, hub = [int(v) for v in case["spec"]]
+    kw = dict(n=n, na=na, nb=nb, positivity=str(case["positivity"]), constrain_spin=bool(spin),
+              constrain_sz=bool(sz))
+    if hub > 0:
+        kw["hubbard"] = tuple(float(v) for v in case["hubbard"])
+    else:
+        kw["h"] = case["h"]
+        kw["g"] = case["g"]
+    return kw
+
+
+@pytest.fixture(scope="session")
+def cuda_device():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda:0")

@@ -1,0 +1,93 @@
+"""Full boundary-point solves on the B200 against the numpy oracle and known answers.
+
+Energies agree with the FP64 oracle to |dE| <= 1e-6 Eh at the same thresholds."""
+import numpy as np
+import pytest
+
+import hilbert_b200 as hb
+from oracle.bpsdp import SDPOptions, run_v2rdm
+from oracle.fci import hubbard_fci
+from oracle.maps import OracleProblem
+
+pytestmark = pytest.mark.gpu
+
+E_TOL = 1e-6
+
+
+def hubbard_options(L, U, r=1e-6, e=1e-6, maxiter=100000, muf=500):
+    return hb.Options({"HUBBARD_HAMILTONIAN": True, "N_HUBBARD_SITES": L, "N_HUBBARD_SPINS": L,
+                       "HUBBARD_T": 1.0, "HUBBARD_U": U, "R_CONVERGENCE": r, "E_CONVERGENCE": e,
+                       "MAXITER": maxiter, "MU_UPDATE_FREQUENCY": muf})
+
+
+def test_two_site_hubbard_exact(cuda_device):
+    helper = hb.v2RDMHelper(None, hubbard_options(2, 4.0))
+    e = helper.compute_energy()
+    assert helper.stats["converged"]
+    assert abs(e - (2.0 - np.sqrt(8.0))) <= E_TOL
+    assert helper.variables["CURRENT ENERGY"] == e
+    assert abs(np.trace(helper.get_opdm()) - 2.0) <= 1e-5
+
+
+def test_four_site_hubbard_matches_oracle_and_bounds_fci(cuda_device):
+    helper = hb.v2RDMHelper(None, hubbard_options(4, 4.0))
+    e = helper.compute_energy()
+    assert helper.stats["converged"]
+    o = OracleProblem(4, 2, 2, "DQG", True, True, hubbard=(1.0, 4.0))
+    xo, so = run_v2rdm(o, o.guess("random"), SDPOptions(1e-6, 1e-6, 1e-9, 10000, 100000), 500)
+    assert so.is_converged()
+    assert abs(e - float(o.c @ xo)) <= E_TOL
+    assert e <= hubbard_fci(4, 4, 1.0, 4.0) + E_TOL
+
+
+def test_external_triplet_matches_oracle(cuda_device):
+    n, na, nb = 3, 2, 1
+    rng = np.random.default_rng(11)
+    h = rng.standard_normal((n, n)); h = 0.5 * (h + h.T)
+    b = rng.standard_normal((n, n, 2)) * 0.3
+    g = np.einsum("ijq,klq->ijkl", b, b)
+    opts = hb.Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6, "MAXITER": 100000,
+                       "MU_UPDATE_FREQUENCY": 500})
+    helper = hb.v2RDMHelper(na, nb, n, h.ravel(), g.ravel(), opts)
+    e = helper.compute_energy()
+    assert helper.stats["converged"]
+    o = OracleProblem(n, na, nb, "DQG", True, True, h=h, g=g)
+    xo, so = run_v2rdm(o, o.guess("random"), SDPOptions(1e-6, 1e-6, 1e-9, 10000, 100000), 500)
+    assert so.is_converged()
+    assert abs(e - float(o.c @ xo)) <= E_TOL
+
+
+def test_host_callback_solver_matches_device_solve(cuda_device):
+    """libsdp-shaped solver with host callbacks (hilbert's evaluate_Au / evaluate_ATu)."""
+    o = OracleProblem(4, 2, 2, "DQG", True, True, hubbard=(1.0, 2.0))
+    opts = hb.Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6, "MAXITER": 100000})
+    s = hb.BPSDPSolver(o.n_primal, o.n_dual, opts)
+    x = o.guess("random")
+    while not s.is_converged() and s.oiter_total() < 100000:
+        s.solve(x, o.b, o.c, o.dims, 500, o.Au, o.ATu)
+    assert s.is_converged()
+    p = hb.V2RDMProblem(4, 2, 2, hubbard_multiplicity=True)
+    xd, st = p.solve(o.guess("random"), o.b, o.c, hb.Options({"R_CONVERGENCE": 1e-6,
+                                                               "E_CONVERGENCE": 1e-6,
+                                                               "MAXITER": 100000,
+                                                               "MU_UPDATE_FREQUENCY": 500}))
+    assert st["converged"]
+    assert abs(float(o.c @ x) - st["energy"]) <= E_TOL
+    # state accessors of the libsdp surface
+    assert s.get_y().shape == (o.n_dual,) and s.get_z().shape == (o.n_primal,)
+    assert s.iiter_total() > 0 and s.get_mu() > 0
+
+
+def test_monitor_protocol(cuda_device):
+    """mu is fixed inside one solve() call of MU_UPDATE_FREQUENCY iterations and
+    becomes mu * eps_p / eps_d afterwards (tests/mcpdft/output.ref:495-506)."""
+    rows = []
+    p = hb.V2RDMProblem(4, 2, 2, hubbard_multiplicity=True)
+    opts = hb.Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6, "MAXITER": 60,
+                       "MU_UPDATE_FREQUENCY": 20})
+    p.solve(p.guess("RANDOM"), p.b(), p.c_hubbard(1.0, 4.0), opts,
+            monitor=lambda pl, oi, ii, ep, ed, mu, erp, erd, d: rows.append((oi, mu, erp, erd)))
+    assert [r[0] for r in rows] == list(range(60))
+    assert rows[0][1] == pytest.approx(0.1)
+    assert all(r[1] == rows[0][1] for r in rows[:20])
+    assert rows[20][1] == pytest.approx(rows[19][1] * rows[19][2] / rows[19][3], rel=1e-12)

@@ -1,0 +1,113 @@
+"""The product library's host-side problem (sizes, b, c, guesses, packed
+operator) through the C ABI, without a GPU, against the oracle."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, case_kwargs
+import hilbert_b200 as hb
+from hilbert_b200 import _capi
+from oracle.maps import OracleProblem
+
+
+def packed_apply(rp, ent, pal, x):
+    """Test-side replay of the packed rows: left-to-right sum, second partial for flagged terms."""
+    out = np.zeros(len(rp) - 1)
+    col = (ent & ((1 << 27) - 1)).astype(np.int64)
+    code = ((ent >> 27) & 15).astype(np.int64)
+    grp = (ent >> 31).astype(bool)
+    for r in range(len(rp) - 1):
+        a0 = 0.0
+        a1 = 0.0
+        g = False
+        for k in range(rp[r], rp[r + 1]):
+            v = pal[code[k]] * x[col[k]]
+            g = g or grp[k]
+            if g:
+                a1 = a1 + v
+            else:
+                a0 = a0 + v
+        out[r] = a0 + a1 if g else a0
+    return out
+
+
+def operator(prob, transposed):
+    lib = prob._lib
+    nrows, nnz, npal = ctypes.c_long(), ctypes.c_long(), ctypes.c_int()
+    _capi.check(lib.v2b_problem_operator_size(prob._h, int(transposed), ctypes.byref(nrows),
+                                              ctypes.byref(nnz), ctypes.byref(npal)))
+    rp = np.zeros(nrows.value + 1, np.uint32)
+    ent = np.zeros(max(nnz.value, 1), np.uint32)
+    pal = np.zeros(max(npal.value, 1))
+    _capi.check(lib.v2b_problem_operator(
+        prob._h, int(transposed), rp.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+        ent.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+        pal.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    return rp.astype(np.int64), ent[:nnz.value], pal
+
+
+def product_problem(kw):
+    return hb.V2RDMProblem(kw["n"], kw["na"], kw["nb"], kw["positivity"], kw["constrain_spin"],
+                           kw["constrain_sz"], hubbard_multiplicity="hubbard" in kw)
+
+
+def test_header_symbols_exported():
+    header = open(os.path.join(ROOT, "include", "v2rdm_b200.h")).read()
+    declared = set(re.findall(r"\b(v2b_[A-Za-z_]+)\s*\(", header))
+    declared -= {"v2b_sdp_callback", "v2b_sdp_monitor"}
+    lib = _capi.load()
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert declared == set(_capi.EXPORTS)
+
+
+@pytest.mark.parametrize("name", ["hub2_dqg", "hub4_dqg", "hub4_d_nospin", "ext3_dqg_triplet",
+                                  "ext4_dq_nosz", "ext4_dg_doublet", "ext1_dqg"])
+def test_host_problem_matches_golden(golden, name):
+    case = golden[name]
+    kw = case_kwargs(case)
+    p = product_problem(kw)
+    assert list(p.dims) == list(case["dims"])
+    assert np.array_equal(p.b(), case["b"])
+    if "hubbard" in kw:
+        c = p.c_hubbard(*kw["hubbard"])
+    else:
+        c = p.c_external(kw["h"], kw["g"])
+    assert np.array_equal(c, case["c"])
+    assert np.array_equal(p.guess("RANDOM"), case["x_random"])
+    assert np.array_equal(p.guess("HF"), case["x_hf"])
+    rp, ent, pal = operator(p, False)
+    assert len(pal) <= 16
+    assert np.array_equal(packed_apply(rp, ent, pal, case["x"]), case["Ax"])
+    rp, ent, pal = operator(p, True)
+    assert np.array_equal(packed_apply(rp, ent, pal, case["y"]), case["ATy"])
+
+
+def test_layout_helper_matches_library():
+    for args in [(4, 2, 2, "DQG", True), (3, 2, 1, "DQG", True), (4, 2, 2, "D", False),
+                 (4, 2, 1, "DG", True)]:
+        p = hb.V2RDMProblem(args[0], args[1], args[2], args[3], args[4])
+        assert [d for _, d in hb.block_layout(*args)] == list(p.dims)
+
+
+def test_bad_arguments_are_rejected():
+    with pytest.raises(hb.V2BError):
+        hb.V2RDMProblem(4, 5, 2)
+    with pytest.raises(hb.V2BError):
+        hb.V2RDMProblem(0, 0, 0)
+    with pytest.raises(ValueError):
+        hb.V2RDMProblem(4, 2, 2, positivity="DQGT2")
+
+
+def test_device_calls_fail_loudly_without_gpu():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    p = hb.V2RDMProblem(2, 1, 1, "DQG", True, True, True)
+    x = np.zeros(p.n_primal)
+    with pytest.raises(hb.V2BError) as e:
+        p.solve(x, p.b(), p.c_hubbard(1.0, 4.0), hb.Options())
+    assert e.value.code == _capi.V2B_NO_DEVICE

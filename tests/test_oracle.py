@@ -1,0 +1,88 @@
+"""The C restatement (oracle) against the reference's golden vectors and,
+where oracle/_ref is built, against hilbert's own compiled map code."""
+import itertools
+
+import numpy as np
+import pytest
+
+from conftest import case_kwargs
+from oracle.maps import OracleProblem, RefProblem, ref_available
+
+
+def same(a, b):
+    """equal as float64 values (the sign of a zero is not compared)"""
+    return a.shape == b.shape and np.array_equal(a, b)
+
+
+def test_golden_cases_present(golden):
+    assert len(golden) >= 8
+
+
+@pytest.mark.parametrize("name", ["hub2_dqg", "hub4_dqg", "hub4_d_nospin", "ext3_dqg_triplet",
+                                  "ext4_dq_nosz", "ext4_dg_doublet", "ext5_dqg", "ext1_dqg"])
+def test_oracle_matches_golden(golden, name):
+    case = golden[name]
+    kw = case_kwargs(case)
+    o = OracleProblem(**kw)
+    assert list(o.dims) == list(case["dims"])
+    bas_ab, ibas_ab, bas_aa, ibas_aa = o.tables()
+    assert np.array_equal(bas_ab, case["bas_ab"]) and np.array_equal(ibas_ab, case["ibas_ab"])
+    assert np.array_equal(bas_aa, case["bas_aa"]) and np.array_equal(ibas_aa, case["ibas_aa"])
+    assert same(o.b, case["b"])
+    assert same(o.c, case["c"])
+    assert same(o.guess("random"), case["x_random"])
+    assert same(o.guess("hf"), case["x_hf"])
+    # bit-exact maps
+    assert same(o.Au(case["x"]), case["Ax"])
+    assert same(o.ATu(case["y"]), case["ATy"])
+
+
+def test_sizes_match_reference_counts():
+    # SURVEY-independent anchors: the reference prints n_primal/n_dual; the
+    # (6,6) D2h deck counts are molecular, so pin the C1 formula on config sizes
+    o = OracleProblem(8, 4, 4, "DQG", True, True, hubbard=(1.0, 4.0))
+    assert (o.n_primal, o.n_dual) == (40256, 47028)
+    o = OracleProblem(20, 10, 10, "DQG", True, True, h=np.zeros((20, 20)), g=np.zeros((20,) * 4))
+    assert (o.n_primal, o.n_dual) == (1586000, 1856304)
+    assert sorted(set(o.dims)) == [20, 190, 400, 800]
+
+
+def test_adjoint_identity():
+    rng = np.random.default_rng(7)
+    for n, na, nb, pos, spin, sz in [(4, 2, 2, "DQG", 1, 1), (5, 3, 2, "DQG", 1, 0), (3, 1, 1, "DG", 0, 1)]:
+        o = OracleProblem(n, na, nb, pos, spin, sz, h=rng.standard_normal((n, n)),
+                          g=rng.standard_normal((n,) * 4))
+        x = rng.standard_normal(o.n_primal)
+        y = rng.standard_normal(o.n_dual)
+        lhs = float(o.Au(x) @ y)
+        rhs = float(x @ o.ATu(y))
+        assert abs(lhs - rhs) <= 1e-11 * max(1.0, abs(lhs))
+
+
+def test_hf_guess_satisfies_d_constraints():
+    # a pure determinant satisfies the trace, D1+Q1=I and partial-trace rows exactly
+    o = OracleProblem(6, 3, 3, "DQG", True, True, hubbard=(1.0, 4.0))
+    x = o.guess("hf")
+    r = o.Au(x) - o.b
+    n, gab, gaa = 6, 36, 15
+    n_d_rows = 3 + 2 * gaa * gaa + gab * gab + 2 * n * n + 4 * n * n
+    assert np.max(np.abs(r[:n_d_rows])) == 0.0
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+def test_oracle_bit_exact_against_reference_grid():
+    rng = np.random.default_rng(3)
+    for n, na, nb, pos, spin, sz in itertools.product([1, 2, 3, 4], [0, 1, 2], [0, 1, 2],
+                                                      ["D", "DQ", "DG", "DQG"], [0, 1], [0, 1]):
+        if na > n or nb > n:
+            continue
+        kw = dict(h=rng.standard_normal((n, n)), g=rng.standard_normal((n,) * 4))
+        r = RefProblem(n, na, nb, pos, spin, sz, **kw)
+        o = OracleProblem(n, na, nb, pos, spin, sz, **kw)
+        assert (r.n_primal, r.n_dual) == (o.n_primal, o.n_dual)
+        assert list(r.dims) == list(o.dims)
+        assert r.offsets == o.offsets
+        x = rng.standard_normal(r.n_primal)
+        y = rng.standard_normal(r.n_dual)
+        assert same(r.Au(x), o.Au(x)) and same(r.ATu(y), o.ATu(y))
+        assert same(r.b, o.b) and same(r.c, o.c)
