@@ -74,6 +74,28 @@ __device__ __forceinline__ double block_sum(double v, double *red /* >= 32 */) {
     return s;
 }
 
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block max; result valid in thread 0.
+__device__ __forceinline__ double block_max(double v, double *red /* >= 32 */) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    v = warp_max(v);
+    __syncthreads();
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        s = lane < nw ? red[lane] : 0.0;
+        s = warp_max(s);
+    }
+    return s;
+}
+
 // Deterministic sum of n partials, every thread of the block gets the result.
 __device__ __forceinline__ double sum_partials(const double *part, int n, double *bcast) {
     if (threadIdx.x < 32) {
@@ -123,7 +145,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *bar, int *status, long lo
                     fail = 1;
                     break;
                 }
-                __nanosleep(128);
+                __nanosleep(32);
             }
         }
         __threadfence();

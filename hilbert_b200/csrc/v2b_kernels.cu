@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(kJacobiThreads)
                           double *__restrict__ zo, double mu, const int64_t *__restrict__ boff,
                           const int *__restrict__ bdim, double2 *__restrict__ rot,
                           const int64_t *__restrict__ rot_off, int max_sweeps, double rel_tol,
-                          int *status, int *sweeps_out) {
+                          int *status, int *sweeps_out, double *__restrict__ Vout) {
     extern __shared__ double sm[];
     const int blk = blockIdx.x;
     const int n = bdim[blk];
@@ -349,6 +349,11 @@ __global__ void __launch_bounds__(kJacobiThreads)
         }
     }
 
+    if (Vout)   // eigenvectors as columns: V[i][k] = component i of vector k
+        for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+            const int i = e / n, k = e % n;
+            Vout[off + e] = Vt[k * np + i];
+        }
     // U+ = sum_k lam_k^+ v_k v_k^T; x = U+ / mu; z = U+ - sym(U)
     const double inv_mu = 1.0 / mu;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {

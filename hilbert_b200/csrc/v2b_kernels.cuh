@@ -59,7 +59,8 @@ __global__ void jacobi_project_kernel(const double *__restrict__ U, double *__re
                                       const int64_t *__restrict__ boff,
                                       const int *__restrict__ bdim, double2 *__restrict__ rot,
                                       const int64_t *__restrict__ rot_off, int max_sweeps,
-                                      double rel_tol, int *status, int *sweeps_out);
+                                      double rel_tol, int *status, int *sweeps_out,
+                                      double *__restrict__ Vout);
 
 inline size_t jacobi_smem_bytes(int n) {
     const int np = n + (n & 1);

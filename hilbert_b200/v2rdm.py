@@ -236,6 +236,13 @@ class V2RDMProblem:
         check(self._lib.v2b_problem_profile(self._h, ms, n))
         return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNEL_CLASSES)}
 
+    def projection_counts(self):
+        """{"warm": n, "redo_warm": n, "cold": n} projections since creation"""
+        w, r, c = ctypes.c_long(), ctypes.c_long(), ctypes.c_long()
+        check(self._lib.v2b_problem_projection_counts(self._h, ctypes.byref(w), ctypes.byref(r),
+                                                      ctypes.byref(c)))
+        return {"warm": w.value, "redo_warm": r.value, "cold": c.value}
+
     def stream_handle(self):
         return self._lib.v2b_problem_stream(self._h)
 
