@@ -1,28 +1,16 @@
-// Warm-started PSD projection of the BPSDP blocks (sm_100a, FP64).
+// Batched FP64 GEMM tiles for the warm-started PSD projection (sm_100a).
 //
 // Between outer iterations U = mu x + A^T y - c changes little, so the
-// previous eigenvectors V are an excellent basis.  Each iteration refines V
-// by one Newton step for the symmetric eigenproblem (Ogita & Aishima,
-// "Iterative refinement for symmetric eigenvalue problems", Japan J. Indust.
-// Appl. Math. 35, 1007 (2018)) and then projects in the refined basis:
-//
-//   round 1:  W = U V0,  S = V0^T W,  G = V0^T V0,  R = I - G
-//             lam_i = S_ii / G_ii,  delta = 2 (||S - diag(lam)||_F + ||S||_F ||R||_F)
-//             E_ij = (S_ij + lam_j R_ij) / (lam_j - lam_i)   if |lam_j - lam_i| > delta
-//                  = R_ij / 2                                 otherwise (and i = j)
-//             V1 = V0 + V0 E
-//   round 2:  S, G, R for V1; M = S + (R o (lam_i + lam_j)/2)  (basis re-orthonormalised
-//             to first order), M+ from the first-order (Daleckii-Krein) formula
-//             M+_ij = Gamma_ij M_ij, Gamma_ij = (m_i+ - m_j+) / (m_i - m_j),
-//             P = M+ + R o (m_i+ + m_j+)/2,   U+ = V1 P V1^T,   x = U+/mu,  z = U+ - U.
-//
-// All n^3 work is batched GEMM tiles over every block of the problem
-// (gemm_tiles_kernel); the elementwise steps run one CTA per block
-// (refine_kernel).  Round 2 estimates the relative error of U+ it leaves,
-//   max over pairs straddling zero of corr_ij^2 |lam_i - lam_j| / ||U||_F + max |R_ij|^2,
-// and flags the block when it exceeds the tolerance; the caller then repeats
-// the warm step from the refined basis (one more Newton round) and falls back
-// to the Jacobi kernel if that is still not enough.
+// eigenvectors of the previous iteration (rows of Vt) nearly diagonalise the
+// new block: per iteration
+//   W  = sym(U) Vt^T          gemm<N,T>
+//   T0 = Vt W                 gemm<N,N>      (= V^T U V, nearly diagonal)
+//   selective Jacobi on T0    jacobi_warm_kernel (shared memory, one CTA per block)
+//   Y  = Vt^T P               gemm<T,N>
+//   U+ = Y Vt                 gemm<N,N> with the projection epilogue
+//                             x = U+ / mu,  z = U+ - sym(U)
+// Every gemm launch covers all blocks of the problem: the grid is the list of
+// 64 x 64 output tiles of every block.
 #include "v2b_eig.cuh"
 
 namespace v2b {
@@ -110,10 +98,11 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+template __global__ void gemm_tiles_kernel<false, true, kEpiStore>(GEMM_ARGS);
 template __global__ void gemm_tiles_kernel<false, false, kEpiStore>(GEMM_ARGS);
 template __global__ void gemm_tiles_kernel<true, false, kEpiStore>(GEMM_ARGS);
+template __global__ void gemm_tiles_kernel<false, false, kEpiProject>(GEMM_ARGS);
 template __global__ void gemm_tiles_kernel<false, false, kEpiAdd>(GEMM_ARGS);
-template __global__ void gemm_tiles_kernel<false, true, kEpiProject>(GEMM_ARGS);
 
 // Us = (U + U^T) / 2 per block, tile by tile
 __global__ void symmetrize_kernel(const double *__restrict__ U, double *__restrict__ Us,
@@ -126,86 +115,6 @@ __global__ void symmetrize_kernel(const double *__restrict__ U, double *__restri
         const int r = t.y * 64 + e / 64, c = t.z * 64 + e % 64;
         if (r < n && c < n)
             Us[off + (int64_t)r * n + c] = 0.5 * (U[off + (int64_t)r * n + c] + U[off + (int64_t)c * n + r]);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// One CTA per block.  mode 0: Newton correction E (written to Eo).
-// mode 1: projected middle factor P (written to Eo) for U+ = V P V^T, and the
-// size of the correction that was not applied (block flagged when large).
-__global__ void __launch_bounds__(kRefineThreads)
-    refine_kernel(const double *__restrict__ S, const double *__restrict__ G,
-                  double *__restrict__ Eo, double *__restrict__ lam_buf,
-                  const int64_t *__restrict__ loff, const int64_t *__restrict__ boff,
-                  const int *__restrict__ bdim, int mode, double flag_tol,
-                  int *__restrict__ flags) {
-    const int blk = blockIdx.x, n = bdim[blk];
-    if (n <= 0) return;
-    const int64_t off = boff[blk];
-    double *lam = lam_buf + loff[blk];
-    __shared__ double red[32];
-    __shared__ double s_delta, s_max;
-    // lam_i = S_ii / G_ii
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
-        lam[i] = S[off + (int64_t)i * n + i] / G[off + (int64_t)i * n + i];
-    __syncthreads();
-    double off2 = 0.0, r2 = 0.0, s2 = 0.0;
-    for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x) {
-        const int i = (int)(e / n), j = (int)(e % n);
-        const double s = 0.5 * (S[off + e] + S[off + (int64_t)j * n + i]);
-        const double r = (i == j ? 1.0 : 0.0) - G[off + e];
-        const double d = (i == j) ? s - lam[i] : s;
-        off2 += d * d;
-        r2 += r * r;
-        s2 += s * s;
-    }
-    off2 = block_sum(off2, red);
-    r2 = block_sum(r2, red);
-    s2 = block_sum(s2, red);
-    if (threadIdx.x == 0) {
-        s_delta = 2.0 * (sqrt(off2) + sqrt(s2) * sqrt(r2));
-        s_max = 0.0;
-    }
-    __syncthreads();
-    const double delta = s_delta;
-    double m_straddle = 0.0, m_orth = 0.0;
-    for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x) {
-        const int i = (int)(e / n), j = (int)(e % n);
-        const double s = 0.5 * (S[off + e] + S[off + (int64_t)j * n + i]);
-        const double r = (i == j ? 1.0 : 0.0) - G[off + e];
-        const double li = lam[i], lj = lam[j];
-        double corr;
-        if (i != j && fabs(lj - li) > delta) corr = (s + lj * r) / (lj - li);
-        else corr = 0.5 * r;
-        if (mode == 0) {
-            Eo[off + e] = corr;
-        } else {
-            // second-order error of leaving (i, j) unresolved matters only when
-            // the pair straddles zero; non-orthonormality enters squared
-            if (li * lj < 0.0) m_straddle = fmax(m_straddle, corr * corr * fabs(lj - li));
-            m_orth = fmax(m_orth, fabs(r));
-            // middle factor in an orthonormal basis, to first order in R
-            const double m = (i == j) ? li : s + r * 0.5 * (li + lj);
-            const double pi = fmax(li, 0.0), pj = fmax(lj, 0.0);
-            double p;
-            if (i == j) {
-                p = pi + r * pi;
-            } else {
-                double gam;
-                if (li != lj) gam = (pi - pj) / (li - lj);
-                else gam = li > 0.0 ? 1.0 : 0.0;
-                p = gam * m + r * 0.5 * (pi + pj);
-            }
-            Eo[off + e] = p;
-        }
-    }
-    if (mode == 1) {
-        m_straddle = block_max(m_straddle, red);
-        m_orth = block_max(m_orth, red);
-        if (threadIdx.x == 0) {
-            const double est = m_straddle / fmax(sqrt(s2), 1e-300) + m_orth * m_orth;
-            if (!(est <= flag_tol)) flags[blk] = 1;
-        }
     }
 }
 

@@ -1,4 +1,4 @@
-// Warm-started PSD projection kernels (see v2b_eig.cu).
+// Batched GEMM tiles of the warm-started PSD projection (see v2b_eig.cu).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -11,7 +11,6 @@ namespace v2b {
 constexpr int kEpiStore = 0;     // C = op(A) op(B)
 constexpr int kEpiAdd = 1;       // C = Cin + op(A) op(B)
 constexpr int kEpiProject = 2;   // x = (op(A) op(B)) / mu, z = op(A) op(B) - Us
-constexpr int kRefineThreads = 512;
 constexpr int kGemmTile = 64;
 
 #define GEMM_ARGS                                                                           \
@@ -27,11 +26,5 @@ __global__ void gemm_tiles_kernel(GEMM_ARGS);
 __global__ void symmetrize_kernel(const double *__restrict__ U, double *__restrict__ Us,
                                   const int4 *__restrict__ tiles, const int64_t *__restrict__ boff,
                                   const int *__restrict__ bdim);
-
-__global__ void refine_kernel(const double *__restrict__ S, const double *__restrict__ G,
-                              double *__restrict__ Eo, double *__restrict__ lam_buf,
-                              const int64_t *__restrict__ loff, const int64_t *__restrict__ boff,
-                              const int *__restrict__ bdim, int mode, double flag_tol,
-                              int *__restrict__ flags);
 
 }  // namespace v2b

@@ -5,8 +5,8 @@
 //   spmv_AT_U_kernel     A^T.y and U = mu x + A^T y - c in one pass over A^T's rows
 //   cg_kernel            persistent conjugate-gradient solve of (A A^T) y = rhs
 //   stats_kernel         eps_p^2, eps_d^2, c.x, b.y (deterministic reductions)
-//   jacobi_project_kernel  per-block symmetric eigensolve (parallel cyclic
-//                        Jacobi in shared memory) and PSD split x = U+/mu, z = U+ - U
+//   jacobi_warm_kernel   per-block selective Jacobi on V^T U V in shared memory,
+//                        middle factor of U+ and the refined eigenvectors
 #include "v2b_kernels.cuh"
 
 namespace v2b {
@@ -221,17 +221,24 @@ __device__ __forceinline__ void rr_pair(int s, int k, int np, int &p, int &q) {
     q = a < b ? b : a;
 }
 
-// One CTA per PSD block (n <= kJacobiMaxDim).  The symmetrised block is
-// diagonalised in shared memory by parallel cyclic Jacobi (sym.schur2
-// rotations, Golub & Van Loan sec. 8.5); the rotations of every sweep are
-// recorded in global scratch and replayed afterwards on V^T held in the same
-// shared buffer, so only one n x n matrix is resident at a time.
+// One CTA per PSD block (n <= kJacobiMaxDim): selective parallel cyclic
+// Jacobi on T = V^T U V, where the rows of Vt (= V^T) are the previous
+// iteration's eigenvectors (the identity on a cold start).
+//
+// A pair (p, q) is rotated (sym.schur2, Golub & Van Loan sec. 8.5) only when
+// the first-order (Daleckii-Krein) projection formula could not settle it:
+//     t_pq^2 > gap_tol * ||T||_F * |t_pp - t_qq|   and   |t_pq| > abs_tol * ||T||_F.
+// Sweeps repeat until a sweep rotates nothing.  The kernel then writes the
+// middle factor of U+ = V P V^T,
+//     P_ii = max(t_ii, 0),   P_ij = t_ij (t_ii+ - t_jj+) / (t_ii - t_jj)   (i != j),
+// and replays the recorded rotations on Vt (rows p, q of Vt per rotation),
+// leaving the refined eigenvectors for the next iteration.
 __global__ void __launch_bounds__(kJacobiThreads)
-    jacobi_project_kernel(const double *__restrict__ U, double *__restrict__ xo,
-                          double *__restrict__ zo, double mu, const int64_t *__restrict__ boff,
-                          const int *__restrict__ bdim, double2 *__restrict__ rot,
-                          const int64_t *__restrict__ rot_off, int max_sweeps, double rel_tol,
-                          int *status, int *sweeps_out, double *__restrict__ Vout) {
+    jacobi_warm_kernel(const double *__restrict__ T0, double *__restrict__ Pout,
+                       double *__restrict__ Vt, const int64_t *__restrict__ boff,
+                       const int *__restrict__ bdim, double2 *__restrict__ rot,
+                       const int64_t *__restrict__ rot_off, int max_sweeps, double abs_tol,
+                       double gap_tol, int *status, int *rot_count) {
     extern __shared__ double sm[];
     const int blk = blockIdx.x;
     const int n = bdim[blk];
@@ -239,81 +246,93 @@ __global__ void __launch_bounds__(kJacobiThreads)
     const int64_t off = boff[blk];
     const int np = n + (n & 1);
     const int m = np / 2;
-    double *T = sm;                              // np*np
-    double2 *cs = (double2 *)(T + (size_t)np * np);  // m
-    double *lam = (double *)(cs + m);            // np
+    double *T = sm;                                   // np*np (later: Vt)
+    double2 *cs = (double2 *)(T + (size_t)np * np);   // m
+    int *act = (int *)(cs + m);                       // m
     __shared__ double red[32];
-    __shared__ int nrot;
-    __shared__ double s_tol;
+    __shared__ int nrot, nstep;
+    __shared__ double s_nrm;
 
-    const double *Ub = U + off;
+    const double *Tb = T0 + off;
     double fro = 0.0;
     for (int e = threadIdx.x; e < np * np; e += blockDim.x) {
         const int i = e / np, j = e % np;
         double v = 0.0;
-        if (i < n && j < n) v = 0.5 * (Ub[(int64_t)i * n + j] + Ub[(int64_t)j * n + i]);
+        if (i < n && j < n) v = 0.5 * (Tb[(int64_t)i * n + j] + Tb[(int64_t)j * n + i]);
         T[e] = v;
         fro += v * v;
     }
     fro = block_sum(fro, red);
-    if (threadIdx.x == 0) s_tol = rel_tol * sqrt(fro) + 1e-300;
+    if (threadIdx.x == 0) s_nrm = sqrt(fro);
     __syncthreads();
-    const double tol = s_tol;
+    const double nrm = s_nrm;
+    const double atol = abs_tol * nrm + 1e-300, gtol = gap_tol * nrm;
 
     double2 *rb = rot + rot_off[blk];
-    int sweep = 0;
+    int sweep = 0, total = 0;
     for (; sweep < max_sweeps; sweep++) {
         if (threadIdx.x == 0) nrot = 0;
         __syncthreads();
         for (int st = 0; st < np - 1; st++) {
+            if (threadIdx.x == 0) nstep = 0;
+            __syncthreads();
             for (int k = threadIdx.x; k < m; k += blockDim.x) {
                 int p, q;
                 rr_pair(st, k, np, p, q);
                 double c = 1.0, s = 0.0;
+                int a = 0;
                 if (q < n) {
                     const double apq = T[p * np + q];
-                    if (fabs(apq) > tol) {
-                        const double app = T[p * np + p], aqq = T[q * np + q];
+                    const double app = T[p * np + p], aqq = T[q * np + q];
+                    if (fabs(apq) > atol && apq * apq > gtol * fabs(aqq - app)) {
                         const double tau = (aqq - app) / (2.0 * apq);
                         const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + hypot(1.0, tau));
                         c = 1.0 / sqrt(1.0 + t * t);
                         s = t * c;
-                        atomicAdd(&nrot, 1);
+                        a = 1;
+                        atomicAdd(&nstep, 1);
                     }
                 }
                 cs[k] = make_double2(c, s);
+                act[k] = a;
                 rb[((int64_t)sweep * (np - 1) + st) * m + k] = make_double2(c, s);
             }
             __syncthreads();
-            // every element belongs to exactly one 2x2 block (P, Q), P <= Q
-            for (int it = threadIdx.x; it < m * m; it += blockDim.x) {
-                const int P = it / m, Q = it % m;
-                if (P > Q) continue;
-                const double2 cp = cs[P], cq = cs[Q];
-                int pP, qP, pQ, qQ;
-                rr_pair(st, P, np, pP, qP);
-                rr_pair(st, Q, np, pQ, qQ);
-                const double b11 = T[pP * np + pQ], b12 = T[pP * np + qQ];
-                const double b21 = T[qP * np + pQ], b22 = T[qP * np + qQ];
-                const double m11 = b11 * cq.x - b12 * cq.y, m12 = b11 * cq.y + b12 * cq.x;
-                const double m21 = b21 * cq.x - b22 * cq.y, m22 = b21 * cq.y + b22 * cq.x;
-                double n11 = cp.x * m11 - cp.y * m21, n12 = cp.x * m12 - cp.y * m22;
-                double n21 = cp.y * m11 + cp.x * m21, n22 = cp.y * m12 + cp.x * m22;
-                if (P == Q) {
-                    if (cp.y != 0.0) { n12 = 0.0; n21 = 0.0; }
-                    T[pP * np + pP] = n11;
-                    T[pP * np + qP] = n12;
-                    T[qP * np + pP] = n21;
-                    T[qP * np + qP] = n22;
-                } else {
-                    T[pP * np + pQ] = n11; T[pQ * np + pP] = n11;
-                    T[pP * np + qQ] = n12; T[qQ * np + pP] = n12;
-                    T[qP * np + pQ] = n21; T[pQ * np + qP] = n21;
-                    T[qP * np + qQ] = n22; T[qQ * np + qP] = n22;
+            const int active = nstep;
+            if (threadIdx.x == 0) nrot += active;
+            if (active) {
+                // 2x2 blocks (P, Q), P <= Q, touched by at least one rotation
+                for (int it = threadIdx.x; it < m * m; it += blockDim.x) {
+                    const int P = it / m, Q = it % m;
+                    if (P > Q || !(act[P] | act[Q])) continue;
+                    const double2 cp = cs[P], cq = cs[Q];
+                    int pP, qP, pQ, qQ;
+                    rr_pair(st, P, np, pP, qP);
+                    rr_pair(st, Q, np, pQ, qQ);
+                    const double b11 = T[pP * np + pQ], b12 = T[pP * np + qQ];
+                    const double b21 = T[qP * np + pQ], b22 = T[qP * np + qQ];
+                    const double m11 = b11 * cq.x - b12 * cq.y, m12 = b11 * cq.y + b12 * cq.x;
+                    const double m21 = b21 * cq.x - b22 * cq.y, m22 = b21 * cq.y + b22 * cq.x;
+                    double n11 = cp.x * m11 - cp.y * m21, n12 = cp.x * m12 - cp.y * m22;
+                    double n21 = cp.y * m11 + cp.x * m21, n22 = cp.y * m12 + cp.x * m22;
+                    if (P == Q) {
+                        n12 = 0.0;
+                        n21 = 0.0;
+                        T[pP * np + pP] = n11;
+                        T[pP * np + qP] = n12;
+                        T[qP * np + pP] = n21;
+                        T[qP * np + qP] = n22;
+                    } else {
+                        T[pP * np + pQ] = n11; T[pQ * np + pP] = n11;
+                        T[pP * np + qQ] = n12; T[qQ * np + pP] = n12;
+                        T[qP * np + pQ] = n21; T[pQ * np + qP] = n21;
+                        T[qP * np + qQ] = n22; T[qQ * np + qP] = n22;
+                    }
                 }
             }
             __syncthreads();
         }
+        total += nrot;
         const int done = (nrot == 0);
         __syncthreads();
         if (done) {
@@ -322,51 +341,74 @@ __global__ void __launch_bounds__(kJacobiThreads)
         }
     }
     if (threadIdx.x == 0) {
-        if (sweeps_out) sweeps_out[blk] = sweep;
-        if (sweep >= max_sweeps && nrot != 0) atomicMax(status, 1);   // not converged: flag only
+        if (rot_count) atomicAdd(rot_count, total);
+        if (sweep >= max_sweeps && nrot != 0) atomicAdd(status, 1);   // sweeps exhausted
     }
-    for (int i = threadIdx.x; i < np; i += blockDim.x) lam[i] = T[i * np + i];
+
+    // middle factor P of U+ = V P V^T (first-order in the remaining couplings)
+    double *Pb = Pout + off;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int i = e / n, j = e % n;
+        const double li = T[i * np + i];
+        double pv;
+        if (i == j) {
+            pv = fmax(li, 0.0);
+        } else {
+            const double lj = T[j * np + j];
+            const double pi = fmax(li, 0.0), pj = fmax(lj, 0.0);
+            const double gam = (li != lj) ? (pi - pj) / (li - lj) : (li > 0.0 ? 1.0 : 0.0);
+            pv = gam * T[i * np + j];
+        }
+        Pb[e] = pv;
+    }
     __syncthreads();
 
-    // replay: V^T (rows = eigenvectors) starts as the identity
-    double *Vt = T;
-    for (int e = threadIdx.x; e < np * np; e += blockDim.x) Vt[e] = (e / np == e % np) ? 1.0 : 0.0;
+    // replay the rotations on Vt (rows = eigenvectors)
+    double *V = T;
+    double *Vb = Vt + off;
+    for (int e = threadIdx.x; e < np * np; e += blockDim.x) {
+        const int i = e / np, j = e % np;
+        V[e] = (i < n && j < n) ? Vb[(int64_t)i * n + j] : (i == j ? 1.0 : 0.0);
+    }
     __syncthreads();
     for (int sw = 0; sw < sweep; sw++) {
         for (int st = 0; st < np - 1; st++) {
             const double2 *rs = rb + ((int64_t)sw * (np - 1) + st) * m;
             for (int it = threadIdx.x; it < m * np; it += blockDim.x) {
                 const int k = it / np, j = it % np;
-                const double2 r = __ldg(rs + k);
+                const double2 r = rs[k];
                 if (r.y == 0.0) continue;
                 int p, q;
                 rr_pair(st, k, np, p, q);
-                const double vp = Vt[p * np + j], vq = Vt[q * np + j];
-                Vt[p * np + j] = r.x * vp - r.y * vq;
-                Vt[q * np + j] = r.y * vp + r.x * vq;
+                const double vp = V[p * np + j], vq = V[q * np + j];
+                V[p * np + j] = r.x * vp - r.y * vq;
+                V[q * np + j] = r.y * vp + r.x * vq;
             }
             __syncthreads();
         }
     }
-
-    if (Vout)   // eigenvectors as columns: V[i][k] = component i of vector k
-        for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-            const int i = e / n, k = e % n;
-            Vout[off + e] = Vt[k * np + i];
-        }
-    // U+ = sum_k lam_k^+ v_k v_k^T; x = U+ / mu; z = U+ - sym(U)
-    const double inv_mu = 1.0 / mu;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int i = e / n, j = e % n;
-        double acc = 0.0;
-        for (int k = 0; k < n; k++) {
-            const double l = lam[k];
-            if (l > 0.0) acc += l * Vt[k * np + i] * Vt[k * np + j];
-        }
-        const double us = 0.5 * (Ub[(int64_t)i * n + j] + Ub[(int64_t)j * n + i]);
-        xo[off + e] = acc * inv_mu;
-        zo[off + e] = acc - us;
+        Vb[e] = V[i * np + j];
     }
+}
+
+// Vt <- identity on every block (cold start of the warm path)
+__global__ void identity_blocks_kernel(double *__restrict__ Vt, const int64_t *__restrict__ boff,
+                                       const int *__restrict__ bdim) {
+    const int n = bdim[blockIdx.x];
+    const int64_t off = boff[blockIdx.x];
+    for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x)
+        Vt[off + e] = (e / n == e % n) ? 1.0 : 0.0;
+}
+
+// H = (I - G) / 2 for the re-orthonormalisation Vt <- Vt + H Vt
+__global__ void half_residual_kernel(const double *__restrict__ G, double *__restrict__ H,
+                                     const int64_t *__restrict__ boff, const int *__restrict__ bdim) {
+    const int n = bdim[blockIdx.x];
+    const int64_t off = boff[blockIdx.x];
+    for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x)
+        H[off + e] = 0.5 * (((e / n == e % n) ? 1.0 : 0.0) - G[off + e]);
 }
 
 }  // namespace v2b

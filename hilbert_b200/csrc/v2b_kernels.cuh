@@ -54,18 +54,19 @@ __global__ void stats_kernel(const double *__restrict__ Ax, const double *__rest
                              const double *__restrict__ y, int64_t np, int64_t nd,
                              double *__restrict__ partials, unsigned int *counter,
                              double *__restrict__ out, int *status);
-__global__ void jacobi_project_kernel(const double *__restrict__ U, double *__restrict__ xo,
-                                      double *__restrict__ zo, double mu,
-                                      const int64_t *__restrict__ boff,
-                                      const int *__restrict__ bdim, double2 *__restrict__ rot,
-                                      const int64_t *__restrict__ rot_off, int max_sweeps,
-                                      double rel_tol, int *status, int *sweeps_out,
-                                      double *__restrict__ Vout);
+__global__ void jacobi_warm_kernel(const double *__restrict__ T0, double *__restrict__ Pout,
+                                   double *__restrict__ Vt, const int64_t *__restrict__ boff,
+                                   const int *__restrict__ bdim, double2 *__restrict__ rot,
+                                   const int64_t *__restrict__ rot_off, int max_sweeps,
+                                   double abs_tol, double gap_tol, int *status, int *rot_count);
+__global__ void identity_blocks_kernel(double *__restrict__ Vt, const int64_t *__restrict__ boff,
+                                       const int *__restrict__ bdim);
+__global__ void half_residual_kernel(const double *__restrict__ G, double *__restrict__ H,
+                                     const int64_t *__restrict__ boff, const int *__restrict__ bdim);
 
 inline size_t jacobi_smem_bytes(int n) {
     const int np = n + (n & 1);
-    return (size_t)np * np * sizeof(double) + (size_t)(np / 2) * sizeof(double2) +
-           (size_t)np * sizeof(double);
+    return (size_t)np * np * sizeof(double) + (size_t)(np / 2) * (sizeof(double2) + sizeof(int));
 }
 
 }  // namespace v2b

@@ -91,110 +91,83 @@ struct DeviceOp {
     }
 };
 
-// Per-block PSD projection for a fixed list of block sizes.
-//   cold(): Jacobi in shared memory (blocks up to kJacobiMaxDim), also
-//           returns the eigenvectors that seed the warm path;
-//   warm(): Newton refinement of the previous eigenvectors + projection in
-//           the refined basis, all as batched GEMM tiles (any block size).
-// project() chooses warm when eigenvectors exist; blocks the warm path
-// flags are re-solved cold by the caller after its next synchronisation.
+// Per-block PSD projection for a fixed list of block sizes (blocks up to
+// kJacobiMaxDim).  The rows of Vt hold each block's eigenvectors from the
+// previous call (the identity before the first), so every call is
+//   symmetrize; W = Us Vt^T; T0 = Vt W; selective Jacobi on T0 (rotations
+//   replayed onto Vt); Y = Vt^T P; U+ = Y Vt -> x, z.
+// Every kReorthEvery calls Vt is re-orthonormalised, Vt <- Vt + (I - Vt Vt^T) Vt / 2.
 struct ProjectPlan {
+    static constexpr int kReorthEvery = 64;
     std::vector<int> dims;
     int nblk = 0;
     int64_t total = 0;
-    int64_t *boff = nullptr, *loff = nullptr, *rot_off = nullptr;
-    int *bdim = nullptr, *sweeps = nullptr, *flags = nullptr;
+    int64_t *boff = nullptr, *rot_off = nullptr;
+    int *bdim = nullptr, *counters = nullptr;   // counters[0] sweep overruns, [1] rotations
     int4 *tiles = nullptr;
     int ntiles = 0;
     double2 *rot = nullptr;
-    double *V = nullptr, *V1 = nullptr, *Us = nullptr, *W = nullptr, *S = nullptr, *G = nullptr,
-           *E = nullptr, *lam = nullptr;
-    int *h_flags = nullptr;   // pinned
+    double *Vt = nullptr, *Vt2 = nullptr, *Us = nullptr, *W = nullptr, *T = nullptr, *P = nullptr;
     size_t smem = 0;
     int max_sweeps = 30;
     int max_dim = 0;
-    bool have_vectors = false;
+    bool fresh = true;
     bool built = false;
-    double flag_tol = 1e-9;   // relative error estimate of U+ that triggers a redo
-    long redo_warm = 0;
-    long cold_solves = 0, warm_solves = 0;
+    long calls = 0;
+    double abs_tol = 1e-14, gap_tol = 1e-13;
 
     void build(const std::vector<int> &d) {
         dims = d;
         nblk = (int)d.size();
-        std::vector<int64_t> off(nblk), roff(nblk), lo(nblk);
+        std::vector<int64_t> off(nblk), roff(nblk);
         std::vector<int4> tl;
-        int64_t o = 0, ro = 0, l = 0;
+        int64_t o = 0, ro = 0;
         smem = 0;
         max_dim = 0;
         for (int i = 0; i < nblk; i++) {
             if (d[i] < 0) throw std::invalid_argument("negative block dimension");
+            if (d[i] > v2b::kJacobiMaxDim)
+                throw std::invalid_argument("PSD block of dimension " + std::to_string(d[i]) +
+                                            " exceeds the shared-memory Jacobi limit " +
+                                            std::to_string(v2b::kJacobiMaxDim));
             off[i] = o;
             o += (int64_t)d[i] * d[i];
-            lo[i] = l;
-            l += d[i];
             max_dim = std::max(max_dim, d[i]);
             const int nt = (d[i] + v2b::kGemmTile - 1) / v2b::kGemmTile;
             for (int a = 0; a < nt; a++)
                 for (int b = 0; b < nt; b++) tl.push_back(make_int4(i, a, b, 0));
-            if (d[i] <= v2b::kJacobiMaxDim) {
-                const int np = d[i] + (d[i] & 1);
-                roff[i] = ro;
-                ro += (int64_t)max_sweeps * std::max(np - 1, 0) * (np / 2);
-                smem = std::max(smem, v2b::jacobi_smem_bytes(d[i]));
-            } else {
-                roff[i] = ro;
-            }
+            const int np = d[i] + (d[i] & 1);
+            roff[i] = ro;
+            ro += (int64_t)max_sweeps * std::max(np - 1, 0) * (np / 2);
+            smem = std::max(smem, v2b::jacobi_smem_bytes(d[i]));
         }
         total = o;
         ntiles = (int)tl.size();
         boff = dalloc<int64_t>(nblk);
-        loff = dalloc<int64_t>(nblk);
         rot_off = dalloc<int64_t>(nblk);
         bdim = dalloc<int>(nblk);
-        sweeps = dalloc<int>(nblk);
-        flags = dalloc<int>(nblk);
+        counters = dalloc<int>(2);
         tiles = dalloc<int4>(std::max(ntiles, 1));
         rot = dalloc<double2>(ro);
-        for (double **b : {&V, &V1, &Us, &W, &S, &G, &E}) *b = dalloc<double>(total);
-        lam = dalloc<double>(l);
-        V2B_CK(cudaMallocHost(&h_flags, std::max(nblk, 1) * sizeof(int)));
+        for (double **b : {&Vt, &Vt2, &Us, &W, &T, &P}) *b = dalloc<double>(total);
         V2B_CK(cudaMemcpy(boff, off.data(), nblk * 8, cudaMemcpyHostToDevice));
-        V2B_CK(cudaMemcpy(loff, lo.data(), nblk * 8, cudaMemcpyHostToDevice));
         V2B_CK(cudaMemcpy(rot_off, roff.data(), nblk * 8, cudaMemcpyHostToDevice));
         V2B_CK(cudaMemcpy(bdim, d.data(), nblk * 4, cudaMemcpyHostToDevice));
-        V2B_CK(cudaMemset(flags, 0, std::max(nblk, 1) * 4));
+        V2B_CK(cudaMemset(counters, 0, 8));
         if (ntiles) V2B_CK(cudaMemcpy(tiles, tl.data(), ntiles * sizeof(int4), cudaMemcpyHostToDevice));
         if (smem)
-            V2B_CK(cudaFuncSetAttribute(v2b::jacobi_project_kernel,
+            V2B_CK(cudaFuncSetAttribute(v2b::jacobi_warm_kernel,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        have_vectors = false;
+        fresh = true;
         built = true;
     }
     void release() {
         if (!built) return;
-        for (void *q : {(void *)boff, (void *)loff, (void *)rot_off, (void *)bdim, (void *)sweeps,
-                        (void *)flags, (void *)tiles, (void *)rot, (void *)V, (void *)V1, (void *)Us,
-                        (void *)W, (void *)S, (void *)G, (void *)E, (void *)lam})
+        for (void *q : {(void *)boff, (void *)rot_off, (void *)bdim, (void *)counters, (void *)tiles,
+                        (void *)rot, (void *)Vt, (void *)Vt2, (void *)Us, (void *)W, (void *)T,
+                        (void *)P})
             cudaFree(q);
-        if (h_flags) cudaFreeHost(h_flags);
-        h_flags = nullptr;
         built = false;
-    }
-
-    void cold(const double *U, double mu, double *x, double *z, int *status, cudaStream_t s,
-              long &launches) {
-        if (nblk == 0) return;
-        if (max_dim > v2b::kJacobiMaxDim)
-            throw std::invalid_argument("PSD block of dimension " + std::to_string(max_dim) +
-                                        " needs a cold eigensolve larger than the shared-memory "
-                                        "Jacobi limit " + std::to_string(v2b::kJacobiMaxDim));
-        v2b::jacobi_project_kernel<<<nblk, v2b::kJacobiThreads, smem, s>>>(
-            U, x, z, mu, boff, bdim, rot, rot_off, max_sweeps, 1e-14, status, sweeps, V);
-        V2B_CK(cudaGetLastError());
-        launches++;
-        have_vectors = true;
-        cold_solves++;
     }
 
     template <bool TA, bool TB, int EPI>
@@ -206,52 +179,37 @@ struct ProjectPlan {
         launches++;
     }
 
-    void warm(const double *U, double mu, double *x, double *z, cudaStream_t s, long &launches) {
+    // forget the eigenvector basis: the next projection starts from V = I
+    void reset() { fresh = true; }
+
+    void project(const double *U, double mu, double *x, double *z, cudaStream_t s, long &launches) {
         using namespace v2b;
+        if (nblk == 0 || ntiles == 0) return;
+        if (fresh) {
+            identity_blocks_kernel<<<nblk, 256, 0, s>>>(Vt, boff, bdim);
+            V2B_CK(cudaGetLastError());
+            launches++;
+            fresh = false;
+        } else if (++calls % kReorthEvery == 0) {
+            gemm<false, true, kEpiStore>(Vt, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches);
+            half_residual_kernel<<<nblk, 256, 0, s>>>(W, T, boff, bdim);
+            V2B_CK(cudaGetLastError());
+            launches++;
+            gemm<false, false, kEpiAdd>(T, Vt, Vt2, Vt, 0.0, nullptr, nullptr, s, launches);
+            std::swap(Vt, Vt2);
+        }
         symmetrize_kernel<<<ntiles, 256, 0, s>>>(U, Us, tiles, boff, bdim);
         V2B_CK(cudaGetLastError());
         launches++;
-        // round 1: Newton correction of V
-        gemm<false, false, kEpiStore>(Us, V, W, nullptr, 0.0, nullptr, nullptr, s, launches);
-        gemm<true, false, kEpiStore>(V, W, S, nullptr, 0.0, nullptr, nullptr, s, launches);
-        gemm<true, false, kEpiStore>(V, V, G, nullptr, 0.0, nullptr, nullptr, s, launches);
-        refine_kernel<<<nblk, kRefineThreads, 0, s>>>(S, G, E, lam, loff, boff, bdim, 0, flag_tol, flags);
+        gemm<false, true, kEpiStore>(Us, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches);
+        gemm<false, false, kEpiStore>(Vt, W, T, nullptr, 0.0, nullptr, nullptr, s, launches);
+        jacobi_warm_kernel<<<nblk, kJacobiThreads, smem, s>>>(T, P, Vt, boff, bdim, rot, rot_off,
+                                                              max_sweeps, abs_tol, gap_tol,
+                                                              counters, counters + 1);
         V2B_CK(cudaGetLastError());
         launches++;
-        gemm<false, false, kEpiAdd>(V, E, V1, V, 0.0, nullptr, nullptr, s, launches);
-        // round 2: project in the refined basis
-        gemm<false, false, kEpiStore>(Us, V1, W, nullptr, 0.0, nullptr, nullptr, s, launches);
-        gemm<true, false, kEpiStore>(V1, W, S, nullptr, 0.0, nullptr, nullptr, s, launches);
-        gemm<true, false, kEpiStore>(V1, V1, G, nullptr, 0.0, nullptr, nullptr, s, launches);
-        refine_kernel<<<nblk, kRefineThreads, 0, s>>>(S, G, E, lam, loff, boff, bdim, 1, flag_tol, flags);
-        V2B_CK(cudaGetLastError());
-        launches++;
-        gemm<false, false, kEpiStore>(V1, E, W, nullptr, 0.0, nullptr, nullptr, s, launches);
-        gemm<false, true, kEpiProject>(W, V1, nullptr, nullptr, 1.0 / mu, x, z, s, launches);
-        std::swap(V, V1);
-        V2B_CK(cudaMemcpyAsync(h_flags, flags, nblk * sizeof(int), cudaMemcpyDeviceToHost, s));
-        V2B_CK(cudaMemsetAsync(flags, 0, nblk * sizeof(int), s));
-        warm_solves++;
-    }
-
-    // enqueue a projection; call flagged() after the stream has synchronised
-    void project(const double *U, double mu, double *x, double *z, int *status, cudaStream_t s,
-                 long &launches) {
-        if (nblk == 0) return;
-        if (!have_vectors) {
-            cold(U, mu, x, z, status, s, launches);
-            for (int i = 0; i < nblk; i++) h_flags[i] = 0;
-        } else {
-            warm(U, mu, x, z, s, launches);
-        }
-    }
-    bool flagged() const {
-        for (int i = 0; i < nblk; i++)
-            if (h_flags[i]) return true;
-        return false;
-    }
-    void clear_flags() {
-        for (int i = 0; i < nblk; i++) h_flags[i] = 0;
+        gemm<true, false, kEpiStore>(Vt, P, W, nullptr, 0.0, nullptr, nullptr, s, launches);
+        gemm<false, false, kEpiProject>(W, Vt, nullptr, nullptr, 1.0 / mu, x, z, s, launches);
     }
 };
 
@@ -419,7 +377,7 @@ struct v2b_problem {
         mark(1, 1);
         mark(2, 0);
         ensure_plan();
-        plan.project(U, mu, x, z, status + 1, stream, launches);
+        plan.project(U, mu, x, z, stream, launches);
         mark(2, 1);
         mark(3, 0);
         v2b::spmv_A2_kernel<<<grid_for(nd, v2b::kSpmvThreads), v2b::kSpmvThreads, 0, stream>>>(
@@ -439,30 +397,6 @@ struct v2b_problem {
         V2B_CK(cudaMemcpyAsync(h_readback + 6, status, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
         V2B_CK(cudaStreamSynchronize(stream));
         collect();
-        for (int attempt = 0; attempt < 2 && plan.flagged(); attempt++) {
-            // the warm refinement left too large an error for some block: redo
-            // this iteration's projection (first one more Newton round from the
-            // refined basis, then from scratch) and the quantities after it
-            plan.clear_flags();
-            if (attempt == 0) {
-                plan.warm(U, mu, x, z, stream, launches);
-                plan.redo_warm++;
-            } else {
-                plan.cold(U, mu, x, z, status + 1, stream, launches);
-            }
-            v2b::spmv_A2_kernel<<<grid_for(nd, v2b::kSpmvThreads), v2b::kSpmvThreads, 0, stream>>>(
-                A.rp, A.ent, nd, x, c, z, Ax, Acz, A.pal);
-            V2B_CK(cudaGetLastError());
-            launches++;
-            v2b::stats_kernel<<<v2b::kStatsBlocks, 256, 0, stream>>>(Ax, b, ATy, z, c, x, y, np, nd,
-                                                                     stats_partials, stats_counter,
-                                                                     stats, status);
-            V2B_CK(cudaGetLastError());
-            launches++;
-            V2B_CK(cudaMemcpyAsync(h_readback, stats, 4 * sizeof(double), cudaMemcpyDeviceToHost, stream));
-            V2B_CK(cudaMemcpyAsync(h_readback + 6, status, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
-            V2B_CK(cudaStreamSynchronize(stream));
-        }
         const int *st = (const int *)(h_readback + 6);
         if (st[0] == V2B_DEVICE_TIMEOUT)
             throw Failure(V2B_DEVICE_TIMEOUT, "grid barrier wait gave up in cg_kernel");
@@ -480,7 +414,7 @@ struct v2b_problem {
         const int64_t np = prob.n_primal, nd = prob.n_dual;
         mu = 0.1;
         ensure_plan();
-        plan.have_vectors = false;
+        plan.reset();
         V2B_CK(cudaMemsetAsync(y, 0, nd * 8, stream));
         V2B_CK(cudaMemsetAsync(z, 0, np * 8, stream));
         V2B_CK(cudaMemsetAsync(status, 0, 8, stream));
@@ -592,14 +526,7 @@ struct v2b_bpsdp {
             ATu(ATy.data(), y.data(), data);
             for (long i = 0; i < np; i++) U[i] = mu * x[i] + ATy[i] - c[i];
             V2B_CK(cudaMemcpyAsync(dU, U.data(), np * 8, cudaMemcpyHostToDevice, stream));
-            plan.project(dU, mu, dx, dz, status + 1, stream, launches);
-            V2B_CK(cudaStreamSynchronize(stream));
-            for (int attempt = 0; attempt < 2 && plan.flagged(); attempt++) {
-                plan.clear_flags();
-                if (attempt == 0) plan.warm(dU, mu, dx, dz, stream, launches);
-                else plan.cold(dU, mu, dx, dz, status + 1, stream, launches);
-                V2B_CK(cudaStreamSynchronize(stream));
-            }
+            plan.project(dU, mu, dx, dz, stream, launches);
             V2B_CK(cudaMemcpyAsync(x, dx, np * 8, cudaMemcpyDeviceToHost, stream));
             V2B_CK(cudaMemcpyAsync(z.data(), dz, np * 8, cudaMemcpyDeviceToHost, stream));
             V2B_CK(cudaStreamSynchronize(stream));
@@ -771,7 +698,9 @@ int v2b_problem_project(v2b_problem *p, const double *d_U, double mu, double *d_
         p->setup();
         p->ensure_plan();
         // a stand-alone projection has no previous basis: solve each block from scratch
-        p->plan.cold(d_U, mu, d_x, d_z, p->status + 1, (cudaStream_t)stream, p->launches);
+        p->plan.reset();
+        p->plan.project(d_U, mu, d_x, d_z, (cudaStream_t)stream, p->launches);
+        p->plan.reset();
         return V2B_OK;
     });
 }
@@ -864,12 +793,18 @@ int v2b_problem_profile(const v2b_problem *p, double *ms, long *launches) {
     return V2B_OK;
 }
 void *v2b_problem_stream(const v2b_problem *p) { return p ? (void *)p->stream : nullptr; }
-int v2b_problem_projection_counts(const v2b_problem *p, long *warm, long *redo_warm, long *cold) {
-    if (!p || !warm || !redo_warm || !cold) return V2B_BAD_ARG;
-    *warm = p->plan.warm_solves;
-    *redo_warm = p->plan.redo_warm;
-    *cold = p->plan.cold_solves;
-    return V2B_OK;
+int v2b_problem_projection_counts(const v2b_problem *p, long *calls, long *rotations,
+                                  long *sweep_overruns) {
+    return guarded([&] {
+        if (!p || !calls || !rotations || !sweep_overruns)
+            throw std::invalid_argument("projection_counts: NULL argument");
+        *calls = p->plan.calls;
+        int h[2] = {0, 0};
+        if (p->plan.built) V2B_CK(cudaMemcpy(h, p->plan.counters, 8, cudaMemcpyDeviceToHost));
+        *rotations = h[1];
+        *sweep_overruns = h[0];
+        return V2B_OK;
+    });
 }
 
 }  // extern "C"

@@ -223,7 +223,7 @@ class V2RDMProblem:
     def kernel_launches(self):
         return self._lib.v2b_problem_kernel_launches(self._h)
 
-    KERNEL_CLASSES = ("cg_kernel", "spmv_AT_U_kernel", "jacobi_project_kernel", "spmv_A2_kernel",
+    KERNEL_CLASSES = ("cg_kernel", "spmv_AT_U_kernel", "projection", "spmv_A2_kernel",
                       "stats_kernel")
 
     def set_profiling(self, on=True):
@@ -237,11 +237,11 @@ class V2RDMProblem:
         return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNEL_CLASSES)}
 
     def projection_counts(self):
-        """{"warm": n, "redo_warm": n, "cold": n} projections since creation"""
+        """{"calls", "rotations", "sweep_overruns"} of the warm-started projection"""
         w, r, c = ctypes.c_long(), ctypes.c_long(), ctypes.c_long()
         check(self._lib.v2b_problem_projection_counts(self._h, ctypes.byref(w), ctypes.byref(r),
                                                       ctypes.byref(c)))
-        return {"warm": w.value, "redo_warm": r.value, "cold": c.value}
+        return {"calls": w.value, "rotations": r.value, "sweep_overruns": c.value}
 
     def stream_handle(self):
         return self._lib.v2b_problem_stream(self._h)

@@ -163,10 +163,10 @@ int v2b_problem_set_profiling(v2b_problem *p, int on);
 int v2b_problem_profile(const v2b_problem *p, double *ms /* [5] */, long *launches /* [5] */);
 /* the cudaStream_t the device solve runs on (after the first device call) */
 void *v2b_problem_stream(const v2b_problem *p);
-/* how the per-block projections were computed: warm (refinement of the
- * previous eigenvectors), warm repeats after a flagged error estimate, and
- * cold Jacobi solves */
-int v2b_problem_projection_counts(const v2b_problem *p, long *warm, long *redo_warm, long *cold);
+/* projection work since the last reset: warm-started calls, Jacobi rotations
+ * applied, and blocks whose Jacobi sweeps hit the sweep cap */
+int v2b_problem_projection_counts(const v2b_problem *p, long *calls, long *rotations,
+                                  long *sweep_overruns);
 
 #ifdef __cplusplus
 }
