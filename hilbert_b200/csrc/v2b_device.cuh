@@ -119,6 +119,16 @@ __device__ __forceinline__ unsigned int ld_volatile_u32(const unsigned int *p) {
     return *((volatile const unsigned int *)p);
 }
 __device__ __forceinline__ int ld_volatile_i32(const int *p) { return *((volatile const int *)p); }
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned int atom_add_acq_rel_u32(unsigned int *p, unsigned int v) {
+    unsigned int old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
 
 // Grid-wide barrier for a cooperatively launched kernel.  Every wait is
 // bounded: after spin_limit polls the waiting block records
@@ -129,26 +139,23 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *bar, int *status, long lo
     __syncthreads();
     if (threadIdx.x == 0) {
         int fail = 0;
-        const unsigned int g = ld_volatile_u32(&bar->gen);
-        __threadfence();
-        const unsigned int arrived = atomicAdd(&bar->count, 1u);
+        const unsigned int g = ld_acquire_u32(&bar->gen);
+        const unsigned int arrived = atom_add_acq_rel_u32(&bar->count, 1u);
         if (arrived == gridDim.x - 1) {
             atomicExch(&bar->count, 0u);
-            __threadfence();
-            atomicAdd(&bar->gen, 1u);
+            atom_add_acq_rel_u32(&bar->gen, 1u);
         } else {
             long long spins = 0;
-            while (ld_volatile_u32(&bar->gen) == g) {
-                if (ld_volatile_i32(status) != 0) { fail = 1; break; }
+            while (ld_acquire_u32(&bar->gen) == g) {
+                if ((spins & 63) == 0 && ld_volatile_i32(status) != 0) { fail = 1; break; }
                 if (++spins > spin_limit) {
                     atomicExch(status, kStatusTimeout);
                     fail = 1;
                     break;
                 }
-                __nanosleep(32);
+                if (spins > 256) __nanosleep(32);
             }
         }
-        __threadfence();
         *s_flag = fail || (ld_volatile_i32(status) != 0);
     }
     __syncthreads();

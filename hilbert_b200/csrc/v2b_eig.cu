@@ -98,11 +98,26 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-template __global__ void gemm_tiles_kernel<false, true, kEpiStore>(GEMM_ARGS);
-template __global__ void gemm_tiles_kernel<false, false, kEpiStore>(GEMM_ARGS);
-template __global__ void gemm_tiles_kernel<true, false, kEpiStore>(GEMM_ARGS);
-template __global__ void gemm_tiles_kernel<false, false, kEpiProject>(GEMM_ARGS);
-template __global__ void gemm_tiles_kernel<false, false, kEpiAdd>(GEMM_ARGS);
+cudaError_t launch_gemm_tiles(GemmVariant v, int ntiles, cudaStream_t s, GEMM_ARGS) {
+    switch (v) {
+        case kGemmNTStore:
+            gemm_tiles_kernel<false, true, kEpiStore><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo);
+            break;
+        case kGemmNNStore:
+            gemm_tiles_kernel<false, false, kEpiStore><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo);
+            break;
+        case kGemmTNStore:
+            gemm_tiles_kernel<true, false, kEpiStore><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo);
+            break;
+        case kGemmNNProject:
+            gemm_tiles_kernel<false, false, kEpiProject><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo);
+            break;
+        case kGemmNNAdd:
+            gemm_tiles_kernel<false, false, kEpiAdd><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo);
+            break;
+    }
+    return cudaGetLastError();
+}
 
 // Us = (U + U^T) / 2 per block, tile by tile
 __global__ void symmetrize_kernel(const double *__restrict__ U, double *__restrict__ Us,

@@ -20,8 +20,12 @@ constexpr int kGemmTile = 64;
         const double *__restrict__ Us, double inv_mu, double *__restrict__ xo,               \
         double *__restrict__ zo
 
-template <bool TA, bool TB, int EPI>
-__global__ void gemm_tiles_kernel(GEMM_ARGS);
+// Host launcher of gemm_tiles_kernel<TA, TB, EPI> (defined, with the kernel
+// instantiations, in v2b_eig.cu).  variant: 0 <N,T,store>, 1 <N,N,store>,
+// 2 <T,N,store>, 3 <N,N,project>, 4 <N,N,add>.
+enum GemmVariant { kGemmNTStore = 0, kGemmNNStore = 1, kGemmTNStore = 2, kGemmNNProject = 3,
+                   kGemmNNAdd = 4 };
+cudaError_t launch_gemm_tiles(GemmVariant v, int ntiles, cudaStream_t s, GEMM_ARGS);
 
 __global__ void symmetrize_kernel(const double *__restrict__ U, double *__restrict__ Us,
                                   const int4 *__restrict__ tiles, const int64_t *__restrict__ boff,

@@ -249,6 +249,7 @@ __global__ void __launch_bounds__(kJacobiThreads)
     double *T = sm;                                   // np*np (later: Vt)
     double2 *cs = (double2 *)(T + (size_t)np * np);   // m
     int *act = (int *)(cs + m);                       // m
+    int *alist = act + m;                             // m
     __shared__ double red[32];
     __shared__ int nrot, nstep;
     __shared__ double s_nrm;
@@ -269,6 +270,8 @@ __global__ void __launch_bounds__(kJacobiThreads)
     const double atol = abs_tol * nrm + 1e-300, gtol = gap_tol * nrm;
 
     double2 *rb = rot + rot_off[blk];
+    // per-step rotation counts live after the block's rotation record
+    int *scount = (int *)(rb + (int64_t)max_sweeps * (np - 1) * m);
     int sweep = 0, total = 0;
     for (; sweep < max_sweeps; sweep++) {
         if (threadIdx.x == 0) nrot = 0;
@@ -301,10 +304,18 @@ __global__ void __launch_bounds__(kJacobiThreads)
             const int active = nstep;
             if (threadIdx.x == 0) nrot += active;
             if (active) {
-                // 2x2 blocks (P, Q), P <= Q, touched by at least one rotation
-                for (int it = threadIdx.x; it < m * m; it += blockDim.x) {
-                    const int P = it / m, Q = it % m;
-                    if (P > Q || !(act[P] | act[Q])) continue;
+                // compact list of the rotated pairs of this step
+                if (threadIdx.x == 0) {
+                    int c = 0;
+                    for (int k = 0; k < m; k++)
+                        if (act[k]) alist[c++] = k;
+                }
+                __syncthreads();
+                // 2x2 blocks (P, Q) with P rotated; a block with both P and Q
+                // rotated is handled once, by the smaller of the two
+                for (int it = threadIdx.x; it < active * m; it += blockDim.x) {
+                    const int P = alist[it / m], Q = it % m;
+                    if (act[Q] && Q < P) continue;
                     const double2 cp = cs[P], cq = cs[Q];
                     int pP, qP, pQ, qQ;
                     rr_pair(st, P, np, pP, qP);
@@ -330,6 +341,7 @@ __global__ void __launch_bounds__(kJacobiThreads)
                     }
                 }
             }
+            if (threadIdx.x == 0) scount[(int64_t)sweep * (np - 1) + st] = active;
             __syncthreads();
         }
         total += nrot;
@@ -373,11 +385,18 @@ __global__ void __launch_bounds__(kJacobiThreads)
     __syncthreads();
     for (int sw = 0; sw < sweep; sw++) {
         for (int st = 0; st < np - 1; st++) {
+            const int active = scount[(int64_t)sw * (np - 1) + st];   // uniform across the CTA
+            if (!active) continue;
             const double2 *rs = rb + ((int64_t)sw * (np - 1) + st) * m;
-            for (int it = threadIdx.x; it < m * np; it += blockDim.x) {
-                const int k = it / np, j = it % np;
+            if (threadIdx.x == 0) {
+                int c = 0;
+                for (int k = 0; k < m; k++)
+                    if (rs[k].y != 0.0) alist[c++] = k;
+            }
+            __syncthreads();
+            for (int it = threadIdx.x; it < active * np; it += blockDim.x) {
+                const int k = alist[it / np], j = it % np;
                 const double2 r = rs[k];
-                if (r.y == 0.0) continue;
                 int p, q;
                 rr_pair(st, k, np, p, q);
                 const double vp = V[p * np + j], vq = V[q * np + j];

@@ -66,7 +66,7 @@ __global__ void half_residual_kernel(const double *__restrict__ G, double *__res
 
 inline size_t jacobi_smem_bytes(int n) {
     const int np = n + (n & 1);
-    return (size_t)np * np * sizeof(double) + (size_t)(np / 2) * (sizeof(double2) + sizeof(int));
+    return (size_t)np * np * sizeof(double) + (size_t)(np / 2) * (sizeof(double2) + 2 * sizeof(int));
 }
 
 }  // namespace v2b

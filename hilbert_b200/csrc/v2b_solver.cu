@@ -138,7 +138,9 @@ struct ProjectPlan {
                 for (int b = 0; b < nt; b++) tl.push_back(make_int4(i, a, b, 0));
             const int np = d[i] + (d[i] & 1);
             roff[i] = ro;
-            ro += (int64_t)max_sweeps * std::max(np - 1, 0) * (np / 2);
+            // rotation record (max_sweeps x steps x pairs) + per-step counts
+            ro += (int64_t)max_sweeps * std::max(np - 1, 0) * (np / 2) +
+                  ((int64_t)max_sweeps * std::max(np - 1, 0) + 3) / 4 + 1;
             smem = std::max(smem, v2b::jacobi_smem_bytes(d[i]));
         }
         total = o;
@@ -170,12 +172,9 @@ struct ProjectPlan {
         built = false;
     }
 
-    template <bool TA, bool TB, int EPI>
-    void gemm(const double *A, const double *B, double *C, const double *Cin, double inv_mu,
-              double *x, double *z, cudaStream_t s, long &launches) {
-        v2b::gemm_tiles_kernel<TA, TB, EPI><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin,
-                                                                  Us, inv_mu, x, z);
-        V2B_CK(cudaGetLastError());
+    void gemm(v2b::GemmVariant v, const double *A, const double *B, double *C, const double *Cin,
+              double inv_mu, double *x, double *z, cudaStream_t s, long &launches) {
+        V2B_CK(v2b::launch_gemm_tiles(v, ntiles, s, A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, x, z));
         launches++;
     }
 
@@ -191,25 +190,25 @@ struct ProjectPlan {
             launches++;
             fresh = false;
         } else if (++calls % kReorthEvery == 0) {
-            gemm<false, true, kEpiStore>(Vt, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches);
+            gemm(kGemmNTStore, Vt, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches);
             half_residual_kernel<<<nblk, 256, 0, s>>>(W, T, boff, bdim);
             V2B_CK(cudaGetLastError());
             launches++;
-            gemm<false, false, kEpiAdd>(T, Vt, Vt2, Vt, 0.0, nullptr, nullptr, s, launches);
+            gemm(kGemmNNAdd, T, Vt, Vt2, Vt, 0.0, nullptr, nullptr, s, launches);
             std::swap(Vt, Vt2);
         }
         symmetrize_kernel<<<ntiles, 256, 0, s>>>(U, Us, tiles, boff, bdim);
         V2B_CK(cudaGetLastError());
         launches++;
-        gemm<false, true, kEpiStore>(Us, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches);
-        gemm<false, false, kEpiStore>(Vt, W, T, nullptr, 0.0, nullptr, nullptr, s, launches);
+        gemm(kGemmNTStore, Us, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches);
+        gemm(kGemmNNStore, Vt, W, T, nullptr, 0.0, nullptr, nullptr, s, launches);
         jacobi_warm_kernel<<<nblk, kJacobiThreads, smem, s>>>(T, P, Vt, boff, bdim, rot, rot_off,
                                                               max_sweeps, abs_tol, gap_tol,
                                                               counters, counters + 1);
         V2B_CK(cudaGetLastError());
         launches++;
-        gemm<true, false, kEpiStore>(Vt, P, W, nullptr, 0.0, nullptr, nullptr, s, launches);
-        gemm<false, false, kEpiProject>(W, Vt, nullptr, nullptr, 1.0 / mu, x, z, s, launches);
+        gemm(kGemmTNStore, Vt, P, W, nullptr, 0.0, nullptr, nullptr, s, launches);
+        gemm(kGemmNNProject, W, Vt, nullptr, nullptr, 1.0 / mu, x, z, s, launches);
     }
 };
 
@@ -309,8 +308,8 @@ struct v2b_problem {
         if (per_sm < 1) throw Failure(V2B_INTERNAL, "cg_kernel cannot be resident");
         // small problems: fewer CTAs make the grid barrier cheaper
         const int64_t rows = std::max(prob.n_primal, prob.n_dual);
-        const int64_t want = (rows + (int64_t)v2b::kCgThreads * 8 - 1) / ((int64_t)v2b::kCgThreads * 8);
-        cg_grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sm_count() * std::min(per_sm, 2)));
+        const int64_t want = (rows + (int64_t)v2b::kCgThreads - 1) / (int64_t)v2b::kCgThreads;
+        cg_grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sm_count() * std::min(per_sm, 1)));
         partials = dalloc<double>(std::max(cg_grid, 4 * v2b::kStatsBlocks));
         stats_partials = dalloc<double>(4 * v2b::kStatsBlocks);
         cg_out = dalloc<double>(2);
