@@ -40,7 +40,10 @@ WORKLOADS = {
 }
 # (outer, CG) iterations the FP64 oracle needed to converge this workload,
 # recorded from a full oracle run; the reference arm scales its sample by them
-ORACLE_ITERS = {"hubbard8": (None, None)}
+# (oracle: C restatement maps + numpy boundary-point loop, 8 host threads; energy
+#  -4.9364448537582035 at eps_p 9.83e-7, eps_d 1.00e-6; 497 s on the build host)
+ORACLE_ITERS = {"hubbard8": (13801, 503997)}
+ORACLE_ENERGY = {"hubbard8": -4.9364448537582035}
 
 METRIC = "time to 1e-6 SDP convergence, mixed/batched vs plain FP64 on B200; |dE| vs FP64"
 
@@ -53,6 +56,9 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="hubbard8", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    ap.add_argument("--max-outer", type=int, default=0,
+                    help="cap the outer iterations of each solve (profiling runs; the line then "
+                         "reports a capped, not a converged, solve)")
     return ap.parse_args()
 
 
@@ -227,7 +233,8 @@ def run_b200(args, w):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     opts = hb.Options({"R_CONVERGENCE": w["r_conv"], "E_CONVERGENCE": w["e_conv"],
-                       "CG_CONVERGENCE": w["cg_conv"], "MAXITER": w["maxiter"],
+                       "CG_CONVERGENCE": w["cg_conv"],
+                       "MAXITER": args.max_outer if args.max_outer else w["maxiter"],
                        "MU_UPDATE_FREQUENCY": w["muf"]})
     p = hb.V2RDMProblem(w["nmo"], w["nalpha"], w["nbeta"], w["positivity"], True, True,
                         hubbard_multiplicity=True)
@@ -321,7 +328,7 @@ def run_b200(args, w):
                                for k, v in prof.items()}
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and args.cpu_sample_seconds > 0:
         t_cg, t_out, kind, reps = cpu_sample(w, args.cpu_sample_seconds)
         cpu = {"value": t_cg * iiter + t_out * oiter, "unit": "s", "cores": cpu_threads(),
                "kind": kind,
@@ -341,7 +348,11 @@ def run_b200(args, w):
                            "parallelism": "replicas" if world > 1 else "single",
                            "l2": "flushed between steps (256 MiB write)",
                            "outer_iterations": oiter, "cg_iterations": iiter,
-                           "energy": energy, "converged": stats["converged"]},
+                           "energy": energy, "converged": stats["converged"],
+                           "oracle_energy": ORACLE_ENERGY.get(args.workload),
+                           "abs_dE_vs_fp64_oracle": (abs(energy - ORACLE_ENERGY[args.workload])
+                                                     if args.workload in ORACLE_ENERGY else None),
+                           "max_outer_cap": args.max_outer or None},
                 "e2e": {"value": te2e, "unit": "s", "h2d_bytes_per_step": 8 * (2 * npr + ndu),
                         "d2h_bytes_per_step": 8 * npr},
                 "gpu_launches": int(launches),
