@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -240,6 +241,7 @@ struct v2b_problem {
     int cg_grid = 0;
     double mu = 0.1;
     long launches = 0;
+    long cur_oiter = 0;
 
     // optional per-kernel-class CUDA-event timing on the launching stream
     // classes: 0 cg_kernel, 1 spmv_AT_U, 2 jacobi_project, 3 spmv_A2, 4 stats
@@ -399,7 +401,15 @@ struct v2b_problem {
         const int *st = (const int *)(h_readback + 6);
         if (st[0] == V2B_DEVICE_TIMEOUT)
             throw Failure(V2B_DEVICE_TIMEOUT, "grid barrier wait gave up in cg_kernel");
-        if (st[0] == V2B_NAN) throw Failure(V2B_NAN, "non-finite value in the iteration");
+        if (st[0] == V2B_NAN) {
+            char msg[256];
+            snprintf(msg, sizeof msg,
+                     "non-finite value at outer iteration %ld: cg iterations %g |r| %g, "
+                     "|Ax-b|^2 %g |ATy+z-c|^2 %g cx %g by %g, mu %g",
+                     cur_oiter, h_readback[4], h_readback[5], h_readback[0], h_readback[1],
+                     h_readback[2], h_readback[3], mu);
+            throw Failure(V2B_NAN, msg);
+        }
         out[0] = h_readback[4];
         out[1] = std::sqrt(h_readback[0]);
         out[2] = std::sqrt(h_readback[1]);
@@ -427,6 +437,7 @@ struct v2b_problem {
         while (!converged && oiter < o.maxiter) {
             const long budget = std::min<long>(muf, o.maxiter - oiter);
             for (long k = 0; k < budget; k++) {
+                cur_oiter = oiter;
                 iterate(o, res);
                 const int it = (int)res[0];
                 if (monitor) monitor(print_level, (int)oiter, it, res[3], res[4], mu, res[1], res[2], data);
