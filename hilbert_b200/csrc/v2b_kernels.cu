@@ -385,15 +385,16 @@ __global__ void __launch_bounds__(kJacobiThreads)
     __syncthreads();
     for (int sw = 0; sw < sweep; sw++) {
         for (int st = 0; st < np - 1; st++) {
-            const int active = scount[(int64_t)sw * (np - 1) + st];   // uniform across the CTA
-            if (!active) continue;
+            if (scount[(int64_t)sw * (np - 1) + st] == 0) continue;   // uniform across the CTA
             const double2 *rs = rb + ((int64_t)sw * (np - 1) + st) * m;
             if (threadIdx.x == 0) {
                 int c = 0;
                 for (int k = 0; k < m; k++)
                     if (rs[k].y != 0.0) alist[c++] = k;
+                nstep = c;
             }
             __syncthreads();
+            const int active = nstep;
             for (int it = threadIdx.x; it < active * np; it += blockDim.x) {
                 const int k = alist[it / np], j = it % np;
                 const double2 r = rs[k];
