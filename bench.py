@@ -303,13 +303,14 @@ def run_b200(args, w):
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
     bf16 = peaks.get("bf16_tflops", 1590.0)
-    if dom == "jacobi_project_kernel":
+    if dom == "projection":
         flops = sum((16.0 / 3.0) * float(d) ** 3 for d in p.dims)
         ach = flops / (ms / n / 1e3) / 1e12
         roof = {"kernel": dom, "bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s",
                 "frac": ach / bf16, "traffic": None,
-                "note": "FP64 SIMT Jacobi; algorithmic flops sum (16/3) n_b^3 per launch; peak is "
-                        "the measured dense bf16 figure (no FP64 peak is measured)"}
+                "note": "FP64 projection (GEMM transforms + selective Jacobi); algorithmic flops "
+                        "sum (16/3) n_b^3 per launch; peak is the measured dense bf16 figure (no "
+                        "FP64 peak is measured)"}
     else:
         cg_iters_per_launch = iiter / max(oiter, 1)
         if dom == "cg_kernel":

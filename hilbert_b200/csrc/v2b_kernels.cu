@@ -71,6 +71,9 @@ __global__ void spmv_AT_U_kernel(const uint32_t *__restrict__ rp,
 //   1. t = A^T (r + beta p_old), p_new = r + beta p_old
 //   2. q = A t,  partial p_new.q
 //   3. y += alpha p_new, r -= alpha q, partial r.r
+// The p.q and r.r partials live in separate arrays: a block that has passed
+// barrier 2 writes its r.r partial while slower blocks may still be summing
+// the p.q partials.
 __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgParams P) {
     __shared__ double palA[16], palT[16];
     __shared__ double red[32];
@@ -121,9 +124,9 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgParams P) {
             loc += pnew[j] * q;
         }
         s = block_sum(loc, red);
-        if (threadIdx.x == 0) P.partials[blockIdx.x] = s;
+        if (threadIdx.x == 0) P.partials[nb + blockIdx.x] = s;
         if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
-        const double pq = sum_partials(P.partials, nb, &bcast);
+        const double pq = sum_partials(P.partials + nb, nb, &bcast);
         if (!(pq > 0.0)) break;   // range of A A^T exhausted (or non-finite)
         const double alpha = rs / pq;
 

@@ -26,7 +26,7 @@ struct CgParams {
     const double *Ax, *Acz, *b;     // rhs = Acz + mu (b - Ax)
     double mu;
     double *y, *r, *p0, *p1, *t, *q;
-    double *partials;               // >= gridDim.x
+    double *partials;               // >= 2 * gridDim.x (r.r partials, then p.q partials)
     GridBarrier *bar;
     int *status;
     long long spin_limit;

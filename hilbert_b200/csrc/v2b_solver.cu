@@ -114,7 +114,7 @@ struct ProjectPlan {
     int max_dim = 0;
     bool fresh = true;
     bool built = false;
-    long calls = 0;
+    long calls = 0, since_reset = 0;
     double abs_tol = 1e-14, gap_tol = 1e-13;
 
     void build(const std::vector<int> &d) {
@@ -180,7 +180,11 @@ struct ProjectPlan {
     }
 
     // forget the eigenvector basis: the next projection starts from V = I
-    void reset() { fresh = true; }
+    // (and the re-orthonormalisation schedule restarts, so solves repeat exactly)
+    void reset() {
+        fresh = true;
+        since_reset = 0;
+    }
 
     void project(const double *U, double mu, double *x, double *z, cudaStream_t s, long &launches) {
         using namespace v2b;
@@ -190,7 +194,7 @@ struct ProjectPlan {
             V2B_CK(cudaGetLastError());
             launches++;
             fresh = false;
-        } else if (++calls % kReorthEvery == 0) {
+        } else if (++calls, ++since_reset % kReorthEvery == 0) {
             gemm(kGemmNTStore, Vt, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches);
             half_residual_kernel<<<nblk, 256, 0, s>>>(W, T, boff, bdim);
             V2B_CK(cudaGetLastError());
@@ -312,7 +316,7 @@ struct v2b_problem {
         const int64_t rows = std::max(prob.n_primal, prob.n_dual);
         const int64_t want = (rows + (int64_t)v2b::kCgThreads - 1) / (int64_t)v2b::kCgThreads;
         cg_grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sm_count() * std::min(per_sm, 1)));
-        partials = dalloc<double>(std::max(cg_grid, 4 * v2b::kStatsBlocks));
+        partials = dalloc<double>(2 * (size_t)cg_grid);
         stats_partials = dalloc<double>(4 * v2b::kStatsBlocks);
         cg_out = dalloc<double>(2);
         stats = dalloc<double>(4);
