@@ -27,6 +27,13 @@ enum GemmVariant { kGemmNTStore = 0, kGemmNNStore = 1, kGemmTNStore = 2, kGemmNN
                    kGemmNNAdd = 4 };
 cudaError_t launch_gemm_tiles(GemmVariant v, int ntiles, cudaStream_t s, GEMM_ARGS);
 
+}  // namespace v2b
+
+#include <string>
+namespace v2b {
+// message returned by v2b_last_error() on the calling thread
+void set_last_error(const std::string &msg);
+
 __global__ void symmetrize_kernel(const double *__restrict__ U, double *__restrict__ Us,
                                   const int4 *__restrict__ tiles, const int64_t *__restrict__ boff,
                                   const int *__restrict__ bdim);

@@ -226,6 +226,8 @@ int sm_count() {
 
 }  // namespace
 
+void v2b::set_last_error(const std::string &msg) { g_last_error = msg; }
+
 // ====================================================================
 // device-map problem
 // ====================================================================

@@ -168,6 +168,22 @@ void *v2b_problem_stream(const v2b_problem *p);
 int v2b_problem_projection_counts(const v2b_problem *p, long *calls, long *rotations,
                                   long *sweep_overruns);
 
+/* ---- 3. allocation-free projection ------------------------------------------ */
+
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * when they need a projection (their host owns all device memory, or the
+ * device synchronisation of an allocation is not acceptable there): projects
+ * ONE n x n block d_U (row-major, device memory) like v2b_problem_project,
+ * writing d_x = U+ / mu and d_z = U+ - sym(U), on the given cudaStream_t.
+ * n <= 128: all scratch is a fixed file-scope device array (about 3.7 MB,
+ * held by every GPU that loads the library until exit); larger n returns
+ * V2B_BAD_ARG.  Allocates nothing.  Every call reuses the same array, so calls
+ * that overlap on the GPU race and must be serialised by the caller.  The
+ * first call on a device looks the array up with cudaGetSymbolAddress; make
+ * it before any stream capture. */
+int v2b_project_block_noalloc(const double *d_U, int n, double mu, double *d_x, double *d_z,
+                              void *stream);
+
 #ifdef __cplusplus
 }
 #endif
