@@ -65,6 +65,23 @@ __global__ void spmv_AT_U_kernel(const uint32_t *__restrict__ rp,
     }
 }
 
+// Long rows inside CG: one warp per row, lanes stride over the entries and the
+// partial sums meet in a shuffle tree (order differs from hilbert's left-to-
+// right sum; the bit-exact kernels above are the ones the map API uses).
+__device__ __forceinline__ double warp_row(const uint32_t *__restrict__ ent, uint32_t b, uint32_t e,
+                                           const double *__restrict__ x, const double *__restrict__ p,
+                                           double beta, const double *pal, int lane) {
+    double acc = 0.0;
+    for (uint32_t k = b + lane; k < e; k += 32) {
+        const uint32_t w = __ldg(ent + k);
+        const uint32_t c = w & kDevColMask;
+        double v = __ldg(x + c);
+        if (p) v = __dadd_rn(v, __dmul_rn(beta, __ldg(p + c)));
+        acc += pal[(w >> 27) & 15u] * v;
+    }
+    return warp_sum(acc);
+}
+
 // ------------------------------------------------------------------ CG
 // Solves (A A^T) y = rhs with rhs = A(c - z) + mu (b - A x), warm-started from
 // y.  Three grid barriers per iteration:
@@ -109,17 +126,37 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgParams P) {
     const double *pold = P.r;   // first direction p = r (beta = 0)
     double *pnew = P.p0;
     bool done = !(sqrt(rs) >= P.tol);
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = gtid >> 5, nwarps = stride >> 5;
     while (!done && it < P.maxit) {
-        for (int64_t i = gtid; i < P.np; i += stride)
-            P.t[i] = packed_row_rbp(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), P.r, pold,
-                                    beta, palT);
+        for (int64_t i = gtid; i < P.np; i += stride) {
+            const uint32_t b = __ldg(P.t_rp + i), e = __ldg(P.t_rp + i + 1);
+            if (e - b <= kCgLongRow) P.t[i] = packed_row_rbp(P.t_ent, b, e, P.r, pold, beta, palT);
+        }
+        for (int64_t w = gwarp; w < P.n_long_t; w += nwarps) {
+            const int64_t i = __ldg(P.long_t + w);
+            const double v = warp_row(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), P.r, pold,
+                                      beta, palT, lane);
+            if (lane == 0) P.t[i] = v;
+        }
         for (int64_t j = gtid; j < P.nd; j += stride)
             pnew[j] = __dadd_rn(P.r[j], __dmul_rn(beta, pold[j]));
         if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
 
         loc = 0.0;
+        for (int64_t w = gwarp; w < P.n_long_a; w += nwarps) {
+            const int64_t j = __ldg(P.long_a + w);
+            const double q = warp_row(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), P.t, nullptr,
+                                      0.0, palA, lane);
+            if (lane == 0) {
+                P.q[j] = q;
+                loc += pnew[j] * q;
+            }
+        }
         for (int64_t j = gtid; j < P.nd; j += stride) {
-            const double q = packed_row(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), P.t, palA);
+            const uint32_t b = __ldg(P.a_rp + j), e = __ldg(P.a_rp + j + 1);
+            if (e - b > kCgLongRow) continue;
+            const double q = packed_row(P.a_ent, b, e, P.t, palA);
             P.q[j] = q;
             loc += pnew[j] * q;
         }
@@ -307,11 +344,17 @@ __global__ void __launch_bounds__(kJacobiThreads)
             const int active = nstep;
             if (threadIdx.x == 0) nrot += active;
             if (active) {
-                // compact list of the rotated pairs of this step
-                if (threadIdx.x == 0) {
-                    int c = 0;
-                    for (int k = 0; k < m; k++)
-                        if (act[k]) alist[c++] = k;
+                // compact list of the rotated pairs of this step (warp 0, ballots)
+                if (threadIdx.x < 32) {
+                    const int lane = threadIdx.x;
+                    int base = 0;
+                    for (int k0 = 0; k0 < m; k0 += 32) {
+                        const int k = k0 + lane;
+                        const int a = (k < m) ? act[k] : 0;
+                        const unsigned bal = __ballot_sync(0xffffffffu, a);
+                        if (a) alist[base + __popc(bal & ((1u << lane) - 1u))] = k;
+                        base += __popc(bal);
+                    }
                 }
                 __syncthreads();
                 // 2x2 blocks (P, Q) with P rotated; a block with both P and Q
@@ -390,11 +433,17 @@ __global__ void __launch_bounds__(kJacobiThreads)
         for (int st = 0; st < np - 1; st++) {
             if (scount[(int64_t)sw * (np - 1) + st] == 0) continue;   // uniform across the CTA
             const double2 *rs = rb + ((int64_t)sw * (np - 1) + st) * m;
-            if (threadIdx.x == 0) {
-                int c = 0;
-                for (int k = 0; k < m; k++)
-                    if (rs[k].y != 0.0) alist[c++] = k;
-                nstep = c;
+            if (threadIdx.x < 32) {
+                const int lane = threadIdx.x;
+                int base = 0;
+                for (int k0 = 0; k0 < m; k0 += 32) {
+                    const int k = k0 + lane;
+                    const int a = (k < m) ? (rs[k].y != 0.0) : 0;
+                    const unsigned bal = __ballot_sync(0xffffffffu, a);
+                    if (a) alist[base + __popc(bal & ((1u << lane) - 1u))] = k;
+                    base += __popc(bal);
+                }
+                if (lane == 0) nstep = base;
             }
             __syncthreads();
             const int active = nstep;

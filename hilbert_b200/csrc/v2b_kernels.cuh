@@ -10,6 +10,7 @@ namespace v2b {
 
 constexpr int kSpmvThreads = 256;
 constexpr int kCgThreads = 512;
+constexpr uint32_t kCgLongRow = 12;   // rows with more entries get a whole warp inside CG
 constexpr int kJacobiThreads = 512;
 constexpr int kJacobiMaxDim = 160;     // np*np doubles + rotations must fit in 227 KB
 constexpr int kStatsBlocks = 256;
@@ -21,6 +22,8 @@ struct Palette {
 struct CgParams {
     const uint32_t *a_rp, *a_ent;   // A   (rows = dual constraints)
     const uint32_t *t_rp, *t_ent;   // A^T (rows = primal variables)
+    const int64_t *long_a, *long_t; // rows longer than kCgLongRow (warp per row)
+    int64_t n_long_a, n_long_t;
     Palette palA, palT;
     int64_t np, nd;
     const double *Ax, *Acz, *b;     // rhs = Acz + mu (b - Ax)

@@ -73,7 +73,8 @@ void ensure_device() {
 
 struct DeviceOp {
     uint32_t *rp = nullptr, *ent = nullptr;
-    int64_t nrows = 0;
+    int64_t *long_rows = nullptr;   // rows longer than kCgLongRow
+    int64_t nrows = 0, n_long = 0;
     size_t nnz = 0;
     v2b::Palette pal{};
     void upload(const v2b::PackedOperator &op) {
@@ -84,11 +85,19 @@ struct DeviceOp {
         V2B_CK(cudaMemcpy(rp, op.row_ptr.data(), op.row_ptr.size() * 4, cudaMemcpyHostToDevice));
         V2B_CK(cudaMemcpy(ent, op.entries.data(), nnz * 4, cudaMemcpyHostToDevice));
         for (int i = 0; i < 16; i++) pal.v[i] = i < (int)op.palette.size() ? op.palette[i] : 0.0;
+        std::vector<int64_t> lr;
+        for (int64_t r = 0; r < nrows; r++)
+            if (op.row_ptr[r + 1] - op.row_ptr[r] > v2b::kCgLongRow) lr.push_back(r);
+        n_long = (int64_t)lr.size();
+        long_rows = dalloc<int64_t>(lr.size());
+        if (n_long) V2B_CK(cudaMemcpy(long_rows, lr.data(), lr.size() * 8, cudaMemcpyHostToDevice));
     }
     void release() {
         cudaFree(rp);
         cudaFree(ent);
+        cudaFree(long_rows);
         rp = ent = nullptr;
+        long_rows = nullptr;
     }
 };
 
@@ -357,6 +366,8 @@ struct v2b_problem {
         V2B_CK(cudaMemsetAsync(bar, 0, sizeof(v2b::GridBarrier), stream));
         v2b::CgParams P;
         P.a_rp = A.rp; P.a_ent = A.ent; P.t_rp = AT.rp; P.t_ent = AT.ent;
+        P.long_a = A.long_rows; P.long_t = AT.long_rows;
+        P.n_long_a = A.n_long; P.n_long_t = AT.n_long;
         P.palA = A.pal; P.palT = AT.pal;
         P.np = prob.n_primal; P.nd = prob.n_dual;
         P.Ax = Ax; P.Acz = Acz; P.b = b; P.mu = mu;
