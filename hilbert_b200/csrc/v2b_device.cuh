@@ -97,10 +97,12 @@ __device__ __forceinline__ double block_max(double v, double *red /* >= 32 */) {
 }
 
 // Deterministic sum of n partials, every thread of the block gets the result.
+// Called right after a grid barrier (whose acquire orders these loads); the
+// loads bypass L1 (__ldcg) and are independent, so they pipeline.
 __device__ __forceinline__ double sum_partials(const double *part, int n, double *bcast) {
     if (threadIdx.x < 32) {
         double s = 0.0;
-        for (int i = threadIdx.x; i < n; i += 32) s += *((volatile const double *)(part + i));
+        for (int i = threadIdx.x; i < n; i += 32) s += __ldcg(part + i);
         s = warp_sum(s);
         if (threadIdx.x == 0) *bcast = s;
     }
