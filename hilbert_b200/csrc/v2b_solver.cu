@@ -21,6 +21,7 @@
 #include <string>
 #include <vector>
 
+#include "v2b_bigjacobi.cuh"
 #include "v2b_eig.cuh"
 #include "v2b_kernels.cuh"
 #include "v2rdm_b200.h"
@@ -101,26 +102,35 @@ struct DeviceOp {
     }
 };
 
-// Per-block PSD projection for a fixed list of block sizes (blocks up to
-// kJacobiMaxDim).  The rows of Vt hold each block's eigenvectors from the
-// previous call (the identity before the first), so every call is
-//   symmetrize; W = Us Vt^T; T0 = Vt W; selective Jacobi on T0 (rotations
-//   replayed onto Vt); Y = Vt^T P; U+ = Y Vt -> x, z.
+// Per-block PSD projection for a fixed list of block sizes.  The rows of Vt
+// hold each block's eigenvectors from the previous call (the identity before
+// the first), so every call is
+//   symmetrize; W = Us Vt^T; T = Vt W;                       (GEMM tiles, all blocks)
+//   selective Jacobi on T, rotations replayed onto Vt:
+//     blocks <= kJacobiMaxDim  jacobi_warm_kernel (one CTA, T in shared memory)
+//     larger blocks            jacobi_big_kernel  (one 8-CTA cluster, T in L2)
+//   Y = Vt^T P; U+ = Y Vt -> x = U+/mu, z = U+ - Us.        (GEMM tiles)
 // Every kReorthEvery calls Vt is re-orthonormalised, Vt <- Vt + (I - Vt Vt^T) Vt / 2.
 struct ProjectPlan {
     static constexpr int kReorthEvery = 64;
+    static constexpr int kBigMaxRounds = 100000;
     std::vector<int> dims;
-    int nblk = 0;
+    int nblk = 0, nsmall = 0, nbig = 0;
     int64_t total = 0;
-    int64_t *boff = nullptr, *rot_off = nullptr;
-    int *bdim = nullptr, *counters = nullptr;   // counters[0] sweep overruns, [1] rotations
+    int64_t *boff = nullptr, *rot_off = nullptr, *boff_s = nullptr, *boff_b = nullptr;
+    int *bdim = nullptr, *bdim_s = nullptr, *bdim_b = nullptr, *counters = nullptr;
     int4 *tiles = nullptr;
     int ntiles = 0;
     double2 *rot = nullptr;
     double *Vt = nullptr, *Vt2 = nullptr, *Us = nullptr, *W = nullptr, *T = nullptr, *P = nullptr;
+    // large-block work arrays
+    int64_t *ioff_b = nullptr, *loff_b = nullptr, *lcap_b = nullptr;
+    double *diag_b = nullptr, *norm_b = nullptr;
+    int *partner_b = nullptr, *act_b = nullptr, *rcnt_b = nullptr;
+    double2 *acs_b = nullptr, *logcs_b = nullptr;
+    int2 *logpq_b = nullptr;
     size_t smem = 0;
     int max_sweeps = 30;
-    int max_dim = 0;
     bool fresh = true;
     bool built = false;
     long calls = 0, since_reset = 0;
@@ -129,47 +139,84 @@ struct ProjectPlan {
     void build(const std::vector<int> &d) {
         dims = d;
         nblk = (int)d.size();
-        std::vector<int64_t> off(nblk), roff(nblk);
+        std::vector<int64_t> off(nblk), roff, off_s, off_b, ioff, loff, lcap;
+        std::vector<int> dim_s, dim_b;
         std::vector<int4> tl;
-        int64_t o = 0, ro = 0;
+        int64_t o = 0, ro = 0, io = 0, lo = 0;
         smem = 0;
-        max_dim = 0;
         for (int i = 0; i < nblk; i++) {
             if (d[i] < 0) throw std::invalid_argument("negative block dimension");
-            if (d[i] > v2b::kJacobiMaxDim)
-                throw std::invalid_argument("PSD block of dimension " + std::to_string(d[i]) +
-                                            " exceeds the shared-memory Jacobi limit " +
-                                            std::to_string(v2b::kJacobiMaxDim));
             off[i] = o;
-            o += (int64_t)d[i] * d[i];
-            max_dim = std::max(max_dim, d[i]);
             const int nt = (d[i] + v2b::kGemmTile - 1) / v2b::kGemmTile;
             for (int a = 0; a < nt; a++)
                 for (int b = 0; b < nt; b++) tl.push_back(make_int4(i, a, b, 0));
-            const int np = d[i] + (d[i] & 1);
-            roff[i] = ro;
-            // rotation record (max_sweeps x steps x pairs) + per-step counts
-            ro += (int64_t)max_sweeps * std::max(np - 1, 0) * (np / 2) +
-                  ((int64_t)max_sweeps * std::max(np - 1, 0) + 3) / 4 + 1;
-            smem = std::max(smem, v2b::jacobi_smem_bytes(d[i]));
+            if (d[i] <= v2b::kJacobiMaxDim) {
+                const int np = d[i] + (d[i] & 1);
+                off_s.push_back(o);
+                dim_s.push_back(d[i]);
+                roff.push_back(ro);
+                // rotation record (max_sweeps x steps x pairs) + per-step counts
+                ro += (int64_t)max_sweeps * std::max(np - 1, 0) * (np / 2) +
+                      ((int64_t)max_sweeps * std::max(np - 1, 0) + 3) / 4 + 1;
+                smem = std::max(smem, v2b::jacobi_smem_bytes(d[i]));
+            } else {
+                off_b.push_back(o);
+                dim_b.push_back(d[i]);
+                ioff.push_back(io);
+                io += d[i];
+                loff.push_back(lo);
+                // room for about six full sweeps of rotations
+                const int64_t c = 3 * (int64_t)d[i] * d[i];
+                lcap.push_back(c);
+                lo += c;
+            }
+            o += (int64_t)d[i] * d[i];
         }
         total = o;
+        nsmall = (int)dim_s.size();
+        nbig = (int)dim_b.size();
         ntiles = (int)tl.size();
         boff = dalloc<int64_t>(nblk);
-        rot_off = dalloc<int64_t>(nblk);
         bdim = dalloc<int>(nblk);
-        counters = dalloc<int>(2);
+        counters = dalloc<int>(4);
         tiles = dalloc<int4>(std::max(ntiles, 1));
-        rot = dalloc<double2>(ro);
         for (double **b : {&Vt, &Vt2, &Us, &W, &T, &P}) *b = dalloc<double>(total);
         V2B_CK(cudaMemcpy(boff, off.data(), nblk * 8, cudaMemcpyHostToDevice));
-        V2B_CK(cudaMemcpy(rot_off, roff.data(), nblk * 8, cudaMemcpyHostToDevice));
         V2B_CK(cudaMemcpy(bdim, d.data(), nblk * 4, cudaMemcpyHostToDevice));
-        V2B_CK(cudaMemset(counters, 0, 8));
+        V2B_CK(cudaMemset(counters, 0, 16));
         if (ntiles) V2B_CK(cudaMemcpy(tiles, tl.data(), ntiles * sizeof(int4), cudaMemcpyHostToDevice));
+        if (nsmall) {
+            boff_s = dalloc<int64_t>(nsmall);
+            bdim_s = dalloc<int>(nsmall);
+            rot_off = dalloc<int64_t>(nsmall);
+            rot = dalloc<double2>(ro);
+            V2B_CK(cudaMemcpy(boff_s, off_s.data(), nsmall * 8, cudaMemcpyHostToDevice));
+            V2B_CK(cudaMemcpy(bdim_s, dim_s.data(), nsmall * 4, cudaMemcpyHostToDevice));
+            V2B_CK(cudaMemcpy(rot_off, roff.data(), nsmall * 8, cudaMemcpyHostToDevice));
+        }
         if (smem)
             V2B_CK(cudaFuncSetAttribute(v2b::jacobi_warm_kernel,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (nbig) {
+            boff_b = dalloc<int64_t>(nbig);
+            bdim_b = dalloc<int>(nbig);
+            ioff_b = dalloc<int64_t>(nbig);
+            loff_b = dalloc<int64_t>(nbig);
+            lcap_b = dalloc<int64_t>(nbig);
+            diag_b = dalloc<double>(io);
+            partner_b = dalloc<int>(io);
+            act_b = dalloc<int>(io);
+            acs_b = dalloc<double2>(io);
+            logpq_b = dalloc<int2>(lo);
+            logcs_b = dalloc<double2>(lo);
+            rcnt_b = dalloc<int>((size_t)nbig * kBigMaxRounds);
+            norm_b = dalloc<double>((size_t)nbig * v2b::kBigCluster);
+            V2B_CK(cudaMemcpy(boff_b, off_b.data(), nbig * 8, cudaMemcpyHostToDevice));
+            V2B_CK(cudaMemcpy(bdim_b, dim_b.data(), nbig * 4, cudaMemcpyHostToDevice));
+            V2B_CK(cudaMemcpy(ioff_b, ioff.data(), nbig * 8, cudaMemcpyHostToDevice));
+            V2B_CK(cudaMemcpy(loff_b, loff.data(), nbig * 8, cudaMemcpyHostToDevice));
+            V2B_CK(cudaMemcpy(lcap_b, lcap.data(), nbig * 8, cudaMemcpyHostToDevice));
+        }
         fresh = true;
         built = true;
     }
@@ -177,7 +224,10 @@ struct ProjectPlan {
         if (!built) return;
         for (void *q : {(void *)boff, (void *)rot_off, (void *)bdim, (void *)counters, (void *)tiles,
                         (void *)rot, (void *)Vt, (void *)Vt2, (void *)Us, (void *)W, (void *)T,
-                        (void *)P})
+                        (void *)P, (void *)boff_s, (void *)bdim_s, (void *)boff_b, (void *)bdim_b,
+                        (void *)ioff_b, (void *)loff_b, (void *)lcap_b, (void *)diag_b,
+                        (void *)partner_b, (void *)act_b, (void *)acs_b, (void *)logpq_b,
+                        (void *)logcs_b, (void *)rcnt_b, (void *)norm_b})
             cudaFree(q);
         built = false;
     }
@@ -216,11 +266,24 @@ struct ProjectPlan {
         launches++;
         gemm(kGemmNTStore, Us, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches);
         gemm(kGemmNNStore, Vt, W, T, nullptr, 0.0, nullptr, nullptr, s, launches);
-        jacobi_warm_kernel<<<nblk, kJacobiThreads, smem, s>>>(T, P, Vt, boff, bdim, rot, rot_off,
-                                                              max_sweeps, abs_tol, gap_tol,
-                                                              counters, counters + 1);
-        V2B_CK(cudaGetLastError());
-        launches++;
+        if (nsmall) {
+            jacobi_warm_kernel<<<nsmall, kJacobiThreads, smem, s>>>(T, P, Vt, boff_s, bdim_s, rot,
+                                                                    rot_off, max_sweeps, abs_tol,
+                                                                    gap_tol, counters, counters + 1);
+            V2B_CK(cudaGetLastError());
+            launches++;
+        }
+        if (nbig) {
+            BigJacobiArgs a;
+            a.T = T; a.P = P; a.Vt = Vt; a.boff = boff_b; a.bdim = bdim_b;
+            a.diag = diag_b; a.partner = partner_b; a.act = act_b; a.acs = acs_b; a.ioff = ioff_b;
+            a.log_pq = logpq_b; a.log_cs = logcs_b; a.loff = loff_b; a.lcap = lcap_b;
+            a.round_cnt = rcnt_b; a.norm_part = norm_b; a.max_rounds = kBigMaxRounds;
+            a.abs_tol = abs_tol; a.gap_tol = gap_tol; a.counters = counters + 2;
+            jacobi_big_kernel<<<nbig * kBigCluster, kBigThreads, 0, s>>>(a);
+            V2B_CK(cudaGetLastError());
+            launches++;
+        }
         gemm(kGemmTNStore, Vt, P, W, nullptr, 0.0, nullptr, nullptr, s, launches);
         gemm(kGemmNNProject, W, Vt, nullptr, nullptr, 1.0 / mu, x, z, s, launches);
     }
@@ -826,10 +889,10 @@ int v2b_problem_projection_counts(const v2b_problem *p, long *calls, long *rotat
         if (!p || !calls || !rotations || !sweep_overruns)
             throw std::invalid_argument("projection_counts: NULL argument");
         *calls = p->plan.calls;
-        int h[2] = {0, 0};
-        if (p->plan.built) V2B_CK(cudaMemcpy(h, p->plan.counters, 8, cudaMemcpyDeviceToHost));
-        *rotations = h[1];
-        *sweep_overruns = h[0];
+        int h[4] = {0, 0, 0, 0};
+        if (p->plan.built) V2B_CK(cudaMemcpy(h, p->plan.counters, 16, cudaMemcpyDeviceToHost));
+        *rotations = (long)h[1] + h[3];
+        *sweep_overruns = (long)h[0] + h[2];
         return V2B_OK;
     });
 }

@@ -11,7 +11,8 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-11
 
 
-@pytest.mark.parametrize("n,na,nb", [(2, 1, 1), (4, 2, 2), (3, 2, 1), (8, 4, 4)])
+@pytest.mark.parametrize("n,na,nb", [(2, 1, 1), (4, 2, 2), (3, 2, 1), (8, 4, 4), (10, 5, 5),
+                                     (20, 10, 10)])
 def test_projection_matches_lapack(cuda_device, n, na, nb):
     import torch
     p = hb.V2RDMProblem(n, na, nb)
@@ -46,3 +47,19 @@ def test_projection_degenerate_and_definite_blocks(cuda_device):
     xr, zr = project_blocks(U, p.dims, 1.0)
     assert np.max(np.abs(x.cpu().numpy() - xr)) <= TOL * 10
     assert np.max(np.abs(z.cpu().numpy() - zr)) <= TOL * 10
+
+
+def test_large_block_repeated_projection(cuda_device):
+    """Repeated cold projections of slowly changing U with a 200-row block (cluster
+    Jacobi) match LAPACK each time (the work arrays are reused between calls)."""
+    import torch
+    p = hb.V2RDMProblem(10, 5, 5)
+    rng = np.random.default_rng(3)
+    U = rng.standard_normal(p.n_primal)
+    for k in range(3):
+        U2 = U + 1e-4 * k * rng.standard_normal(p.n_primal)
+        x, z = p.project(torch.from_numpy(U2).to(cuda_device), 0.5)
+        xr, zr = project_blocks(U2, p.dims, 0.5)
+        scale = max(1.0, np.linalg.norm(U2))
+        assert np.max(np.abs(x.cpu().numpy() - xr)) <= TOL * scale
+        assert np.max(np.abs(z.cpu().numpy() - zr)) <= TOL * scale

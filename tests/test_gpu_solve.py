@@ -92,3 +92,22 @@ def test_monitor_protocol(cuda_device):
     assert rows[0][1] == pytest.approx(0.1)
     assert all(r[1] == rows[0][1] for r in rows[:20])
     assert rows[20][1] == pytest.approx(rows[19][1] * rows[19][2] / rows[19][3], rel=1e-12)
+
+
+def test_large_block_trajectory_matches_oracle(cuda_device):
+    """100 boundary-point iterations of a 9-site ring (G2aa block of 162 rows, past the
+    shared-memory Jacobi limit, so the cluster kernel runs) follow the numpy oracle."""
+    from oracle.bpsdp import BPSDPSolver
+    n = 9
+    o = OracleProblem(n, 4, 4, "DQG", True, True, hubbard=(1.0, 4.0))
+    assert max(o.dims) > 160
+    so = BPSDPSolver(o.n_primal, o.n_dual, SDPOptions(1e-12, 1e-12, 1e-9, 10000, 100))
+    xo = o.guess("random")
+    so.solve(xo, o.b, o.c, o.dims, 100, o.Au, o.ATu)
+    p = hb.V2RDMProblem(n, 4, 4, hubbard_multiplicity=True)
+    opts = hb.Options({"R_CONVERGENCE": 1e-12, "E_CONVERGENCE": 1e-12, "MAXITER": 100,
+                       "MU_UPDATE_FREQUENCY": 100})
+    xg, st = p.solve(o.guess("random"), o.b, o.c, opts)
+    assert st["oiter"] == 100
+    assert np.max(np.abs(xg - xo)) <= 1e-6
+    assert abs(float(o.c @ xg) - float(o.c @ xo)) <= 1e-7
