@@ -17,21 +17,20 @@ struct BigJacobiArgs {
     double *Vt;                  // eigenvector rows (in / out)
     const int64_t *boff;         // matrix offset of each block
     const int *bdim;
-    double *diag;                // per-index work arrays, offset ioff[b]
-    int *partner;
-    int *act;
-    double2 *acs;
-    const int64_t *ioff;
-    int2 *log_pq;                // rotation log, offset loff[b], capacity lcap[b]
-    double2 *log_cs;
-    const int64_t *loff;
-    const int64_t *lcap;
-    int *round_cnt;              // max_rounds ints per block
+    double2 *rot;                // rotation record + step counters, offset roff[b]
+    const int64_t *roff;
+    int max_sweeps;
     double *norm_part;           // kBigCluster doubles per block
-    int max_rounds;
     double abs_tol, gap_tol;
-    int *counters;               // [0] blocks that stopped early, [1] rotations
+    int *counters;               // [0] blocks that hit max_sweeps, [1] rotations
 };
+
+// double2 slots of one block's record: sweeps x steps x pairs rotations,
+// then sweeps x (steps + 1) int counters
+inline int64_t big_record_slots(int n, int max_sweeps) {
+    const int np = n + (n & 1), nsteps = np - 1, m = np / 2;
+    return (int64_t)max_sweeps * nsteps * m + ((int64_t)max_sweeps * (nsteps + 1) + 3) / 4 + 1;
+}
 
 __global__ void jacobi_big_kernel(BigJacobiArgs a);
 

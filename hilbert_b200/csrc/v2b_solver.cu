@@ -113,7 +113,6 @@ struct DeviceOp {
 // Every kReorthEvery calls Vt is re-orthonormalised, Vt <- Vt + (I - Vt Vt^T) Vt / 2.
 struct ProjectPlan {
     static constexpr int kReorthEvery = 64;
-    static constexpr int kBigMaxRounds = 100000;
     std::vector<int> dims;
     int nblk = 0, nsmall = 0, nbig = 0;
     int64_t total = 0;
@@ -124,11 +123,11 @@ struct ProjectPlan {
     double2 *rot = nullptr;
     double *Vt = nullptr, *Vt2 = nullptr, *Us = nullptr, *W = nullptr, *T = nullptr, *P = nullptr;
     // large-block work arrays
-    int64_t *ioff_b = nullptr, *loff_b = nullptr, *lcap_b = nullptr;
-    double *diag_b = nullptr, *norm_b = nullptr;
-    int *partner_b = nullptr, *act_b = nullptr, *rcnt_b = nullptr;
-    double2 *acs_b = nullptr, *logcs_b = nullptr;
-    int2 *logpq_b = nullptr;
+    static constexpr int kBigSweeps = 16;
+    int64_t *roff_b = nullptr;
+    double *norm_b = nullptr;
+    double2 *rec_b = nullptr;
+    int max_big = 0;
     size_t smem = 0;
     int max_sweeps = 30;
     bool fresh = true;
@@ -139,10 +138,10 @@ struct ProjectPlan {
     void build(const std::vector<int> &d) {
         dims = d;
         nblk = (int)d.size();
-        std::vector<int64_t> off(nblk), roff, off_s, off_b, ioff, loff, lcap;
+        std::vector<int64_t> off(nblk), roff, off_s, off_b, roffb;
         std::vector<int> dim_s, dim_b;
         std::vector<int4> tl;
-        int64_t o = 0, ro = 0, io = 0, lo = 0;
+        int64_t o = 0, ro = 0, rb = 0;
         smem = 0;
         for (int i = 0; i < nblk; i++) {
             if (d[i] < 0) throw std::invalid_argument("negative block dimension");
@@ -162,13 +161,9 @@ struct ProjectPlan {
             } else {
                 off_b.push_back(o);
                 dim_b.push_back(d[i]);
-                ioff.push_back(io);
-                io += d[i];
-                loff.push_back(lo);
-                // room for about six full sweeps of rotations
-                const int64_t c = 3 * (int64_t)d[i] * d[i];
-                lcap.push_back(c);
-                lo += c;
+                roffb.push_back(rb);
+                rb += v2b::big_record_slots(d[i], kBigSweeps);
+                max_big = std::max(max_big, d[i]);
             }
             o += (int64_t)d[i] * d[i];
         }
@@ -200,22 +195,12 @@ struct ProjectPlan {
         if (nbig) {
             boff_b = dalloc<int64_t>(nbig);
             bdim_b = dalloc<int>(nbig);
-            ioff_b = dalloc<int64_t>(nbig);
-            loff_b = dalloc<int64_t>(nbig);
-            lcap_b = dalloc<int64_t>(nbig);
-            diag_b = dalloc<double>(io);
-            partner_b = dalloc<int>(io);
-            act_b = dalloc<int>(io);
-            acs_b = dalloc<double2>(io);
-            logpq_b = dalloc<int2>(lo);
-            logcs_b = dalloc<double2>(lo);
-            rcnt_b = dalloc<int>((size_t)nbig * kBigMaxRounds);
+            roff_b = dalloc<int64_t>(nbig);
+            rec_b = dalloc<double2>(rb);
             norm_b = dalloc<double>((size_t)nbig * v2b::kBigCluster);
             V2B_CK(cudaMemcpy(boff_b, off_b.data(), nbig * 8, cudaMemcpyHostToDevice));
             V2B_CK(cudaMemcpy(bdim_b, dim_b.data(), nbig * 4, cudaMemcpyHostToDevice));
-            V2B_CK(cudaMemcpy(ioff_b, ioff.data(), nbig * 8, cudaMemcpyHostToDevice));
-            V2B_CK(cudaMemcpy(loff_b, loff.data(), nbig * 8, cudaMemcpyHostToDevice));
-            V2B_CK(cudaMemcpy(lcap_b, lcap.data(), nbig * 8, cudaMemcpyHostToDevice));
+            V2B_CK(cudaMemcpy(roff_b, roffb.data(), nbig * 8, cudaMemcpyHostToDevice));
         }
         fresh = true;
         built = true;
@@ -225,9 +210,7 @@ struct ProjectPlan {
         for (void *q : {(void *)boff, (void *)rot_off, (void *)bdim, (void *)counters, (void *)tiles,
                         (void *)rot, (void *)Vt, (void *)Vt2, (void *)Us, (void *)W, (void *)T,
                         (void *)P, (void *)boff_s, (void *)bdim_s, (void *)boff_b, (void *)bdim_b,
-                        (void *)ioff_b, (void *)loff_b, (void *)lcap_b, (void *)diag_b,
-                        (void *)partner_b, (void *)act_b, (void *)acs_b, (void *)logpq_b,
-                        (void *)logcs_b, (void *)rcnt_b, (void *)norm_b})
+                        (void *)roff_b, (void *)rec_b, (void *)norm_b})
             cudaFree(q);
         built = false;
     }
@@ -276,11 +259,10 @@ struct ProjectPlan {
         if (nbig) {
             BigJacobiArgs a;
             a.T = T; a.P = P; a.Vt = Vt; a.boff = boff_b; a.bdim = bdim_b;
-            a.diag = diag_b; a.partner = partner_b; a.act = act_b; a.acs = acs_b; a.ioff = ioff_b;
-            a.log_pq = logpq_b; a.log_cs = logcs_b; a.loff = loff_b; a.lcap = lcap_b;
-            a.round_cnt = rcnt_b; a.norm_part = norm_b; a.max_rounds = kBigMaxRounds;
+            a.rot = rec_b; a.roff = roff_b; a.max_sweeps = kBigSweeps; a.norm_part = norm_b;
             a.abs_tol = abs_tol; a.gap_tol = gap_tol; a.counters = counters + 2;
-            jacobi_big_kernel<<<nbig * kBigCluster, kBigThreads, 0, s>>>(a);
+            const size_t alist_bytes = (size_t)((max_big + 1) / 2 + 1) * sizeof(int);
+            jacobi_big_kernel<<<nbig * kBigCluster, kBigThreads, alist_bytes, s>>>(a);
             V2B_CK(cudaGetLastError());
             launches++;
         }
@@ -389,7 +371,7 @@ struct v2b_problem {
         // small problems: fewer CTAs make the grid barrier cheaper
         const int64_t rows = std::max(prob.n_primal, prob.n_dual);
         const int64_t want = (rows + (int64_t)v2b::kCgThreads - 1) / (int64_t)v2b::kCgThreads;
-        cg_grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sm_count() * std::min(per_sm, 1)));
+        cg_grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sm_count() * per_sm));
         partials = dalloc<double>(2 * (size_t)cg_grid);
         stats_partials = dalloc<double>(4 * v2b::kStatsBlocks);
         cg_out = dalloc<double>(2);
