@@ -28,7 +28,6 @@ import os
 import statistics
 import subprocess
 import sys
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -63,7 +62,12 @@ def parse():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region.
+
+    One ``nvidia-smi -lms 200`` process runs for the whole sampling window and
+    writes to a temporary file: the benchmark process forks once, before the
+    work it measures (a fork per sample from a process holding a CUDA context
+    stalls that context for tens of milliseconds each time)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -72,35 +76,50 @@ class ClockSampler:
     def __init__(self, index=0):
         self.index = index
         self.rows = []
-        self._stop = threading.Event()
-        self._t = None
+        self._proc = None
+        self._file = None
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.index}",
-                                      f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits"],
-                                     capture_output=True, text=True, timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([v.strip() for v in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
-
-    def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+    def start(self):
+        import tempfile
+        self._file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self._file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self._proc = None
         return self
 
+    def stop(self):
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=10)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+                self._proc.wait()
+        if self._file is not None:
+            self._file.flush()
+            self._file.seek(0)
+            for line in self._file.read().splitlines():
+                if line.strip():
+                    self.rows.append([v.strip() for v in line.split(",")])
+            self._file.close()
+            os.unlink(self._file.name)
+            self._file = None
+
+    def __enter__(self):
+        return self.start()
+
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        self.stop()
 
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        sm = [float(r[1]) for r in self.rows if len(r) > 1 and r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in self.rows for k in range(4)
                           if len(r) > 5 + k and r[5 + k].lower() == "active"})
@@ -255,12 +274,13 @@ def run_b200(args, w):
         st = p.solve_device(dx, db, dc, opts)
         return st
 
+    clk = ClockSampler(local).start()   # started before the warm-up: no fork in the timed region
     for _ in range(args.warmup):
         one()
     times, stats = [], None
     launches0 = p.kernel_launches()
     p.set_profiling(True)
-    with ClockSampler(local) as clk:
+    with clk:
         for _ in range(args.steps):
             dx.copy_(dx0)
             flush.fill_(1.0)

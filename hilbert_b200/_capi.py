@@ -32,11 +32,12 @@ EXPORTS = (
     "v2b_problem_create", "v2b_problem_destroy", "v2b_problem_n_primal", "v2b_problem_n_dual",
     "v2b_problem_n_blocks", "v2b_problem_block_dims", "v2b_problem_build_b",
     "v2b_problem_build_c_hubbard", "v2b_problem_build_c_external", "v2b_problem_guess",
-    "v2b_problem_Au", "v2b_problem_ATu", "v2b_problem_project", "v2b_problem_solve",
+    "v2b_problem_Au", "v2b_problem_ATu", "v2b_problem_project", "v2b_problem_project_warm",
+    "v2b_problem_solve",
     "v2b_problem_solve_device", "v2b_problem_get_y", "v2b_problem_get_z", "v2b_problem_get_mu",
     "v2b_problem_kernel_launches", "v2b_problem_operator_size", "v2b_problem_operator",
     "v2b_problem_set_profiling", "v2b_problem_profile", "v2b_problem_stream",
-    "v2b_problem_projection_counts", "v2b_project_block_noalloc",
+    "v2b_problem_projection_counts", "v2b_problem_refine_counts", "v2b_project_block_noalloc",
 )
 
 
@@ -105,6 +106,7 @@ def load(path=LIB_PATH):
         "v2b_problem_Au": (ctypes.c_int, [vp, vp, vp, vp]),
         "v2b_problem_ATu": (ctypes.c_int, [vp, vp, vp, vp]),
         "v2b_problem_project": (ctypes.c_int, [vp, vp, ctypes.c_double, vp, vp, vp]),
+        "v2b_problem_project_warm": (ctypes.c_int, [vp, vp, ctypes.c_double, vp, vp, vp]),
         "v2b_problem_solve": (ctypes.c_int, [vp, dp, dp, dp, ctypes.POINTER(SDPOptions), ctypes.c_int,
                                              SDP_MONITOR, ctypes.c_int, vp, lp, lp, dp]),
         "v2b_problem_solve_device": (ctypes.c_int, [vp, vp, vp, vp, ctypes.POINTER(SDPOptions),
@@ -118,6 +120,7 @@ def load(path=LIB_PATH):
         "v2b_problem_profile": (ctypes.c_int, [vp, dp, lp]),
         "v2b_problem_stream": (ctypes.c_void_p, [vp]),
         "v2b_problem_projection_counts": (ctypes.c_int, [vp, lp, lp, lp]),
+        "v2b_problem_refine_counts": (ctypes.c_int, [vp, lp, lp, lp, lp]),
         "v2b_project_block_noalloc": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, vp, vp, vp]),
         "v2b_problem_operator_size": (ctypes.c_int, [vp, ctypes.c_int, lp, lp, ip]),
         "v2b_problem_operator": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint32),

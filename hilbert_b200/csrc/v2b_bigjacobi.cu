@@ -24,21 +24,6 @@ namespace cg = cooperative_groups;
 
 namespace v2b {
 
-// same pairing as the shared-memory kernel
-__device__ __forceinline__ void rr_pair_big(int s, int k, int np, int &p, int &q) {
-    const int m1 = np - 1;
-    int a, b;
-    if (k == 0) {
-        a = m1;
-        b = s;
-    } else {
-        a = (s + k) % m1;
-        b = (s - k + m1) % m1;
-    }
-    p = a < b ? a : b;
-    q = a < b ? b : a;
-}
-
 __global__ void __cluster_dims__(kBigCluster, 1, 1) __launch_bounds__(kBigThreads)
     jacobi_big_kernel(BigJacobiArgs a) {
     cg::cluster_group cl = cg::this_cluster();
@@ -95,7 +80,7 @@ __global__ void __cluster_dims__(kBigCluster, 1, 1) __launch_bounds__(kBigThread
             // A: rotations of this step's pairs
             for (int64_t k = ctid; k < m; k += cstride) {
                 int p, q;
-                rr_pair_big(st, (int)k, np, p, q);
+                rr_pair(st, (int)k, np, p, q);
                 double c = 1.0, s = 0.0;
                 if (q < n) {
                     const double apq = __ldcg(T + (int64_t)p * n + q);
@@ -134,8 +119,8 @@ __global__ void __cluster_dims__(kBigCluster, 1, 1) __launch_bounds__(kBigThread
                 if (cq.y != 0.0 && Qk < Pk) continue;
                 const double2 cp = __ldcg(rs + Pk);
                 int pP, qP, pQ, qQ;
-                rr_pair_big(st, Pk, np, pP, qP);
-                rr_pair_big(st, Qk, np, pQ, qQ);
+                rr_pair(st, Pk, np, pP, qP);
+                rr_pair(st, Qk, np, pQ, qQ);
                 const bool qPin = qP < n, qQin = qQ < n;   // n odd: index n is padding
                 const double b11 = __ldcg(T + (int64_t)pP * n + pQ);
                 const double b12 = qQin ? __ldcg(T + (int64_t)pP * n + qQ) : 0.0;
@@ -205,7 +190,7 @@ __global__ void __cluster_dims__(kBigCluster, 1, 1) __launch_bounds__(kBigThread
             for (int64_t it = ctid; it < (int64_t)active * n; it += cstride) {
                 const int k = alist[it / n], j = (int)(it % n);
                 int p, q;
-                rr_pair_big(st, k, np, p, q);
+                rr_pair(st, k, np, p, q);
                 const double2 r2 = __ldcg(rs + k);
                 const double vp = __ldcg(Vt + (int64_t)p * n + j), vq = __ldcg(Vt + (int64_t)q * n + j);
                 Vt[(int64_t)p * n + j] = r2.x * vp - r2.y * vq;

@@ -25,12 +25,14 @@ __global__ void __launch_bounds__(256)
                       double *__restrict__ C, const int4 *__restrict__ tiles,
                       const int64_t *__restrict__ boff, const int *__restrict__ bdim,
                       const double *__restrict__ Cin, const double *__restrict__ Us, double inv_mu,
-                      double *__restrict__ xo, double *__restrict__ zo) {
+                      double *__restrict__ xo, double *__restrict__ zo,
+                      const int *__restrict__ bstate, unsigned long long *__restrict__ orth) {
     constexpr int BM = 64, BK = 16;
     __shared__ double As[BK][BM + 2];
     __shared__ double Bs[BK][BM + 2];
     const int4 t = tiles[blockIdx.x];
     const int blk = t.x, n = bdim[blk];
+    if (bstate && bstate[blk] != 0) return;   // uniform over the CTA
     const int64_t off = boff[blk];
     const int r0 = t.y * BM, c0 = t.z * BM;
     const double *Ab = A + off, *Bb = B + off;
@@ -77,6 +79,7 @@ __global__ void __launch_bounds__(256)
         }
         __syncthreads();
     }
+    double dev = 0.0;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         const int r = r0 + ty * 4 + i;
@@ -90,30 +93,44 @@ __global__ void __launch_bounds__(256)
                 C[e] = acc[i][j];
             } else if (EPI == kEpiAdd) {
                 C[e] = Cin[e] + acc[i][j];
+            } else if (EPI == kEpiNS) {   // acc = Vt Vt^T
+                const double id = (r == c) ? 1.0 : 0.0;
+                C[e] = 1.5 * id - 0.5 * acc[i][j];
+                dev = fmax(dev, fabs(acc[i][j] - id));
             } else {   // kEpiProject: acc = U+
                 xo[e] = acc[i][j] * inv_mu;
                 zo[e] = acc[i][j] - Us[e];
             }
         }
     }
+    if (EPI == kEpiNS) {
+        // non-negative doubles order like their bit patterns
+        dev = warp_max(dev);
+        if ((threadIdx.x & 31) == 0 && dev > 0.0)
+            atomicMax(orth + blk, (unsigned long long)__double_as_longlong(dev));
+    }
 }
 
 cudaError_t launch_gemm_tiles(GemmVariant v, int ntiles, cudaStream_t s, GEMM_ARGS) {
+    if (ntiles <= 0) return cudaSuccess;
     switch (v) {
+        case kGemmNTNewtonSchulz:
+            gemm_tiles_kernel<false, true, kEpiNS><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate, orth);
+            break;
         case kGemmNTStore:
-            gemm_tiles_kernel<false, true, kEpiStore><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo);
+            gemm_tiles_kernel<false, true, kEpiStore><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate, orth);
             break;
         case kGemmNNStore:
-            gemm_tiles_kernel<false, false, kEpiStore><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo);
+            gemm_tiles_kernel<false, false, kEpiStore><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate, orth);
             break;
         case kGemmTNStore:
-            gemm_tiles_kernel<true, false, kEpiStore><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo);
+            gemm_tiles_kernel<true, false, kEpiStore><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate, orth);
             break;
         case kGemmNNProject:
-            gemm_tiles_kernel<false, false, kEpiProject><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo);
+            gemm_tiles_kernel<false, false, kEpiProject><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate, orth);
             break;
         case kGemmNNAdd:
-            gemm_tiles_kernel<false, false, kEpiAdd><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo);
+            gemm_tiles_kernel<false, false, kEpiAdd><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate, orth);
             break;
     }
     return cudaGetLastError();

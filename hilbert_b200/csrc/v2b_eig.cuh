@@ -11,6 +11,7 @@ namespace v2b {
 constexpr int kEpiStore = 0;     // C = op(A) op(B)
 constexpr int kEpiAdd = 1;       // C = Cin + op(A) op(B)
 constexpr int kEpiProject = 2;   // x = (op(A) op(B)) / mu, z = op(A) op(B) - Us
+constexpr int kEpiNS = 3;        // C = 3/2 I - 1/2 op(A) op(B); orth[b] = max |op(A) op(B) - I|
 constexpr int kGemmTile = 64;
 
 #define GEMM_ARGS                                                                           \
@@ -18,13 +19,16 @@ constexpr int kGemmTile = 64;
         const int4 *__restrict__ tiles, const int64_t *__restrict__ boff,                    \
         const int *__restrict__ bdim, const double *__restrict__ Cin,                        \
         const double *__restrict__ Us, double inv_mu, double *__restrict__ xo,               \
-        double *__restrict__ zo
+        double *__restrict__ zo, const int *__restrict__ bstate,                             \
+        unsigned long long *__restrict__ orth
 
 // Host launcher of gemm_tiles_kernel<TA, TB, EPI> (defined, with the kernel
 // instantiations, in v2b_eig.cu).  variant: 0 <N,T,store>, 1 <N,N,store>,
-// 2 <T,N,store>, 3 <N,N,project>, 4 <N,N,add>.
+// 2 <T,N,store>, 3 <N,N,project>, 4 <N,N,add>, 5 <N,T,Newton-Schulz>.
+// With bstate non-null, tiles of blocks whose state is not 0 (refinement in
+// progress) are skipped.
 enum GemmVariant { kGemmNTStore = 0, kGemmNNStore = 1, kGemmTNStore = 2, kGemmNNProject = 3,
-                   kGemmNNAdd = 4 };
+                   kGemmNNAdd = 4, kGemmNTNewtonSchulz = 5 };
 cudaError_t launch_gemm_tiles(GemmVariant v, int ntiles, cudaStream_t s, GEMM_ARGS);
 
 }  // namespace v2b

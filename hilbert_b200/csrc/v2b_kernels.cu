@@ -245,21 +245,6 @@ __global__ void stats_kernel(const double *__restrict__ Ax, const double *__rest
 }
 
 // --------------------------------------------------------- projection
-// Round-robin ("circle method") pairing of np (even) indices: in step s the
-// fixed index np-1 meets s and, for k >= 1, (s+k) meets (s-k) mod (np-1).
-__device__ __forceinline__ void rr_pair(int s, int k, int np, int &p, int &q) {
-    const int m1 = np - 1;
-    int a, b;
-    if (k == 0) {
-        a = m1;
-        b = s;
-    } else {
-        a = (s + k) % m1;
-        b = (s - k + m1) % m1;
-    }
-    p = a < b ? a : b;
-    q = a < b ? b : a;
-}
 
 // One CTA per PSD block (n <= kJacobiMaxDim): selective parallel cyclic
 // Jacobi on T = V^T U V, where the rows of Vt (= V^T) are the previous

@@ -146,10 +146,10 @@ extern "C" int v2b_project_block_noalloc(const double *d_U, int n, double mu, do
     jacobi_warm_kernel<<<1, kJacobiThreads, jacobi_smem_bytes(n), s>>>(
         Us, P, Vt, boff, bdim, rot, rot_off, kNoAllocSweeps, 1e-14, 1e-13, counters, counters + 1);
     e = launch_gemm_tiles(kGemmTNStore, nt * nt, s, Vt, P, W, tiles, boff, bdim, nullptr, Us, 0.0,
-                          nullptr, nullptr);
+                          nullptr, nullptr, nullptr, nullptr);
     if (e == cudaSuccess)
         e = launch_gemm_tiles(kGemmNNProject, nt * nt, s, W, Vt, nullptr, tiles, boff, bdim, nullptr,
-                              Us, 1.0 / mu, d_x, d_z);
+                              Us, 1.0 / mu, d_x, d_z, nullptr, nullptr);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return fail(V2B_CUDA_ERROR, cudaGetErrorString(e));
     return V2B_OK;

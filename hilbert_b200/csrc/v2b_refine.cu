@@ -1,0 +1,352 @@
+// Warm eigen-refinement of the per-block PSD projection (sm_100a).
+//
+// The projection needs U+ = V f(L) V^T with f(l) = max(l, 0).  The rows of
+// Vt from the previous outer iteration nearly diagonalise the new block, so
+// T = Vt U Vt^T = D + E with E small, and to first order
+//     f(T) = Gamma o T,   Gamma_pq = (f(d_p) - f(d_q)) / (d_p - d_q)
+// (Daleckii-Krein).  f is linear on each side of zero, so the first-order
+// formula loses accuracy only through couplings between the two sides, and
+// through couplings that blur the sign of a diagonal entry.  A pair (p, q) is
+// accepted when
+//     t_pq^2 <= gap_tol ||T||_F Delta_pq   or   |t_pq| <= abs_tol ||T||_F,
+//     Delta_pq = |d_p - d_q|            (d_p, d_q of opposite sign)
+//              = min(|d_p|, |d_q|)      (same sign: distance to zero)
+// (the same tolerances as the Jacobi kernels' rotation test, with the gap
+// replaced by the distance that governs f's second divided differences).
+// A block whose pairs all pass takes P = Gamma o T directly.  Otherwise one
+// pass refines Vt:
+//   * non-separable failing pairs (|t_pq| > rho |d_p - d_q|) form a graph; its
+//     connected components ("clusters", found on the host from the recorded
+//     edges) are diagonalised exactly (cluster_eig_kernel) and applied to the
+//     cluster rows and columns of T and to the cluster rows of Vt;
+//   * every remaining separable failing pair takes one Newton step of the
+//     eigenvector equation, Vt <- (I - K) Vt with K_pq = t_pq / (d_q - d_p),
+//     followed by one Newton-Schulz orthonormalisation
+//     Vt <- (3/2 I - 1/2 Vt Vt^T) Vt (GEMMs).  Accepted pairs take the step only
+//     when it is tiny: inside a near-degenerate same-sign cluster t/(d_q - d_p)
+//     is large and meaningless (f is linear there) and would only cost
+//     orthogonality;
+// and T is recomputed.  Blocks that still fail after kRefinePasses passes, or
+// whose clusters exceed kRefineMaxCluster rows, fall back to the selective
+// Jacobi kernels, restarted from the basis and T the call began with.
+#include "v2b_kernels.cuh"
+#include "v2b_refine.cuh"
+
+namespace v2b {
+
+__device__ __forceinline__ double gamma_pq(double li, double lj) {
+    const double pi = fmax(li, 0.0), pj = fmax(lj, 0.0);
+    return (li != lj) ? (pi - pj) / (li - lj) : (li > 0.0 ? 1.0 : 0.0);
+}
+
+__global__ void __launch_bounds__(kRefineThreads)
+    refine_classify_kernel(const double *__restrict__ T, double *__restrict__ P,
+                           const int64_t *__restrict__ boff, const int *__restrict__ bdim,
+                           int *__restrict__ bstate, const unsigned long long *__restrict__ orth,
+                           int force, double gap_tol, double abs_tol, double *__restrict__ bnorm,
+                           int *h_state, int *h_nbad, int *h_nedge, int2 *h_edges) {
+    const int blk = blockIdx.x;
+    if (bstate[blk] != kStWork) return;   // uniform over the CTA
+    const int n = bdim[blk];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+    __shared__ double red[32];
+    __shared__ double s_nrm;
+    __shared__ int s_bad, s_ne;
+    extern __shared__ double dg[];   // n diagonal entries
+    if (n <= 0) {
+        if (tid == 0) {
+            bstate[blk] = kStDone;
+            h_state[blk] = kStDone;
+            h_nbad[blk] = 0;
+            h_nedge[blk] = 0;
+        }
+        return;
+    }
+    const int64_t off = boff[blk];
+    const double *Tb = T + off;
+    if (tid == 0) {
+        s_bad = 0;
+        s_ne = 0;
+    }
+    for (int i = tid; i < n; i += blockDim.x) dg[i] = Tb[(int64_t)i * n + i];
+    double fro = 0.0;
+    for (int64_t e = tid; e < (int64_t)n * n; e += blockDim.x) {
+        const double v = Tb[e];
+        fro += v * v;
+    }
+    fro = block_sum(fro, red);
+    if (tid == 0) {
+        s_nrm = sqrt(fro);
+        bnorm[blk] = s_nrm;
+    }
+    __syncthreads();
+    const double nrm = s_nrm;
+    const double atol = abs_tol * nrm, gtol = gap_tol * nrm;
+    int bad = 0;
+    int2 *eb = h_edges + (int64_t)blk * kRefineEdgeCap;
+    for (int i = warp; i < n; i += nwarp) {
+        const double di = dg[i];
+        for (int j = i + 1 + lane; j < n; j += 32) {
+            const double t = 0.5 * (Tb[(int64_t)i * n + j] + Tb[(int64_t)j * n + i]);
+            const double at = fabs(t);
+            if (at <= atol) continue;
+            const double dj = dg[j];
+            const double g = fabs(di - dj);
+            const bool cross = (di >= 0.0) != (dj >= 0.0);
+            const double delta = cross ? g : fmin(fabs(di), fabs(dj));
+            if (t * t > gtol * delta) {
+                bad++;
+                if (at > kRefineRho * g) {
+                    const int e = atomicAdd(&s_ne, 1);
+                    if (e < kRefineEdgeCap) eb[e] = make_int2(i, j);
+                }
+            }
+        }
+    }
+    bad = __reduce_add_sync(0xffffffffu, bad);
+    if (lane == 0 && bad) atomicAdd(&s_bad, bad);
+    __syncthreads();
+    const int nbad = s_bad;
+    const bool done = nbad == 0 && __longlong_as_double((long long)orth[blk]) <= kRefineOrthDone;
+    if (done) {
+        double *Pb = P + off;
+        for (int64_t e = tid; e < (int64_t)n * n; e += blockDim.x) {
+            const int i = (int)(e / n), j = (int)(e % n);
+            Pb[e] = (i == j) ? fmax(dg[i], 0.0)
+                             : gamma_pq(dg[i], dg[j]) * 0.5 * (Tb[e] + Tb[(int64_t)j * n + i]);
+        }
+    }
+    if (tid == 0) {
+        const int st = done ? kStDone : (force ? kStJacobi : kStWork);
+        bstate[blk] = st;
+        h_state[blk] = st;
+        h_nbad[blk] = nbad;
+        h_nedge[blk] = s_ne;
+    }
+}
+
+// ---------------------------------------------------------------- clusters
+__global__ void __launch_bounds__(256)
+    cluster_eig_kernel(const double *__restrict__ T, const int64_t *__restrict__ boff,
+                       const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,
+                       const int *__restrict__ mem, double *__restrict__ Qt,
+                       double *__restrict__ lam) {
+    const ClusterJob jb = jobs[blockIdx.x];
+    const int k = jb.k, n = bdim[jb.blk];
+    const int kp = k + (k & 1), ld = kp + 1, m = kp / 2;
+    const int *C = mem + jb.moff;
+    const double *Tb = T + boff[jb.blk];
+    extern __shared__ double sm[];
+    double *A = sm;              // kp x ld
+    double *Q = A + kp * ld;     // kp x ld, rows = eigenvectors
+    __shared__ double2 cs[kRefineMaxCluster / 2];
+    __shared__ double red[32];
+    __shared__ double s_thr;
+    __shared__ int s_nrot;
+    double fro = 0.0;
+    for (int e = threadIdx.x; e < kp * kp; e += blockDim.x) {
+        const int i = e / kp, j = e % kp;
+        double v = 0.0;
+        if (i < k && j < k) {
+            const int64_t a = C[i], b = C[j];
+            v = 0.5 * (Tb[a * n + b] + Tb[b * n + a]);
+        }
+        A[i * ld + j] = v;
+        Q[i * ld + j] = (i == j) ? 1.0 : 0.0;
+        fro += v * v;
+    }
+    fro = block_sum(fro, red);
+    if (threadIdx.x == 0) s_thr = 1e-15 * sqrt(fro) + 1e-300;
+    __syncthreads();
+    const double thr = s_thr;
+    for (int sweep = 0; sweep < 40; sweep++) {
+        if (threadIdx.x == 0) s_nrot = 0;
+        __syncthreads();
+        for (int st = 0; st < kp - 1; st++) {
+            for (int kk = threadIdx.x; kk < m; kk += blockDim.x) {
+                int p, q;
+                rr_pair(st, kk, kp, p, q);
+                double c = 1.0, s = 0.0;
+                if (q < k) {
+                    const double apq = A[p * ld + q];
+                    if (fabs(apq) > thr) {
+                        const double app = A[p * ld + p], aqq = A[q * ld + q];
+                        const double tau = (aqq - app) / (2.0 * apq);
+                        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + hypot(1.0, tau));
+                        c = 1.0 / sqrt(1.0 + t * t);
+                        s = t * c;
+                        atomicAdd(&s_nrot, 1);
+                    }
+                }
+                cs[kk] = make_double2(c, s);
+            }
+            __syncthreads();
+            // A <- A G^T (columns p, q)
+            for (int e = threadIdx.x; e < m * kp; e += blockDim.x) {
+                const int kk = e / kp, r = e % kp;
+                const double2 g = cs[kk];
+                if (g.y == 0.0) continue;
+                int p, q;
+                rr_pair(st, kk, kp, p, q);
+                const double ap = A[r * ld + p], aq = A[r * ld + q];
+                A[r * ld + p] = g.x * ap - g.y * aq;
+                A[r * ld + q] = g.y * ap + g.x * aq;
+            }
+            __syncthreads();
+            // A <- G A, Q <- G Q (rows p, q)
+            for (int e = threadIdx.x; e < m * kp; e += blockDim.x) {
+                const int kk = e / kp, col = e % kp;
+                const double2 g = cs[kk];
+                if (g.y == 0.0) continue;
+                int p, q;
+                rr_pair(st, kk, kp, p, q);
+                const double ap = A[p * ld + col], aq = A[q * ld + col];
+                A[p * ld + col] = g.x * ap - g.y * aq;
+                A[q * ld + col] = g.y * ap + g.x * aq;
+                const double qp = Q[p * ld + col], qq = Q[q * ld + col];
+                Q[p * ld + col] = g.x * qp - g.y * qq;
+                Q[q * ld + col] = g.y * qp + g.x * qq;
+            }
+            __syncthreads();
+        }
+        if (s_nrot == 0) break;   // uniform: read after the step's final barrier
+        __syncthreads();
+    }
+    double *Qo = Qt + jb.qoff;
+    for (int e = threadIdx.x; e < k * k; e += blockDim.x) Qo[e] = Q[(e / k) * ld + e % k];
+    for (int i = threadIdx.x; i < k; i += blockDim.x) lam[jb.moff + i] = A[i * ld + i];
+}
+
+__global__ void __launch_bounds__(256)
+    cluster_rows_kernel(const double *__restrict__ T, const double *__restrict__ Vt,
+                        double *__restrict__ W, double *__restrict__ Vt2,
+                        const int64_t *__restrict__ boff, const int *__restrict__ bdim,
+                        const ClusterJob *__restrict__ jobs, const int *__restrict__ mem,
+                        const double *__restrict__ Qt) {
+    const ClusterJob jb = jobs[blockIdx.x];
+    const int k = jb.k, n = bdim[jb.blk];
+    const int c0 = blockIdx.y * 64;
+    if (c0 >= n) return;
+    const int64_t off = boff[jb.blk];
+    const int *C = mem + jb.moff;
+    extern __shared__ double sm[];
+    double *sQ = sm;            // k x k
+    double *S = sQ + k * k;     // k x 64
+    for (int e = threadIdx.x; e < k * k; e += blockDim.x) sQ[e] = Qt[jb.qoff + e];
+    for (int pass = 0; pass < 2; pass++) {
+        const double *src = (pass == 0 ? T : Vt) + off;
+        double *dst = (pass == 0 ? W : Vt2) + off;
+        for (int e = threadIdx.x; e < k * 64; e += blockDim.x) {
+            const int l = e / 64, cc = e % 64;
+            S[e] = (c0 + cc < n) ? src[(int64_t)C[l] * n + c0 + cc] : 0.0;
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < k * 64; e += blockDim.x) {
+            const int i = e / 64, cc = e % 64;
+            if (c0 + cc >= n) continue;
+            double acc = 0.0;
+            for (int l = 0; l < k; l++) acc = fma(sQ[i * k + l], S[l * 64 + cc], acc);
+            dst[(int64_t)C[i] * n + c0 + cc] = acc;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256)
+    cluster_cols_kernel(double *__restrict__ T, const double *__restrict__ W,
+                        const int64_t *__restrict__ boff, const int *__restrict__ bdim,
+                        const ClusterJob *__restrict__ jobs, const int *__restrict__ mem,
+                        const int *__restrict__ rowclus, const int *__restrict__ rowbase,
+                        const double *__restrict__ Qt, const double *__restrict__ lam) {
+    const int jid = blockIdx.x;
+    const ClusterJob jb = jobs[jid];
+    const int k = jb.k, n = bdim[jb.blk];
+    const int r0 = blockIdx.y * 32;
+    if (r0 >= n) return;
+    const int64_t off = boff[jb.blk];
+    const int *C = mem + jb.moff;
+    const int *rc = rowclus + rowbase[jb.blk];
+    extern __shared__ double sm[];
+    double *sQ = sm;            // k x k
+    double *S = sQ + k * k;     // 32 x k: R(a)[C_m]
+    for (int e = threadIdx.x; e < k * k; e += blockDim.x) sQ[e] = Qt[jb.qoff + e];
+    for (int e = threadIdx.x; e < 32 * k; e += blockDim.x) {
+        const int a = r0 + e / k, mm = e % k;
+        double v = 0.0;
+        if (a < n) v = (rc[a] >= 0 ? W : T)[off + (int64_t)a * n + C[mm]];
+        S[e] = v;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < 32 * k; e += blockDim.x) {
+        const int a = r0 + e / k, i = e % k;
+        if (a >= n) continue;
+        double out;
+        if (rc[a] == jid) {
+            out = (a == C[i]) ? lam[jb.moff + i] : 0.0;
+        } else {
+            out = 0.0;
+            for (int mm = 0; mm < k; mm++) out = fma(S[(e / k) * k + mm], sQ[i * k + mm], out);
+        }
+        T[off + (int64_t)a * n + C[i]] = out;
+    }
+}
+
+__global__ void __launch_bounds__(256)
+    cluster_commit_kernel(double *__restrict__ T, const double *__restrict__ W,
+                          double *__restrict__ Vt, const double *__restrict__ Vt2,
+                          const int64_t *__restrict__ boff, const int *__restrict__ bdim,
+                          const ClusterJob *__restrict__ jobs, const int *__restrict__ mem,
+                          const int *__restrict__ rowclus, const int *__restrict__ rowbase) {
+    const ClusterJob jb = jobs[blockIdx.x];
+    const int k = jb.k, n = bdim[jb.blk];
+    const int c0 = blockIdx.y * 64;
+    if (c0 >= n) return;
+    const int64_t off = boff[jb.blk];
+    const int *C = mem + jb.moff;
+    const int *rc = rowclus + rowbase[jb.blk];
+    for (int e = threadIdx.x; e < k * 64; e += blockDim.x) {
+        const int i = e / 64, b = c0 + e % 64;
+        if (b >= n) continue;
+        const int64_t idx = off + (int64_t)C[i] * n + b;
+        if (rc[b] < 0) T[idx] = W[idx];
+        Vt[idx] = Vt2[idx];
+    }
+}
+
+// ---------------------------------------------------------------- Newton
+__global__ void __launch_bounds__(256)
+    newton_m_kernel(const double *__restrict__ T, double *__restrict__ M,
+                    const int4 *__restrict__ tiles, const int64_t *__restrict__ boff,
+                    const int *__restrict__ bdim, const int *__restrict__ bstate,
+                    const double *__restrict__ bnorm, double gap_tol, double abs_tol) {
+    const int4 t = tiles[blockIdx.x];
+    if (bstate[t.x] != kStWork) return;
+    const int n = bdim[t.x];
+    const int64_t off = boff[t.x];
+    const double *Tb = T + off;
+    const double nrm = bnorm[t.x];
+    const double atol = abs_tol * nrm, gtol = gap_tol * nrm;
+    for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
+        const int r = t.y * 64 + e / 64, c = t.z * 64 + e % 64;
+        if (r >= n || c >= n) continue;
+        double v;
+        if (r == c) {
+            v = 1.0;
+        } else {
+            const double tv = 0.5 * (Tb[(int64_t)r * n + c] + Tb[(int64_t)c * n + r]);
+            const double dr = Tb[(int64_t)r * n + r], dc = Tb[(int64_t)c * n + c];
+            const double g = dc - dr;
+            v = 0.0;
+            if (tv != 0.0 && fabs(tv) <= kRefineRho * fabs(g)) {
+                const double k = tv / g;
+                const bool cross = (dr >= 0.0) != (dc >= 0.0);
+                const double delta = cross ? fabs(g) : fmin(fabs(dr), fabs(dc));
+                const bool bad = fabs(tv) > atol && tv * tv > gtol * delta;
+                if (bad || fabs(k) <= kRefineKappa) v = -k;
+            }
+        }
+        M[off + (int64_t)r * n + c] = v;
+    }
+}
+
+}  // namespace v2b

@@ -24,6 +24,7 @@
 #include "v2b_bigjacobi.cuh"
 #include "v2b_eig.cuh"
 #include "v2b_kernels.cuh"
+#include "v2b_refine.cuh"
 #include "v2rdm_b200.h"
 #include "v2rdm_problem.h"
 
@@ -103,33 +104,66 @@ struct DeviceOp {
 };
 
 // Per-block PSD projection for a fixed list of block sizes.  The rows of Vt
-// hold each block's eigenvectors from the previous call (the identity before
-// the first), so every call is
-//   symmetrize; W = Us Vt^T; T = Vt W;                       (GEMM tiles, all blocks)
-//   selective Jacobi on T, rotations replayed onto Vt:
+// hold each block's eigenvector basis from the previous call (the identity
+// before the first), so every call starts with
+//   symmetrize; W = Us Vt^T; T = Vt W                        (GEMM tiles, all blocks)
+// and then, per block, either
+//   warm refinement (v2b_refine.cu): accept T when its remaining couplings
+//     leave the first-order formula P = Gamma o T exact to the tolerances;
+//     else diagonalise the non-separable clusters exactly, take one Newton
+//     step for the separable pairs, re-orthonormalise and recompute T (up to
+//     kRefinePasses times), or
+//   selective Jacobi on T (blocks below kRefineMinDim, the first call after a
+//   reset, and blocks the refinement hands over):
 //     blocks <= kJacobiMaxDim  jacobi_warm_kernel (one CTA, T in shared memory)
 //     larger blocks            jacobi_big_kernel  (one 8-CTA cluster, T in L2)
-//   Y = Vt^T P; U+ = Y Vt -> x = U+/mu, z = U+ - Us.        (GEMM tiles)
+// and finally Y = Vt^T P; U+ = Y Vt -> x = U+/mu, z = U+ - Us.   (GEMM tiles)
 // Every kReorthEvery calls Vt is re-orthonormalised, Vt <- Vt + (I - Vt Vt^T) Vt / 2.
 struct ProjectPlan {
     static constexpr int kReorthEvery = 64;
     std::vector<int> dims;
+    std::vector<int64_t> h_off;
+    std::vector<int64_t> h_roff_small, h_roff_big;   // per block, -1 if not of that kind
     int nblk = 0, nsmall = 0, nbig = 0;
-    int64_t total = 0;
-    int64_t *boff = nullptr, *rot_off = nullptr, *boff_s = nullptr, *boff_b = nullptr;
-    int *bdim = nullptr, *bdim_s = nullptr, *bdim_b = nullptr, *counters = nullptr;
+    int64_t total = 0, rows_total = 0;
+    int64_t *boff = nullptr, *rot_off = nullptr;
+    int *bdim = nullptr, *counters = nullptr;
     int4 *tiles = nullptr;
     int ntiles = 0;
     double2 *rot = nullptr;
     double *Vt = nullptr, *Vt2 = nullptr, *Us = nullptr, *W = nullptr, *T = nullptr, *P = nullptr;
     // large-block work arrays
     static constexpr int kBigSweeps = 16;
-    int64_t *roff_b = nullptr;
     double *norm_b = nullptr;
     double2 *rec_b = nullptr;
     int max_big = 0;
     size_t smem = 0;
     int max_sweeps = 30;
+    // Jacobi block lists of one call (subsets), device copies and pinned staging
+    int64_t *sub_boff = nullptr, *sub_roff = nullptr;
+    int *sub_bdim = nullptr;
+    int64_t *h_sub = nullptr;   // pinned: 3 x nblk int64 (boff, roff, bdim) for small then big
+    // refinement state
+    int *bstate = nullptr, *h_bstate_up = nullptr;   // device / pinned staging
+    unsigned long long *orth = nullptr;
+    double *bnorm = nullptr;
+    double *Vsave = nullptr, *Tsave = nullptr;   // the call's starting basis and T
+    int *h_state = nullptr, *h_nbad = nullptr, *h_nedge = nullptr;   // mapped host memory
+    int2 *h_edges = nullptr;
+    int *d_state = nullptr, *d_nbad = nullptr, *d_nedge = nullptr;   // their device aliases
+    int2 *d_edges = nullptr;
+    v2b::ClusterJob *jobs = nullptr;
+    int *mem = nullptr, *rowclus = nullptr, *rowbase = nullptr;
+    double *Qt = nullptr, *lam = nullptr;
+    unsigned char *h_clus = nullptr;   // pinned staging: jobs, mem, rowclus
+    size_t clus_bytes = 0;
+    size_t classify_smem = 0;
+    // recorded after a call's last upload from the pinned staging buffers; the
+    // next call waits for it before writing them again
+    cudaEvent_t staged = nullptr;
+    bool staged_pending = false;
+    // host-side counters
+    long refine_accepted = 0, refine_jacobi = 0, refine_passes = 0, refine_clusters = 0;
     bool fresh = true;
     bool built = false;
     long calls = 0, since_reset = 0;
@@ -138,86 +172,125 @@ struct ProjectPlan {
     void build(const std::vector<int> &d) {
         dims = d;
         nblk = (int)d.size();
-        std::vector<int64_t> off(nblk), roff, off_s, off_b, roffb;
-        std::vector<int> dim_s, dim_b;
+        h_off.assign(nblk, 0);
+        h_roff_small.assign(nblk, -1);
+        h_roff_big.assign(nblk, -1);
         std::vector<int4> tl;
-        int64_t o = 0, ro = 0, rb = 0;
+        std::vector<int> rb_host(nblk, 0);
+        int64_t o = 0, ro = 0, rb = 0, rows = 0;
         smem = 0;
+        int maxn = 0;
         for (int i = 0; i < nblk; i++) {
             if (d[i] < 0) throw std::invalid_argument("negative block dimension");
-            off[i] = o;
+            h_off[i] = o;
+            rb_host[i] = (int)rows;
+            rows += d[i];
+            maxn = std::max(maxn, d[i]);
             const int nt = (d[i] + v2b::kGemmTile - 1) / v2b::kGemmTile;
             for (int a = 0; a < nt; a++)
                 for (int b = 0; b < nt; b++) tl.push_back(make_int4(i, a, b, 0));
             if (d[i] <= v2b::kJacobiMaxDim) {
                 const int np = d[i] + (d[i] & 1);
-                off_s.push_back(o);
-                dim_s.push_back(d[i]);
-                roff.push_back(ro);
+                h_roff_small[i] = ro;
+                nsmall++;
                 // rotation record (max_sweeps x steps x pairs) + per-step counts
                 ro += (int64_t)max_sweeps * std::max(np - 1, 0) * (np / 2) +
                       ((int64_t)max_sweeps * std::max(np - 1, 0) + 3) / 4 + 1;
                 smem = std::max(smem, v2b::jacobi_smem_bytes(d[i]));
             } else {
-                off_b.push_back(o);
-                dim_b.push_back(d[i]);
-                roffb.push_back(rb);
+                h_roff_big[i] = rb;
+                nbig++;
                 rb += v2b::big_record_slots(d[i], kBigSweeps);
                 max_big = std::max(max_big, d[i]);
             }
             o += (int64_t)d[i] * d[i];
         }
         total = o;
-        nsmall = (int)dim_s.size();
-        nbig = (int)dim_b.size();
+        rows_total = rows;
         ntiles = (int)tl.size();
         boff = dalloc<int64_t>(nblk);
         bdim = dalloc<int>(nblk);
         counters = dalloc<int>(4);
         tiles = dalloc<int4>(std::max(ntiles, 1));
         for (double **b : {&Vt, &Vt2, &Us, &W, &T, &P}) *b = dalloc<double>(total);
-        V2B_CK(cudaMemcpy(boff, off.data(), nblk * 8, cudaMemcpyHostToDevice));
+        V2B_CK(cudaMemcpy(boff, h_off.data(), nblk * 8, cudaMemcpyHostToDevice));
         V2B_CK(cudaMemcpy(bdim, d.data(), nblk * 4, cudaMemcpyHostToDevice));
         V2B_CK(cudaMemset(counters, 0, 16));
         if (ntiles) V2B_CK(cudaMemcpy(tiles, tl.data(), ntiles * sizeof(int4), cudaMemcpyHostToDevice));
-        if (nsmall) {
-            boff_s = dalloc<int64_t>(nsmall);
-            bdim_s = dalloc<int>(nsmall);
-            rot_off = dalloc<int64_t>(nsmall);
-            rot = dalloc<double2>(ro);
-            V2B_CK(cudaMemcpy(boff_s, off_s.data(), nsmall * 8, cudaMemcpyHostToDevice));
-            V2B_CK(cudaMemcpy(bdim_s, dim_s.data(), nsmall * 4, cudaMemcpyHostToDevice));
-            V2B_CK(cudaMemcpy(rot_off, roff.data(), nsmall * 8, cudaMemcpyHostToDevice));
-        }
+        if (nsmall) rot = dalloc<double2>(ro);
         if (smem)
             V2B_CK(cudaFuncSetAttribute(v2b::jacobi_warm_kernel,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         if (nbig) {
-            boff_b = dalloc<int64_t>(nbig);
-            bdim_b = dalloc<int>(nbig);
-            roff_b = dalloc<int64_t>(nbig);
             rec_b = dalloc<double2>(rb);
             norm_b = dalloc<double>((size_t)nbig * v2b::kBigCluster);
-            V2B_CK(cudaMemcpy(boff_b, off_b.data(), nbig * 8, cudaMemcpyHostToDevice));
-            V2B_CK(cudaMemcpy(bdim_b, dim_b.data(), nbig * 4, cudaMemcpyHostToDevice));
-            V2B_CK(cudaMemcpy(roff_b, roffb.data(), nbig * 8, cudaMemcpyHostToDevice));
         }
+        sub_boff = dalloc<int64_t>(nblk);
+        sub_roff = dalloc<int64_t>(nblk);
+        sub_bdim = dalloc<int>(nblk);
+        V2B_CK(cudaMallocHost(&h_sub, std::max(nblk, 1) * 3 * sizeof(int64_t)));
+        // refinement
+        bstate = dalloc<int>(nblk);
+        orth = dalloc<unsigned long long>(nblk);
+        bnorm = dalloc<double>(nblk);
+        Vsave = dalloc<double>(total);
+        Tsave = dalloc<double>(total);
+        V2B_CK(cudaMallocHost(&h_bstate_up, std::max(nblk, 1) * sizeof(int)));
+        V2B_CK(cudaHostAlloc(&h_state, std::max(nblk, 1) * 3 * sizeof(int), cudaHostAllocMapped));
+        h_nbad = h_state + nblk;
+        h_nedge = h_nbad + nblk;
+        V2B_CK(cudaHostAlloc(&h_edges, std::max<size_t>(nblk, 1) * v2b::kRefineEdgeCap * sizeof(int2),
+                             cudaHostAllocMapped));
+        V2B_CK(cudaHostGetDevicePointer((void **)&d_state, h_state, 0));
+        d_nbad = d_state + nblk;
+        d_nedge = d_nbad + nblk;
+        V2B_CK(cudaHostGetDevicePointer((void **)&d_edges, h_edges, 0));
+        const int64_t max_jobs = std::max<int64_t>(rows_total / 2, 1);
+        jobs = dalloc<v2b::ClusterJob>(max_jobs);
+        mem = dalloc<int>(rows_total);
+        rowclus = dalloc<int>(rows_total);
+        rowbase = dalloc<int>(nblk);
+        lam = dalloc<double>(rows_total);
+        Qt = dalloc<double>((size_t)rows_total * v2b::kRefineMaxCluster);
+        V2B_CK(cudaMemcpy(rowbase, rb_host.data(), nblk * 4, cudaMemcpyHostToDevice));
+        clus_bytes = max_jobs * sizeof(v2b::ClusterJob) + 2 * rows_total * sizeof(int);
+        V2B_CK(cudaMallocHost(&h_clus, std::max<size_t>(clus_bytes, 16)));
+        classify_smem = (size_t)maxn * sizeof(double);
+        if (classify_smem > 48 * 1024)
+            V2B_CK(cudaFuncSetAttribute(v2b::refine_classify_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)classify_smem));
+        const int kc = v2b::kRefineMaxCluster;
+        V2B_CK(cudaFuncSetAttribute(v2b::cluster_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(2 * kc * (kc + 1) * sizeof(double))));
+        V2B_CK(cudaFuncSetAttribute(v2b::cluster_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)((kc * kc + 64 * kc) * sizeof(double))));
+        V2B_CK(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
         fresh = true;
         built = true;
     }
     void release() {
         if (!built) return;
+        if (staged) cudaEventDestroy(staged);
+        staged = nullptr;
+        staged_pending = false;
         for (void *q : {(void *)boff, (void *)rot_off, (void *)bdim, (void *)counters, (void *)tiles,
                         (void *)rot, (void *)Vt, (void *)Vt2, (void *)Us, (void *)W, (void *)T,
-                        (void *)P, (void *)boff_s, (void *)bdim_s, (void *)boff_b, (void *)bdim_b,
-                        (void *)roff_b, (void *)rec_b, (void *)norm_b})
+                        (void *)P, (void *)rec_b, (void *)norm_b, (void *)sub_boff, (void *)sub_roff,
+                        (void *)sub_bdim, (void *)bstate, (void *)orth, (void *)bnorm, (void *)Vsave,
+                        (void *)Tsave, (void *)jobs, (void *)mem,
+                        (void *)rowclus, (void *)rowbase, (void *)lam, (void *)Qt})
             cudaFree(q);
+        for (void *q : {(void *)h_sub, (void *)h_bstate_up, (void *)h_state, (void *)h_edges,
+                        (void *)h_clus})
+            if (q) cudaFreeHost(q);
         built = false;
     }
 
     void gemm(v2b::GemmVariant v, const double *A, const double *B, double *C, const double *Cin,
-              double inv_mu, double *x, double *z, cudaStream_t s, long &launches) {
-        V2B_CK(v2b::launch_gemm_tiles(v, ntiles, s, A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, x, z));
+              double inv_mu, double *x, double *z, cudaStream_t s, long &launches,
+              const int *only_work = nullptr) {
+        V2B_CK(v2b::launch_gemm_tiles(v, ntiles, s, A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, x, z,
+                                      only_work, orth));
         launches++;
     }
 
@@ -228,9 +301,202 @@ struct ProjectPlan {
         since_reset = 0;
     }
 
+    // connected components of one block's recorded non-separable pairs;
+    // returns false when a component exceeds kRefineMaxCluster rows
+    bool clusters_of(int b, std::vector<std::vector<int>> &out) const {
+        const int n = dims[b];
+        const int ne = h_nedge[b];
+        std::vector<int> parent(n);
+        for (int i = 0; i < n; i++) parent[i] = i;
+        auto find = [&](int a) {
+            while (parent[a] != a) {
+                parent[a] = parent[parent[a]];
+                a = parent[a];
+            }
+            return a;
+        };
+        const volatile int2 *eb = h_edges + (int64_t)b * v2b::kRefineEdgeCap;
+        std::vector<char> touched(n, 0);
+        for (int e = 0; e < ne; e++) {
+            const int i = eb[e].x, j = eb[e].y;
+            if (i < 0 || j < 0 || i >= n || j >= n) throw Failure(V2B_INTERNAL, "bad cluster edge");
+            touched[i] = touched[j] = 1;
+            const int ri = find(i), rj = find(j);
+            if (ri != rj) parent[std::max(ri, rj)] = std::min(ri, rj);
+        }
+        std::vector<int> id(n, -1);
+        for (int i = 0; i < n; i++) {
+            if (!touched[i]) continue;
+            const int r = find(i);
+            if (id[r] < 0) {
+                id[r] = (int)out.size();
+                out.emplace_back();
+            }
+            out[id[r]].push_back(i);   // ascending: rows are visited in order
+        }
+        for (const auto &c : out)
+            if ((int)c.size() > v2b::kRefineMaxCluster) return false;
+        return true;
+    }
+
+    void upload_states(cudaStream_t s, const std::vector<int> &st) {
+        std::copy(st.begin(), st.end(), h_bstate_up);
+        V2B_CK(cudaMemcpyAsync(bstate, h_bstate_up, nblk * sizeof(int), cudaMemcpyHostToDevice, s));
+    }
+
+    // the refinement passes; returns per-block final states (Done or Jacobi).
+    // A block handed to Jacobi after its basis was changed restarts from the
+    // call's saved basis and T, so the Jacobi kernels always see an
+    // orthonormal Vt.
+    void refine(std::vector<int> &st, cudaStream_t s, long &launches) {
+        using namespace v2b;
+        bool any = false;
+        for (int b = 0; b < nblk; b++) any = any || st[b] == kStWork;
+        if (!any) return;
+        V2B_CK(cudaMemsetAsync(orth, 0, nblk * sizeof(unsigned long long), s));
+        V2B_CK(cudaMemcpyAsync(Vsave, Vt, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        V2B_CK(cudaMemcpyAsync(Tsave, T, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        std::vector<char> changed(nblk, 0);
+        auto restore = [&](int b) {
+            if (!changed[b]) return;
+            const size_t bytes = (size_t)dims[b] * dims[b] * sizeof(double);
+            V2B_CK(cudaMemcpyAsync(Vt + h_off[b], Vsave + h_off[b], bytes, cudaMemcpyDeviceToDevice, s));
+            V2B_CK(cudaMemcpyAsync(T + h_off[b], Tsave + h_off[b], bytes, cudaMemcpyDeviceToDevice, s));
+            changed[b] = 0;
+        };
+        for (int pass = 0; pass <= kRefinePasses; pass++) {
+            if (pass > 0) {
+                gemm(kGemmNTStore, Us, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
+                gemm(kGemmNNStore, Vt, W, T, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
+            }
+            refine_classify_kernel<<<nblk, kRefineThreads, classify_smem, s>>>(
+                T, P, boff, bdim, bstate, orth, pass == kRefinePasses ? 1 : 0, gap_tol, abs_tol, bnorm,
+                d_state, d_nbad, d_nedge, d_edges);
+            V2B_CK(cudaGetLastError());
+            launches++;
+            V2B_CK(cudaStreamSynchronize(s));
+            refine_passes++;
+            // clusters of the blocks still in work
+            std::vector<ClusterJob> jl;
+            std::vector<int> ml;
+            std::vector<int> rc((size_t)rows_total, -1);
+            int64_t qoff = 0;
+            int nwork = 0;
+            for (int b = 0; b < nblk; b++) {
+                if (st[b] != kStWork) continue;
+                st[b] = h_state[b];
+                if (st[b] == kStDone) refine_accepted++;
+                if (st[b] == kStJacobi) restore(b);
+                if (st[b] != kStWork) continue;
+                std::vector<std::vector<int>> cl;
+                if (h_nedge[b] > kRefineEdgeCap || !clusters_of(b, cl)) {
+                    st[b] = kStJacobi;
+                    restore(b);
+                    continue;
+                }
+                changed[b] = 1;
+                nwork++;
+                int64_t base = 0;
+                for (int q = 0; q < b; q++) base += dims[q];
+                for (const auto &c : cl) {
+                    ClusterJob j;
+                    j.blk = b;
+                    j.k = (int)c.size();
+                    j.moff = (int)ml.size();
+                    j.qoff = (int)qoff;
+                    qoff += (int64_t)j.k * j.k;
+                    for (int r : c) {
+                        rc[base + r] = (int)jl.size();
+                        ml.push_back(r);
+                    }
+                    jl.push_back(j);
+                }
+            }
+            if (nwork == 0) break;
+            upload_states(s, st);
+            refine_clusters += (long)jl.size();
+            if (!jl.empty()) {
+                const int nj = (int)jl.size();
+                unsigned char *hp = h_clus;
+                const size_t jb = nj * sizeof(ClusterJob), mb = ml.size() * sizeof(int),
+                             rb = rc.size() * sizeof(int);
+                std::memcpy(hp, jl.data(), jb);
+                std::memcpy(hp + jb, ml.data(), mb);
+                std::memcpy(hp + jb + mb, rc.data(), rb);
+                V2B_CK(cudaMemcpyAsync(jobs, hp, jb, cudaMemcpyHostToDevice, s));
+                V2B_CK(cudaMemcpyAsync(mem, hp + jb, mb, cudaMemcpyHostToDevice, s));
+                V2B_CK(cudaMemcpyAsync(rowclus, hp + jb + mb, rb, cudaMemcpyHostToDevice, s));
+                const int kc = kRefineMaxCluster;
+                const int maxn = *std::max_element(dims.begin(), dims.end());
+                cluster_eig_kernel<<<nj, 256, 2 * kc * (kc + 1) * sizeof(double), s>>>(
+                    T, boff, bdim, jobs, mem, Qt, lam);
+                cluster_rows_kernel<<<dim3(nj, (maxn + 63) / 64), 256, (kc * kc + 64 * kc) * sizeof(double),
+                                      s>>>(T, Vt, W, Vt2, boff, bdim, jobs, mem, Qt);
+                cluster_cols_kernel<<<dim3(nj, (maxn + 31) / 32), 256, (kc * kc + 32 * kc) * sizeof(double),
+                                      s>>>(T, W, boff, bdim, jobs, mem, rowclus, rowbase, Qt, lam);
+                cluster_commit_kernel<<<dim3(nj, (maxn + 63) / 64), 256, 0, s>>>(
+                    T, W, Vt, Vt2, boff, bdim, jobs, mem, rowclus, rowbase);
+                V2B_CK(cudaGetLastError());
+                launches += 4;
+            }
+            newton_m_kernel<<<ntiles, 256, 0, s>>>(T, W, tiles, boff, bdim, bstate, bnorm, gap_tol, abs_tol);
+            V2B_CK(cudaGetLastError());
+            launches++;
+            V2B_CK(cudaMemsetAsync(orth, 0, nblk * sizeof(unsigned long long), s));
+            gemm(kGemmNNStore, W, Vt, Vt2, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
+            gemm(kGemmNTNewtonSchulz, Vt2, Vt2, W, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
+            gemm(kGemmNNStore, W, Vt2, Vt, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
+        }
+    }
+
+    // selective Jacobi on the blocks in state kStJacobi
+    void jacobi(const std::vector<int> &st, cudaStream_t s, long &launches) {
+        using namespace v2b;
+        int ns = 0, nb = 0;
+        int64_t *hb = h_sub, *hr = h_sub + nblk, *hd = h_sub + 2 * nblk;
+        for (int pass = 0; pass < 2; pass++)
+            for (int b = 0; b < nblk; b++) {
+                if (st[b] != kStJacobi) continue;
+                const bool small = h_roff_small[b] >= 0;
+                if ((pass == 0) != small) continue;
+                const int k = ns + nb;
+                hb[k] = h_off[b];
+                hr[k] = small ? h_roff_small[b] : h_roff_big[b];
+                hd[k] = dims[b];
+                (small ? ns : nb)++;
+            }
+        const int m = ns + nb;
+        if (m == 0) return;
+        refine_jacobi += m;
+        std::vector<int> dd(m);
+        for (int k = 0; k < m; k++) dd[k] = (int)hd[k];
+        std::memcpy(hd, dd.data(), m * sizeof(int));
+        V2B_CK(cudaMemcpyAsync(sub_boff, hb, m * 8, cudaMemcpyHostToDevice, s));
+        V2B_CK(cudaMemcpyAsync(sub_roff, hr, m * 8, cudaMemcpyHostToDevice, s));
+        V2B_CK(cudaMemcpyAsync(sub_bdim, hd, m * 4, cudaMemcpyHostToDevice, s));
+        if (ns) {
+            jacobi_warm_kernel<<<ns, kJacobiThreads, smem, s>>>(T, P, Vt, sub_boff, sub_bdim, rot, sub_roff,
+                                                                max_sweeps, abs_tol, gap_tol, counters,
+                                                                counters + 1);
+            V2B_CK(cudaGetLastError());
+            launches++;
+        }
+        if (nb) {
+            BigJacobiArgs a;
+            a.T = T; a.P = P; a.Vt = Vt; a.boff = sub_boff + ns; a.bdim = sub_bdim + ns;
+            a.rot = rec_b; a.roff = sub_roff + ns; a.max_sweeps = kBigSweeps; a.norm_part = norm_b;
+            a.abs_tol = abs_tol; a.gap_tol = gap_tol; a.counters = counters + 2;
+            const size_t alist_bytes = (size_t)((max_big + 1) / 2 + 1) * sizeof(int);
+            jacobi_big_kernel<<<nb * kBigCluster, kBigThreads, alist_bytes, s>>>(a);
+            V2B_CK(cudaGetLastError());
+            launches++;
+        }
+    }
+
     void project(const double *U, double mu, double *x, double *z, cudaStream_t s, long &launches) {
         using namespace v2b;
         if (nblk == 0 || ntiles == 0) return;
+        const bool cold = fresh;
         if (fresh) {
             identity_blocks_kernel<<<nblk, 256, 0, s>>>(Vt, boff, bdim);
             V2B_CK(cudaGetLastError());
@@ -249,23 +515,16 @@ struct ProjectPlan {
         launches++;
         gemm(kGemmNTStore, Us, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches);
         gemm(kGemmNNStore, Vt, W, T, nullptr, 0.0, nullptr, nullptr, s, launches);
-        if (nsmall) {
-            jacobi_warm_kernel<<<nsmall, kJacobiThreads, smem, s>>>(T, P, Vt, boff_s, bdim_s, rot,
-                                                                    rot_off, max_sweeps, abs_tol,
-                                                                    gap_tol, counters, counters + 1);
-            V2B_CK(cudaGetLastError());
-            launches++;
-        }
-        if (nbig) {
-            BigJacobiArgs a;
-            a.T = T; a.P = P; a.Vt = Vt; a.boff = boff_b; a.bdim = bdim_b;
-            a.rot = rec_b; a.roff = roff_b; a.max_sweeps = kBigSweeps; a.norm_part = norm_b;
-            a.abs_tol = abs_tol; a.gap_tol = gap_tol; a.counters = counters + 2;
-            const size_t alist_bytes = (size_t)((max_big + 1) / 2 + 1) * sizeof(int);
-            jacobi_big_kernel<<<nbig * kBigCluster, kBigThreads, alist_bytes, s>>>(a);
-            V2B_CK(cudaGetLastError());
-            launches++;
-        }
+        std::vector<int> st(nblk);
+        for (int b = 0; b < nblk; b++)
+            st[b] = dims[b] == 0 ? kStDone
+                    : (cold || dims[b] < kRefineMinDim) ? kStJacobi : kStWork;
+        if (staged_pending) V2B_CK(cudaEventSynchronize(staged));
+        upload_states(s, st);
+        refine(st, s, launches);
+        jacobi(st, s, launches);
+        V2B_CK(cudaEventRecord(staged, s));
+        staged_pending = true;
         gemm(kGemmTNStore, Vt, P, W, nullptr, 0.0, nullptr, nullptr, s, launches);
         gemm(kGemmNNProject, W, Vt, nullptr, nullptr, 1.0 / mu, x, z, s, launches);
     }
@@ -776,6 +1035,17 @@ int v2b_problem_project(v2b_problem *p, const double *d_U, double mu, double *d_
         return V2B_OK;
     });
 }
+int v2b_problem_project_warm(v2b_problem *p, const double *d_U, double mu, double *d_x, double *d_z,
+                             void *stream) {
+    return guarded([&] {
+        if (!p || !d_U || !d_x || !d_z || !(mu > 0.0))
+            throw std::invalid_argument("project_warm: bad argument");
+        p->setup();
+        p->ensure_plan();
+        p->plan.project(d_U, mu, d_x, d_z, (cudaStream_t)stream, p->launches);
+        return V2B_OK;
+    });
+}
 int v2b_problem_solve_device(v2b_problem *p, double *d_x, const double *d_b, const double *d_c,
                              const v2b_sdp_options *options, int mu_update_frequency,
                              v2b_sdp_monitor monitor, int print_level, void *data, long *oiter,
@@ -875,6 +1145,19 @@ int v2b_problem_projection_counts(const v2b_problem *p, long *calls, long *rotat
         if (p->plan.built) V2B_CK(cudaMemcpy(h, p->plan.counters, 16, cudaMemcpyDeviceToHost));
         *rotations = (long)h[1] + h[3];
         *sweep_overruns = (long)h[0] + h[2];
+        return V2B_OK;
+    });
+}
+
+int v2b_problem_refine_counts(const v2b_problem *p, long *accepted, long *jacobi, long *passes,
+                              long *clusters) {
+    return guarded([&] {
+        if (!p || !accepted || !jacobi || !passes || !clusters)
+            throw std::invalid_argument("refine_counts: NULL argument");
+        *accepted = p->plan.refine_accepted;
+        *jacobi = p->plan.refine_jacobi;
+        *passes = p->plan.refine_passes;
+        *clusters = p->plan.refine_clusters;
         return V2B_OK;
     });
 }

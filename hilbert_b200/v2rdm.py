@@ -166,13 +166,16 @@ class V2RDMProblem:
         check(self._lib.v2b_problem_ATu(self._h, _tptr(y), _tptr(out), self._stream()))
         return out
 
-    def project(self, U, mu):
+    def project(self, U, mu, warm=False):
+        """x = U+ / mu, z = U+ - sym(U) per PSD block.  warm=True starts each block
+        from the eigenvector basis the previous warm projection (or device solve)
+        left, as the solver's iterations do; the default solves every block afresh."""
         import torch
         self._check_tensor(U, self.n_primal)
         x = torch.empty_like(U)
         z = torch.empty_like(U)
-        check(self._lib.v2b_problem_project(self._h, _tptr(U), float(mu), _tptr(x), _tptr(z),
-                                            self._stream()))
+        fn = self._lib.v2b_problem_project_warm if warm else self._lib.v2b_problem_project
+        check(fn(self._h, _tptr(U), float(mu), _tptr(x), _tptr(z), self._stream()))
         return x, z
 
     def solve(self, x0, b, c, options, monitor=None):
@@ -242,6 +245,12 @@ class V2RDMProblem:
         check(self._lib.v2b_problem_projection_counts(self._h, ctypes.byref(w), ctypes.byref(r),
                                                       ctypes.byref(c)))
         return {"calls": w.value, "rotations": r.value, "sweep_overruns": c.value}
+
+    def refine_counts(self):
+        """{"accepted", "jacobi", "passes", "clusters"} of the warm eigen-refinement"""
+        v = [ctypes.c_long() for _ in range(4)]
+        check(self._lib.v2b_problem_refine_counts(self._h, *[ctypes.byref(x) for x in v]))
+        return dict(zip(("accepted", "jacobi", "passes", "clusters"), (x.value for x in v)))
 
     def stream_handle(self):
         return self._lib.v2b_problem_stream(self._h)

@@ -126,6 +126,12 @@ int v2b_problem_ATu(v2b_problem *p, const double *d_in, double *d_out, void *str
  * one block per entry of the problem's block_dims. */
 int v2b_problem_project(v2b_problem *p, const double *d_U, double mu, double *d_x, double *d_z,
                         void *stream);
+/* No counterpart in the reference.  Like v2b_problem_project, but each block
+ * starts from the eigenvector basis that the previous warm projection or
+ * device solve of this problem left (the identity after creation or after a
+ * v2b_problem_project call), as every iteration of the device solve does. */
+int v2b_problem_project_warm(v2b_problem *p, const double *d_U, double mu, double *d_x, double *d_z,
+                             void *stream);
 /* Runs the outer protocol of v2RDMSolver::compute_energy for Hubbard /
  * external Hamiltonians (v2rdm_solver.cc:1296-1361): repeated solve() calls
  * of mu_update_frequency iterations, mu <- mu*eps_p/eps_d between calls,
@@ -167,6 +173,13 @@ void *v2b_problem_stream(const v2b_problem *p);
  * applied, and blocks whose Jacobi sweeps hit the sweep cap */
 int v2b_problem_projection_counts(const v2b_problem *p, long *calls, long *rotations,
                                   long *sweep_overruns);
+/* No counterpart in the reference (libsdp diagonalises every block with LAPACK
+ * each iteration).  Warm refinement of the projection since the problem was
+ * created: blocks accepted without Jacobi, blocks handed to the Jacobi
+ * kernels, acceptance tests run (one per pass and call), clusters
+ * diagonalised exactly. */
+int v2b_problem_refine_counts(const v2b_problem *p, long *accepted, long *jacobi, long *passes,
+                              long *clusters);
 
 /* ---- 3. allocation-free projection ------------------------------------------ */
 

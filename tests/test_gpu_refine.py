@@ -1,0 +1,72 @@
+"""Warm eigen-refinement of the PSD projection on the B200 against numpy's
+LAPACK eigendecomposition, over sequences of slowly changing blocks whose
+spectra hold the hard cases: degenerate same-sign clusters, eigenvalues near
+zero of both signs, exact zeros."""
+import numpy as np
+import pytest
+
+import hilbert_b200 as hb
+from oracle.bpsdp import project_blocks
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-11   # |x - x_ref|_max <= TOL * max(1, |U|_F)
+
+
+def hard_spectrum(d, rng):
+    lam = rng.uniform(-3.0, 3.0, d)
+    if d < 24:   # blocks this small always take the Jacobi kernels
+        return lam
+    k = d // 8
+    lam[:k] = 1.0 + 1e-9 * rng.standard_normal(k)                 # degenerate, positive
+    lam[k:2 * k] = -0.5 + 1e-10 * rng.standard_normal(k)          # degenerate, negative
+    lam[2 * k:3 * k] = 1e-10 * rng.standard_normal(k)             # near zero, both signs
+    lam[3 * k] = 0.0
+    return lam
+
+
+def drift(q, rng, step):
+    a = rng.standard_normal(q.shape) * step
+    a = a - a.T
+    r, _ = np.linalg.qr(np.eye(len(q)) + a)
+    return q @ (r * np.sign(np.diag(r)))
+
+
+@pytest.mark.parametrize("n,steps,step", [(6, 12, 1e-4), (10, 8, 1e-4), (10, 6, 3e-3)])
+def test_warm_projection_sequence(cuda_device, n, steps, step):
+    import torch
+    p = hb.V2RDMProblem(n, n // 2, n // 2)
+    rng = np.random.default_rng(100 + n)
+    qs = [np.linalg.qr(rng.standard_normal((d, d)))[0] for d in p.dims]
+    ls = [hard_spectrum(d, rng) for d in p.dims]
+    mu = 0.7
+    for it in range(steps):
+        U = np.concatenate([((q * l) @ q.T).ravel() for q, l in zip(qs, ls)])
+        x, z = p.project(torch.from_numpy(U).to(cuda_device), mu, warm=True)
+        xr, zr = project_blocks(U, p.dims, mu)
+        scale = max(1.0, np.linalg.norm(U))
+        ex = np.max(np.abs(x.cpu().numpy() - xr))
+        ez = np.max(np.abs(z.cpu().numpy() - zr))
+        assert ex <= TOL * scale and ez <= TOL * scale, (it, ex, ez, scale)
+        qs = [drift(q, rng, step) for q in qs]
+        ls = [l + 1e-6 * rng.standard_normal(len(l)) for l in ls]
+    rc = p.refine_counts()
+    # blocks of at least 24 rows are refined after the first (cold) call
+    assert rc["accepted"] > 0, rc
+    assert rc["passes"] > 0, rc
+
+
+def test_cold_projection_resets_warm_basis(cuda_device):
+    """A stand-alone projection between warm ones leaves the next warm call cold
+    (identity basis) and both stay exact."""
+    import torch
+    p = hb.V2RDMProblem(6, 3, 3)
+    rng = np.random.default_rng(7)
+    U = rng.standard_normal(p.n_primal)
+    for warm in (True, True, False, True):
+        x, z = p.project(torch.from_numpy(U).to(cuda_device), 0.4, warm=warm)
+        xr, zr = project_blocks(U, p.dims, 0.4)
+        scale = max(1.0, np.linalg.norm(U))
+        assert np.max(np.abs(x.cpu().numpy() - xr)) <= TOL * scale
+        assert np.max(np.abs(z.cpu().numpy() - zr)) <= TOL * scale
+        U = U + 1e-5 * rng.standard_normal(p.n_primal)
