@@ -120,7 +120,7 @@ def load(path=LIB_PATH):
         "v2b_problem_profile": (ctypes.c_int, [vp, dp, lp]),
         "v2b_problem_stream": (ctypes.c_void_p, [vp]),
         "v2b_problem_projection_counts": (ctypes.c_int, [vp, lp, lp, lp]),
-        "v2b_problem_refine_counts": (ctypes.c_int, [vp, lp, lp, lp, lp]),
+        "v2b_problem_refine_counts": (ctypes.c_int, [vp, lp, ctypes.c_int]),
         "v2b_project_block_noalloc": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, vp, vp, vp]),
         "v2b_problem_operator_size": (ctypes.c_int, [vp, ctypes.c_int, lp, lp, ip]),
         "v2b_problem_operator": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint32),

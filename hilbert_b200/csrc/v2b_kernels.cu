@@ -256,6 +256,7 @@ __global__ void stats_kernel(const double *__restrict__ Ax, const double *__rest
 // Sweeps repeat until a sweep rotates nothing.  The kernel then writes the
 // middle factor of U+ = V P V^T,
 //     P_ii = max(t_ii, 0),   P_ij = t_ij (t_ii+ - t_jj+) / (t_ii - t_jj)   (i != j),
+// (with raw != 0: the rotated T itself, for callers that want eigenvalues)
 // and replays the recorded rotations on Vt (rows p, q of Vt per rotation),
 // leaving the refined eigenvectors for the next iteration.
 __global__ void __launch_bounds__(kJacobiThreads)
@@ -263,7 +264,7 @@ __global__ void __launch_bounds__(kJacobiThreads)
                        double *__restrict__ Vt, const int64_t *__restrict__ boff,
                        const int *__restrict__ bdim, double2 *__restrict__ rot,
                        const int64_t *__restrict__ rot_off, int max_sweeps, double abs_tol,
-                       double gap_tol, int *status, int *rot_count) {
+                       double gap_tol, int *status, int *rot_count, int raw) {
     extern __shared__ double sm[];
     const int blk = blockIdx.x;
     const int n = bdim[blk];
@@ -394,7 +395,9 @@ __global__ void __launch_bounds__(kJacobiThreads)
         const int i = e / n, j = e % n;
         const double li = T[i * np + i];
         double pv;
-        if (i == j) {
+        if (raw) {
+            pv = T[i * np + j];   // the rotated matrix itself (its diagonal: the eigenvalues)
+        } else if (i == j) {
             pv = fmax(li, 0.0);
         } else {
             const double lj = T[j * np + j];

@@ -61,7 +61,8 @@ __global__ void jacobi_warm_kernel(const double *__restrict__ T0, double *__rest
                                    double *__restrict__ Vt, const int64_t *__restrict__ boff,
                                    const int *__restrict__ bdim, double2 *__restrict__ rot,
                                    const int64_t *__restrict__ rot_off, int max_sweeps,
-                                   double abs_tol, double gap_tol, int *status, int *rot_count);
+                                   double abs_tol, double gap_tol, int *status, int *rot_count,
+                                   int raw = 0);
 __global__ void identity_blocks_kernel(double *__restrict__ Vt, const int64_t *__restrict__ boff,
                                        const int *__restrict__ bdim);
 __global__ void half_residual_kernel(const double *__restrict__ G, double *__restrict__ H,

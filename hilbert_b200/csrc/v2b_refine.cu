@@ -17,8 +17,11 @@
 // pass refines Vt:
 //   * non-separable failing pairs (|t_pq| > rho |d_p - d_q|) form a graph; its
 //     connected components ("clusters", found on the host from the recorded
-//     edges) are diagonalised exactly (cluster_eig_kernel) and applied to the
-//     cluster rows and columns of T and to the cluster rows of Vt;
+//     edges) are diagonalised exactly -- up to kRefineSmallCluster rows by
+//     cluster_eig_kernel, larger ones gathered into compact matrices for the
+//     selective Jacobi kernels with the gap test off -- and the rotation G
+//     (identity outside the clusters) is applied as T <- G T G^T, Vt <- G Vt
+//     with gathered GEMM tiles;
 //   * every remaining separable failing pair takes one Newton step of the
 //     eigenvector equation, Vt <- (I - K) Vt with K_pq = t_pq / (d_q - d_p),
 //     followed by one Newton-Schulz orthonormalisation
@@ -27,8 +30,8 @@
 //     is large and meaningless (f is linear there) and would only cost
 //     orthogonality;
 // and T is recomputed.  Blocks that still fail after kRefinePasses passes, or
-// whose clusters exceed kRefineMaxCluster rows, fall back to the selective
-// Jacobi kernels, restarted from the basis and T the call began with.
+// record more than kRefineEdgeCap non-separable pairs, fall back to the
+// selective Jacobi kernels, restarted from the basis and T the call began with.
 #include "v2b_kernels.cuh"
 #include "v2b_refine.cuh"
 
@@ -139,7 +142,7 @@ __global__ void __launch_bounds__(256)
     extern __shared__ double sm[];
     double *A = sm;              // kp x ld
     double *Q = A + kp * ld;     // kp x ld, rows = eigenvectors
-    __shared__ double2 cs[kRefineMaxCluster / 2];
+    __shared__ double2 cs[kRefineSmallCluster / 2];
     __shared__ double red[32];
     __shared__ double s_thr;
     __shared__ int s_nrot;
@@ -217,99 +220,199 @@ __global__ void __launch_bounds__(256)
     for (int i = threadIdx.x; i < k; i += blockDim.x) lam[jb.moff + i] = A[i * ld + i];
 }
 
+// Gathered GEMM tiles of the cluster transform G (identity outside the
+// clusters, Qt on each cluster): tile (job, ti, tc) of
+//     W[C_i, c]   = sum_l Qt[i][l] T[C_l, c],   Vt2[C_i, c] = sum_l Qt[i][l] Vt[C_l, c]
+// for i in [32 ti, 32 ti + 32), c in [64 tc, 64 tc + 64).
 __global__ void __launch_bounds__(256)
     cluster_rows_kernel(const double *__restrict__ T, const double *__restrict__ Vt,
                         double *__restrict__ W, double *__restrict__ Vt2,
                         const int64_t *__restrict__ boff, const int *__restrict__ bdim,
                         const ClusterJob *__restrict__ jobs, const int *__restrict__ mem,
-                        const double *__restrict__ Qt) {
-    const ClusterJob jb = jobs[blockIdx.x];
+                        const double *__restrict__ Qt, const int4 *__restrict__ ctiles) {
+    const int4 ct = ctiles[blockIdx.x];
+    const ClusterJob jb = jobs[ct.x];
     const int k = jb.k, n = bdim[jb.blk];
-    const int c0 = blockIdx.y * 64;
-    if (c0 >= n) return;
+    const int i0 = ct.y * 32, c0 = ct.z * 64;
     const int64_t off = boff[jb.blk];
     const int *C = mem + jb.moff;
-    extern __shared__ double sm[];
-    double *sQ = sm;            // k x k
-    double *S = sQ + k * k;     // k x 64
-    for (int e = threadIdx.x; e < k * k; e += blockDim.x) sQ[e] = Qt[jb.qoff + e];
-    for (int pass = 0; pass < 2; pass++) {
-        const double *src = (pass == 0 ? T : Vt) + off;
-        double *dst = (pass == 0 ? W : Vt2) + off;
-        for (int e = threadIdx.x; e < k * 64; e += blockDim.x) {
-            const int l = e / 64, cc = e % 64;
-            S[e] = (c0 + cc < n) ? src[(int64_t)C[l] * n + c0 + cc] : 0.0;
+    const double *Q = Qt + jb.qoff;
+    __shared__ double sQ[32][17];
+    __shared__ double sT[16][65], sV[16][65];
+    const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+    double aT[2][4] = {}, aV[2][4] = {};
+    for (int l0 = 0; l0 < k; l0 += 16) {
+        for (int e = tid; e < 32 * 16; e += 256) {
+            const int ii = e >> 4, ll = e & 15;
+            const int i = i0 + ii, l = l0 + ll;
+            sQ[ii][ll] = (i < k && l < k) ? Q[(int64_t)i * k + l] : 0.0;
+        }
+        for (int e = tid; e < 16 * 64; e += 256) {
+            const int ll = e >> 6, cc = e & 63;
+            const int l = l0 + ll, c = c0 + cc;
+            double vt = 0.0, vv = 0.0;
+            if (l < k && c < n) {
+                const int64_t idx = off + (int64_t)C[l] * n + c;
+                vt = T[idx];
+                vv = Vt[idx];
+            }
+            sT[ll][cc] = vt;
+            sV[ll][cc] = vv;
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < k * 64; e += blockDim.x) {
-            const int i = e / 64, cc = e % 64;
-            if (c0 + cc >= n) continue;
-            double acc = 0.0;
-            for (int l = 0; l < k; l++) acc = fma(sQ[i * k + l], S[l * 64 + cc], acc);
-            dst[(int64_t)C[i] * n + c0 + cc] = acc;
+#pragma unroll
+        for (int ll = 0; ll < 16; ll++) {
+            const double q0 = sQ[ty * 2][ll], q1 = sQ[ty * 2 + 1][ll];
+#pragma unroll
+            for (int jj = 0; jj < 4; jj++) {
+                const double bt = sT[ll][tx * 4 + jj], bv = sV[ll][tx * 4 + jj];
+                aT[0][jj] = fma(q0, bt, aT[0][jj]);
+                aT[1][jj] = fma(q1, bt, aT[1][jj]);
+                aV[0][jj] = fma(q0, bv, aV[0][jj]);
+                aV[1][jj] = fma(q1, bv, aV[1][jj]);
+            }
         }
         __syncthreads();
     }
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int i = i0 + ty * 2 + r;
+        if (i >= k) continue;
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) {
+            const int c = c0 + tx * 4 + jj;
+            if (c >= n) continue;
+            const int64_t idx = off + (int64_t)C[i] * n + c;
+            W[idx] = aT[r][jj];
+            Vt2[idx] = aV[r][jj];
+        }
+    }
 }
 
+// tile (job, ta, ti): P[a, C_i] = sum_l R(a)[C_l] Qt[i][l] for a in [64 ta, 64 ta + 64),
+// i in [32 ti, 32 ti + 32), with R(a) = W[a, :] on cluster rows (already
+// rotated by their own cluster) and T[a, :] elsewhere; a row of this same
+// cluster gets delta_ai lam_i.  P is free scratch for blocks in refinement.
 __global__ void __launch_bounds__(256)
-    cluster_cols_kernel(double *__restrict__ T, const double *__restrict__ W,
-                        const int64_t *__restrict__ boff, const int *__restrict__ bdim,
-                        const ClusterJob *__restrict__ jobs, const int *__restrict__ mem,
-                        const int *__restrict__ rowclus, const int *__restrict__ rowbase,
-                        const double *__restrict__ Qt, const double *__restrict__ lam) {
-    const int jid = blockIdx.x;
+    cluster_cols_kernel(const double *__restrict__ T, const double *__restrict__ W,
+                        double *__restrict__ P, const int64_t *__restrict__ boff,
+                        const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,
+                        const int *__restrict__ mem, const int *__restrict__ rowclus,
+                        const int *__restrict__ rowbase, const double *__restrict__ Qt,
+                        const double *__restrict__ lam, const int4 *__restrict__ ctiles) {
+    const int4 ct = ctiles[blockIdx.x];
+    const int jid = ct.x;
     const ClusterJob jb = jobs[jid];
     const int k = jb.k, n = bdim[jb.blk];
-    const int r0 = blockIdx.y * 32;
-    if (r0 >= n) return;
+    const int a0 = ct.y * 64, i0 = ct.z * 32;
     const int64_t off = boff[jb.blk];
     const int *C = mem + jb.moff;
     const int *rc = rowclus + rowbase[jb.blk];
-    extern __shared__ double sm[];
-    double *sQ = sm;            // k x k
-    double *S = sQ + k * k;     // 32 x k: R(a)[C_m]
-    for (int e = threadIdx.x; e < k * k; e += blockDim.x) sQ[e] = Qt[jb.qoff + e];
-    for (int e = threadIdx.x; e < 32 * k; e += blockDim.x) {
-        const int a = r0 + e / k, mm = e % k;
-        double v = 0.0;
-        if (a < n) v = (rc[a] >= 0 ? W : T)[off + (int64_t)a * n + C[mm]];
-        S[e] = v;
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < 32 * k; e += blockDim.x) {
-        const int a = r0 + e / k, i = e % k;
-        if (a >= n) continue;
-        double out;
-        if (rc[a] == jid) {
-            out = (a == C[i]) ? lam[jb.moff + i] : 0.0;
-        } else {
-            out = 0.0;
-            for (int mm = 0; mm < k; mm++) out = fma(S[(e / k) * k + mm], sQ[i * k + mm], out);
+    const double *Q = Qt + jb.qoff;
+    __shared__ double sR[64][17];
+    __shared__ double sQ[32][17];
+    const int tid = threadIdx.x, ta = tid >> 3, ti = tid & 7;
+    double acc[2][4] = {};
+    for (int l0 = 0; l0 < k; l0 += 16) {
+        for (int e = tid; e < 64 * 16; e += 256) {
+            const int aa = e >> 4, ll = e & 15;
+            const int a = a0 + aa, l = l0 + ll;
+            double v = 0.0;
+            if (a < n && l < k) v = (rc[a] >= 0 ? W : T)[off + (int64_t)a * n + C[l]];
+            sR[aa][ll] = v;
         }
-        T[off + (int64_t)a * n + C[i]] = out;
+        for (int e = tid; e < 32 * 16; e += 256) {
+            const int ii = e >> 4, ll = e & 15;
+            const int i = i0 + ii, l = l0 + ll;
+            sQ[ii][ll] = (i < k && l < k) ? Q[(int64_t)i * k + l] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ll = 0; ll < 16; ll++) {
+            const double r0 = sR[ta * 2][ll], r1 = sR[ta * 2 + 1][ll];
+#pragma unroll
+            for (int jj = 0; jj < 4; jj++) {
+                const double q = sQ[ti * 4 + jj][ll];
+                acc[0][jj] = fma(r0, q, acc[0][jj]);
+                acc[1][jj] = fma(r1, q, acc[1][jj]);
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int a = a0 + ta * 2 + r;
+        if (a >= n) continue;
+        const bool own = rc[a] == jid;
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) {
+            const int i = i0 + ti * 4 + jj;
+            if (i >= k) continue;
+            const double v = own ? (a == C[i] ? lam[jb.moff + i] : 0.0) : acc[r][jj];
+            P[off + (int64_t)a * n + C[i]] = v;
+        }
     }
 }
 
+// tile (job, t): T[a, C_i] = P[a, C_i] for rows a in [64 t, 64 t + 64), and
+// for columns b in that range outside every cluster T[C_i, b] = W[C_i, b];
+// Vt[C_i, b] = Vt2[C_i, b] for every b in the range.
 __global__ void __launch_bounds__(256)
     cluster_commit_kernel(double *__restrict__ T, const double *__restrict__ W,
-                          double *__restrict__ Vt, const double *__restrict__ Vt2,
-                          const int64_t *__restrict__ boff, const int *__restrict__ bdim,
-                          const ClusterJob *__restrict__ jobs, const int *__restrict__ mem,
-                          const int *__restrict__ rowclus, const int *__restrict__ rowbase) {
-    const ClusterJob jb = jobs[blockIdx.x];
+                          const double *__restrict__ P, double *__restrict__ Vt,
+                          const double *__restrict__ Vt2, const int64_t *__restrict__ boff,
+                          const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,
+                          const int *__restrict__ mem, const int *__restrict__ rowclus,
+                          const int *__restrict__ rowbase, const int4 *__restrict__ ctiles) {
+    const int4 ct = ctiles[blockIdx.x];
+    const ClusterJob jb = jobs[ct.x];
     const int k = jb.k, n = bdim[jb.blk];
-    const int c0 = blockIdx.y * 64;
-    if (c0 >= n) return;
+    const int t0 = ct.y * 64;
     const int64_t off = boff[jb.blk];
     const int *C = mem + jb.moff;
     const int *rc = rowclus + rowbase[jb.blk];
-    for (int e = threadIdx.x; e < k * 64; e += blockDim.x) {
-        const int i = e / 64, b = c0 + e % 64;
-        if (b >= n) continue;
-        const int64_t idx = off + (int64_t)C[i] * n + b;
-        if (rc[b] < 0) T[idx] = W[idx];
-        Vt[idx] = Vt2[idx];
+    for (int e = threadIdx.x; e < 64 * k; e += blockDim.x) {
+        const int i = e / 64, x = t0 + e % 64;
+        if (x >= n) continue;
+        const int64_t col = off + (int64_t)x * n + C[i];   // (row x, cluster column C_i)
+        T[col] = P[col];
+        const int64_t row = off + (int64_t)C[i] * n + x;   // (cluster row C_i, column x)
+        if (rc[x] < 0) T[row] = W[row];
+        Vt[row] = Vt2[row];
+    }
+}
+
+// Tc = sym(T[C, C]) and Vc = I in compact k x k storage at qoff, for clusters
+// diagonalised by the Jacobi kernels (grid: jobs x 16, grid-stride inside)
+__global__ void __launch_bounds__(256)
+    cluster_gather_kernel(const double *__restrict__ T, const int64_t *__restrict__ boff,
+                          const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,
+                          const int *__restrict__ mem, const int *__restrict__ jlist,
+                          double *__restrict__ Tc, double *__restrict__ Vc) {
+    const ClusterJob jb = jobs[jlist[blockIdx.x]];
+    const int k = jb.k, n = bdim[jb.blk];
+    const int *C = mem + jb.moff;
+    const double *Tb = T + boff[jb.blk];
+    const int64_t kk = (int64_t)k * k;
+    for (int64_t e = (int64_t)blockIdx.y * blockDim.x + threadIdx.x; e < kk;
+         e += (int64_t)gridDim.y * blockDim.x) {
+        const int i = (int)(e / k), j = (int)(e % k);
+        const int64_t a = C[i], b = C[j];
+        Tc[jb.qoff + e] = 0.5 * (Tb[a * n + b] + Tb[b * n + a]);
+        Vc[jb.qoff + e] = (i == j) ? 1.0 : 0.0;
+    }
+}
+
+// lam[moff + i] = D[qoff + i k + i]: the eigenvalues left on the diagonal of
+// the rotated compact matrix D by the Jacobi kernels
+__global__ void cluster_lam_kernel(const ClusterJob *__restrict__ jobs, const int *__restrict__ jlist,
+                                   int njobs, const double *__restrict__ Dsmall,
+                                   const double *__restrict__ Dbig, int big_from,
+                                   double *__restrict__ lam) {
+    for (int q = blockIdx.x; q < njobs; q += gridDim.x) {
+        const ClusterJob jb = jobs[jlist[q]];
+        const double *D = (q >= big_from ? Dbig : Dsmall) + jb.qoff;
+        for (int i = threadIdx.x; i < jb.k; i += blockDim.x) lam[jb.moff + i] = D[(int64_t)i * jb.k + i];
     }
 }
 

@@ -13,8 +13,8 @@ constexpr int kStWork = 0;     // refinement passes continue
 constexpr int kStDone = 1;     // T passed the acceptance test; P written
 constexpr int kStJacobi = 2;   // handed to the selective Jacobi kernels
 
-constexpr int kRefineMaxCluster = 64;    // largest cluster diagonalised in place
-constexpr int kRefineEdgeCap = 8192;     // non-separable pairs recorded per block and pass
+constexpr int kRefineSmallCluster = 64;  // clusters up to this size: cluster_eig_kernel
+constexpr int kRefineEdgeCap = 32768;    // non-separable pairs recorded per block and pass
 constexpr int kRefinePasses = 3;         // Newton passes before the Jacobi fallback
 constexpr int kRefineMinDim = 24;        // smaller blocks always take the Jacobi kernel
 constexpr int kRefineThreads = 512;
@@ -44,27 +44,34 @@ __global__ void cluster_eig_kernel(const double *__restrict__ T, const int64_t *
                                    const int *__restrict__ mem, double *__restrict__ Qt,
                                    double *__restrict__ lam);
 
-// new cluster rows: W[C_i, :] = sum_l Qt[i][l] T[C_l, :],  Vt2[C_i, :] = sum_l Qt[i][l] Vt[C_l, :]
+// gathered GEMM tiles of the cluster transform; ctiles = (job, tile row, tile col)
 __global__ void cluster_rows_kernel(const double *__restrict__ T, const double *__restrict__ Vt,
                                     double *__restrict__ W, double *__restrict__ Vt2,
                                     const int64_t *__restrict__ boff, const int *__restrict__ bdim,
                                     const ClusterJob *__restrict__ jobs, const int *__restrict__ mem,
-                                    const double *__restrict__ Qt);
-
-// cluster columns of every row: T[a, C_i] = sum_l R(a)[C_l] Qt[i][l], with
-// R(a) = W[a, :] for cluster rows and T[a, :] otherwise; T[C, C] = diag(lam)
-__global__ void cluster_cols_kernel(double *__restrict__ T, const double *__restrict__ W,
-                                    const int64_t *__restrict__ boff, const int *__restrict__ bdim,
-                                    const ClusterJob *__restrict__ jobs, const int *__restrict__ mem,
-                                    const int *__restrict__ rowclus, const int *__restrict__ rowbase,
-                                    const double *__restrict__ Qt, const double *__restrict__ lam);
-
-// cluster rows outside cluster columns: T[C_i, b] = W[C_i, b]; Vt[C_i, :] = Vt2[C_i, :]
+                                    const double *__restrict__ Qt, const int4 *__restrict__ ctiles);
+__global__ void cluster_cols_kernel(const double *__restrict__ T, const double *__restrict__ W,
+                                    double *__restrict__ P, const int64_t *__restrict__ boff,
+                                    const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,
+                                    const int *__restrict__ mem, const int *__restrict__ rowclus,
+                                    const int *__restrict__ rowbase, const double *__restrict__ Qt,
+                                    const double *__restrict__ lam, const int4 *__restrict__ ctiles);
 __global__ void cluster_commit_kernel(double *__restrict__ T, const double *__restrict__ W,
-                                      double *__restrict__ Vt, const double *__restrict__ Vt2,
-                                      const int64_t *__restrict__ boff, const int *__restrict__ bdim,
-                                      const ClusterJob *__restrict__ jobs, const int *__restrict__ mem,
-                                      const int *__restrict__ rowclus, const int *__restrict__ rowbase);
+                                      const double *__restrict__ P, double *__restrict__ Vt,
+                                      const double *__restrict__ Vt2, const int64_t *__restrict__ boff,
+                                      const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,
+                                      const int *__restrict__ mem, const int *__restrict__ rowclus,
+                                      const int *__restrict__ rowbase, const int4 *__restrict__ ctiles);
+// compact sym(T[C, C]) and identity for the clusters in jlist
+__global__ void cluster_gather_kernel(const double *__restrict__ T, const int64_t *__restrict__ boff,
+                                      const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,
+                                      const int *__restrict__ mem, const int *__restrict__ jlist,
+                                      double *__restrict__ Tc, double *__restrict__ Vc);
+// eigenvalues of Jacobi-diagonalised clusters: jlist[0 .. big_from) read Dsmall, the rest Dbig
+__global__ void cluster_lam_kernel(const ClusterJob *__restrict__ jobs, const int *__restrict__ jlist,
+                                   int njobs, const double *__restrict__ Dsmall,
+                                   const double *__restrict__ Dbig, int big_from,
+                                   double *__restrict__ lam);
 
 // M = I - K, K_pq = t_pq / (d_q - d_p) for separable pairs that fail the
 // acceptance test or whose step is at most kRefineKappa, 0 otherwise (GEMM tile grid)

@@ -152,11 +152,18 @@ struct ProjectPlan {
     int2 *h_edges = nullptr;
     int *d_state = nullptr, *d_nbad = nullptr, *d_nedge = nullptr;   // their device aliases
     int2 *d_edges = nullptr;
-    v2b::ClusterJob *jobs = nullptr;
-    int *mem = nullptr, *rowclus = nullptr, *rowbase = nullptr;
-    double *Qt = nullptr, *lam = nullptr;
-    unsigned char *h_clus = nullptr;   // pinned staging: jobs, mem, rowclus
-    size_t clus_bytes = 0;
+    int *rowbase = nullptr;
+    double *Qt = nullptr, *lam = nullptr;     // cluster eigenvectors (rows) and eigenvalues
+    double *Tc = nullptr, *Pc = nullptr;      // compact clusters for the Jacobi kernels
+    // per-pass cluster lists: one device arena filled from one pinned staging
+    // buffer (jobs, members, row -> cluster, tile lists, Jacobi lists); both grow
+    unsigned char *arena = nullptr, *h_arena = nullptr;
+    size_t arena_bytes = 0;
+    double2 *crec = nullptr;                  // rotation records of Jacobi-diagonalised clusters
+    int64_t crec_slots = 0;
+    double *cnorm = nullptr;
+    int cnorm_n = 0;
+    size_t mid_smem = 0;
     size_t classify_smem = 0;
     // recorded after a call's last upload from the pinned staging buffers; the
     // next call waits for it before writing them again
@@ -164,6 +171,8 @@ struct ProjectPlan {
     bool staged_pending = false;
     // host-side counters
     long refine_accepted = 0, refine_jacobi = 0, refine_passes = 0, refine_clusters = 0;
+    long refine_large_clusters = 0;   // clusters diagonalised by the Jacobi kernels
+    long fb_edges = 0, fb_passes = 0;  // why refined blocks went to Jacobi
     bool fresh = true;
     bool built = false;
     long calls = 0, since_reset = 0;
@@ -245,25 +254,23 @@ struct ProjectPlan {
         d_nbad = d_state + nblk;
         d_nedge = d_nbad + nblk;
         V2B_CK(cudaHostGetDevicePointer((void **)&d_edges, h_edges, 0));
-        const int64_t max_jobs = std::max<int64_t>(rows_total / 2, 1);
-        jobs = dalloc<v2b::ClusterJob>(max_jobs);
-        mem = dalloc<int>(rows_total);
-        rowclus = dalloc<int>(rows_total);
         rowbase = dalloc<int>(nblk);
         lam = dalloc<double>(rows_total);
-        Qt = dalloc<double>((size_t)rows_total * v2b::kRefineMaxCluster);
+        Qt = dalloc<double>(total);   // sum of k^2 over the clusters of a block is at most n^2
+        Tc = dalloc<double>(total);
+        Pc = dalloc<double>(total);
         V2B_CK(cudaMemcpy(rowbase, rb_host.data(), nblk * 4, cudaMemcpyHostToDevice));
-        clus_bytes = max_jobs * sizeof(v2b::ClusterJob) + 2 * rows_total * sizeof(int);
-        V2B_CK(cudaMallocHost(&h_clus, std::max<size_t>(clus_bytes, 16)));
         classify_smem = (size_t)maxn * sizeof(double);
         if (classify_smem > 48 * 1024)
             V2B_CK(cudaFuncSetAttribute(v2b::refine_classify_kernel,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)classify_smem));
-        const int kc = v2b::kRefineMaxCluster;
+        const int kc = v2b::kRefineSmallCluster;
         V2B_CK(cudaFuncSetAttribute(v2b::cluster_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)(2 * kc * (kc + 1) * sizeof(double))));
-        V2B_CK(cudaFuncSetAttribute(v2b::cluster_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)((kc * kc + 64 * kc) * sizeof(double))));
+        // clusters of kRefineSmallCluster+1 .. kJacobiMaxDim rows use jacobi_warm_kernel
+        mid_smem = v2b::jacobi_smem_bytes(v2b::kJacobiMaxDim);
+        V2B_CK(cudaFuncSetAttribute(v2b::jacobi_warm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)std::max(smem, mid_smem)));
         V2B_CK(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
         fresh = true;
         built = true;
@@ -277,11 +284,12 @@ struct ProjectPlan {
                         (void *)rot, (void *)Vt, (void *)Vt2, (void *)Us, (void *)W, (void *)T,
                         (void *)P, (void *)rec_b, (void *)norm_b, (void *)sub_boff, (void *)sub_roff,
                         (void *)sub_bdim, (void *)bstate, (void *)orth, (void *)bnorm, (void *)Vsave,
-                        (void *)Tsave, (void *)jobs, (void *)mem,
-                        (void *)rowclus, (void *)rowbase, (void *)lam, (void *)Qt})
+                        (void *)Tsave, (void *)arena, (void *)crec, (void *)cnorm, (void *)Tc,
+                        (void *)Pc,
+                        (void *)rowbase, (void *)lam, (void *)Qt})
             cudaFree(q);
         for (void *q : {(void *)h_sub, (void *)h_bstate_up, (void *)h_state, (void *)h_edges,
-                        (void *)h_clus})
+                        (void *)h_arena})
             if (q) cudaFreeHost(q);
         built = false;
     }
@@ -301,9 +309,8 @@ struct ProjectPlan {
         since_reset = 0;
     }
 
-    // connected components of one block's recorded non-separable pairs;
-    // returns false when a component exceeds kRefineMaxCluster rows
-    bool clusters_of(int b, std::vector<std::vector<int>> &out) const {
+    // connected components of one block's recorded non-separable pairs
+    void clusters_of(int b, std::vector<std::vector<int>> &out) const {
         const int n = dims[b];
         const int ne = h_nedge[b];
         std::vector<int> parent(n);
@@ -334,14 +341,183 @@ struct ProjectPlan {
             }
             out[id[r]].push_back(i);   // ascending: rows are visited in order
         }
-        for (const auto &c : out)
-            if ((int)c.size() > v2b::kRefineMaxCluster) return false;
-        return true;
+    }
+
+    // grow-only device buffers of the cluster pass (called with the stream idle)
+    void ensure_arena(size_t bytes) {
+        if (bytes <= arena_bytes) return;
+        bytes = std::max(bytes, arena_bytes * 2);
+        if (arena) cudaFree(arena);
+        if (h_arena) cudaFreeHost(h_arena);
+        arena = nullptr;
+        h_arena = nullptr;
+        arena_bytes = 0;
+        arena = dalloc<unsigned char>(bytes);
+        V2B_CK(cudaMallocHost(&h_arena, bytes));
+        arena_bytes = bytes;
+    }
+    void ensure_crec(int64_t slots, int nbig_jobs) {
+        if (slots > crec_slots) {
+            if (crec) cudaFree(crec);
+            crec = nullptr;
+            crec = dalloc<double2>(slots);
+            crec_slots = slots;
+        }
+        if (nbig_jobs > cnorm_n) {
+            if (cnorm) cudaFree(cnorm);
+            cnorm = nullptr;
+            cnorm = dalloc<double>((size_t)nbig_jobs * v2b::kBigCluster);
+            cnorm_n = nbig_jobs;
+        }
     }
 
     void upload_states(cudaStream_t s, const std::vector<int> &st) {
         std::copy(st.begin(), st.end(), h_bstate_up);
         V2B_CK(cudaMemcpyAsync(bstate, h_bstate_up, nblk * sizeof(int), cudaMemcpyHostToDevice, s));
+    }
+
+    // Diagonalise every cluster exactly and apply the rotation G (identity
+    // outside the clusters): T <- G T G^T, Vt <- G Vt.  Jobs are ordered by
+    // size class: up to kRefineSmallCluster rows (cluster_eig_kernel), up to
+    // kJacobiMaxDim (jacobi_warm_kernel on a compact copy), larger
+    // (jacobi_big_kernel on a compact copy).
+    void cluster_pass(const std::vector<std::vector<int>> &members, const std::vector<int> &jblk,
+                      cudaStream_t s, long &launches) {
+        using namespace v2b;
+        const int nj_all = (int)members.size();
+        std::vector<int> order(nj_all);
+        for (int q = 0; q < nj_all; q++) order[q] = q;
+        auto cls = [&](int q) {
+            const int k = (int)members[q].size();
+            return k <= kRefineSmallCluster ? 0 : (k <= kJacobiMaxDim ? 1 : 2);
+        };
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cls(a) < cls(b); });
+        std::vector<ClusterJob> jl(nj_all);
+        std::vector<int> ml, rc((size_t)rows_total, -1), jlist;
+        std::vector<int4> trows, tcols, tcommit;
+        std::vector<int64_t> cboff, croff;
+        std::vector<int> cdim;
+        std::vector<int> base(nblk, 0);
+        for (int b = 1; b < nblk; b++) base[b] = base[b - 1] + dims[b - 1];
+        int64_t qoff = 0, roff = 0;
+        int nsm = 0, nmid = 0, nbg = 0, kmax_big = 0;
+        for (int q = 0; q < nj_all; q++) {
+            const auto &c = members[order[q]];
+            ClusterJob &j = jl[q];
+            j.blk = jblk[order[q]];
+            j.k = (int)c.size();
+            j.moff = (int)ml.size();
+            j.qoff = (int)qoff;
+            qoff += (int64_t)j.k * j.k;
+            for (int r : c) {
+                rc[base[j.blk] + r] = q;
+                ml.push_back(r);
+            }
+            const int n = dims[j.blk];
+            const int nti = (j.k + 31) / 32, ntc = (n + 63) / 64;
+            for (int a = 0; a < nti; a++)
+                for (int b = 0; b < ntc; b++) trows.push_back(make_int4(q, a, b, 0));
+            for (int a = 0; a < ntc; a++)
+                for (int b = 0; b < nti; b++) tcols.push_back(make_int4(q, a, b, 0));
+            for (int a = 0; a < ntc; a++) tcommit.push_back(make_int4(q, a, 0, 0));
+            const int kind = cls(order[q]);
+            if (kind == 0) {
+                nsm++;
+                continue;
+            }
+            jlist.push_back(q);
+            cboff.push_back(j.qoff);
+            cdim.push_back(j.k);
+            croff.push_back(roff);
+            if (kind == 1) {
+                const int np = j.k + (j.k & 1);
+                roff += (int64_t)max_sweeps * (np - 1) * (np / 2) + ((int64_t)max_sweeps * (np - 1) + 3) / 4 + 1;
+                nmid++;
+            } else {
+                roff += big_record_slots(j.k, kBigSweeps);
+                kmax_big = std::max(kmax_big, j.k);
+                nbg++;
+            }
+        }
+        refine_clusters += nj_all;
+        refine_large_clusters += nmid + nbg;
+        // pack the lists into the arena (16-byte aligned sections)
+        size_t off = 0;
+        auto sect = [&](size_t bytes) {
+            const size_t o = off;
+            off += (bytes + 15) & ~(size_t)15;
+            return o;
+        };
+        const size_t o_jobs = sect(jl.size() * sizeof(ClusterJob)), o_mem = sect(ml.size() * 4),
+                     o_rc = sect(rc.size() * 4), o_tr = sect(trows.size() * 16),
+                     o_tc = sect(tcols.size() * 16), o_tm = sect(tcommit.size() * 16),
+                     o_jl = sect(jlist.size() * 4), o_cb = sect(cboff.size() * 8),
+                     o_cd = sect(cdim.size() * 4), o_cr = sect(croff.size() * 8);
+        ensure_arena(off);
+        ensure_crec(std::max<int64_t>(roff, 1), nbg);
+        auto put = [&](size_t o, const void *src, size_t bytes) {
+            if (bytes) std::memcpy(h_arena + o, src, bytes);
+        };
+        put(o_jobs, jl.data(), jl.size() * sizeof(ClusterJob));
+        put(o_mem, ml.data(), ml.size() * 4);
+        put(o_rc, rc.data(), rc.size() * 4);
+        put(o_tr, trows.data(), trows.size() * 16);
+        put(o_tc, tcols.data(), tcols.size() * 16);
+        put(o_tm, tcommit.data(), tcommit.size() * 16);
+        put(o_jl, jlist.data(), jlist.size() * 4);
+        put(o_cb, cboff.data(), cboff.size() * 8);
+        put(o_cd, cdim.data(), cdim.size() * 4);
+        put(o_cr, croff.data(), croff.size() * 8);
+        V2B_CK(cudaMemcpyAsync(arena, h_arena, off, cudaMemcpyHostToDevice, s));
+        const ClusterJob *d_jobs = (const ClusterJob *)(arena + o_jobs);
+        const int *d_mem = (const int *)(arena + o_mem), *d_rc = (const int *)(arena + o_rc);
+        const int4 *d_tr = (const int4 *)(arena + o_tr), *d_tc = (const int4 *)(arena + o_tc),
+                   *d_tm = (const int4 *)(arena + o_tm);
+        const int *d_jl = (const int *)(arena + o_jl);
+        const int64_t *d_cb = (const int64_t *)(arena + o_cb), *d_cr = (const int64_t *)(arena + o_cr);
+        const int *d_cd = (const int *)(arena + o_cd);
+        if (nsm) {
+            const int kc = kRefineSmallCluster;
+            cluster_eig_kernel<<<nsm, 256, 2 * kc * (kc + 1) * sizeof(double), s>>>(T, boff, bdim, d_jobs,
+                                                                                 d_mem, Qt, lam);
+            V2B_CK(cudaGetLastError());
+            launches++;
+        }
+        if (nmid + nbg) {
+            cluster_gather_kernel<<<dim3(nmid + nbg, 16), 256, 0, s>>>(T, boff, bdim, d_jobs, d_mem, d_jl,
+                                                                       Tc, Qt);
+            V2B_CK(cudaGetLastError());
+            launches++;
+            // gap test off (gap_tol 0): the cluster is diagonalised to 1e-15 of its norm
+            if (nmid) {
+                jacobi_warm_kernel<<<nmid, kJacobiThreads, mid_smem, s>>>(
+                    Tc, Pc, Qt, d_cb, d_cd, crec, d_cr, max_sweeps, 1e-15, 0.0, counters, counters + 1, 1);
+                V2B_CK(cudaGetLastError());
+                launches++;
+            }
+            if (nbg) {
+                BigJacobiArgs a;
+                a.T = Tc; a.P = Pc; a.Vt = Qt; a.boff = d_cb + nmid; a.bdim = d_cd + nmid;
+                a.rot = crec; a.roff = d_cr + nmid; a.max_sweeps = kBigSweeps; a.norm_part = cnorm;
+                a.abs_tol = 1e-15; a.gap_tol = 0.0; a.counters = counters + 2;
+                const size_t alist_bytes = (size_t)((kmax_big + 1) / 2 + 1) * sizeof(int);
+                jacobi_big_kernel<<<nbg * kBigCluster, kBigThreads, alist_bytes, s>>>(a);
+                V2B_CK(cudaGetLastError());
+                launches++;
+            }
+            cluster_lam_kernel<<<std::min(nmid + nbg, 148), 256, 0, s>>>(d_jobs, d_jl, nmid + nbg, Pc, Tc,
+                                                                          nmid, lam);
+            V2B_CK(cudaGetLastError());
+            launches++;
+        }
+        cluster_rows_kernel<<<(int)trows.size(), 256, 0, s>>>(T, Vt, W, Vt2, boff, bdim, d_jobs, d_mem, Qt,
+                                                               d_tr);
+        cluster_cols_kernel<<<(int)tcols.size(), 256, 0, s>>>(T, W, P, boff, bdim, d_jobs, d_mem, d_rc,
+                                                               rowbase, Qt, lam, d_tc);
+        cluster_commit_kernel<<<(int)tcommit.size(), 256, 0, s>>>(T, W, P, Vt, Vt2, boff, bdim, d_jobs,
+                                                                   d_mem, d_rc, rowbase, d_tm);
+        V2B_CK(cudaGetLastError());
+        launches += 3;
     }
 
     // the refinement passes; returns per-block final states (Done or Jacobi).
@@ -377,68 +553,36 @@ struct ProjectPlan {
             V2B_CK(cudaStreamSynchronize(s));
             refine_passes++;
             // clusters of the blocks still in work
-            std::vector<ClusterJob> jl;
-            std::vector<int> ml;
-            std::vector<int> rc((size_t)rows_total, -1);
-            int64_t qoff = 0;
+            std::vector<std::vector<int>> members;   // per job
+            std::vector<int> jblk;
             int nwork = 0;
             for (int b = 0; b < nblk; b++) {
                 if (st[b] != kStWork) continue;
                 st[b] = h_state[b];
                 if (st[b] == kStDone) refine_accepted++;
-                if (st[b] == kStJacobi) restore(b);
+                if (st[b] == kStJacobi) {
+                    fb_passes++;
+                    restore(b);
+                }
                 if (st[b] != kStWork) continue;
-                std::vector<std::vector<int>> cl;
-                if (h_nedge[b] > kRefineEdgeCap || !clusters_of(b, cl)) {
+                if (h_nedge[b] > kRefineEdgeCap) {
+                    fb_edges++;
                     st[b] = kStJacobi;
                     restore(b);
                     continue;
                 }
+                std::vector<std::vector<int>> cl;
+                clusters_of(b, cl);
                 changed[b] = 1;
                 nwork++;
-                int64_t base = 0;
-                for (int q = 0; q < b; q++) base += dims[q];
-                for (const auto &c : cl) {
-                    ClusterJob j;
-                    j.blk = b;
-                    j.k = (int)c.size();
-                    j.moff = (int)ml.size();
-                    j.qoff = (int)qoff;
-                    qoff += (int64_t)j.k * j.k;
-                    for (int r : c) {
-                        rc[base + r] = (int)jl.size();
-                        ml.push_back(r);
-                    }
-                    jl.push_back(j);
+                for (auto &c : cl) {
+                    members.push_back(std::move(c));
+                    jblk.push_back(b);
                 }
             }
             if (nwork == 0) break;
             upload_states(s, st);
-            refine_clusters += (long)jl.size();
-            if (!jl.empty()) {
-                const int nj = (int)jl.size();
-                unsigned char *hp = h_clus;
-                const size_t jb = nj * sizeof(ClusterJob), mb = ml.size() * sizeof(int),
-                             rb = rc.size() * sizeof(int);
-                std::memcpy(hp, jl.data(), jb);
-                std::memcpy(hp + jb, ml.data(), mb);
-                std::memcpy(hp + jb + mb, rc.data(), rb);
-                V2B_CK(cudaMemcpyAsync(jobs, hp, jb, cudaMemcpyHostToDevice, s));
-                V2B_CK(cudaMemcpyAsync(mem, hp + jb, mb, cudaMemcpyHostToDevice, s));
-                V2B_CK(cudaMemcpyAsync(rowclus, hp + jb + mb, rb, cudaMemcpyHostToDevice, s));
-                const int kc = kRefineMaxCluster;
-                const int maxn = *std::max_element(dims.begin(), dims.end());
-                cluster_eig_kernel<<<nj, 256, 2 * kc * (kc + 1) * sizeof(double), s>>>(
-                    T, boff, bdim, jobs, mem, Qt, lam);
-                cluster_rows_kernel<<<dim3(nj, (maxn + 63) / 64), 256, (kc * kc + 64 * kc) * sizeof(double),
-                                      s>>>(T, Vt, W, Vt2, boff, bdim, jobs, mem, Qt);
-                cluster_cols_kernel<<<dim3(nj, (maxn + 31) / 32), 256, (kc * kc + 32 * kc) * sizeof(double),
-                                      s>>>(T, W, boff, bdim, jobs, mem, rowclus, rowbase, Qt, lam);
-                cluster_commit_kernel<<<dim3(nj, (maxn + 63) / 64), 256, 0, s>>>(
-                    T, W, Vt, Vt2, boff, bdim, jobs, mem, rowclus, rowbase);
-                V2B_CK(cudaGetLastError());
-                launches += 4;
-            }
+            if (!members.empty()) cluster_pass(members, jblk, s, launches);
             newton_m_kernel<<<ntiles, 256, 0, s>>>(T, W, tiles, boff, bdim, bstate, bnorm, gap_tol, abs_tol);
             V2B_CK(cudaGetLastError());
             launches++;
@@ -1149,15 +1293,13 @@ int v2b_problem_projection_counts(const v2b_problem *p, long *calls, long *rotat
     });
 }
 
-int v2b_problem_refine_counts(const v2b_problem *p, long *accepted, long *jacobi, long *passes,
-                              long *clusters) {
+int v2b_problem_refine_counts(const v2b_problem *p, long *counts, int n) {
     return guarded([&] {
-        if (!p || !accepted || !jacobi || !passes || !clusters)
-            throw std::invalid_argument("refine_counts: NULL argument");
-        *accepted = p->plan.refine_accepted;
-        *jacobi = p->plan.refine_jacobi;
-        *passes = p->plan.refine_passes;
-        *clusters = p->plan.refine_clusters;
+        if (!p || !counts || n < 0) throw std::invalid_argument("refine_counts: bad argument");
+        const ProjectPlan &q = p->plan;
+        const long v[7] = {q.refine_accepted, q.refine_jacobi, q.refine_passes, q.refine_clusters,
+                           q.refine_large_clusters, q.fb_edges, q.fb_passes};
+        for (int i = 0; i < n && i < 7; i++) counts[i] = v[i];
         return V2B_OK;
     });
 }

@@ -246,11 +246,14 @@ class V2RDMProblem:
                                                       ctypes.byref(c)))
         return {"calls": w.value, "rotations": r.value, "sweep_overruns": c.value}
 
+    REFINE_COUNTS = ("accepted", "jacobi", "passes", "clusters", "large_clusters",
+                     "fallback_edges", "fallback_passes")
+
     def refine_counts(self):
-        """{"accepted", "jacobi", "passes", "clusters"} of the warm eigen-refinement"""
-        v = [ctypes.c_long() for _ in range(4)]
-        check(self._lib.v2b_problem_refine_counts(self._h, *[ctypes.byref(x) for x in v]))
-        return dict(zip(("accepted", "jacobi", "passes", "clusters"), (x.value for x in v)))
+        """counts of the warm eigen-refinement, keyed by REFINE_COUNTS"""
+        v = (ctypes.c_long * len(self.REFINE_COUNTS))()
+        check(self._lib.v2b_problem_refine_counts(self._h, v, len(v)))
+        return dict(zip(self.REFINE_COUNTS, v))
 
     def stream_handle(self):
         return self._lib.v2b_problem_stream(self._h)

@@ -175,11 +175,12 @@ int v2b_problem_projection_counts(const v2b_problem *p, long *calls, long *rotat
                                   long *sweep_overruns);
 /* No counterpart in the reference (libsdp diagonalises every block with LAPACK
  * each iteration).  Warm refinement of the projection since the problem was
- * created: blocks accepted without Jacobi, blocks handed to the Jacobi
- * kernels, acceptance tests run (one per pass and call), clusters
- * diagonalised exactly. */
-int v2b_problem_refine_counts(const v2b_problem *p, long *accepted, long *jacobi, long *passes,
-                              long *clusters);
+ * created, the first n of: [0] blocks accepted without Jacobi, [1] blocks
+ * projected by the Jacobi kernels, [2] acceptance tests run (one per pass and
+ * call), [3] clusters diagonalised exactly, [4] of them by the Jacobi
+ * kernels (more than 64 rows), and the reasons refined blocks went to
+ * Jacobi: [5] too many non-separable pairs, [6] passes exhausted. */
+int v2b_problem_refine_counts(const v2b_problem *p, long *counts, int n);
 
 /* ---- 3. allocation-free projection ------------------------------------------ */
 

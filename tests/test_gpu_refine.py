@@ -13,9 +13,15 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-11   # |x - x_ref|_max <= TOL * max(1, |U|_F)
 
 
-def hard_spectrum(d, rng):
+def hard_spectrum(d, rng, zero_frac=0.0):
     lam = rng.uniform(-3.0, 3.0, d)
     if d < 24:   # blocks this small always take the Jacobi kernels
+        return lam
+    if zero_frac:
+        # a large group near zero of both signs: its eigenvectors turn freely
+        # from one step to the next, so the whole group forms one cluster
+        m = int(zero_frac * d)
+        lam[:m] = 1e-8 * rng.standard_normal(m)
         return lam
     k = d // 8
     lam[:k] = 1.0 + 1e-9 * rng.standard_normal(k)                 # degenerate, positive
@@ -32,13 +38,14 @@ def drift(q, rng, step):
     return q @ (r * np.sign(np.diag(r)))
 
 
-@pytest.mark.parametrize("n,steps,step", [(6, 12, 1e-4), (10, 8, 1e-4), (10, 6, 3e-3)])
-def test_warm_projection_sequence(cuda_device, n, steps, step):
+@pytest.mark.parametrize("n,steps,step,zero_frac", [(6, 12, 1e-4, 0.0), (10, 8, 1e-4, 0.0),
+                                                    (10, 6, 3e-3, 0.0), (10, 5, 1e-4, 0.85)])
+def test_warm_projection_sequence(cuda_device, n, steps, step, zero_frac):
     import torch
     p = hb.V2RDMProblem(n, n // 2, n // 2)
     rng = np.random.default_rng(100 + n)
     qs = [np.linalg.qr(rng.standard_normal((d, d)))[0] for d in p.dims]
-    ls = [hard_spectrum(d, rng) for d in p.dims]
+    ls = [hard_spectrum(d, rng, zero_frac) for d in p.dims]
     mu = 0.7
     for it in range(steps):
         U = np.concatenate([((q * l) @ q.T).ravel() for q, l in zip(qs, ls)])
@@ -54,6 +61,9 @@ def test_warm_projection_sequence(cuda_device, n, steps, step):
     # blocks of at least 24 rows are refined after the first (cold) call
     assert rc["accepted"] > 0, rc
     assert rc["passes"] > 0, rc
+    if zero_frac:
+        # the near-zero groups (85 and 170 rows) went to the Jacobi kernels as clusters
+        assert rc["large_clusters"] > 0, rc
 
 
 def test_cold_projection_resets_warm_basis(cuda_device):
