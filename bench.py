@@ -1,17 +1,24 @@
 """Benchmark: time to 1e-6 boundary-point SDP convergence of a v2RDM problem on B200.
 
-Workload (default ``hubbard8``): plain v2RDM, POSITIVITY DQG, fixed orbitals,
-FP64, C1, on the 1D periodic Hubbard ring with 8 sites, 8 electrons, t = 1,
-U = 4 (hilbert's own Hubbard path: h = -t on ring neighbours, (ii|ii) = U),
-converged to primal and dual error < 1e-6 and |E_p - E_d| < 1e-6, from the
-reference's random guess (srand(0)), MU_UPDATE_FREQUENCY 500, CG_CONVERGENCE
-1e-9.  Data are synthetic by construction (the Hamiltonian is the model).
+Workloads (plain v2RDM, POSITIVITY DQG, fixed orbitals, FP64, C1, converged to
+primal and dual error < 1e-6 and |E_p - E_d| < 1e-6 from the reference's
+random guess (srand(0)), MU_UPDATE_FREQUENCY 500, CG_CONVERGENCE 1e-9):
+
+  df20 (default)  the (20e, 20o) active space on synthetic density-fitted
+                  integrals: naux = 400, B^Q_pq ~ N(0, 0.05) symmetrised (seed 4),
+                  h = diag(linspace(-2, -0.1, 20)) + N(0, 0.02) symmetrised
+                  off-diagonal (seed 5), g_pqrs = sum_Q B^Q_pq B^Q_rs through
+                  the external-Hamiltonian path.  PSD blocks 20, 190, 210, 400, 800.
+  hubbard8        the 1D periodic Hubbard ring with 8 sites, 8 electrons,
+                  t = 1, U = 4 (hilbert's own Hubbard path).
+
+Data are synthetic by construction (no molecular integrals exist offline).
 
 One step = one full solve to convergence.  ``value`` is the device solve
 time with b, c, x already in HBM (CUDA events on the library's stream);
 ``e2e`` is the same solve through the public API with host arrays (pinned
 H2D of x0, b, c and D2H of x inside the timed region).  L2 is flushed between
-steps (a 256 MiB write); inside one solve the working set stays L2-resident.
+steps (a 256 MiB write).
 
 Multi-GPU: replicas only.  Each rank solves its own copy of the workload;
 the reported time is the max over ranks; nothing crosses NVLink in the data
@@ -20,7 +27,8 @@ path.
 ``--impl reference`` times the reference's own CPU implementation of the path
 (hilbert's compiled constraint maps from oracle/_ref, else the C restatement,
 driven by the numpy boundary-point restatement), each step a bounded sample
-of outer iterations extrapolated to the workload's iteration count.
+of CG iterations and outer-iteration bodies extrapolated to the workload's
+iteration counts.
 """
 import argparse
 import json
@@ -34,15 +42,35 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
-    "hubbard8": dict(nmo=8, nalpha=4, nbeta=4, positivity="DQG", hubbard=(1.0, 4.0),
+    "df20": dict(nmo=20, nalpha=10, nbeta=10, positivity="DQG", hamiltonian="df",
+                 df=dict(n=20, naux=400, seed_b=4, seed_h=5), hubbard_multiplicity=False,
+                 r_conv=1e-6, e_conv=1e-6, cg_conv=1e-9, muf=500, maxiter=400000),
+    "hubbard8": dict(nmo=8, nalpha=4, nbeta=4, positivity="DQG", hamiltonian="hubbard",
+                     hubbard=(1.0, 4.0), hubbard_multiplicity=True,
                      r_conv=1e-6, e_conv=1e-6, cg_conv=1e-9, muf=500, maxiter=400000),
 }
-# (outer, CG) iterations the FP64 oracle needed to converge this workload,
-# recorded from a full oracle run; the reference arm scales its sample by them
-# (oracle: C restatement maps + numpy boundary-point loop, 8 host threads; energy
-#  -4.9364448537582035 at eps_p 9.83e-7, eps_d 1.00e-6; 497 s on the build host)
-ORACLE_ITERS = {"hubbard8": (13801, 503997)}
-ORACLE_ENERGY = {"hubbard8": -4.9364448537582035}
+# (outer, CG) iterations of the FP64 solve to convergence; the reference arm
+# scales its per-iteration sample by them.
+#  hubbard8: the CPU oracle run (C restatement maps + numpy boundary-point
+#    loop): energy -4.9364448537582035 at eps_p 9.83e-7, eps_d 1.00e-6.
+#  df20: the FP64 device solve (one outer iteration of the CPU path takes
+#    seconds here, so a CPU solve to convergence takes hours; the device path
+#    reproduces the CPU oracle's iteration counts on the Hubbard rings).
+FP64_ITERS = {"hubbard8": (13801, 503997), "df20": (4102, 179742)}
+# FP64 energies the device result is compared with:
+#  hubbard8: the CPU oracle; df20: the FP64 device solve that diagonalises
+#  every block by selective Jacobi each iteration (no warm refinement).
+FP64_ENERGY = {"hubbard8": (-4.9364448537582035, "cpu oracle"),
+               "df20": (-103.6150114058378, "fp64 device solve, Jacobi every iteration")}
+
+
+def hamiltonian(w):
+    """('hubbard', (t, U)) or ('external', (h, g)) for a workload"""
+    if w["hamiltonian"] == "hubbard":
+        return "hubbard", w["hubbard"]
+    from hilbert_b200.synthetic import df_hamiltonian
+    return "external", df_hamiltonian(**w["df"])
+
 
 METRIC = "time to 1e-6 SDP convergence, mixed/batched vs plain FP64 on B200; |dE| vs FP64"
 
@@ -50,10 +78,10 @@ METRIC = "time to 1e-6 SDP convergence, mixed/batched vs plain FP64 on B200; |dE
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="hubbard8", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="df20", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--max-outer", type=int, default=0,
                     help="cap the outer iterations of each solve (profiling runs; the line then "
@@ -182,9 +210,10 @@ def cpu_sample(w, seconds):
     from oracle.bpsdp import project_blocks
     kind = "reference" if maps.ref_available() else "port"
     P = maps.RefProblem if kind == "reference" else maps.OracleProblem
-    prob = P(w["nmo"], w["nalpha"], w["nbeta"], w["positivity"], True, True, hubbard=w["hubbard"])
-    o = maps.OracleProblem(w["nmo"], w["nalpha"], w["nbeta"], w["positivity"], True, True,
-                           hubbard=w["hubbard"])
+    kind_h, ham = hamiltonian(w)
+    kw = dict(hubbard=ham) if kind_h == "hubbard" else dict(h=ham[0], g=ham[1])
+    prob = P(w["nmo"], w["nalpha"], w["nbeta"], w["positivity"], True, True, **kw)
+    o = maps.OracleProblem(w["nmo"], w["nalpha"], w["nbeta"], w["positivity"], True, True, **kw)
     x = o.guess("random")
     z = np.zeros(prob.n_primal)
     y = np.random.default_rng(0).standard_normal(prob.n_dual)
@@ -222,7 +251,7 @@ def run_reference(args, w):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    oiter, iiter = ORACLE_ITERS.get(args.workload, (None, None))
+    oiter, iiter = FP64_ITERS.get(args.workload, (None, None))
     vals = []
     for k in range(args.warmup + args.steps):
         t_cg, t_out, kind, reps = cpu_sample(w, max(2.0, args.cpu_sample_seconds / 3))
@@ -233,7 +262,7 @@ def run_reference(args, w):
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload, **{k: v for k, v in w.items()},
-                       "oracle_outer_iterations": oiter, "oracle_cg_iterations": iiter,
+                       "fp64_outer_iterations": oiter, "fp64_cg_iterations": iiter,
                        "parallelism": "replicas"},
             "cpu_baseline": {"value": total, "unit": "s", "cores": cpu_threads(), "kind": kind,
                              "sample": f"per step: {reps[0]} CG iterations ({t_cg*1e3:.2f} ms each) and "
@@ -256,9 +285,10 @@ def run_b200(args, w):
                        "MAXITER": args.max_outer if args.max_outer else w["maxiter"],
                        "MU_UPDATE_FREQUENCY": w["muf"]})
     p = hb.V2RDMProblem(w["nmo"], w["nalpha"], w["nbeta"], w["positivity"], True, True,
-                        hubbard_multiplicity=True)
+                        hubbard_multiplicity=w["hubbard_multiplicity"])
     b = p.b()
-    c = p.c_hubbard(*w["hubbard"])
+    kind_h, ham = hamiltonian(w)
+    c = p.c_hubbard(*ham) if kind_h == "hubbard" else p.c_external(*ham)
     x0 = p.guess("RANDOM")
     db = torch.from_numpy(b).to(dev)
     dc = torch.from_numpy(c).to(dev)
@@ -311,42 +341,38 @@ def run_b200(args, w):
         e2e_times.append(time.perf_counter() - t0)
     te2e = max_over_ranks(max(e2e_times), world)
 
-    # roofline of the dominant kernel class
-    dom = max(prof, key=lambda k: prof[k][0])
-    ms, n = prof[dom]
+    # roofline: cg_kernel, the largest single kernel (the projection is a
+    # sequence of GEMM-tile, test and Jacobi kernels; its FLOP rate is reported
+    # beside it)
     oiter, iiter = stats["oiter"], stats["iiter"]
     npr, ndu = p.n_primal, p.n_dual
+    nnz_a, nnz_t = p.operator_nnz()
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
-    bf16 = peaks.get("bf16_tflops", 1590.0)
-    if dom == "projection":
-        flops = sum((16.0 / 3.0) * float(d) ** 3 for d in p.dims)
-        ach = flops / (ms / n / 1e3) / 1e12
-        roof = {"kernel": dom, "bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s",
-                "frac": ach / bf16, "traffic": None,
-                "note": "FP64 projection (GEMM transforms + selective Jacobi); algorithmic flops "
-                        "sum (16/3) n_b^3 per launch; peak is the measured dense bf16 figure (no "
-                        "FP64 peak is measured)"}
-    else:
-        cg_iters_per_launch = iiter / max(oiter, 1)
-        if dom == "cg_kernel":
-            bytes_ = 8.0 * (cg_iters_per_launch * (2 * npr + 7 * ndu) + 2 * npr + 5 * ndu)
-        elif dom == "spmv_AT_U_kernel":
-            bytes_ = 8.0 * (4 * npr + ndu)
-        elif dom == "spmv_A2_kernel":
-            bytes_ = 8.0 * (3 * npr + 2 * ndu)
-        else:
-            bytes_ = 8.0 * (5 * npr + 3 * ndu)
-        ach = bytes_ / (ms / n / 1e3) / 1e9
-        roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                "frac": ach / hbm, "traffic": None}
-    roof["peak_source"] = "MEASURED_PEAKS.json" if peaks else "fallback"
-    roof["kernel_ms_share"] = {k: round(v[0] / sum(x[0] for x in prof.values()), 4)
-                               for k, v in prof.items()}
+    ms_cg, n_cg = prof["cg_kernel"]
+    m = iiter / max(oiter, 1)   # CG iterations per launch (one launch per outer iteration)
+    per_iter = 8.0 * (2 * npr + 7 * ndu) + 4.0 * (nnz_a + nnz_t + npr + ndu)
+    bytes_launch = (m + 1) * per_iter   # + the initial residual, one A^T and one A pass
+    ach = bytes_launch / (ms_cg / n_cg / 1e3) / 1e9
+    roof = {"kernel": "cg_kernel", "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+            "frac": ach / hbm, "traffic": None,
+            "algorithmic_bytes": "per CG iteration 8 (2 n_p + 7 n_d) vector bytes + 4 (nnz(A) + "
+                                 "nnz(A^T) + n_p + n_d) operator-table bytes; (m + 1) iterations "
+                                 f"per launch, m = {m:.1f}",
+            "peak_source": ("MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s")}
+    ms_pj, n_pj = prof["projection"]
+    flops = sum((16.0 / 3.0) * float(d) ** 3 for d in p.dims)
+    roof["projection"] = {"ms_per_call": ms_pj / max(n_pj, 1),
+                          "fp64_tflops": flops / (ms_pj / max(n_pj, 1) / 1e3) / 1e12,
+                          "flops_per_call": flops,
+                          "note": "sum (16/3) n_b^3 per call (eigendecomposition + back-transform "
+                                  "counted as for LAPACK), FP64; no FP64 peak is measured"}
+    tot = sum(x[0] for x in prof.values())
+    roof["kernel_ms_share"] = {k: round(v[0] / tot, 4) for k, v in prof.items()}
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_sample_seconds > 0:
@@ -363,16 +389,20 @@ def run_b200(args, w):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": args.workload, "nmo": w["nmo"], "nalpha": w["nalpha"],
                            "nbeta": w["nbeta"], "positivity": w["positivity"],
-                           "hubbard_t_U": list(w["hubbard"]), "r_convergence": w["r_conv"],
+                           "hamiltonian": ({"hubbard_t_U": list(w["hubbard"])} if kind_h == "hubbard"
+                                           else {"synthetic_df": w["df"]}),
+                           "r_convergence": w["r_conv"],
                            "e_convergence": w["e_conv"], "cg_convergence": w["cg_conv"],
                            "mu_update_frequency": w["muf"], "n_primal": npr, "n_dual": ndu,
+                           "block_dims": sorted(set(int(d) for d in p.dims)),
                            "parallelism": "replicas" if world > 1 else "single",
                            "l2": "flushed between steps (256 MiB write)",
                            "outer_iterations": oiter, "cg_iterations": iiter,
                            "energy": energy, "converged": stats["converged"],
-                           "oracle_energy": ORACLE_ENERGY.get(args.workload),
-                           "abs_dE_vs_fp64_oracle": (abs(energy - ORACLE_ENERGY[args.workload])
-                                                     if args.workload in ORACLE_ENERGY else None),
+                           "fp64_energy": FP64_ENERGY[args.workload][0],
+                           "fp64_energy_source": FP64_ENERGY[args.workload][1],
+                           "abs_dE_vs_fp64": abs(energy - FP64_ENERGY[args.workload][0]),
+                           "projection_refine_counts": p.refine_counts(),
                            "max_outer_cap": args.max_outer or None},
                 "e2e": {"value": te2e, "unit": "s", "h2d_bytes_per_step": 8 * (2 * npr + ndu),
                         "d2h_bytes_per_step": 8 * npr},

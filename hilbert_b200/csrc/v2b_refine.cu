@@ -49,7 +49,8 @@ __global__ void __launch_bounds__(kRefineThreads)
                            int force, double gap_tol, double abs_tol, double *__restrict__ bnorm,
                            int *h_state, int *h_nbad, int *h_nedge, int2 *h_edges) {
     const int blk = blockIdx.x;
-    if (bstate[blk] != kStWork) return;   // uniform over the CTA
+    const int st_in = bstate[blk];
+    if (st_in != kStWork && st_in != kStBlockJacobi) return;   // uniform over the CTA
     const int n = bdim[blk];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
     __shared__ double red[32];
@@ -120,7 +121,7 @@ __global__ void __launch_bounds__(kRefineThreads)
         }
     }
     if (tid == 0) {
-        const int st = done ? kStDone : (force ? kStJacobi : kStWork);
+        const int st = done ? kStDone : (force ? kStJacobi : st_in);
         bstate[blk] = st;
         h_state[blk] = st;
         h_nbad[blk] = nbad;
@@ -133,8 +134,9 @@ __global__ void __launch_bounds__(256)
     cluster_eig_kernel(const double *__restrict__ T, const int64_t *__restrict__ boff,
                        const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,
                        const int *__restrict__ mem, double *__restrict__ Qt,
-                       double *__restrict__ lam) {
+                       double *__restrict__ lam, const int *__restrict__ only, int max_sweeps) {
     const ClusterJob jb = jobs[blockIdx.x];
+    if (only && !only[jb.blk]) return;   // uniform over the CTA
     const int k = jb.k, n = bdim[jb.blk];
     const int kp = k + (k & 1), ld = kp + 1, m = kp / 2;
     const int *C = mem + jb.moff;
@@ -159,10 +161,13 @@ __global__ void __launch_bounds__(256)
         fro += v * v;
     }
     fro = block_sum(fro, red);
-    if (threadIdx.x == 0) s_thr = 1e-15 * sqrt(fro) + 1e-300;
+    // rotate down to 1e-14 of the cluster's norm: below the acceptance test's
+    // floor (1e-14 of the block's norm) and above the rounding noise the
+    // rotations themselves leave, so the sweeps end
+    if (threadIdx.x == 0) s_thr = 1e-14 * sqrt(fro) + 1e-300;
     __syncthreads();
     const double thr = s_thr;
-    for (int sweep = 0; sweep < 40; sweep++) {
+    for (int sweep = 0; sweep < max_sweeps; sweep++) {
         if (threadIdx.x == 0) s_nrot = 0;
         __syncthreads();
         for (int st = 0; st < kp - 1; st++) {
@@ -229,9 +234,11 @@ __global__ void __launch_bounds__(256)
                         double *__restrict__ W, double *__restrict__ Vt2,
                         const int64_t *__restrict__ boff, const int *__restrict__ bdim,
                         const ClusterJob *__restrict__ jobs, const int *__restrict__ mem,
-                        const double *__restrict__ Qt, const int4 *__restrict__ ctiles) {
+                        const double *__restrict__ Qt, const int4 *__restrict__ ctiles,
+                        const int *__restrict__ only) {
     const int4 ct = ctiles[blockIdx.x];
     const ClusterJob jb = jobs[ct.x];
+    if (only && !only[jb.blk]) return;
     const int k = jb.k, n = bdim[jb.blk];
     const int i0 = ct.y * 32, c0 = ct.z * 64;
     const int64_t off = boff[jb.blk];
@@ -291,18 +298,22 @@ __global__ void __launch_bounds__(256)
 
 // tile (job, ta, ti): P[a, C_i] = sum_l R(a)[C_l] Qt[i][l] for a in [64 ta, 64 ta + 64),
 // i in [32 ti, 32 ti + 32), with R(a) = W[a, :] on cluster rows (already
-// rotated by their own cluster) and T[a, :] elsewhere; a row of this same
-// cluster gets delta_ai lam_i.  P is free scratch for blocks in refinement.
+// rotated by their own cluster) and T[a, :] elsewhere.  The cluster's own
+// block comes out as Qt T[C, C] Qt^T: diagonal when the cluster solve was
+// exact, and still the rotated block when its sweeps were capped.  P is free
+// scratch for blocks in refinement.
 __global__ void __launch_bounds__(256)
     cluster_cols_kernel(const double *__restrict__ T, const double *__restrict__ W,
                         double *__restrict__ P, const int64_t *__restrict__ boff,
                         const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,
                         const int *__restrict__ mem, const int *__restrict__ rowclus,
                         const int *__restrict__ rowbase, const double *__restrict__ Qt,
-                        const double *__restrict__ lam, const int4 *__restrict__ ctiles) {
+                        const double *__restrict__ lam, const int4 *__restrict__ ctiles,
+                        const int *__restrict__ only) {
     const int4 ct = ctiles[blockIdx.x];
     const int jid = ct.x;
     const ClusterJob jb = jobs[jid];
+    if (only && !only[jb.blk]) return;
     const int k = jb.k, n = bdim[jb.blk];
     const int a0 = ct.y * 64, i0 = ct.z * 32;
     const int64_t off = boff[jb.blk];
@@ -343,13 +354,11 @@ __global__ void __launch_bounds__(256)
     for (int r = 0; r < 2; r++) {
         const int a = a0 + ta * 2 + r;
         if (a >= n) continue;
-        const bool own = rc[a] == jid;
 #pragma unroll
         for (int jj = 0; jj < 4; jj++) {
             const int i = i0 + ti * 4 + jj;
             if (i >= k) continue;
-            const double v = own ? (a == C[i] ? lam[jb.moff + i] : 0.0) : acc[r][jj];
-            P[off + (int64_t)a * n + C[i]] = v;
+            P[off + (int64_t)a * n + C[i]] = acc[r][jj];
         }
     }
 }
@@ -363,9 +372,11 @@ __global__ void __launch_bounds__(256)
                           const double *__restrict__ Vt2, const int64_t *__restrict__ boff,
                           const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,
                           const int *__restrict__ mem, const int *__restrict__ rowclus,
-                          const int *__restrict__ rowbase, const int4 *__restrict__ ctiles) {
+                          const int *__restrict__ rowbase, const int4 *__restrict__ ctiles,
+                          const int *__restrict__ only) {
     const int4 ct = ctiles[blockIdx.x];
     const ClusterJob jb = jobs[ct.x];
+    if (only && !only[jb.blk]) return;
     const int k = jb.k, n = bdim[jb.blk];
     const int t0 = ct.y * 64;
     const int64_t off = boff[jb.blk];

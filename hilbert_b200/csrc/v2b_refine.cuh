@@ -12,6 +12,12 @@ namespace v2b {
 constexpr int kStWork = 0;     // refinement passes continue
 constexpr int kStDone = 1;     // T passed the acceptance test; P written
 constexpr int kStJacobi = 2;   // handed to the selective Jacobi kernels
+constexpr int kStBlockJacobi = 3;   // block-Jacobi sweeps over pairs of row groups
+
+constexpr int kBJGroup = 32;           // rows per block-Jacobi group (pairs: 64-row subproblems)
+constexpr int kBJMaxSweeps = 24;
+constexpr int kBJInnerSweeps = 2;      // Jacobi sweeps per 64-row subproblem and step
+constexpr int kClusterSweeps = 40;     // cap of the exact cluster diagonalisation
 
 constexpr int kRefineSmallCluster = 64;  // clusters up to this size: cluster_eig_kernel
 constexpr int kRefineEdgeCap = 32768;    // non-separable pairs recorded per block and pass
@@ -37,31 +43,37 @@ __global__ void refine_classify_kernel(const double *__restrict__ T, double *__r
                                        double gap_tol, double abs_tol, double *__restrict__ bnorm,
                                        int *h_state, int *h_nbad, int *h_nedge, int2 *h_edges);
 
-// exact eigen-decomposition of each cluster's T[C, C]: rows of Qt (k x k) are
-// the eigenvectors, lam the eigenvalues
+// cyclic Jacobi on each cluster's T[C, C] (at most max_sweeps sweeps; enough
+// sweeps diagonalise it exactly): rows of Qt (k x k) are the eigenvectors,
+// lam the diagonal left
 __global__ void cluster_eig_kernel(const double *__restrict__ T, const int64_t *__restrict__ boff,
                                    const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,
                                    const int *__restrict__ mem, double *__restrict__ Qt,
-                                   double *__restrict__ lam);
+                                   double *__restrict__ lam, const int *__restrict__ only,
+                                   int max_sweeps);
 
-// gathered GEMM tiles of the cluster transform; ctiles = (job, tile row, tile col)
+// gathered GEMM tiles of the cluster transform; ctiles = (job, tile row, tile col).
+// With `only` non-null, jobs of blocks b with only[b] == 0 are skipped.
 __global__ void cluster_rows_kernel(const double *__restrict__ T, const double *__restrict__ Vt,
                                     double *__restrict__ W, double *__restrict__ Vt2,
                                     const int64_t *__restrict__ boff, const int *__restrict__ bdim,
                                     const ClusterJob *__restrict__ jobs, const int *__restrict__ mem,
-                                    const double *__restrict__ Qt, const int4 *__restrict__ ctiles);
+                                    const double *__restrict__ Qt, const int4 *__restrict__ ctiles,
+                                    const int *__restrict__ only);
 __global__ void cluster_cols_kernel(const double *__restrict__ T, const double *__restrict__ W,
                                     double *__restrict__ P, const int64_t *__restrict__ boff,
                                     const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,
                                     const int *__restrict__ mem, const int *__restrict__ rowclus,
                                     const int *__restrict__ rowbase, const double *__restrict__ Qt,
-                                    const double *__restrict__ lam, const int4 *__restrict__ ctiles);
+                                    const double *__restrict__ lam, const int4 *__restrict__ ctiles,
+                                    const int *__restrict__ only);
 __global__ void cluster_commit_kernel(double *__restrict__ T, const double *__restrict__ W,
                                       const double *__restrict__ P, double *__restrict__ Vt,
                                       const double *__restrict__ Vt2, const int64_t *__restrict__ boff,
                                       const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,
                                       const int *__restrict__ mem, const int *__restrict__ rowclus,
-                                      const int *__restrict__ rowbase, const int4 *__restrict__ ctiles);
+                                      const int *__restrict__ rowbase, const int4 *__restrict__ ctiles,
+                                      const int *__restrict__ only);
 // compact sym(T[C, C]) and identity for the clusters in jlist
 __global__ void cluster_gather_kernel(const double *__restrict__ T, const int64_t *__restrict__ boff,
                                       const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,

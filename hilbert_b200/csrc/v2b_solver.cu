@@ -164,6 +164,18 @@ struct ProjectPlan {
     double *cnorm = nullptr;
     int cnorm_n = 0;
     size_t mid_smem = 0;
+    // block-Jacobi schedule (fixed by the block sizes): per step, the pairs of
+    // kBJGroup-row groups of every block of at least kRefineMinDim rows, as
+    // cluster jobs with their tile lists, device-resident
+    struct BJStep {
+        size_t o_jobs = 0, o_mem = 0, o_rc = 0, o_tr = 0, o_tc = 0, o_tm = 0;
+        int njobs = 0, ntr = 0, ntc = 0, ntm = 0;
+    };
+    std::vector<BJStep> bj_steps;
+    std::vector<int> bj_nsteps;   // steps per sweep of each block (0: not scheduled)
+    unsigned char *bj_dev = nullptr;
+    int *bj_on = nullptr, *h_bjon = nullptr;
+    long refine_bj_sweeps = 0;
     size_t classify_smem = 0;
     // recorded after a call's last upload from the pinned staging buffers; the
     // next call waits for it before writing them again
@@ -271,6 +283,7 @@ struct ProjectPlan {
         mid_smem = v2b::jacobi_smem_bytes(v2b::kJacobiMaxDim);
         V2B_CK(cudaFuncSetAttribute(v2b::jacobi_warm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)std::max(smem, mid_smem)));
+        build_block_jacobi(rb_host);
         V2B_CK(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
         fresh = true;
         built = true;
@@ -285,11 +298,11 @@ struct ProjectPlan {
                         (void *)P, (void *)rec_b, (void *)norm_b, (void *)sub_boff, (void *)sub_roff,
                         (void *)sub_bdim, (void *)bstate, (void *)orth, (void *)bnorm, (void *)Vsave,
                         (void *)Tsave, (void *)arena, (void *)crec, (void *)cnorm, (void *)Tc,
-                        (void *)Pc,
+                        (void *)Pc, (void *)bj_dev, (void *)bj_on,
                         (void *)rowbase, (void *)lam, (void *)Qt})
             cudaFree(q);
         for (void *q : {(void *)h_sub, (void *)h_bstate_up, (void *)h_state, (void *)h_edges,
-                        (void *)h_arena})
+                        (void *)h_arena, (void *)h_bjon})
             if (q) cudaFreeHost(q);
         built = false;
     }
@@ -340,6 +353,127 @@ struct ProjectPlan {
                 out.emplace_back();
             }
             out[id[r]].push_back(i);   // ascending: rows are visited in order
+        }
+    }
+
+    // Round-robin pairing of the kBJGroup-row groups of each block (the
+    // circle method over an even number of groups, a padding group when the
+    // count is odd): one sweep of ng_even - 1 steps meets every pair of groups
+    // once; every step's pairs are disjoint, so a step diagonalises each
+    // paired 2 x kBJGroup sub-block exactly and applies all of them at once.
+    void build_block_jacobi(const std::vector<int> &rbase) {
+        using namespace v2b;
+        bj_nsteps.assign(nblk, 0);
+        int S = 0;
+        std::vector<int> ng(nblk, 0);
+        for (int b = 0; b < nblk; b++) {
+            if (dims[b] < kRefineMinDim) continue;
+            ng[b] = (dims[b] + kBJGroup - 1) / kBJGroup;
+            const int ge = ng[b] + (ng[b] & 1);
+            bj_nsteps[b] = std::max(ge - 1, 1);
+            S = std::max(S, bj_nsteps[b]);
+        }
+        std::vector<unsigned char> buf;
+        auto sect = [&](const void *src, size_t bytes) {
+            const size_t o = buf.size();
+            buf.resize(o + ((bytes + 15) & ~(size_t)15));
+            if (bytes) std::memcpy(buf.data() + o, src, bytes);
+            return o;
+        };
+        bj_steps.assign(S, BJStep());
+        for (int st = 0; st < S; st++) {
+            std::vector<ClusterJob> jl;
+            std::vector<int> ml, rc((size_t)rows_total, -1);
+            std::vector<int4> tr, tc, tm;
+            int qoff = 0;
+            for (int b = 0; b < nblk; b++) {
+                if (st >= bj_nsteps[b]) continue;
+                const int n = dims[b], ge = ng[b] + (ng[b] & 1);
+                for (int kk = 0; kk < std::max(ge / 2, 1); kk++) {
+                    int ga = 0, gb = 1;
+                    if (ge >= 2) {
+                        const int m1 = ge - 1;
+                        int a, c;
+                        if (kk == 0) {
+                            a = m1;
+                            c = st;
+                        } else {
+                            a = (st + kk) % m1;
+                            c = (st - kk + m1) % m1;
+                        }
+                        ga = std::min(a, c);
+                        gb = std::max(a, c);
+                    }
+                    ClusterJob j;
+                    j.blk = b;
+                    j.moff = (int)ml.size();
+                    j.qoff = qoff;
+                    for (int g : {ga, gb}) {
+                        if (g >= ng[b]) continue;   // the padding group
+                        for (int r = g * kBJGroup; r < std::min(n, (g + 1) * kBJGroup); r++) {
+                            rc[rbase[b] + r] = (int)jl.size();
+                            ml.push_back(r);
+                        }
+                    }
+                    j.k = (int)ml.size() - j.moff;
+                    if (j.k == 0) continue;
+                    qoff += j.k * j.k;
+                    const int q = (int)jl.size();
+                    const int nti = (j.k + 31) / 32, ntc = (n + 63) / 64;
+                    for (int a = 0; a < nti; a++)
+                        for (int c = 0; c < ntc; c++) tr.push_back(make_int4(q, a, c, 0));
+                    for (int a = 0; a < ntc; a++)
+                        for (int c = 0; c < nti; c++) tc.push_back(make_int4(q, a, c, 0));
+                    for (int a = 0; a < ntc; a++) tm.push_back(make_int4(q, a, 0, 0));
+                    jl.push_back(j);
+                }
+            }
+            BJStep &bs = bj_steps[st];
+            bs.njobs = (int)jl.size();
+            bs.ntr = (int)tr.size();
+            bs.ntc = (int)tc.size();
+            bs.ntm = (int)tm.size();
+            bs.o_jobs = sect(jl.data(), jl.size() * sizeof(ClusterJob));
+            bs.o_mem = sect(ml.data(), ml.size() * 4);
+            bs.o_rc = sect(rc.data(), rc.size() * 4);
+            bs.o_tr = sect(tr.data(), tr.size() * 16);
+            bs.o_tc = sect(tc.data(), tc.size() * 16);
+            bs.o_tm = sect(tm.data(), tm.size() * 16);
+        }
+        bj_dev = dalloc<unsigned char>(std::max<size_t>(buf.size(), 16));
+        if (!buf.empty()) V2B_CK(cudaMemcpy(bj_dev, buf.data(), buf.size(), cudaMemcpyHostToDevice));
+        bj_on = dalloc<int>(nblk);
+        V2B_CK(cudaMallocHost(&h_bjon, std::max(nblk, 1) * sizeof(int)));
+    }
+
+    // one block-Jacobi sweep of the blocks with st == kStBlockJacobi
+    void block_jacobi_sweep(const std::vector<int> &st, cudaStream_t s, long &launches) {
+        using namespace v2b;
+        int S = 0;
+        for (int b = 0; b < nblk; b++) {
+            h_bjon[b] = st[b] == kStBlockJacobi;
+            if (h_bjon[b]) S = std::max(S, bj_nsteps[b]);
+        }
+        if (S == 0) return;
+        V2B_CK(cudaMemcpyAsync(bj_on, h_bjon, nblk * sizeof(int), cudaMemcpyHostToDevice, s));
+        refine_bj_sweeps++;
+        const int kc = kRefineSmallCluster;
+        for (int i = 0; i < S; i++) {
+            const BJStep &bs = bj_steps[i];
+            if (bs.njobs == 0) continue;
+            const ClusterJob *jobs = (const ClusterJob *)(bj_dev + bs.o_jobs);
+            const int *mem = (const int *)(bj_dev + bs.o_mem), *rc = (const int *)(bj_dev + bs.o_rc);
+            cluster_eig_kernel<<<bs.njobs, 256, 2 * kc * (kc + 1) * sizeof(double), s>>>(T, boff, bdim, jobs,
+                                                                                      mem, Qt, lam, bj_on,
+                                                                                      kBJInnerSweeps);
+            cluster_rows_kernel<<<bs.ntr, 256, 0, s>>>(T, Vt, W, Vt2, boff, bdim, jobs, mem, Qt,
+                                                        (const int4 *)(bj_dev + bs.o_tr), bj_on);
+            cluster_cols_kernel<<<bs.ntc, 256, 0, s>>>(T, W, P, boff, bdim, jobs, mem, rc, rowbase, Qt, lam,
+                                                        (const int4 *)(bj_dev + bs.o_tc), bj_on);
+            cluster_commit_kernel<<<bs.ntm, 256, 0, s>>>(T, W, P, Vt, Vt2, boff, bdim, jobs, mem, rc, rowbase,
+                                                          (const int4 *)(bj_dev + bs.o_tm), bj_on);
+            V2B_CK(cudaGetLastError());
+            launches += 4;
         }
     }
 
@@ -479,7 +613,8 @@ struct ProjectPlan {
         if (nsm) {
             const int kc = kRefineSmallCluster;
             cluster_eig_kernel<<<nsm, 256, 2 * kc * (kc + 1) * sizeof(double), s>>>(T, boff, bdim, d_jobs,
-                                                                                 d_mem, Qt, lam);
+                                                                                 d_mem, Qt, lam, nullptr,
+                                                                                 kClusterSweeps);
             V2B_CK(cudaGetLastError());
             launches++;
         }
@@ -511,86 +646,130 @@ struct ProjectPlan {
             launches++;
         }
         cluster_rows_kernel<<<(int)trows.size(), 256, 0, s>>>(T, Vt, W, Vt2, boff, bdim, d_jobs, d_mem, Qt,
-                                                               d_tr);
+                                                               d_tr, nullptr);
         cluster_cols_kernel<<<(int)tcols.size(), 256, 0, s>>>(T, W, P, boff, bdim, d_jobs, d_mem, d_rc,
-                                                               rowbase, Qt, lam, d_tc);
+                                                               rowbase, Qt, lam, d_tc, nullptr);
         cluster_commit_kernel<<<(int)tcommit.size(), 256, 0, s>>>(T, W, P, Vt, Vt2, boff, bdim, d_jobs,
-                                                                   d_mem, d_rc, rowbase, d_tm);
+                                                                   d_mem, d_rc, rowbase, d_tm, nullptr);
         V2B_CK(cudaGetLastError());
         launches += 3;
     }
 
-    // the refinement passes; returns per-block final states (Done or Jacobi).
-    // A block handed to Jacobi after its basis was changed restarts from the
-    // call's saved basis and T, so the Jacobi kernels always see an
-    // orthonormal Vt.
+    // The refinement passes; leaves every block Done or Jacobi.  Per pass,
+    // after the acceptance test, a block in Newton mode (kStWork) takes the
+    // cluster diagonalisation and one Newton step; it changes to block-Jacobi
+    // mode (kStBlockJacobi) when it records too many non-separable pairs, has
+    // a cluster above kRefineSmallCluster rows or runs out of Newton passes,
+    // restarting from the call's saved basis and T (block-Jacobi keeps Vt
+    // orthonormal by construction, the Newton steps only to the accepted
+    // tolerance).  A block in block-Jacobi mode takes one sweep per pass, and
+    // after kBJMaxSweeps goes to the selective Jacobi kernels.
     void refine(std::vector<int> &st, cudaStream_t s, long &launches) {
         using namespace v2b;
         bool any = false;
-        for (int b = 0; b < nblk; b++) any = any || st[b] == kStWork;
+        for (int b = 0; b < nblk; b++) any = any || st[b] == kStWork || st[b] == kStBlockJacobi;
         if (!any) return;
         V2B_CK(cudaMemsetAsync(orth, 0, nblk * sizeof(unsigned long long), s));
         V2B_CK(cudaMemcpyAsync(Vsave, Vt, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
         V2B_CK(cudaMemcpyAsync(Tsave, T, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
         std::vector<char> changed(nblk, 0);
+        std::vector<int> newton(nblk, 0), sweeps(nblk, 0);
         auto restore = [&](int b) {
             if (!changed[b]) return;
             const size_t bytes = (size_t)dims[b] * dims[b] * sizeof(double);
             V2B_CK(cudaMemcpyAsync(Vt + h_off[b], Vsave + h_off[b], bytes, cudaMemcpyDeviceToDevice, s));
             V2B_CK(cudaMemcpyAsync(T + h_off[b], Tsave + h_off[b], bytes, cudaMemcpyDeviceToDevice, s));
+            V2B_CK(cudaMemsetAsync(orth + b, 0, sizeof(unsigned long long), s));
             changed[b] = 0;
         };
-        for (int pass = 0; pass <= kRefinePasses; pass++) {
-            if (pass > 0) {
-                gemm(kGemmNTStore, Us, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
-                gemm(kGemmNNStore, Vt, W, T, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
+        auto to_block_jacobi = [&](int b) {
+            restore(b);
+            st[b] = kStBlockJacobi;
+        };
+        for (int pass = 0;; pass++) {
+            if (pass > 0) {   // T of the blocks that took a Newton step (bstate == kStWork)
+                bool nw = false;
+                for (int b = 0; b < nblk; b++) nw = nw || st[b] == kStWork;
+                if (nw) {
+                    gemm(kGemmNTStore, Us, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
+                    gemm(kGemmNNStore, Vt, W, T, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
+                }
             }
             refine_classify_kernel<<<nblk, kRefineThreads, classify_smem, s>>>(
-                T, P, boff, bdim, bstate, orth, pass == kRefinePasses ? 1 : 0, gap_tol, abs_tol, bnorm,
-                d_state, d_nbad, d_nedge, d_edges);
+                T, P, boff, bdim, bstate, orth, 0, gap_tol, abs_tol, bnorm, d_state, d_nbad, d_nedge, d_edges);
             V2B_CK(cudaGetLastError());
             launches++;
             V2B_CK(cudaStreamSynchronize(s));
             refine_passes++;
-            // clusters of the blocks still in work
-            std::vector<std::vector<int>> members;   // per job
+            std::vector<std::vector<int>> members;   // clusters of the Newton-mode blocks
             std::vector<int> jblk;
-            int nwork = 0;
+            int nwork = 0, nbj = 0;
             for (int b = 0; b < nblk; b++) {
-                if (st[b] != kStWork) continue;
-                st[b] = h_state[b];
-                if (st[b] == kStDone) refine_accepted++;
-                if (st[b] == kStJacobi) {
-                    fb_passes++;
-                    restore(b);
+                if (st[b] != kStWork && st[b] != kStBlockJacobi) continue;
+                if (h_state[b] == kStDone) {
+                    st[b] = kStDone;
+                    refine_accepted++;
+                    continue;
                 }
-                if (st[b] != kStWork) continue;
+                if (st[b] == kStBlockJacobi) {
+                    if (sweeps[b] >= kBJMaxSweeps) {
+                        fb_passes++;
+                        st[b] = kStJacobi;
+                    } else {
+                        nbj++;
+                    }
+                    continue;
+                }
+                // Newton mode
+                if (newton[b] >= kRefinePasses) {
+                    to_block_jacobi(b);
+                    nbj++;
+                    continue;
+                }
                 if (h_nedge[b] > kRefineEdgeCap) {
                     fb_edges++;
-                    st[b] = kStJacobi;
-                    restore(b);
+                    to_block_jacobi(b);
+                    nbj++;
                     continue;
                 }
                 std::vector<std::vector<int>> cl;
                 clusters_of(b, cl);
+                size_t kmax = 0;
+                for (const auto &c : cl) kmax = std::max(kmax, c.size());
+                if ((int)kmax > kRefineSmallCluster) {
+                    refine_large_clusters++;
+                    to_block_jacobi(b);
+                    nbj++;
+                    continue;
+                }
                 changed[b] = 1;
+                newton[b]++;
                 nwork++;
                 for (auto &c : cl) {
                     members.push_back(std::move(c));
                     jblk.push_back(b);
                 }
             }
-            if (nwork == 0) break;
+            if (nwork == 0 && nbj == 0) break;
             upload_states(s, st);
-            if (!members.empty()) cluster_pass(members, jblk, s, launches);
-            newton_m_kernel<<<ntiles, 256, 0, s>>>(T, W, tiles, boff, bdim, bstate, bnorm, gap_tol, abs_tol);
-            V2B_CK(cudaGetLastError());
-            launches++;
-            V2B_CK(cudaMemsetAsync(orth, 0, nblk * sizeof(unsigned long long), s));
-            gemm(kGemmNNStore, W, Vt, Vt2, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
-            gemm(kGemmNTNewtonSchulz, Vt2, Vt2, W, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
-            gemm(kGemmNNStore, W, Vt2, Vt, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
+            if (nbj) {
+                block_jacobi_sweep(st, s, launches);
+                for (int b = 0; b < nblk; b++)
+                    if (st[b] == kStBlockJacobi) sweeps[b]++;
+            }
+            if (nwork) {
+                if (!members.empty()) cluster_pass(members, jblk, s, launches);
+                newton_m_kernel<<<ntiles, 256, 0, s>>>(T, W, tiles, boff, bdim, bstate, bnorm, gap_tol,
+                                                       abs_tol);
+                V2B_CK(cudaGetLastError());
+                launches++;
+                V2B_CK(cudaMemsetAsync(orth, 0, nblk * sizeof(unsigned long long), s));
+                gemm(kGemmNNStore, W, Vt, Vt2, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
+                gemm(kGemmNTNewtonSchulz, Vt2, Vt2, W, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
+                gemm(kGemmNNStore, W, Vt2, Vt, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
+            }
         }
+        upload_states(s, st);
     }
 
     // selective Jacobi on the blocks in state kStJacobi
@@ -662,7 +841,7 @@ struct ProjectPlan {
         std::vector<int> st(nblk);
         for (int b = 0; b < nblk; b++)
             st[b] = dims[b] == 0 ? kStDone
-                    : (cold || dims[b] < kRefineMinDim) ? kStJacobi : kStWork;
+                    : dims[b] < kRefineMinDim ? kStJacobi : (cold ? kStBlockJacobi : kStWork);
         if (staged_pending) V2B_CK(cudaEventSynchronize(staged));
         upload_states(s, st);
         refine(st, s, launches);
@@ -1297,9 +1476,9 @@ int v2b_problem_refine_counts(const v2b_problem *p, long *counts, int n) {
     return guarded([&] {
         if (!p || !counts || n < 0) throw std::invalid_argument("refine_counts: bad argument");
         const ProjectPlan &q = p->plan;
-        const long v[7] = {q.refine_accepted, q.refine_jacobi, q.refine_passes, q.refine_clusters,
-                           q.refine_large_clusters, q.fb_edges, q.fb_passes};
-        for (int i = 0; i < n && i < 7; i++) counts[i] = v[i];
+        const long v[8] = {q.refine_accepted, q.refine_jacobi, q.refine_passes, q.refine_clusters,
+                           q.refine_large_clusters, q.fb_edges, q.fb_passes, q.refine_bj_sweeps};
+        for (int i = 0; i < n && i < 8; i++) counts[i] = v[i];
         return V2B_OK;
     });
 }

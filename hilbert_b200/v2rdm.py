@@ -246,8 +246,18 @@ class V2RDMProblem:
                                                       ctypes.byref(c)))
         return {"calls": w.value, "rotations": r.value, "sweep_overruns": c.value}
 
+    def operator_nnz(self):
+        """(nnz(A), nnz(A^T)) of the packed constraint operator"""
+        out = []
+        for t in (0, 1):
+            nr, nnz, npal = ctypes.c_long(), ctypes.c_long(), ctypes.c_int()
+            check(self._lib.v2b_problem_operator_size(self._h, t, ctypes.byref(nr), ctypes.byref(nnz),
+                                                      ctypes.byref(npal)))
+            out.append(nnz.value)
+        return tuple(out)
+
     REFINE_COUNTS = ("accepted", "jacobi", "passes", "clusters", "large_clusters",
-                     "fallback_edges", "fallback_passes")
+                     "fallback_edges", "fallback_passes", "block_jacobi_sweeps")
 
     def refine_counts(self):
         """counts of the warm eigen-refinement, keyed by REFINE_COUNTS"""

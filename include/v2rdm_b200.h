@@ -177,9 +177,10 @@ int v2b_problem_projection_counts(const v2b_problem *p, long *calls, long *rotat
  * each iteration).  Warm refinement of the projection since the problem was
  * created, the first n of: [0] blocks accepted without Jacobi, [1] blocks
  * projected by the Jacobi kernels, [2] acceptance tests run (one per pass and
- * call), [3] clusters diagonalised exactly, [4] of them by the Jacobi
- * kernels (more than 64 rows), and the reasons refined blocks went to
- * Jacobi: [5] too many non-separable pairs, [6] passes exhausted. */
+ * call), [3] clusters diagonalised exactly, [4] blocks that changed to
+ * block-Jacobi sweeps for a cluster above 64 rows, [5] ... for too many
+ * non-separable pairs, [6] blocks handed to the Jacobi kernels after their
+ * passes or sweeps ran out, [7] block-Jacobi sweeps run. */
 int v2b_problem_refine_counts(const v2b_problem *p, long *counts, int n);
 
 /* ---- 3. allocation-free projection ------------------------------------------ */
