@@ -130,6 +130,12 @@ __global__ void __launch_bounds__(kRefineThreads)
 }
 
 // ---------------------------------------------------------------- clusters
+// Cyclic Jacobi on one cluster per CTA (k <= kRefineSmallCluster), A and the
+// eigenvector rows Q in shared memory.  The round-robin pairs of every step
+// are tabulated once; a step computes the rotations of its m = kp/2 disjoint
+// pairs (sym.schur2), then applies all of them at once, each thread updating
+// whole 2 x 2 blocks (rows of pair P, columns of pair Q) two-sidedly and the
+// rows p, q of Q: two barriers per step.
 __global__ void __launch_bounds__(256)
     cluster_eig_kernel(const double *__restrict__ T, const int64_t *__restrict__ boff,
                        const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,
@@ -138,18 +144,27 @@ __global__ void __launch_bounds__(256)
     const ClusterJob jb = jobs[blockIdx.x];
     if (only && !only[jb.blk]) return;   // uniform over the CTA
     const int k = jb.k, n = bdim[jb.blk];
-    const int kp = k + (k & 1), ld = kp + 1, m = kp / 2;
+    const int kp = k + (k & 1), ld = kp + 1, m = kp / 2, nst = kp - 1;
     const int *C = mem + jb.moff;
     const double *Tb = T + boff[jb.blk];
     extern __shared__ double sm[];
     double *A = sm;              // kp x ld
     double *Q = A + kp * ld;     // kp x ld, rows = eigenvectors
-    __shared__ double2 cs[kRefineSmallCluster / 2];
+    constexpr int KM = kRefineSmallCluster;
+    __shared__ unsigned char pr[KM - 1][KM / 2], qr[KM - 1][KM / 2];
+    __shared__ double2 cs[KM / 2];
     __shared__ double red[32];
     __shared__ double s_thr;
     __shared__ int s_nrot;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < nst * m; e += blockDim.x) {
+        int p, q;
+        rr_pair(e / m, e % m, kp, p, q);
+        pr[e / m][e % m] = (unsigned char)p;
+        qr[e / m][e % m] = (unsigned char)q;
+    }
     double fro = 0.0;
-    for (int e = threadIdx.x; e < kp * kp; e += blockDim.x) {
+    for (int e = tid; e < kp * kp; e += blockDim.x) {
         const int i = e / kp, j = e % kp;
         double v = 0.0;
         if (i < k && j < k) {
@@ -164,16 +179,16 @@ __global__ void __launch_bounds__(256)
     // rotate down to 1e-14 of the cluster's norm: below the acceptance test's
     // floor (1e-14 of the block's norm) and above the rounding noise the
     // rotations themselves leave, so the sweeps end
-    if (threadIdx.x == 0) s_thr = 1e-14 * sqrt(fro) + 1e-300;
+    if (tid == 0) s_thr = 1e-14 * sqrt(fro) + 1e-300;
     __syncthreads();
     const double thr = s_thr;
+    const int P = tid >> 3, sub = tid & 7;   // 32 pair rows x 8 lanes
     for (int sweep = 0; sweep < max_sweeps; sweep++) {
-        if (threadIdx.x == 0) s_nrot = 0;
+        if (tid == 0) s_nrot = 0;
         __syncthreads();
-        for (int st = 0; st < kp - 1; st++) {
-            for (int kk = threadIdx.x; kk < m; kk += blockDim.x) {
-                int p, q;
-                rr_pair(st, kk, kp, p, q);
+        for (int st = 0; st < nst; st++) {
+            if (tid < m) {
+                const int p = pr[st][tid], q = qr[st][tid];
                 double c = 1.0, s = 0.0;
                 if (q < k) {
                     const double apq = A[p * ld + q];
@@ -186,43 +201,153 @@ __global__ void __launch_bounds__(256)
                         atomicAdd(&s_nrot, 1);
                     }
                 }
-                cs[kk] = make_double2(c, s);
+                cs[tid] = make_double2(c, s);
             }
             __syncthreads();
-            // A <- A G^T (columns p, q)
-            for (int e = threadIdx.x; e < m * kp; e += blockDim.x) {
-                const int kk = e / kp, r = e % kp;
-                const double2 g = cs[kk];
-                if (g.y == 0.0) continue;
-                int p, q;
-                rr_pair(st, kk, kp, p, q);
-                const double ap = A[r * ld + p], aq = A[r * ld + q];
-                A[r * ld + p] = g.x * ap - g.y * aq;
-                A[r * ld + q] = g.y * ap + g.x * aq;
-            }
-            __syncthreads();
-            // A <- G A, Q <- G Q (rows p, q)
-            for (int e = threadIdx.x; e < m * kp; e += blockDim.x) {
-                const int kk = e / kp, col = e % kp;
-                const double2 g = cs[kk];
-                if (g.y == 0.0) continue;
-                int p, q;
-                rr_pair(st, kk, kp, p, q);
-                const double ap = A[p * ld + col], aq = A[q * ld + col];
-                A[p * ld + col] = g.x * ap - g.y * aq;
-                A[q * ld + col] = g.y * ap + g.x * aq;
-                const double qp = Q[p * ld + col], qq = Q[q * ld + col];
-                Q[p * ld + col] = g.x * qp - g.y * qq;
-                Q[q * ld + col] = g.y * qp + g.x * qq;
+            if (P < m) {
+                const double2 cp = cs[P];
+                const int pP = pr[st][P], qP = qr[st][P];
+                // A <- G A G^T on the 2 x 2 blocks (P, Q2)
+                for (int Q2 = sub; Q2 < m; Q2 += 8) {
+                    const double2 cq = cs[Q2];
+                    if (cp.y == 0.0 && cq.y == 0.0) continue;
+                    const int pQ = pr[st][Q2], qQ = qr[st][Q2];
+                    const double b11 = A[pP * ld + pQ], b12 = A[pP * ld + qQ];
+                    const double b21 = A[qP * ld + pQ], b22 = A[qP * ld + qQ];
+                    const double m11 = b11 * cq.x - b12 * cq.y, m12 = b11 * cq.y + b12 * cq.x;
+                    const double m21 = b21 * cq.x - b22 * cq.y, m22 = b21 * cq.y + b22 * cq.x;
+                    double n11 = cp.x * m11 - cp.y * m21, n12 = cp.x * m12 - cp.y * m22;
+                    double n21 = cp.y * m11 + cp.x * m21, n22 = cp.y * m12 + cp.x * m22;
+                    if (Q2 == P) n12 = n21 = 0.0;   // the pair's own coupling, annihilated
+                    A[pP * ld + pQ] = n11;
+                    A[pP * ld + qQ] = n12;
+                    A[qP * ld + pQ] = n21;
+                    A[qP * ld + qQ] = n22;
+                }
+                // Q <- G Q on rows p, q
+                if (cp.y != 0.0)
+                    for (int jc = sub; jc < kp; jc += 8) {
+                        const double qp = Q[pP * ld + jc], qq = Q[qP * ld + jc];
+                        Q[pP * ld + jc] = cp.x * qp - cp.y * qq;
+                        Q[qP * ld + jc] = cp.y * qp + cp.x * qq;
+                    }
             }
             __syncthreads();
         }
-        if (s_nrot == 0) break;   // uniform: read after the step's final barrier
+        const int nrot = s_nrot;   // read by all before thread 0 resets it
         __syncthreads();
+        if (nrot == 0) break;
     }
     double *Qo = Qt + jb.qoff;
-    for (int e = threadIdx.x; e < k * k; e += blockDim.x) Qo[e] = Q[(e / k) * ld + e % k];
-    for (int i = threadIdx.x; i < k; i += blockDim.x) lam[jb.moff + i] = A[i * ld + i];
+    for (int e = tid; e < k * k; e += blockDim.x) Qo[e] = Q[(e / k) * ld + e % k];
+    for (int i = tid; i < k; i += blockDim.x) lam[jb.moff + i] = A[i * ld + i];
+}
+
+// One block-Jacobi step applied in place.  The step's jobs partition each
+// block's rows, so T splits into job tiles T[C_I, C_J] that only their own
+// CTA reads and writes:  tile kind 0 (I, J):  T[C_I, C_J] <- Qt_I T[C_I, C_J] Qt_J^T;
+// kind 1 (I, t):  Vt[C_I, 64 t .. 64 t + 64) <- Qt_I Vt[C_I, ...].
+__global__ void __launch_bounds__(256)
+    bj_apply_kernel(double *__restrict__ T, double *__restrict__ Vt, const int64_t *__restrict__ boff,
+                    const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,
+                    const int *__restrict__ mem, const double *__restrict__ Qt,
+                    const int4 *__restrict__ tiles, const int *__restrict__ only) {
+    const int4 tl = tiles[blockIdx.x];
+    const ClusterJob jI = jobs[tl.x];
+    if (only && !only[jI.blk]) return;   // uniform over the CTA
+    const int n = bdim[jI.blk];
+    const int64_t off = boff[jI.blk];
+    constexpr int KM = kRefineSmallCluster, LD = KM + 1;
+    extern __shared__ double sm[];
+    double *sQ = sm;              // KM x LD: Qt_I
+    double *sX = sQ + KM * LD;    // KM x LD: the tile, then Qt_I x tile
+    double *sR = sX + KM * LD;    // KM x LD: Qt_J (kind 0)
+    const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+    const int kI = jI.k;
+    const int *CI = mem + jI.moff;
+    for (int e = tid; e < kI * kI; e += blockDim.x) sQ[(e / kI) * LD + e % kI] = Qt[jI.qoff + e];
+    if (tl.z == 0) {
+        const ClusterJob jJ = jobs[tl.y];
+        const int kJ = jJ.k;
+        const int *CJ = mem + jJ.moff;
+        for (int e = tid; e < kJ * kJ; e += blockDim.x) sR[(e / kJ) * LD + e % kJ] = Qt[jJ.qoff + e];
+        for (int e = tid; e < kI * kJ; e += blockDim.x) {
+            const int i = e / kJ, j = e % kJ;
+            sX[i * LD + j] = T[off + (int64_t)CI[i] * n + CJ[j]];
+        }
+        __syncthreads();
+        // Y = Qt_I X (rows 4 ty .., cols 4 tx ..)
+        double y[4][4] = {};
+        for (int l = 0; l < kI; l++) {
+            double a[4], b[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) a[r] = (4 * ty + r < kI) ? sQ[(4 * ty + r) * LD + l] : 0.0;
+#pragma unroll
+            for (int c = 0; c < 4; c++) b[c] = (4 * tx + c < kJ) ? sX[l * LD + 4 * tx + c] : 0.0;
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) y[r][c] = fma(a[r], b[c], y[r][c]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) sX[(4 * ty + r) * LD + 4 * tx + c] = y[r][c];
+        __syncthreads();
+        // Z = Y Qt_J^T
+        double z[4][4] = {};
+        for (int l = 0; l < kJ; l++) {
+            double a[4], b[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) a[r] = sX[(4 * ty + r) * LD + l];
+#pragma unroll
+            for (int c = 0; c < 4; c++) b[c] = (4 * tx + c < kJ) ? sR[(4 * tx + c) * LD + l] : 0.0;
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) z[r][c] = fma(a[r], b[c], z[r][c]);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int i = 4 * ty + r;
+            if (i >= kI) continue;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int j = 4 * tx + c;
+                if (j < kJ) T[off + (int64_t)CI[i] * n + CJ[j]] = z[r][c];
+            }
+        }
+    } else {
+        const int c0 = tl.y * 64;
+        for (int e = tid; e < kI * 64; e += blockDim.x) {
+            const int i = e >> 6, c = c0 + (e & 63);
+            sX[i * LD + (e & 63)] = (c < n) ? Vt[off + (int64_t)CI[i] * n + c] : 0.0;
+        }
+        __syncthreads();
+        double y[4][4] = {};
+        for (int l = 0; l < kI; l++) {
+            double a[4], b[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) a[r] = (4 * ty + r < kI) ? sQ[(4 * ty + r) * LD + l] : 0.0;
+#pragma unroll
+            for (int c = 0; c < 4; c++) b[c] = sX[l * LD + 4 * tx + c];
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) y[r][c] = fma(a[r], b[c], y[r][c]);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int i = 4 * ty + r;
+            if (i >= kI) continue;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int cc = c0 + 4 * tx + c;
+                if (cc < n) Vt[off + (int64_t)CI[i] * n + cc] = y[r][c];
+            }
+        }
+    }
 }
 
 // Gathered GEMM tiles of the cluster transform G (identity outside the

@@ -74,6 +74,14 @@ __global__ void cluster_commit_kernel(double *__restrict__ T, const double *__re
                                       const int *__restrict__ mem, const int *__restrict__ rowclus,
                                       const int *__restrict__ rowbase, const int4 *__restrict__ ctiles,
                                       const int *__restrict__ only);
+// one block-Jacobi step in place: tiles (I, J, 0) T[C_I, C_J] <- Qt_I T Qt_J^T,
+// (I, t, 1) Vt[C_I, 64 t ..] <- Qt_I Vt[C_I, ..]; dynamic shared memory
+// 3 x 64 x 65 doubles
+__global__ void bj_apply_kernel(double *__restrict__ T, double *__restrict__ Vt,
+                                const int64_t *__restrict__ boff, const int *__restrict__ bdim,
+                                const ClusterJob *__restrict__ jobs, const int *__restrict__ mem,
+                                const double *__restrict__ Qt, const int4 *__restrict__ tiles,
+                                const int *__restrict__ only);
 // compact sym(T[C, C]) and identity for the clusters in jlist
 __global__ void cluster_gather_kernel(const double *__restrict__ T, const int64_t *__restrict__ boff,
                                       const int *__restrict__ bdim, const ClusterJob *__restrict__ jobs,

@@ -168,8 +168,8 @@ struct ProjectPlan {
     // kBJGroup-row groups of every block of at least kRefineMinDim rows, as
     // cluster jobs with their tile lists, device-resident
     struct BJStep {
-        size_t o_jobs = 0, o_mem = 0, o_rc = 0, o_tr = 0, o_tc = 0, o_tm = 0;
-        int njobs = 0, ntr = 0, ntc = 0, ntm = 0;
+        size_t o_jobs = 0, o_mem = 0, o_tiles = 0;
+        int njobs = 0, ntiles = 0;
     };
     std::vector<BJStep> bj_steps;
     std::vector<int> bj_nsteps;   // steps per sweep of each block (0: not scheduled)
@@ -279,11 +279,13 @@ struct ProjectPlan {
         const int kc = v2b::kRefineSmallCluster;
         V2B_CK(cudaFuncSetAttribute(v2b::cluster_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)(2 * kc * (kc + 1) * sizeof(double))));
+        V2B_CK(cudaFuncSetAttribute(v2b::bj_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(3 * kc * (kc + 1) * sizeof(double))));
         // clusters of kRefineSmallCluster+1 .. kJacobiMaxDim rows use jacobi_warm_kernel
         mid_smem = v2b::jacobi_smem_bytes(v2b::kJacobiMaxDim);
         V2B_CK(cudaFuncSetAttribute(v2b::jacobi_warm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)std::max(smem, mid_smem)));
-        build_block_jacobi(rb_host);
+        build_block_jacobi();
         V2B_CK(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
         fresh = true;
         built = true;
@@ -359,9 +361,11 @@ struct ProjectPlan {
     // Round-robin pairing of the kBJGroup-row groups of each block (the
     // circle method over an even number of groups, a padding group when the
     // count is odd): one sweep of ng_even - 1 steps meets every pair of groups
-    // once; every step's pairs are disjoint, so a step diagonalises each
-    // paired 2 x kBJGroup sub-block exactly and applies all of them at once.
-    void build_block_jacobi(const std::vector<int> &rbase) {
+    // once.  A step's pairs are disjoint and cover the block, so each step
+    // runs kBJInnerSweeps Jacobi sweeps on every paired 2 x kBJGroup sub-block
+    // (cluster_eig_kernel) and applies all rotations at once, in place, tile
+    // by tile (bj_apply_kernel).
+    void build_block_jacobi() {
         using namespace v2b;
         bj_nsteps.assign(nblk, 0);
         int S = 0;
@@ -383,12 +387,13 @@ struct ProjectPlan {
         bj_steps.assign(S, BJStep());
         for (int st = 0; st < S; st++) {
             std::vector<ClusterJob> jl;
-            std::vector<int> ml, rc((size_t)rows_total, -1);
-            std::vector<int4> tr, tc, tm;
+            std::vector<int> ml;
+            std::vector<int4> tl;
             int qoff = 0;
             for (int b = 0; b < nblk; b++) {
                 if (st >= bj_nsteps[b]) continue;
                 const int n = dims[b], ge = ng[b] + (ng[b] & 1);
+                const int first = (int)jl.size();
                 for (int kk = 0; kk < std::max(ge / 2, 1); kk++) {
                     int ga = 0, gb = 1;
                     if (ge >= 2) {
@@ -410,35 +415,26 @@ struct ProjectPlan {
                     j.qoff = qoff;
                     for (int g : {ga, gb}) {
                         if (g >= ng[b]) continue;   // the padding group
-                        for (int r = g * kBJGroup; r < std::min(n, (g + 1) * kBJGroup); r++) {
-                            rc[rbase[b] + r] = (int)jl.size();
-                            ml.push_back(r);
-                        }
+                        for (int r = g * kBJGroup; r < std::min(n, (g + 1) * kBJGroup); r++) ml.push_back(r);
                     }
                     j.k = (int)ml.size() - j.moff;
                     if (j.k == 0) continue;
                     qoff += j.k * j.k;
-                    const int q = (int)jl.size();
-                    const int nti = (j.k + 31) / 32, ntc = (n + 63) / 64;
-                    for (int a = 0; a < nti; a++)
-                        for (int c = 0; c < ntc; c++) tr.push_back(make_int4(q, a, c, 0));
-                    for (int a = 0; a < ntc; a++)
-                        for (int c = 0; c < nti; c++) tc.push_back(make_int4(q, a, c, 0));
-                    for (int a = 0; a < ntc; a++) tm.push_back(make_int4(q, a, 0, 0));
                     jl.push_back(j);
+                }
+                // every row of the block is in exactly one job of this step
+                const int last = (int)jl.size(), ntc = (n + 63) / 64;
+                for (int I = first; I < last; I++) {
+                    for (int J = first; J < last; J++) tl.push_back(make_int4(I, J, 0, 0));
+                    for (int t = 0; t < ntc; t++) tl.push_back(make_int4(I, t, 1, 0));
                 }
             }
             BJStep &bs = bj_steps[st];
             bs.njobs = (int)jl.size();
-            bs.ntr = (int)tr.size();
-            bs.ntc = (int)tc.size();
-            bs.ntm = (int)tm.size();
+            bs.ntiles = (int)tl.size();
             bs.o_jobs = sect(jl.data(), jl.size() * sizeof(ClusterJob));
             bs.o_mem = sect(ml.data(), ml.size() * 4);
-            bs.o_rc = sect(rc.data(), rc.size() * 4);
-            bs.o_tr = sect(tr.data(), tr.size() * 16);
-            bs.o_tc = sect(tc.data(), tc.size() * 16);
-            bs.o_tm = sect(tm.data(), tm.size() * 16);
+            bs.o_tiles = sect(tl.data(), tl.size() * 16);
         }
         bj_dev = dalloc<unsigned char>(std::max<size_t>(buf.size(), 16));
         if (!buf.empty()) V2B_CK(cudaMemcpy(bj_dev, buf.data(), buf.size(), cudaMemcpyHostToDevice));
@@ -462,18 +458,14 @@ struct ProjectPlan {
             const BJStep &bs = bj_steps[i];
             if (bs.njobs == 0) continue;
             const ClusterJob *jobs = (const ClusterJob *)(bj_dev + bs.o_jobs);
-            const int *mem = (const int *)(bj_dev + bs.o_mem), *rc = (const int *)(bj_dev + bs.o_rc);
+            const int *mem = (const int *)(bj_dev + bs.o_mem);
             cluster_eig_kernel<<<bs.njobs, 256, 2 * kc * (kc + 1) * sizeof(double), s>>>(T, boff, bdim, jobs,
                                                                                       mem, Qt, lam, bj_on,
                                                                                       kBJInnerSweeps);
-            cluster_rows_kernel<<<bs.ntr, 256, 0, s>>>(T, Vt, W, Vt2, boff, bdim, jobs, mem, Qt,
-                                                        (const int4 *)(bj_dev + bs.o_tr), bj_on);
-            cluster_cols_kernel<<<bs.ntc, 256, 0, s>>>(T, W, P, boff, bdim, jobs, mem, rc, rowbase, Qt, lam,
-                                                        (const int4 *)(bj_dev + bs.o_tc), bj_on);
-            cluster_commit_kernel<<<bs.ntm, 256, 0, s>>>(T, W, P, Vt, Vt2, boff, bdim, jobs, mem, rc, rowbase,
-                                                          (const int4 *)(bj_dev + bs.o_tm), bj_on);
+            bj_apply_kernel<<<bs.ntiles, 256, 3 * kc * (kc + 1) * sizeof(double), s>>>(
+                T, Vt, boff, bdim, jobs, mem, Qt, (const int4 *)(bj_dev + bs.o_tiles), bj_on);
             V2B_CK(cudaGetLastError());
-            launches += 4;
+            launches += 2;
         }
     }
 
