@@ -42,53 +42,77 @@ __device__ __forceinline__ double gamma_pq(double li, double lj) {
     return (li != lj) ? (pi - pj) / (li - lj) : (li > 0.0 ? 1.0 : 0.0);
 }
 
+// Row pairs (r, n-1-r) hold n-1 upper-triangle pairs together: CTA s of a
+// block takes row pairs [s R, (s+1) R), R = ceil(ceil(n/2) / kClassifySplit).
+__device__ __forceinline__ void split_rows(int n, int s, int &r0, int &r1) {
+    const int half = (n + 1) / 2, R = (half + kClassifySplit - 1) / kClassifySplit;
+    r0 = min(half, s * R);
+    r1 = min(half, (s + 1) * R);
+}
+
+// Frobenius norms of the symmetrised blocks, in kClassifySplit partial sums per
+// block (summed in a fixed order by the readers: the result is deterministic)
+__global__ void __launch_bounds__(256)
+    block_norm_kernel(const double *__restrict__ Us, const int64_t *__restrict__ boff,
+                      const int *__restrict__ bdim, double *__restrict__ part) {
+    const int blk = blockIdx.x, sidx = blockIdx.y, n = bdim[blk];
+    __shared__ double red[32];
+    int r0, r1;
+    split_rows(n, sidx, r0, r1);
+    const double *Ub = Us + boff[blk];
+    double acc = 0.0;
+    for (int r = r0; r < r1; r++)
+        for (int side = 0; side < 2; side++) {
+            const int row = side ? n - 1 - r : r;
+            if (side && row == r) continue;   // the middle row of an odd block
+            for (int c = threadIdx.x; c < n; c += blockDim.x) {
+                const double v = Ub[(int64_t)row * n + c];
+                acc += v * v;
+            }
+        }
+    acc = block_sum(acc, red);
+    if (threadIdx.x == 0) part[blk * kClassifySplit + sidx] = acc;
+}
+
+__device__ __forceinline__ double block_norm(const double *part, int blk) {
+    double s = 0.0;
+    for (int k = 0; k < kClassifySplit; k++) s += part[blk * kClassifySplit + k];
+    return sqrt(s);
+}
+
+// Acceptance test, kClassifySplit CTAs per block.  Failing pairs are counted
+// and non-separable ones recorded as edges; the last CTA of a block to finish
+// sets its state (done -> done_stamp = stamp, for write_p_kernel).
 __global__ void __launch_bounds__(kRefineThreads)
-    refine_classify_kernel(const double *__restrict__ T, double *__restrict__ P,
-                           const int64_t *__restrict__ boff, const int *__restrict__ bdim,
-                           int *__restrict__ bstate, const unsigned long long *__restrict__ orth,
-                           int force, double gap_tol, double abs_tol, double *__restrict__ bnorm,
+    refine_classify_kernel(const double *__restrict__ T, const int64_t *__restrict__ boff,
+                           const int *__restrict__ bdim, int *__restrict__ bstate,
+                           const unsigned long long *__restrict__ orth, const double *__restrict__ part,
+                           double gap_tol, double abs_tol, double *__restrict__ bnorm,
+                           int *__restrict__ counts, int *__restrict__ done_stamp, int stamp,
                            int *h_state, int *h_nbad, int *h_nedge, int2 *h_edges) {
-    const int blk = blockIdx.x;
+    const int blk = blockIdx.x, sidx = blockIdx.y;
     const int st_in = bstate[blk];
     if (st_in != kStWork && st_in != kStBlockJacobi) return;   // uniform over the CTA
     const int n = bdim[blk];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
-    __shared__ double red[32];
-    __shared__ double s_nrm;
-    __shared__ int s_bad, s_ne;
+    int *cnt = counts + 3 * blk;   // [0] failing pairs, [1] edges, [2] finished CTAs
+    __shared__ int s_last;
     extern __shared__ double dg[];   // n diagonal entries
-    if (n <= 0) {
-        if (tid == 0) {
-            bstate[blk] = kStDone;
-            h_state[blk] = kStDone;
-            h_nbad[blk] = 0;
-            h_nedge[blk] = 0;
-        }
-        return;
-    }
     const int64_t off = boff[blk];
     const double *Tb = T + off;
-    if (tid == 0) {
-        s_bad = 0;
-        s_ne = 0;
-    }
-    for (int i = tid; i < n; i += blockDim.x) dg[i] = Tb[(int64_t)i * n + i];
-    double fro = 0.0;
-    for (int64_t e = tid; e < (int64_t)n * n; e += blockDim.x) {
-        const double v = Tb[e];
-        fro += v * v;
-    }
-    fro = block_sum(fro, red);
-    if (tid == 0) {
-        s_nrm = sqrt(fro);
-        bnorm[blk] = s_nrm;
-    }
-    __syncthreads();
-    const double nrm = s_nrm;
+    const double nrm = block_norm(part, blk);
     const double atol = abs_tol * nrm, gtol = gap_tol * nrm;
+    for (int i = tid; i < n; i += blockDim.x) dg[i] = Tb[(int64_t)i * n + i];
+    __syncthreads();
+    int r0, r1;
+    split_rows(n, sidx, r0, r1);
     int bad = 0;
     int2 *eb = h_edges + (int64_t)blk * kRefineEdgeCap;
-    for (int i = warp; i < n; i += nwarp) {
+    // rows r0..r1-1 and their partners n-1-r, one warp per row
+    for (int w = warp; w < 2 * (r1 - r0); w += nwarp) {
+        const int r = r0 + (w >> 1);
+        const int i = (w & 1) ? n - 1 - r : r;
+        if ((w & 1) && i == r) continue;
         const double di = dg[i];
         for (int j = i + 1 + lane; j < n; j += 32) {
             const double t = 0.5 * (Tb[(int64_t)i * n + j] + Tb[(int64_t)j * n + i]);
@@ -101,31 +125,58 @@ __global__ void __launch_bounds__(kRefineThreads)
             if (t * t > gtol * delta) {
                 bad++;
                 if (at > kRefineRho * g) {
-                    const int e = atomicAdd(&s_ne, 1);
+                    const int e = atomicAdd(cnt + 1, 1);
                     if (e < kRefineEdgeCap) eb[e] = make_int2(i, j);
                 }
             }
         }
     }
     bad = __reduce_add_sync(0xffffffffu, bad);
-    if (lane == 0 && bad) atomicAdd(&s_bad, bad);
+    if (lane == 0 && bad) atomicAdd(cnt, bad);
+    __threadfence();
     __syncthreads();
-    const int nbad = s_bad;
-    const bool done = nbad == 0 && __longlong_as_double((long long)orth[blk]) <= kRefineOrthDone;
-    if (done) {
-        double *Pb = P + off;
-        for (int64_t e = tid; e < (int64_t)n * n; e += blockDim.x) {
-            const int i = (int)(e / n), j = (int)(e % n);
-            Pb[e] = (i == j) ? fmax(dg[i], 0.0)
-                             : gamma_pq(dg[i], dg[j]) * 0.5 * (Tb[e] + Tb[(int64_t)j * n + i]);
-        }
-    }
+    if (tid == 0) s_last = (atomicAdd(cnt + 2, 1) == kClassifySplit - 1);
+    __syncthreads();
+    if (!s_last) return;
     if (tid == 0) {
-        const int st = done ? kStDone : (force ? kStJacobi : st_in);
+        __threadfence();
+        const int nbad = atomicAdd(cnt, 0), ne = atomicAdd(cnt + 1, 0);
+        const bool done = nbad == 0 && __longlong_as_double((long long)orth[blk]) <= kRefineOrthDone;
+        const int st = done ? kStDone : st_in;
+        if (done) done_stamp[blk] = stamp;
         bstate[blk] = st;
+        bnorm[blk] = nrm;
         h_state[blk] = st;
         h_nbad[blk] = nbad;
-        h_nedge[blk] = s_ne;
+        h_nedge[blk] = ne;
+        cnt[0] = cnt[1] = cnt[2] = 0;   // ready for the next launch
+    }
+}
+
+// P = Gamma o T on the tiles of the blocks accepted by the classify launch
+// with this stamp
+__global__ void __launch_bounds__(256)
+    write_p_kernel(const double *__restrict__ T, double *__restrict__ P,
+                   const int4 *__restrict__ tiles, const int64_t *__restrict__ boff,
+                   const int *__restrict__ bdim, const int *__restrict__ done_stamp, int stamp) {
+    const int4 t = tiles[blockIdx.x];
+    if (done_stamp[t.x] != stamp) return;
+    const int n = bdim[t.x];
+    const int64_t off = boff[t.x];
+    const double *Tb = T + off;
+    double *Pb = P + off;
+    for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
+        const int i = t.y * 64 + e / 64, j = t.z * 64 + e % 64;
+        if (i >= n || j >= n) continue;
+        const double di = Tb[(int64_t)i * n + i];
+        double v;
+        if (i == j) {
+            v = fmax(di, 0.0);
+        } else {
+            const double dj = Tb[(int64_t)j * n + j];
+            v = gamma_pq(di, dj) * 0.5 * (Tb[(int64_t)i * n + j] + Tb[(int64_t)j * n + i]);
+        }
+        Pb[(int64_t)i * n + j] = v;
     }
 }
 

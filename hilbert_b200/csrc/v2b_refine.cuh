@@ -35,13 +35,24 @@ struct ClusterJob {
     int blk, k, moff, qoff;
 };
 
-// acceptance test, pair classification and, for accepted blocks, P = Gamma o T
-__global__ void refine_classify_kernel(const double *__restrict__ T, double *__restrict__ P,
-                                       const int64_t *__restrict__ boff, const int *__restrict__ bdim,
-                                       int *__restrict__ bstate,
-                                       const unsigned long long *__restrict__ orth, int force,
-                                       double gap_tol, double abs_tol, double *__restrict__ bnorm,
-                                       int *h_state, int *h_nbad, int *h_nedge, int2 *h_edges);
+constexpr int kClassifySplit = 16;   // CTAs per block in the acceptance test
+
+// Frobenius norms of the symmetrised blocks as kClassifySplit partial sums each
+__global__ void block_norm_kernel(const double *__restrict__ Us, const int64_t *__restrict__ boff,
+                                  const int *__restrict__ bdim, double *__restrict__ part);
+// acceptance test and pair classification (grid nblk x kClassifySplit)
+__global__ void refine_classify_kernel(const double *__restrict__ T, const int64_t *__restrict__ boff,
+                                       const int *__restrict__ bdim, int *__restrict__ bstate,
+                                       const unsigned long long *__restrict__ orth,
+                                       const double *__restrict__ part, double gap_tol, double abs_tol,
+                                       double *__restrict__ bnorm, int *__restrict__ counts,
+                                       int *__restrict__ done_stamp, int stamp, int *h_state,
+                                       int *h_nbad, int *h_nedge, int2 *h_edges);
+// P = Gamma o T for the blocks accepted under this stamp (GEMM tile grid)
+__global__ void write_p_kernel(const double *__restrict__ T, double *__restrict__ P,
+                               const int4 *__restrict__ tiles, const int64_t *__restrict__ boff,
+                               const int *__restrict__ bdim, const int *__restrict__ done_stamp,
+                               int stamp);
 
 // cyclic Jacobi on each cluster's T[C, C] (at most max_sweeps sweeps; enough
 // sweeps diagonalise it exactly): rows of Qt (k x k) are the eigenvectors,

@@ -147,6 +147,10 @@ struct ProjectPlan {
     int *bstate = nullptr, *h_bstate_up = nullptr;   // device / pinned staging
     unsigned long long *orth = nullptr;
     double *bnorm = nullptr;
+    double *norm_part = nullptr;     // kClassifySplit partial squared norms per block
+    int *cls_counts = nullptr;       // per block: failing pairs, edges, finished CTAs
+    int *done_stamp = nullptr;       // classify launch that accepted the block
+    int stamp = 0;
     double *Vsave = nullptr, *Tsave = nullptr;   // the call's starting basis and T
     int *h_state = nullptr, *h_nbad = nullptr, *h_nedge = nullptr;   // mapped host memory
     int2 *h_edges = nullptr;
@@ -254,6 +258,11 @@ struct ProjectPlan {
         bstate = dalloc<int>(nblk);
         orth = dalloc<unsigned long long>(nblk);
         bnorm = dalloc<double>(nblk);
+        norm_part = dalloc<double>((size_t)nblk * v2b::kClassifySplit);
+        cls_counts = dalloc<int>(3 * (size_t)nblk);
+        done_stamp = dalloc<int>(nblk);
+        V2B_CK(cudaMemset(cls_counts, 0, 3 * sizeof(int) * nblk));
+        V2B_CK(cudaMemset(done_stamp, 0xff, sizeof(int) * nblk));
         Vsave = dalloc<double>(total);
         Tsave = dalloc<double>(total);
         V2B_CK(cudaMallocHost(&h_bstate_up, std::max(nblk, 1) * sizeof(int)));
@@ -298,7 +307,8 @@ struct ProjectPlan {
         for (void *q : {(void *)boff, (void *)rot_off, (void *)bdim, (void *)counters, (void *)tiles,
                         (void *)rot, (void *)Vt, (void *)Vt2, (void *)Us, (void *)W, (void *)T,
                         (void *)P, (void *)rec_b, (void *)norm_b, (void *)sub_boff, (void *)sub_roff,
-                        (void *)sub_bdim, (void *)bstate, (void *)orth, (void *)bnorm, (void *)Vsave,
+                        (void *)sub_bdim, (void *)bstate, (void *)orth, (void *)bnorm, (void *)norm_part,
+                        (void *)cls_counts, (void *)done_stamp, (void *)Vsave,
                         (void *)Tsave, (void *)arena, (void *)crec, (void *)cnorm, (void *)Tc,
                         (void *)Pc, (void *)bj_dev, (void *)bj_on,
                         (void *)rowbase, (void *)lam, (void *)Qt})
@@ -664,6 +674,10 @@ struct ProjectPlan {
         V2B_CK(cudaMemsetAsync(orth, 0, nblk * sizeof(unsigned long long), s));
         V2B_CK(cudaMemcpyAsync(Vsave, Vt, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
         V2B_CK(cudaMemcpyAsync(Tsave, T, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        // ||T||_F = ||sym(U)||_F for an orthonormal Vt: the tests use the block norms of Us
+        block_norm_kernel<<<dim3(nblk, kClassifySplit), 256, 0, s>>>(Us, boff, bdim, norm_part);
+        V2B_CK(cudaGetLastError());
+        launches++;
         std::vector<char> changed(nblk, 0);
         std::vector<int> newton(nblk, 0), sweeps(nblk, 0);
         auto restore = [&](int b) {
@@ -687,10 +701,13 @@ struct ProjectPlan {
                     gemm(kGemmNNStore, Vt, W, T, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
                 }
             }
-            refine_classify_kernel<<<nblk, kRefineThreads, classify_smem, s>>>(
-                T, P, boff, bdim, bstate, orth, 0, gap_tol, abs_tol, bnorm, d_state, d_nbad, d_nedge, d_edges);
+            ++stamp;
+            refine_classify_kernel<<<dim3(nblk, kClassifySplit), kRefineThreads, classify_smem, s>>>(
+                T, boff, bdim, bstate, orth, norm_part, gap_tol, abs_tol, bnorm, cls_counts, done_stamp,
+                stamp, d_state, d_nbad, d_nedge, d_edges);
+            write_p_kernel<<<ntiles, 256, 0, s>>>(T, P, tiles, boff, bdim, done_stamp, stamp);
             V2B_CK(cudaGetLastError());
-            launches++;
+            launches += 2;
             V2B_CK(cudaStreamSynchronize(s));
             refine_passes++;
             std::vector<std::vector<int>> members;   // clusters of the Newton-mode blocks
