@@ -82,6 +82,35 @@ __device__ __forceinline__ double warp_row(const uint32_t *__restrict__ ent, uin
     return warp_sum(acc);
 }
 
+// One SELL slice per warp: lane l forms row perm[32 s + l] of the operator
+// applied to x (RBP: to r + beta p, formed per operand as in the stored
+// update), summing its entries in stored order (the group flag splits the
+// sum as packed_row does).  Table loads stream (evict first) so the vectors
+// stay in L2.
+template <bool RBP>
+__device__ __forceinline__ double sell_row(const SellOp &S, int64_t sl, int lane,
+                                           const double *__restrict__ x, const double *__restrict__ p,
+                                           double beta, const double *pal, uint32_t &row) {
+    const int64_t pos = sl * 32 + lane;
+    row = __ldcs(S.perm + pos);
+    const int len = __ldcs(S.len + pos);
+    const uint32_t base = __ldcs(S.off + sl) + lane;
+    double acc0 = 0.0, acc1 = 0.0;
+    bool grp = false;
+#pragma unroll 4
+    for (int k = 0; k < len; k++) {
+        const uint32_t w = __ldcs(S.ent + base + 32u * k);
+        const uint32_t c = w & kDevColMask;
+        double xv = __ldg(x + c);
+        if (RBP) xv = __dadd_rn(xv, __dmul_rn(beta, __ldg(p + c)));
+        const double v = __dmul_rn(pal[(w >> 27) & 15u], xv);
+        grp = grp || (w >> 31);
+        if (grp) acc1 = __dadd_rn(acc1, v);
+        else acc0 = __dadd_rn(acc0, v);
+    }
+    return grp ? __dadd_rn(acc0, acc1) : acc0;
+}
+
 // ------------------------------------------------------------------ CG
 // Solves (A A^T) y = rhs with rhs = A(c - z) + mu (b - A x), warm-started from
 // y.  Three grid barriers per iteration:
@@ -90,7 +119,9 @@ __device__ __forceinline__ double warp_row(const uint32_t *__restrict__ ent, uin
 //   3. y += alpha p_new, r -= alpha q, partial r.r
 // The p.q and r.r partials live in separate arrays: a block that has passed
 // barrier 2 writes its r.r partial while slower blocks may still be summing
-// the p.q partials.
+// the p.q partials.  Operator rows of up to kCgLongRow entries are applied
+// from the sliced-ELL copies (one warp per 32-row slice), longer rows by a
+// warp each from the CSR tables.
 __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgParams P) {
     __shared__ double palA[16], palT[16];
     __shared__ double red[32];
@@ -105,16 +136,41 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgParams P) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int nb = gridDim.x;
 
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = gtid >> 5, nwarps = stride >> 5;
+
     // r = rhs - A A^T y
-    for (int64_t i = gtid; i < P.np; i += stride)
-        P.t[i] = packed_row(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), P.y, palT);
+    for (int64_t sl = gwarp; sl < P.st.nslices; sl += nwarps) {
+        uint32_t row;
+        const double v = sell_row<false>(P.st, sl, lane, P.y, nullptr, 0.0, palT, row);
+        if (row != 0xffffffffu) P.t[row] = v;
+    }
+    for (int64_t w = gwarp; w < P.n_long_t; w += nwarps) {
+        const int64_t i = __ldg(P.long_t + w);
+        const double v = warp_row(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), P.y, nullptr, 0.0,
+                                  palT, lane);
+        if (lane == 0) P.t[i] = v;
+    }
     if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
     double loc = 0.0;
-    for (int64_t j = gtid; j < P.nd; j += stride) {
-        const double rhs = P.Acz[j] + P.mu * (P.b[j] - P.Ax[j]);
-        const double v = rhs - packed_row(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), P.t, palA);
-        P.r[j] = v;
-        loc += v * v;
+    for (int64_t sl = gwarp; sl < P.sa.nslices; sl += nwarps) {
+        uint32_t row;
+        const double av = sell_row<false>(P.sa, sl, lane, P.t, nullptr, 0.0, palA, row);
+        if (row != 0xffffffffu) {
+            const double v = P.Acz[row] + P.mu * (P.b[row] - P.Ax[row]) - av;
+            P.r[row] = v;
+            loc += v * v;
+        }
+    }
+    for (int64_t w = gwarp; w < P.n_long_a; w += nwarps) {
+        const int64_t j = __ldg(P.long_a + w);
+        const double av = warp_row(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), P.t, nullptr, 0.0,
+                                   palA, lane);
+        if (lane == 0) {
+            const double v = P.Acz[j] + P.mu * (P.b[j] - P.Ax[j]) - av;
+            P.r[j] = v;
+            loc += v * v;
+        }
     }
     double s = block_sum(loc, red);
     if (threadIdx.x == 0) P.partials[blockIdx.x] = s;
@@ -126,12 +182,11 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgParams P) {
     const double *pold = P.r;   // first direction p = r (beta = 0)
     double *pnew = P.p0;
     bool done = !(sqrt(rs) >= P.tol);
-    const int lane = threadIdx.x & 31;
-    const int64_t gwarp = gtid >> 5, nwarps = stride >> 5;
     while (!done && it < P.maxit) {
-        for (int64_t i = gtid; i < P.np; i += stride) {
-            const uint32_t b = __ldg(P.t_rp + i), e = __ldg(P.t_rp + i + 1);
-            if (e - b <= kCgLongRow) P.t[i] = packed_row_rbp(P.t_ent, b, e, P.r, pold, beta, palT);
+        for (int64_t sl = gwarp; sl < P.st.nslices; sl += nwarps) {
+            uint32_t row;
+            const double v = sell_row<true>(P.st, sl, lane, P.r, pold, beta, palT, row);
+            if (row != 0xffffffffu) P.t[row] = v;
         }
         for (int64_t w = gwarp; w < P.n_long_t; w += nwarps) {
             const int64_t i = __ldg(P.long_t + w);
@@ -153,12 +208,13 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgParams P) {
                 loc += pnew[j] * q;
             }
         }
-        for (int64_t j = gtid; j < P.nd; j += stride) {
-            const uint32_t b = __ldg(P.a_rp + j), e = __ldg(P.a_rp + j + 1);
-            if (e - b > kCgLongRow) continue;
-            const double q = packed_row(P.a_ent, b, e, P.t, palA);
-            P.q[j] = q;
-            loc += pnew[j] * q;
+        for (int64_t sl = gwarp; sl < P.sa.nslices; sl += nwarps) {
+            uint32_t row;
+            const double q = sell_row<false>(P.sa, sl, lane, P.t, nullptr, 0.0, palA, row);
+            if (row != 0xffffffffu) {
+                P.q[row] = q;
+                loc += pnew[row] * q;
+            }
         }
         s = block_sum(loc, red);
         if (threadIdx.x == 0) P.partials[nb + blockIdx.x] = s;

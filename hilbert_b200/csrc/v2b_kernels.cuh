@@ -10,7 +10,20 @@ namespace v2b {
 
 constexpr int kSpmvThreads = 256;
 constexpr int kCgThreads = 512;
-constexpr uint32_t kCgLongRow = 12;   // rows with more entries get a whole warp inside CG
+constexpr uint32_t kCgLongRow = 32;   // rows with more entries get a whole warp inside CG
+
+// Sliced ELL copy of an operator for the CG kernel (SELL-C-sigma, C = 32):
+// rows of at most kCgLongRow entries, sorted by length inside windows of
+// kSellSigma rows, in slices of 32 rows stored column-major (entry k of the
+// slice's lane l at off[s] + 32 k + l), perm = original row (0xffffffff on
+// padding lanes), len = its entry count.  A warp handles a slice: its loads
+// are coalesced and independent of one another.
+constexpr int kSellSigma = 8192;
+struct SellOp {
+    const uint32_t *ent, *perm, *off;
+    const uint8_t *len;
+    int64_t nslices;
+};
 constexpr int kJacobiThreads = 512;
 constexpr int kJacobiMaxDim = 160;     // np*np doubles + rotations must fit in 227 KB
 constexpr int kStatsBlocks = 256;
@@ -24,6 +37,7 @@ struct CgParams {
     const uint32_t *t_rp, *t_ent;   // A^T (rows = primal variables)
     const int64_t *long_a, *long_t; // rows longer than kCgLongRow (warp per row)
     int64_t n_long_a, n_long_t;
+    SellOp sa, st;                  // the other rows of A and A^T
     Palette palA, palT;
     int64_t np, nd;
     const double *Ax, *Acz, *b;     // rhs = Acz + mu (b - Ax)

@@ -79,6 +79,11 @@ struct DeviceOp {
     int64_t nrows = 0, n_long = 0;
     size_t nnz = 0;
     v2b::Palette pal{};
+    // sliced-ELL copy of the other rows, for the CG kernel
+    uint32_t *sell_ent = nullptr, *sell_perm = nullptr, *sell_off = nullptr;
+    uint8_t *sell_len = nullptr;
+    int64_t nslices = 0;
+
     void upload(const v2b::PackedOperator &op) {
         nrows = op.nrows;
         nnz = op.entries.size();
@@ -93,12 +98,72 @@ struct DeviceOp {
         n_long = (int64_t)lr.size();
         long_rows = dalloc<int64_t>(lr.size());
         if (n_long) V2B_CK(cudaMemcpy(long_rows, lr.data(), lr.size() * 8, cudaMemcpyHostToDevice));
+        build_sell(op);
+    }
+
+    // SELL-C-sigma with C = 32: inside each window of kSellSigma rows the
+    // short rows are sorted by length (longest first, stable), cut into
+    // slices of 32 (the window's last slice padded with empty lanes) and
+    // stored column-major at the slice's width
+    void build_sell(const v2b::PackedOperator &op) {
+        std::vector<uint32_t> e, perm, off;
+        std::vector<uint8_t> len;
+        std::vector<std::pair<uint32_t, uint32_t>> w;   // (length, row)
+        for (int64_t w0 = 0; w0 < nrows; w0 += v2b::kSellSigma) {
+            const int64_t w1 = std::min<int64_t>(nrows, w0 + v2b::kSellSigma);
+            w.clear();
+            for (int64_t r = w0; r < w1; r++) {
+                const uint32_t L = op.row_ptr[r + 1] - op.row_ptr[r];
+                if (L <= v2b::kCgLongRow) w.push_back({L, (uint32_t)r});
+            }
+            std::stable_sort(w.begin(), w.end(), [](const std::pair<uint32_t, uint32_t> &a,
+                                                    const std::pair<uint32_t, uint32_t> &b) {
+                return a.first > b.first;
+            });
+            for (size_t s0 = 0; s0 < w.size(); s0 += 32) {
+                const size_t cnt = std::min<size_t>(32, w.size() - s0);
+                const uint32_t width = w[s0].first;
+                off.push_back((uint32_t)e.size());
+                for (uint32_t k = 0; k < width; k++)
+                    for (size_t l = 0; l < 32; l++) {
+                        uint32_t v = 0;
+                        if (l < cnt && k < w[s0 + l].first) v = op.entries[op.row_ptr[w[s0 + l].second] + k];
+                        e.push_back(v);
+                    }
+                for (size_t l = 0; l < 32; l++) {
+                    perm.push_back(l < cnt ? w[s0 + l].second : 0xffffffffu);
+                    len.push_back(l < cnt ? (uint8_t)w[s0 + l].first : 0);
+                }
+            }
+        }
+        nslices = (int64_t)off.size();
+        off.push_back((uint32_t)e.size());
+        sell_ent = dalloc<uint32_t>(e.size());
+        sell_perm = dalloc<uint32_t>(perm.size());
+        sell_len = dalloc<uint8_t>(len.size());
+        sell_off = dalloc<uint32_t>(off.size());
+        if (!e.empty()) V2B_CK(cudaMemcpy(sell_ent, e.data(), e.size() * 4, cudaMemcpyHostToDevice));
+        if (!perm.empty()) {
+            V2B_CK(cudaMemcpy(sell_perm, perm.data(), perm.size() * 4, cudaMemcpyHostToDevice));
+            V2B_CK(cudaMemcpy(sell_len, len.data(), len.size(), cudaMemcpyHostToDevice));
+        }
+        V2B_CK(cudaMemcpy(sell_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice));
+    }
+    v2b::SellOp sell() const {
+        v2b::SellOp s;
+        s.ent = sell_ent;
+        s.perm = sell_perm;
+        s.off = sell_off;
+        s.len = sell_len;
+        s.nslices = nslices;
+        return s;
     }
     void release() {
-        cudaFree(rp);
-        cudaFree(ent);
-        cudaFree(long_rows);
-        rp = ent = nullptr;
+        for (void *p : {(void *)rp, (void *)ent, (void *)long_rows, (void *)sell_ent, (void *)sell_perm,
+                        (void *)sell_off, (void *)sell_len})
+            cudaFree(p);
+        rp = ent = sell_ent = sell_perm = sell_off = nullptr;
+        sell_len = nullptr;
         long_rows = nullptr;
     }
 };
@@ -1004,6 +1069,7 @@ struct v2b_problem {
         P.a_rp = A.rp; P.a_ent = A.ent; P.t_rp = AT.rp; P.t_ent = AT.ent;
         P.long_a = A.long_rows; P.long_t = AT.long_rows;
         P.n_long_a = A.n_long; P.n_long_t = AT.n_long;
+        P.sa = A.sell(); P.st = AT.sell();
         P.palA = A.pal; P.palT = AT.pal;
         P.np = prob.n_primal; P.nd = prob.n_dual;
         P.Ax = Ax; P.Acz = Acz; P.b = b; P.mu = mu;
