@@ -83,6 +83,9 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="df20", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip the solve on the plain FP64 path (selective Jacobi on every block "
+                         "every iteration) that a 1-GPU run times for comparison")
     ap.add_argument("--max-outer", type=int, default=0,
                     help="cap the outer iterations of each solve (profiling runs; the line then "
                          "reports a capped, not a converged, solve)")
@@ -341,6 +344,26 @@ def run_b200(args, w):
         e2e_times.append(time.perf_counter() - t0)
     te2e = max_over_ranks(max(e2e_times), world)
 
+    # the plain FP64 path on the same problem (1 GPU only): every block fully
+    # diagonalised by selective Jacobi every iteration, as libsdp does with LAPACK
+    plain = None
+    if world == 1 and not args.no_plain:
+        p.set_projection_mode("jacobi")
+        dx.copy_(dx0)
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        st_plain = p.solve_device(dx, db, dc, opts)
+        ev1.record()
+        torch.cuda.synchronize()
+        e_plain = float(c @ dx.cpu().numpy())
+        p.set_projection_mode("refine")
+        plain = {"seconds": ev0.elapsed_time(ev1) / 1e3, "energy": e_plain,
+                 "outer_iterations": st_plain["oiter"], "cg_iterations": st_plain["iiter"],
+                 "converged": st_plain["converged"]}
+
     # roofline: cg_kernel, the largest single kernel (the projection is a
     # sequence of GEMM-tile, test and Jacobi kernels; its FLOP rate is reported
     # beside it)
@@ -402,6 +425,9 @@ def run_b200(args, w):
                            "fp64_energy": FP64_ENERGY[args.workload][0],
                            "fp64_energy_source": FP64_ENERGY[args.workload][1],
                            "abs_dE_vs_fp64": abs(energy - FP64_ENERGY[args.workload][0]),
+                           "plain_fp64_path": plain,
+                           "speedup_vs_plain_fp64": (plain["seconds"] / t) if plain else None,
+                           "abs_dE_vs_plain_fp64": abs(energy - plain["energy"]) if plain else None,
                            "projection_refine_counts": p.refine_counts(),
                            "max_outer_cap": args.max_outer or None},
                 "e2e": {"value": te2e, "unit": "s", "h2d_bytes_per_step": 8 * (2 * npr + ndu),

@@ -256,6 +256,7 @@ struct ProjectPlan {
     long fb_edges = 0, fb_passes = 0;  // why refined blocks went to Jacobi
     bool fresh = true;
     bool built = false;
+    int mode = 0;   // 0: warm refinement, 1: selective Jacobi on every block, every call
     long calls = 0, since_reset = 0;
     double abs_tol = 1e-14, gap_tol = 1e-13;
 
@@ -915,7 +916,8 @@ struct ProjectPlan {
         std::vector<int> st(nblk);
         for (int b = 0; b < nblk; b++)
             st[b] = dims[b] == 0 ? kStDone
-                    : dims[b] < kRefineMinDim ? kStJacobi : (cold ? kStBlockJacobi : kStWork);
+                    : (mode == 1 || dims[b] < kRefineMinDim) ? kStJacobi
+                    : (cold ? kStBlockJacobi : kStWork);
         if (staged_pending) V2B_CK(cudaEventSynchronize(staged));
         upload_states(s, st);
         refine(st, s, launches);
@@ -1547,6 +1549,13 @@ int v2b_problem_projection_counts(const v2b_problem *p, long *calls, long *rotat
     });
 }
 
+int v2b_problem_set_projection_mode(v2b_problem *p, int mode) {
+    return guarded([&] {
+        if (!p || mode < 0 || mode > 1) throw std::invalid_argument("set_projection_mode: bad argument");
+        p->plan.mode = mode;
+        return V2B_OK;
+    });
+}
 int v2b_problem_refine_counts(const v2b_problem *p, long *counts, int n) {
     return guarded([&] {
         if (!p || !counts || n < 0) throw std::invalid_argument("refine_counts: bad argument");

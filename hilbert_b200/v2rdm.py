@@ -256,6 +256,11 @@ class V2RDMProblem:
             out.append(nnz.value)
         return tuple(out)
 
+    def set_projection_mode(self, mode):
+        """"refine" (default: warm refinement) or "jacobi" (selective Jacobi on
+        every block every iteration: the plain FP64 path)"""
+        check(self._lib.v2b_problem_set_projection_mode(self._h, {"refine": 0, "jacobi": 1}[mode]))
+
     REFINE_COUNTS = ("accepted", "jacobi", "passes", "clusters", "large_clusters",
                      "fallback_edges", "fallback_passes", "block_jacobi_sweeps")
 

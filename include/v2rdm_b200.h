@@ -182,6 +182,11 @@ int v2b_problem_projection_counts(const v2b_problem *p, long *calls, long *rotat
  * non-separable pairs, [6] blocks handed to the Jacobi kernels after their
  * passes or sweeps ran out, [7] block-Jacobi sweeps run. */
 int v2b_problem_refine_counts(const v2b_problem *p, long *counts, int n);
+/* No counterpart in the reference.  Projection method of the device solve:
+ * 0 (default) warm refinement with block-Jacobi and Jacobi fallbacks; 1 the
+ * plain path, selective Jacobi on every block in every iteration (the
+ * per-iteration full eigendecomposition libsdp performs, in FP64). */
+int v2b_problem_set_projection_mode(v2b_problem *p, int mode);
 
 /* ---- 3. allocation-free projection ------------------------------------------ */
 
