@@ -18,7 +18,7 @@ Problem make_problem(const ProblemSpec &spec) {
     if (spec.nmo < 1 || spec.nalpha < 0 || spec.nbeta < 0 || spec.nalpha > spec.nmo ||
         spec.nbeta > spec.nmo)
         throw std::invalid_argument("invalid orbital / electron counts");
-    if (spec.positivity < POS_D || spec.positivity > POS_DQG)
+    if (spec.positivity < POS_D || spec.positivity > POS_DQGT2)
         throw std::invalid_argument("unsupported POSITIVITY");
     Problem p;
     p.spec = spec;
@@ -26,8 +26,9 @@ Problem make_problem(const ProblemSpec &spec) {
     p.n = n;
     p.gab = n * n;
     p.gaa = n * (n - 1) / 2;
-    p.q2 = spec.positivity == POS_DQ || spec.positivity == POS_DQG;
-    p.g2 = spec.positivity == POS_DG || spec.positivity == POS_DQG;
+    p.q2 = spec.positivity == POS_DQ || spec.positivity == POS_DQG || spec.positivity == POS_DQGT2;
+    p.g2 = spec.positivity == POS_DG || spec.positivity == POS_DQG || spec.positivity == POS_DQGT2;
+    p.t2 = spec.positivity == POS_DQGT2;   // v2rdm_solver.cc:4106-4109
     p.mult = spec.hubbard_multiplicity ? 2 * (spec.nalpha - spec.nbeta) + 1
                                        : (spec.nalpha - spec.nbeta) + 1;
 
@@ -81,6 +82,21 @@ Problem make_problem(const ProblemSpec &spec) {
         add_block(p.g2ba, p.gab);
         add_block(p.g2aa, 2 * p.gab);
     }
+    if (p.t2) {   // v2rdm_solver.cc:3879-3906
+        p.trip_aba = n * n * n;
+        for (int i = 0; i < n; i++)
+            for (int j = i + 1; j < n; j++)
+                for (int k = 0; k < n; k++) {
+                    p.bas_aab.push_back(i);
+                    p.bas_aab.push_back(j);
+                    p.bas_aab.push_back(k);
+                }
+        p.trip_aab = (int)(p.bas_aab.size() / 3);
+        add_block(p.t2aaa, p.trip_aab + p.trip_aba);
+        add_block(p.t2bbb, p.trip_aab + p.trip_aba);
+        add_block(p.t2aab, p.trip_aab);
+        add_block(p.t2bba, p.trip_aab);
+    }
     p.n_primal = off;
 
     const int64_t gab2 = (int64_t)p.gab * p.gab, gaa2 = (int64_t)p.gaa * p.gaa, n2 = (int64_t)n * n;
@@ -92,6 +108,10 @@ Problem make_problem(const ProblemSpec &spec) {
     }
     if (p.q2) d += gab2 + 2 * gaa2;
     if (p.g2) d += 6 * gab2;
+    if (p.t2) {
+        const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
+        d += 2 * aab * aab + 2 * big * big;
+    }
     p.n_dual = d;
     if (p.n_primal > (int64_t)kColMask || p.n_dual > (int64_t)kColMask)
         throw std::invalid_argument("problem too large for 27-bit packed column indices");
@@ -199,6 +219,140 @@ void build_c_external(const Problem &p, const double *h, const double *g, double
     }
 }
 
+// ------------------------------------------------------------------ T2
+// The T2 rows (t2.cc:1236-1843, T2_constraints_Au_slow, C1): one row per
+// element (I, J) of the T2aab, T2bba, T2aaa and T2bbb blocks, in that order of
+// dual rows, each -T2(I, J) + delta-masked D2 and D1 terms with coefficients
+// +-1.  f(dual_row, t2_col, sub, cols, coefs, nterms) receives a row's D terms
+// in the order the reference adds them, rows in the reference's loop order
+// (which is also the order T2_constraints_ATu_slow scatters them, t2.cc:3376).
+// sub numbers the sub-blocks 0 aab, 1 bba, 2-5 aaa (aaa/aaa, aaa/abb, abb/aaa,
+// abb/abb), 6-9 bbb (bbb/bbb, bbb/baa, baa/bbb, baa/baa).
+namespace {
+constexpr int kT2AaaAbb = 3;
+
+template <class F>
+void t2_rows(const Problem &p, int64_t off, F &&f) {
+    const int N = p.n, gab = p.gab, gaa = p.gaa, aab = p.trip_aab, aba = p.trip_aba;
+    const int64_t big = (int64_t)aab + aba;
+    int64_t cols[8];
+    double coef[8];
+    int nt = 0;
+    auto add = [&](int64_t c, double v) {
+        cols[nt] = c;
+        coef[nt] = v;
+        nt++;
+    };
+    auto trip = [&](int idx, bool is_aab, int &i, int &j, int &k) {
+        if (is_aab) {
+            i = p.bas_aab[3 * idx];
+            j = p.bas_aab[3 * idx + 1];
+            k = p.bas_aab[3 * idx + 2];
+        } else {
+            i = idx / (N * N);
+            j = (idx / N) % N;
+            k = idx % N;
+        }
+    };
+    auto d2aa_t = [&](int64_t base, int a, int b, int c, int d) { return base + (int64_t)p.iaa(a, b) * gaa + p.iaa(c, d); };
+    auto d2ab_t = [&](int a, int b, int c, int d) { return p.d2ab + (int64_t)p.iab(a, b) * gab + p.iab(c, d); };
+    // sign of the aa geminal terms: s = (n > j ? -1 : 1) (k > m ? -1 : 1)
+    auto sgn = [](int a, int b, int c, int d) { return (a > b ? -1.0 : 1.0) * (c > d ? -1.0 : 1.0); };
+
+    // T2aab (t2.cc:1239-1302) and T2bba (t2.cc:1305-1368)
+    for (int spin = 0; spin < 2; spin++) {
+        const int64_t t2 = spin ? p.t2bba : p.t2aab;
+        const int64_t d2same = spin ? p.d2bb : p.d2aa, d1other = spin ? p.d1a : p.d1b;
+        for (int ijk = 0; ijk < aab; ijk++) {
+            int i, j, k;
+            trip(ijk, true, i, j, k);
+            for (int lmn = 0; lmn < aab; lmn++) {
+                int l, m, n;
+                trip(lmn, true, l, m, n);
+                nt = 0;
+                if (k == n) add(d2aa_t(d2same, i, j, l, m), 1.0);
+                if (j == m && i == l) add(d1other + (int64_t)n * N + k, 1.0);
+                if (j == l && i == m) add(d1other + (int64_t)n * N + k, -1.0);
+                if (spin == 0) {
+                    if (i == l) add(d2ab_t(j, n, m, k), -1.0);
+                    if (j == l) add(d2ab_t(i, n, m, k), 1.0);
+                    if (i == m) add(d2ab_t(j, n, l, k), 1.0);
+                    if (j == m) add(d2ab_t(i, n, l, k), -1.0);
+                } else {
+                    if (i == l) add(d2ab_t(n, j, k, m), -1.0);
+                    if (j == l) add(d2ab_t(n, i, k, m), 1.0);
+                    if (i == m) add(d2ab_t(n, j, k, l), 1.0);
+                    if (j == m) add(d2ab_t(n, i, k, l), -1.0);
+                }
+                const int64_t e = (int64_t)ijk * aab + lmn;
+                f(off + e, t2 + e, spin, cols, coef, nt);
+            }
+        }
+        off += (int64_t)aab * aab;
+    }
+    // big blocks T2aaa (t2.cc:1371-1601) and T2bbb (t2.cc:1604-1840)
+    for (int spin = 0; spin < 2; spin++) {
+        const int64_t t2 = spin ? p.t2bbb : p.t2aaa;
+        const int64_t d2s = spin ? p.d2bb : p.d2aa, d2o = spin ? p.d2aa : p.d2bb;
+        const int64_t d1s = spin ? p.d1b : p.d1a, d1o = spin ? p.d1a : p.d1b;
+        for (int sb = 0; sb < 4; sb++) {
+            const bool rowaab = sb < 2, colaab = (sb % 2) == 0;
+            const int nr = rowaab ? aab : aba, nc = colaab ? aab : aba;
+            for (int ijk = 0; ijk < nr; ijk++) {
+                int i, j, k;
+                trip(ijk, rowaab, i, j, k);
+                for (int lmn = 0; lmn < nc; lmn++) {
+                    int l, m, n;
+                    trip(lmn, colaab, l, m, n);
+                    nt = 0;
+                    if (sb == 0) {   // aaa/aaa, bbb/bbb
+                        if (k == n) add(d2aa_t(d2s, i, j, l, m), 1.0);
+                        if (j == m && i == l) add(d1s + (int64_t)n * N + k, 1.0);
+                        if (j == l && i == m) add(d1s + (int64_t)n * N + k, -1.0);
+                        if (i == l && n != j && k != m) add(d2aa_t(d2s, n, j, k, m), -sgn(n, j, k, m));
+                        if (j == l && n != i && k != m) add(d2aa_t(d2s, n, i, k, m), sgn(n, i, k, m));
+                        if (i == m && n != j && k != l) add(d2aa_t(d2s, n, j, k, l), sgn(n, j, k, l));
+                        if (j == m && n != i && k != l) add(d2aa_t(d2s, n, i, k, l), -sgn(n, i, k, l));
+                    } else if (sb == 1) {   // aaa/abb, bbb/baa
+                        if (spin == 0) {
+                            if (i == l) add(d2ab_t(j, n, k, m), 1.0);
+                            if (j == l) add(d2ab_t(i, n, k, m), -1.0);
+                        } else {
+                            if (i == l) add(d2ab_t(n, j, m, k), 1.0);
+                            if (j == l) add(d2ab_t(n, i, m, k), -1.0);
+                        }
+                    } else if (sb == 2) {   // abb/aaa, baa/bbb
+                        if (spin == 0) {
+                            if (i == l) add(d2ab_t(n, j, m, k), 1.0);
+                            if (i == m) add(d2ab_t(n, j, l, k), -1.0);
+                        } else {
+                            if (i == l) add(d2ab_t(j, n, k, m), 1.0);
+                            if (i == m) add(d2ab_t(j, n, k, l), -1.0);
+                        }
+                    } else {   // abb/abb, baa/baa
+                        if (spin == 0) {
+                            if (k == n) add(d2ab_t(i, j, l, m), 1.0);
+                            if (j == m && i == l) add(d1o + (int64_t)n * N + k, 1.0);
+                            if (i == l && n != j && k != m) add(d2aa_t(d2o, n, j, k, m), -sgn(n, j, k, m));
+                            if (j == m) add(d2ab_t(i, n, l, k), -1.0);
+                        } else {
+                            if (k == n) add(d2ab_t(j, i, m, l), 1.0);
+                            if (j == m && i == l) add(d1o + (int64_t)n * N + k, 1.0);
+                            if (i == l && n != j && k != m) add(d2aa_t(d2o, n, j, k, m), -sgn(n, j, k, m));
+                            if (j == m) add(d2ab_t(n, i, k, l), -1.0);
+                        }
+                    }
+                    const int64_t I = rowaab ? ijk : aab + ijk, J = colaab ? lmn : aab + lmn;
+                    const int64_t e = I * big + J;
+                    f(off + e, t2 + e, 2 + 4 * spin + sb, cols, coef, nt);
+                }
+            }
+        }
+        off += big * big;
+    }
+}
+}  // namespace
+
 void guess_random(const Problem &p, double *x) {
     // v2rdm_solver.cc:1799-1806 (C library rand() seeded with 0)
     srand(0);
@@ -299,6 +453,13 @@ void guess_hf(const Problem &p, double *x) {
                 x[p.g2aa + (gab + ij) * w + kl] = 0.0 + x[p.d2ab + (int64_t)p.iab(l, i) * gab + p.iab(k, j)];
             }
         }
+    }
+    if (p.t2) {   // t2.cc:1845-2452: each element from its row's D terms (the aaa/abb part zero)
+        t2_rows(p, 0, [&](int64_t, int64_t t2c, int sub, const int64_t *cols, const double *coef, int nt) {
+            double dum = 0.0;
+            for (int q = 0; q < nt; q++) dum += coef[q] * x[cols[q]];
+            x[t2c] = sub == kT2AaaAbb ? 0.0 : dum;
+        });
     }
 }
 
@@ -601,6 +762,14 @@ void visit_A(const Problem &p, S &s) {
         }
         off += 4 * (int64_t)gab * gab;
     }
+    if (p.t2) {   // t2.cc:1236-1843
+        t2_rows(p, off, [&](int64_t row, int64_t t2c, int, const int64_t *cols, const double *coef, int nt) {
+            s.t(row, t2c, -1.0);
+            for (int q = 0; q < nt; q++) s.t(row, cols[q], coef[q]);
+        });
+        const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
+        off += 2 * aab * aab + 2 * big * big;
+    }
     if (off != p.n_dual) throw std::logic_error("A emitter row count mismatch");
 }
 
@@ -887,6 +1056,14 @@ void visit_AT(const Problem &p, S &s) {
             }
         }
         off += 4 * (int64_t)gab * gab;
+    }
+    if (p.t2) {   // t2.cc:3376-3966 scatters in the same loop order as the A rows
+        t2_rows(p, off, [&](int64_t row, int64_t t2c, int, const int64_t *cols, const double *coef, int nt) {
+            s.t(t2c, row, -1.0);
+            for (int q = 0; q < nt; q++) s.t(cols[q], row, coef[q]);
+        });
+        const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
+        off += 2 * aab * aab + 2 * big * big;
     }
     if (off != p.n_dual) throw std::logic_error("A^T emitter row count mismatch");
 }

@@ -422,10 +422,13 @@ def block_layout(nmo, nalpha, nbeta, positivity="DQG", constrain_spin=True):
     if constrain_spin:
         blocks.append(("d200", gab if nalpha == nbeta else 2 * gab))
     blocks += [("d1a", n), ("d1b", n), ("q1a", n), ("q1b", n)]
-    if pos in ("DQ", "DQG"):
+    if pos in ("DQ", "DQG", "DQGT2"):
         blocks += [("q2ab", gab), ("q2aa", gaa), ("q2bb", gaa)]
-    if pos in ("DG", "DQG"):
+    if pos in ("DG", "DQG", "DQGT2"):
         blocks += [("g2ab", gab), ("g2ba", gab), ("g2aa", 2 * gab)]
+    if pos == "DQGT2":
+        aab, aba = n * (n - 1) // 2 * n, n ** 3
+        blocks += [("t2aaa", aab + aba), ("t2bbb", aab + aba), ("t2aab", aab), ("t2bba", aab)]
     return blocks
 
 

@@ -40,6 +40,7 @@ extern "C" {
 #define V2B_POSITIVITY_DQ  1
 #define V2B_POSITIVITY_DG  2
 #define V2B_POSITIVITY_DQG 3
+#define V2B_POSITIVITY_DQGT2 4   /* DQG + T2 (t2.cc:1236-1843, 3376-3966) */
 
 /* libsdp::SDPOptions as hilbert fills it (src/v2rdm_casscf/v2rdm_solver.cc:426-431) */
 typedef struct {

@@ -27,6 +27,8 @@ CASES = [
     ("ext4_dg_doublet", 4, 2, 1, "DG", True, False, None),
     ("ext5_dqg", 5, 3, 3, "DQG", True, True, None),
     ("ext1_dqg", 1, 1, 0, "DQG", True, True, None),
+    ("hub3_dqgt2", 3, 1, 1, "DQGT2", True, True, (1.0, 4.0)),
+    ("ext3_dqgt2_doublet", 3, 2, 1, "DQGT2", True, True, None),
 ]
 
 

@@ -15,7 +15,8 @@ def gpu_problem(kw):
 
 
 @pytest.mark.parametrize("name", ["hub2_dqg", "hub4_dqg", "hub4_d_nospin", "ext3_dqg_triplet",
-                                  "ext4_dq_nosz", "ext4_dg_doublet", "ext5_dqg", "ext1_dqg"])
+                                  "ext4_dq_nosz", "ext4_dg_doublet", "ext5_dqg", "ext1_dqg",
+                                  "hub3_dqgt2", "ext3_dqgt2_doublet"])
 def test_maps_bit_exact_golden(golden, cuda_device, name):
     import torch
     case = golden[name]

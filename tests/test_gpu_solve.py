@@ -111,3 +111,38 @@ def test_large_block_trajectory_matches_oracle(cuda_device):
     assert st["oiter"] == 100
     assert np.max(np.abs(xg - xo)) <= 1e-6
     assert abs(float(o.c @ xg) - float(o.c @ xo)) <= 1e-7
+
+
+def test_dqgt2_trajectory_matches_oracle_on_reference_maps(cuda_device):
+    """60 boundary-point iterations with the T2 condition (DQGT2, 4-site ring:
+    T2aaa/bbb blocks of 88 rows, T2aab/bba of 24) follow the numpy oracle driven
+    by hilbert's own compiled maps (t2.cc through oracle/_ref)."""
+    from oracle.bpsdp import BPSDPSolver
+    from oracle.maps import RefProblem, ref_available
+    if not ref_available():
+        pytest.skip("oracle/_ref not built")
+    n = 4
+    r = RefProblem(n, 2, 2, "DQGT2", True, True, hubbard=(1.0, 4.0))
+    so = BPSDPSolver(r.n_primal, r.n_dual, SDPOptions(1e-12, 1e-12, 1e-9, 10000, 60))
+    xo = r.x0.copy()
+    so.solve(xo, r.b, r.c, r.dims, 60, r.Au, r.ATu)
+    p = hb.V2RDMProblem(n, 2, 2, "DQGT2", hubbard_multiplicity=True)
+    opts = hb.Options({"R_CONVERGENCE": 1e-12, "E_CONVERGENCE": 1e-12, "MAXITER": 60,
+                       "MU_UPDATE_FREQUENCY": 100})
+    xg, st = p.solve(r.x0, r.b, r.c, opts)
+    assert st["oiter"] == 60
+    assert np.max(np.abs(xg - xo)) <= 1e-6
+    assert abs(float(r.c @ xg) - float(r.c @ xo)) <= 1e-7
+
+
+def test_dqgt2_energy_between_dqg_and_fci(cuda_device):
+    """The T2 condition tightens the DQG lower bound: E(DQG) <= E(DQGT2) <= E(FCI)."""
+    e = {}
+    for pos in ("DQG", "DQGT2"):
+        o = hubbard_options(4, 4.0)
+        o.set("POSITIVITY", pos)
+        helper = hb.v2RDMHelper(None, o)
+        e[pos] = helper.compute_energy()
+        assert helper.stats["converged"], pos
+    assert e["DQG"] <= e["DQGT2"] + E_TOL
+    assert e["DQGT2"] <= hubbard_fci(4, 4, 1.0, 4.0) + E_TOL

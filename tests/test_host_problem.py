@@ -65,7 +65,8 @@ def test_header_symbols_exported():
 
 
 @pytest.mark.parametrize("name", ["hub2_dqg", "hub4_dqg", "hub4_d_nospin", "ext3_dqg_triplet",
-                                  "ext4_dq_nosz", "ext4_dg_doublet", "ext1_dqg"])
+                                  "ext4_dq_nosz", "ext4_dg_doublet", "ext1_dqg", "hub3_dqgt2",
+                                  "ext3_dqgt2_doublet"])
 def test_host_problem_matches_golden(golden, name):
     case = golden[name]
     kw = case_kwargs(case)
@@ -88,7 +89,7 @@ def test_host_problem_matches_golden(golden, name):
 
 def test_layout_helper_matches_library():
     for args in [(4, 2, 2, "DQG", True), (3, 2, 1, "DQG", True), (4, 2, 2, "D", False),
-                 (4, 2, 1, "DG", True)]:
+                 (4, 2, 1, "DG", True), (3, 2, 1, "DQGT2", True)]:
         p = hb.V2RDMProblem(args[0], args[1], args[2], args[3], args[4])
         assert [d for _, d in hb.block_layout(*args)] == list(p.dims)
 
@@ -99,7 +100,7 @@ def test_bad_arguments_are_rejected():
     with pytest.raises(hb.V2BError):
         hb.V2RDMProblem(0, 0, 0)
     with pytest.raises(ValueError):
-        hb.V2RDMProblem(4, 2, 2, positivity="DQGT2")
+        hb.V2RDMProblem(4, 2, 2, positivity="DQGT1")
 
 
 def test_device_calls_fail_loudly_without_gpu():
