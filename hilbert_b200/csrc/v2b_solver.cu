@@ -24,6 +24,7 @@
 #include "v2b_bigjacobi.cuh"
 #include "v2b_eig.cuh"
 #include "v2b_kernels.cuh"
+#include "v2b_orbital.cuh"
 #include "v2b_refine.cuh"
 #include "v2rdm_b200.h"
 #include "v2rdm_problem.h"
@@ -954,6 +955,7 @@ struct v2b_problem {
     double *partials = nullptr, *cg_out = nullptr, *stats = nullptr, *stats_partials = nullptr;
     unsigned int *stats_counter = nullptr;
     v2b::GridBarrier *bar = nullptr;
+    int *ibas_aa_dev = nullptr;   // n x n aa geminal numbers, for the density packing
     int *status = nullptr;   // [0] fatal device status, [1] projection sweeps exhausted
     double *h_readback = nullptr;   // pinned: stats[4], cg_out[2], status[2]
     int cg_grid = 0;
@@ -997,6 +999,7 @@ struct v2b_problem {
             cudaFree(p);
         cudaFree(stats_counter);
         cudaFree(bar);
+        cudaFree(ibas_aa_dev);
         cudaFree(status);
         if (h_readback) cudaFreeHost(h_readback);
         for (auto &e : ev)
@@ -1553,6 +1556,38 @@ int v2b_problem_set_projection_mode(v2b_problem *p, int mode) {
     return guarded([&] {
         if (!p || mode < 0 || mode > 1) throw std::invalid_argument("set_projection_mode: bad argument");
         p->plan.mode = mode;
+        return V2B_OK;
+    });
+}
+int v2b_problem_pack_dims(const v2b_problem *p, long *d2_size, long *d1_size) {
+    return guarded([&] {
+        if (!p || !d2_size || !d1_size) throw std::invalid_argument("pack_dims: NULL argument");
+        const long g00 = (long)p->prob.n * (p->prob.n + 1) / 2;
+        *d2_size = g00 * (g00 + 1) / 2;
+        *d1_size = g00;
+        return V2B_OK;
+    });
+}
+int v2b_problem_pack_spatial_density(v2b_problem *p, const double *d_x, double *d_d2, double *d_d1,
+                                     void *stream) {
+    return guarded([&] {
+        if (!p || !d_x || !d_d2 || !d_d1) throw std::invalid_argument("pack_spatial_density: NULL argument");
+        p->setup();
+        const v2b::Problem &q = p->prob;
+        if (!p->ibas_aa_dev) {
+            p->ibas_aa_dev = dalloc<int>((size_t)q.n * q.n);
+            V2B_CK(cudaMemcpy(p->ibas_aa_dev, q.ibas_aa.data(), sizeof(int) * q.n * q.n,
+                              cudaMemcpyHostToDevice));
+        }
+        v2b::PackArgs a;
+        a.n = q.n;
+        a.d2ab = q.d2ab; a.d2aa = q.d2aa; a.d2bb = q.d2bb; a.d1a = q.d1a; a.d1b = q.d1b;
+        a.ibas_aa = p->ibas_aa_dev;
+        const int64_t g00 = (int64_t)q.n * (q.n + 1) / 2, total = g00 * (g00 + 1) / 2 + g00;
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 148 * 8));
+        v2b::pack_spatial_density_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(d_x, a, d_d2, d_d1);
+        V2B_CK(cudaGetLastError());
+        p->launches++;
         return V2B_OK;
     });
 }

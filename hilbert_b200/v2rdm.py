@@ -256,6 +256,19 @@ class V2RDMProblem:
             out.append(nnz.value)
         return tuple(out)
 
+    def pack_spatial_density(self, x):
+        """hilbert's PackSpatialDensity of a device primal vector x (float64 CUDA
+        tensor): (packed spin-summed active D2, packed D1), on the current stream"""
+        import torch
+        self._check_tensor(x, self.n_primal)
+        n2, n1 = ctypes.c_long(), ctypes.c_long()
+        check(self._lib.v2b_problem_pack_dims(self._h, ctypes.byref(n2), ctypes.byref(n1)))
+        d2 = torch.empty(n2.value, dtype=torch.float64, device=x.device)
+        d1 = torch.empty(n1.value, dtype=torch.float64, device=x.device)
+        check(self._lib.v2b_problem_pack_spatial_density(self._h, _tptr(x), _tptr(d2), _tptr(d1),
+                                                         self._stream()))
+        return d2, d1
+
     def set_projection_mode(self, mode):
         """"refine" (default: warm refinement) or "jacobi" (selective Jacobi on
         every block every iteration: the plain FP64 path)"""

@@ -189,6 +189,17 @@ int v2b_problem_refine_counts(const v2b_problem *p, long *counts, int n);
  * per-iteration full eigendecomposition libsdp performs, in FP64). */
 int v2b_problem_set_projection_mode(v2b_problem *p, int mode);
 
+/* ---- 2b. densities for the orbital optimiser --------------------------------- */
+
+/* PackSpatialDensity (v2rdm_solver.cc:3110-3219, C1): from a primal x on the
+ * device, the spin-summed active 2-RDM packed over the n(n+1)/2 symmetric
+ * geminals (lower triangle of geminal pairs, off-diagonal pairs doubled;
+ * d2_size = g00 (g00 + 1) / 2, g00 = n (n + 1) / 2) and the spin-summed 1-RDM
+ * (lower triangle, d1_size = g00), bit-identical to hilbert's. */
+int v2b_problem_pack_dims(const v2b_problem *p, long *d2_size, long *d1_size);
+int v2b_problem_pack_spatial_density(v2b_problem *p, const double *d_x, double *d_d2, double *d_d1,
+                                     void *stream);
+
 /* ---- 3. allocation-free projection ------------------------------------------ */
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -43,14 +43,14 @@ gen="$out/v2rdm_solver_extract.cc"
   echo 'namespace hilbert {'
   extract "$src/v2rdm_solver.cc" SymmetryPair TotalSym set_constraints \
       determine_n_primal determine_n_dual set_primal_offsets BuildConstraints \
-      Guess bpsdp_Au bpsdp_ATu
+      Guess bpsdp_Au bpsdp_ATu PackSpatialDensity
   extract "$src/oei.cc" GetOEI_external GetOEI_hubbard
   echo '}'
 } > "$gen"
 
 for name in SymmetryPair TotalSym set_constraints determine_n_primal determine_n_dual \
-            set_primal_offsets BuildConstraints Guess bpsdp_Au bpsdp_ATu GetOEI_external \
-            GetOEI_hubbard; do
+            set_primal_offsets BuildConstraints Guess bpsdp_Au bpsdp_ATu PackSpatialDensity \
+            GetOEI_external GetOEI_hubbard; do
   grep -q "v2RDMSolver::${name}(" "$gen" || { echo "build_ref.sh: could not extract ${name}" >&2; exit 3; }
 done
 

@@ -90,6 +90,9 @@ def _ref_lib():
             getattr(lib, f).argtypes = [ctypes.c_void_p, _dp]
         lib.v2b_ref_Au.argtypes = [ctypes.c_void_p, _dp, _dp]
         lib.v2b_ref_ATu.argtypes = [ctypes.c_void_p, _dp, _dp]
+        lib.v2b_ref_pack_dims.restype = ctypes.c_long
+        lib.v2b_ref_pack_dims.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long)]
+        lib.v2b_ref_pack_spatial.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
         lib.v2b_ref_gems.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         lib.v2b_ref_tables.argtypes = [ctypes.c_void_p, _ip, _ip, _ip, _ip]
         _rlib = lib
@@ -227,6 +230,17 @@ class RefProblem:
         if self._lib.v2b_ref_Au(self._p, out, np.ascontiguousarray(x, np.float64)):
             raise RuntimeError(self._lib.v2b_ref_last_error().decode())
         return out
+
+    def pack_spatial_density(self, x):
+        """hilbert's PackSpatialDensity (v2rdm_solver.cc:3110-3219) of x: the
+        packed spin-summed active D2 (n(n+1)/2 geminals, lower triangle) and D1"""
+        d1n = ctypes.c_long()
+        d2n = self._lib.v2b_ref_pack_dims(self._p, ctypes.byref(d1n))
+        d2 = np.zeros(d2n)
+        d1 = np.zeros(d1n.value)
+        if self._lib.v2b_ref_pack_spatial(self._p, np.ascontiguousarray(x, np.float64), d2, d1):
+            raise RuntimeError(self._lib.v2b_ref_last_error().decode())
+        return d2, d1
 
     def ATu(self, y):
         out = np.zeros(self.n_primal)

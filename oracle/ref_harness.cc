@@ -12,6 +12,7 @@
  * Everything else (index tables, block sizes, offsets, b, c repacking, guess,
  * A.x and A^T.y) runs the reference's own compiled functions.
  */
+#include <cstring>
 #include <psi4/psi4-dec.h>
 #include <psi4/libqt/qt.h>
 #include "v2rdm_solver.h"
@@ -126,6 +127,15 @@ class RefProblem : public v2RDMSolver {
     double *bp() { return b->pointer(); }
     double *cp() { return c->pointer(); }
     double *xp() { return x->pointer(); }
+    // v2rdm_solver.cc:3110-3219 on a given primal vector
+    void pack(const double *xin, double *d2, double *d1) {
+        std::memcpy(x->pointer(), xin, sizeof(double) * n_primal_);
+        PackSpatialDensity();
+        std::memcpy(d2, d2_act_spatial_sym_, sizeof(double) * d2_act_spatial_dim_);
+        std::memcpy(d1, d1_act_spatial_sym_, sizeof(double) * d1_act_spatial_dim_);
+    }
+    long d2_dim() const { return d2_act_spatial_dim_; }
+    long d1_dim() const { return d1_act_spatial_dim_; }
     double efzc() const { return efzc_; }
 
     long block_offset(const std::string &name) const {
@@ -239,6 +249,17 @@ void v2b_ref_tables(void *p, int *bas_ab, int *ibas_ab, int *bas_aa, int *ibas_a
 }
 void v2b_ref_triplets(void *p, int *aaa, int *aab, int *aba) {
     static_cast<RefProblem *>(p)->triplet_sizes(aaa, aab, aba);
+}
+
+long v2b_ref_pack_dims(void *p, long *d1n) {
+    *d1n = static_cast<RefProblem *>(p)->d1_dim();
+    return static_cast<RefProblem *>(p)->d2_dim();
+}
+int v2b_ref_pack_spatial(void *p, const double *x, double *d2, double *d1) {
+    try {
+        static_cast<RefProblem *>(p)->pack(x, d2, d1);
+        return 0;
+    } catch (const std::exception &e) { g_last_error = e.what(); return 1; }
 }
 
 }  // extern "C"

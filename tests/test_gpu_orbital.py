@@ -1,0 +1,62 @@
+"""Orbital side of v2RDM-CASSCF on the B200: hilbert's PackSpatialDensity as a
+device kernel, bit-exact against the reference's compiled function, and the
+orbital gradient of the synthetic DF CASSCF problem (nbf 40, naux 160, 5 core +
+(10e, 10o) active, 25 virtual; 425 rotations) from the device v2RDM solution,
+against the focas gradient formulas and central finite differences."""
+import numpy as np
+import pytest
+
+import hilbert_b200 as hb
+from hilbert_b200 import orbital as ho
+from oracle import orbital as oo
+from oracle.maps import RefProblem, ref_available
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")]
+
+
+@pytest.mark.parametrize("n,na,nb", [(2, 1, 1), (3, 2, 1), (4, 2, 2), (6, 3, 3), (10, 5, 5)])
+def test_pack_kernel_bit_exact(cuda_device, n, na, nb):
+    import torch
+    rng = np.random.default_rng(70 + n)
+    h = rng.standard_normal((n, n)); h = h + h.T
+    g = rng.standard_normal((n, n, n, n))
+    r = RefProblem(n, na, nb, "DQG", True, True, h=h, g=g)
+    x = rng.standard_normal(r.n_primal)
+    d2r, d1r = r.pack_spatial_density(x)
+    p = hb.V2RDMProblem(n, na, nb)
+    d2, d1 = p.pack_spatial_density(torch.from_numpy(x).to(cuda_device))
+    assert np.array_equal(d2.cpu().numpy(), d2r)
+    assert np.array_equal(d1.cpu().numpy(), d1r)
+
+
+def test_df_casscf_orbital_gradient(cuda_device):
+    import torch
+    nc, na_, nv = 5, 10, 25
+    h_mo, B_mo, h_act, g_act, e_core = ho.casscf_df_problem(40, 160, nc, na_)
+    p = hb.V2RDMProblem(na_, 5, 5)
+    b, c = p.b(), p.c_external(h_act, g_act)
+    dev = cuda_device
+    dx = torch.from_numpy(p.guess("RANDOM")).to(dev)
+    opts = hb.Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6, "MAXITER": 100000,
+                       "MU_UPDATE_FREQUENCY": 500})
+    st = p.solve_device(dx, torch.from_numpy(b).to(dev), torch.from_numpy(c).to(dev), opts)
+    assert st["converged"]
+    d2p, d1p = p.pack_spatial_density(dx)
+    Da, Ga = ho.unpack_densities(d2p, d1p, na_)
+    D, G = ho.full_densities(Da, Ga, nc, nv)
+    h, B = torch.from_numpy(h_mo).to(dev), torch.from_numpy(B_mo).to(dev)
+    pairs = ho.rotation_pairs(nc, na_, nv)
+    assert len(pairs) == 425
+    E, g = ho.orbital_gradient(h, B, D, G, pairs)
+    assert abs(E.item() - (e_core + float(c @ dx.cpu().numpy()))) <= 1e-9 * max(1.0, abs(E.item()))
+    gf = oo.focas_gradient(h_mo, B_mo, Da.cpu().numpy(), Ga.cpu().numpy(), nc, na_)
+    g = g.cpu().numpy()
+    for k, pq in enumerate(pairs):
+        assert abs(g[k] - gf[pq]) <= 1e-9 * max(1.0, abs(gf[pq])), pq
+    n = nc + na_ + nv
+    for k, (pp, qq) in enumerate(pairs):
+        dK = torch.zeros((n, n), dtype=torch.float64, device=dev)
+        dK[pp, qq], dK[qq, pp] = 1e-5, -1e-5
+        fd = (ho.rotated_energy(dK, h, B, D, G).item() - ho.rotated_energy(-dK, h, B, D, G).item()) / 2e-5
+        assert abs(fd - g[k]) <= 1e-6, (pp, qq, fd, g[k])
