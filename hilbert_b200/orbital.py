@@ -155,3 +155,78 @@ def casscf_df_problem(nbf=40, naux=160, ncore=5, nact=10, seed_b=0, seed_h=1, se
     Ba = B_mo[:, act][:, :, act]
     g_act = np.einsum("Qtu,Qvw->tuvw", Ba, Ba)
     return h_mo, B_mo, Fi[np.ix_(act, act)], g_act, e_core
+
+
+def optimize_orbitals(h, B, D, G, pairs, max_iter=100, gtol=1e-10):
+    """Orbital optimisation at fixed densities (what focas iterates between SDP
+    solves, orbopt_optimize.cc:25-98): minimise E(kappa) over the given
+    rotation pairs by L-BFGS with the adjoint gradient.  Returns U = exp(kappa),
+    the energy there, and the gradient norms (over the pairs) at the start and
+    at the end."""
+    n = h.shape[0]
+    p = torch.tensor([a for a, _ in pairs], device=h.device)
+    q = torch.tensor([b for _, b in pairs], device=h.device)
+    theta = torch.zeros(len(pairs), dtype=h.dtype, device=h.device, requires_grad=True)
+
+    def kappa(t):
+        K = torch.zeros((n, n), dtype=h.dtype, device=h.device)
+        K = K.index_put((p, q), t)
+        return K.index_put((q, p), -t)
+
+    Gm = G.reshape(n * n, n * n)
+    E0 = RotatedEnergy.apply(kappa(theta), h, B, D, Gm)
+    (g0,) = torch.autograd.grad(E0, theta)
+    opt = torch.optim.LBFGS([theta], max_iter=max_iter, tolerance_grad=gtol, tolerance_change=1e-14,
+                            history_size=20, line_search_fn="strong_wolfe")
+
+    def closure():
+        opt.zero_grad()
+        E = RotatedEnergy.apply(kappa(theta), h, B, D, Gm)
+        E.backward()
+        return E
+
+    opt.step(closure)   # returns the first evaluation; the final state is taken below
+    K = kappa(theta)
+    E = RotatedEnergy.apply(K, h, B, D, Gm)
+    (g1,) = torch.autograd.grad(E, theta)
+    with torch.no_grad():
+        U = torch.linalg.matrix_exp(K)
+    return U, float(E.detach()), float(g0.norm()), float(g1.norm())
+
+
+def active_space(h, B, ncore, nact):
+    """Frozen-core energy, active one-electron integrals (the inactive Fock
+    block) and active (tu|vw) from MO-basis h and DF factors B (torch)."""
+    core = slice(0, ncore)
+    act = slice(ncore, ncore + nact)
+    occ = torch.diagonal(B[:, core, core], dim1=1, dim2=2).sum(1)
+    J = torch.einsum("Qpq,Q->pq", B, occ)
+    K = torch.einsum("Qpi,Qiq->pq", B[:, :, core], B[:, core, :])
+    Fi = h + 2.0 * J - K
+    e_core = float((torch.diagonal(h)[core] + torch.diagonal(Fi)[core]).sum())
+    Ba = B[:, act, act]
+    g = torch.einsum("Qtu,Qvw->tuvw", Ba, Ba)
+    return e_core, Fi[act, act], g
+
+
+def casscf(h, B, ncore, nact, solve_active, macro_iterations=8, active_active=False):
+    """v2RDM-CASSCF macro-iterations: solve the active-space v2RDM in the
+    current orbitals (solve_active(h_act, g_act) -> (E_active, packed d2,
+    packed d1) on the same device as h), optimise the orbitals at those
+    densities, rotate h and B, repeat.  Returns the energies after each SDP
+    solve and the orbital-gradient norms at each orbital step."""
+    nmo = h.shape[0]
+    nvirt = nmo - ncore - nact
+    pairs = rotation_pairs(ncore, nact, nvirt, active_active)
+    energies, gnorms = [], []
+    for _ in range(macro_iterations):
+        e_core, h_act, g_act = active_space(h, B, ncore, nact)
+        e_act, d2p, d1p = solve_active(h_act, g_act)
+        energies.append(e_core + e_act)
+        Da, Ga = unpack_densities(d2p, d1p, nact)
+        D, G = full_densities(Da, Ga, ncore, nvirt)
+        U, _, gn, _ = optimize_orbitals(h, B, D, G, pairs)
+        gnorms.append(gn)
+        h = U.T @ h @ U
+        B = U.T @ B @ U
+    return energies, gnorms, h, B

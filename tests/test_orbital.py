@@ -84,3 +84,20 @@ def test_adjoint_matches_focas_and_finite_differences(small_casscf):
             fd = (ho.rotated_energy(K0 + dK, h, B, D, G).item()
                   - ho.rotated_energy(K0 - dK, h, B, D, G).item()) / 2e-5
             assert abs(fd - (gk[p, q] - gk[q, p]).item()) <= FD_TOL, (p, q)
+
+
+def test_orbital_step_lowers_energy_at_fixed_densities(small_casscf):
+    s = small_casscf
+    nc, na_, nv = s["nc"], s["na"], s["nv"]
+    Da, Ga = ho.unpack_densities(torch.from_numpy(s["d2p"]), torch.from_numpy(s["d1p"]), na_)
+    D, G = ho.full_densities(Da, Ga, nc, nv)
+    h, B = torch.from_numpy(s["h"]), torch.from_numpy(s["B"])
+    pairs = ho.rotation_pairs(nc, na_, nv)
+    U, e_opt, g0, g1 = ho.optimize_orbitals(h, B, D, G, pairs)
+    n = h.shape[0]
+    assert torch.allclose(U.T @ U, torch.eye(n, dtype=torch.float64), atol=1e-13)
+    assert e_opt < s["e"] - 1e-3 and g0 > 1e-2
+    assert g1 <= 1e-3 * g0   # (near-)stationary over the rotation pairs
+    # the rotated integrals give the optimised energy at kappa = 0
+    e2, _ = ho.orbital_gradient(U.T @ h @ U, U.T @ B @ U, D, G, pairs)
+    assert abs(e2.item() - e_opt) <= 1e-10
