@@ -255,6 +255,44 @@ struct ProjectPlan {
     long refine_accepted = 0, refine_jacobi = 0, refine_passes = 0, refine_clusters = 0;
     long refine_large_clusters = 0;   // clusters diagonalised by the Jacobi kernels
     long fb_edges = 0, fb_passes = 0;  // why refined blocks went to Jacobi
+    // optional CUDA-event timing of the projection's phases (with the
+    // problem's profiling): 0 GEMM tiles, 1 acceptance test (norms, test,
+    // P), 2 clusters + Newton step, 3 block-Jacobi sweeps, 4 Jacobi kernels
+    static constexpr int kPhases = 5;
+    bool prof = false;
+    std::vector<cudaEvent_t> pev;
+    std::vector<int> pev_phase;
+    int pev_used = 0;
+    double ph_ms[kPhases] = {};
+    long ph_n[kPhases] = {};
+    void ph_begin(int ph, cudaStream_t s) {
+        if (!prof) return;
+        if ((size_t)(2 * pev_used + 2) > pev.size()) {
+            for (int k = 0; k < 64; k++) {
+                cudaEvent_t e;
+                V2B_CK(cudaEventCreate(&e));
+                pev.push_back(e);
+            }
+            pev_phase.resize(pev.size() / 2);
+        }
+        pev_phase[pev_used] = ph;
+        V2B_CK(cudaEventRecord(pev[2 * pev_used], s));
+    }
+    void ph_end(cudaStream_t s) {
+        if (!prof) return;
+        V2B_CK(cudaEventRecord(pev[2 * pev_used + 1], s));
+        pev_used++;
+    }
+    // after the stream has been synchronised
+    void ph_collect() {
+        for (int k = 0; k < pev_used; k++) {
+            float ms = 0.f;
+            V2B_CK(cudaEventElapsedTime(&ms, pev[2 * k], pev[2 * k + 1]));
+            ph_ms[pev_phase[k]] += ms;
+            ph_n[pev_phase[k]]++;
+        }
+        pev_used = 0;
+    }
     bool fresh = true;
     bool built = false;
     int mode = 0;   // 0: warm refinement, 1: selective Jacobi on every block, every call
@@ -368,6 +406,8 @@ struct ProjectPlan {
     }
     void release() {
         if (!built) return;
+        for (auto e : pev) cudaEventDestroy(e);
+        pev.clear();
         if (staged) cudaEventDestroy(staged);
         staged = nullptr;
         staged_pending = false;
@@ -389,8 +429,10 @@ struct ProjectPlan {
     void gemm(v2b::GemmVariant v, const double *A, const double *B, double *C, const double *Cin,
               double inv_mu, double *x, double *z, cudaStream_t s, long &launches,
               const int *only_work = nullptr) {
+        ph_begin(0, s);
         V2B_CK(v2b::launch_gemm_tiles(v, ntiles, s, A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, x, z,
                                       only_work, orth));
+        ph_end(s);
         launches++;
     }
 
@@ -742,7 +784,9 @@ struct ProjectPlan {
         V2B_CK(cudaMemcpyAsync(Vsave, Vt, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
         V2B_CK(cudaMemcpyAsync(Tsave, T, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
         // ||T||_F = ||sym(U)||_F for an orthonormal Vt: the tests use the block norms of Us
+        ph_begin(1, s);
         block_norm_kernel<<<dim3(nblk, kClassifySplit), 256, 0, s>>>(Us, boff, bdim, norm_part);
+        ph_end(s);
         V2B_CK(cudaGetLastError());
         launches++;
         std::vector<char> changed(nblk, 0);
@@ -769,10 +813,12 @@ struct ProjectPlan {
                 }
             }
             ++stamp;
+            ph_begin(1, s);
             refine_classify_kernel<<<dim3(nblk, kClassifySplit), kRefineThreads, classify_smem, s>>>(
                 T, boff, bdim, bstate, orth, norm_part, gap_tol, abs_tol, bnorm, cls_counts, done_stamp,
                 stamp, d_state, d_nbad, d_nedge, d_edges);
             write_p_kernel<<<ntiles, 256, 0, s>>>(T, P, tiles, boff, bdim, done_stamp, stamp);
+            ph_end(s);
             V2B_CK(cudaGetLastError());
             launches += 2;
             V2B_CK(cudaStreamSynchronize(s));
@@ -829,14 +875,18 @@ struct ProjectPlan {
             if (nwork == 0 && nbj == 0) break;
             upload_states(s, st);
             if (nbj) {
+                ph_begin(3, s);
                 block_jacobi_sweep(st, s, launches);
+                ph_end(s);
                 for (int b = 0; b < nblk; b++)
                     if (st[b] == kStBlockJacobi) sweeps[b]++;
             }
             if (nwork) {
+                ph_begin(2, s);
                 if (!members.empty()) cluster_pass(members, jblk, s, launches);
                 newton_m_kernel<<<ntiles, 256, 0, s>>>(T, W, tiles, boff, bdim, bstate, bnorm, gap_tol,
                                                        abs_tol);
+                ph_end(s);
                 V2B_CK(cudaGetLastError());
                 launches++;
                 V2B_CK(cudaMemsetAsync(orth, 0, nblk * sizeof(unsigned long long), s));
@@ -922,7 +972,9 @@ struct ProjectPlan {
         if (staged_pending) V2B_CK(cudaEventSynchronize(staged));
         upload_states(s, st);
         refine(st, s, launches);
+        ph_begin(4, s);
         jacobi(st, s, launches);
+        ph_end(s);
         V2B_CK(cudaEventRecord(staged, s));
         staged_pending = true;
         gemm(kGemmTNStore, Vt, P, W, nullptr, 0.0, nullptr, nullptr, s, launches);
@@ -975,6 +1027,7 @@ struct v2b_problem {
     }
     void collect() {
         if (!profiling) return;
+        if (plan.built) plan.ph_collect();
         for (int k = 0; k < kClasses; k++) {
             float ms = 0.f;
             V2B_CK(cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]));
@@ -987,6 +1040,9 @@ struct v2b_problem {
             for (auto &e : ev) V2B_CK(cudaEventCreate(&e));
         profiling = on;
         for (int k = 0; k < kClasses; k++) { prof_ms[k] = 0.0; prof_n[k] = 0; }
+        plan.prof = on;
+        plan.pev_used = 0;
+        for (int k = 0; k < ProjectPlan::kPhases; k++) { plan.ph_ms[k] = 0.0; plan.ph_n[k] = 0; }
     }
 
     ~v2b_problem() {
@@ -1556,6 +1612,16 @@ int v2b_problem_set_projection_mode(v2b_problem *p, int mode) {
     return guarded([&] {
         if (!p || mode < 0 || mode > 1) throw std::invalid_argument("set_projection_mode: bad argument");
         p->plan.mode = mode;
+        return V2B_OK;
+    });
+}
+int v2b_problem_projection_profile(const v2b_problem *p, double *ms, long *n, int count) {
+    return guarded([&] {
+        if (!p || !ms || !n || count < 0) throw std::invalid_argument("projection_profile: bad argument");
+        for (int k = 0; k < count && k < ProjectPlan::kPhases; k++) {
+            ms[k] = p->plan.ph_ms[k];
+            n[k] = p->plan.ph_n[k];
+        }
         return V2B_OK;
     });
 }

@@ -239,6 +239,15 @@ class V2RDMProblem:
         check(self._lib.v2b_problem_profile(self._h, ms, n))
         return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNEL_CLASSES)}
 
+    PROJECTION_PHASES = ("gemm", "acceptance", "clusters_newton", "block_jacobi", "jacobi")
+
+    def projection_profile(self):
+        """{phase: (total_ms, count)} of the projection, with profiling on"""
+        k = len(self.PROJECTION_PHASES)
+        ms, n = (ctypes.c_double * k)(), (ctypes.c_long * k)()
+        check(self._lib.v2b_problem_projection_profile(self._h, ms, n, k))
+        return {name: (ms[i], n[i]) for i, name in enumerate(self.PROJECTION_PHASES)}
+
     def projection_counts(self):
         """{"calls", "rotations", "sweep_overruns"} of the warm-started projection"""
         w, r, c = ctypes.c_long(), ctypes.c_long(), ctypes.c_long()

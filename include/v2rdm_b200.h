@@ -167,6 +167,10 @@ long v2b_problem_kernel_launches(const v2b_problem *p);
  * the library's stream: 0 cg_kernel, 1 spmv_AT_U_kernel, 2 jacobi_project_kernel,
  * 3 spmv_A2_kernel, 4 stats_kernel.  set_profiling resets the totals. */
 int v2b_problem_set_profiling(v2b_problem *p, int on);
+/* with profiling on: CUDA-event time of the projection's phases, the first
+ * count of: [0] GEMM tiles, [1] acceptance test, [2] clusters + Newton step,
+ * [3] block-Jacobi sweeps, [4] Jacobi kernels (no reference counterpart) */
+int v2b_problem_projection_profile(const v2b_problem *p, double *ms, long *n, int count);
 int v2b_problem_profile(const v2b_problem *p, double *ms /* [5] */, long *launches /* [5] */);
 /* the cudaStream_t the device solve runs on (after the first device call) */
 void *v2b_problem_stream(const v2b_problem *p);
