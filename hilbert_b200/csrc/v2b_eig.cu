@@ -13,127 +13,246 @@
 // 64 x 64 output tiles of every block.
 #include "v2b_eig.cuh"
 
+#include <algorithm>
+
 namespace v2b {
 
 // ---------------------------------------------------------------------------
 // batched FP64 GEMM over square blocks: C_b = op(A_b) op(B_b) [+ epilogue]
-// 64 x 64 output tile per CTA, 256 threads, 4 x 4 outputs per thread, K in
-// chunks of 16 staged through shared memory.
+//
+// FP64 tensor cores (mma.sync m8n8k4 .f64): a 64 x 64 output tile per CTA of
+// 4 warps, each warp a 32 x 32 sub-tile of 4 x 4 m8n8 fragments (32
+// accumulators per thread).  K runs in chunks of 16 through a 3-stage
+// cp.async pipeline (8-byte copies: a block of odd dimension starts at an
+// odd double, so 16-byte alignment is not available; out-of-range elements
+// are zero-filled by the copy itself).  Each operand tile is stored with its
+// global contiguous index innermost (k-major when the matrix is read down
+// its columns), padded so that both the copies and the fragment reads are
+// free of bank conflicts.
+//
+// With a scheduler counter the grid is persistent (the SM count times the
+// CTAs an SM holds) and CTAs take tiles in list order, the tile list sorted
+// by block dimension (its K) descending: the longest tiles start first and
+// the short ones fill in behind them.  Without one, CTA i computes tile i.
+constexpr int kGemmBK = 16;
+constexpr int kGemmStages = 3;
+constexpr int kGemmThreads = 128;
+constexpr int kPadM = kGemmTile + 4;    // k-major rows: 64 + 4 doubles
+constexpr int kPadK = kGemmBK + 4;      // m-major rows: 16 + 4 doubles
+constexpr int kOpDoubles = (kGemmTile * kPadK > kGemmBK * kPadM) ? kGemmTile * kPadK : kGemmBK * kPadM;
+constexpr int kGemmSmem = kGemmStages * 2 * kOpDoubles * (int)sizeof(double);
+
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool pred) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    const int bytes = pred ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// D (8 x 8) += A (8 x 4, row) B (4 x 8, col); per lane: A[l/4][l%4],
+// B[l%4][l/4], D[l/4][2 (l%4) + {0, 1}]
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// shared-memory index of element (m, k) of a 64 x 16 operand tile
+template <bool KMAJOR>
+__device__ __forceinline__ int op_idx(int m, int k) {
+    return KMAJOR ? k * kPadM + m : m * kPadK + k;
+}
+
+// one 64 x 16 operand tile: rows m of the operand (rows of op(A) or columns of
+// op(B)) from m0, k from k0.  KMAJOR: the global matrix is contiguous in m
+// (element (m, k) at X[k n + m]), else in k (X[m n + k]).
+template <bool KMAJOR>
+__device__ __forceinline__ void load_op(double *sm, const double *__restrict__ X, int n, int m0, int k0) {
+#pragma unroll
+    for (int it = 0; it < kGemmTile * kGemmBK / kGemmThreads; it++) {
+        const int e = it * kGemmThreads + threadIdx.x;
+        const int m = KMAJOR ? e % kGemmTile : e / kGemmBK;
+        const int k = KMAJOR ? e / kGemmTile : e % kGemmBK;
+        const int gm = m0 + m, gk = k0 + k;
+        const bool ok = gm < n && gk < n;
+        const double *src = ok ? (KMAJOR ? X + (int64_t)gk * n + gm : X + (int64_t)gm * n + gk) : X;
+        cp_async8(sm + op_idx<KMAJOR>(m, k), src, ok);
+    }
+}
+
 template <bool TA, bool TB, int EPI>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kGemmThreads, 3)
     gemm_tiles_kernel(const double *__restrict__ A, const double *__restrict__ B,
                       double *__restrict__ C, const int4 *__restrict__ tiles,
                       const int64_t *__restrict__ boff, const int *__restrict__ bdim,
                       const double *__restrict__ Cin, const double *__restrict__ Us, double inv_mu,
                       double *__restrict__ xo, double *__restrict__ zo,
-                      const int *__restrict__ bstate, unsigned long long *__restrict__ orth) {
-    constexpr int BM = 64, BK = 16;
-    __shared__ double As[BK][BM + 2];
-    __shared__ double Bs[BK][BM + 2];
-    const int4 t = tiles[blockIdx.x];
-    const int blk = t.x, n = bdim[blk];
-    if (bstate && bstate[blk] != 0) return;   // uniform over the CTA
-    const int64_t off = boff[blk];
-    const int r0 = t.y * BM, c0 = t.z * BM;
-    const double *Ab = A + off, *Bb = B + off;
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    double acc[4][4];
+                      const int *__restrict__ bstate, unsigned long long *__restrict__ orth,
+                      int ntiles, int *__restrict__ sched) {
+    // op(A) rows are m-contiguous in memory when A is read transposed;
+    // op(B) columns are m-contiguous when B is read as stored
+    constexpr bool AK = TA, BKM = !TB;
+    extern __shared__ double gsm[];
+    __shared__ int s_tile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int fr = lane >> 2, fk = lane & 3;
+    for (int iter = 0;; iter++) {
+        int ti;
+        if (sched) {
+            if (threadIdx.x == 0) {
+                int t = atomicAdd(sched, 1);
+                if (t >= ntiles) {
+                    // the last CTA to run out re-arms the counter for the next launch
+                    if (atomicAdd(sched + 1, 1) == (int)gridDim.x - 1) {
+                        sched[0] = 0;
+                        sched[1] = 0;
+                    }
+                    t = -1;
+                }
+                s_tile = t;
+            }
+            __syncthreads();
+            ti = s_tile;
+            __syncthreads();
+        } else {
+            ti = iter == 0 ? (int)blockIdx.x : -1;
+        }
+        if (ti < 0) break;
+        const int4 t = tiles[ti];
+        const int blk = t.x, n = bdim[blk];
+        if (bstate && bstate[blk] != 0) continue;   // uniform over the CTA
+        const int64_t off = boff[blk];
+        const int r0 = t.y * kGemmTile, c0 = t.z * kGemmTile;
+        const double *Ab = A + off, *Bb = B + off;
+        double acc[4][4][2];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+        for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+            for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-    for (int k0 = 0; k0 < n; k0 += BK) {
-        // op(A)[r][k] for r in [r0, r0+64), k in [k0, k0+16)
-        for (int e = threadIdx.x; e < BM * BK; e += 256) {
-            int rr, kk;
-            if (TA) { kk = e / BM; rr = e % BM; }   // A[k][r]: contiguous in r
-            else { rr = e / BK; kk = e % BK; }      // A[r][k]: contiguous in k
-            const int r = r0 + rr, k = k0 + kk;
-            double v = 0.0;
-            if (r < n && k < n) v = TA ? Ab[(int64_t)k * n + r] : Ab[(int64_t)r * n + k];
-            As[kk][rr] = v;
+        const int nk = (n + kGemmBK - 1) / kGemmBK;
+#pragma unroll
+        for (int st = 0; st < kGemmStages - 1; st++) {
+            if (st < nk) {
+                double *sa = gsm + st * 2 * kOpDoubles;
+                load_op<AK>(sa, Ab, n, r0, st * kGemmBK);
+                load_op<BKM>(sa + kOpDoubles, Bb, n, c0, st * kGemmBK);
+            }
+            cp_async_commit();
         }
-        // op(B)[k][c] for k in [k0, k0+16), c in [c0, c0+64)
-        for (int e = threadIdx.x; e < BM * BK; e += 256) {
-            int cc, kk;
-            if (TB) { cc = e / BK; kk = e % BK; }   // B[c][k]: contiguous in k
-            else { kk = e / BM; cc = e % BM; }      // B[k][c]: contiguous in c
-            const int c = c0 + cc, k = k0 + kk;
-            double v = 0.0;
-            if (c < n && k < n) v = TB ? Bb[(int64_t)c * n + k] : Bb[(int64_t)k * n + c];
-            Bs[kk][cc] = v;
-        }
-        __syncthreads();
+        for (int kt = 0; kt < nk; kt++) {
+            cp_async_wait<kGemmStages - 2>();
+            __syncthreads();
+            // refill the stage consumed one step ago (every warp is past it)
+            const int kn = kt + kGemmStages - 1;
+            if (kn < nk) {
+                double *sa = gsm + (kn % kGemmStages) * 2 * kOpDoubles;
+                load_op<AK>(sa, Ab, n, r0, kn * kGemmBK);
+                load_op<BKM>(sa + kOpDoubles, Bb, n, c0, kn * kGemmBK);
+            }
+            cp_async_commit();
+            const double *sa = gsm + (kt % kGemmStages) * 2 * kOpDoubles;
+            const double *sb = sa + kOpDoubles;
 #pragma unroll
-        for (int kk = 0; kk < BK; kk++) {
-            double a[4], b[4];
+            for (int k4 = 0; k4 < kGemmBK; k4 += 4) {
+                double a[4], b[4];
 #pragma unroll
-            for (int i = 0; i < 4; i++) a[i] = As[kk][ty * 4 + i];
+                for (int i = 0; i < 4; i++) a[i] = sa[op_idx<AK>(wm + i * 8 + fr, k4 + fk)];
 #pragma unroll
-            for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx * 4 + j];
+                for (int j = 0; j < 4; j++) b[j] = sb[op_idx<BKM>(wn + j * 8 + fr, k4 + fk)];
 #pragma unroll
-            for (int i = 0; i < 4; i++)
+                for (int i = 0; i < 4; i++)
 #pragma unroll
-                for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-        }
-        __syncthreads();
-    }
-    double dev = 0.0;
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int r = r0 + ty * 4 + i;
-        if (r >= n) continue;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int c = c0 + tx * 4 + j;
-            if (c >= n) continue;
-            const int64_t e = off + (int64_t)r * n + c;
-            if (EPI == kEpiStore) {
-                C[e] = acc[i][j];
-            } else if (EPI == kEpiAdd) {
-                C[e] = Cin[e] + acc[i][j];
-            } else if (EPI == kEpiNS) {   // acc = Vt Vt^T
-                const double id = (r == c) ? 1.0 : 0.0;
-                C[e] = 1.5 * id - 0.5 * acc[i][j];
-                dev = fmax(dev, fabs(acc[i][j] - id));
-            } else {   // kEpiProject: acc = U+
-                xo[e] = acc[i][j] * inv_mu;
-                zo[e] = acc[i][j] - Us[e];
+                    for (int j = 0; j < 4; j++) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
             }
         }
-    }
-    if (EPI == kEpiNS) {
-        // non-negative doubles order like their bit patterns
-        dev = warp_max(dev);
-        if ((threadIdx.x & 31) == 0 && dev > 0.0)
-            atomicMax(orth + blk, (unsigned long long)__double_as_longlong(dev));
+        cp_async_wait<0>();
+        __syncthreads();   // the next tile's copies reuse the stages
+
+        double dev = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int r = r0 + wm + i * 8 + fr;
+            if (r >= n) continue;
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int c = c0 + wn + j * 8 + 2 * fk + h;
+                    if (c >= n) continue;
+                    const double v = acc[i][j][h];
+                    const int64_t e = off + (int64_t)r * n + c;
+                    if (EPI == kEpiStore) {
+                        C[e] = v;
+                    } else if (EPI == kEpiAdd) {
+                        C[e] = Cin[e] + v;
+                    } else if (EPI == kEpiNS) {   // v = (Vt Vt^T)[r][c]
+                        const double id = (r == c) ? 1.0 : 0.0;
+                        C[e] = 1.5 * id - 0.5 * v;
+                        dev = fmax(dev, fabs(v - id));
+                    } else {   // kEpiProject: v = U+
+                        xo[e] = v * inv_mu;
+                        zo[e] = v - Us[e];
+                    }
+                }
+        }
+        if (EPI == kEpiNS) {
+            // non-negative doubles order like their bit patterns
+            dev = warp_max(dev);
+            if (lane == 0 && dev > 0.0)
+                atomicMax(orth + blk, (unsigned long long)__double_as_longlong(dev));
+        }
     }
 }
 
-cudaError_t launch_gemm_tiles(GemmVariant v, int ntiles, cudaStream_t s, GEMM_ARGS) {
-    if (ntiles <= 0) return cudaSuccess;
-    switch (v) {
-        case kGemmNTNewtonSchulz:
-            gemm_tiles_kernel<false, true, kEpiNS><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate, orth);
-            break;
-        case kGemmNTStore:
-            gemm_tiles_kernel<false, true, kEpiStore><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate, orth);
-            break;
-        case kGemmNNStore:
-            gemm_tiles_kernel<false, false, kEpiStore><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate, orth);
-            break;
-        case kGemmTNStore:
-            gemm_tiles_kernel<true, false, kEpiStore><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate, orth);
-            break;
-        case kGemmNNProject:
-            gemm_tiles_kernel<false, false, kEpiProject><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate, orth);
-            break;
-        case kGemmNNAdd:
-            gemm_tiles_kernel<false, false, kEpiAdd><<<ntiles, 256, 0, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate, orth);
-            break;
-    }
+template <bool TA, bool TB, int EPI>
+static cudaError_t launch_variant(int ntiles, cudaStream_t s, GEMM_ARGS, int *sched) {
+    auto kern = gemm_tiles_kernel<TA, TB, EPI>;
+    // opt in to the pipeline's shared memory and size the persistent grid,
+    // once per variant (thread-safe static initialisation)
+    struct Cfg {
+        cudaError_t err = cudaSuccess;
+        int slots = 1;
+    };
+    static const Cfg cfg = [kern] {
+        Cfg c;
+        int dev = 0, sms = 0, occ = 0;
+        c.err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
+        if (c.err == cudaSuccess) c.err = cudaGetDevice(&dev);
+        if (c.err == cudaSuccess) c.err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (c.err == cudaSuccess)
+            c.err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kGemmThreads, kGemmSmem);
+        c.slots = std::max(1, sms * occ);
+        return c;
+    }();
+    if (cfg.err != cudaSuccess) return cfg.err;
+    const int grid = sched ? std::min(ntiles, cfg.slots) : ntiles;
+    kern<<<grid, kGemmThreads, kGemmSmem, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate,
+                                               orth, ntiles, sched);
     return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_tiles(GemmVariant v, int ntiles, cudaStream_t s, GEMM_ARGS, int *sched) {
+    if (ntiles <= 0) return cudaSuccess;
+#define V2B_GEMM_CASE(NAME, TA, TB, EPI) \
+    case NAME:                           \
+        return launch_variant<TA, TB, EPI>(ntiles, s, A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate, orth, sched);
+    switch (v) {
+        V2B_GEMM_CASE(kGemmNTNewtonSchulz, false, true, kEpiNS)
+        V2B_GEMM_CASE(kGemmNTStore, false, true, kEpiStore)
+        V2B_GEMM_CASE(kGemmNNStore, false, false, kEpiStore)
+        V2B_GEMM_CASE(kGemmTNStore, true, false, kEpiStore)
+        V2B_GEMM_CASE(kGemmNNProject, false, false, kEpiProject)
+        V2B_GEMM_CASE(kGemmNNAdd, false, false, kEpiAdd)
+    }
+#undef V2B_GEMM_CASE
+    return cudaErrorInvalidValue;
 }
 
 // Us = (U + U^T) / 2 per block, tile by tile

@@ -26,10 +26,14 @@ constexpr int kGemmTile = 64;
 // instantiations, in v2b_eig.cu).  variant: 0 <N,T,store>, 1 <N,N,store>,
 // 2 <T,N,store>, 3 <N,N,project>, 4 <N,N,add>, 5 <N,T,Newton-Schulz>.
 // With bstate non-null, tiles of blocks whose state is not 0 (refinement in
-// progress) are skipped.
+// progress) are skipped.  sched: two ints, zero before the first launch, that
+// make the grid persistent (tiles taken in list order; the kernel leaves them
+// zero again); null launches one CTA per tile.  Launches that share a sched
+// pair must be ordered (one stream).
 enum GemmVariant { kGemmNTStore = 0, kGemmNNStore = 1, kGemmTNStore = 2, kGemmNNProject = 3,
                    kGemmNNAdd = 4, kGemmNTNewtonSchulz = 5 };
-cudaError_t launch_gemm_tiles(GemmVariant v, int ntiles, cudaStream_t s, GEMM_ARGS);
+cudaError_t launch_gemm_tiles(GemmVariant v, int ntiles, cudaStream_t s, GEMM_ARGS,
+                              int *sched = nullptr);
 
 }  // namespace v2b
 

@@ -196,6 +196,7 @@ struct ProjectPlan {
     int *bdim = nullptr, *counters = nullptr;
     int4 *tiles = nullptr;
     int ntiles = 0;
+    int *gemm_sched = nullptr;   // persistent-grid tile counter of the GEMM launches
     double2 *rot = nullptr;
     double *Vt = nullptr, *Vt2 = nullptr, *Us = nullptr, *W = nullptr, *T = nullptr, *P = nullptr;
     // large-block work arrays
@@ -337,8 +338,12 @@ struct ProjectPlan {
         }
         total = o;
         rows_total = rows;
+        // longest K first: the persistent GEMM grid takes tiles in this order
+        std::stable_sort(tl.begin(), tl.end(), [&](const int4 &a, const int4 &b) { return d[a.x] > d[b.x]; });
         ntiles = (int)tl.size();
         boff = dalloc<int64_t>(nblk);
+        gemm_sched = dalloc<int>(2);
+        V2B_CK(cudaMemset(gemm_sched, 0, 2 * sizeof(int)));
         bdim = dalloc<int>(nblk);
         counters = dalloc<int>(4);
         tiles = dalloc<int4>(std::max(ntiles, 1));
@@ -412,7 +417,7 @@ struct ProjectPlan {
         staged = nullptr;
         staged_pending = false;
         for (void *q : {(void *)boff, (void *)rot_off, (void *)bdim, (void *)counters, (void *)tiles,
-                        (void *)rot, (void *)Vt, (void *)Vt2, (void *)Us, (void *)W, (void *)T,
+                        (void *)gemm_sched, (void *)rot, (void *)Vt, (void *)Vt2, (void *)Us, (void *)W, (void *)T,
                         (void *)P, (void *)rec_b, (void *)norm_b, (void *)sub_boff, (void *)sub_roff,
                         (void *)sub_bdim, (void *)bstate, (void *)orth, (void *)bnorm, (void *)norm_part,
                         (void *)cls_counts, (void *)done_stamp, (void *)Vsave,
@@ -431,7 +436,7 @@ struct ProjectPlan {
               const int *only_work = nullptr) {
         ph_begin(0, s);
         V2B_CK(v2b::launch_gemm_tiles(v, ntiles, s, A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, x, z,
-                                      only_work, orth));
+                                      only_work, orth, gemm_sched));
         ph_end(s);
         launches++;
     }
