@@ -38,6 +38,7 @@ EXPORTS = (
     "v2b_problem_kernel_launches", "v2b_problem_operator_size", "v2b_problem_operator",
     "v2b_problem_set_profiling", "v2b_problem_profile", "v2b_problem_stream",
     "v2b_problem_projection_counts", "v2b_problem_refine_counts", "v2b_problem_set_projection_mode", "v2b_problem_pack_dims", "v2b_problem_projection_profile",
+    "v2b_problem_cg_profile",
     "v2b_problem_pack_spatial_density", "v2b_project_block_noalloc",
 )
 
@@ -125,6 +126,7 @@ def load(path=LIB_PATH):
         "v2b_problem_set_projection_mode": (ctypes.c_int, [vp, ctypes.c_int]),
         "v2b_problem_pack_dims": (ctypes.c_int, [vp, lp, lp]),
         "v2b_problem_projection_profile": (ctypes.c_int, [vp, dp, lp, ctypes.c_int]),
+        "v2b_problem_cg_profile": (ctypes.c_int, [vp, dp, ctypes.c_int]),
         "v2b_problem_pack_spatial_density": (ctypes.c_int, [vp, vp, vp, vp, vp]),
         "v2b_project_block_noalloc": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, vp, vp, vp]),
         "v2b_problem_operator_size": (ctypes.c_int, [vp, ctypes.c_int, lp, lp, ip]),

@@ -52,6 +52,13 @@ __device__ __forceinline__ double packed_row_rbp(const uint32_t *__restrict__ en
     return grp ? __dadd_rn(acc0, acc1) : acc0;
 }
 
+// the GPU's nanosecond clock (PTX %globaltimer)
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);

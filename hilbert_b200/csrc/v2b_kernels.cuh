@@ -50,6 +50,7 @@ struct CgParams {
     double tol;
     int maxit;
     double *out;                    // out[0] = iterations, out[1] = final ||r||
+    unsigned long long *phase_ns;   // null, or 4 sums of ns: initial residual, A^T p, A t, update
 };
 
 __global__ void spmv_kernel(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ent,

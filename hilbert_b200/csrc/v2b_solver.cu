@@ -1027,6 +1027,9 @@ struct v2b_problem {
     cudaEvent_t ev[2 * kClasses] = {};
     double prof_ms[kClasses] = {};
     long prof_n[kClasses] = {};
+    // CG phases, summed by the kernel's own clock: initial residual, A^T p, A t, update
+    static constexpr int kCgPhases = 4;
+    unsigned long long *cg_phase = nullptr;
     void mark(int cls, int edge) {
         if (profiling) V2B_CK(cudaEventRecord(ev[2 * cls + edge], stream));
     }
@@ -1043,6 +1046,8 @@ struct v2b_problem {
     void set_profiling(bool on) {
         if (on && !ev[0])
             for (auto &e : ev) V2B_CK(cudaEventCreate(&e));
+        if (on && !cg_phase) cg_phase = dalloc<unsigned long long>(kCgPhases);
+        if (cg_phase) V2B_CK(cudaMemset(cg_phase, 0, kCgPhases * sizeof(unsigned long long)));
         profiling = on;
         for (int k = 0; k < kClasses; k++) { prof_ms[k] = 0.0; prof_n[k] = 0; }
         plan.prof = on;
@@ -1058,6 +1063,7 @@ struct v2b_problem {
         for (double *p : {x, b, c, y, z, Ax, Acz, ATy, U, r, p0, p1, t, q, partials, cg_out, stats,
                           stats_partials})
             cudaFree(p);
+        if (cg_phase) cudaFree(cg_phase);
         cudaFree(stats_counter);
         cudaFree(bar);
         cudaFree(ibas_aa_dev);
@@ -1143,6 +1149,7 @@ struct v2b_problem {
         P.partials = partials; P.bar = bar; P.status = status;
         P.spin_limit = 40000000LL;   // a few seconds of 32 ns polls
         P.tol = tol; P.maxit = maxit; P.out = cg_out;
+        P.phase_ns = profiling ? cg_phase : nullptr;
         void *args[] = {&P};
         V2B_CK(cudaLaunchCooperativeKernel((const void *)v2b::cg_kernel, dim3(cg_grid),
                                            dim3(v2b::kCgThreads), args, 0, stream));
@@ -1609,6 +1616,19 @@ int v2b_problem_projection_counts(const v2b_problem *p, long *calls, long *rotat
         if (p->plan.built) V2B_CK(cudaMemcpy(h, p->plan.counters, 16, cudaMemcpyDeviceToHost));
         *rotations = (long)h[1] + h[3];
         *sweep_overruns = (long)h[0] + h[2];
+        return V2B_OK;
+    });
+}
+
+int v2b_problem_cg_profile(const v2b_problem *p, double *ms, int count) {
+    return guarded([&] {
+        if (!p || !ms || count < 0) throw std::invalid_argument("cg_profile: bad argument");
+        unsigned long long h[v2b_problem::kCgPhases] = {};
+        if (p->cg_phase) {
+            V2B_CK(cudaStreamSynchronize(p->stream));
+            V2B_CK(cudaMemcpy(h, p->cg_phase, sizeof(h), cudaMemcpyDeviceToHost));
+        }
+        for (int k = 0; k < count && k < v2b_problem::kCgPhases; k++) ms[k] = 1e-6 * (double)h[k];
         return V2B_OK;
     });
 }

@@ -248,6 +248,15 @@ class V2RDMProblem:
         check(self._lib.v2b_problem_projection_profile(self._h, ms, n, k))
         return {name: (ms[i], n[i]) for i, name in enumerate(self.PROJECTION_PHASES)}
 
+    CG_PHASES = ("initial_residual", "transpose_gather", "gather_dot", "update")
+
+    def cg_profile(self):
+        """{phase: total_ms} of the CG kernel, barrier to barrier, with profiling on"""
+        k = len(self.CG_PHASES)
+        ms = (ctypes.c_double * k)()
+        check(self._lib.v2b_problem_cg_profile(self._h, ms, k))
+        return {name: ms[i] for i, name in enumerate(self.CG_PHASES)}
+
     def projection_counts(self):
         """{"calls", "rotations", "sweep_overruns"} of the warm-started projection"""
         w, r, c = ctypes.c_long(), ctypes.c_long(), ctypes.c_long()

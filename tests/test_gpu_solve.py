@@ -146,3 +146,26 @@ def test_dqgt2_energy_between_dqg_and_fci(cuda_device):
         assert helper.stats["converged"], pos
     assert e["DQG"] <= e["DQGT2"] + E_TOL
     assert e["DQGT2"] <= hubbard_fci(4, 4, 1.0, 4.0) + E_TOL
+
+
+def test_profiling_timers_leave_the_solve_unchanged(cuda_device):
+    """Kernel-class events, projection phases and the CG kernel's own phase
+    clock: all populated, consistent with each other, and the solve with them
+    on is bit-identical to the solve without."""
+    opts = hb.Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6, "MAXITER": 60,
+                       "MU_UPDATE_FREQUENCY": 20})
+    runs = []
+    for on in (False, True):
+        p = hb.V2RDMProblem(6, 3, 3, hubbard_multiplicity=True)
+        p.set_profiling(on)
+        x, st = p.solve(p.guess("RANDOM"), p.b(), p.c_hubbard(1.0, 4.0), opts)
+        runs.append((p, x, st))
+    assert np.array_equal(runs[0][1], runs[1][1])
+    p = runs[1][0]
+    classes, cg, phases = p.profile(), p.cg_profile(), p.projection_profile()
+    assert classes["cg_kernel"][1] == 60
+    assert all(v >= 0.0 for v in cg.values())
+    assert cg["transpose_gather"] > 0.0 and cg["gather_dot"] > 0.0 and cg["update"] > 0.0
+    # barrier-to-barrier phases lie inside the kernels' event-timed span
+    assert sum(cg.values()) <= 1.05 * classes["cg_kernel"][0] + 0.5
+    assert phases["gemm"][1] > 0
