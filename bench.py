@@ -328,6 +328,8 @@ def run_b200(args, w):
             torch.cuda.synchronize()
             times.append(ev0.elapsed_time(ev1) / 1e3)
     prof = p.profile()
+    phases = {"cg_kernel": {k: round(v, 1) for k, v in p.cg_profile().items()},
+              "projection": {k: [round(v[0], 1), v[1]] for k, v in p.projection_profile().items()}}
     p.set_profiling(False)
     launches = p.kernel_launches() - launches0
     t = max_over_ranks(max(times), world)
@@ -396,6 +398,9 @@ def run_b200(args, w):
                                   "counted as for LAPACK), FP64; no FP64 peak is measured"}
     tot = sum(x[0] for x in prof.values())
     roof["kernel_ms_share"] = {k: round(v[0] / tot, 4) for k, v in prof.items()}
+    # ms per part of the timed solve: the CG kernel's phases barrier to barrier
+    # (its own clock), the projection's phases as [ms, launches or calls]
+    roof["phases_ms"] = phases
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_sample_seconds > 0:
