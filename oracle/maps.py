@@ -14,9 +14,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libv2rdm_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libv2rdm_ref.so")
 
-POSITIVITY = {"D": 0, "DQ": 1, "DG": 2, "DQG": 3}
+POSITIVITY = {"D": 0, "DQ": 1, "DG": 2, "DQG": 3, "DQGT2": 4}
 BLOCK_NAMES = ("d2ab", "d2aa", "d2bb", "d200", "d1a", "d1b", "q1a", "q1b",
-               "q2ab", "q2aa", "q2bb", "g2ab", "g2ba", "g2aa")
+               "q2ab", "q2aa", "q2bb", "g2ab", "g2ba", "g2aa", "t2aaa", "t2bbb", "t2aab", "t2bba")
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -122,7 +122,7 @@ class OracleProblem:
         gab, gaa = ctypes.c_int(), ctypes.c_int()
         lib.v2o_gems(self._p, ctypes.byref(gab), ctypes.byref(gaa))
         self.gab, self.gaa = gab.value, gaa.value
-        offs = np.zeros(14, np.int64)
+        offs = np.zeros(len(BLOCK_NAMES), np.int64)
         lib.v2o_offsets(self._p, offs)
         self.offsets = {k: int(v) for k, v in zip(BLOCK_NAMES, offs) if v >= 0}
         self.b = np.zeros(self.n_dual)

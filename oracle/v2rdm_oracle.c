@@ -8,7 +8,7 @@
  * the reference bit for bit.  Each function cites the reference code it
  * restates (paths relative to the hilbert source tree).
  *
- * Supported constraint sets: POSITIVITY D / DQ / DG / DQG with
+ * Supported constraint sets: POSITIVITY D / DQ / DG / DQG / DQGT2 with
  * CONSTRAIN_SPIN and CONSTRAIN_SZ on or off, singlet and non-singlet.
  */
 #include <math.h>
@@ -18,11 +18,14 @@
 typedef struct {
     int n;            /* active orbitals (amo_) */
     int na, nb;       /* alpha / beta electrons */
-    int q2, g2, spin, sz;
+    int q2, g2, t2, spin, sz;
     int mult;         /* 2S+1 as the reference stores it */
     int gab, gaa;
     int *bas_ab, *ibas_ab, *bas_aa, *ibas_aa;
     long d2ab, d2aa, d2bb, d200, d1a, d1b, q1a, q1b, q2ab, q2aa, q2bb, g2ab, g2ba, g2aa;
+    long t2aaa, t2bbb, t2aab, t2bba;
+    int trip_aab, trip_aba;   /* triplets (i<j, k) and (i, j, k) */
+    int *bas_aab, *bas_aba;   /* 3 ints per triplet */
     long n_primal, n_dual;
     int nblocks;
     int dims[32];
@@ -61,6 +64,10 @@ static void build_tables(v2o_problem *p) {
 #define IAB(p, i, j) ((p)->ibas_ab[(i) * (p)->n + (j)])
 #define IAA(p, i, j) ((p)->ibas_aa[(i) * (p)->n + (j)])
 
+enum { T2_AU = 0, T2_ATU = 1, T2_GUESS = 2 };
+static void t2_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
+                     double *x);
+
 /* v2rdm_solver.cc:3729-4079 (set_primal_offsets) and 3294-3727 (sizes) */
 static void set_offsets(v2o_problem *p) {
     long off = 0;
@@ -90,6 +97,15 @@ static void set_offsets(v2o_problem *p) {
         p->g2ba = off; off += (long)gab * gab; p->dims[nb++] = gab;
         p->g2aa = off; off += 4L * gab * gab; p->dims[nb++] = 2 * gab;
     }
+    /* v2rdm_solver.cc:3879-3906: T2aaa, T2bbb (dim aab + aba), T2aab, T2bba (dim aab) */
+    p->t2aaa = p->t2bbb = p->t2aab = p->t2bba = -1;
+    if (p->t2) {
+        long w = (long)p->trip_aab + p->trip_aba, ta = p->trip_aab;
+        p->t2aaa = off; off += w * w; p->dims[nb++] = (int)w;
+        p->t2bbb = off; off += w * w; p->dims[nb++] = (int)w;
+        p->t2aab = off; off += ta * ta; p->dims[nb++] = (int)ta;
+        p->t2bba = off; off += ta * ta; p->dims[nb++] = (int)ta;
+    }
     p->n_primal = off;
     p->nblocks = nb;
 
@@ -106,21 +122,48 @@ static void set_offsets(v2o_problem *p) {
     }
     if (p->q2) d += (long)gab * gab + 2L * gaa * gaa;
     if (p->g2) d += 6L * gab * gab;
+    if (p->t2) {   /* v2rdm_solver.cc:3568-3580 */
+        long w = (long)p->trip_aab + p->trip_aba, ta = p->trip_aab;
+        d += 2 * w * w + 2 * ta * ta;
+    }
     p->n_dual = d;
 }
 
-/* positivity: 0 D, 1 DQ, 2 DG, 3 DQG (v2rdm_solver.cc:4081-4118).
+/* basis.cc:640-745 (C1): every (i, j, k) in i, j, k order is an aba triplet;
+ * those with i < j are also aab triplets, numbered in the same sweep. */
+static void build_triplets(v2o_problem *p) {
+    int n = p->n;
+    long n3 = (long)n * n * n;
+    p->bas_aba = (int *)malloc(sizeof(int) * 3 * (n3 > 0 ? n3 : 1));
+    p->bas_aab = (int *)malloc(sizeof(int) * 3 * (n3 > 0 ? n3 : 1));
+    int ca = 0, cb = 0;
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++)
+            for (int k = 0; k < n; k++) {
+                int *t = p->bas_aba + 3 * cb++;
+                t[0] = i; t[1] = j; t[2] = k;
+                if (i >= j) continue;
+                t = p->bas_aab + 3 * ca++;
+                t[0] = i; t[1] = j; t[2] = k;
+            }
+    p->trip_aab = ca;
+    p->trip_aba = cb;
+}
+
+/* positivity: 0 D, 1 DQ, 2 DG, 3 DQG, 4 DQGT2 (v2rdm_solver.cc:4081-4118).
  * hubbard selects the multiplicity convention of
  * v2rdm_solver.cc:862-863 (Hubbard) versus :983-984 (external). */
 v2o_problem *v2o_create(int n, int na, int nb, int positivity, int spin, int sz, int hubbard) {
-    if (n < 1 || na < 0 || nb < 0 || na > n || nb > n) return NULL;
+    if (n < 1 || na < 0 || nb < 0 || na > n || nb > n || positivity < 0 || positivity > 4) return NULL;
     v2o_problem *p = (v2o_problem *)calloc(1, sizeof(v2o_problem));
     p->n = n; p->na = na; p->nb = nb;
-    p->q2 = (positivity == 1 || positivity == 3);
-    p->g2 = (positivity == 2 || positivity == 3);
+    p->q2 = (positivity == 1 || positivity == 3 || positivity == 4);
+    p->g2 = (positivity == 2 || positivity == 3 || positivity == 4);
+    p->t2 = positivity == 4;
     p->spin = spin != 0; p->sz = sz != 0;
     p->mult = hubbard ? 2 * (na - nb) + 1 : (na - nb) + 1;
     build_tables(p);
+    if (p->t2) build_triplets(p);
     set_offsets(p);
     return p;
 }
@@ -128,6 +171,7 @@ v2o_problem *v2o_create(int n, int na, int nb, int positivity, int spin, int sz,
 void v2o_destroy(v2o_problem *p) {
     if (!p) return;
     free(p->bas_ab); free(p->ibas_ab); free(p->bas_aa); free(p->ibas_aa);
+    free(p->bas_aab); free(p->bas_aba);
     free(p);
 }
 
@@ -144,8 +188,9 @@ void v2o_tables(const v2o_problem *p, int *bas_ab, int *ibas_ab, int *bas_aa, in
 }
 /* block offsets in the order d2ab d2aa d2bb d200 d1a d1b q1a q1b q2ab q2aa q2bb g2ab g2ba g2aa */
 void v2o_offsets(const v2o_problem *p, long *o) {
-    long v[14] = {p->d2ab, p->d2aa, p->d2bb, p->d200, p->d1a, p->d1b, p->q1a,
-                  p->q1b,  p->q2ab, p->q2aa, p->q2bb, p->g2ab, p->g2ba, p->g2aa};
+    long v[18] = {p->d2ab, p->d2aa, p->d2bb, p->d200, p->d1a, p->d1b, p->q1a,
+                  p->q1b,  p->q2ab, p->q2aa, p->q2bb, p->g2ab, p->g2ba, p->g2aa,
+                  p->t2aaa, p->t2bbb, p->t2aab, p->t2bba};
     memcpy(o, v, sizeof(v));
 }
 
@@ -395,6 +440,139 @@ void v2o_guess_hf(const v2o_problem *p, double *x) {
     for (int i = occ; i < n; i++) x[p->q1b + i * n + i] = 1.0;
     if (p->q2) q2_guess(p, x);
     if (p->g2) g2_guess(p, x);
+    if (p->t2) t2_visit(p, 0, T2_GUESS, NULL, NULL, x);   /* v2rdm_solver.cc:1820-1822 */
+}
+
+/* ------------------------------------------------------------- T2 ---- */
+/* The T2 rows of t2.cc:1236-1843 (T2_constraints_Au_slow, C1).  Each dual
+ * row belongs to one element (r, c) of a T2 block and reads
+ *     -T2(r, c) + sum of conditional D2 / D1 terms with coefficients +-1,
+ * the terms added left to right in the order the reference adds them.  The
+ * ten sub-blocks, in the reference's order of dual rows:
+ *   0 T2aab (rows, cols: aab triplets)            t2.cc:1239-1302
+ *   1 T2bba                                        t2.cc:1305-1368
+ *   2-5 T2aaa: aaa/aaa, aaa/abb, abb/aaa, abb/abb t2.cc:1371-1601
+ *   6-9 T2bbb: bbb/bbb, bbb/baa, baa/bbb, baa/baa t2.cc:1604-1840
+ * ("aaa" rows/cols are the aab triplets, "abb" / "baa" the aba triplets,
+ * placed after them in the big blocks). */
+typedef struct { long col; double coef; } t2_term;
+
+#define T2_D2AA(a, b, c, d) (p->d2aa + (long)IAA(p, a, b) * p->gaa + IAA(p, c, d))
+#define T2_D2BB(a, b, c, d) (p->d2bb + (long)IAA(p, a, b) * p->gaa + IAA(p, c, d))
+#define T2_D2AB(a, b, c, d) (p->d2ab + (long)IAB(p, a, b) * p->gab + IAB(p, c, d))
+#define T2_D1A(a, b) (p->d1a + (long)(a) * p->n + (b))
+#define T2_D1B(a, b) (p->d1b + (long)(a) * p->n + (b))
+#define T2_ADD(c, v) do { t[nt].col = (c); t[nt].coef = (v); nt++; } while (0)
+
+/* sign of an aa geminal read as (a, b): -1 when a > b (the reference's s) */
+static double pair_sign(int a, int b) { return a > b ? -1.0 : 1.0; }
+
+/* terms of row (i, j, k) x column (l, m, q) of sub-block sb, at most 7 */
+static int t2_terms(const v2o_problem *p, int sb, int i, int j, int k, int l, int m, int q,
+                    t2_term *t) {
+    int nt = 0;
+    switch (sb) {
+    case 0:   /* T2aab */
+    case 1: { /* T2bba: the same terms with alpha and beta exchanged */
+        const int b = sb == 1;
+        if (k == q) T2_ADD(b ? T2_D2BB(i, j, l, m) : T2_D2AA(i, j, l, m), 1.0);
+        if (j == m && i == l) T2_ADD(b ? T2_D1A(q, k) : T2_D1B(q, k), 1.0);
+        if (j == l && i == m) T2_ADD(b ? T2_D1A(q, k) : T2_D1B(q, k), -1.0);
+        if (i == l) T2_ADD(b ? T2_D2AB(q, j, k, m) : T2_D2AB(j, q, m, k), -1.0);
+        if (j == l) T2_ADD(b ? T2_D2AB(q, i, k, m) : T2_D2AB(i, q, m, k), 1.0);
+        if (i == m) T2_ADD(b ? T2_D2AB(q, j, k, l) : T2_D2AB(j, q, l, k), 1.0);
+        if (j == m) T2_ADD(b ? T2_D2AB(q, i, k, l) : T2_D2AB(i, q, l, k), -1.0);
+        break;
+    }
+    case 2:   /* aaa/aaa */
+    case 6: { /* bbb/bbb */
+        const int b = sb == 6;
+        if (k == q) T2_ADD(b ? T2_D2BB(i, j, l, m) : T2_D2AA(i, j, l, m), 1.0);
+        if (j == m && i == l) T2_ADD(b ? T2_D1B(q, k) : T2_D1A(q, k), 1.0);
+        if (j == l && i == m) T2_ADD(b ? T2_D1B(q, k) : T2_D1A(q, k), -1.0);
+        if (i == l && q != j && k != m)
+            T2_ADD(b ? T2_D2BB(q, j, k, m) : T2_D2AA(q, j, k, m), -pair_sign(q, j) * pair_sign(k, m));
+        if (j == l && q != i && k != m)
+            T2_ADD(b ? T2_D2BB(q, i, k, m) : T2_D2AA(q, i, k, m), pair_sign(q, i) * pair_sign(k, m));
+        if (i == m && q != j && k != l)
+            T2_ADD(b ? T2_D2BB(q, j, k, l) : T2_D2AA(q, j, k, l), pair_sign(q, j) * pair_sign(k, l));
+        if (j == m && q != i && k != l)
+            T2_ADD(b ? T2_D2BB(q, i, k, l) : T2_D2AA(q, i, k, l), -pair_sign(q, i) * pair_sign(k, l));
+        break;
+    }
+    case 3:   /* aaa/abb */
+        if (i == l) T2_ADD(T2_D2AB(j, q, k, m), 1.0);
+        if (j == l) T2_ADD(T2_D2AB(i, q, k, m), -1.0);
+        break;
+    case 7:   /* bbb/baa */
+        if (i == l) T2_ADD(T2_D2AB(q, j, m, k), 1.0);
+        if (j == l) T2_ADD(T2_D2AB(q, i, m, k), -1.0);
+        break;
+    case 4:   /* abb/aaa */
+        if (i == l) T2_ADD(T2_D2AB(q, j, m, k), 1.0);
+        if (i == m) T2_ADD(T2_D2AB(q, j, l, k), -1.0);
+        break;
+    case 8:   /* baa/bbb */
+        if (i == l) T2_ADD(T2_D2AB(j, q, k, m), 1.0);
+        if (i == m) T2_ADD(T2_D2AB(j, q, k, l), -1.0);
+        break;
+    case 5:   /* abb/abb */
+        if (k == q) T2_ADD(T2_D2AB(i, j, l, m), 1.0);
+        if (j == m && i == l) T2_ADD(T2_D1B(q, k), 1.0);
+        if (i == l && q != j && k != m) T2_ADD(T2_D2BB(q, j, k, m), -pair_sign(q, j) * pair_sign(k, m));
+        if (j == m) T2_ADD(T2_D2AB(i, q, l, k), -1.0);
+        break;
+    case 9:   /* baa/baa */
+        if (k == q) T2_ADD(T2_D2AB(j, i, m, l), 1.0);
+        if (j == m && i == l) T2_ADD(T2_D1A(q, k), 1.0);
+        if (i == l && q != j && k != m) T2_ADD(T2_D2AA(q, j, k, m), -pair_sign(q, j) * pair_sign(k, m));
+        if (j == m) T2_ADD(T2_D2AB(q, i, k, l), -1.0);
+        break;
+    }
+    return nt;
+}
+
+/* Visit every T2 row in the reference's order, dual rows from off.
+ *  T2_AU:    A[row] = -u[t2] + terms                       (t2.cc:1236-1843)
+ *  T2_ATU:   A[t2] -= u[row], A[col] += coef u[row]         (t2.cc:3376-3966,
+ *            the scatter of the same terms in the same order)
+ *  T2_GUESS: u[t2] = 0 + terms, zero on aaa/abb             (t2.cc:1845-2452) */
+static void t2_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
+                     double *x) {
+    const long ta = p->trip_aab, tb = p->trip_aba, w = ta + tb;
+    const long dual[4] = {off, off + ta * ta, off + 2 * ta * ta, off + 2 * ta * ta + w * w};
+    const long prim[4] = {p->t2aab, p->t2bba, p->t2aaa, p->t2bbb};
+    for (int sb = 0; sb < 10; sb++) {
+        const int blk = sb < 2 ? sb : (sb < 6 ? 2 : 3);
+        const long width = sb < 2 ? ta : w;
+        const int rows_aba = (sb == 4 || sb == 5 || sb == 8 || sb == 9);
+        const int cols_aba = (sb == 3 || sb == 5 || sb == 7 || sb == 9);
+        const long nr = rows_aba ? tb : ta, nc = cols_aba ? tb : ta;
+        const long r0 = rows_aba ? ta : 0, c0 = cols_aba ? ta : 0;
+        const int *rb = rows_aba ? p->bas_aba : p->bas_aab, *cb = cols_aba ? p->bas_aba : p->bas_aab;
+        for (long r = 0; r < nr; r++) {
+            const int i = rb[3 * r], j = rb[3 * r + 1], k = rb[3 * r + 2];
+            for (long c = 0; c < nc; c++) {
+                const int l = cb[3 * c], m = cb[3 * c + 1], q = cb[3 * c + 2];
+                const long id = (r0 + r) * width + (c0 + c);
+                t2_term t[8];
+                const int nt = t2_terms(p, sb, i, j, k, l, m, q, t);
+                if (mode == T2_AU) {
+                    double dum = -u[prim[blk] + id];
+                    for (int e = 0; e < nt; e++) dum += t[e].coef * u[t[e].col];
+                    A[dual[blk] + id] = dum;
+                } else if (mode == T2_ATU) {
+                    const double dum = u[dual[blk] + id];
+                    A[prim[blk] + id] -= dum;
+                    for (int e = 0; e < nt; e++) A[t[e].col] += t[e].coef * dum;
+                } else {
+                    double dum = 0.0;
+                    for (int e = 0; e < nt; e++) dum += t[e].coef * x[t[e].col];
+                    x[prim[blk] + id] = sb == 3 ? 0.0 : dum;
+                }
+            }
+        }
+    }
 }
 
 /* ------------------------------------------------------------- A.x ---- */
@@ -737,6 +915,7 @@ void v2o_Au(const v2o_problem *p, const double *u, double *A) {
         }
         off += 4L * gab * gab;
     }
+    if (p->t2) t2_visit(p, off, T2_AU, u, A, NULL);   /* v2rdm_solver.cc:3019-3022 */
 }
 
 /* ----------------------------------------------------------- A^T.y ---- */
@@ -1068,4 +1247,5 @@ void v2o_ATu(const v2o_problem *p, const double *u, double *A) {
         }
         off += 4L * gab * gab;
     }
+    if (p->t2) t2_visit(p, off, T2_ATU, u, A, NULL);   /* v2rdm_solver.cc:3077-3080 */
 }

@@ -19,7 +19,8 @@ def test_golden_cases_present(golden):
 
 
 @pytest.mark.parametrize("name", ["hub2_dqg", "hub4_dqg", "hub4_d_nospin", "ext3_dqg_triplet",
-                                  "ext4_dq_nosz", "ext4_dg_doublet", "ext5_dqg", "ext1_dqg"])
+                                  "ext4_dq_nosz", "ext4_dg_doublet", "ext5_dqg", "ext1_dqg",
+                                  "hub3_dqgt2", "ext3_dqgt2_doublet"])
 def test_oracle_matches_golden(golden, name):
     case = golden[name]
     kw = case_kwargs(case)
@@ -49,7 +50,8 @@ def test_sizes_match_reference_counts():
 
 def test_adjoint_identity():
     rng = np.random.default_rng(7)
-    for n, na, nb, pos, spin, sz in [(4, 2, 2, "DQG", 1, 1), (5, 3, 2, "DQG", 1, 0), (3, 1, 1, "DG", 0, 1)]:
+    for n, na, nb, pos, spin, sz in [(4, 2, 2, "DQG", 1, 1), (5, 3, 2, "DQG", 1, 0), (3, 1, 1, "DG", 0, 1),
+                                     (3, 2, 1, "DQGT2", 1, 1), (4, 2, 2, "DQGT2", 0, 1)]:
         o = OracleProblem(n, na, nb, pos, spin, sz, h=rng.standard_normal((n, n)),
                           g=rng.standard_normal((n,) * 4))
         x = rng.standard_normal(o.n_primal)
@@ -73,7 +75,7 @@ def test_hf_guess_satisfies_d_constraints():
 def test_oracle_bit_exact_against_reference_grid():
     rng = np.random.default_rng(3)
     for n, na, nb, pos, spin, sz in itertools.product([1, 2, 3, 4], [0, 1, 2], [0, 1, 2],
-                                                      ["D", "DQ", "DG", "DQG"], [0, 1], [0, 1]):
+                                                      ["D", "DQ", "DG", "DQG", "DQGT2"], [0, 1], [0, 1]):
         if na > n or nb > n:
             continue
         kw = dict(h=rng.standard_normal((n, n)), g=rng.standard_normal((n,) * 4))
@@ -86,3 +88,31 @@ def test_oracle_bit_exact_against_reference_grid():
         y = rng.standard_normal(r.n_dual)
         assert same(r.Au(x), o.Au(x)) and same(r.ATu(y), o.ATu(y))
         assert same(r.b, o.b) and same(r.c, o.c)
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+def test_oracle_t2_guesses_bit_exact_against_reference_grid():
+    """The T2 part of the HF guess (t2.cc:1845-2452) and the random guess
+    with T2 blocks present, against hilbert's compiled code."""
+    rng = np.random.default_rng(11)
+    for n, na, nb, spin, sz in itertools.product([1, 2, 3, 4], [0, 1, 2], [0, 1, 2], [0, 1], [0, 1]):
+        if na > n or nb > n:
+            continue
+        kw = dict(h=rng.standard_normal((n, n)), g=rng.standard_normal((n,) * 4))
+        o = OracleProblem(n, na, nb, "DQGT2", spin, sz, **kw)
+        for kind in ("random", "hf"):
+            r = RefProblem(n, na, nb, "DQGT2", spin, sz, guess=kind, **kw)
+            assert same(r.x0, o.guess(kind)), (n, na, nb, spin, sz, kind)
+
+
+def test_t2_blocks_and_rows_follow_the_triplet_counts():
+    """T2aaa / T2bbb have n^2 (n - 1) / 2 + n^3 rows, T2aab / T2bba
+    n^2 (n - 1) / 2 (v2rdm_solver.cc:3879-3906); the T2 rows are zero in b."""
+    n = 4
+    o = OracleProblem(n, 2, 2, "DQGT2", True, True, hubbard=(1.0, 4.0))
+    d = OracleProblem(n, 2, 2, "DQG", True, True, hubbard=(1.0, 4.0))
+    ta, tb = n * n * (n - 1) // 2, n ** 3
+    assert list(o.dims[len(d.dims):]) == [ta + tb, ta + tb, ta, ta]
+    assert o.n_primal - d.n_primal == 2 * (ta + tb) ** 2 + 2 * ta * ta
+    assert o.n_dual - d.n_dual == o.n_primal - d.n_primal
+    assert not np.any(o.b[d.n_dual:])
