@@ -4,7 +4,7 @@ through a hand-written adjoint of the integral transform.
 
 With U = exp(kappa) (kappa antisymmetric), the transformed integrals are
 h' = U^T h U and B'^Q = U^T B^Q U ((pq|rs) = sum_Q B^Q_pq B^Q_rs, focas's DF
-transform, src/focas/C_files/orbopt_integraltransform_cpu.cc:25-329), and
+transform, src/focas/orbopt_integraltransform_cpu.cc:25-329), and
 
     E(kappa) = sum_pq h'_pq D_pq + 1/2 sum_Q b'_Q^T Gm b'_Q,    b'_Q = vec(B'^Q),
 
@@ -16,6 +16,12 @@ as the upper-right block of exp([[kappa^T, dE/dU], [0, kappa^T]]).  At
 kappa = 0 the rotation-pair gradient dE/dkappa_pq - dE/dkappa_qp (p > q) is
 focas's orbital gradient (orbopt_gradient.cc:26-147: ed = 4 (Fi + Fa),
 ea = 2 (Q + Z), ad = 4 (Fi + Fa) - 2 (Q + Z)).
+
+Orbital steps at fixed densities: optimize_orbitals (L-BFGS on the adjoint
+gradient) or optimize_orbitals_focas, focas's own step (src/focas/
+orbopt_optimize.cc:25-96): kappa = -r g / max(|H_diag|, 1e-2) with focas's
+exact diagonal Hessian (diagonal_hessian, orbopt_hessian.cc) and its trust
+factor r.
 
 The densities come from the device solve through
 V2RDMProblem.pack_spatial_density (hilbert's PackSpatialDensity) and
@@ -194,6 +200,165 @@ def optimize_orbitals(h, B, D, G, pairs, max_iter=100, gtol=1e-10):
     return U, float(E.detach()), float(g0.norm()), float(g1.norm())
 
 
+def _fock_q_z(h, B, Da, Ga, ncore, nact):
+    """focas's intermediates on the full orbital range (orbopt_gradient.cc:
+    Fi 852-1118, Fa 441-851, Q 218-440, Z 185-216):
+    Fi_pq = h_pq + sum_i 2 (pq|ii) - (pi|iq),
+    Fa_pq = sum_tu D_tu [(pq|tu) - 1/2 (pt|uq)],
+    Q_tp = sum_uvw G_tuvw (pu|vw),  Z_tp = sum_u D_tu Fi_pu."""
+    c = slice(0, ncore)
+    a = slice(ncore, ncore + nact)
+    Bd = torch.diagonal(B, dim1=1, dim2=2)                        # B^Q_pp
+    Fi = (h + 2.0 * torch.einsum("Qpq,Q->pq", B, Bd[:, c].sum(1))
+          - torch.einsum("Qpi,Qiq->pq", B[:, :, c], B[:, c, :]))
+    Ba = B[:, a, a]
+    Fa = (torch.einsum("Qpq,Q->pq", B, torch.einsum("Qtu,tu->Q", Ba, Da))
+          - 0.5 * torch.einsum("Qpt,tu,Quq->pq", B[:, :, a], Da, B[:, a, :]))
+    Qm = torch.einsum("Qpu,Qtu->tp", B[:, :, a], torch.einsum("tuvw,Qvw->Qtu", Ga, Ba))
+    Z = Da @ Fi[a, :]
+    return Fi, Fa, Qm, Z
+
+
+def diagonal_hessian(h, B, Da, Ga, ncore, nact):
+    """focas's exact diagonal orbital Hessian (ORBOPT_EXACT_DIAGONAL_HESSIAN,
+    on by default) for the rotation pairs of rotation_pairs(ncore, nact,
+    nvirt) (no active-active pairs), from src/focas/orbopt_hessian.cc:
+      ed (a, i) :426-463   4 [F_aa - F_ii + 3 (ia|ia) - (ii|aa)],  F = Fi + Fa
+      ea (a, t) :830-1047  2 [D_tt Fi_aa - Q_tt - Z_tt] + 2 sum_uv G_ttuv (uv|aa)
+                           + 4 sum_uv G_utvt (ua|va)
+      ad (t, i) :135-424   2 [2 (F_tt - F_ii) + D_tt Fi_ii - Q_tt - Z_tt]
+                           + 2 sum_uv G_ttuv (uv|ii) + 4 [sum_u D_tu (tu|ii) - (tt|ii)]
+                           + 4 sum_uv G_utvt (ui|vi) + 12 [(ti|ti) - sum_u D_tu (ui|ti)]
+    G is the dense spin-summed active 2-RDM, the d2 focas works with after
+    its Sort (orbopt_sort.cc:40-117 rescales the packed elements by 2 / m);
+    the half-triangle sums of the reference become full sums by the pair
+    symmetries of G.  Every (pq|rs) is a contraction of the DF factors."""
+    nmo = h.shape[0]
+    c = slice(0, ncore)
+    a = slice(ncore, ncore + nact)
+    v = slice(ncore + nact, nmo)
+    Fi, Fa, Qm, Z = _fock_q_z(h, B, Da, Ga, ncore, nact)
+    Fd, Fid = torch.diagonal(Fi + Fa), torch.diagonal(Fi)
+    Qtt = torch.diagonal(Qm[:, a])
+    Ztt = torch.diagonal(Z[:, a])
+    Dtt = torch.diagonal(Da)
+    Bd = torch.diagonal(B, dim1=1, dim2=2)                        # (Q, nmo)
+    Ba = B[:, a, a]
+    Bap = B[:, a, :]                                              # B^Q_up
+    # sum_uv G_ttuv (uv|pp) and sum_uv G_utvt (up|vp), for every p
+    coul = torch.einsum("uvt,Quv->tQ", torch.diagonal(Ga, dim1=0, dim2=1), Ba) @ Bd
+    exch = torch.einsum("Qup,uvt,Qvp->tp", Bap, torch.diagonal(Ga, dim1=1, dim2=3), Bap)
+    # ed
+    Bvc = B[:, v, c]
+    H_ed = 4.0 * (Fd[v][:, None] - Fd[c][None, :] + 3.0 * (Bvc * Bvc).sum(0)
+                  - torch.einsum("Qa,Qi->ai", Bd[:, v], Bd[:, c]))
+    # ea, indexed (a, t)
+    H_ea = (2.0 * (Dtt[None, :] * Fid[v][:, None] - (Qtt + Ztt)[None, :])
+            + 2.0 * coul[:, v].T + 4.0 * exch[:, v].T)
+    # ad, indexed (t, i)
+    tupp = torch.einsum("tu,Qtu,Qp->tp", Da, Ba, Bd[:, c])        # sum_u D_tu (tu|ii)
+    ttpp = torch.diagonal(Ba, dim1=1, dim2=2).T @ Bd[:, c]         # (tt|ii)
+    tptp = (Bap[:, :, c] * Bap[:, :, c]).sum(0)                   # (ti|ti)
+    uptp = torch.einsum("tu,Qup,Qtp->tp", Da, Bap[:, :, c], Bap[:, :, c])
+    H_ad = (2.0 * (2.0 * (Fd[a][:, None] - Fd[c][None, :]) + Dtt[:, None] * Fid[c][None, :]
+                   - (Qtt + Ztt)[:, None])
+            + 2.0 * coul[:, c] + 4.0 * (tupp - ttpp) + 4.0 * exch[:, c] + 12.0 * (tptp - uptp))
+    return torch.cat([H_ed.reshape(-1), H_ea.reshape(-1), H_ad.reshape(-1)])
+
+
+def _pair_kappa(theta, pairs, n):
+    p = torch.tensor([x for x, _ in pairs], device=theta.device)
+    q = torch.tensor([y for _, y in pairs], device=theta.device)
+    K = torch.zeros((n, n), dtype=theta.dtype, device=theta.device)
+    K = K.index_put((p, q), theta)
+    return K.index_put((q, p), -theta)
+
+
+def optimize_orbitals_focas(h, B, Da, Ga, ncore, nact, maxiter=10, g_conv=1e-4, e_conv=1e-8):
+    """focas's orbital optimisation at fixed densities (src/focas/
+    orbopt_optimize.cc:25-96; ORBOPT_MAXITER 10, ORBOPT_GRADIENT_CONVERGENCE
+    1e-4, ORBOPT_ENERGY_CONVERGENCE 1e-8 by default, plugin.cc:153-168):
+
+    * with the gradient due: E, g, H at the current orbitals; the quadratic
+      model dE_quad = g.k + 1/2 sum H k^2 of the step k held then (zero on
+      the first iteration, afterwards the last accepted step:
+      Compute_Quadratic_dE runs before Precondition_Step, :162-176); the
+      preconditioned step k_ref = -g / max(|H|, 1e-2) (:247-264), k = r k_ref;
+    * rotate by exp(k) and take dE = E_new - E (the integrals accumulate the
+      rotations, as TransformIntegrals does);
+    * stop on |g| < g_conv, |dE| < e_conv or the last iteration;
+    * Update_r (:117-146): dE < 0: r *= 1.2 if dE / dE_quad > 0.75, r *= 0.7
+      if < 0.25; dE > 0: r *= 0.7 and the gradient is not re-evaluated; the
+      next step k' = r k_ref - k, and the saved step accumulates it
+      (Update_kappa, :98-115);
+    * after the loop, dE > 0 undoes the last step (when converged) and the
+      steps since the last gradient (when it was not re-evaluated)
+      (Restore_last_step, :226-245).
+    Returns U (the product of the rotations), the final energy and a list of
+    per-iteration records (E_new, dE, |g|, r)."""
+    nmo = h.shape[0]
+    nvirt = nmo - ncore - nact
+    pairs = rotation_pairs(ncore, nact, nvirt)
+    D, G = full_densities(Da, Ga, ncore, nvirt)
+    Gm = G.reshape(nmo * nmo, nmo * nmo)
+    zero = torch.zeros((nmo, nmo), dtype=h.dtype, device=h.device)
+    Utot = torch.eye(nmo, dtype=h.dtype, device=h.device)
+
+    def rotate(k):
+        nonlocal h, B, Utot
+        U = torch.linalg.matrix_exp(_pair_kappa(k, pairs, nmo))
+        h = U.T @ h @ U
+        B = U.T @ B @ U
+        Utot = Utot @ U
+
+    def energy():
+        return float(RotatedEnergy.apply(zero, h, B, D, Gm))
+
+    r = 1.0
+    eval_g = True
+    k_cur = torch.zeros(len(pairs), dtype=h.dtype, device=h.device)
+    k_ref = k_save = k_cur
+    E_init = gnorm = dE = 0.0
+    conv_e = conv_g = False
+    history = []
+    for it in range(maxiter):
+        if eval_g:
+            E0, g = orbital_gradient(h, B, D, G, pairs)
+            E_init = float(E0)
+            gnorm = float(torch.sqrt(g @ g))
+            Hd = diagonal_hessian(h, B, Da, Ga, ncore, nact)
+            dE_quad = float(0.5 * (2.0 * (g @ k_cur) + (k_cur * Hd * k_cur).sum()))
+            k_ref = -g / torch.clamp(Hd.abs(), min=1e-2)
+            k_cur = r * k_ref
+            k_save = k_cur.clone()
+        rotate(k_cur)
+        E_new = energy()
+        dE = E_new - E_init
+        history.append((E_new, dE, gnorm, r))
+        conv_g = gnorm < g_conv
+        conv_e = abs(dE) < e_conv
+        if conv_e or conv_g or it == maxiter - 1:
+            break
+        eval_g = not (dE > 0.0)
+        ratio = dE / dE_quad if dE_quad != 0.0 else (-np.inf if dE < 0 else np.inf)
+        if dE < 0.0:
+            if ratio > 0.75:
+                r *= 1.2
+            if ratio < 0.25:
+                r *= 0.7
+        else:
+            r *= 0.7
+        if not eval_g:
+            k_cur = r * k_ref - k_cur
+            k_save = k_save + k_cur
+    if dE > 0.0:
+        if conv_e or conv_g:
+            rotate(-k_cur)
+        if not eval_g:
+            rotate(-k_save)
+    return Utot, energy(), history
+
+
 def active_space(h, B, ncore, nact):
     """Frozen-core energy, active one-electron integrals (the inactive Fock
     block) and active (tu|vw) from MO-basis h and DF factors B (torch)."""
@@ -209,12 +374,19 @@ def active_space(h, B, ncore, nact):
     return e_core, Fi[act, act], g
 
 
-def casscf(h, B, ncore, nact, solve_active, macro_iterations=8, active_active=False):
+def casscf(h, B, ncore, nact, solve_active, macro_iterations=8, active_active=False,
+           orbital_step="lbfgs"):
     """v2RDM-CASSCF macro-iterations: solve the active-space v2RDM in the
     current orbitals (solve_active(h_act, g_act) -> (E_active, packed d2,
     packed d1) on the same device as h), optimise the orbitals at those
-    densities, rotate h and B, repeat.  Returns the energies after each SDP
+    densities, rotate h and B, repeat.  orbital_step: "lbfgs"
+    (optimize_orbitals) or "focas" (optimize_orbitals_focas with focas's
+    defaults; no active-active pairs).  Returns the energies after each SDP
     solve and the orbital-gradient norms at each orbital step."""
+    if orbital_step not in ("lbfgs", "focas"):
+        raise ValueError(f"orbital_step: {orbital_step!r}")
+    if orbital_step == "focas" and active_active:
+        raise ValueError("the focas step takes no active-active rotations")
     nmo = h.shape[0]
     nvirt = nmo - ncore - nact
     pairs = rotation_pairs(ncore, nact, nvirt, active_active)
@@ -224,9 +396,13 @@ def casscf(h, B, ncore, nact, solve_active, macro_iterations=8, active_active=Fa
         e_act, d2p, d1p = solve_active(h_act, g_act)
         energies.append(e_core + e_act)
         Da, Ga = unpack_densities(d2p, d1p, nact)
-        D, G = full_densities(Da, Ga, ncore, nvirt)
-        U, _, gn, _ = optimize_orbitals(h, B, D, G, pairs)
-        gnorms.append(gn)
+        if orbital_step == "focas":
+            U, _, hist = optimize_orbitals_focas(h, B, Da, Ga, ncore, nact)
+            gnorms.append(hist[0][2])
+        else:
+            D, G = full_densities(Da, Ga, ncore, nvirt)
+            U, _, gn, _ = optimize_orbitals(h, B, D, G, pairs)
+            gnorms.append(gn)
         h = U.T @ h @ U
         B = U.T @ B @ U
     return energies, gnorms, h, B

@@ -6,12 +6,16 @@ never the measured path).
   (src/v2rdm_casscf/v2rdm_solver.cc:3110-3219) for C1 active spaces.
   Pinned bit-exactly to the reference's own compiled function
   (oracle/_ref, tests/test_orbital.py).
-* focas_gradient: the orbital gradient of focas (src/focas/C_files/
-  orbopt_gradient.cc:26-147 with Fi 863-1130, Fa 450-860, Q 223-449,
-  Z 189-222) restated on dense matrices from the same definitions: inactive
+* focas_gradient: the orbital gradient of focas (src/focas/
+  orbopt_gradient.cc:26-146 with Fi 852-1118, Fa 441-851, Q 218-440,
+  Z 185-216) restated on dense matrices from the same definitions: inactive
   Fock Fi, active Fock Fa, Q and Z, gradient blocks
   ed = 4 (Fi + Fa), ea = 2 (Q + Z), ad = 4 (Fi + Fa) - 2 (Q + Z), aa
   (optional) = 2 (Q + Z - (Q + Z)^T).
+* focas_diagonal_hessian: focas's exact diagonal Hessian
+  (src/focas/orbopt_hessian.cc), literally, loops and half-triangle sums.
+* focas_optimize: focas's orbital step loop (src/focas/orbopt_optimize.cc:
+  25-264) on these, with scipy's expm.
 """
 import numpy as np
 
@@ -130,13 +134,9 @@ def energy(h, eri, D, G):
     return float(np.einsum("pq,pq->", h, D) + 0.5 * np.einsum("pqrs,pqrs->", eri, G))
 
 
-def focas_gradient(h, B, D_act, G_act, ncore, nact, active_active=False):
-    """focas's orbital gradient on dense matrices (see module docstring).
-
-    h: (nmo, nmo) one-electron integrals; B: (naux, nmo, nmo) DF factors,
-    (pq|rs) = sum_Q B[Q,p,q] B[Q,r,s]; D_act, G_act: dense spin-summed active
-    densities.  Returns {(p, q): g} for the rotation pairs p > q of different
-    classes (core 0, active 1, virtual 2), focas's sign convention."""
+def _focas_intermediates(h, B, D_act, G_act, ncore, nact):
+    """eri, Fi, Fa, Q (nact x nmo) and Z (nact x nmo) as focas defines them
+    (orbopt_gradient.cc: Fi 852-1118, Fa 441-851, Q 218-440, Z 185-216)."""
     nmo = h.shape[0]
     core = list(range(ncore))
     act = list(range(ncore, ncore + nact))
@@ -160,6 +160,89 @@ def focas_gradient(h, B, D_act, G_act, ncore, nact, active_active=False):
     for ti in range(nact):
         for p in range(nmo):
             Zm[ti, p] = sum(D_act[ti, ui] * Fi[p, u] for ui, u in enumerate(act))
+    return eri, Fi, Fa, Qm, Zm
+
+
+def focas_diagonal_hessian(h, B, d2p, d1p, ncore, nact):
+    """focas's exact diagonal orbital Hessian (ORBOPT_EXACT_DIAGONAL_HESSIAN,
+    on by default, plugin.cc:162), restated on dense integrals from
+    orbopt_hessian.cc.  d2p, d1p: PackSpatialDensity's output; focas's Sort
+    (orbopt_sort.cc:40-117) rescales each packed element by 2 / m (m the size
+    of its index orbit) on entry, so the d2(tu|vw) of the formulas below is
+    the dense spin-summed 2-RDM G_tuvw:
+      ed (a, i)  ComputeH_diag_ed, :426-463
+                 4 [F_aa - F_ii + 3 (ia|ia) - (ii|aa)],   F = Fi + Fa
+      ad (t, i)  ComputeH_diag_ad, :135-188, and tei_terms_H_ad, :190-424
+                 2 [2 (F_tt - F_ii) + D_tt Fi_ii - Q_tt - Z_tt]
+                 + sum_u [sum_{v<u} 4 d2(tt|uv) (uv|ii) + 2 d2(tt|uu) (uu|ii)]
+                 + 4 [sum_u D_tu (tu|ii) - (tt|ii)]
+                 + sum_uv 4 d2(tu|tv) (ui|vi) + 12 [(ti|ti) - sum_u D_tu (ui|ti)]
+      ea (a, t)  ComputeH_diag_ea, :830-870, and tei_terms_H_ea, :872-1047
+                 2 [D_tt Fi_aa - Q_tt - Z_tt]
+                 + 4 sum_u [sum_{v<u} d2(tt|uv) (uv|aa) + 1/2 d2(tt|uu) (uu|aa)]
+                 + 8 sum_u [sum_{v<u} (ua|va) d2(ut|vt) + 1/2 (ua|ua) d2(ut|ut)]
+    Returns {(p, q): H} for the pairs of different classes, keyed like
+    focas_gradient."""
+    nmo = h.shape[0]
+    core = list(range(ncore))
+    act = list(range(ncore, ncore + nact))
+    virt = list(range(ncore + nact, nmo))
+    D_act, G_act = unpack_active(d2p, d1p, nact)
+    eri, Fi, Fa, Qm, Zm = _focas_intermediates(h, B, D_act, G_act, ncore, nact)
+    F = Fi + Fa
+
+    def P(a, b, c, d):   # focas's d2(ab|cd) after its rescale (active local indices)
+        return G_act[a, b, c, d]
+
+    H = {}
+    for a_ in virt:
+        for i in core:
+            H[(a_, i)] = 4.0 * (F[a_, a_] - F[i, i] + 3.0 * eri[i, a_, i, a_] - eri[i, i, a_, a_])
+    for a_ in virt:
+        for t in range(nact):
+            T = act[t]
+            v = 2.0 * (D_act[t, t] * Fi[a_, a_] - Qm[t, T] - Zm[t, T])
+            c = 0.0
+            for u in range(nact):
+                for w in range(u):
+                    c += P(t, t, u, w) * eri[act[u], act[w], a_, a_]
+                c += 0.5 * P(t, t, u, u) * eri[act[u], act[u], a_, a_]
+            x = 0.0
+            for u in range(nact):
+                for w in range(u):
+                    x += eri[act[u], a_, act[w], a_] * P(u, t, w, t)
+                x += 0.5 * eri[act[u], a_, act[u], a_] * P(u, t, u, t)
+            H[(a_, T)] = v + 4.0 * c + 8.0 * x
+    for t in range(nact):
+        T = act[t]
+        for i in core:
+            v = 2.0 * (2.0 * (F[T, T] - F[i, i]) + D_act[t, t] * Fi[i, i] - Qm[t, T] - Zm[t, T])
+            c = 0.0
+            for u in range(nact):
+                for w in range(u):
+                    c += 4.0 * P(t, t, u, w) * eri[act[u], act[w], i, i]
+                c += 2.0 * P(t, t, u, u) * eri[act[u], act[u], i, i]
+            d = -eri[T, T, i, i] + sum(D_act[t, u] * eri[T, act[u], i, i] for u in range(nact))
+            x = 0.0
+            for u in range(nact):
+                for w in range(nact):
+                    x += 4.0 * P(t, u, t, w) * eri[act[u], i, act[w], i]
+            e = eri[T, i, T, i] - sum(D_act[t, u] * eri[act[u], i, T, i] for u in range(nact))
+            H[(T, i)] = v + c + 4.0 * d + x + 12.0 * e
+    return H
+
+
+def focas_gradient(h, B, D_act, G_act, ncore, nact, active_active=False):
+    """focas's orbital gradient on dense matrices (see module docstring).
+
+    h: (nmo, nmo) one-electron integrals; B: (naux, nmo, nmo) DF factors,
+    (pq|rs) = sum_Q B[Q,p,q] B[Q,r,s]; D_act, G_act: dense spin-summed active
+    densities.  Returns {(p, q): g} for the rotation pairs p > q of different
+    classes (core 0, active 1, virtual 2), focas's sign convention."""
+    nmo = h.shape[0]
+    core = list(range(ncore))
+    act = list(range(ncore, ncore + nact))
+    eri, Fi, Fa, Qm, Zm = _focas_intermediates(h, B, D_act, G_act, ncore, nact)
     virt = list(range(ncore + nact, nmo))
     g = {}
     for a_ in virt:
@@ -176,3 +259,97 @@ def focas_gradient(h, B, D_act, G_act, ncore, nact, active_active=False):
             for ui, u in enumerate(act[:ti]):
                 g[(t, u)] = 2.0 * (Qm[ui, t] + Zm[ui, t] - Qm[ti, u] - Zm[ti, u])
     return g
+
+
+def rotation_pairs(ncore, nact, nvirt):
+    """focas's rotation order without active-active pairs (Grad_IndMap,
+    orbopt_gradient.cc:147-183): virtual-core, virtual-active, active-core."""
+    core = range(ncore)
+    act = range(ncore, ncore + nact)
+    virt = range(ncore + nact, ncore + nact + nvirt)
+    return ([(p, q) for p in virt for q in core] + [(p, q) for p in virt for q in act]
+            + [(p, q) for p in act for q in core])
+
+
+def focas_optimize(h, B, d2p, d1p, ncore, nact, maxiter=10, g_conv=1e-4, e_conv=1e-8):
+    """focas's optimize_orbitals (src/focas/orbopt_optimize.cc:25-96) with
+    Update_kappa (:98-115), Update_r (:117-146), Compute_Quadratic_dE
+    (:162-176), Restore_last_step (:226-245) and Precondition_Step
+    (:247-264), at fixed densities, on dense numpy integrals.  The rotation
+    of a step k is expm(K), K[p, q] = k_pq, K[q, p] = -k_pq for the pairs
+    p > q (ExponentiateKappa, orbopt_exponential.cc:151-182); the integrals
+    accumulate the rotations.  Returns (h, B, U, history) with history the
+    per-iteration (E_new, dE, |g|, r)."""
+    from scipy.linalg import expm
+    nmo = h.shape[0]
+    nvirt = nmo - ncore - nact
+    pairs = rotation_pairs(ncore, nact, nvirt)
+    D_act, G_act = unpack_active(d2p, d1p, nact)
+    D, G = full_densities(D_act, G_act, ncore)
+    if nvirt:
+        Dn = np.zeros((nmo, nmo)); Dn[:D.shape[0], :D.shape[0]] = D
+        Gn = np.zeros((nmo,) * 4); m = D.shape[0]; Gn[:m, :m, :m, :m] = G
+        D, G = Dn, Gn
+    h, B = h.copy(), B.copy()
+    U = np.eye(nmo)
+
+    def rotate(k):
+        nonlocal h, B, U
+        K = np.zeros((nmo, nmo))
+        for (p, q), v in zip(pairs, k):
+            K[p, q], K[q, p] = v, -v
+        R = expm(K)
+        h = R.T @ h @ R
+        B = np.einsum("mp,Qmn,nq->Qpq", R, B, R)
+        U = U @ R
+
+    def E():
+        return energy(h, np.einsum("Qpq,Qrs->pqrs", B, B), D, G)
+
+    r, eval_g = 1.0, True
+    k_cur = np.zeros(len(pairs))
+    k_ref, k_save = k_cur.copy(), k_cur.copy()
+    E_init = gnorm = dE = 0.0
+    conv_e = conv_g = False
+    hist = []
+    for it in range(maxiter):
+        if eval_g:
+            E_init = E()
+            gd = focas_gradient(h, B, D_act, G_act, ncore, nact)
+            g = np.array([gd[pq] for pq in pairs])
+            gnorm = float(np.sqrt(g @ g))
+            Hd_ = focas_diagonal_hessian(h, B, d2p, d1p, ncore, nact)
+            Hd = np.array([Hd_[pq] for pq in pairs])
+            dE_quad = 0.5 * (2.0 * (g @ k_cur) + float(np.sum(k_cur * Hd * k_cur)))
+            Hc = np.abs(Hd)
+            Hc[Hc < 1e-2] = 1e-2
+            k_ref = -g / Hc
+            k_cur = r * k_ref
+            k_save = k_cur.copy()
+        rotate(k_cur)
+        E_new = E()
+        dE = E_new - E_init
+        hist.append((E_new, dE, gnorm, r))
+        conv_g = gnorm < g_conv
+        conv_e = abs(dE) < e_conv
+        if conv_e or conv_g or it == maxiter - 1:
+            break
+        eval_g = not (dE > 0.0)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            ratio = np.float64(dE) / np.float64(dE_quad)
+        if dE < 0.0:
+            if ratio > 0.75:
+                r *= 1.2
+            if ratio < 0.25:
+                r *= 0.7
+        else:
+            r *= 0.7
+        if not eval_g:
+            k_cur = r * k_ref - k_cur
+            k_save = k_save + k_cur
+    if dE > 0.0:
+        if conv_e or conv_g:
+            rotate(-k_cur)
+        if not eval_g:
+            rotate(-k_save)
+    return h, B, U, hist

@@ -101,3 +101,73 @@ def test_orbital_step_lowers_energy_at_fixed_densities(small_casscf):
     # the rotated integrals give the optimised energy at kappa = 0
     e2, _ = ho.orbital_gradient(U.T @ h @ U, U.T @ B @ U, D, G, pairs)
     assert abs(e2.item() - e_opt) <= 1e-10
+
+
+def test_diagonal_hessian_matches_focas_and_second_differences(small_casscf):
+    """focas's exact diagonal Hessian: the product's contraction form against
+    the literal restatement of orbopt_hessian.cc (after focas's 2/m rescale
+    of the packed d2), and both against central second differences of E."""
+    s = small_casscf
+    nc, na_, nv = s["nc"], s["na"], s["nv"]
+    Da, Ga = ho.unpack_densities(torch.from_numpy(s["d2p"]), torch.from_numpy(s["d1p"]), na_)
+    h, B = torch.from_numpy(s["h"]), torch.from_numpy(s["B"])
+    pairs = ho.rotation_pairs(nc, na_, nv)
+    H = ho.diagonal_hessian(h, B, Da, Ga, nc, na_).numpy()
+    Hf = oo.focas_diagonal_hessian(s["h"], s["B"], s["d2p"], s["d1p"], nc, na_)
+    Hf = np.array([Hf[pq] for pq in pairs])
+    assert np.max(np.abs(H - Hf)) <= 1e-12 * np.max(np.abs(Hf))
+    D, G = ho.full_densities(Da, Ga, nc, nv)
+    n = h.shape[0]
+    E0 = ho.rotated_energy(torch.zeros((n, n), dtype=torch.float64), h, B, D, G).item()
+    st = 2e-4
+    for k, (p, q) in enumerate(pairs):
+        dK = torch.zeros((n, n), dtype=torch.float64)
+        dK[p, q], dK[q, p] = st, -st
+        fd = (ho.rotated_energy(dK, h, B, D, G).item() - 2.0 * E0
+              + ho.rotated_energy(-dK, h, B, D, G).item()) / st ** 2
+        assert abs(fd - H[k]) <= 1e-5 * max(1.0, abs(H[k])), (p, q, fd, H[k])
+
+
+def _check_focas_trajectory(h, B, s, maxiter, g_conv=1e-4, e_conv=1e-8):
+    nc, na_ = s["nc"], s["na"]
+    Da, Ga = ho.unpack_densities(torch.from_numpy(s["d2p"]), torch.from_numpy(s["d1p"]), na_)
+    U, E, hist = ho.optimize_orbitals_focas(torch.from_numpy(h), torch.from_numpy(B), Da, Ga, nc, na_,
+                                            maxiter=maxiter, g_conv=g_conv, e_conv=e_conv)
+    _, _, Uo, histo = oo.focas_optimize(h, B, s["d2p"], s["d1p"], nc, na_, maxiter=maxiter,
+                                        g_conv=g_conv, e_conv=e_conv)
+    assert len(hist) == len(histo)
+    for a, b in zip(hist, histo):
+        assert abs(a[0] - b[0]) <= 1e-9 and a[3] == b[3]   # energies; identical trust factors
+    assert np.max(np.abs(U.numpy() - Uo)) <= 1e-9
+    return U, E, hist
+
+
+def test_focas_step_follows_the_oracle_with_rejections(small_casscf):
+    """From the fixture's random orbitals (|g| ~ 9): one accepted step, then
+    rejected ones (Update_r, Update_kappa), and Restore_last_step at the end
+    returns to the accepted point; the product and the restated loop take the
+    same path."""
+    s = small_casscf
+    U, E, hist = _check_focas_trajectory(s["h"], s["B"], s, maxiter=10)
+    assert hist[0][1] < 0.0 and any(rec[1] > 0.0 for rec in hist)
+    assert abs(E - hist[0][0]) <= 1e-9          # restored to the accepted step
+    assert E < s["e"] - 1e-2
+
+
+def test_focas_step_converges_near_a_minimum(small_casscf):
+    """Near stationary orbitals (L-BFGS optimum rotated by ~0.02 rad) the
+    accepted focas steps lower the energy and the gradient."""
+    s = small_casscf
+    nc, na_, nv = s["nc"], s["na"], s["nv"]
+    Da, Ga = ho.unpack_densities(torch.from_numpy(s["d2p"]), torch.from_numpy(s["d1p"]), na_)
+    D, G = ho.full_densities(Da, Ga, nc, nv)
+    h, B = torch.from_numpy(s["h"]), torch.from_numpy(s["B"])
+    pairs = ho.rotation_pairs(nc, na_, nv)
+    Ul, _, _, _ = ho.optimize_orbitals(h, B, D, G, pairs, max_iter=500, gtol=1e-12)
+    theta = torch.from_numpy(np.random.default_rng(3).normal(0.0, 0.02, len(pairs)))
+    Up = Ul @ torch.linalg.matrix_exp(ho._pair_kappa(theta, pairs, h.shape[0]))
+    h1, B1 = (Up.T @ h @ Up).numpy(), (Up.T @ B @ Up).numpy()
+    E1, g1 = ho.orbital_gradient(torch.from_numpy(h1), torch.from_numpy(B1), D, G, pairs)
+    U, E, hist = _check_focas_trajectory(h1, B1, s, maxiter=30, g_conv=1e-6, e_conv=1e-12)
+    assert E < E1.item()
+    assert hist[-1][2] < 0.5 * float(g1.norm())
