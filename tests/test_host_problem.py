@@ -112,3 +112,11 @@ def test_device_calls_fail_loudly_without_gpu():
     with pytest.raises(hb.V2BError) as e:
         p.solve(x, p.b(), p.c_hubbard(1.0, 4.0), hb.Options())
     assert e.value.code == _capi.V2B_NO_DEVICE
+
+
+def test_config5_sizes_match_the_oracle():
+    """4x4 Hubbard lattice, DQG + T2: the product's host tables give the
+    reference's sizes and block dimensions (T2 blocks of 1920 and 6016 rows)."""
+    p = hb.V2RDMProblem(16, 8, 8, "DQGT2", True, True, hubbard_multiplicity=True)
+    assert (p.n_primal, p.n_dual) == (80405760, 80515780)
+    assert sorted(set(int(d) for d in p.dims)) == [16, 120, 256, 512, 1920, 6016]
