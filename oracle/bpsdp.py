@@ -21,8 +21,8 @@ Outer protocol (v2rdm_solver.cc:1296-1361 and the reference trace
 tests/mcpdft/output.ref:495-506, 1021-1024): mu starts at 0.1, stays fixed
 inside one ``solve(maxiter)`` call, and afterwards becomes mu * eps_p / eps_d
 (e.g. 0.100 * 6.58093e-3 / 4.47092e-5 = 14.719 at oiter 499).
-The norms (absolute 2-norms) and the CG stopping rule are this build's
-choices: libsdp's own are not available to pin them.
+The norms (absolute 2-norms) and the CG stopping rule are this
+restatement's choices: libsdp's own are not available to pin them.
 """
 import numpy as np
 

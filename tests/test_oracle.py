@@ -39,8 +39,8 @@ def test_oracle_matches_golden(golden, name):
 
 
 def test_sizes_match_reference_counts():
-    # SURVEY-independent anchors: the reference prints n_primal/n_dual; the
-    # (6,6) D2h deck counts are molecular, so pin the C1 formula on config sizes
+    # the reference prints n_primal / n_dual only for its molecular (D2h)
+    # decks, so the C1 formula is pinned on the sizes of the workloads
     o = OracleProblem(8, 4, 4, "DQG", True, True, hubbard=(1.0, 4.0))
     assert (o.n_primal, o.n_dual) == (40256, 47028)
     o = OracleProblem(20, 10, 10, "DQG", True, True, h=np.zeros((20, 20)), g=np.zeros((20,) * 4))
