@@ -35,6 +35,15 @@ def problem(nmo, nalpha, nbeta, positivity="DQG", constrain_spin=True, constrain
     return p
 
 
+def clear():
+    """Release the cached problems (and their device memory)."""
+    with _lock:
+        items = list(_problems.values())
+        _problems.clear()
+    for p in items:
+        p.close()
+
+
 def _sizes(nmo, nalpha, nbeta, positivity, constrain_spin, constrain_sz, hubbard_multiplicity):
     # the host tables alone (no device work): n_primal, n_dual
     p = V2RDMProblem(nmo, nalpha, nbeta, positivity, constrain_spin, constrain_sz,

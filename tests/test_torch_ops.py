@@ -31,3 +31,11 @@ def test_cpu_tensors_are_refused():
     x = torch.zeros(p.n_primal, dtype=torch.float64)
     with pytest.raises((NotImplementedError, RuntimeError)):
         torch.ops.v2rdm.Au(x, *SPEC)
+
+
+def test_clear_releases_cached_problems():
+    from hilbert_b200 import torch_ops
+    p = hb.V2RDMProblem(2, 1, 1, "DQG", True, True, hubbard_multiplicity=True)
+    torch_ops._problems[("test",)] = p
+    torch_ops.clear()
+    assert not torch_ops._problems and p._h is None
