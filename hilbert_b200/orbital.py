@@ -219,16 +219,19 @@ def _fock_q_z(h, B, Da, Ga, ncore, nact):
     return Fi, Fa, Qm, Z
 
 
-def diagonal_hessian(h, B, Da, Ga, ncore, nact):
+def diagonal_hessian(h, B, Da, Ga, ncore, nact, active_active=False):
     """focas's exact diagonal orbital Hessian (ORBOPT_EXACT_DIAGONAL_HESSIAN,
     on by default) for the rotation pairs of rotation_pairs(ncore, nact,
-    nvirt) (no active-active pairs), from src/focas/orbopt_hessian.cc:
+    nvirt, active_active), from src/focas/orbopt_hessian.cc:
       ed (a, i) :426-463   4 [F_aa - F_ii + 3 (ia|ia) - (ii|aa)],  F = Fi + Fa
       ea (a, t) :830-1047  2 [D_tt Fi_aa - Q_tt - Z_tt] + 2 sum_uv G_ttuv (uv|aa)
                            + 4 sum_uv G_utvt (ua|va)
       ad (t, i) :135-424   2 [2 (F_tt - F_ii) + D_tt Fi_ii - Q_tt - Z_tt]
                            + 2 sum_uv G_ttuv (uv|ii) + 4 [sum_u D_tu (tu|ii) - (tt|ii)]
                            + 4 sum_uv G_utvt (ui|vi) + 12 [(ti|ti) - sum_u D_tu (ui|ti)]
+      aa (t, u) :465-827   2 [D_tt Fi_uu + D_uu Fi_tt - Q_tt - Z_tt - Q_uu - Z_uu - 2 D_tu Fi_tu]
+           (t > u)         + sum_rs [(tt|rs) G_uurs + (uu|rs) G_ttrs - 2 (tu|rs) G_turs]
+                           + 2 sum_rs [(tr|ts) G_urus + (ur|us) G_trts - 2 (ur|ts) G_urts]
     G is the dense spin-summed active 2-RDM, the d2 focas works with after
     its Sort (orbopt_sort.cc:40-117 rescales the packed elements by 2 / m);
     the half-triangle sums of the reference become full sums by the pair
@@ -263,7 +266,21 @@ def diagonal_hessian(h, B, Da, Ga, ncore, nact):
     H_ad = (2.0 * (2.0 * (Fd[a][:, None] - Fd[c][None, :]) + Dtt[:, None] * Fid[c][None, :]
                    - (Qtt + Ztt)[:, None])
             + 2.0 * coul[:, c] + 4.0 * (tupp - ttpp) + 4.0 * exch[:, c] + 12.0 * (tptp - uptp))
-    return torch.cat([H_ed.reshape(-1), H_ea.reshape(-1), H_ad.reshape(-1)])
+    parts = [H_ed.reshape(-1), H_ea.reshape(-1), H_ad.reshape(-1)]
+    if active_active:
+        X = torch.einsum("tuvw,Qvw->Qtu", Ga, Ba)                 # sum_rs G_turs B^Q_rs
+        Bt, Xt = torch.diagonal(Ba, dim1=1, dim2=2), torch.diagonal(X, dim1=1, dim2=2)
+        tt_uu = torch.einsum("Qt,Qu->tu", Bt, Xt)                 # sum_rs (tt|rs) G_uurs
+        coul = tt_uu + tt_uu.T - 2.0 * (Ba * X).sum(0)
+        Y = torch.einsum("Qtr,urs,Qts->tu", Ba, torch.diagonal(Ga, dim1=0, dim2=2).permute(2, 0, 1), Ba)
+        W = torch.einsum("Qur,Qts,urts->tu", Ba, Ba, Ga)          # sum_rs (ur|ts) G_urts
+        Fia = Fi[a, a]
+        H_aa = (2.0 * (Dtt[:, None] * torch.diagonal(Fia)[None, :] + Dtt[None, :] * torch.diagonal(Fia)[:, None]
+                       - (Qtt + Ztt)[:, None] - (Qtt + Ztt)[None, :] - 2.0 * Da * Fia)
+                + coul + 2.0 * (Y + Y.T - 2.0 * W))
+        t_idx, u_idx = torch.tril_indices(nact, nact, offset=-1, device=h.device)
+        parts.append(H_aa[t_idx, u_idx])
+    return torch.cat(parts)
 
 
 def _pair_kappa(theta, pairs, n):
@@ -274,7 +291,8 @@ def _pair_kappa(theta, pairs, n):
     return K.index_put((q, p), -theta)
 
 
-def optimize_orbitals_focas(h, B, Da, Ga, ncore, nact, maxiter=10, g_conv=1e-4, e_conv=1e-8):
+def optimize_orbitals_focas(h, B, Da, Ga, ncore, nact, maxiter=10, g_conv=1e-4, e_conv=1e-8,
+                            active_active=False):
     """focas's orbital optimisation at fixed densities (src/focas/
     orbopt_optimize.cc:25-96; ORBOPT_MAXITER 10, ORBOPT_GRADIENT_CONVERGENCE
     1e-4, ORBOPT_ENERGY_CONVERGENCE 1e-8 by default, plugin.cc:153-168):
@@ -298,7 +316,7 @@ def optimize_orbitals_focas(h, B, Da, Ga, ncore, nact, maxiter=10, g_conv=1e-4, 
     per-iteration records (E_new, dE, |g|, r)."""
     nmo = h.shape[0]
     nvirt = nmo - ncore - nact
-    pairs = rotation_pairs(ncore, nact, nvirt)
+    pairs = rotation_pairs(ncore, nact, nvirt, active_active)
     D, G = full_densities(Da, Ga, ncore, nvirt)
     Gm = G.reshape(nmo * nmo, nmo * nmo)
     zero = torch.zeros((nmo, nmo), dtype=h.dtype, device=h.device)
@@ -326,7 +344,7 @@ def optimize_orbitals_focas(h, B, Da, Ga, ncore, nact, maxiter=10, g_conv=1e-4, 
             E0, g = orbital_gradient(h, B, D, G, pairs)
             E_init = float(E0)
             gnorm = float(torch.sqrt(g @ g))
-            Hd = diagonal_hessian(h, B, Da, Ga, ncore, nact)
+            Hd = diagonal_hessian(h, B, Da, Ga, ncore, nact, active_active)
             dE_quad = float(0.5 * (2.0 * (g @ k_cur) + (k_cur * Hd * k_cur).sum()))
             k_ref = -g / torch.clamp(Hd.abs(), min=1e-2)
             k_cur = r * k_ref
@@ -381,12 +399,10 @@ def casscf(h, B, ncore, nact, solve_active, macro_iterations=8, active_active=Fa
     packed d1) on the same device as h), optimise the orbitals at those
     densities, rotate h and B, repeat.  orbital_step: "lbfgs"
     (optimize_orbitals) or "focas" (optimize_orbitals_focas with focas's
-    defaults; no active-active pairs).  Returns the energies after each SDP
+    defaults).  Returns the energies after each SDP
     solve and the orbital-gradient norms at each orbital step."""
     if orbital_step not in ("lbfgs", "focas"):
         raise ValueError(f"orbital_step: {orbital_step!r}")
-    if orbital_step == "focas" and active_active:
-        raise ValueError("the focas step takes no active-active rotations")
     nmo = h.shape[0]
     nvirt = nmo - ncore - nact
     pairs = rotation_pairs(ncore, nact, nvirt, active_active)
@@ -397,7 +413,7 @@ def casscf(h, B, ncore, nact, solve_active, macro_iterations=8, active_active=Fa
         energies.append(e_core + e_act)
         Da, Ga = unpack_densities(d2p, d1p, nact)
         if orbital_step == "focas":
-            U, _, hist = optimize_orbitals_focas(h, B, Da, Ga, ncore, nact)
+            U, _, hist = optimize_orbitals_focas(h, B, Da, Ga, ncore, nact, active_active=active_active)
             gnorms.append(hist[0][2])
         else:
             D, G = full_densities(Da, Ga, ncore, nvirt)

@@ -163,7 +163,7 @@ def _focas_intermediates(h, B, D_act, G_act, ncore, nact):
     return eri, Fi, Fa, Qm, Zm
 
 
-def focas_diagonal_hessian(h, B, d2p, d1p, ncore, nact):
+def focas_diagonal_hessian(h, B, d2p, d1p, ncore, nact, active_active=False):
     """focas's exact diagonal orbital Hessian (ORBOPT_EXACT_DIAGONAL_HESSIAN,
     on by default, plugin.cc:162), restated on dense integrals from
     orbopt_hessian.cc.  d2p, d1p: PackSpatialDensity's output; focas's Sort
@@ -181,8 +181,12 @@ def focas_diagonal_hessian(h, B, d2p, d1p, ncore, nact):
                  2 [D_tt Fi_aa - Q_tt - Z_tt]
                  + 4 sum_u [sum_{v<u} d2(tt|uv) (uv|aa) + 1/2 d2(tt|uu) (uu|aa)]
                  + 8 sum_u [sum_{v<u} (ua|va) d2(ut|vt) + 1/2 (ua|ua) d2(ut|ut)]
-    Returns {(p, q): H} for the pairs of different classes, keyed like
-    focas_gradient."""
+      aa (t, u), t > u, with active_active (ComputeH_diag_aa, :465-827)
+                 2 [D_tt Fi_uu + D_uu Fi_tt - Q_tt - Z_tt - Q_uu - Z_uu - 2 D_tu Fi_tu]
+                 + sum_rs [(tt|rs) d2(uu|rs) + (uu|rs) d2(tt|rs) - 2 (tu|rs) d2(tu|rs)]
+                 + 2 sum_rs [(tr|ts) d2(ur|us) + (ur|us) d2(tr|ts) - 2 (ur|ts) d2(ur|ts)]
+    Returns {(p, q): H} for the pairs of different classes (and the
+    active-active pairs when asked), keyed like focas_gradient."""
     nmo = h.shape[0]
     core = list(range(ncore))
     act = list(range(ncore, ncore + nact))
@@ -229,6 +233,23 @@ def focas_diagonal_hessian(h, B, d2p, d1p, ncore, nact):
                     x += 4.0 * P(t, u, t, w) * eri[act[u], i, act[w], i]
             e = eri[T, i, T, i] - sum(D_act[t, u] * eri[act[u], i, T, i] for u in range(nact))
             H[(T, i)] = v + c + 4.0 * d + x + 12.0 * e
+    if active_active:
+        A = act
+        for t in range(nact):
+            for u in range(t):
+                T, Uo = A[t], A[u]
+                v = 2.0 * (-(Qm[t, T] + Zm[t, T] + Qm[u, Uo] + Zm[u, Uo] + 2.0 * D_act[t, u] * Fi[T, Uo])
+                           + D_act[t, t] * Fi[Uo, Uo] + D_act[u, u] * Fi[T, T])
+                c = 0.0
+                x = 0.0
+                for r in range(nact):
+                    for q in range(nact):
+                        R, S = A[r], A[q]
+                        c += (eri[T, T, R, S] * P(u, u, r, q) + eri[Uo, Uo, R, S] * P(t, t, r, q)
+                              - 2.0 * eri[T, Uo, R, S] * P(t, u, r, q))
+                        x += (eri[T, R, T, S] * P(u, r, u, q) + eri[Uo, R, Uo, S] * P(t, r, t, q)
+                              - 2.0 * eri[Uo, R, T, S] * P(u, r, t, q))
+                H[(T, Uo)] = v + c + 2.0 * x
     return H
 
 
@@ -261,17 +282,21 @@ def focas_gradient(h, B, D_act, G_act, ncore, nact, active_active=False):
     return g
 
 
-def rotation_pairs(ncore, nact, nvirt):
-    """focas's rotation order without active-active pairs (Grad_IndMap,
-    orbopt_gradient.cc:147-183): virtual-core, virtual-active, active-core."""
+def rotation_pairs(ncore, nact, nvirt, active_active=False):
+    """focas's rotation order (Grad_IndMap, orbopt_gradient.cc:147-183):
+    virtual-core, virtual-active, active-core, then active-active (t > u)."""
     core = range(ncore)
     act = range(ncore, ncore + nact)
     virt = range(ncore + nact, ncore + nact + nvirt)
-    return ([(p, q) for p in virt for q in core] + [(p, q) for p in virt for q in act]
-            + [(p, q) for p in act for q in core])
+    pairs = ([(p, q) for p in virt for q in core] + [(p, q) for p in virt for q in act]
+             + [(p, q) for p in act for q in core])
+    if active_active:
+        pairs += [(p, q) for p in act for q in act if q < p]
+    return pairs
 
 
-def focas_optimize(h, B, d2p, d1p, ncore, nact, maxiter=10, g_conv=1e-4, e_conv=1e-8):
+def focas_optimize(h, B, d2p, d1p, ncore, nact, maxiter=10, g_conv=1e-4, e_conv=1e-8,
+                   active_active=False):
     """focas's optimize_orbitals (src/focas/orbopt_optimize.cc:25-96) with
     Update_kappa (:98-115), Update_r (:117-146), Compute_Quadratic_dE
     (:162-176), Restore_last_step (:226-245) and Precondition_Step
@@ -283,7 +308,7 @@ def focas_optimize(h, B, d2p, d1p, ncore, nact, maxiter=10, g_conv=1e-4, e_conv=
     from scipy.linalg import expm
     nmo = h.shape[0]
     nvirt = nmo - ncore - nact
-    pairs = rotation_pairs(ncore, nact, nvirt)
+    pairs = rotation_pairs(ncore, nact, nvirt, active_active)
     D_act, G_act = unpack_active(d2p, d1p, nact)
     D, G = full_densities(D_act, G_act, ncore)
     if nvirt:
@@ -315,10 +340,10 @@ def focas_optimize(h, B, d2p, d1p, ncore, nact, maxiter=10, g_conv=1e-4, e_conv=
     for it in range(maxiter):
         if eval_g:
             E_init = E()
-            gd = focas_gradient(h, B, D_act, G_act, ncore, nact)
+            gd = focas_gradient(h, B, D_act, G_act, ncore, nact, active_active)
             g = np.array([gd[pq] for pq in pairs])
             gnorm = float(np.sqrt(g @ g))
-            Hd_ = focas_diagonal_hessian(h, B, d2p, d1p, ncore, nact)
+            Hd_ = focas_diagonal_hessian(h, B, d2p, d1p, ncore, nact, active_active)
             Hd = np.array([Hd_[pq] for pq in pairs])
             dE_quad = 0.5 * (2.0 * (g @ k_cur) + float(np.sum(k_cur * Hd * k_cur)))
             Hc = np.abs(Hd)

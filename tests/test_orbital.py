@@ -171,3 +171,27 @@ def test_focas_step_converges_near_a_minimum(small_casscf):
     U, E, hist = _check_focas_trajectory(h1, B1, s, maxiter=30, g_conv=1e-6, e_conv=1e-12)
     assert E < E1.item()
     assert hist[-1][2] < 0.5 * float(g1.norm())
+
+
+def test_active_active_hessian_block_and_step_follow_the_oracle(small_casscf):
+    """ComputeH_diag_aa (orbopt_hessian.cc:465-827), used with
+    ORBOPT_ACTIVE_ACTIVE_ROTATIONS: the contraction form equals the literal
+    restatement, and the focas loop with active-active pairs follows the
+    oracle's.  (This block is focas's approximation, not the exact second
+    derivative, so it is pinned to the restatement alone.)"""
+    s = small_casscf
+    nc, na_, nv = s["nc"], s["na"], s["nv"]
+    Da, Ga = ho.unpack_densities(torch.from_numpy(s["d2p"]), torch.from_numpy(s["d1p"]), na_)
+    h, B = torch.from_numpy(s["h"]), torch.from_numpy(s["B"])
+    pairs = ho.rotation_pairs(nc, na_, nv, active_active=True)
+    H = ho.diagonal_hessian(h, B, Da, Ga, nc, na_, active_active=True).numpy()
+    Hf = oo.focas_diagonal_hessian(s["h"], s["B"], s["d2p"], s["d1p"], nc, na_, active_active=True)
+    Hf = np.array([Hf[pq] for pq in pairs])
+    assert len(H) == len(pairs)
+    assert np.max(np.abs(H - Hf)) <= 1e-12 * np.max(np.abs(Hf))
+    U, E, hist = ho.optimize_orbitals_focas(h, B, Da, Ga, nc, na_, maxiter=10, active_active=True)
+    _, _, Uo, histo = oo.focas_optimize(s["h"], s["B"], s["d2p"], s["d1p"], nc, na_, maxiter=10,
+                                        active_active=True)
+    assert len(hist) == len(histo)
+    assert all(abs(a[0] - b[0]) <= 1e-9 and a[3] == b[3] for a, b in zip(hist, histo))
+    assert np.max(np.abs(U.numpy() - Uo)) <= 1e-9
