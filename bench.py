@@ -56,12 +56,12 @@ WORKLOADS = {
 #  df20: the FP64 device solve (one outer iteration of the CPU path takes
 #    seconds here, so a CPU solve to convergence takes hours; the device path
 #    reproduces the CPU oracle's iteration counts on the Hubbard rings).
-FP64_ITERS = {"hubbard8": (13801, 503997), "df20": (4102, 179742)}
+FP64_ITERS = {"hubbard8": (13801, 503997), "df20": (4080, 183147)}
 # FP64 energies the device result is compared with:
 #  hubbard8: the CPU oracle; df20: the FP64 device solve that diagonalises
 #  every block by selective Jacobi each iteration (no warm refinement).
 FP64_ENERGY = {"hubbard8": (-4.9364448537582035, "cpu oracle"),
-               "df20": (-103.6150114058378, "fp64 device solve, Jacobi every iteration")}
+               "df20": (-103.6150114064154, "fp64 device solve, Jacobi every iteration")}
 
 
 def hamiltonian(w):
