@@ -46,6 +46,10 @@ def test_sizes_match_reference_counts():
     o = OracleProblem(20, 10, 10, "DQG", True, True, h=np.zeros((20, 20)), g=np.zeros((20,) * 4))
     assert (o.n_primal, o.n_dual) == (1586000, 1856304)
     assert sorted(set(o.dims)) == [20, 190, 400, 800]
+    # the half-filled Hubbard rings of the 64-instance batch, L = 6 .. 14
+    for L, sizes, big in ((6, (12708, 14863), 72), (14, (379652, 443895), 392)):
+        o = OracleProblem(L, L // 2, L // 2, "DQG", True, True, hubbard=(1.0, 4.0))
+        assert (o.n_primal, o.n_dual) == sizes and max(o.dims) == big
     # config 5: the 4x4 Hubbard lattice with T2 (80 M primal variables)
     o = OracleProblem(16, 8, 8, "DQGT2", True, True, hubbard=(1.0, 4.0))
     assert (o.n_primal, o.n_dual) == (80405760, 80515780)
