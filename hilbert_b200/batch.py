@@ -1,0 +1,130 @@
+"""Batches of independent v2RDM instances, sharded across GPUs.
+
+The instances of a batch share no data, so a batch runs as replicas: each
+rank solves a disjoint slice on its own device, and the host gathers the
+per-instance scalars (energy, convergence, iteration counts).  No device
+collective takes part.
+
+hubbard_batch() draws the 64-ring workload: L ~ U{6..14} sites, N in
+{L-2, L, L+2} electrons, U/t ~ U[1, 8], periodic, seed 3.  Even N runs
+through hilbert's Hubbard path (nalpha = nbeta = N/2,
+v2rdm_solver.cc:841-863).  Odd N runs through the external-Hamiltonian
+constructor with the ring's integrals and nalpha = ceil(N/2), nbeta =
+floor(N/2) (v2rdm_solver.cc:147-195), because the Hubbard path requires
+even N.
+"""
+from dataclasses import dataclass
+
+import numpy as np
+
+from .v2rdm import Options, V2RDMProblem, block_layout
+
+
+@dataclass(frozen=True)
+class RingInstance:
+    index: int
+    sites: int        # L, one orbital per site
+    electrons: int    # N
+    U: float          # on-site repulsion, in units of t = 1
+    positivity: str = "DQG"
+
+    @property
+    def nalpha(self):
+        return (self.electrons + 1) // 2
+
+    @property
+    def nbeta(self):
+        return self.electrons // 2
+
+    @property
+    def hubbard_path(self):
+        return self.electrons % 2 == 0
+
+    def cost(self):
+        """Relative work of a solve: the projection's sum (16/3) n_b^3."""
+        dims = [d for _, d in block_layout(self.sites, self.nalpha, self.nbeta, self.positivity, True)]
+        return float(sum((16.0 / 3.0) * float(d) ** 3 for d in dims))
+
+    def integrals(self):
+        """(h, g) of the periodic ring: h_{i,i+-1} = -1 (once for L = 2,
+        oei.cc:76-95), (ii|ii) = U (tei.cc:285-292); g in (pq|rs) order."""
+        L = self.sites
+        h = np.zeros((L, L))
+        for i in range(L):
+            j = (i + 1) % L
+            if j != i:
+                h[i, j] = h[j, i] = -1.0
+        g = np.zeros((L, L, L, L))
+        for i in range(L):
+            g[i, i, i, i] = self.U
+        return h, g
+
+    def problem(self):
+        """The device problem and its b and c (host arrays)."""
+        p = V2RDMProblem(self.sites, self.nalpha, self.nbeta, self.positivity, True, True,
+                         hubbard_multiplicity=self.hubbard_path)
+        c = p.c_hubbard(1.0, self.U) if self.hubbard_path else p.c_external(*self.integrals())
+        return p, p.b(), c
+
+
+def hubbard_batch(count=64, seed=3, positivity="DQG"):
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        L = int(rng.integers(6, 15))
+        N = L + int(rng.choice([-2, 0, 2]))
+        U = float(rng.uniform(1.0, 8.0))
+        out.append(RingInstance(k, L, N, U, positivity))
+    return out
+
+
+def shard(instances, world):
+    """Instance indices per rank: longest first, each to the least-loaded
+    rank (ties to the lower rank); every instance exactly once."""
+    loads = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for inst in sorted(instances, key=lambda i: (-i.cost(), i.index)):
+        r = min(range(world), key=lambda k: (loads[k], k))
+        parts[r].append(inst.index)
+        loads[r] += inst.cost()
+    return [sorted(p) for p in parts]
+
+
+def solve_on_device(inst, options, device=None):
+    """One instance through the device path from the RANDOM guess."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    p, b, c = inst.problem()
+    try:
+        x = torch.from_numpy(p.guess("RANDOM")).to(dev)
+        st = p.solve_device(x, torch.from_numpy(b).to(dev), torch.from_numpy(c).to(dev), options)
+        energy = float(np.dot(c, x.cpu().numpy()))
+    finally:
+        p.close()
+    return {"energy": energy, "converged": bool(st["converged"]), "oiter": int(st["oiter"]),
+            "iiter": int(st["iiter"])}
+
+
+def solve_batch(instances, options=None, rank=0, world=1, group=None, solve=solve_on_device):
+    """Solve this rank's slice, then gather every rank's results on the host
+    (torch.distributed.all_gather_object over `group`, which should be a
+    gloo group when the default one is NCCL).  Returns the results of all
+    instances, ordered by index, each {"index", "rank", ...solve's dict}."""
+    if options is None:
+        options = Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6, "MAXITER": 400000,
+                           "MU_UPDATE_FREQUENCY": 500})
+    by_index = {i.index: i for i in instances}
+    if len(by_index) != len(instances):
+        raise ValueError("instance indices must be unique")
+    mine = shard(instances, world)[rank]
+    results = []
+    for k in mine:
+        r = dict(solve(by_index[k], options))
+        r.update(index=k, rank=rank)
+        results.append(r)
+    if world > 1:
+        import torch.distributed as dist
+        gathered = [None] * world
+        dist.all_gather_object(gathered, results, group=group)
+        results = [r for part in gathered for r in part]
+    return sorted(results, key=lambda r: r["index"])
