@@ -18,7 +18,7 @@ Problem make_problem(const ProblemSpec &spec) {
     if (spec.nmo < 1 || spec.nalpha < 0 || spec.nbeta < 0 || spec.nalpha > spec.nmo ||
         spec.nbeta > spec.nmo)
         throw std::invalid_argument("invalid orbital / electron counts");
-    if (spec.positivity < POS_D || spec.positivity > POS_DQGT2)
+    if (spec.positivity < POS_D || spec.positivity > POS_DQGT1T2)
         throw std::invalid_argument("unsupported POSITIVITY");
     Problem p;
     p.spec = spec;
@@ -26,9 +26,11 @@ Problem make_problem(const ProblemSpec &spec) {
     p.n = n;
     p.gab = n * n;
     p.gaa = n * (n - 1) / 2;
-    p.q2 = spec.positivity == POS_DQ || spec.positivity == POS_DQG || spec.positivity == POS_DQGT2;
-    p.g2 = spec.positivity == POS_DG || spec.positivity == POS_DQG || spec.positivity == POS_DQGT2;
-    p.t2 = spec.positivity == POS_DQGT2;   // v2rdm_solver.cc:4106-4109
+    // v2rdm_solver.cc:4081-4118: every T option keeps Q2 and G2
+    p.q2 = spec.positivity == POS_DQ || spec.positivity >= POS_DQG;
+    p.g2 = spec.positivity == POS_DG || spec.positivity >= POS_DQG;
+    p.t1 = spec.positivity == POS_DQGT1 || spec.positivity == POS_DQGT1T2;
+    p.t2 = spec.positivity == POS_DQGT2 || spec.positivity == POS_DQGT1T2;
     p.mult = spec.hubbard_multiplicity ? 2 * (spec.nalpha - spec.nbeta) + 1
                                        : (spec.nalpha - spec.nbeta) + 1;
 
@@ -82,7 +84,7 @@ Problem make_problem(const ProblemSpec &spec) {
         add_block(p.g2ba, p.gab);
         add_block(p.g2aa, 2 * p.gab);
     }
-    if (p.t2) {   // v2rdm_solver.cc:3879-3906
+    if (p.t1 || p.t2) {   // basis.cc:640-745: lexicographic triplets
         p.trip_aba = n * n * n;
         for (int i = 0; i < n; i++)
             for (int j = i + 1; j < n; j++)
@@ -90,8 +92,22 @@ Problem make_problem(const ProblemSpec &spec) {
                     p.bas_aab.push_back(i);
                     p.bas_aab.push_back(j);
                     p.bas_aab.push_back(k);
+                    if (k > j) {
+                        p.bas_aaa.push_back(i);
+                        p.bas_aaa.push_back(j);
+                        p.bas_aaa.push_back(k);
+                    }
                 }
         p.trip_aab = (int)(p.bas_aab.size() / 3);
+        p.trip_aaa = (int)(p.bas_aaa.size() / 3);
+    }
+    if (p.t1) {   // v2rdm_solver.cc:3848-3877
+        add_block(p.t1aaa, p.trip_aaa);
+        add_block(p.t1bbb, p.trip_aaa);
+        add_block(p.t1aab, p.trip_aab);
+        add_block(p.t1bba, p.trip_aab);
+    }
+    if (p.t2) {   // v2rdm_solver.cc:3879-3906
         add_block(p.t2aaa, p.trip_aab + p.trip_aba);
         add_block(p.t2bbb, p.trip_aab + p.trip_aba);
         add_block(p.t2aab, p.trip_aab);
@@ -108,6 +124,7 @@ Problem make_problem(const ProblemSpec &spec) {
     }
     if (p.q2) d += gab2 + 2 * gaa2;
     if (p.g2) d += 6 * gab2;
+    if (p.t1) d += 2 * (int64_t)p.trip_aaa * p.trip_aaa + 2 * (int64_t)p.trip_aab * p.trip_aab;
     if (p.t2) {
         const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
         d += 2 * aab * aab + 2 * big * big;
@@ -230,6 +247,78 @@ void build_c_external(const Problem &p, const double *h, const double *g, double
 // abb/abb), 6-9 bbb (bbb/bbb, bbb/baa, baa/bbb, baa/baa).
 namespace {
 constexpr int kT2AaaAbb = 3;
+
+// ------------------------------------------------------------------ T1
+// The T1 rows (t1.cc:419-795, T1_constraints_Au, C1): one row per element
+// of T1aab, T1bba (aab triplets) and T1aaa, T1bbb (aaa triplets, i < j < k),
+// in that order of dual rows, each -T1(I, J) + delta-masked Q2, D2, G2 and
+// D1 terms with coefficients +-1.  f(dual_row, t1_col, sub, cols, coefs,
+// nterms) receives them in the reference's order; T1_constraints_ATu
+// (t1.cc:795-1200) scatters the same terms in the same order, and the guess
+// (t1.cc:45-419) sums them from zero.
+template <class F>
+void t1_rows(const Problem &p, int64_t off, F &&f) {
+    const int N = p.n, gab = p.gab, gaa = p.gaa;
+    int64_t cols[12];
+    double coef[12];
+    int nt = 0;
+    auto add = [&](int64_t c, double v) {
+        cols[nt] = c;
+        coef[nt] = v;
+        nt++;
+    };
+    auto aa = [&](int64_t base, int a, int b, int c, int d) { return base + (int64_t)p.iaa(a, b) * gaa + p.iaa(c, d); };
+    auto ab = [&](int64_t base, int a, int b, int c, int d) { return base + (int64_t)p.iab(a, b) * gab + p.iab(c, d); };
+    for (int sub = 0; sub < 4; sub++) {
+        const bool aab = sub < 2, beta = (sub % 2) == 1;
+        const std::vector<int> &tb = aab ? p.bas_aab : p.bas_aaa;
+        const int nr = aab ? p.trip_aab : p.trip_aaa;
+        const int64_t t1 = sub == 0 ? p.t1aab : sub == 1 ? p.t1bba : sub == 2 ? p.t1aaa : p.t1bbb;
+        const int64_t q2 = beta ? p.q2bb : p.q2aa;
+        for (int r = 0; r < nr; r++) {
+            const int i = tb[3 * r], j = tb[3 * r + 1], k = tb[3 * r + 2];
+            for (int c = 0; c < nr; c++) {
+                const int l = tb[3 * c], m = tb[3 * c + 1], n = tb[3 * c + 2];
+                nt = 0;
+                if (aab) {   // t1.cc:421-515
+                    const int64_t g2 = beta ? p.g2ab : p.g2ba;
+                    if (k == n) add(aa(q2, i, j, l, m), 1.0);
+                    if (j == l) add(beta ? ab(p.d2ab, n, m, k, i) : ab(p.d2ab, m, n, i, k), -1.0);
+                    if (l == i) add(beta ? ab(p.d2ab, n, m, k, j) : ab(p.d2ab, m, n, j, k), 1.0);
+                    if (j == m) add(ab(g2, n, i, k, l), -1.0);
+                    if (i == m) add(ab(g2, n, j, k, l), 1.0);
+                } else {     // t1.cc:517-793
+                    const int64_t d2 = beta ? p.d2bb : p.d2aa, d1 = beta ? p.d1b : p.d1a;
+                    const int64_t sh = beta ? gab : 0, w = 2 * (int64_t)gab;
+                    auto g2 = [&](int a, int b, int cc, int d) {
+                        return p.g2aa + (p.iab(a, b) + sh) * w + (p.iab(cc, d) + sh);
+                    };
+                    if (k == n) add(aa(q2, i, j, l, m), 1.0);
+                    if (j == n) add(aa(q2, i, k, l, m), -1.0);
+                    if (i == n) add(aa(q2, j, k, l, m), 1.0);
+                    if (l == k) add(aa(d2, n, m, j, i), 1.0);
+                    if (j == l) add(aa(d2, n, m, k, i), -1.0);
+                    if (l == i) add(aa(d2, n, m, k, j), 1.0);
+                    if (k == m) {
+                        if (j == l) add(d1 + (int64_t)n * N + i, -1.0);
+                        add(g2(n, i, j, l), 1.0);
+                    }
+                    if (j == m) {
+                        if (k == l) add(d1 + (int64_t)n * N + i, 1.0);
+                        add(g2(n, i, k, l), -1.0);
+                    }
+                    if (i == m) {
+                        if (k == l) add(d1 + (int64_t)n * N + j, -1.0);
+                        add(g2(n, j, k, l), 1.0);
+                    }
+                }
+                const int64_t e = (int64_t)r * nr + c;
+                f(off + e, t1 + e, sub, cols, coef, nt);
+            }
+        }
+        off += (int64_t)nr * nr;
+    }
+}
 
 template <class F>
 void t2_rows(const Problem &p, int64_t off, F &&f) {
@@ -453,6 +542,13 @@ void guess_hf(const Problem &p, double *x) {
                 x[p.g2aa + (gab + ij) * w + kl] = 0.0 + x[p.d2ab + (int64_t)p.iab(l, i) * gab + p.iab(k, j)];
             }
         }
+    }
+    if (p.t1) {   // t1.cc:45-419: each element from its row's terms
+        t1_rows(p, 0, [&](int64_t, int64_t t1c, int, const int64_t *cols, const double *coef, int nt) {
+            double dum = 0.0;
+            for (int q = 0; q < nt; q++) dum += coef[q] * x[cols[q]];
+            x[t1c] = dum;
+        });
     }
     if (p.t2) {   // t2.cc:1845-2452: each element from its row's D terms (the aaa/abb part zero)
         t2_rows(p, 0, [&](int64_t, int64_t t2c, int sub, const int64_t *cols, const double *coef, int nt) {
@@ -762,6 +858,13 @@ void visit_A(const Problem &p, S &s) {
         }
         off += 4 * (int64_t)gab * gab;
     }
+    if (p.t1) {   // t1.cc:419-795
+        t1_rows(p, off, [&](int64_t row, int64_t t1c, int, const int64_t *cols, const double *coef, int nt) {
+            s.t(row, t1c, -1.0);
+            for (int q = 0; q < nt; q++) s.t(row, cols[q], coef[q]);
+        });
+        off += 2 * (int64_t)p.trip_aab * p.trip_aab + 2 * (int64_t)p.trip_aaa * p.trip_aaa;
+    }
     if (p.t2) {   // t2.cc:1236-1843
         t2_rows(p, off, [&](int64_t row, int64_t t2c, int, const int64_t *cols, const double *coef, int nt) {
             s.t(row, t2c, -1.0);
@@ -1056,6 +1159,13 @@ void visit_AT(const Problem &p, S &s) {
             }
         }
         off += 4 * (int64_t)gab * gab;
+    }
+    if (p.t1) {   // t1.cc:795-1200 scatters in the same loop order as the A rows
+        t1_rows(p, off, [&](int64_t row, int64_t t1c, int, const int64_t *cols, const double *coef, int nt) {
+            s.t(t1c, row, -1.0);
+            for (int q = 0; q < nt; q++) s.t(cols[q], row, coef[q]);
+        });
+        off += 2 * (int64_t)p.trip_aab * p.trip_aab + 2 * (int64_t)p.trip_aaa * p.trip_aaa;
     }
     if (p.t2) {   // t2.cc:3376-3966 scatters in the same loop order as the A rows
         t2_rows(p, off, [&](int64_t row, int64_t t2c, int, const int64_t *cols, const double *coef, int nt) {

@@ -15,7 +15,8 @@
 
 namespace v2b {
 
-enum Positivity { POS_D = 0, POS_DQ = 1, POS_DG = 2, POS_DQG = 3, POS_DQGT2 = 4 };
+enum Positivity { POS_D = 0, POS_DQ = 1, POS_DG = 2, POS_DQG = 3, POS_DQGT2 = 4, POS_DQGT1 = 5,
+                  POS_DQGT1T2 = 6 };
 
 struct ProblemSpec {
     int nmo = 0;          // active orbitals (C1, no frozen/restricted orbitals)
@@ -44,12 +45,14 @@ constexpr uint32_t kGroupFlag = 1u << 31;
 struct Problem {
     ProblemSpec spec;
     int n = 0, gab = 0, gaa = 0, mult = 1;
-    bool q2 = false, g2 = false, t2 = false;
+    bool q2 = false, g2 = false, t1 = false, t2 = false;
     std::vector<int> bas_ab, ibas_ab, bas_aa, ibas_aa;
     // triplets (basis.cc:640-727, C1): aba = every (i, j, k), numbered
     // i n^2 + j n + k; aab = those with i < j, in the same order
-    int trip_aab = 0, trip_aba = 0;
+    int trip_aaa = 0, trip_aab = 0, trip_aba = 0;
+    std::vector<int> bas_aaa;        // 3 per aaa triplet (i < j < k)
     std::vector<int> bas_aab;        // 3 per aab triplet
+    int64_t t1aaa = -1, t1bbb = -1, t1aab = -1, t1bba = -1;
     int64_t t2aaa = -1, t2bbb = -1, t2aab = -1, t2bba = -1;
     int64_t d2ab = -1, d2aa = -1, d2bb = -1, d200 = -1, d1a = -1, d1b = -1, q1a = -1, q1b = -1;
     int64_t q2ab = -1, q2aa = -1, q2bb = -1, g2ab = -1, g2ba = -1, g2aa = -1;

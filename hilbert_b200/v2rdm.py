@@ -453,12 +453,15 @@ def block_layout(nmo, nalpha, nbeta, positivity="DQG", constrain_spin=True):
     if constrain_spin:
         blocks.append(("d200", gab if nalpha == nbeta else 2 * gab))
     blocks += [("d1a", n), ("d1b", n), ("q1a", n), ("q1b", n)]
-    if pos in ("DQ", "DQG", "DQGT2"):
+    t_opts = ("DQGT1", "DQGT2", "DQGT1T2", "DQGT")
+    if pos in ("DQ", "DQG") + t_opts:
         blocks += [("q2ab", gab), ("q2aa", gaa), ("q2bb", gaa)]
-    if pos in ("DG", "DQG", "DQGT2"):
+    if pos in ("DG", "DQG") + t_opts:
         blocks += [("g2ab", gab), ("g2ba", gab), ("g2aa", 2 * gab)]
-    if pos == "DQGT2":
-        aab, aba = n * (n - 1) // 2 * n, n ** 3
+    aaa, aab, aba = n * (n - 1) * (n - 2) // 6, n * (n - 1) // 2 * n, n ** 3
+    if pos in ("DQGT1", "DQGT1T2", "DQGT"):
+        blocks += [("t1aaa", aaa), ("t1bbb", aaa), ("t1aab", aab), ("t1bba", aab)]
+    if pos in ("DQGT2", "DQGT1T2", "DQGT"):
         blocks += [("t2aaa", aab + aba), ("t2bbb", aab + aba), ("t2aab", aab), ("t2bba", aab)]
     return blocks
 

@@ -41,6 +41,8 @@ extern "C" {
 #define V2B_POSITIVITY_DG  2
 #define V2B_POSITIVITY_DQG 3
 #define V2B_POSITIVITY_DQGT2 4   /* DQG + T2 (t2.cc:1236-1843, 3376-3966) */
+#define V2B_POSITIVITY_DQGT1 5   /* DQG + T1 (t1.cc:419-795, 795-1200) */
+#define V2B_POSITIVITY_DQGT1T2 6 /* DQG + T1 + T2 ("DQGT1T2" and "DQGT", v2rdm_solver.cc:4110-4119) */
 
 /* libsdp::SDPOptions as hilbert fills it (src/v2rdm_casscf/v2rdm_solver.cc:426-431) */
 typedef struct {

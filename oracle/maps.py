@@ -14,9 +14,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libv2rdm_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libv2rdm_ref.so")
 
-POSITIVITY = {"D": 0, "DQ": 1, "DG": 2, "DQG": 3, "DQGT2": 4}
+POSITIVITY = {"D": 0, "DQ": 1, "DG": 2, "DQG": 3, "DQGT2": 4, "DQGT1": 5, "DQGT1T2": 6}
 BLOCK_NAMES = ("d2ab", "d2aa", "d2bb", "d200", "d1a", "d1b", "q1a", "q1b",
-               "q2ab", "q2aa", "q2bb", "g2ab", "g2ba", "g2aa", "t2aaa", "t2bbb", "t2aab", "t2bba")
+               "q2ab", "q2aa", "q2bb", "g2ab", "g2ba", "g2aa", "t2aaa", "t2bbb", "t2aab", "t2bba",
+               "t1aaa", "t1bbb", "t1aab", "t1bba")
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")

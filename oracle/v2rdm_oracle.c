@@ -8,7 +8,8 @@
  * the reference bit for bit.  Each function cites the reference code it
  * restates (paths relative to the hilbert source tree).
  *
- * Supported constraint sets: POSITIVITY D / DQ / DG / DQG / DQGT2 with
+ * Supported constraint sets: POSITIVITY D / DQ / DG / DQG / DQGT1 / DQGT2 /
+ * DQGT1T2 with
  * CONSTRAIN_SPIN and CONSTRAIN_SZ on or off, singlet and non-singlet.
  */
 #include <math.h>
@@ -18,14 +19,14 @@
 typedef struct {
     int n;            /* active orbitals (amo_) */
     int na, nb;       /* alpha / beta electrons */
-    int q2, g2, t2, spin, sz;
+    int q2, g2, t1, t2, spin, sz;
     int mult;         /* 2S+1 as the reference stores it */
     int gab, gaa;
     int *bas_ab, *ibas_ab, *bas_aa, *ibas_aa;
     long d2ab, d2aa, d2bb, d200, d1a, d1b, q1a, q1b, q2ab, q2aa, q2bb, g2ab, g2ba, g2aa;
-    long t2aaa, t2bbb, t2aab, t2bba;
-    int trip_aab, trip_aba;   /* triplets (i<j, k) and (i, j, k) */
-    int *bas_aab, *bas_aba;   /* 3 ints per triplet */
+    long t1aaa, t1bbb, t1aab, t1bba, t2aaa, t2bbb, t2aab, t2bba;
+    int trip_aaa, trip_aab, trip_aba;   /* triplets (i<j<k), (i<j, k) and (i, j, k) */
+    int *bas_aaa, *bas_aab, *bas_aba;   /* 3 ints per triplet */
     long n_primal, n_dual;
     int nblocks;
     int dims[32];
@@ -65,6 +66,8 @@ static void build_tables(v2o_problem *p) {
 #define IAA(p, i, j) ((p)->ibas_aa[(i) * (p)->n + (j)])
 
 enum { T2_AU = 0, T2_ATU = 1, T2_GUESS = 2 };
+static void t1_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
+                     double *x);
 static void t2_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
                      double *x);
 
@@ -97,6 +100,15 @@ static void set_offsets(v2o_problem *p) {
         p->g2ba = off; off += (long)gab * gab; p->dims[nb++] = gab;
         p->g2aa = off; off += 4L * gab * gab; p->dims[nb++] = 2 * gab;
     }
+    /* v2rdm_solver.cc:3848-3877: T1aaa, T1bbb (dim aaa), T1aab, T1bba (dim aab) */
+    p->t1aaa = p->t1bbb = p->t1aab = p->t1bba = -1;
+    if (p->t1) {
+        long t3 = p->trip_aaa, ta = p->trip_aab;
+        p->t1aaa = off; off += t3 * t3; p->dims[nb++] = (int)t3;
+        p->t1bbb = off; off += t3 * t3; p->dims[nb++] = (int)t3;
+        p->t1aab = off; off += ta * ta; p->dims[nb++] = (int)ta;
+        p->t1bba = off; off += ta * ta; p->dims[nb++] = (int)ta;
+    }
     /* v2rdm_solver.cc:3879-3906: T2aaa, T2bbb (dim aab + aba), T2aab, T2bba (dim aab) */
     p->t2aaa = p->t2bbb = p->t2aab = p->t2bba = -1;
     if (p->t2) {
@@ -122,6 +134,10 @@ static void set_offsets(v2o_problem *p) {
     }
     if (p->q2) d += (long)gab * gab + 2L * gaa * gaa;
     if (p->g2) d += 6L * gab * gab;
+    if (p->t1) {   /* v2rdm_solver.cc:3554-3567 */
+        long t3 = p->trip_aaa, ta = p->trip_aab;
+        d += 2 * t3 * t3 + 2 * ta * ta;
+    }
     if (p->t2) {   /* v2rdm_solver.cc:3568-3580 */
         long w = (long)p->trip_aab + p->trip_aba, ta = p->trip_aab;
         d += 2 * w * w + 2 * ta * ta;
@@ -130,13 +146,15 @@ static void set_offsets(v2o_problem *p) {
 }
 
 /* basis.cc:640-745 (C1): every (i, j, k) in i, j, k order is an aba triplet;
- * those with i < j are also aab triplets, numbered in the same sweep. */
+ * those with i < j are also aab triplets, and those with i < j < k aaa
+ * triplets, each numbered in the same sweep. */
 static void build_triplets(v2o_problem *p) {
     int n = p->n;
     long n3 = (long)n * n * n;
     p->bas_aba = (int *)malloc(sizeof(int) * 3 * (n3 > 0 ? n3 : 1));
     p->bas_aab = (int *)malloc(sizeof(int) * 3 * (n3 > 0 ? n3 : 1));
-    int ca = 0, cb = 0;
+    p->bas_aaa = (int *)malloc(sizeof(int) * 3 * (n3 > 0 ? n3 : 1));
+    int c3 = 0, ca = 0, cb = 0;
     for (int i = 0; i < n; i++)
         for (int j = 0; j < n; j++)
             for (int k = 0; k < n; k++) {
@@ -145,25 +163,31 @@ static void build_triplets(v2o_problem *p) {
                 if (i >= j) continue;
                 t = p->bas_aab + 3 * ca++;
                 t[0] = i; t[1] = j; t[2] = k;
+                if (j >= k) continue;
+                t = p->bas_aaa + 3 * c3++;
+                t[0] = i; t[1] = j; t[2] = k;
             }
+    p->trip_aaa = c3;
     p->trip_aab = ca;
     p->trip_aba = cb;
 }
 
-/* positivity: 0 D, 1 DQ, 2 DG, 3 DQG, 4 DQGT2 (v2rdm_solver.cc:4081-4118).
+/* positivity: 0 D, 1 DQ, 2 DG, 3 DQG, 4 DQGT2, 5 DQGT1, 6 DQGT1T2 (= DQGT)
+ * (v2rdm_solver.cc:4081-4118).
  * hubbard selects the multiplicity convention of
  * v2rdm_solver.cc:862-863 (Hubbard) versus :983-984 (external). */
 v2o_problem *v2o_create(int n, int na, int nb, int positivity, int spin, int sz, int hubbard) {
-    if (n < 1 || na < 0 || nb < 0 || na > n || nb > n || positivity < 0 || positivity > 4) return NULL;
+    if (n < 1 || na < 0 || nb < 0 || na > n || nb > n || positivity < 0 || positivity > 6) return NULL;
     v2o_problem *p = (v2o_problem *)calloc(1, sizeof(v2o_problem));
     p->n = n; p->na = na; p->nb = nb;
-    p->q2 = (positivity == 1 || positivity == 3 || positivity == 4);
-    p->g2 = (positivity == 2 || positivity == 3 || positivity == 4);
-    p->t2 = positivity == 4;
+    p->q2 = (positivity == 1 || positivity >= 3);
+    p->g2 = (positivity >= 2);
+    p->t1 = (positivity == 5 || positivity == 6);
+    p->t2 = (positivity == 4 || positivity == 6);
     p->spin = spin != 0; p->sz = sz != 0;
     p->mult = hubbard ? 2 * (na - nb) + 1 : (na - nb) + 1;
     build_tables(p);
-    if (p->t2) build_triplets(p);
+    if (p->t1 || p->t2) build_triplets(p);
     set_offsets(p);
     return p;
 }
@@ -171,7 +195,7 @@ v2o_problem *v2o_create(int n, int na, int nb, int positivity, int spin, int sz,
 void v2o_destroy(v2o_problem *p) {
     if (!p) return;
     free(p->bas_ab); free(p->ibas_ab); free(p->bas_aa); free(p->ibas_aa);
-    free(p->bas_aab); free(p->bas_aba);
+    free(p->bas_aaa); free(p->bas_aab); free(p->bas_aba);
     free(p);
 }
 
@@ -188,9 +212,10 @@ void v2o_tables(const v2o_problem *p, int *bas_ab, int *ibas_ab, int *bas_aa, in
 }
 /* block offsets in the order d2ab d2aa d2bb d200 d1a d1b q1a q1b q2ab q2aa q2bb g2ab g2ba g2aa */
 void v2o_offsets(const v2o_problem *p, long *o) {
-    long v[18] = {p->d2ab, p->d2aa, p->d2bb, p->d200, p->d1a, p->d1b, p->q1a,
+    long v[22] = {p->d2ab, p->d2aa, p->d2bb, p->d200, p->d1a, p->d1b, p->q1a,
                   p->q1b,  p->q2ab, p->q2aa, p->q2bb, p->g2ab, p->g2ba, p->g2aa,
-                  p->t2aaa, p->t2bbb, p->t2aab, p->t2bba};
+                  p->t2aaa, p->t2bbb, p->t2aab, p->t2bba,
+                  p->t1aaa, p->t1bbb, p->t1aab, p->t1bba};
     memcpy(o, v, sizeof(v));
 }
 
@@ -440,6 +465,7 @@ void v2o_guess_hf(const v2o_problem *p, double *x) {
     for (int i = occ; i < n; i++) x[p->q1b + i * n + i] = 1.0;
     if (p->q2) q2_guess(p, x);
     if (p->g2) g2_guess(p, x);
+    if (p->t1) t1_visit(p, 0, T2_GUESS, NULL, NULL, x);   /* v2rdm_solver.cc:1817-1819 */
     if (p->t2) t2_visit(p, 0, T2_GUESS, NULL, NULL, x);   /* v2rdm_solver.cc:1820-1822 */
 }
 
@@ -569,6 +595,97 @@ static void t2_visit(const v2o_problem *p, long off, int mode, const double *u, 
                     double dum = 0.0;
                     for (int e = 0; e < nt; e++) dum += t[e].coef * x[t[e].col];
                     x[prim[blk] + id] = sb == 3 ? 0.0 : dum;
+                }
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------- T1 ---- */
+/* The T1 rows of t1.cc:419-795 (T1_constraints_Au, C1): each dual row is
+ *     -T1(r, c) + conditional Q2 / D2 / G2 / D1 terms (coefficients +-1),
+ * added in the reference's order, four sub-blocks in the order of dual rows:
+ *   0 T1aab (rows, cols: aab triplets)   t1.cc:421-467
+ *   1 T1bba                              t1.cc:469-515
+ *   2 T1aaa (aaa triplets, i<j<k)        t1.cc:517-650
+ *   3 T1bbb                              t1.cc:652-793
+ * A^T.y scatters the same terms in the same order (t1.cc:795-1200) and the
+ * guess sums them from zero (t1.cc:45-419). */
+#define T1_G2S(r, c, sh) (p->g2aa + ((long)(r) + (sh)) * 2 * p->gab + ((c) + (sh)))
+#define T1_G2H(base, r, c) ((base) + (long)(r) * p->gab + (c))
+
+static int t1_terms(const v2o_problem *p, int sb, int i, int j, int k, int l, int m, int q,
+                    t2_term *t) {
+    int nt = 0;
+    if (sb < 2) {   /* aab, bba */
+        const int b = sb == 1;
+        const long q2 = b ? p->q2bb : p->q2aa, g2 = b ? p->g2ab : p->g2ba;
+        if (k == q) T2_ADD(q2 + (long)IAA(p, i, j) * p->gaa + IAA(p, l, m), 1.0);
+        if (b) {
+            if (j == l) T2_ADD(T2_D2AB(q, m, k, i), -1.0);
+            if (l == i) T2_ADD(T2_D2AB(q, m, k, j), 1.0);
+        } else {
+            if (j == l) T2_ADD(T2_D2AB(m, q, i, k), -1.0);
+            if (l == i) T2_ADD(T2_D2AB(m, q, j, k), 1.0);
+        }
+        if (j == m) T2_ADD(T1_G2H(g2, IAB(p, q, i), IAB(p, k, l)), -1.0);
+        if (i == m) T2_ADD(T1_G2H(g2, IAB(p, q, j), IAB(p, k, l)), 1.0);
+        return nt;
+    }
+    /* aaa, bbb */
+    const int b = sb == 3;
+    const long q2 = b ? p->q2bb : p->q2aa, d2 = b ? p->d2bb : p->d2aa, d1 = b ? p->d1b : p->d1a;
+    const int sh = b ? p->gab : 0;
+#define T1_AA(base, a, bb, c, d) ((base) + (long)IAA(p, a, bb) * p->gaa + IAA(p, c, d))
+    if (k == q) T2_ADD(T1_AA(q2, i, j, l, m), 1.0);
+    if (j == q) T2_ADD(T1_AA(q2, i, k, l, m), -1.0);
+    if (i == q) T2_ADD(T1_AA(q2, j, k, l, m), 1.0);
+    if (l == k) T2_ADD(T1_AA(d2, q, m, j, i), 1.0);
+    if (j == l) T2_ADD(T1_AA(d2, q, m, k, i), -1.0);
+    if (l == i) T2_ADD(T1_AA(d2, q, m, k, j), 1.0);
+    if (k == m) {
+        if (j == l) T2_ADD(d1 + (long)q * p->n + i, -1.0);
+        T2_ADD(T1_G2S(IAB(p, q, i), IAB(p, j, l), sh), 1.0);
+    }
+    if (j == m) {
+        if (k == l) T2_ADD(d1 + (long)q * p->n + i, 1.0);
+        T2_ADD(T1_G2S(IAB(p, q, i), IAB(p, k, l), sh), -1.0);
+    }
+    if (i == m) {
+        if (k == l) T2_ADD(d1 + (long)q * p->n + j, -1.0);
+        T2_ADD(T1_G2S(IAB(p, q, j), IAB(p, k, l), sh), 1.0);
+    }
+#undef T1_AA
+    return nt;
+}
+
+static void t1_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
+                     double *x) {
+    const long ta = p->trip_aab, t3 = p->trip_aaa;
+    const long dual[4] = {off, off + ta * ta, off + 2 * ta * ta, off + 2 * ta * ta + t3 * t3};
+    const long prim[4] = {p->t1aab, p->t1bba, p->t1aaa, p->t1bbb};
+    for (int sb = 0; sb < 4; sb++) {
+        const long nr = sb < 2 ? ta : t3;
+        const int *tb = sb < 2 ? p->bas_aab : p->bas_aaa;
+        for (long r = 0; r < nr; r++) {
+            const int i = tb[3 * r], j = tb[3 * r + 1], k = tb[3 * r + 2];
+            for (long c = 0; c < nr; c++) {
+                const int l = tb[3 * c], m = tb[3 * c + 1], q = tb[3 * c + 2];
+                const long id = r * nr + c;
+                t2_term t[12];
+                const int nt = t1_terms(p, sb, i, j, k, l, m, q, t);
+                if (mode == T2_AU) {
+                    double dum = -u[prim[sb] + id];
+                    for (int e = 0; e < nt; e++) dum += t[e].coef * u[t[e].col];
+                    A[dual[sb] + id] = dum;
+                } else if (mode == T2_ATU) {
+                    const double dum = u[dual[sb] + id];
+                    A[prim[sb] + id] -= dum;
+                    for (int e = 0; e < nt; e++) A[t[e].col] += t[e].coef * dum;
+                } else {
+                    double dum = 0.0;
+                    for (int e = 0; e < nt; e++) dum += t[e].coef * x[t[e].col];
+                    x[prim[sb] + id] = dum;
                 }
             }
         }
@@ -915,6 +1032,10 @@ void v2o_Au(const v2o_problem *p, const double *u, double *A) {
         }
         off += 4L * gab * gab;
     }
+    if (p->t1) {   /* v2rdm_solver.cc:3015-3017 */
+        t1_visit(p, off, T2_AU, u, A, NULL);
+        off += 2L * p->trip_aab * p->trip_aab + 2L * p->trip_aaa * p->trip_aaa;
+    }
     if (p->t2) t2_visit(p, off, T2_AU, u, A, NULL);   /* v2rdm_solver.cc:3019-3022 */
 }
 
@@ -1246,6 +1367,10 @@ void v2o_ATu(const v2o_problem *p, const double *u, double *A) {
             }
         }
         off += 4L * gab * gab;
+    }
+    if (p->t1) {   /* v2rdm_solver.cc:3073-3075 */
+        t1_visit(p, off, T2_ATU, u, A, NULL);
+        off += 2L * p->trip_aab * p->trip_aab + 2L * p->trip_aaa * p->trip_aaa;
     }
     if (p->t2) t2_visit(p, off, T2_ATU, u, A, NULL);   /* v2rdm_solver.cc:3077-3080 */
 }

@@ -29,6 +29,8 @@ CASES = [
     ("ext1_dqg", 1, 1, 0, "DQG", True, True, None),
     ("hub3_dqgt2", 3, 1, 1, "DQGT2", True, True, (1.0, 4.0)),
     ("ext3_dqgt2_doublet", 3, 2, 1, "DQGT2", True, True, None),
+    ("hub4_dqgt1", 4, 2, 2, "DQGT1", True, True, (1.0, 4.0)),
+    ("ext4_dqgt1t2_doublet", 4, 2, 1, "DQGT1T2", True, True, None),
 ]
 
 

@@ -66,7 +66,7 @@ def test_header_symbols_exported():
 
 @pytest.mark.parametrize("name", ["hub2_dqg", "hub4_dqg", "hub4_d_nospin", "ext3_dqg_triplet",
                                   "ext4_dq_nosz", "ext4_dg_doublet", "ext1_dqg", "hub3_dqgt2",
-                                  "ext3_dqgt2_doublet"])
+                                  "ext3_dqgt2_doublet", "hub4_dqgt1", "ext4_dqgt1t2_doublet"])
 def test_host_problem_matches_golden(golden, name):
     case = golden[name]
     kw = case_kwargs(case)
@@ -89,7 +89,8 @@ def test_host_problem_matches_golden(golden, name):
 
 def test_layout_helper_matches_library():
     for args in [(4, 2, 2, "DQG", True), (3, 2, 1, "DQG", True), (4, 2, 2, "D", False),
-                 (4, 2, 1, "DG", True), (3, 2, 1, "DQGT2", True)]:
+                 (4, 2, 1, "DG", True), (3, 2, 1, "DQGT2", True), (4, 2, 2, "DQGT1", True),
+                 (4, 2, 1, "DQGT1T2", True), (3, 1, 1, "DQGT", False)]:
         p = hb.V2RDMProblem(args[0], args[1], args[2], args[3], args[4])
         assert [d for _, d in hb.block_layout(*args)] == list(p.dims)
 
@@ -100,7 +101,7 @@ def test_bad_arguments_are_rejected():
     with pytest.raises(hb.V2BError):
         hb.V2RDMProblem(0, 0, 0)
     with pytest.raises(ValueError):
-        hb.V2RDMProblem(4, 2, 2, positivity="DQGT1")
+        hb.V2RDMProblem(4, 2, 2, positivity="3POS")
 
 
 def test_device_calls_fail_loudly_without_gpu():
@@ -120,3 +121,28 @@ def test_config5_sizes_match_the_oracle():
     p = hb.V2RDMProblem(16, 8, 8, "DQGT2", True, True, hubbard_multiplicity=True)
     assert (p.n_primal, p.n_dual) == (80405760, 80515780)
     assert sorted(set(int(d) for d in p.dims)) == [16, 120, 256, 512, 1920, 6016]
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libv2rdm_ref.so")),
+                    reason="oracle/_ref not built")
+def test_triplet_families_bit_exact_against_reference_grid():
+    """T1 and T2 together (DQGT1T2): sizes, b, c, both guesses and the
+    packed A / A^T, against hilbert's compiled code, n = 1..3."""
+    import itertools
+    from oracle.maps import RefProblem
+    rng = np.random.default_rng(31)
+    for n, na, nb, spin, sz in itertools.product([1, 2, 3], [0, 1, 2], [0, 1, 2], [0, 1], [0, 1]):
+        if na > n or nb > n:
+            continue
+        h, g = rng.standard_normal((n, n)), rng.standard_normal((n,) * 4)
+        r = RefProblem(n, na, nb, "DQGT1T2", spin, sz, h=h, g=g)
+        rh = RefProblem(n, na, nb, "DQGT1T2", spin, sz, h=h, g=g, guess="hf")
+        p = hb.V2RDMProblem(n, na, nb, "DQGT1T2", bool(spin), bool(sz))
+        assert (p.n_primal, p.n_dual) == (r.n_primal, r.n_dual) and list(p.dims) == list(r.dims)
+        assert np.array_equal(p.b(), r.b) and np.array_equal(p.c_external(h, g), r.c)
+        assert np.array_equal(p.guess("RANDOM"), r.x0) and np.array_equal(p.guess("HF"), rh.x0)
+        x, y = rng.standard_normal(r.n_primal), rng.standard_normal(r.n_dual)
+        rp, ent, pal = operator(p, False)
+        assert np.array_equal(packed_apply(rp, ent, pal, x), r.Au(x))
+        rp, ent, pal = operator(p, True)
+        assert np.array_equal(packed_apply(rp, ent, pal, y), r.ATu(y))

@@ -20,7 +20,8 @@ def test_golden_cases_present(golden):
 
 @pytest.mark.parametrize("name", ["hub2_dqg", "hub4_dqg", "hub4_d_nospin", "ext3_dqg_triplet",
                                   "ext4_dq_nosz", "ext4_dg_doublet", "ext5_dqg", "ext1_dqg",
-                                  "hub3_dqgt2", "ext3_dqgt2_doublet"])
+                                  "hub3_dqgt2", "ext3_dqgt2_doublet", "hub4_dqgt1",
+                                  "ext4_dqgt1t2_doublet"])
 def test_oracle_matches_golden(golden, name):
     case = golden[name]
     kw = case_kwargs(case)
@@ -83,7 +84,8 @@ def test_hf_guess_satisfies_d_constraints():
 def test_oracle_bit_exact_against_reference_grid():
     rng = np.random.default_rng(3)
     for n, na, nb, pos, spin, sz in itertools.product([1, 2, 3, 4], [0, 1, 2], [0, 1, 2],
-                                                      ["D", "DQ", "DG", "DQG", "DQGT2"], [0, 1], [0, 1]):
+                                                      ["D", "DQ", "DG", "DQG", "DQGT2", "DQGT1",
+                                                       "DQGT1T2"], [0, 1], [0, 1]):
         if na > n or nb > n:
             continue
         kw = dict(h=rng.standard_normal((n, n)), g=rng.standard_normal((n,) * 4))
@@ -99,17 +101,18 @@ def test_oracle_bit_exact_against_reference_grid():
 
 
 @pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
-def test_oracle_t2_guesses_bit_exact_against_reference_grid():
-    """The T2 part of the HF guess (t2.cc:1845-2452) and the random guess
-    with T2 blocks present, against hilbert's compiled code."""
+@pytest.mark.parametrize("pos", ["DQGT2", "DQGT1", "DQGT1T2"])
+def test_oracle_triplet_guesses_bit_exact_against_reference_grid(pos):
+    """The T1 / T2 parts of the HF guess (t1.cc:45-419, t2.cc:1845-2452) and
+    the random guess with those blocks present, against hilbert's compiled code."""
     rng = np.random.default_rng(11)
     for n, na, nb, spin, sz in itertools.product([1, 2, 3, 4], [0, 1, 2], [0, 1, 2], [0, 1], [0, 1]):
         if na > n or nb > n:
             continue
         kw = dict(h=rng.standard_normal((n, n)), g=rng.standard_normal((n,) * 4))
-        o = OracleProblem(n, na, nb, "DQGT2", spin, sz, **kw)
+        o = OracleProblem(n, na, nb, pos, spin, sz, **kw)
         for kind in ("random", "hf"):
-            r = RefProblem(n, na, nb, "DQGT2", spin, sz, guess=kind, **kw)
+            r = RefProblem(n, na, nb, pos, spin, sz, guess=kind, **kw)
             assert same(r.x0, o.guess(kind)), (n, na, nb, spin, sz, kind)
 
 
