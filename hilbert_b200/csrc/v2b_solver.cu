@@ -1426,7 +1426,8 @@ int v2b_problem_create(int nmo, int nalpha, int nbeta, int positivity, int const
         spec.nmo = nmo;
         spec.nalpha = nalpha;
         spec.nbeta = nbeta;
-        spec.positivity = positivity;
+        spec.positivity = positivity & 15;
+        spec.constrain_d3 = (positivity & V2B_CONSTRAIN_D3) != 0;
         spec.constrain_spin = constrain_spin != 0;
         spec.constrain_sz = constrain_sz != 0;
         spec.hubbard_multiplicity = hubbard_multiplicity != 0;

@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <stdexcept>
+#include <vector>
 
 namespace v2b {
 
@@ -31,6 +32,7 @@ Problem make_problem(const ProblemSpec &spec) {
     p.g2 = spec.positivity == POS_DG || spec.positivity >= POS_DQG;
     p.t1 = spec.positivity == POS_DQGT1 || spec.positivity == POS_DQGT1T2;
     p.t2 = spec.positivity == POS_DQGT2 || spec.positivity == POS_DQGT1T2;
+    p.d3 = spec.constrain_d3;
     p.mult = spec.hubbard_multiplicity ? 2 * (spec.nalpha - spec.nbeta) + 1
                                        : (spec.nalpha - spec.nbeta) + 1;
 
@@ -84,15 +86,23 @@ Problem make_problem(const ProblemSpec &spec) {
         add_block(p.g2ba, p.gab);
         add_block(p.g2aa, 2 * p.gab);
     }
-    if (p.t1 || p.t2) {   // basis.cc:640-745: lexicographic triplets
+    if (p.t1 || p.t2 || p.d3) {   // basis.cc:640-745: lexicographic triplets
         p.trip_aba = n * n * n;
+        p.ibas_aaa.assign((size_t)n * n * n, -999);
+        p.ibas_aab.assign((size_t)n * n * n, -999);
+        auto at = [&](int a, int b, int c) { return ((size_t)a * n + b) * n + c; };
         for (int i = 0; i < n; i++)
             for (int j = i + 1; j < n; j++)
                 for (int k = 0; k < n; k++) {
+                    const int ta = (int)(p.bas_aab.size() / 3);
+                    p.ibas_aab[at(i, j, k)] = p.ibas_aab[at(j, i, k)] = ta;
                     p.bas_aab.push_back(i);
                     p.bas_aab.push_back(j);
                     p.bas_aab.push_back(k);
                     if (k > j) {
+                        const int t3 = (int)(p.bas_aaa.size() / 3);
+                        for (size_t e : {at(i, j, k), at(i, k, j), at(j, i, k), at(j, k, i), at(k, i, j), at(k, j, i)})
+                            p.ibas_aaa[e] = t3;
                         p.bas_aaa.push_back(i);
                         p.bas_aaa.push_back(j);
                         p.bas_aaa.push_back(k);
@@ -113,6 +123,12 @@ Problem make_problem(const ProblemSpec &spec) {
         add_block(p.t2aab, p.trip_aab);
         add_block(p.t2bba, p.trip_aab);
     }
+    if (p.d3) {   // v2rdm_solver.cc:4000-4029
+        add_block(p.d3aaa, p.trip_aaa);
+        add_block(p.d3bbb, p.trip_aaa);
+        add_block(p.d3aab, p.trip_aab);
+        add_block(p.d3bba, p.trip_aab);
+    }
     p.n_primal = off;
 
     const int64_t gab2 = (int64_t)p.gab * p.gab, gaa2 = (int64_t)p.gaa * p.gaa, n2 = (int64_t)n * n;
@@ -128,6 +144,11 @@ Problem make_problem(const ProblemSpec &spec) {
     if (p.t2) {
         const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
         d += 2 * aab * aab + 2 * big * big;
+    }
+    if (p.d3) {   // v2rdm_solver.cc:3624-3660
+        d += spec.constrain_sz ? 4 * gaa2 + 2 * gab2 : 2 * gaa2 + gab2;
+        if (spec.constrain_spin && singlet)
+            d += (int64_t)p.trip_aab * p.trip_aab + 2 * (int64_t)p.trip_aaa * p.trip_aaa;
     }
     p.n_dual = d;
     if (p.n_primal > (int64_t)kColMask || p.n_dual > (int64_t)kColMask)
@@ -317,6 +338,106 @@ void t1_rows(const Problem &p, int64_t off, F &&f) {
             }
         }
         off += (int64_t)nr * nr;
+    }
+}
+
+// ------------------------------------------------------------------ D3
+// CONSTRAIN_D3 rows (d3.cc:45-406, D3_constraints_Au, C1): plain term lists,
+// first a D2 element times an electron count, then D3 elements with
+// coefficients -+1 (contractions D3 -> D2, with CONSTRAIN_SZ six families,
+// d3.cc:49-212, without it three, :213-330) and, for singlets with
+// CONSTRAIN_SPIN, D3aab - D3bba and D3aaa (D3bbb) minus a third of nine D3aab
+// (D3bba) elements (:332-404).  D3_constraints_ATu (d3.cc:408-766) scatters
+// the same terms in the same order.  f(dual_row, cols, coefs, nterms).
+template <class F>
+void d3_rows(const Problem &p, int64_t off, F &&f) {
+    const int N = p.n, gab = p.gab, gaa = p.gaa;
+    const int64_t t3 = p.trip_aaa, ta = p.trip_aab;
+    const double na = p.spec.nalpha, nb = p.spec.nbeta;
+    const bool sz = p.spec.constrain_sz;
+    std::vector<int64_t> cols;
+    std::vector<double> coef;
+    auto add = [&](int64_t c, double v) {
+        cols.push_back(c);
+        coef.push_back(v);
+    };
+    auto emit = [&]() {
+        f(off++, cols.data(), coef.data(), (int)cols.size());
+        cols.clear();
+        coef.clear();
+    };
+    auto aaa = [&](int a, int b, int c) { return (int64_t)p.ibas_aaa[((size_t)a * N + b) * N + c]; };
+    auto aab = [&](int a, int b, int c) { return (int64_t)p.ibas_aab[((size_t)a * N + b) * N + c]; };
+    // parity of sorting (a, b, q) with a < b into triplet order: odd when a < q < b
+    auto mid = [](int a, int q, int b) { return (a < q && q < b) ? -1.0 : 1.0; };
+    for (int fam = 0; fam < (sz ? 4 : 2); fam++) {
+        const bool beta = fam % 2 == 1;
+        const int64_t d2 = beta ? p.d2bb : p.d2aa;
+        const int64_t same = beta ? p.d3bbb : p.d3aaa, mixed = beta ? p.d3bba : p.d3aab;
+        for (int ij = 0; ij < gaa; ij++) {
+            const int i = p.bas_aa[2 * ij], j = p.bas_aa[2 * ij + 1];
+            for (int kl = 0; kl < gaa; kl++) {
+                const int k = p.bas_aa[2 * kl], l = p.bas_aa[2 * kl + 1];
+                const int64_t d2e = d2 + (int64_t)ij * gaa + kl;
+                if (sz && fam < 2) {
+                    add(d2e, (beta ? nb : na) - 2.0);
+                    for (int q = 0; q < N; q++) {
+                        if (q == i || q == j || q == k || q == l) continue;
+                        add(same + aaa(i, j, q) * t3 + aaa(k, l, q), -mid(i, q, j) * mid(k, q, l));
+                    }
+                } else if (sz) {
+                    add(d2e, beta ? na : nb);
+                    for (int q = 0; q < N; q++) add(mixed + aab(i, j, q) * ta + aab(k, l, q), -1.0);
+                } else {
+                    add(d2e, na + nb - 2.0);
+                    for (int q = 0; q < N; q++) {
+                        add(mixed + aab(i, j, q) * ta + aab(k, l, q), -1.0);
+                        if (q == i || q == j || q == k || q == l) continue;
+                        add(same + aaa(i, j, q) * t3 + aaa(k, l, q), -mid(i, q, j) * mid(k, q, l));
+                    }
+                }
+                emit();
+            }
+        }
+    }
+    for (int fam = 0; fam < (sz ? 2 : 1); fam++) {
+        for (int ij = 0; ij < gab; ij++) {
+            const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+                add(p.d2ab + (int64_t)ij * gab + kl, !sz ? na + nb - 2.0 : (fam ? nb - 1.0 : na - 1.0));
+                for (int q = 0; q < N; q++) {
+                    if ((!sz || fam == 0) && q != i && q != k)
+                        add(p.d3aab + aab(i, q, j) * ta + aab(k, q, l), -((q < i ? -1.0 : 1.0) * (q < k ? -1.0 : 1.0)));
+                    if ((!sz || fam == 1) && q != j && q != l)
+                        add(p.d3bba + aab(j, q, i) * ta + aab(l, q, k), -((q < j ? -1.0 : 1.0) * (q < l ? -1.0 : 1.0)));
+                }
+                emit();
+            }
+        }
+    }
+    if (p.spec.constrain_spin && p.spec.nalpha == p.spec.nbeta) {
+        for (int64_t e = 0; e < ta * ta; e++) {
+            add(p.d3aab + e, 1.0);
+            add(p.d3bba + e, -1.0);
+            emit();
+        }
+        const double third = 1.0 / 3.0;
+        for (int beta = 0; beta < 2; beta++) {
+            const int64_t same = beta ? p.d3bbb : p.d3aaa, mixed = beta ? p.d3bba : p.d3aab;
+            for (int64_t r = 0; r < t3; r++) {
+                const int a = p.bas_aaa[3 * r], b = p.bas_aaa[3 * r + 1], c = p.bas_aaa[3 * r + 2];
+                const int64_t rr[3] = {aab(a, b, c), aab(a, c, b), aab(b, c, a)};
+                for (int64_t s = 0; s < t3; s++) {
+                    const int x = p.bas_aaa[3 * s], y = p.bas_aaa[3 * s + 1], z = p.bas_aaa[3 * s + 2];
+                    const int64_t cc[3] = {aab(x, y, z), aab(x, z, y), aab(y, z, x)};
+                    add(same + r * t3 + s, 1.0);
+                    for (int u = 0; u < 3; u++)
+                        for (int v = 0; v < 3; v++) add(mixed + rr[u] * ta + cc[v], (u + v) % 2 ? third : -third);
+                    emit();
+                }
+            }
+        }
     }
 }
 
@@ -873,6 +994,12 @@ void visit_A(const Problem &p, S &s) {
         const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
         off += 2 * aab * aab + 2 * big * big;
     }
+    if (p.d3) {   // d3.cc:45-406
+        d3_rows(p, off, [&](int64_t row, const int64_t *cols, const double *coef, int nt) {
+            for (int q = 0; q < nt; q++) s.t(row, cols[q], coef[q]);
+            off++;
+        });
+    }
     if (off != p.n_dual) throw std::logic_error("A emitter row count mismatch");
 }
 
@@ -1174,6 +1301,12 @@ void visit_AT(const Problem &p, S &s) {
         });
         const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
         off += 2 * aab * aab + 2 * big * big;
+    }
+    if (p.d3) {   // d3.cc:408-766 scatters in the same order as the A rows
+        d3_rows(p, off, [&](int64_t row, const int64_t *cols, const double *coef, int nt) {
+            for (int q = 0; q < nt; q++) s.t(cols[q], row, coef[q]);
+            off++;
+        });
     }
     if (off != p.n_dual) throw std::logic_error("A^T emitter row count mismatch");
 }

@@ -27,6 +27,7 @@ DEFAULTS = {
     "POSITIVITY": "DQG",            # :220
     "CONSTRAIN_SPIN": True,         # :306
     "CONSTRAIN_SZ": True,           # :309
+    "CONSTRAIN_D3": False,          # :226
     "TPDM_GUESS": "RANDOM",         # :205
     "SDP_SOLVER": "BPSDP",          # :246
     "HUBBARD_HAMILTONIAN": False,   # :249
@@ -87,11 +88,12 @@ class V2RDMProblem:
         lib = _capi.load()
         self._lib = lib
         h = ctypes.c_void_p()
-        pos = positivity.upper()
-        if pos not in _capi.POSITIVITY:
+        pos, _, extra = positivity.upper().partition("+")
+        if pos not in _capi.POSITIVITY or extra not in ("", "D3"):
             raise ValueError(f"POSITIVITY {positivity} is not on the device path "
-                             f"(supported: {sorted(_capi.POSITIVITY)})")
-        check(lib.v2b_problem_create(int(nmo), int(nalpha), int(nbeta), _capi.POSITIVITY[pos],
+                             f"(supported: {sorted(_capi.POSITIVITY)}, each optionally +D3)")
+        code = _capi.POSITIVITY[pos] | (_capi.V2B_CONSTRAIN_D3 if extra == "D3" else 0)
+        check(lib.v2b_problem_create(int(nmo), int(nalpha), int(nbeta), code,
                                      int(bool(constrain_spin)), int(bool(constrain_sz)),
                                      int(bool(hubbard_multiplicity)), ctypes.byref(h)))
         self._h = h
@@ -411,7 +413,8 @@ class v2RDMHelper:
         else:
             raise TypeError("v2RDMHelper(nalpha, nbeta, nmo, h, g, options) or v2RDMHelper(ref_wfn, options)")
         o = self.options
-        self.problem = V2RDMProblem(nmo, nalpha, nbeta, o.get("POSITIVITY"), o.get("CONSTRAIN_SPIN"),
+        pos = o.get("POSITIVITY") + ("+D3" if o.get("CONSTRAIN_D3") else "")
+        self.problem = V2RDMProblem(nmo, nalpha, nbeta, pos, o.get("CONSTRAIN_SPIN"),
                                     o.get("CONSTRAIN_SZ"), hubbard_multiplicity=self._hubbard)
         p = self.problem
         if self._hubbard:
@@ -448,7 +451,7 @@ def block_layout(nmo, nalpha, nbeta, positivity="DQG", constrain_spin=True):
     """[(name, dim)] in the primal order of set_primal_offsets (v2rdm_solver.cc:3729-4079)."""
     n = int(nmo)
     gab, gaa = n * n, n * (n - 1) // 2
-    pos = positivity.upper()
+    pos, _, extra = positivity.upper().partition("+")
     blocks = [("d2ab", gab), ("d2aa", gaa), ("d2bb", gaa)]
     if constrain_spin:
         blocks.append(("d200", gab if nalpha == nbeta else 2 * gab))
@@ -463,6 +466,8 @@ def block_layout(nmo, nalpha, nbeta, positivity="DQG", constrain_spin=True):
         blocks += [("t1aaa", aaa), ("t1bbb", aaa), ("t1aab", aab), ("t1bba", aab)]
     if pos in ("DQGT2", "DQGT1T2", "DQGT"):
         blocks += [("t2aaa", aab + aba), ("t2bbb", aab + aba), ("t2aab", aab), ("t2bba", aab)]
+    if extra == "D3":
+        blocks += [("d3aaa", aaa), ("d3bbb", aaa), ("d3aab", aab), ("d3bba", aab)]
     return blocks
 
 

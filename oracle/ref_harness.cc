@@ -145,7 +145,8 @@ class RefProblem : public v2RDMSolver {
             {"q2ab", q2aboff}, {"q2aa", q2aaoff}, {"q2bb", q2bboff}, {"g2ab", g2aboff},
             {"g2ba", g2baoff}, {"g2aa", g2aaoff}, {"t2aaa", t2aaaoff}, {"t2bbb", t2bbboff},
             {"t2aab", t2aaboff}, {"t2bba", t2bbaoff}, {"t1aaa", t1aaaoff}, {"t1bbb", t1bbboff},
-            {"t1aab", t1aaboff}, {"t1bba", t1bbaoff}};
+            {"t1aab", t1aaboff}, {"t1bba", t1bbaoff}, {"d3aaa", d3aaaoff}, {"d3bbb", d3bbboff},
+            {"d3aab", d3aaboff}, {"d3bba", d3bbaoff}};
         auto it = m.find(name);
         if (it == m.end()) return -1;
         bool present = false;
@@ -154,6 +155,7 @@ class RefProblem : public v2RDMSolver {
         else if (name[0] == 'g') present = constrain_g2_;
         else if (name[0] == 't' && name[1] == '2') present = constrain_t2_;
         else if (name[0] == 't' && name[1] == '1') present = constrain_t1_;
+        else if (name[0] == 'd' && name[1] == '3') present = constrain_d3_;
         else present = true;
         if (!present || it->second == nullptr) return -1;
         return it->second[0];
@@ -186,13 +188,23 @@ extern "C" {
 
 const char *v2b_ref_last_error() { return g_last_error.c_str(); }
 
-/* positivity: "D", "DQ", "DG", "DQG", "DQGT1", "DQGT2", "DQGT1T2"; guess_hf: 0 random, 1 HF */
+/* positivity: "D", "DQ", "DG", "DQG", "DQGT1", "DQGT2", "DQGT1T2", optionally followed by
+ * "+D3" (CONSTRAIN_D3 true); guess_hf: 0 random, 1 HF */
 void *v2b_ref_create(int nmo, int nalpha, int nbeta, const char *positivity, int constrain_spin,
                      int constrain_sz, int hubbard, double hub_t, double hub_u, const double *h,
                      const double *g, int guess_hf) {
     try {
         auto *opts = new Options();
-        opts->set_str("POSITIVITY", positivity);
+        std::string pos(positivity);
+        bool d3 = false;
+        const size_t plus = pos.find('+');
+        if (plus != std::string::npos) {
+            if (pos.substr(plus + 1) != "D3") throw std::invalid_argument("unknown constraint suffix");
+            d3 = true;
+            pos = pos.substr(0, plus);
+        }
+        opts->set_str("POSITIVITY", pos);
+        opts->set_bool("CONSTRAIN_D3", d3);
         opts->set_bool("CONSTRAIN_SPIN", constrain_spin != 0);
         opts->set_bool("CONSTRAIN_SZ", constrain_sz != 0);
         opts->set_str("GPC_CONSTRAINTS", "NONE");

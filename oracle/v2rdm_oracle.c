@@ -9,7 +9,7 @@
  * restates (paths relative to the hilbert source tree).
  *
  * Supported constraint sets: POSITIVITY D / DQ / DG / DQG / DQGT1 / DQGT2 /
- * DQGT1T2 with
+ * DQGT1T2, each optionally with CONSTRAIN_D3, with
  * CONSTRAIN_SPIN and CONSTRAIN_SZ on or off, singlet and non-singlet.
  */
 #include <math.h>
@@ -19,14 +19,15 @@
 typedef struct {
     int n;            /* active orbitals (amo_) */
     int na, nb;       /* alpha / beta electrons */
-    int q2, g2, t1, t2, spin, sz;
+    int q2, g2, t1, t2, d3, spin, sz;
     int mult;         /* 2S+1 as the reference stores it */
     int gab, gaa;
     int *bas_ab, *ibas_ab, *bas_aa, *ibas_aa;
     long d2ab, d2aa, d2bb, d200, d1a, d1b, q1a, q1b, q2ab, q2aa, q2bb, g2ab, g2ba, g2aa;
-    long t1aaa, t1bbb, t1aab, t1bba, t2aaa, t2bbb, t2aab, t2bba;
+    long t1aaa, t1bbb, t1aab, t1bba, t2aaa, t2bbb, t2aab, t2bba, d3aaa, d3bbb, d3aab, d3bba;
     int trip_aaa, trip_aab, trip_aba;   /* triplets (i<j<k), (i<j, k) and (i, j, k) */
     int *bas_aaa, *bas_aab, *bas_aba;   /* 3 ints per triplet */
+    int *ibas_aaa, *ibas_aab;           /* n^3: any order of an aaa set / of the aa pair */
     long n_primal, n_dual;
     int nblocks;
     int dims[32];
@@ -70,6 +71,7 @@ static void t1_visit(const v2o_problem *p, long off, int mode, const double *u, 
                      double *x);
 static void t2_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
                      double *x);
+static void d3_visit(const v2o_problem *p, long off, int mode, const double *u, double *A);
 
 /* v2rdm_solver.cc:3729-4079 (set_primal_offsets) and 3294-3727 (sizes) */
 static void set_offsets(v2o_problem *p) {
@@ -118,6 +120,15 @@ static void set_offsets(v2o_problem *p) {
         p->t2aab = off; off += ta * ta; p->dims[nb++] = (int)ta;
         p->t2bba = off; off += ta * ta; p->dims[nb++] = (int)ta;
     }
+    /* v2rdm_solver.cc:4000-4029: D3aaa, D3bbb (dim aaa), D3aab, D3bba (dim aab) */
+    p->d3aaa = p->d3bbb = p->d3aab = p->d3bba = -1;
+    if (p->d3) {
+        long t3 = p->trip_aaa, ta = p->trip_aab;
+        p->d3aaa = off; off += t3 * t3; p->dims[nb++] = (int)t3;
+        p->d3bbb = off; off += t3 * t3; p->dims[nb++] = (int)t3;
+        p->d3aab = off; off += ta * ta; p->dims[nb++] = (int)ta;
+        p->d3bba = off; off += ta * ta; p->dims[nb++] = (int)ta;
+    }
     p->n_primal = off;
     p->nblocks = nb;
 
@@ -142,6 +153,11 @@ static void set_offsets(v2o_problem *p) {
         long w = (long)p->trip_aab + p->trip_aba, ta = p->trip_aab;
         d += 2 * w * w + 2 * ta * ta;
     }
+    if (p->d3) {   /* v2rdm_solver.cc:3624-3660 */
+        long t3 = p->trip_aaa, ta = p->trip_aab;
+        d += p->sz ? 4L * gaa * gaa + 2L * gab * gab : 2L * gaa * gaa + (long)gab * gab;
+        if (p->spin && p->na == p->nb) d += ta * ta + 2 * t3 * t3;
+    }
     p->n_dual = d;
 }
 
@@ -154,6 +170,10 @@ static void build_triplets(v2o_problem *p) {
     p->bas_aba = (int *)malloc(sizeof(int) * 3 * (n3 > 0 ? n3 : 1));
     p->bas_aab = (int *)malloc(sizeof(int) * 3 * (n3 > 0 ? n3 : 1));
     p->bas_aaa = (int *)malloc(sizeof(int) * 3 * (n3 > 0 ? n3 : 1));
+    p->ibas_aaa = (int *)malloc(sizeof(int) * (n3 > 0 ? n3 : 1));
+    p->ibas_aab = (int *)malloc(sizeof(int) * (n3 > 0 ? n3 : 1));
+    for (long e = 0; e < n3; e++) p->ibas_aaa[e] = p->ibas_aab[e] = -999;
+#define TRIP(a, b, c) (((long)(a) * n + (b)) * n + (c))
     int c3 = 0, ca = 0, cb = 0;
     for (int i = 0; i < n; i++)
         for (int j = 0; j < n; j++)
@@ -161,25 +181,32 @@ static void build_triplets(v2o_problem *p) {
                 int *t = p->bas_aba + 3 * cb++;
                 t[0] = i; t[1] = j; t[2] = k;
                 if (i >= j) continue;
+                p->ibas_aab[TRIP(i, j, k)] = p->ibas_aab[TRIP(j, i, k)] = ca;
                 t = p->bas_aab + 3 * ca++;
                 t[0] = i; t[1] = j; t[2] = k;
                 if (j >= k) continue;
+                p->ibas_aaa[TRIP(i, j, k)] = p->ibas_aaa[TRIP(i, k, j)] = p->ibas_aaa[TRIP(j, i, k)] = c3;
+                p->ibas_aaa[TRIP(j, k, i)] = p->ibas_aaa[TRIP(k, i, j)] = p->ibas_aaa[TRIP(k, j, i)] = c3;
                 t = p->bas_aaa + 3 * c3++;
                 t[0] = i; t[1] = j; t[2] = k;
             }
+#undef TRIP
     p->trip_aaa = c3;
     p->trip_aab = ca;
     p->trip_aba = cb;
 }
 
 /* positivity: 0 D, 1 DQ, 2 DG, 3 DQG, 4 DQGT2, 5 DQGT1, 6 DQGT1T2 (= DQGT)
- * (v2rdm_solver.cc:4081-4118).
+ * (v2rdm_solver.cc:4081-4118), plus 16 for CONSTRAIN_D3 (:4120-4122).
  * hubbard selects the multiplicity convention of
  * v2rdm_solver.cc:862-863 (Hubbard) versus :983-984 (external). */
 v2o_problem *v2o_create(int n, int na, int nb, int positivity, int spin, int sz, int hubbard) {
+    const int d3 = (positivity >> 4) & 1;
+    positivity &= 15;
     if (n < 1 || na < 0 || nb < 0 || na > n || nb > n || positivity < 0 || positivity > 6) return NULL;
     v2o_problem *p = (v2o_problem *)calloc(1, sizeof(v2o_problem));
     p->n = n; p->na = na; p->nb = nb;
+    p->d3 = d3;
     p->q2 = (positivity == 1 || positivity >= 3);
     p->g2 = (positivity >= 2);
     p->t1 = (positivity == 5 || positivity == 6);
@@ -187,7 +214,7 @@ v2o_problem *v2o_create(int n, int na, int nb, int positivity, int spin, int sz,
     p->spin = spin != 0; p->sz = sz != 0;
     p->mult = hubbard ? 2 * (na - nb) + 1 : (na - nb) + 1;
     build_tables(p);
-    if (p->t1 || p->t2) build_triplets(p);
+    if (p->t1 || p->t2 || p->d3) build_triplets(p);
     set_offsets(p);
     return p;
 }
@@ -195,7 +222,7 @@ v2o_problem *v2o_create(int n, int na, int nb, int positivity, int spin, int sz,
 void v2o_destroy(v2o_problem *p) {
     if (!p) return;
     free(p->bas_ab); free(p->ibas_ab); free(p->bas_aa); free(p->ibas_aa);
-    free(p->bas_aaa); free(p->bas_aab); free(p->bas_aba);
+    free(p->bas_aaa); free(p->bas_aab); free(p->bas_aba); free(p->ibas_aaa); free(p->ibas_aab);
     free(p);
 }
 
@@ -212,10 +239,10 @@ void v2o_tables(const v2o_problem *p, int *bas_ab, int *ibas_ab, int *bas_aa, in
 }
 /* block offsets in the order d2ab d2aa d2bb d200 d1a d1b q1a q1b q2ab q2aa q2bb g2ab g2ba g2aa */
 void v2o_offsets(const v2o_problem *p, long *o) {
-    long v[22] = {p->d2ab, p->d2aa, p->d2bb, p->d200, p->d1a, p->d1b, p->q1a,
+    long v[26] = {p->d2ab, p->d2aa, p->d2bb, p->d200, p->d1a, p->d1b, p->q1a,
                   p->q1b,  p->q2ab, p->q2aa, p->q2bb, p->g2ab, p->g2ba, p->g2aa,
                   p->t2aaa, p->t2bbb, p->t2aab, p->t2bba,
-                  p->t1aaa, p->t1bbb, p->t1aab, p->t1bba};
+                  p->t1aaa, p->t1bbb, p->t1aab, p->t1bba, p->d3aaa, p->d3bbb, p->d3aab, p->d3bba};
     memcpy(o, v, sizeof(v));
 }
 
@@ -692,6 +719,140 @@ static void t1_visit(const v2o_problem *p, long off, int mode, const double *u, 
     }
 }
 
+/* ------------------------------------------------------------- D3 ---- */
+/* CONSTRAIN_D3 rows of d3.cc:45-406 (D3_constraints_Au, C1), each a plain
+ * list of terms summed left to right (the first one a D2 element times an
+ * electron count), and their scatter in the same order (d3.cc:408-766):
+ *  with CONSTRAIN_SZ (d3.cc:49-212)
+ *    (na-2) D2aa(ij,kl) - sum_p s D3aaa(ijp,klp)      p not in {i,j,k,l}
+ *    (nb-2) D2bb(ij,kl) - sum_p s D3bbb(ijp,klp)
+ *    nb D2aa(ij,kl)     - sum_p D3aab(ij p, kl p)
+ *    na D2bb(ij,kl)     - sum_p D3bba(ij p, kl p)
+ *    (na-1) D2ab(ij,kl) - sum_p s D3aab(ip j, kp l)   p != i, k
+ *    (nb-1) D2ab(ij,kl) - sum_p s D3bba(jp i, lp k)   p != j, l
+ *  without it (d3.cc:213-330): (na+nb-2) D2 - the D3 terms of both spins;
+ *  singlets with CONSTRAIN_SPIN (d3.cc:332-404): D3aab - D3bba, and D3aaa
+ *  (D3bbb) minus a third of nine D3aab (D3bba) elements.
+ * s: the parity that sorts (i, j, p) (resp. (p, i)) into triplet order. */
+typedef struct {
+    const v2o_problem *p;
+    int mode;
+    const double *u;
+    double *A;
+    long row;
+    int nt;
+    t2_term t[64];
+} d3_row;
+
+static void d3_add(d3_row *r, long col, double coef) {
+    r->t[r->nt].col = col;
+    r->t[r->nt].coef = coef;
+    r->nt++;
+}
+
+static void d3_emit(d3_row *r) {
+    if (r->mode == T2_AU) {
+        double dum = 0.0;
+        for (int e = 0; e < r->nt; e++) dum += r->t[e].coef * r->u[r->t[e].col];
+        r->A[r->row] = dum;
+    } else {
+        const double dum = r->u[r->row];
+        for (int e = 0; e < r->nt; e++) r->A[r->t[e].col] += r->t[e].coef * dum;
+    }
+    r->row++;
+    r->nt = 0;
+}
+
+#define D3_AAA(a, b, c) (p->ibas_aaa[((long)(a) * p->n + (b)) * p->n + (c)])
+#define D3_AAB(a, b, c) (p->ibas_aab[((long)(a) * p->n + (b)) * p->n + (c)])
+
+static void d3_visit(const v2o_problem *p, long off, int mode, const double *u, double *A) {
+    const int n = p->n, gaa = p->gaa, gab = p->gab;
+    const long t3 = p->trip_aaa, ta = p->trip_aab;
+    const double na = p->na, nb = p->nb;
+    d3_row r;
+    r.p = p; r.mode = mode; r.u = u; r.A = A; r.row = off; r.nt = 0;
+    /* aa rows against D3aaa (and D3aab) for one spin */
+    for (int fam = 0; fam < (p->sz ? 4 : 2); fam++) {
+        const int beta = fam % 2;
+        const long d2 = beta ? p->d2bb : p->d2aa;
+        const long d3s = beta ? p->d3bbb : p->d3aaa, d3m = beta ? p->d3bba : p->d3aab;
+        for (int ij = 0; ij < gaa; ij++) {
+            const int i = p->bas_aa[2 * ij], j = p->bas_aa[2 * ij + 1];
+            for (int kl = 0; kl < gaa; kl++) {
+                const int k = p->bas_aa[2 * kl], l = p->bas_aa[2 * kl + 1];
+                if (p->sz && fam < 2) {          /* same-spin triples */
+                    d3_add(&r, d2 + (long)ij * gaa + kl, (beta ? nb : na) - 2.0);
+                    for (int q = 0; q < n; q++) {
+                        if (i == q || j == q || k == q || l == q) continue;
+                        const double sg = ((i < q && q < j) ? -1.0 : 1.0) * ((k < q && q < l) ? -1.0 : 1.0);
+                        d3_add(&r, d3s + (long)D3_AAA(i, j, q) * t3 + D3_AAA(k, l, q), -sg);
+                    }
+                } else if (p->sz) {              /* mixed triples */
+                    d3_add(&r, d2 + (long)ij * gaa + kl, beta ? na : nb);
+                    for (int q = 0; q < n; q++)
+                        d3_add(&r, d3m + (long)D3_AAB(i, j, q) * ta + D3_AAB(k, l, q), -1.0);
+                } else {                         /* both */
+                    d3_add(&r, d2 + (long)ij * gaa + kl, na + nb - 2.0);
+                    for (int q = 0; q < n; q++) {
+                        d3_add(&r, d3m + (long)D3_AAB(i, j, q) * ta + D3_AAB(k, l, q), -1.0);
+                        if (i == q || j == q || k == q || l == q) continue;
+                        const double sg = ((i < q && q < j) ? -1.0 : 1.0) * ((k < q && q < l) ? -1.0 : 1.0);
+                        d3_add(&r, d3s + (long)D3_AAA(i, j, q) * t3 + D3_AAA(k, l, q), -sg);
+                    }
+                }
+                d3_emit(&r);
+            }
+        }
+    }
+    /* ab rows */
+    for (int fam = 0; fam < (p->sz ? 2 : 1); fam++) {
+        for (int ij = 0; ij < gab; ij++) {
+            const int i = p->bas_ab[2 * ij], j = p->bas_ab[2 * ij + 1];
+            for (int kl = 0; kl < gab; kl++) {
+                const int k = p->bas_ab[2 * kl], l = p->bas_ab[2 * kl + 1];
+                const double c0 = !p->sz ? na + nb - 2.0 : (fam ? nb - 1.0 : na - 1.0);
+                d3_add(&r, p->d2ab + (long)ij * gab + kl, c0);
+                for (int q = 0; q < n; q++) {
+                    if ((!p->sz || fam == 0) && i != q && k != q) {
+                        const double sg = (q < i ? -1.0 : 1.0) * (q < k ? -1.0 : 1.0);
+                        d3_add(&r, p->d3aab + (long)D3_AAB(i, q, j) * ta + D3_AAB(k, q, l), -sg);
+                    }
+                    if ((!p->sz || fam == 1) && j != q && l != q) {
+                        const double sg = (q < j ? -1.0 : 1.0) * (q < l ? -1.0 : 1.0);
+                        d3_add(&r, p->d3bba + (long)D3_AAB(j, q, i) * ta + D3_AAB(l, q, k), -sg);
+                    }
+                }
+                d3_emit(&r);
+            }
+        }
+    }
+    if (p->spin && p->na == p->nb) {
+        for (long e = 0; e < ta * ta; e++) {
+            d3_add(&r, p->d3aab + e, 1.0);
+            d3_add(&r, p->d3bba + e, -1.0);
+            d3_emit(&r);
+        }
+        const double third = 1.0 / 3.0;
+        for (int beta = 0; beta < 2; beta++) {
+            const long d3s = beta ? p->d3bbb : p->d3aaa, d3m = beta ? p->d3bba : p->d3aab;
+            for (long pqr = 0; pqr < t3; pqr++) {
+                const int a = p->bas_aaa[3 * pqr], b = p->bas_aaa[3 * pqr + 1], c = p->bas_aaa[3 * pqr + 2];
+                const long rows3[3] = {D3_AAB(a, b, c), D3_AAB(a, c, b), D3_AAB(b, c, a)};
+                for (long stv = 0; stv < t3; stv++) {
+                    const int s_ = p->bas_aaa[3 * stv], t_ = p->bas_aaa[3 * stv + 1], v_ = p->bas_aaa[3 * stv + 2];
+                    const long cols3[3] = {D3_AAB(s_, t_, v_), D3_AAB(s_, v_, t_), D3_AAB(t_, v_, s_)};
+                    d3_add(&r, d3s + pqr * t3 + stv, 1.0);
+                    for (int x = 0; x < 3; x++)
+                        for (int y = 0; y < 3; y++)
+                            d3_add(&r, d3m + rows3[x] * ta + cols3[y], ((x + y) % 2) ? third : -third);
+                    d3_emit(&r);
+                }
+            }
+        }
+    }
+}
+
 /* ------------------------------------------------------------- A.x ---- */
 /* v2rdm_solver.cc:2995-3050 (bpsdp_Au) -> d2.cc:314-594, spin.cc:276-508,
  * q2.cc:170-318, g2.cc:245-442 */
@@ -1036,7 +1197,12 @@ void v2o_Au(const v2o_problem *p, const double *u, double *A) {
         t1_visit(p, off, T2_AU, u, A, NULL);
         off += 2L * p->trip_aab * p->trip_aab + 2L * p->trip_aaa * p->trip_aaa;
     }
-    if (p->t2) t2_visit(p, off, T2_AU, u, A, NULL);   /* v2rdm_solver.cc:3019-3022 */
+    if (p->t2) {   /* v2rdm_solver.cc:3019-3022 */
+        t2_visit(p, off, T2_AU, u, A, NULL);
+        const long w = (long)p->trip_aab + p->trip_aba;
+        off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
+    }
+    if (p->d3) d3_visit(p, off, T2_AU, u, A);   /* v2rdm_solver.cc:3036-3038 */
 }
 
 /* ----------------------------------------------------------- A^T.y ---- */
@@ -1372,5 +1538,10 @@ void v2o_ATu(const v2o_problem *p, const double *u, double *A) {
         t1_visit(p, off, T2_ATU, u, A, NULL);
         off += 2L * p->trip_aab * p->trip_aab + 2L * p->trip_aaa * p->trip_aaa;
     }
-    if (p->t2) t2_visit(p, off, T2_ATU, u, A, NULL);   /* v2rdm_solver.cc:3077-3080 */
+    if (p->t2) {   /* v2rdm_solver.cc:3077-3080 */
+        t2_visit(p, off, T2_ATU, u, A, NULL);
+        const long w = (long)p->trip_aab + p->trip_aba;
+        off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
+    }
+    if (p->d3) d3_visit(p, off, T2_ATU, u, A);   /* v2rdm_solver.cc:3094-3096 */
 }

@@ -31,6 +31,8 @@ CASES = [
     ("ext3_dqgt2_doublet", 3, 2, 1, "DQGT2", True, True, None),
     ("hub4_dqgt1", 4, 2, 2, "DQGT1", True, True, (1.0, 4.0)),
     ("ext4_dqgt1t2_doublet", 4, 2, 1, "DQGT1T2", True, True, None),
+    ("hub4_dqg_d3", 4, 2, 2, "DQG+D3", True, True, (1.0, 4.0)),
+    ("ext3_d_d3_nosz_doublet", 3, 2, 1, "D+D3", True, False, None),
 ]
 
 

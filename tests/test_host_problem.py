@@ -66,7 +66,8 @@ def test_header_symbols_exported():
 
 @pytest.mark.parametrize("name", ["hub2_dqg", "hub4_dqg", "hub4_d_nospin", "ext3_dqg_triplet",
                                   "ext4_dq_nosz", "ext4_dg_doublet", "ext1_dqg", "hub3_dqgt2",
-                                  "ext3_dqgt2_doublet", "hub4_dqgt1", "ext4_dqgt1t2_doublet"])
+                                  "ext3_dqgt2_doublet", "hub4_dqgt1", "ext4_dqgt1t2_doublet",
+                                  "hub4_dqg_d3", "ext3_d_d3_nosz_doublet"])
 def test_host_problem_matches_golden(golden, name):
     case = golden[name]
     kw = case_kwargs(case)
@@ -90,7 +91,8 @@ def test_host_problem_matches_golden(golden, name):
 def test_layout_helper_matches_library():
     for args in [(4, 2, 2, "DQG", True), (3, 2, 1, "DQG", True), (4, 2, 2, "D", False),
                  (4, 2, 1, "DG", True), (3, 2, 1, "DQGT2", True), (4, 2, 2, "DQGT1", True),
-                 (4, 2, 1, "DQGT1T2", True), (3, 1, 1, "DQGT", False)]:
+                 (4, 2, 1, "DQGT1T2", True), (3, 1, 1, "DQGT", False), (4, 2, 2, "DQG+D3", True),
+                 (3, 2, 1, "D+D3", False)]:
         p = hb.V2RDMProblem(args[0], args[1], args[2], args[3], args[4])
         assert [d for _, d in hb.block_layout(*args)] == list(p.dims)
 
@@ -125,9 +127,10 @@ def test_config5_sizes_match_the_oracle():
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libv2rdm_ref.so")),
                     reason="oracle/_ref not built")
-def test_triplet_families_bit_exact_against_reference_grid():
-    """T1 and T2 together (DQGT1T2): sizes, b, c, both guesses and the
-    packed A / A^T, against hilbert's compiled code, n = 1..3."""
+@pytest.mark.parametrize("pos", ["DQGT1T2", "DQG+D3"])
+def test_triplet_families_bit_exact_against_reference_grid(pos):
+    """T1 and T2 together (DQGT1T2), and D3 (CONSTRAIN_D3): sizes, b, c, both
+    guesses and the packed A / A^T, against hilbert's compiled code, n = 1..3."""
     import itertools
     from oracle.maps import RefProblem
     rng = np.random.default_rng(31)
@@ -135,9 +138,9 @@ def test_triplet_families_bit_exact_against_reference_grid():
         if na > n or nb > n:
             continue
         h, g = rng.standard_normal((n, n)), rng.standard_normal((n,) * 4)
-        r = RefProblem(n, na, nb, "DQGT1T2", spin, sz, h=h, g=g)
-        rh = RefProblem(n, na, nb, "DQGT1T2", spin, sz, h=h, g=g, guess="hf")
-        p = hb.V2RDMProblem(n, na, nb, "DQGT1T2", bool(spin), bool(sz))
+        r = RefProblem(n, na, nb, pos, spin, sz, h=h, g=g)
+        rh = RefProblem(n, na, nb, pos, spin, sz, h=h, g=g, guess="hf")
+        p = hb.V2RDMProblem(n, na, nb, pos, bool(spin), bool(sz))
         assert (p.n_primal, p.n_dual) == (r.n_primal, r.n_dual) and list(p.dims) == list(r.dims)
         assert np.array_equal(p.b(), r.b) and np.array_equal(p.c_external(h, g), r.c)
         assert np.array_equal(p.guess("RANDOM"), r.x0) and np.array_equal(p.guess("HF"), rh.x0)

@@ -21,7 +21,7 @@ def test_golden_cases_present(golden):
 @pytest.mark.parametrize("name", ["hub2_dqg", "hub4_dqg", "hub4_d_nospin", "ext3_dqg_triplet",
                                   "ext4_dq_nosz", "ext4_dg_doublet", "ext5_dqg", "ext1_dqg",
                                   "hub3_dqgt2", "ext3_dqgt2_doublet", "hub4_dqgt1",
-                                  "ext4_dqgt1t2_doublet"])
+                                  "ext4_dqgt1t2_doublet", "hub4_dqg_d3", "ext3_d_d3_nosz_doublet"])
 def test_oracle_matches_golden(golden, name):
     case = golden[name]
     kw = case_kwargs(case)
@@ -47,6 +47,9 @@ def test_sizes_match_reference_counts():
     o = OracleProblem(20, 10, 10, "DQG", True, True, h=np.zeros((20, 20)), g=np.zeros((20,) * 4))
     assert (o.n_primal, o.n_dual) == (1586000, 1856304)
     assert sorted(set(o.dims)) == [20, 190, 400, 800]
+    # tests/v2rdm3 (H3 doublet, POSITIVITY D + CONSTRAIN_D3) prints 623 primal
+    # variables (output.ref:363); its C1 formula gives the same
+    assert OracleProblem(3, 2, 1, "D+D3", True, True, h=np.zeros((3, 3)), g=np.zeros((3,) * 4)).n_primal == 623
     # the half-filled Hubbard rings of the 64-instance batch, L = 6 .. 14
     for L, sizes, big in ((6, (12708, 14863), 72), (14, (379652, 443895), 392)):
         o = OracleProblem(L, L // 2, L // 2, "DQG", True, True, hubbard=(1.0, 4.0))
@@ -85,7 +88,7 @@ def test_oracle_bit_exact_against_reference_grid():
     rng = np.random.default_rng(3)
     for n, na, nb, pos, spin, sz in itertools.product([1, 2, 3, 4], [0, 1, 2], [0, 1, 2],
                                                       ["D", "DQ", "DG", "DQG", "DQGT2", "DQGT1",
-                                                       "DQGT1T2"], [0, 1], [0, 1]):
+                                                       "DQGT1T2", "DQG+D3", "D+D3"], [0, 1], [0, 1]):
         if na > n or nb > n:
             continue
         kw = dict(h=rng.standard_normal((n, n)), g=rng.standard_normal((n,) * 4))
@@ -101,7 +104,7 @@ def test_oracle_bit_exact_against_reference_grid():
 
 
 @pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
-@pytest.mark.parametrize("pos", ["DQGT2", "DQGT1", "DQGT1T2"])
+@pytest.mark.parametrize("pos", ["DQGT2", "DQGT1", "DQGT1T2", "DQGT1T2+D3"])
 def test_oracle_triplet_guesses_bit_exact_against_reference_grid(pos):
     """The T1 / T2 parts of the HF guess (t1.cc:45-419, t2.cc:1845-2452) and
     the random guess with those blocks present, against hilbert's compiled code."""
