@@ -130,3 +130,27 @@ def test_t2_blocks_and_rows_follow_the_triplet_counts():
     assert o.n_primal - d.n_primal == 2 * (ta + tb) ** 2 + 2 * ta * ta
     assert o.n_dual - d.n_dual == o.n_primal - d.n_primal
     assert not np.any(o.b[d.n_dual:])
+
+
+@pytest.mark.parametrize("n", [3, 4])
+def test_d3_is_exact_for_three_electrons(n):
+    """Known answer (the reference's tests/v2rdm3 deck compares D + D3 with
+    FCI for H3): with the 3-RDM positive and contracting to the 2-RDM, three
+    electrons reach the full-CI energy of their Ms sector, while D alone lies
+    far below it."""
+    from oracle.bpsdp import SDPOptions, run_v2rdm
+    from oracle.fci import fci_energy
+    rng = np.random.default_rng(7)
+    h = rng.standard_normal((n, n))
+    h = 0.5 * (h + h.T)
+    B = rng.standard_normal((6, n, n))
+    B = 0.5 * (B + B.transpose(0, 2, 1))
+    g = np.einsum("Qij,Qkl->ijkl", B, B)
+    e_fci = fci_energy(h, g, 2, 1)
+    o = OracleProblem(n, 2, 1, "D+D3", False, True, h=h, g=g)
+    x, so = run_v2rdm(o, o.guess("random"), SDPOptions(1e-8, 1e-8, 1e-10, 10000, 200000), 500)
+    assert so.is_converged()
+    assert abs(float(o.c @ x) - e_fci) <= 1e-6
+    o = OracleProblem(n, 2, 1, "D", False, True, h=h, g=g)
+    x, so = run_v2rdm(o, o.guess("random"), SDPOptions(1e-8, 1e-8, 1e-10, 10000, 200000), 500)
+    assert float(o.c @ x) < e_fci - 1.0
