@@ -32,7 +32,10 @@ Problem make_problem(const ProblemSpec &spec) {
     p.g2 = spec.positivity == POS_DG || spec.positivity >= POS_DQG;
     p.t1 = spec.positivity == POS_DQGT1 || spec.positivity == POS_DQGT1T2;
     p.t2 = spec.positivity == POS_DQGT2 || spec.positivity == POS_DQGT1T2;
-    p.d3 = spec.constrain_d3;
+    p.q3 = spec.constrain_q3;
+    p.d3 = spec.constrain_d3 || p.q3;
+    if (p.q3 && !(p.q2 && p.g2))
+        throw std::invalid_argument("CONSTRAIN_Q3 needs the Q2 and G2 conditions (POSITIVITY DQG or a T option)");
     p.mult = spec.hubbard_multiplicity ? 2 * (spec.nalpha - spec.nbeta) + 1
                                        : (spec.nalpha - spec.nbeta) + 1;
 
@@ -123,6 +126,12 @@ Problem make_problem(const ProblemSpec &spec) {
         add_block(p.t2aab, p.trip_aab);
         add_block(p.t2bba, p.trip_aab);
     }
+    if (p.q3) {   // v2rdm_solver.cc:3970-3998
+        add_block(p.q3aaa, p.trip_aaa);
+        add_block(p.q3bbb, p.trip_aaa);
+        add_block(p.q3aab, p.trip_aab);
+        add_block(p.q3bba, p.trip_aab);
+    }
     if (p.d3) {   // v2rdm_solver.cc:4000-4029
         add_block(p.d3aaa, p.trip_aaa);
         add_block(p.d3bbb, p.trip_aaa);
@@ -145,6 +154,7 @@ Problem make_problem(const ProblemSpec &spec) {
         const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
         d += 2 * aab * aab + 2 * big * big;
     }
+    if (p.q3) d += 2 * (int64_t)p.trip_aaa * p.trip_aaa + 2 * (int64_t)p.trip_aab * p.trip_aab;
     if (p.d3) {   // v2rdm_solver.cc:3624-3660
         d += spec.constrain_sz ? 4 * gaa2 + 2 * gab2 : 2 * gaa2 + gab2;
         if (spec.constrain_spin && singlet)
@@ -277,8 +287,11 @@ constexpr int kT2AaaAbb = 3;
 // nterms) receives them in the reference's order; T1_constraints_ATu
 // (t1.cc:795-1200) scatters the same terms in the same order, and the guess
 // (t1.cc:45-419) sums them from zero.
+// The Q3 rows (q3.cc:45-423, scatter :425-803) carry the same terms with
+// -Q3 - D3 in front: t1_rows(p, off, f, true) hands f the Q3 element as the
+// leading column (its D3 twin sits at the same place in the D3 block).
 template <class F>
-void t1_rows(const Problem &p, int64_t off, F &&f) {
+void t1_rows(const Problem &p, int64_t off, F &&f, bool q3 = false) {
     const int N = p.n, gab = p.gab, gaa = p.gaa;
     int64_t cols[12];
     double coef[12];
@@ -294,7 +307,8 @@ void t1_rows(const Problem &p, int64_t off, F &&f) {
         const bool aab = sub < 2, beta = (sub % 2) == 1;
         const std::vector<int> &tb = aab ? p.bas_aab : p.bas_aaa;
         const int nr = aab ? p.trip_aab : p.trip_aaa;
-        const int64_t t1 = sub == 0 ? p.t1aab : sub == 1 ? p.t1bba : sub == 2 ? p.t1aaa : p.t1bbb;
+        const int64_t t1 = q3 ? (sub == 0 ? p.q3aab : sub == 1 ? p.q3bba : sub == 2 ? p.q3aaa : p.q3bbb)
+                              : (sub == 0 ? p.t1aab : sub == 1 ? p.t1bba : sub == 2 ? p.t1aaa : p.t1bbb);
         const int64_t q2 = beta ? p.q2bb : p.q2aa;
         for (int r = 0; r < nr; r++) {
             const int i = tb[3 * r], j = tb[3 * r + 1], k = tb[3 * r + 2];
@@ -339,6 +353,14 @@ void t1_rows(const Problem &p, int64_t off, F &&f) {
         }
         off += (int64_t)nr * nr;
     }
+}
+
+// the D3 element at the place of a Q3 element (blocks of equal shape)
+int64_t d3_twin(const Problem &p, int64_t q3col) {
+    if (q3col >= p.q3bba) return p.d3bba + (q3col - p.q3bba);
+    if (q3col >= p.q3aab) return p.d3aab + (q3col - p.q3aab);
+    if (q3col >= p.q3bbb) return p.d3bbb + (q3col - p.q3bbb);
+    return p.d3aaa + (q3col - p.q3aaa);
 }
 
 // ------------------------------------------------------------------ D3
@@ -994,6 +1016,14 @@ void visit_A(const Problem &p, S &s) {
         const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
         off += 2 * aab * aab + 2 * big * big;
     }
+    if (p.q3) {   // q3.cc:45-423
+        t1_rows(p, off, [&](int64_t row, int64_t q3c, int, const int64_t *cols, const double *coef, int nt) {
+            s.t(row, q3c, -1.0);
+            s.t(row, d3_twin(p, q3c), -1.0);
+            for (int q = 0; q < nt; q++) s.t(row, cols[q], coef[q]);
+        }, true);
+        off += 2 * (int64_t)p.trip_aab * p.trip_aab + 2 * (int64_t)p.trip_aaa * p.trip_aaa;
+    }
     if (p.d3) {   // d3.cc:45-406
         d3_rows(p, off, [&](int64_t row, const int64_t *cols, const double *coef, int nt) {
             for (int q = 0; q < nt; q++) s.t(row, cols[q], coef[q]);
@@ -1301,6 +1331,14 @@ void visit_AT(const Problem &p, S &s) {
         });
         const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
         off += 2 * aab * aab + 2 * big * big;
+    }
+    if (p.q3) {   // q3.cc:425-803 scatters in the same order as the A rows
+        t1_rows(p, off, [&](int64_t row, int64_t q3c, int, const int64_t *cols, const double *coef, int nt) {
+            s.t(q3c, row, -1.0);
+            s.t(d3_twin(p, q3c), row, -1.0);
+            for (int q = 0; q < nt; q++) s.t(cols[q], row, coef[q]);
+        }, true);
+        off += 2 * (int64_t)p.trip_aab * p.trip_aab + 2 * (int64_t)p.trip_aaa * p.trip_aaa;
     }
     if (p.d3) {   // d3.cc:408-766 scatters in the same order as the A rows
         d3_rows(p, off, [&](int64_t row, const int64_t *cols, const double *coef, int nt) {

@@ -28,6 +28,7 @@ DEFAULTS = {
     "CONSTRAIN_SPIN": True,         # :306
     "CONSTRAIN_SZ": True,           # :309
     "CONSTRAIN_D3": False,          # :226
+    "CONSTRAIN_Q3": False,          # :235
     "TPDM_GUESS": "RANDOM",         # :205
     "SDP_SOLVER": "BPSDP",          # :246
     "HUBBARD_HAMILTONIAN": False,   # :249
@@ -88,11 +89,12 @@ class V2RDMProblem:
         lib = _capi.load()
         self._lib = lib
         h = ctypes.c_void_p()
-        pos, _, extra = positivity.upper().partition("+")
-        if pos not in _capi.POSITIVITY or extra not in ("", "D3"):
+        pos, *extras = positivity.upper().split("+")
+        if pos not in _capi.POSITIVITY or not set(extras) <= {"D3", "Q3"}:
             raise ValueError(f"POSITIVITY {positivity} is not on the device path "
-                             f"(supported: {sorted(_capi.POSITIVITY)}, each optionally +D3)")
-        code = _capi.POSITIVITY[pos] | (_capi.V2B_CONSTRAIN_D3 if extra == "D3" else 0)
+                             f"(supported: {sorted(_capi.POSITIVITY)}, each optionally +D3 / +Q3)")
+        code = (_capi.POSITIVITY[pos] | (_capi.V2B_CONSTRAIN_D3 if "D3" in extras else 0)
+                | (_capi.V2B_CONSTRAIN_Q3 if "Q3" in extras else 0))
         check(lib.v2b_problem_create(int(nmo), int(nalpha), int(nbeta), code,
                                      int(bool(constrain_spin)), int(bool(constrain_sz)),
                                      int(bool(hubbard_multiplicity)), ctypes.byref(h)))
@@ -413,7 +415,8 @@ class v2RDMHelper:
         else:
             raise TypeError("v2RDMHelper(nalpha, nbeta, nmo, h, g, options) or v2RDMHelper(ref_wfn, options)")
         o = self.options
-        pos = o.get("POSITIVITY") + ("+D3" if o.get("CONSTRAIN_D3") else "")
+        pos = (o.get("POSITIVITY") + ("+D3" if o.get("CONSTRAIN_D3") else "")
+               + ("+Q3" if o.get("CONSTRAIN_Q3") else ""))
         self.problem = V2RDMProblem(nmo, nalpha, nbeta, pos, o.get("CONSTRAIN_SPIN"),
                                     o.get("CONSTRAIN_SZ"), hubbard_multiplicity=self._hubbard)
         p = self.problem
@@ -451,7 +454,7 @@ def block_layout(nmo, nalpha, nbeta, positivity="DQG", constrain_spin=True):
     """[(name, dim)] in the primal order of set_primal_offsets (v2rdm_solver.cc:3729-4079)."""
     n = int(nmo)
     gab, gaa = n * n, n * (n - 1) // 2
-    pos, _, extra = positivity.upper().partition("+")
+    pos, *extras = positivity.upper().split("+")
     blocks = [("d2ab", gab), ("d2aa", gaa), ("d2bb", gaa)]
     if constrain_spin:
         blocks.append(("d200", gab if nalpha == nbeta else 2 * gab))
@@ -466,7 +469,9 @@ def block_layout(nmo, nalpha, nbeta, positivity="DQG", constrain_spin=True):
         blocks += [("t1aaa", aaa), ("t1bbb", aaa), ("t1aab", aab), ("t1bba", aab)]
     if pos in ("DQGT2", "DQGT1T2", "DQGT"):
         blocks += [("t2aaa", aab + aba), ("t2bbb", aab + aba), ("t2aab", aab), ("t2bba", aab)]
-    if extra == "D3":
+    if "Q3" in extras:
+        blocks += [("q3aaa", aaa), ("q3bbb", aaa), ("q3aab", aab), ("q3bba", aab)]
+    if "D3" in extras or "Q3" in extras:
         blocks += [("d3aaa", aaa), ("d3bbb", aaa), ("d3aab", aab), ("d3bba", aab)]
     return blocks
 

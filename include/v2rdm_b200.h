@@ -43,8 +43,10 @@ extern "C" {
 #define V2B_POSITIVITY_DQGT2 4   /* DQG + T2 (t2.cc:1236-1843, 3376-3966) */
 #define V2B_POSITIVITY_DQGT1 5   /* DQG + T1 (t1.cc:419-795, 795-1200) */
 #define V2B_POSITIVITY_DQGT1T2 6 /* DQG + T1 + T2 ("DQGT1T2" and "DQGT", v2rdm_solver.cc:4110-4119) */
-/* OR-ed into a POSITIVITY value: CONSTRAIN_D3 (d3.cc:45-406, 408-766) */
+/* OR-ed into a POSITIVITY value: CONSTRAIN_D3 (d3.cc:45-406, 408-766) and
+ * CONSTRAIN_Q3 (q3.cc:45-423, 425-803; implies D3, needs Q2 and G2) */
 #define V2B_CONSTRAIN_D3 16
+#define V2B_CONSTRAIN_Q3 32
 
 /* libsdp::SDPOptions as hilbert fills it (src/v2rdm_casscf/v2rdm_solver.cc:426-431) */
 typedef struct {

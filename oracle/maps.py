@@ -17,7 +17,8 @@ REF_SO = os.path.join(HERE, "_ref", "libv2rdm_ref.so")
 POSITIVITY = {"D": 0, "DQ": 1, "DG": 2, "DQG": 3, "DQGT2": 4, "DQGT1": 5, "DQGT1T2": 6}
 BLOCK_NAMES = ("d2ab", "d2aa", "d2bb", "d200", "d1a", "d1b", "q1a", "q1b",
                "q2ab", "q2aa", "q2bb", "g2ab", "g2ba", "g2aa", "t2aaa", "t2bbb", "t2aab", "t2bba",
-               "t1aaa", "t1bbb", "t1aab", "t1bba", "d3aaa", "d3bbb", "d3aab", "d3bba")
+               "t1aaa", "t1bbb", "t1aab", "t1bba", "d3aaa", "d3bbb", "d3aab", "d3bba",
+               "q3aaa", "q3bbb", "q3aab", "q3bba")
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -109,10 +110,10 @@ class OracleProblem:
         self.n, self.na, self.nb = n, na, nb
         self.positivity = positivity
         self.hubbard = hubbard
-        base, _, extra = positivity.partition("+")
-        if extra not in ("", "D3"):
-            raise ValueError(f"unknown constraint suffix {extra!r}")
-        code = POSITIVITY[base] | (16 if extra == "D3" else 0)
+        base, *extras = positivity.split("+")
+        if not set(extras) <= {"D3", "Q3"}:
+            raise ValueError(f"unknown constraint suffix in {positivity!r}")
+        code = POSITIVITY[base] | (16 if "D3" in extras else 0) | (32 if "Q3" in extras else 0)
         p = lib.v2o_create(n, na, nb, code, int(constrain_spin),
                            int(constrain_sz), int(hubbard is not None))
         if not p:

@@ -9,7 +9,7 @@
  * restates (paths relative to the hilbert source tree).
  *
  * Supported constraint sets: POSITIVITY D / DQ / DG / DQG / DQGT1 / DQGT2 /
- * DQGT1T2, each optionally with CONSTRAIN_D3, with
+ * DQGT1T2, each optionally with CONSTRAIN_D3 and CONSTRAIN_Q3, with
  * CONSTRAIN_SPIN and CONSTRAIN_SZ on or off, singlet and non-singlet.
  */
 #include <math.h>
@@ -19,12 +19,13 @@
 typedef struct {
     int n;            /* active orbitals (amo_) */
     int na, nb;       /* alpha / beta electrons */
-    int q2, g2, t1, t2, d3, spin, sz;
+    int q2, g2, t1, t2, d3, q3, spin, sz;
     int mult;         /* 2S+1 as the reference stores it */
     int gab, gaa;
     int *bas_ab, *ibas_ab, *bas_aa, *ibas_aa;
     long d2ab, d2aa, d2bb, d200, d1a, d1b, q1a, q1b, q2ab, q2aa, q2bb, g2ab, g2ba, g2aa;
     long t1aaa, t1bbb, t1aab, t1bba, t2aaa, t2bbb, t2aab, t2bba, d3aaa, d3bbb, d3aab, d3bba;
+    long q3aaa, q3bbb, q3aab, q3bba;
     int trip_aaa, trip_aab, trip_aba;   /* triplets (i<j<k), (i<j, k) and (i, j, k) */
     int *bas_aaa, *bas_aab, *bas_aba;   /* 3 ints per triplet */
     int *ibas_aaa, *ibas_aab;           /* n^3: any order of an aaa set / of the aa pair */
@@ -69,6 +70,8 @@ static void build_tables(v2o_problem *p) {
 enum { T2_AU = 0, T2_ATU = 1, T2_GUESS = 2 };
 static void t1_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
                      double *x);
+static void t1_like_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
+                          double *x, int q3);
 static void t2_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
                      double *x);
 static void d3_visit(const v2o_problem *p, long off, int mode, const double *u, double *A);
@@ -120,6 +123,15 @@ static void set_offsets(v2o_problem *p) {
         p->t2aab = off; off += ta * ta; p->dims[nb++] = (int)ta;
         p->t2bba = off; off += ta * ta; p->dims[nb++] = (int)ta;
     }
+    /* v2rdm_solver.cc:3970-3998: Q3aaa, Q3bbb (dim aaa), Q3aab, Q3bba (dim aab) */
+    p->q3aaa = p->q3bbb = p->q3aab = p->q3bba = -1;
+    if (p->q3) {
+        long t3 = p->trip_aaa, ta = p->trip_aab;
+        p->q3aaa = off; off += t3 * t3; p->dims[nb++] = (int)t3;
+        p->q3bbb = off; off += t3 * t3; p->dims[nb++] = (int)t3;
+        p->q3aab = off; off += ta * ta; p->dims[nb++] = (int)ta;
+        p->q3bba = off; off += ta * ta; p->dims[nb++] = (int)ta;
+    }
     /* v2rdm_solver.cc:4000-4029: D3aaa, D3bbb (dim aaa), D3aab, D3bba (dim aab) */
     p->d3aaa = p->d3bbb = p->d3aab = p->d3bba = -1;
     if (p->d3) {
@@ -152,6 +164,10 @@ static void set_offsets(v2o_problem *p) {
     if (p->t2) {   /* v2rdm_solver.cc:3568-3580 */
         long w = (long)p->trip_aab + p->trip_aba, ta = p->trip_aab;
         d += 2 * w * w + 2 * ta * ta;
+    }
+    if (p->q3) {   /* v2rdm_solver.cc:3610-3623 */
+        long t3 = p->trip_aaa, ta = p->trip_aab;
+        d += 2 * t3 * t3 + 2 * ta * ta;
     }
     if (p->d3) {   /* v2rdm_solver.cc:3624-3660 */
         long t3 = p->trip_aaa, ta = p->trip_aab;
@@ -197,20 +213,26 @@ static void build_triplets(v2o_problem *p) {
 }
 
 /* positivity: 0 D, 1 DQ, 2 DG, 3 DQG, 4 DQGT2, 5 DQGT1, 6 DQGT1T2 (= DQGT)
- * (v2rdm_solver.cc:4081-4118), plus 16 for CONSTRAIN_D3 (:4120-4122).
+ * (v2rdm_solver.cc:4081-4118), plus 16 for CONSTRAIN_D3 (:4120-4122) and 32 for
+ * CONSTRAIN_Q3 (which implies D3, :4132-4135).
  * hubbard selects the multiplicity convention of
  * v2rdm_solver.cc:862-863 (Hubbard) versus :983-984 (external). */
 v2o_problem *v2o_create(int n, int na, int nb, int positivity, int spin, int sz, int hubbard) {
-    const int d3 = (positivity >> 4) & 1;
+    const int q3 = (positivity >> 5) & 1, d3 = ((positivity >> 4) & 1) | q3;
     positivity &= 15;
     if (n < 1 || na < 0 || nb < 0 || na > n || nb > n || positivity < 0 || positivity > 6) return NULL;
     v2o_problem *p = (v2o_problem *)calloc(1, sizeof(v2o_problem));
     p->n = n; p->na = na; p->nb = nb;
     p->d3 = d3;
+    p->q3 = q3;
     p->q2 = (positivity == 1 || positivity >= 3);
     p->g2 = (positivity >= 2);
     p->t1 = (positivity == 5 || positivity == 6);
     p->t2 = (positivity == 4 || positivity == 6);
+    if (p->q3 && !(p->q2 && p->g2)) {   /* the Q3 rows read Q2 and G2 elements */
+        free(p);
+        return NULL;
+    }
     p->spin = spin != 0; p->sz = sz != 0;
     p->mult = hubbard ? 2 * (na - nb) + 1 : (na - nb) + 1;
     build_tables(p);
@@ -239,10 +261,11 @@ void v2o_tables(const v2o_problem *p, int *bas_ab, int *ibas_ab, int *bas_aa, in
 }
 /* block offsets in the order d2ab d2aa d2bb d200 d1a d1b q1a q1b q2ab q2aa q2bb g2ab g2ba g2aa */
 void v2o_offsets(const v2o_problem *p, long *o) {
-    long v[26] = {p->d2ab, p->d2aa, p->d2bb, p->d200, p->d1a, p->d1b, p->q1a,
+    long v[30] = {p->d2ab, p->d2aa, p->d2bb, p->d200, p->d1a, p->d1b, p->q1a,
                   p->q1b,  p->q2ab, p->q2aa, p->q2bb, p->g2ab, p->g2ba, p->g2aa,
                   p->t2aaa, p->t2bbb, p->t2aab, p->t2bba,
-                  p->t1aaa, p->t1bbb, p->t1aab, p->t1bba, p->d3aaa, p->d3bbb, p->d3aab, p->d3bba};
+                  p->t1aaa, p->t1bbb, p->t1aab, p->t1bba, p->d3aaa, p->d3bbb, p->d3aab, p->d3bba,
+                  p->q3aaa, p->q3bbb, p->q3aab, p->q3bba};
     memcpy(o, v, sizeof(v));
 }
 
@@ -686,11 +709,15 @@ static int t1_terms(const v2o_problem *p, int sb, int i, int j, int k, int l, in
     return nt;
 }
 
-static void t1_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
-                     double *x) {
+/* T1 rows lead with -T1; the Q3 rows of q3.cc:45-423 (scatter :425-803)
+ * lead with -Q3 - D3 and continue with the same terms as T1. */
+static void t1_like_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
+                          double *x, int q3) {
     const long ta = p->trip_aab, t3 = p->trip_aaa;
     const long dual[4] = {off, off + ta * ta, off + 2 * ta * ta, off + 2 * ta * ta + t3 * t3};
-    const long prim[4] = {p->t1aab, p->t1bba, p->t1aaa, p->t1bbb};
+    const long prim[4] = {q3 ? p->q3aab : p->t1aab, q3 ? p->q3bba : p->t1bba,
+                          q3 ? p->q3aaa : p->t1aaa, q3 ? p->q3bbb : p->t1bbb};
+    const long prim2[4] = {p->d3aab, p->d3bba, p->d3aaa, p->d3bbb};
     for (int sb = 0; sb < 4; sb++) {
         const long nr = sb < 2 ? ta : t3;
         const int *tb = sb < 2 ? p->bas_aab : p->bas_aaa;
@@ -703,11 +730,13 @@ static void t1_visit(const v2o_problem *p, long off, int mode, const double *u, 
                 const int nt = t1_terms(p, sb, i, j, k, l, m, q, t);
                 if (mode == T2_AU) {
                     double dum = -u[prim[sb] + id];
+                    if (q3) dum -= u[prim2[sb] + id];
                     for (int e = 0; e < nt; e++) dum += t[e].coef * u[t[e].col];
                     A[dual[sb] + id] = dum;
                 } else if (mode == T2_ATU) {
                     const double dum = u[dual[sb] + id];
                     A[prim[sb] + id] -= dum;
+                    if (q3) A[prim2[sb] + id] -= dum;
                     for (int e = 0; e < nt; e++) A[t[e].col] += t[e].coef * dum;
                 } else {
                     double dum = 0.0;
@@ -717,6 +746,11 @@ static void t1_visit(const v2o_problem *p, long off, int mode, const double *u, 
             }
         }
     }
+}
+
+static void t1_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
+                     double *x) {
+    t1_like_visit(p, off, mode, u, A, x, 0);
 }
 
 /* ------------------------------------------------------------- D3 ---- */
@@ -1202,6 +1236,10 @@ void v2o_Au(const v2o_problem *p, const double *u, double *A) {
         const long w = (long)p->trip_aab + p->trip_aba;
         off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
     }
+    if (p->q3) {   /* v2rdm_solver.cc:3032-3034 */
+        t1_like_visit(p, off, T2_AU, u, A, NULL, 1);
+        off += 2L * p->trip_aab * p->trip_aab + 2L * p->trip_aaa * p->trip_aaa;
+    }
     if (p->d3) d3_visit(p, off, T2_AU, u, A);   /* v2rdm_solver.cc:3036-3038 */
 }
 
@@ -1542,6 +1580,10 @@ void v2o_ATu(const v2o_problem *p, const double *u, double *A) {
         t2_visit(p, off, T2_ATU, u, A, NULL);
         const long w = (long)p->trip_aab + p->trip_aba;
         off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
+    }
+    if (p->q3) {   /* v2rdm_solver.cc:3090-3092 */
+        t1_like_visit(p, off, T2_ATU, u, A, NULL, 1);
+        off += 2L * p->trip_aab * p->trip_aab + 2L * p->trip_aaa * p->trip_aaa;
     }
     if (p->d3) d3_visit(p, off, T2_ATU, u, A);   /* v2rdm_solver.cc:3094-3096 */
 }

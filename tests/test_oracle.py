@@ -21,7 +21,8 @@ def test_golden_cases_present(golden):
 @pytest.mark.parametrize("name", ["hub2_dqg", "hub4_dqg", "hub4_d_nospin", "ext3_dqg_triplet",
                                   "ext4_dq_nosz", "ext4_dg_doublet", "ext5_dqg", "ext1_dqg",
                                   "hub3_dqgt2", "ext3_dqgt2_doublet", "hub4_dqgt1",
-                                  "ext4_dqgt1t2_doublet", "hub4_dqg_d3", "ext3_d_d3_nosz_doublet"])
+                                  "ext4_dqgt1t2_doublet", "hub4_dqg_d3", "ext3_d_d3_nosz_doublet",
+                                  "ext3_dqg_q3_doublet"])
 def test_oracle_matches_golden(golden, name):
     case = golden[name]
     kw = case_kwargs(case)
@@ -88,7 +89,7 @@ def test_oracle_bit_exact_against_reference_grid():
     rng = np.random.default_rng(3)
     for n, na, nb, pos, spin, sz in itertools.product([1, 2, 3, 4], [0, 1, 2], [0, 1, 2],
                                                       ["D", "DQ", "DG", "DQG", "DQGT2", "DQGT1",
-                                                       "DQGT1T2", "DQG+D3", "D+D3"], [0, 1], [0, 1]):
+                                                       "DQGT1T2", "DQG+D3", "D+D3", "DQG+Q3"], [0, 1], [0, 1]):
         if na > n or nb > n:
             continue
         kw = dict(h=rng.standard_normal((n, n)), g=rng.standard_normal((n,) * 4))
@@ -104,7 +105,7 @@ def test_oracle_bit_exact_against_reference_grid():
 
 
 @pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
-@pytest.mark.parametrize("pos", ["DQGT2", "DQGT1", "DQGT1T2", "DQGT1T2+D3"])
+@pytest.mark.parametrize("pos", ["DQGT2", "DQGT1", "DQGT1T2", "DQGT1T2+D3", "DQGT2+Q3"])
 def test_oracle_triplet_guesses_bit_exact_against_reference_grid(pos):
     """The T1 / T2 parts of the HF guess (t1.cc:45-419, t2.cc:1845-2452) and
     the random guess with those blocks present, against hilbert's compiled code."""
@@ -154,3 +155,10 @@ def test_d3_is_exact_for_three_electrons(n):
     o = OracleProblem(n, 2, 1, "D", False, True, h=h, g=g)
     x, so = run_v2rdm(o, o.guess("random"), SDPOptions(1e-8, 1e-8, 1e-10, 10000, 200000), 500)
     assert float(o.c @ x) < e_fci - 1.0
+
+
+def test_q3_without_q2_and_g2_is_refused():
+    """The Q3 rows read Q2 and G2 elements: with POSITIVITY D they would read
+    blocks that do not exist, so the combination is refused."""
+    with pytest.raises(ValueError):
+        OracleProblem(3, 1, 1, "D+Q3", True, True, h=np.eye(3), g=np.zeros((3,) * 4))
