@@ -33,7 +33,8 @@ Problem make_problem(const ProblemSpec &spec) {
     p.t1 = spec.positivity == POS_DQGT1 || spec.positivity == POS_DQGT1T2;
     p.t2 = spec.positivity == POS_DQGT2 || spec.positivity == POS_DQGT1T2;
     p.q3 = spec.constrain_q3;
-    p.d3 = spec.constrain_d3 || p.q3;
+    p.e3 = spec.constrain_e3;
+    p.d3 = spec.constrain_d3 || p.q3 || p.e3;
     if (p.q3 && !(p.q2 && p.g2))
         throw std::invalid_argument("CONSTRAIN_Q3 needs the Q2 and G2 conditions (POSITIVITY DQG or a T option)");
     p.mult = spec.hubbard_multiplicity ? 2 * (spec.nalpha - spec.nbeta) + 1
@@ -126,6 +127,12 @@ Problem make_problem(const ProblemSpec &spec) {
         add_block(p.t2aab, p.trip_aab);
         add_block(p.t2bba, p.trip_aab);
     }
+    if (p.e3) {   // v2rdm_solver.cc:3909-3938
+        add_block(p.e3aaa, p.trip_aab + p.trip_aba);
+        add_block(p.e3bbb, p.trip_aab + p.trip_aba);
+        add_block(p.e3aab, p.trip_aab);
+        add_block(p.e3bba, p.trip_aab);
+    }
     if (p.q3) {   // v2rdm_solver.cc:3970-3998
         add_block(p.q3aaa, p.trip_aaa);
         add_block(p.q3bbb, p.trip_aaa);
@@ -151,6 +158,10 @@ Problem make_problem(const ProblemSpec &spec) {
     if (p.g2) d += 6 * gab2;
     if (p.t1) d += 2 * (int64_t)p.trip_aaa * p.trip_aaa + 2 * (int64_t)p.trip_aab * p.trip_aab;
     if (p.t2) {
+        const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
+        d += 2 * aab * aab + 2 * big * big;
+    }
+    if (p.e3) {
         const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
         d += 2 * aab * aab + 2 * big * big;
     }
@@ -460,6 +471,101 @@ void d3_rows(const Problem &p, int64_t off, F &&f) {
                 }
             }
         }
+    }
+}
+
+// ------------------------------------------------------------------ E3
+// CONSTRAIN_E3 rows (e3.cc:45-566, E3_constraints_Au, C1) in the T2 layout
+// (sub-blocks 0 aab, 1 bba, 2-5 aaa, 6-9 bbb as for T2): -E3(I, J), one D3
+// element whose third index is exchanged between row and column,
+// (i j n | l m k), with the sign that reorders it, and d_kn times a D2
+// element.  E3_constraints_ATu (e3.cc:570-1082) scatters the same terms in
+// the same order.  f(dual_row, e3_col, sub, cols, coefs, nterms).
+template <class F>
+void e3_rows(const Problem &p, int64_t off, F &&f) {
+    const int N = p.n, gab = p.gab, gaa = p.gaa, aab = p.trip_aab, aba = p.trip_aba;
+    const int64_t big = (int64_t)aab + aba, t3 = p.trip_aaa;
+    int64_t cols[4];
+    double coef[4];
+    int nt = 0;
+    auto add = [&](int64_t c, double v) {
+        cols[nt] = c;
+        coef[nt] = v;
+        nt++;
+    };
+    auto trip = [&](int idx, bool is_aab, int &i, int &j, int &k) {
+        if (is_aab) {
+            i = p.bas_aab[3 * idx];
+            j = p.bas_aab[3 * idx + 1];
+            k = p.bas_aab[3 * idx + 2];
+        } else {
+            i = idx / (N * N);
+            j = (idx / N) % N;
+            k = idx % N;
+        }
+    };
+    auto x3 = [&](int a, int b, int c) { return (int64_t)p.ibas_aab[((size_t)a * N + b) * N + c]; };
+    auto y3 = [&](int a, int b, int c) { return (int64_t)p.ibas_aaa[((size_t)a * N + b) * N + c]; };
+    auto mixed = [&](int64_t base, int a, int b, int c, int d, int e, int g) { return base + x3(a, b, c) * aab + x3(d, e, g); };
+    auto same = [&](int64_t base, int a, int b, int c, int d, int e, int g) { return base + y3(a, b, c) * t3 + y3(d, e, g); };
+    auto aa2 = [&](int64_t base, int a, int b, int c, int d) { return base + (int64_t)p.iaa(a, b) * gaa + p.iaa(c, d); };
+    auto ab2 = [&](int a, int b, int c, int d) { return p.d2ab + (int64_t)p.iab(a, b) * gab + p.iab(c, d); };
+    auto neg = [](bool flip) { return flip ? -1.0 : 1.0; };
+
+    for (int spin = 0; spin < 2; spin++) {   // E3aab (e3.cc:47-92), E3bba (:94-139)
+        const int64_t e3 = spin ? p.e3bba : p.e3aab;
+        for (int ijk = 0; ijk < aab; ijk++) {
+            int i, j, k;
+            trip(ijk, true, i, j, k);
+            for (int lmn = 0; lmn < aab; lmn++) {
+                int l, m, n;
+                trip(lmn, true, l, m, n);
+                nt = 0;
+                add(mixed(spin ? p.d3bba : p.d3aab, i, j, n, l, m, k), -1.0);
+                if (k == n) add(aa2(spin ? p.d2bb : p.d2aa, i, j, l, m), 1.0);
+                const int64_t e = (int64_t)ijk * aab + lmn;
+                f(off + e, e3 + e, spin, cols, coef, nt);
+            }
+        }
+        off += (int64_t)aab * aab;
+    }
+    for (int spin = 0; spin < 2; spin++) {   // E3aaa (e3.cc:142-355), E3bbb (:359-564)
+        const int64_t e3 = spin ? p.e3bbb : p.e3aaa;
+        for (int sb = 0; sb < 4; sb++) {
+            const bool rowaab = sb < 2, colaab = (sb % 2) == 0;
+            const int nr = rowaab ? aab : aba, nc = colaab ? aab : aba;
+            for (int ijk = 0; ijk < nr; ijk++) {
+                int i, j, k;
+                trip(ijk, rowaab, i, j, k);
+                for (int lmn = 0; lmn < nc; lmn++) {
+                    int l, m, n;
+                    trip(lmn, colaab, l, m, n);
+                    nt = 0;
+                    if (sb == 0) {
+                        if (i != n && j != n && l != k && m != k)
+                            add(same(spin ? p.d3bbb : p.d3aaa, i, j, n, l, m, k),
+                                -(neg(i < n && n < j) * neg(l < k && k < m)));
+                        if (k == n) add(aa2(spin ? p.d2bb : p.d2aa, i, j, l, m), 1.0);
+                    } else if (sb == 1) {
+                        if (i != j && l != k)
+                            add(mixed(spin ? p.d3bba : p.d3aab, i, j, n, l, k, m),
+                                spin ? neg(i > j) * neg(l > k) : neg(l > k));
+                    } else if (sb == 2) {
+                        if (i != n && l != m)
+                            add(mixed(spin ? p.d3bba : p.d3aab, i, n, j, l, m, k),
+                                spin ? neg(i > n) * neg(l > m) : neg(i > n));
+                    } else {
+                        if (j != n && m != k)
+                            add(mixed(spin ? p.d3aab : p.d3bba, j, n, i, m, k, l), -(neg(j > n) * neg(m > k)));
+                        if (k == n) add(spin ? ab2(j, i, m, l) : ab2(i, j, l, m), 1.0);
+                    }
+                    const int64_t I = rowaab ? ijk : aab + ijk, J = colaab ? lmn : aab + lmn;
+                    const int64_t e = I * big + J;
+                    f(off + e, e3 + e, 2 + 4 * spin + sb, cols, coef, nt);
+                }
+            }
+        }
+        off += big * big;
     }
 }
 
@@ -1016,6 +1122,14 @@ void visit_A(const Problem &p, S &s) {
         const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
         off += 2 * aab * aab + 2 * big * big;
     }
+    if (p.e3) {   // e3.cc:45-566
+        e3_rows(p, off, [&](int64_t row, int64_t e3c, int, const int64_t *cols, const double *coef, int nt) {
+            s.t(row, e3c, -1.0);
+            for (int q = 0; q < nt; q++) s.t(row, cols[q], coef[q]);
+        });
+        const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
+        off += 2 * aab * aab + 2 * big * big;
+    }
     if (p.q3) {   // q3.cc:45-423
         t1_rows(p, off, [&](int64_t row, int64_t q3c, int, const int64_t *cols, const double *coef, int nt) {
             s.t(row, q3c, -1.0);
@@ -1327,6 +1441,14 @@ void visit_AT(const Problem &p, S &s) {
     if (p.t2) {   // t2.cc:3376-3966 scatters in the same loop order as the A rows
         t2_rows(p, off, [&](int64_t row, int64_t t2c, int, const int64_t *cols, const double *coef, int nt) {
             s.t(t2c, row, -1.0);
+            for (int q = 0; q < nt; q++) s.t(cols[q], row, coef[q]);
+        });
+        const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
+        off += 2 * aab * aab + 2 * big * big;
+    }
+    if (p.e3) {   // e3.cc:570-1082 scatters in the same order as the A rows
+        e3_rows(p, off, [&](int64_t row, int64_t e3c, int, const int64_t *cols, const double *coef, int nt) {
+            s.t(e3c, row, -1.0);
             for (int q = 0; q < nt; q++) s.t(cols[q], row, coef[q]);
         });
         const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;

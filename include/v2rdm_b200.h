@@ -47,6 +47,8 @@ extern "C" {
  * CONSTRAIN_Q3 (q3.cc:45-423, 425-803; implies D3, needs Q2 and G2) */
 #define V2B_CONSTRAIN_D3 16
 #define V2B_CONSTRAIN_Q3 32
+/* CONSTRAIN_E3 (e3.cc:45-566, 570-1082; implies D3) */
+#define V2B_CONSTRAIN_E3 64
 
 /* libsdp::SDPOptions as hilbert fills it (src/v2rdm_casscf/v2rdm_solver.cc:426-431) */
 typedef struct {

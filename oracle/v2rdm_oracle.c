@@ -9,7 +9,7 @@
  * restates (paths relative to the hilbert source tree).
  *
  * Supported constraint sets: POSITIVITY D / DQ / DG / DQG / DQGT1 / DQGT2 /
- * DQGT1T2, each optionally with CONSTRAIN_D3 and CONSTRAIN_Q3, with
+ * DQGT1T2, each optionally with CONSTRAIN_D3, CONSTRAIN_Q3 and CONSTRAIN_E3, with
  * CONSTRAIN_SPIN and CONSTRAIN_SZ on or off, singlet and non-singlet.
  */
 #include <math.h>
@@ -19,13 +19,13 @@
 typedef struct {
     int n;            /* active orbitals (amo_) */
     int na, nb;       /* alpha / beta electrons */
-    int q2, g2, t1, t2, d3, q3, spin, sz;
+    int q2, g2, t1, t2, d3, q3, e3, spin, sz;
     int mult;         /* 2S+1 as the reference stores it */
     int gab, gaa;
     int *bas_ab, *ibas_ab, *bas_aa, *ibas_aa;
     long d2ab, d2aa, d2bb, d200, d1a, d1b, q1a, q1b, q2ab, q2aa, q2bb, g2ab, g2ba, g2aa;
     long t1aaa, t1bbb, t1aab, t1bba, t2aaa, t2bbb, t2aab, t2bba, d3aaa, d3bbb, d3aab, d3bba;
-    long q3aaa, q3bbb, q3aab, q3bba;
+    long q3aaa, q3bbb, q3aab, q3bba, e3aaa, e3bbb, e3aab, e3bba;
     int trip_aaa, trip_aab, trip_aba;   /* triplets (i<j<k), (i<j, k) and (i, j, k) */
     int *bas_aaa, *bas_aab, *bas_aba;   /* 3 ints per triplet */
     int *ibas_aaa, *ibas_aab;           /* n^3: any order of an aaa set / of the aa pair */
@@ -66,6 +66,8 @@ static void build_tables(v2o_problem *p) {
 
 #define IAB(p, i, j) ((p)->ibas_ab[(i) * (p)->n + (j)])
 #define IAA(p, i, j) ((p)->ibas_aa[(i) * (p)->n + (j)])
+#define D3_AAA(a, b, c) (p->ibas_aaa[((long)(a) * p->n + (b)) * p->n + (c)])
+#define D3_AAB(a, b, c) (p->ibas_aab[((long)(a) * p->n + (b)) * p->n + (c)])
 
 enum { T2_AU = 0, T2_ATU = 1, T2_GUESS = 2 };
 static void t1_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
@@ -123,6 +125,15 @@ static void set_offsets(v2o_problem *p) {
         p->t2aab = off; off += ta * ta; p->dims[nb++] = (int)ta;
         p->t2bba = off; off += ta * ta; p->dims[nb++] = (int)ta;
     }
+    /* v2rdm_solver.cc:3909-3938: E3aaa, E3bbb (dim aab + aba), E3aab, E3bba (dim aab) */
+    p->e3aaa = p->e3bbb = p->e3aab = p->e3bba = -1;
+    if (p->e3) {
+        long w = (long)p->trip_aab + p->trip_aba, ta = p->trip_aab;
+        p->e3aaa = off; off += w * w; p->dims[nb++] = (int)w;
+        p->e3bbb = off; off += w * w; p->dims[nb++] = (int)w;
+        p->e3aab = off; off += ta * ta; p->dims[nb++] = (int)ta;
+        p->e3bba = off; off += ta * ta; p->dims[nb++] = (int)ta;
+    }
     /* v2rdm_solver.cc:3970-3998: Q3aaa, Q3bbb (dim aaa), Q3aab, Q3bba (dim aab) */
     p->q3aaa = p->q3bbb = p->q3aab = p->q3bba = -1;
     if (p->q3) {
@@ -164,6 +175,10 @@ static void set_offsets(v2o_problem *p) {
     if (p->t2) {   /* v2rdm_solver.cc:3568-3580 */
         long w = (long)p->trip_aab + p->trip_aba, ta = p->trip_aab;
         d += 2 * w * w + 2 * ta * ta;
+    }
+    if (p->e3) {   /* v2rdm_solver.cc:3582-3595 */
+        long w = (long)p->trip_aab + p->trip_aba, ta = p->trip_aab;
+        d += 2 * ta * ta + 2 * w * w;
     }
     if (p->q3) {   /* v2rdm_solver.cc:3610-3623 */
         long t3 = p->trip_aaa, ta = p->trip_aab;
@@ -214,17 +229,20 @@ static void build_triplets(v2o_problem *p) {
 
 /* positivity: 0 D, 1 DQ, 2 DG, 3 DQG, 4 DQGT2, 5 DQGT1, 6 DQGT1T2 (= DQGT)
  * (v2rdm_solver.cc:4081-4118), plus 16 for CONSTRAIN_D3 (:4120-4122) and 32 for
- * CONSTRAIN_Q3 (which implies D3, :4132-4135).
+ * CONSTRAIN_Q3 (which implies D3, :4132-4135), 64 for CONSTRAIN_E3 (implies D3,
+ * :4124-4127).
  * hubbard selects the multiplicity convention of
  * v2rdm_solver.cc:862-863 (Hubbard) versus :983-984 (external). */
 v2o_problem *v2o_create(int n, int na, int nb, int positivity, int spin, int sz, int hubbard) {
-    const int q3 = (positivity >> 5) & 1, d3 = ((positivity >> 4) & 1) | q3;
+    const int q3 = (positivity >> 5) & 1, e3 = (positivity >> 6) & 1;
+    const int d3 = ((positivity >> 4) & 1) | q3 | e3;
     positivity &= 15;
     if (n < 1 || na < 0 || nb < 0 || na > n || nb > n || positivity < 0 || positivity > 6) return NULL;
     v2o_problem *p = (v2o_problem *)calloc(1, sizeof(v2o_problem));
     p->n = n; p->na = na; p->nb = nb;
     p->d3 = d3;
     p->q3 = q3;
+    p->e3 = e3;
     p->q2 = (positivity == 1 || positivity >= 3);
     p->g2 = (positivity >= 2);
     p->t1 = (positivity == 5 || positivity == 6);
@@ -261,11 +279,11 @@ void v2o_tables(const v2o_problem *p, int *bas_ab, int *ibas_ab, int *bas_aa, in
 }
 /* block offsets in the order d2ab d2aa d2bb d200 d1a d1b q1a q1b q2ab q2aa q2bb g2ab g2ba g2aa */
 void v2o_offsets(const v2o_problem *p, long *o) {
-    long v[30] = {p->d2ab, p->d2aa, p->d2bb, p->d200, p->d1a, p->d1b, p->q1a,
+    long v[34] = {p->d2ab, p->d2aa, p->d2bb, p->d200, p->d1a, p->d1b, p->q1a,
                   p->q1b,  p->q2ab, p->q2aa, p->q2bb, p->g2ab, p->g2ba, p->g2aa,
                   p->t2aaa, p->t2bbb, p->t2aab, p->t2bba,
                   p->t1aaa, p->t1bbb, p->t1aab, p->t1bba, p->d3aaa, p->d3bbb, p->d3aab, p->d3bba,
-                  p->q3aaa, p->q3bbb, p->q3aab, p->q3bba};
+                  p->q3aaa, p->q3bbb, p->q3aab, p->q3bba, p->e3aaa, p->e3bbb, p->e3aab, p->e3bba};
     memcpy(o, v, sizeof(v));
 }
 
@@ -613,11 +631,15 @@ static int t2_terms(const v2o_problem *p, int sb, int i, int j, int k, int l, in
  *  T2_ATU:   A[t2] -= u[row], A[col] += coef u[row]         (t2.cc:3376-3966,
  *            the scatter of the same terms in the same order)
  *  T2_GUESS: u[t2] = 0 + terms, zero on aaa/abb             (t2.cc:1845-2452) */
-static void t2_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
-                     double *x) {
+typedef int (*big_terms_fn)(const v2o_problem *, int, int, int, int, int, int, int, t2_term *);
+
+/* the T2 block layout (aab, bba, then the aab+aba blocks), rows led by
+ * -X(r, c) for X in lead = {aab, bba, aaa, bbb} */
+static void big_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
+                      double *x, big_terms_fn terms, const long lead[4]) {
     const long ta = p->trip_aab, tb = p->trip_aba, w = ta + tb;
     const long dual[4] = {off, off + ta * ta, off + 2 * ta * ta, off + 2 * ta * ta + w * w};
-    const long prim[4] = {p->t2aab, p->t2bba, p->t2aaa, p->t2bbb};
+    const long *prim = lead;
     for (int sb = 0; sb < 10; sb++) {
         const int blk = sb < 2 ? sb : (sb < 6 ? 2 : 3);
         const long width = sb < 2 ? ta : w;
@@ -632,7 +654,7 @@ static void t2_visit(const v2o_problem *p, long off, int mode, const double *u, 
                 const int l = cb[3 * c], m = cb[3 * c + 1], q = cb[3 * c + 2];
                 const long id = (r0 + r) * width + (c0 + c);
                 t2_term t[8];
-                const int nt = t2_terms(p, sb, i, j, k, l, m, q, t);
+                const int nt = terms(p, sb, i, j, k, l, m, q, t);
                 if (mode == T2_AU) {
                     double dum = -u[prim[blk] + id];
                     for (int e = 0; e < nt; e++) dum += t[e].coef * u[t[e].col];
@@ -649,6 +671,76 @@ static void t2_visit(const v2o_problem *p, long off, int mode, const double *u, 
             }
         }
     }
+}
+
+static void t2_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
+                     double *x) {
+    const long lead[4] = {p->t2aab, p->t2bba, p->t2aaa, p->t2bbb};
+    big_visit(p, off, mode, u, A, x, t2_terms, lead);
+}
+
+/* ------------------------------------------------------------- E3 ---- */
+/* CONSTRAIN_E3 rows of e3.cc:45-566 (scatter :570-1082) in T2's layout:
+ * -E3(r, c), then one D3 element (the row's third index swapped with the
+ * column's: (i j n | l m k)) with a sign, then d_kn times a D2 element.
+ * Sub-blocks as for T2. */
+static int e3_terms(const v2o_problem *p, int sb, int i, int j, int k, int l, int m, int q,
+                    t2_term *t) {
+    int nt = 0;
+    const long ta = p->trip_aab, t3 = p->trip_aaa;
+#define E3_AB(base, a, b, c, d, e, f) ((base) + (long)D3_AAB(a, b, c) * ta + D3_AAB(d, e, f))
+#define E3_AA3(base, a, b, c, d, e, f) ((base) + (long)D3_AAA(a, b, c) * t3 + D3_AAA(d, e, f))
+    switch (sb) {
+    case 0:
+    case 1: {
+        const int b = sb == 1;
+        T2_ADD(E3_AB(b ? p->d3bba : p->d3aab, i, j, q, l, m, k), -1.0);
+        if (k == q) T2_ADD(b ? T2_D2BB(i, j, l, m) : T2_D2AA(i, j, l, m), 1.0);
+        break;
+    }
+    case 2:
+    case 6: {
+        const int b = sb == 6;
+        if (i != q && j != q && l != k && m != k) {
+            const double sg = ((i < q && q < j) ? -1.0 : 1.0) * ((l < k && k < m) ? -1.0 : 1.0);
+            T2_ADD(E3_AA3(b ? p->d3bbb : p->d3aaa, i, j, q, l, m, k), -sg);
+        }
+        if (k == q) T2_ADD(b ? T2_D2BB(i, j, l, m) : T2_D2AA(i, j, l, m), 1.0);
+        break;
+    }
+    case 3:
+        if (i != j && l != k) T2_ADD(E3_AB(p->d3aab, i, j, q, l, k, m), l > k ? -1.0 : 1.0);
+        break;
+    case 7:
+        if (i != j && l != k)
+            T2_ADD(E3_AB(p->d3bba, i, j, q, l, k, m), (i > j ? -1.0 : 1.0) * (l > k ? -1.0 : 1.0));
+        break;
+    case 4:
+        if (i != q && l != m) T2_ADD(E3_AB(p->d3aab, i, q, j, l, m, k), i > q ? -1.0 : 1.0);
+        break;
+    case 8:
+        if (i != q && l != m)
+            T2_ADD(E3_AB(p->d3bba, i, q, j, l, m, k), (i > q ? -1.0 : 1.0) * (l > m ? -1.0 : 1.0));
+        break;
+    case 5:
+    case 9: {
+        const int b = sb == 9;
+        if (j != q && m != k) {
+            const double sg = (j > q ? -1.0 : 1.0) * (m > k ? -1.0 : 1.0);
+            T2_ADD(E3_AB(b ? p->d3aab : p->d3bba, j, q, i, m, k, l), -sg);
+        }
+        if (k == q) T2_ADD(b ? T2_D2AB(j, i, m, l) : T2_D2AB(i, j, l, m), 1.0);
+        break;
+    }
+    }
+#undef E3_AB
+#undef E3_AA3
+    return nt;
+}
+
+static void e3_visit(const v2o_problem *p, long off, int mode, const double *u, double *A) {
+    const long lead[4] = {p->e3aab, p->e3bba, p->e3aaa, p->e3bbb};
+    big_visit(p, off, mode, u, A, NULL, e3_terms, lead);
 }
 
 /* ------------------------------------------------------------- T1 ---- */
@@ -797,8 +889,6 @@ static void d3_emit(d3_row *r) {
     r->nt = 0;
 }
 
-#define D3_AAA(a, b, c) (p->ibas_aaa[((long)(a) * p->n + (b)) * p->n + (c)])
-#define D3_AAB(a, b, c) (p->ibas_aab[((long)(a) * p->n + (b)) * p->n + (c)])
 
 static void d3_visit(const v2o_problem *p, long off, int mode, const double *u, double *A) {
     const int n = p->n, gaa = p->gaa, gab = p->gab;
@@ -1236,6 +1326,11 @@ void v2o_Au(const v2o_problem *p, const double *u, double *A) {
         const long w = (long)p->trip_aab + p->trip_aba;
         off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
     }
+    if (p->e3) {   /* v2rdm_solver.cc:3024-3026 */
+        e3_visit(p, off, T2_AU, u, A);
+        const long w = (long)p->trip_aab + p->trip_aba;
+        off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
+    }
     if (p->q3) {   /* v2rdm_solver.cc:3032-3034 */
         t1_like_visit(p, off, T2_AU, u, A, NULL, 1);
         off += 2L * p->trip_aab * p->trip_aab + 2L * p->trip_aaa * p->trip_aaa;
@@ -1578,6 +1673,11 @@ void v2o_ATu(const v2o_problem *p, const double *u, double *A) {
     }
     if (p->t2) {   /* v2rdm_solver.cc:3077-3080 */
         t2_visit(p, off, T2_ATU, u, A, NULL);
+        const long w = (long)p->trip_aab + p->trip_aba;
+        off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
+    }
+    if (p->e3) {   /* v2rdm_solver.cc:3082-3084 */
+        e3_visit(p, off, T2_ATU, u, A);
         const long w = (long)p->trip_aab + p->trip_aba;
         off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
     }
