@@ -34,7 +34,8 @@ Problem make_problem(const ProblemSpec &spec) {
     p.t2 = spec.positivity == POS_DQGT2 || spec.positivity == POS_DQGT1T2;
     p.q3 = spec.constrain_q3;
     p.e3 = spec.constrain_e3;
-    p.d3 = spec.constrain_d3 || p.q3 || p.e3;
+    p.f3 = spec.constrain_f3;
+    p.d3 = spec.constrain_d3 || p.q3 || p.e3 || p.f3;
     if (p.q3 && !(p.q2 && p.g2))
         throw std::invalid_argument("CONSTRAIN_Q3 needs the Q2 and G2 conditions (POSITIVITY DQG or a T option)");
     p.mult = spec.hubbard_multiplicity ? 2 * (spec.nalpha - spec.nbeta) + 1
@@ -133,6 +134,12 @@ Problem make_problem(const ProblemSpec &spec) {
         add_block(p.e3aab, p.trip_aab);
         add_block(p.e3bba, p.trip_aab);
     }
+    if (p.f3) {   // v2rdm_solver.cc:3940-3968
+        add_block(p.f3aaa, p.trip_aab + p.trip_aba);
+        add_block(p.f3bbb, p.trip_aab + p.trip_aba);
+        add_block(p.f3aab, p.trip_aab);
+        add_block(p.f3bba, p.trip_aab);
+    }
     if (p.q3) {   // v2rdm_solver.cc:3970-3998
         add_block(p.q3aaa, p.trip_aaa);
         add_block(p.q3bbb, p.trip_aaa);
@@ -162,6 +169,10 @@ Problem make_problem(const ProblemSpec &spec) {
         d += 2 * aab * aab + 2 * big * big;
     }
     if (p.e3) {
+        const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
+        d += 2 * aab * aab + 2 * big * big;
+    }
+    if (p.f3) {
         const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
         d += 2 * aab * aab + 2 * big * big;
     }
@@ -569,12 +580,15 @@ void e3_rows(const Problem &p, int64_t off, F &&f) {
     }
 }
 
+// f3 = true gives the CONSTRAIN_F3 rows (f3.cc:45-836, scatter :842-1623):
+// led by F3, then the D3 element of the E3 row with the opposite sign, then
+// the T2 terms without the d_kn D2 term (T2 = E3 + F3).
 template <class F>
-void t2_rows(const Problem &p, int64_t off, F &&f) {
+void t2_rows(const Problem &p, int64_t off, F &&f, bool f3 = false) {
     const int N = p.n, gab = p.gab, gaa = p.gaa, aab = p.trip_aab, aba = p.trip_aba;
-    const int64_t big = (int64_t)aab + aba;
-    int64_t cols[8];
-    double coef[8];
+    const int64_t big = (int64_t)aab + aba, t3 = p.trip_aaa;
+    int64_t cols[9];
+    double coef[9];
     int nt = 0;
     auto add = [&](int64_t c, double v) {
         cols[nt] = c;
@@ -596,10 +610,14 @@ void t2_rows(const Problem &p, int64_t off, F &&f) {
     auto d2ab_t = [&](int a, int b, int c, int d) { return p.d2ab + (int64_t)p.iab(a, b) * gab + p.iab(c, d); };
     // sign of the aa geminal terms: s = (n > j ? -1 : 1) (k > m ? -1 : 1)
     auto sgn = [](int a, int b, int c, int d) { return (a > b ? -1.0 : 1.0) * (c > d ? -1.0 : 1.0); };
+    auto x3 = [&](int a, int b, int c) { return (int64_t)p.ibas_aab[((size_t)a * N + b) * N + c]; };
+    auto y3 = [&](int a, int b, int c) { return (int64_t)p.ibas_aaa[((size_t)a * N + b) * N + c]; };
+    auto mixed = [&](int64_t base, int a, int b, int c, int d, int e, int g) { return base + x3(a, b, c) * aab + x3(d, e, g); };
+    auto neg = [](bool flip) { return flip ? -1.0 : 1.0; };
 
     // T2aab (t2.cc:1239-1302) and T2bba (t2.cc:1305-1368)
     for (int spin = 0; spin < 2; spin++) {
-        const int64_t t2 = spin ? p.t2bba : p.t2aab;
+        const int64_t t2 = f3 ? (spin ? p.f3bba : p.f3aab) : (spin ? p.t2bba : p.t2aab);
         const int64_t d2same = spin ? p.d2bb : p.d2aa, d1other = spin ? p.d1a : p.d1b;
         for (int ijk = 0; ijk < aab; ijk++) {
             int i, j, k;
@@ -608,7 +626,8 @@ void t2_rows(const Problem &p, int64_t off, F &&f) {
                 int l, m, n;
                 trip(lmn, true, l, m, n);
                 nt = 0;
-                if (k == n) add(d2aa_t(d2same, i, j, l, m), 1.0);
+                if (f3) add(mixed(spin ? p.d3bba : p.d3aab, i, j, n, l, m, k), 1.0);
+                else if (k == n) add(d2aa_t(d2same, i, j, l, m), 1.0);
                 if (j == m && i == l) add(d1other + (int64_t)n * N + k, 1.0);
                 if (j == l && i == m) add(d1other + (int64_t)n * N + k, -1.0);
                 if (spin == 0) {
@@ -630,7 +649,7 @@ void t2_rows(const Problem &p, int64_t off, F &&f) {
     }
     // big blocks T2aaa (t2.cc:1371-1601) and T2bbb (t2.cc:1604-1840)
     for (int spin = 0; spin < 2; spin++) {
-        const int64_t t2 = spin ? p.t2bbb : p.t2aaa;
+        const int64_t t2 = f3 ? (spin ? p.f3bbb : p.f3aaa) : (spin ? p.t2bbb : p.t2aaa);
         const int64_t d2s = spin ? p.d2bb : p.d2aa, d2o = spin ? p.d2aa : p.d2bb;
         const int64_t d1s = spin ? p.d1b : p.d1a, d1o = spin ? p.d1a : p.d1b;
         for (int sb = 0; sb < 4; sb++) {
@@ -644,7 +663,13 @@ void t2_rows(const Problem &p, int64_t off, F &&f) {
                     trip(lmn, colaab, l, m, n);
                     nt = 0;
                     if (sb == 0) {   // aaa/aaa, bbb/bbb
-                        if (k == n) add(d2aa_t(d2s, i, j, l, m), 1.0);
+                        if (f3) {
+                            if (i != n && j != n && l != k && m != k)
+                                add((spin ? p.d3bbb : p.d3aaa) + y3(i, j, n) * t3 + y3(l, m, k),
+                                    neg(i < n && n < j) * neg(l < k && k < m));
+                        } else if (k == n) {
+                            add(d2aa_t(d2s, i, j, l, m), 1.0);
+                        }
                         if (j == m && i == l) add(d1s + (int64_t)n * N + k, 1.0);
                         if (j == l && i == m) add(d1s + (int64_t)n * N + k, -1.0);
                         if (i == l && n != j && k != m) add(d2aa_t(d2s, n, j, k, m), -sgn(n, j, k, m));
@@ -652,6 +677,9 @@ void t2_rows(const Problem &p, int64_t off, F &&f) {
                         if (i == m && n != j && k != l) add(d2aa_t(d2s, n, j, k, l), sgn(n, j, k, l));
                         if (j == m && n != i && k != l) add(d2aa_t(d2s, n, i, k, l), -sgn(n, i, k, l));
                     } else if (sb == 1) {   // aaa/abb, bbb/baa
+                        if (f3 && i != j && l != k)
+                            add(mixed(spin ? p.d3bba : p.d3aab, i, j, n, l, k, m),
+                                -(spin ? neg(i > j) * neg(l > k) : neg(l > k)));
                         if (spin == 0) {
                             if (i == l) add(d2ab_t(j, n, k, m), 1.0);
                             if (j == l) add(d2ab_t(i, n, k, m), -1.0);
@@ -660,6 +688,9 @@ void t2_rows(const Problem &p, int64_t off, F &&f) {
                             if (j == l) add(d2ab_t(n, i, m, k), -1.0);
                         }
                     } else if (sb == 2) {   // abb/aaa, baa/bbb
+                        if (f3 && i != n && l != m)
+                            add(mixed(spin ? p.d3bba : p.d3aab, i, n, j, l, m, k),
+                                -(spin ? neg(i > n) * neg(l > m) : neg(i > n)));
                         if (spin == 0) {
                             if (i == l) add(d2ab_t(n, j, m, k), 1.0);
                             if (i == m) add(d2ab_t(n, j, l, k), -1.0);
@@ -668,13 +699,15 @@ void t2_rows(const Problem &p, int64_t off, F &&f) {
                             if (i == m) add(d2ab_t(j, n, k, l), -1.0);
                         }
                     } else {   // abb/abb, baa/baa
+                        if (f3 && j != n && m != k)
+                            add(mixed(spin ? p.d3aab : p.d3bba, j, n, i, m, k, l), neg(j > n) * neg(m > k));
                         if (spin == 0) {
-                            if (k == n) add(d2ab_t(i, j, l, m), 1.0);
+                            if (!f3 && k == n) add(d2ab_t(i, j, l, m), 1.0);
                             if (j == m && i == l) add(d1o + (int64_t)n * N + k, 1.0);
                             if (i == l && n != j && k != m) add(d2aa_t(d2o, n, j, k, m), -sgn(n, j, k, m));
                             if (j == m) add(d2ab_t(i, n, l, k), -1.0);
                         } else {
-                            if (k == n) add(d2ab_t(j, i, m, l), 1.0);
+                            if (!f3 && k == n) add(d2ab_t(j, i, m, l), 1.0);
                             if (j == m && i == l) add(d1o + (int64_t)n * N + k, 1.0);
                             if (i == l && n != j && k != m) add(d2aa_t(d2o, n, j, k, m), -sgn(n, j, k, m));
                             if (j == m) add(d2ab_t(n, i, k, l), -1.0);
@@ -1130,6 +1163,14 @@ void visit_A(const Problem &p, S &s) {
         const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
         off += 2 * aab * aab + 2 * big * big;
     }
+    if (p.f3) {   // f3.cc:45-836
+        t2_rows(p, off, [&](int64_t row, int64_t f3c, int, const int64_t *cols, const double *coef, int nt) {
+            s.t(row, f3c, -1.0);
+            for (int q = 0; q < nt; q++) s.t(row, cols[q], coef[q]);
+        }, true);
+        const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
+        off += 2 * aab * aab + 2 * big * big;
+    }
     if (p.q3) {   // q3.cc:45-423
         t1_rows(p, off, [&](int64_t row, int64_t q3c, int, const int64_t *cols, const double *coef, int nt) {
             s.t(row, q3c, -1.0);
@@ -1451,6 +1492,14 @@ void visit_AT(const Problem &p, S &s) {
             s.t(e3c, row, -1.0);
             for (int q = 0; q < nt; q++) s.t(cols[q], row, coef[q]);
         });
+        const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
+        off += 2 * aab * aab + 2 * big * big;
+    }
+    if (p.f3) {   // f3.cc:842-1623 scatters in the same order as the A rows
+        t2_rows(p, off, [&](int64_t row, int64_t f3c, int, const int64_t *cols, const double *coef, int nt) {
+            s.t(f3c, row, -1.0);
+            for (int q = 0; q < nt; q++) s.t(cols[q], row, coef[q]);
+        }, true);
         const int64_t aab = p.trip_aab, big = (int64_t)p.trip_aab + p.trip_aba;
         off += 2 * aab * aab + 2 * big * big;
     }

@@ -49,6 +49,8 @@ extern "C" {
 #define V2B_CONSTRAIN_Q3 32
 /* CONSTRAIN_E3 (e3.cc:45-566, 570-1082; implies D3) */
 #define V2B_CONSTRAIN_E3 64
+/* CONSTRAIN_F3 (f3.cc:45-836, 842-1623; implies D3) */
+#define V2B_CONSTRAIN_F3 128
 
 /* libsdp::SDPOptions as hilbert fills it (src/v2rdm_casscf/v2rdm_solver.cc:426-431) */
 typedef struct {

@@ -9,7 +9,7 @@
  * restates (paths relative to the hilbert source tree).
  *
  * Supported constraint sets: POSITIVITY D / DQ / DG / DQG / DQGT1 / DQGT2 /
- * DQGT1T2, each optionally with CONSTRAIN_D3, CONSTRAIN_Q3 and CONSTRAIN_E3, with
+ * DQGT1T2, each optionally with CONSTRAIN_D3, _Q3, _E3 and _F3, with
  * CONSTRAIN_SPIN and CONSTRAIN_SZ on or off, singlet and non-singlet.
  */
 #include <math.h>
@@ -19,19 +19,19 @@
 typedef struct {
     int n;            /* active orbitals (amo_) */
     int na, nb;       /* alpha / beta electrons */
-    int q2, g2, t1, t2, d3, q3, e3, spin, sz;
+    int q2, g2, t1, t2, d3, q3, e3, f3, spin, sz;
     int mult;         /* 2S+1 as the reference stores it */
     int gab, gaa;
     int *bas_ab, *ibas_ab, *bas_aa, *ibas_aa;
     long d2ab, d2aa, d2bb, d200, d1a, d1b, q1a, q1b, q2ab, q2aa, q2bb, g2ab, g2ba, g2aa;
     long t1aaa, t1bbb, t1aab, t1bba, t2aaa, t2bbb, t2aab, t2bba, d3aaa, d3bbb, d3aab, d3bba;
-    long q3aaa, q3bbb, q3aab, q3bba, e3aaa, e3bbb, e3aab, e3bba;
+    long q3aaa, q3bbb, q3aab, q3bba, e3aaa, e3bbb, e3aab, e3bba, f3aaa, f3bbb, f3aab, f3bba;
     int trip_aaa, trip_aab, trip_aba;   /* triplets (i<j<k), (i<j, k) and (i, j, k) */
     int *bas_aaa, *bas_aab, *bas_aba;   /* 3 ints per triplet */
     int *ibas_aaa, *ibas_aab;           /* n^3: any order of an aaa set / of the aa pair */
     long n_primal, n_dual;
     int nblocks;
-    int dims[32];
+    int dims[64];     /* at most 46 blocks: every family of the reference on */
 } v2o_problem;
 
 /* basis.cc:426-533 (C1): geminal (j,i) is pushed for i outer, j inner, so
@@ -134,6 +134,15 @@ static void set_offsets(v2o_problem *p) {
         p->e3aab = off; off += ta * ta; p->dims[nb++] = (int)ta;
         p->e3bba = off; off += ta * ta; p->dims[nb++] = (int)ta;
     }
+    /* v2rdm_solver.cc:3940-3968: F3aaa, F3bbb (dim aab + aba), F3aab, F3bba (dim aab) */
+    p->f3aaa = p->f3bbb = p->f3aab = p->f3bba = -1;
+    if (p->f3) {
+        long w = (long)p->trip_aab + p->trip_aba, ta = p->trip_aab;
+        p->f3aaa = off; off += w * w; p->dims[nb++] = (int)w;
+        p->f3bbb = off; off += w * w; p->dims[nb++] = (int)w;
+        p->f3aab = off; off += ta * ta; p->dims[nb++] = (int)ta;
+        p->f3bba = off; off += ta * ta; p->dims[nb++] = (int)ta;
+    }
     /* v2rdm_solver.cc:3970-3998: Q3aaa, Q3bbb (dim aaa), Q3aab, Q3bba (dim aab) */
     p->q3aaa = p->q3bbb = p->q3aab = p->q3bba = -1;
     if (p->q3) {
@@ -154,6 +163,7 @@ static void set_offsets(v2o_problem *p) {
     }
     p->n_primal = off;
     p->nblocks = nb;
+    if (nb > (int)(sizeof(p->dims) / sizeof(p->dims[0]))) abort();
 
     long d = 0;
     d += p->sz ? 3 : 1;
@@ -177,6 +187,10 @@ static void set_offsets(v2o_problem *p) {
         d += 2 * w * w + 2 * ta * ta;
     }
     if (p->e3) {   /* v2rdm_solver.cc:3582-3595 */
+        long w = (long)p->trip_aab + p->trip_aba, ta = p->trip_aab;
+        d += 2 * ta * ta + 2 * w * w;
+    }
+    if (p->f3) {   /* v2rdm_solver.cc:3596-3609 */
         long w = (long)p->trip_aab + p->trip_aba, ta = p->trip_aab;
         d += 2 * ta * ta + 2 * w * w;
     }
@@ -230,12 +244,12 @@ static void build_triplets(v2o_problem *p) {
 /* positivity: 0 D, 1 DQ, 2 DG, 3 DQG, 4 DQGT2, 5 DQGT1, 6 DQGT1T2 (= DQGT)
  * (v2rdm_solver.cc:4081-4118), plus 16 for CONSTRAIN_D3 (:4120-4122) and 32 for
  * CONSTRAIN_Q3 (which implies D3, :4132-4135), 64 for CONSTRAIN_E3 (implies D3,
- * :4124-4127).
+ * :4124-4127) and 128 for CONSTRAIN_F3 (implies D3, :4128-4131).
  * hubbard selects the multiplicity convention of
  * v2rdm_solver.cc:862-863 (Hubbard) versus :983-984 (external). */
 v2o_problem *v2o_create(int n, int na, int nb, int positivity, int spin, int sz, int hubbard) {
-    const int q3 = (positivity >> 5) & 1, e3 = (positivity >> 6) & 1;
-    const int d3 = ((positivity >> 4) & 1) | q3 | e3;
+    const int q3 = (positivity >> 5) & 1, e3 = (positivity >> 6) & 1, f3 = (positivity >> 7) & 1;
+    const int d3 = ((positivity >> 4) & 1) | q3 | e3 | f3;
     positivity &= 15;
     if (n < 1 || na < 0 || nb < 0 || na > n || nb > n || positivity < 0 || positivity > 6) return NULL;
     v2o_problem *p = (v2o_problem *)calloc(1, sizeof(v2o_problem));
@@ -243,6 +257,7 @@ v2o_problem *v2o_create(int n, int na, int nb, int positivity, int spin, int sz,
     p->d3 = d3;
     p->q3 = q3;
     p->e3 = e3;
+    p->f3 = f3;
     p->q2 = (positivity == 1 || positivity >= 3);
     p->g2 = (positivity >= 2);
     p->t1 = (positivity == 5 || positivity == 6);
@@ -279,11 +294,12 @@ void v2o_tables(const v2o_problem *p, int *bas_ab, int *ibas_ab, int *bas_aa, in
 }
 /* block offsets in the order d2ab d2aa d2bb d200 d1a d1b q1a q1b q2ab q2aa q2bb g2ab g2ba g2aa */
 void v2o_offsets(const v2o_problem *p, long *o) {
-    long v[34] = {p->d2ab, p->d2aa, p->d2bb, p->d200, p->d1a, p->d1b, p->q1a,
+    long v[38] = {p->d2ab, p->d2aa, p->d2bb, p->d200, p->d1a, p->d1b, p->q1a,
                   p->q1b,  p->q2ab, p->q2aa, p->q2bb, p->g2ab, p->g2ba, p->g2aa,
                   p->t2aaa, p->t2bbb, p->t2aab, p->t2bba,
                   p->t1aaa, p->t1bbb, p->t1aab, p->t1bba, p->d3aaa, p->d3bbb, p->d3aab, p->d3bba,
-                  p->q3aaa, p->q3bbb, p->q3aab, p->q3bba, p->e3aaa, p->e3bbb, p->e3aab, p->e3bba};
+                  p->q3aaa, p->q3bbb, p->q3aab, p->q3bba, p->e3aaa, p->e3bbb, p->e3aab, p->e3bba,
+                  p->f3aaa, p->f3bbb, p->f3aab, p->f3bba};
     memcpy(o, v, sizeof(v));
 }
 
@@ -741,6 +757,32 @@ static int e3_terms(const v2o_problem *p, int sb, int i, int j, int k, int l, in
 static void e3_visit(const v2o_problem *p, long off, int mode, const double *u, double *A) {
     const long lead[4] = {p->e3aab, p->e3bba, p->e3aaa, p->e3bbb};
     big_visit(p, off, mode, u, A, NULL, e3_terms, lead);
+}
+
+
+/* ------------------------------------------------------------- F3 ---- */
+/* CONSTRAIN_F3 rows of f3.cc:45-836 (scatter :842-1623), T2's layout: -F3,
+ * then E3's D3 element with the opposite sign, then T2's terms without the
+ * d_kn D2 term that E3 carries (T2 = E3 + F3), all in the reference's order. */
+static int f3_terms(const v2o_problem *p, int sb, int i, int j, int k, int l, int m, int q,
+                    t2_term *t) {
+    t2_term e[8], w[8];
+    const int ne = e3_terms(p, sb, i, j, k, l, m, q, e);
+    const int nw = t2_terms(p, sb, i, j, k, l, m, q, w);
+    int nt = 0;
+    if (ne > 0 && e[0].col >= p->d3aaa) {   /* the D3 element, when the row has one */
+        t[nt] = e[0];
+        t[nt].coef = -e[0].coef;
+        nt++;
+    }
+    const int skip = (k == q && (sb == 0 || sb == 1 || sb == 2 || sb == 5 || sb == 6 || sb == 9));
+    for (int x = skip; x < nw; x++) t[nt++] = w[x];
+    return nt;
+}
+
+static void f3_visit(const v2o_problem *p, long off, int mode, const double *u, double *A) {
+    const long lead[4] = {p->f3aab, p->f3bba, p->f3aaa, p->f3bbb};
+    big_visit(p, off, mode, u, A, NULL, f3_terms, lead);
 }
 
 /* ------------------------------------------------------------- T1 ---- */
@@ -1331,6 +1373,11 @@ void v2o_Au(const v2o_problem *p, const double *u, double *A) {
         const long w = (long)p->trip_aab + p->trip_aba;
         off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
     }
+    if (p->f3) {   /* v2rdm_solver.cc:3028-3030 */
+        f3_visit(p, off, T2_AU, u, A);
+        const long w = (long)p->trip_aab + p->trip_aba;
+        off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
+    }
     if (p->q3) {   /* v2rdm_solver.cc:3032-3034 */
         t1_like_visit(p, off, T2_AU, u, A, NULL, 1);
         off += 2L * p->trip_aab * p->trip_aab + 2L * p->trip_aaa * p->trip_aaa;
@@ -1678,6 +1725,11 @@ void v2o_ATu(const v2o_problem *p, const double *u, double *A) {
     }
     if (p->e3) {   /* v2rdm_solver.cc:3082-3084 */
         e3_visit(p, off, T2_ATU, u, A);
+        const long w = (long)p->trip_aab + p->trip_aba;
+        off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
+    }
+    if (p->f3) {   /* v2rdm_solver.cc:3086-3088 */
+        f3_visit(p, off, T2_ATU, u, A);
         const long w = (long)p->trip_aab + p->trip_aba;
         off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
     }

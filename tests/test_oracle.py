@@ -22,7 +22,7 @@ def test_golden_cases_present(golden):
                                   "ext4_dq_nosz", "ext4_dg_doublet", "ext5_dqg", "ext1_dqg",
                                   "hub3_dqgt2", "ext3_dqgt2_doublet", "hub4_dqgt1",
                                   "ext4_dqgt1t2_doublet", "hub4_dqg_d3", "ext3_d_d3_nosz_doublet",
-                                  "ext3_dqg_q3_doublet", "hub3_d_e3"])
+                                  "ext3_dqg_q3_doublet", "hub3_d_e3", "ext3_d_f3_doublet"])
 def test_oracle_matches_golden(golden, name):
     case = golden[name]
     kw = case_kwargs(case)
@@ -89,7 +89,8 @@ def test_oracle_bit_exact_against_reference_grid():
     rng = np.random.default_rng(3)
     for n, na, nb, pos, spin, sz in itertools.product([1, 2, 3, 4], [0, 1, 2], [0, 1, 2],
                                                       ["D", "DQ", "DG", "DQG", "DQGT2", "DQGT1",
-                                                       "DQGT1T2", "DQG+D3", "D+D3", "DQG+Q3", "D+E3"], [0, 1], [0, 1]):
+                                                       "DQGT1T2", "DQG+D3", "D+D3", "DQG+Q3", "D+E3", "D+F3",
+                                                       "DQGT1T2+D3+Q3+E3+F3"], [0, 1], [0, 1]):
         if na > n or nb > n:
             continue
         kw = dict(h=rng.standard_normal((n, n)), g=rng.standard_normal((n,) * 4))
