@@ -26,6 +26,7 @@ V2B_CONSTRAIN_D3 = 16   # OR-ed into a POSITIVITY value
 V2B_CONSTRAIN_Q3 = 32   # (implies D3)
 V2B_CONSTRAIN_E3 = 64   # (implies D3)
 V2B_CONSTRAIN_F3 = 128  # (implies D3)
+V2B_CONSTRAIN_D4 = 256  # (implies D3)
 
 #: every symbol declared in include/v2rdm_b200.h
 EXPORTS = (

@@ -1427,13 +1427,15 @@ int v2b_problem_create(int nmo, int nalpha, int nbeta, int positivity, int const
         spec.nalpha = nalpha;
         spec.nbeta = nbeta;
         if (positivity < 0 ||
-            (positivity & ~(15 | V2B_CONSTRAIN_D3 | V2B_CONSTRAIN_Q3 | V2B_CONSTRAIN_E3 | V2B_CONSTRAIN_F3)))
+            (positivity & ~(15 | V2B_CONSTRAIN_D3 | V2B_CONSTRAIN_Q3 | V2B_CONSTRAIN_E3 | V2B_CONSTRAIN_F3 |
+                            V2B_CONSTRAIN_D4)))
             throw std::invalid_argument("v2b_problem_create: unknown POSITIVITY bits");
         spec.positivity = positivity & 15;
         spec.constrain_d3 = (positivity & V2B_CONSTRAIN_D3) != 0;
         spec.constrain_q3 = (positivity & V2B_CONSTRAIN_Q3) != 0;
         spec.constrain_e3 = (positivity & V2B_CONSTRAIN_E3) != 0;
         spec.constrain_f3 = (positivity & V2B_CONSTRAIN_F3) != 0;
+        spec.constrain_d4 = (positivity & V2B_CONSTRAIN_D4) != 0;
         spec.constrain_spin = constrain_spin != 0;
         spec.constrain_sz = constrain_sz != 0;
         spec.hubbard_multiplicity = hubbard_multiplicity != 0;

@@ -35,7 +35,8 @@ Problem make_problem(const ProblemSpec &spec) {
     p.q3 = spec.constrain_q3;
     p.e3 = spec.constrain_e3;
     p.f3 = spec.constrain_f3;
-    p.d3 = spec.constrain_d3 || p.q3 || p.e3 || p.f3;
+    p.d4 = spec.constrain_d4;
+    p.d3 = spec.constrain_d3 || p.q3 || p.e3 || p.f3 || p.d4;
     if (p.q3 && !(p.q2 && p.g2))
         throw std::invalid_argument("CONSTRAIN_Q3 needs the Q2 and G2 conditions (POSITIVITY DQG or a T option)");
     p.mult = spec.hubbard_multiplicity ? 2 * (spec.nalpha - spec.nbeta) + 1
@@ -116,6 +117,39 @@ Problem make_problem(const ProblemSpec &spec) {
         p.trip_aab = (int)(p.bas_aab.size() / 3);
         p.trip_aaa = (int)(p.bas_aaa.size() / 3);
     }
+    if (p.d4) {   // basis.cc:747-900
+        const size_t n4 = (size_t)n * n * n * n;
+        p.ibas_aaaa.assign(n4, -999);
+        p.ibas_aaab.assign(n4, -999);
+        p.ibas_aabb.assign(n4, -999);
+        auto at = [&](int a, int b, int c, int d) { return (((size_t)a * n + b) * n + c) * n + d; };
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++)
+                for (int k = 0; k < n; k++)
+                    for (int l = 0; l < n; l++) {
+                        if (i < j && k < l) {
+                            for (size_t e : {at(i, j, k, l), at(j, i, k, l), at(i, j, l, k), at(j, i, l, k)})
+                                p.ibas_aabb[e] = p.quad_aabb;
+                            p.quad_aabb++;
+                        }
+                        if (i < j && j < k) {
+                            const int t[3] = {i, j, k};
+                            for (int a = 0; a < 3; a++)
+                                for (int b = 0; b < 3; b++)
+                                    if (a != b) p.ibas_aaab[at(t[a], t[b], t[3 - a - b], l)] = p.quad_aaab;
+                            p.quad_aaab++;
+                        }
+                        if (i < j && j < k && k < l) {
+                            const int t[4] = {i, j, k, l};
+                            for (int a = 0; a < 4; a++)
+                                for (int b = 0; b < 4; b++)
+                                    for (int c = 0; c < 4; c++)
+                                        if (a != b && a != c && b != c)
+                                            p.ibas_aaaa[at(t[a], t[b], t[c], t[6 - a - b - c])] = p.quad_aaaa;
+                            p.quad_aaaa++;
+                        }
+                    }
+    }
     if (p.t1) {   // v2rdm_solver.cc:3848-3877
         add_block(p.t1aaa, p.trip_aaa);
         add_block(p.t1bbb, p.trip_aaa);
@@ -152,6 +186,13 @@ Problem make_problem(const ProblemSpec &spec) {
         add_block(p.d3aab, p.trip_aab);
         add_block(p.d3bba, p.trip_aab);
     }
+    if (p.d4) {   // v2rdm_solver.cc:4030-4061
+        add_block(p.d4aaaa, p.quad_aaaa);
+        add_block(p.d4aaab, p.quad_aaab);
+        add_block(p.d4aabb, p.quad_aabb);
+        add_block(p.d4bbba, p.quad_aaab);
+        add_block(p.d4bbbb, p.quad_aaaa);
+    }
     p.n_primal = off;
 
     const int64_t gab2 = (int64_t)p.gab * p.gab, gaa2 = (int64_t)p.gaa * p.gaa, n2 = (int64_t)n * n;
@@ -181,6 +222,17 @@ Problem make_problem(const ProblemSpec &spec) {
         d += spec.constrain_sz ? 4 * gaa2 + 2 * gab2 : 2 * gaa2 + gab2;
         if (spec.constrain_spin && singlet)
             d += (int64_t)p.trip_aab * p.trip_aab + 2 * (int64_t)p.trip_aaa * p.trip_aaa;
+    }
+    if (p.d4) {   // v2rdm_solver.cc:3678-3720
+        const int64_t t3 = p.trip_aaa, ta = p.trip_aab;
+        const int na = spec.nalpha, nb = spec.nbeta;
+        if (na > 3) d += t3 * t3;
+        if (na > 2 && nb > 0) d += t3 * t3 + ta * ta;
+        // the reference counts the aabb family twice and writes it once: the
+        // second 2 aab^2 rows are empty, at the end of the dual vector
+        if (na > 1 && nb > 1) d += 4 * ta * ta;
+        if (na > 0 && nb > 2) d += t3 * t3 + ta * ta;
+        if (nb > 3) d += t3 * t3;
     }
     p.n_dual = d;
     if (p.n_primal > (int64_t)kColMask || p.n_dual > (int64_t)kColMask)
@@ -583,6 +635,91 @@ void e3_rows(const Problem &p, int64_t off, F &&f) {
 // f3 = true gives the CONSTRAIN_F3 rows (f3.cc:45-836, scatter :842-1623):
 // led by F3, then the D3 element of the E3 row with the opposite sign, then
 // the T2 terms without the d_kn D2 term (T2 = E3 + F3).
+// ------------------------------------------------------------------ D4
+// CONSTRAIN_D4 rows (d4.cc:44-297, scatter :300-557): contractions of the
+// 4-RDM to the 3-RDM, families gated on the electron counts, in the
+// reference's order: aaaa->aaa (na > 3); aaab->aaa, aaab->aab (na > 2,
+// nb > 0); aabb->aab, aabb->bba (na, nb > 1); bbba->bbb, bbba->bba (na > 0,
+// nb > 2); bbbb->bbb (nb > 3).  A row: count x D3 element - sum_p (sign) D4
+// element; the sign is the parity of the positions p passes.  f(dual_row,
+// cols, coefs, nterms); returns the rows written.
+template <class F>
+int64_t d4_rows(const Problem &p, int64_t off, F &&f) {
+    const int N = p.n, na = p.spec.nalpha, nb = p.spec.nbeta;
+    const int64_t t3 = p.trip_aaa, ta = p.trip_aab;
+    const int64_t q4 = p.quad_aaaa, q31 = p.quad_aaab, q22 = p.quad_aabb;
+    const int64_t first = off;
+    std::vector<int64_t> cols;
+    std::vector<double> coef;
+    auto at = [&](int a, int b, int c, int d) { return (((size_t)a * N + b) * N + c) * N + d; };
+    auto lt = [](int q, int x) { return q < x ? -1.0 : 1.0; };
+    for (int fam = 0; fam < 8; fam++) {
+        bool on;
+        switch (fam) {
+            case 0: on = na > 3; break;
+            case 1: case 2: on = na > 2 && nb > 0; break;
+            case 3: case 4: on = na > 1 && nb > 1; break;
+            case 5: case 6: on = na > 0 && nb > 2; break;
+            default: on = nb > 3; break;
+        }
+        if (!on) continue;
+        const bool aaa_rows = fam == 0 || fam == 1 || fam == 5 || fam == 7;
+        const int64_t nr = aaa_rows ? t3 : ta;
+        const std::vector<int> &tb = aaa_rows ? p.bas_aaa : p.bas_aab;
+        for (int64_t x = 0; x < nr; x++) {
+            const int i = tb[3 * x], j = tb[3 * x + 1], k = tb[3 * x + 2];
+            for (int64_t y = 0; y < nr; y++) {
+                const int l = tb[3 * y], m = tb[3 * y + 1], n = tb[3 * y + 2];
+                const int64_t e = x * nr + y;
+                cols.clear();
+                coef.clear();
+                auto add = [&](int64_t c, double v) {
+                    cols.push_back(c);
+                    coef.push_back(v);
+                };
+                if (fam == 0 || fam == 7) {
+                    add((fam ? p.d3bbb : p.d3aaa) + e, fam ? nb - 3.0 : na - 3.0);
+                    for (int q = 0; q < N; q++) {
+                        if (q == i || q == j || q == k || q == l || q == m || q == n) continue;
+                        const double sg = lt(q, i) * lt(q, j) * lt(q, k) * lt(q, l) * lt(q, m) * lt(q, n);
+                        add((fam ? p.d4bbbb : p.d4aaaa) + (int64_t)p.ibas_aaaa[at(i, j, k, q)] * q4 +
+                                p.ibas_aaaa[at(l, m, n, q)], -sg);
+                    }
+                } else if (fam == 1 || fam == 5) {
+                    add((fam == 5 ? p.d3bbb : p.d3aaa) + e, fam == 5 ? (double)na : (double)nb);
+                    for (int q = 0; q < N; q++)
+                        add((fam == 5 ? p.d4bbba : p.d4aaab) + (int64_t)p.ibas_aaab[at(i, j, k, q)] * q31 +
+                                p.ibas_aaab[at(l, m, n, q)], -1.0);
+                } else if (fam == 2 || fam == 6) {
+                    add((fam == 6 ? p.d3bba : p.d3aab) + e, fam == 6 ? nb - 2.0 : na - 2.0);
+                    for (int q = 0; q < N; q++) {
+                        if (q == i || q == j || q == l || q == m) continue;
+                        const double sg = lt(q, i) * lt(q, j) * lt(q, l) * lt(q, m);
+                        add((fam == 6 ? p.d4bbba : p.d4aaab) + (int64_t)p.ibas_aaab[at(i, j, q, k)] * q31 +
+                                p.ibas_aaab[at(l, m, q, n)], -sg);
+                    }
+                } else if (fam == 3) {
+                    add(p.d3aab + e, nb - 1.0);
+                    for (int q = 0; q < N; q++) {
+                        if (q == k || q == n) continue;
+                        add(p.d4aabb + (int64_t)p.ibas_aabb[at(i, j, k, q)] * q22 + p.ibas_aabb[at(l, m, n, q)],
+                            -(lt(q, k) * lt(q, n)));
+                    }
+                } else {   // fam == 4
+                    add(p.d3bba + e, na - 1.0);
+                    for (int q = 0; q < N; q++) {
+                        if (q == k || q == n) continue;
+                        add(p.d4aabb + (int64_t)p.ibas_aabb[at(k, q, i, j)] * q22 + p.ibas_aabb[at(n, q, l, m)],
+                            -(lt(q, k) * lt(q, n)));
+                    }
+                }
+                f(off++, cols.data(), coef.data(), (int)cols.size());
+            }
+        }
+    }
+    return off - first;
+}
+
 template <class F>
 void t2_rows(const Problem &p, int64_t off, F &&f, bool f3 = false) {
     const int N = p.n, gab = p.gab, gaa = p.gaa, aab = p.trip_aab, aba = p.trip_aba;
@@ -1185,6 +1322,12 @@ void visit_A(const Problem &p, S &s) {
             off++;
         });
     }
+    if (p.d4) {   // d4.cc:44-297, then the empty rows of the reference's double count
+        off += d4_rows(p, off, [&](int64_t row, const int64_t *cols, const double *coef, int nt) {
+            for (int q = 0; q < nt; q++) s.t(row, cols[q], coef[q]);
+        });
+        if (p.spec.nalpha > 1 && p.spec.nbeta > 1) off += 2 * (int64_t)p.trip_aab * p.trip_aab;
+    }
     if (off != p.n_dual) throw std::logic_error("A emitter row count mismatch");
 }
 
@@ -1516,6 +1659,12 @@ void visit_AT(const Problem &p, S &s) {
             for (int q = 0; q < nt; q++) s.t(cols[q], row, coef[q]);
             off++;
         });
+    }
+    if (p.d4) {   // d4.cc:300-557 scatters in the same order as the A rows
+        off += d4_rows(p, off, [&](int64_t row, const int64_t *cols, const double *coef, int nt) {
+            for (int q = 0; q < nt; q++) s.t(cols[q], row, coef[q]);
+        });
+        if (p.spec.nalpha > 1 && p.spec.nbeta > 1) off += 2 * (int64_t)p.trip_aab * p.trip_aab;
     }
     if (off != p.n_dual) throw std::logic_error("A^T emitter row count mismatch");
 }

@@ -30,6 +30,7 @@ struct ProblemSpec {
     bool constrain_q3 = false;          // CONSTRAIN_Q3, implies D3 (:4132-4135)
     bool constrain_e3 = false;          // CONSTRAIN_E3, implies D3 (:4124-4127)
     bool constrain_f3 = false;          // CONSTRAIN_F3, implies D3 (:4128-4131)
+    bool constrain_d4 = false;          // CONSTRAIN_D4, implies D3 (:4144-4149)
 };
 
 // Packed sparse operator: entry = col (bits 0..26) | coef code (27..30) | group flag (31).
@@ -50,6 +51,7 @@ struct Problem {
     ProblemSpec spec;
     int n = 0, gab = 0, gaa = 0, mult = 1;
     bool q2 = false, g2 = false, t1 = false, t2 = false, d3 = false, q3 = false, e3 = false, f3 = false;
+    bool d4 = false;
     std::vector<int> bas_ab, ibas_ab, bas_aa, ibas_aa;
     // triplets (basis.cc:640-727, C1): aba = every (i, j, k), numbered
     // i n^2 + j n + k; aab = those with i < j, in the same order
@@ -65,6 +67,12 @@ struct Problem {
     int64_t q3aaa = -1, q3bbb = -1, q3aab = -1, q3bba = -1;
     int64_t e3aaa = -1, e3bbb = -1, e3aab = -1, e3bba = -1;
     int64_t f3aaa = -1, f3bbb = -1, f3aab = -1, f3bba = -1;
+    int64_t d4aaaa = -1, d4aaab = -1, d4aabb = -1, d4bbba = -1, d4bbbb = -1;
+    // quartets (basis.cc:747-900): aaaa i<j<k<l, aaab i<j<k with any l, aabb
+    // i<j with k<l; numbers at ((a n + b) n + c) n + d for every order the
+    // reference maps to the same quartet, -999 otherwise
+    int quad_aaaa = 0, quad_aaab = 0, quad_aabb = 0;
+    std::vector<int> ibas_aaaa, ibas_aaab, ibas_aabb;
     int64_t d2ab = -1, d2aa = -1, d2bb = -1, d200 = -1, d1a = -1, d1b = -1, q1a = -1, q1b = -1;
     int64_t q2ab = -1, q2aa = -1, q2bb = -1, g2ab = -1, g2ba = -1, g2aa = -1;
     int64_t n_primal = 0, n_dual = 0;

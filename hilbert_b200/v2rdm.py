@@ -31,6 +31,7 @@ DEFAULTS = {
     "CONSTRAIN_Q3": False,          # :235
     "CONSTRAIN_E3": False,          # :229
     "CONSTRAIN_F3": False,          # :232
+    "CONSTRAIN_D4": False,          # :303
     "TPDM_GUESS": "RANDOM",         # :205
     "SDP_SOLVER": "BPSDP",          # :246
     "HUBBARD_HAMILTONIAN": False,   # :249
@@ -92,14 +93,15 @@ class V2RDMProblem:
         self._lib = lib
         h = ctypes.c_void_p()
         pos, *extras = positivity.upper().split("+")
-        if pos not in _capi.POSITIVITY or not set(extras) <= {"D3", "Q3", "E3", "F3"}:
+        if pos not in _capi.POSITIVITY or not set(extras) <= {"D3", "Q3", "E3", "F3", "D4"}:
             raise ValueError(f"POSITIVITY {positivity} is not on the device path "
                              f"(supported: {sorted(_capi.POSITIVITY)}, each optionally "
-                             f"+D3 / +Q3 / +E3 / +F3)")
+                             f"+D3 / +Q3 / +E3 / +F3 / +D4)")
         code = (_capi.POSITIVITY[pos] | (_capi.V2B_CONSTRAIN_D3 if "D3" in extras else 0)
                 | (_capi.V2B_CONSTRAIN_Q3 if "Q3" in extras else 0)
                 | (_capi.V2B_CONSTRAIN_E3 if "E3" in extras else 0)
-                | (_capi.V2B_CONSTRAIN_F3 if "F3" in extras else 0))
+                | (_capi.V2B_CONSTRAIN_F3 if "F3" in extras else 0)
+                | (_capi.V2B_CONSTRAIN_D4 if "D4" in extras else 0))
         check(lib.v2b_problem_create(int(nmo), int(nalpha), int(nbeta), code,
                                      int(bool(constrain_spin)), int(bool(constrain_sz)),
                                      int(bool(hubbard_multiplicity)), ctypes.byref(h)))
@@ -422,7 +424,7 @@ class v2RDMHelper:
         o = self.options
         pos = (o.get("POSITIVITY") + ("+D3" if o.get("CONSTRAIN_D3") else "")
                + ("+Q3" if o.get("CONSTRAIN_Q3") else "") + ("+E3" if o.get("CONSTRAIN_E3") else "")
-               + ("+F3" if o.get("CONSTRAIN_F3") else ""))
+               + ("+F3" if o.get("CONSTRAIN_F3") else "") + ("+D4" if o.get("CONSTRAIN_D4") else ""))
         self.problem = V2RDMProblem(nmo, nalpha, nbeta, pos, o.get("CONSTRAIN_SPIN"),
                                     o.get("CONSTRAIN_SZ"), hubbard_multiplicity=self._hubbard)
         p = self.problem
@@ -481,8 +483,11 @@ def block_layout(nmo, nalpha, nbeta, positivity="DQG", constrain_spin=True):
         blocks += [("f3aaa", aab + aba), ("f3bbb", aab + aba), ("f3aab", aab), ("f3bba", aab)]
     if "Q3" in extras:
         blocks += [("q3aaa", aaa), ("q3bbb", aaa), ("q3aab", aab), ("q3bba", aab)]
-    if set(extras) & {"D3", "Q3", "E3", "F3"}:
+    if set(extras) & {"D3", "Q3", "E3", "F3", "D4"}:
         blocks += [("d3aaa", aaa), ("d3bbb", aaa), ("d3aab", aab), ("d3bba", aab)]
+    if "D4" in extras:
+        q4, q31, q22 = n * (n - 1) * (n - 2) * (n - 3) // 24, aaa * n, gaa * gaa
+        blocks += [("d4aaaa", q4), ("d4aaab", q31), ("d4aabb", q22), ("d4bbba", q31), ("d4bbbb", q4)]
     return blocks
 
 

@@ -51,6 +51,8 @@ extern "C" {
 #define V2B_CONSTRAIN_E3 64
 /* CONSTRAIN_F3 (f3.cc:45-836, 842-1623; implies D3) */
 #define V2B_CONSTRAIN_F3 128
+/* CONSTRAIN_D4 (d4.cc:44-297, 300-557; implies D3) */
+#define V2B_CONSTRAIN_D4 256
 
 /* libsdp::SDPOptions as hilbert fills it (src/v2rdm_casscf/v2rdm_solver.cc:426-431) */
 typedef struct {

@@ -19,7 +19,7 @@ BLOCK_NAMES = ("d2ab", "d2aa", "d2bb", "d200", "d1a", "d1b", "q1a", "q1b",
                "q2ab", "q2aa", "q2bb", "g2ab", "g2ba", "g2aa", "t2aaa", "t2bbb", "t2aab", "t2bba",
                "t1aaa", "t1bbb", "t1aab", "t1bba", "d3aaa", "d3bbb", "d3aab", "d3bba",
                "q3aaa", "q3bbb", "q3aab", "q3bba", "e3aaa", "e3bbb", "e3aab", "e3bba",
-               "f3aaa", "f3bbb", "f3aab", "f3bba")
+               "f3aaa", "f3bbb", "f3aab", "f3bba", "d4aaaa", "d4aaab", "d4aabb", "d4bbba", "d4bbbb")
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -112,10 +112,11 @@ class OracleProblem:
         self.positivity = positivity
         self.hubbard = hubbard
         base, *extras = positivity.split("+")
-        if not set(extras) <= {"D3", "Q3", "E3", "F3"}:
+        if not set(extras) <= {"D3", "Q3", "E3", "F3", "D4"}:
             raise ValueError(f"unknown constraint suffix in {positivity!r}")
         code = (POSITIVITY[base] | (16 if "D3" in extras else 0) | (32 if "Q3" in extras else 0)
-                | (64 if "E3" in extras else 0) | (128 if "F3" in extras else 0))
+                | (64 if "E3" in extras else 0) | (128 if "F3" in extras else 0)
+                | (256 if "D4" in extras else 0))
         p = lib.v2o_create(n, na, nb, code, int(constrain_spin),
                            int(constrain_sz), int(hubbard is not None))
         if not p:

@@ -149,7 +149,8 @@ class RefProblem : public v2RDMSolver {
             {"d3aab", d3aaboff}, {"d3bba", d3bbaoff}, {"q3aaa", q3aaaoff}, {"q3bbb", q3bbboff},
             {"q3aab", q3aaboff}, {"q3bba", q3bbaoff}, {"e3aaa", e3aaaoff}, {"e3bbb", e3bbboff},
             {"e3aab", e3aaboff}, {"e3bba", e3bbaoff}, {"f3aaa", f3aaaoff}, {"f3bbb", f3bbboff},
-            {"f3aab", f3aaboff}, {"f3bba", f3bbaoff}};
+            {"f3aab", f3aaboff}, {"f3bba", f3bbaoff}, {"d4aaaa", d4aaaaoff}, {"d4aaab", d4aaaboff},
+            {"d4aabb", d4aabboff}, {"d4bbba", d4bbbaoff}, {"d4bbbb", d4bbbboff}};
         auto it = m.find(name);
         if (it == m.end()) return -1;
         bool present = false;
@@ -162,6 +163,7 @@ class RefProblem : public v2RDMSolver {
         else if (name[0] == 'q' && name[1] == '3') present = constrain_q3_;
         else if (name[0] == 'e' && name[1] == '3') present = constrain_e3_;
         else if (name[0] == 'f' && name[1] == '3') present = constrain_f3_;
+        else if (name[0] == 'd' && name[1] == '4') present = constrain_d4_;
         else present = true;
         if (!present || it->second == nullptr) return -1;
         return it->second[0];
@@ -195,14 +197,14 @@ extern "C" {
 const char *v2b_ref_last_error() { return g_last_error.c_str(); }
 
 /* positivity: "D", "DQ", "DG", "DQG", "DQGT1", "DQGT2", "DQGT1T2", optionally followed by
- * "+D3", "+Q3", "+E3", "+F3" (CONSTRAIN_D3 / _Q3 / _E3 / _F3); guess_hf: 0 random, 1 HF */
+ * "+D3", "+Q3", "+E3", "+F3", "+D4" (CONSTRAIN_D3 / _Q3 / _E3 / _F3 / _D4); guess_hf: 0 random, 1 HF */
 void *v2b_ref_create(int nmo, int nalpha, int nbeta, const char *positivity, int constrain_spin,
                      int constrain_sz, int hubbard, double hub_t, double hub_u, const double *h,
                      const double *g, int guess_hf) {
     try {
         auto *opts = new Options();
         std::string pos(positivity);
-        bool d3 = false, q3 = false, e3 = false, f3 = false;
+        bool d3 = false, q3 = false, e3 = false, f3 = false, d4 = false;
         size_t plus = pos.find('+');
         const std::string base = pos.substr(0, plus);
         while (plus != std::string::npos) {
@@ -212,6 +214,7 @@ void *v2b_ref_create(int nmo, int nalpha, int nbeta, const char *positivity, int
             else if (tok == "Q3") q3 = true;
             else if (tok == "E3") e3 = true;
             else if (tok == "F3") f3 = true;
+            else if (tok == "D4") d4 = true;
             else throw std::invalid_argument("unknown constraint suffix");
             plus = next;
         }
@@ -220,6 +223,7 @@ void *v2b_ref_create(int nmo, int nalpha, int nbeta, const char *positivity, int
         opts->set_bool("CONSTRAIN_Q3", q3);
         opts->set_bool("CONSTRAIN_E3", e3);
         opts->set_bool("CONSTRAIN_F3", f3);
+        opts->set_bool("CONSTRAIN_D4", d4);
         opts->set_bool("CONSTRAIN_SPIN", constrain_spin != 0);
         opts->set_bool("CONSTRAIN_SZ", constrain_sz != 0);
         opts->set_str("GPC_CONSTRAINTS", "NONE");

@@ -9,7 +9,7 @@
  * restates (paths relative to the hilbert source tree).
  *
  * Supported constraint sets: POSITIVITY D / DQ / DG / DQG / DQGT1 / DQGT2 /
- * DQGT1T2, each optionally with CONSTRAIN_D3, _Q3, _E3 and _F3, with
+ * DQGT1T2, each optionally with CONSTRAIN_D3, _Q3, _E3, _F3 and _D4, with
  * CONSTRAIN_SPIN and CONSTRAIN_SZ on or off, singlet and non-singlet.
  */
 #include <math.h>
@@ -19,19 +19,22 @@
 typedef struct {
     int n;            /* active orbitals (amo_) */
     int na, nb;       /* alpha / beta electrons */
-    int q2, g2, t1, t2, d3, q3, e3, f3, spin, sz;
+    int q2, g2, t1, t2, d3, q3, e3, f3, d4, spin, sz;
     int mult;         /* 2S+1 as the reference stores it */
     int gab, gaa;
     int *bas_ab, *ibas_ab, *bas_aa, *ibas_aa;
     long d2ab, d2aa, d2bb, d200, d1a, d1b, q1a, q1b, q2ab, q2aa, q2bb, g2ab, g2ba, g2aa;
     long t1aaa, t1bbb, t1aab, t1bba, t2aaa, t2bbb, t2aab, t2bba, d3aaa, d3bbb, d3aab, d3bba;
     long q3aaa, q3bbb, q3aab, q3bba, e3aaa, e3bbb, e3aab, e3bba, f3aaa, f3bbb, f3aab, f3bba;
+    long d4aaaa, d4aaab, d4aabb, d4bbba, d4bbbb;
+    int quad_aaaa, quad_aaab, quad_aabb;            /* quartets: i<j<k<l; i<j<k, l; i<j, k<l */
+    int *ibas_aaaa, *ibas_aaab, *ibas_aabb;         /* n^4 each */
     int trip_aaa, trip_aab, trip_aba;   /* triplets (i<j<k), (i<j, k) and (i, j, k) */
     int *bas_aaa, *bas_aab, *bas_aba;   /* 3 ints per triplet */
     int *ibas_aaa, *ibas_aab;           /* n^3: any order of an aaa set / of the aa pair */
     long n_primal, n_dual;
     int nblocks;
-    int dims[64];     /* at most 46 blocks: every family of the reference on */
+    int dims[64];     /* at most 51 blocks: every family of the reference on */
 } v2o_problem;
 
 /* basis.cc:426-533 (C1): geminal (j,i) is pushed for i outer, j inner, so
@@ -77,6 +80,14 @@ static void t1_like_visit(const v2o_problem *p, long off, int mode, const double
 static void t2_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
                      double *x);
 static void d3_visit(const v2o_problem *p, long off, int mode, const double *u, double *A);
+static void d4_visit(const v2o_problem *p, long off, int mode, const double *u, double *A);
+/* number of D3 rows (v2rdm_solver.cc:3624-3660) */
+static long d3_rows_count(const v2o_problem *p) {
+    const long gaa = p->gaa, gab = p->gab, t3 = p->trip_aaa, ta = p->trip_aab;
+    long d = p->sz ? 4 * gaa * gaa + 2 * gab * gab : 2 * gaa * gaa + gab * gab;
+    if (p->spin && p->na == p->nb) d += ta * ta + 2 * t3 * t3;
+    return d;
+}
 
 /* v2rdm_solver.cc:3729-4079 (set_primal_offsets) and 3294-3727 (sizes) */
 static void set_offsets(v2o_problem *p) {
@@ -161,6 +172,16 @@ static void set_offsets(v2o_problem *p) {
         p->d3aab = off; off += ta * ta; p->dims[nb++] = (int)ta;
         p->d3bba = off; off += ta * ta; p->dims[nb++] = (int)ta;
     }
+    /* v2rdm_solver.cc:4030-4061: D4aaaa, D4aaab, D4aabb, D4bbba, D4bbbb */
+    p->d4aaaa = p->d4aaab = p->d4aabb = p->d4bbba = p->d4bbbb = -1;
+    if (p->d4) {
+        long q4 = p->quad_aaaa, q31 = p->quad_aaab, q22 = p->quad_aabb;
+        p->d4aaaa = off; off += q4 * q4; p->dims[nb++] = (int)q4;
+        p->d4aaab = off; off += q31 * q31; p->dims[nb++] = (int)q31;
+        p->d4aabb = off; off += q22 * q22; p->dims[nb++] = (int)q22;
+        p->d4bbba = off; off += q31 * q31; p->dims[nb++] = (int)q31;
+        p->d4bbbb = off; off += q4 * q4; p->dims[nb++] = (int)q4;
+    }
     p->n_primal = off;
     p->nblocks = nb;
     if (nb > (int)(sizeof(p->dims) / sizeof(p->dims[0]))) abort();
@@ -203,6 +224,17 @@ static void set_offsets(v2o_problem *p) {
         d += p->sz ? 4L * gaa * gaa + 2L * gab * gab : 2L * gaa * gaa + (long)gab * gab;
         if (p->spin && p->na == p->nb) d += ta * ta + 2 * t3 * t3;
     }
+    if (p->d4) {   /* v2rdm_solver.cc:3678-3707 */
+        long t3 = p->trip_aaa, ta = p->trip_aab;
+        if (p->na > 3) d += t3 * t3;
+        if (p->na > 2 && p->nb > 0) d += t3 * t3 + ta * ta;
+        /* counted twice by the reference (v2rdm_solver.cc:3692-3707) but written
+         * once by D4_constraints_Au: the second 2 aab^2 rows stay empty, at the
+         * end of the dual vector, and the dual vector keeps the reference's length */
+        if (p->na > 1 && p->nb > 1) d += 4 * ta * ta;
+        if (p->na > 0 && p->nb > 2) d += t3 * t3 + ta * ta;
+        if (p->nb > 3) d += t3 * t3;
+    }
     p->n_dual = d;
 }
 
@@ -241,15 +273,63 @@ static void build_triplets(v2o_problem *p) {
     p->trip_aba = cb;
 }
 
+/* basis.cc:747-900 (C1): quartets (i, j, k, l) in lexicographic order; aabb
+ * those with i < j and k < l (either order within each pair maps to it),
+ * aaab those with i < j < k (any order of the first three), aaaa those with
+ * i < j < k < l (any order). */
+static void build_quartets(v2o_problem *p) {
+    const int n = p->n;
+    const long n4 = (long)n * n * n * n;
+    p->ibas_aaaa = (int *)malloc(sizeof(int) * (n4 > 0 ? n4 : 1));
+    p->ibas_aaab = (int *)malloc(sizeof(int) * (n4 > 0 ? n4 : 1));
+    p->ibas_aabb = (int *)malloc(sizeof(int) * (n4 > 0 ? n4 : 1));
+    for (long e = 0; e < n4; e++) p->ibas_aaaa[e] = p->ibas_aaab[e] = p->ibas_aabb[e] = -999;
+#define Q4(a, b, c, d) ((((long)(a) * n + (b)) * n + (c)) * n + (d))
+    int c4 = 0, c31 = 0, c22 = 0;
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++)
+            for (int k = 0; k < n; k++)
+                for (int l = 0; l < n; l++) {
+                    if (i < j && k < l) {
+                        p->ibas_aabb[Q4(i, j, k, l)] = p->ibas_aabb[Q4(j, i, k, l)] = c22;
+                        p->ibas_aabb[Q4(i, j, l, k)] = p->ibas_aabb[Q4(j, i, l, k)] = c22;
+                        c22++;
+                    }
+                    if (i < j && j < k) {
+                        const int t[3] = {i, j, k};
+                        for (int a = 0; a < 3; a++)
+                            for (int b = 0; b < 3; b++)
+                                if (b != a) p->ibas_aaab[Q4(t[a], t[b], t[3 - a - b], l)] = c31;
+                        c31++;
+                    }
+                    if (i < j && j < k && k < l) {
+                        const int t[4] = {i, j, k, l};
+                        for (int a = 0; a < 4; a++)
+                            for (int b = 0; b < 4; b++)
+                                for (int c = 0; c < 4; c++) {
+                                    if (b == a || c == a || c == b) continue;
+                                    p->ibas_aaaa[Q4(t[a], t[b], t[c], t[6 - a - b - c])] = c4;
+                                }
+                        c4++;
+                    }
+                }
+#undef Q4
+    p->quad_aaaa = c4;
+    p->quad_aaab = c31;
+    p->quad_aabb = c22;
+}
+
 /* positivity: 0 D, 1 DQ, 2 DG, 3 DQG, 4 DQGT2, 5 DQGT1, 6 DQGT1T2 (= DQGT)
  * (v2rdm_solver.cc:4081-4118), plus 16 for CONSTRAIN_D3 (:4120-4122) and 32 for
  * CONSTRAIN_Q3 (which implies D3, :4132-4135), 64 for CONSTRAIN_E3 (implies D3,
- * :4124-4127) and 128 for CONSTRAIN_F3 (implies D3, :4128-4131).
+ * :4124-4127), 128 for CONSTRAIN_F3 (implies D3, :4128-4131) and 256 for
+ * CONSTRAIN_D4 (implies D3, :4144-4149).
  * hubbard selects the multiplicity convention of
  * v2rdm_solver.cc:862-863 (Hubbard) versus :983-984 (external). */
 v2o_problem *v2o_create(int n, int na, int nb, int positivity, int spin, int sz, int hubbard) {
     const int q3 = (positivity >> 5) & 1, e3 = (positivity >> 6) & 1, f3 = (positivity >> 7) & 1;
-    const int d3 = ((positivity >> 4) & 1) | q3 | e3 | f3;
+    const int d4 = (positivity >> 8) & 1;
+    const int d3 = ((positivity >> 4) & 1) | q3 | e3 | f3 | d4;
     positivity &= 15;
     if (n < 1 || na < 0 || nb < 0 || na > n || nb > n || positivity < 0 || positivity > 6) return NULL;
     v2o_problem *p = (v2o_problem *)calloc(1, sizeof(v2o_problem));
@@ -258,6 +338,7 @@ v2o_problem *v2o_create(int n, int na, int nb, int positivity, int spin, int sz,
     p->q3 = q3;
     p->e3 = e3;
     p->f3 = f3;
+    p->d4 = d4;
     p->q2 = (positivity == 1 || positivity >= 3);
     p->g2 = (positivity >= 2);
     p->t1 = (positivity == 5 || positivity == 6);
@@ -270,6 +351,7 @@ v2o_problem *v2o_create(int n, int na, int nb, int positivity, int spin, int sz,
     p->mult = hubbard ? 2 * (na - nb) + 1 : (na - nb) + 1;
     build_tables(p);
     if (p->t1 || p->t2 || p->d3) build_triplets(p);
+    if (p->d4) build_quartets(p);
     set_offsets(p);
     return p;
 }
@@ -278,6 +360,7 @@ void v2o_destroy(v2o_problem *p) {
     if (!p) return;
     free(p->bas_ab); free(p->ibas_ab); free(p->bas_aa); free(p->ibas_aa);
     free(p->bas_aaa); free(p->bas_aab); free(p->bas_aba); free(p->ibas_aaa); free(p->ibas_aab);
+    free(p->ibas_aaaa); free(p->ibas_aaab); free(p->ibas_aabb);
     free(p);
 }
 
@@ -294,12 +377,13 @@ void v2o_tables(const v2o_problem *p, int *bas_ab, int *ibas_ab, int *bas_aa, in
 }
 /* block offsets in the order d2ab d2aa d2bb d200 d1a d1b q1a q1b q2ab q2aa q2bb g2ab g2ba g2aa */
 void v2o_offsets(const v2o_problem *p, long *o) {
-    long v[38] = {p->d2ab, p->d2aa, p->d2bb, p->d200, p->d1a, p->d1b, p->q1a,
+    long v[43] = {p->d2ab, p->d2aa, p->d2bb, p->d200, p->d1a, p->d1b, p->q1a,
                   p->q1b,  p->q2ab, p->q2aa, p->q2bb, p->g2ab, p->g2ba, p->g2aa,
                   p->t2aaa, p->t2bbb, p->t2aab, p->t2bba,
                   p->t1aaa, p->t1bbb, p->t1aab, p->t1bba, p->d3aaa, p->d3bbb, p->d3aab, p->d3bba,
                   p->q3aaa, p->q3bbb, p->q3aab, p->q3bba, p->e3aaa, p->e3bbb, p->e3aab, p->e3bba,
-                  p->f3aaa, p->f3bbb, p->f3aab, p->f3bba};
+                  p->f3aaa, p->f3bbb, p->f3aab, p->f3bba, p->d4aaaa, p->d4aaab, p->d4aabb,
+                  p->d4bbba, p->d4bbbb};
     memcpy(o, v, sizeof(v));
 }
 
@@ -1019,6 +1103,95 @@ static void d3_visit(const v2o_problem *p, long off, int mode, const double *u, 
     }
 }
 
+/* ------------------------------------------------------------- D4 ---- */
+/* CONSTRAIN_D4 rows of d4.cc:44-297 (scatter :300-557): contractions of the
+ * 4-RDM to the 3-RDM, each family present only when the electron counts
+ * allow it.  A row: count x D3 element - sum_p (sign) D4 element, the sign
+ * the parity of the positions p passes when inserted into the sets. */
+static void d4_visit(const v2o_problem *p, long off, int mode, const double *u, double *A) {
+    const int n = p->n;
+    const long t3 = p->trip_aaa, ta = p->trip_aab;
+    const long q4 = p->quad_aaaa, q31 = p->quad_aaab, q22 = p->quad_aabb;
+    const double na = p->na, nb = p->nb;
+    d3_row r;
+    r.p = p; r.mode = mode; r.u = u; r.A = A; r.row = off; r.nt = 0;
+#define I4(tab, a, b, c, d) (p->tab[(((long)(a) * n + (b)) * n + (c)) * n + (d)])
+#define LT(q, x) ((q) < (x) ? -1.0 : 1.0)
+    /* families in the reference's order: aaaa->aaa (d4.cc:48-85); aaab->aaa,
+     * aaab->aab (:86-148); aabb->aab, aabb->bba (:149-199); bbba->bbb,
+     * bbba->bba (:200-257); bbbb->bbb (:258-295) */
+    for (int fam = 0; fam < 8; fam++) {
+        int on;
+        switch (fam) {
+        case 0: on = p->na > 3; break;
+        case 1: case 2: on = p->na > 2 && p->nb > 0; break;
+        case 3: case 4: on = p->na > 1 && p->nb > 1; break;
+        case 5: case 6: on = p->na > 0 && p->nb > 2; break;
+        default: on = p->nb > 3; break;
+        }
+        if (!on) continue;
+        const int rows_aaa = (fam == 0 || fam == 1 || fam == 5 || fam == 7);
+        const long nr = rows_aaa ? t3 : ta;
+        const int *tb = rows_aaa ? p->bas_aaa : p->bas_aab;
+        for (long x = 0; x < nr; x++) {
+            const int i = tb[3 * x], j = tb[3 * x + 1], k = tb[3 * x + 2];
+            for (long y = 0; y < nr; y++) {
+                const int l = tb[3 * y], m = tb[3 * y + 1], q = tb[3 * y + 2];
+                const long e = x * nr + y;
+                switch (fam) {
+                case 0:
+                case 7: {
+                    d3_add(&r, (fam ? p->d3bbb : p->d3aaa) + e, fam ? nb - 3.0 : na - 3.0);
+                    for (int s = 0; s < n; s++) {
+                        if (s == i || s == j || s == k || s == l || s == m || s == q) continue;
+                        const double sg = LT(s, i) * LT(s, j) * LT(s, k) * LT(s, l) * LT(s, m) * LT(s, q);
+                        d3_add(&r, (fam ? p->d4bbbb : p->d4aaaa) + (long)I4(ibas_aaaa, i, j, k, s) * q4
+                                   + I4(ibas_aaaa, l, m, q, s), -sg);
+                    }
+                    break;
+                }
+                case 1:
+                case 5:
+                    d3_add(&r, (fam == 5 ? p->d3bbb : p->d3aaa) + e, fam == 5 ? na : nb);
+                    for (int s = 0; s < n; s++)
+                        d3_add(&r, (fam == 5 ? p->d4bbba : p->d4aaab) + (long)I4(ibas_aaab, i, j, k, s) * q31
+                                   + I4(ibas_aaab, l, m, q, s), -1.0);
+                    break;
+                case 2:
+                case 6:
+                    d3_add(&r, (fam == 6 ? p->d3bba : p->d3aab) + e, fam == 6 ? nb - 2.0 : na - 2.0);
+                    for (int s = 0; s < n; s++) {
+                        if (s == i || s == j || s == l || s == m) continue;
+                        const double sg = LT(s, i) * LT(s, j) * LT(s, l) * LT(s, m);
+                        d3_add(&r, (fam == 6 ? p->d4bbba : p->d4aaab) + (long)I4(ibas_aaab, i, j, s, k) * q31
+                                   + I4(ibas_aaab, l, m, s, q), -sg);
+                    }
+                    break;
+                case 3:
+                    d3_add(&r, p->d3aab + e, nb - 1.0);
+                    for (int s = 0; s < n; s++) {
+                        if (s == k || s == q) continue;
+                        d3_add(&r, p->d4aabb + (long)I4(ibas_aabb, i, j, k, s) * q22 + I4(ibas_aabb, l, m, q, s),
+                               -(LT(s, k) * LT(s, q)));
+                    }
+                    break;
+                case 4:
+                    d3_add(&r, p->d3bba + e, na - 1.0);
+                    for (int s = 0; s < n; s++) {
+                        if (s == k || s == q) continue;
+                        d3_add(&r, p->d4aabb + (long)I4(ibas_aabb, k, s, i, j) * q22 + I4(ibas_aabb, q, s, l, m),
+                               -(LT(s, k) * LT(s, q)));
+                    }
+                    break;
+                }
+                d3_emit(&r);
+            }
+        }
+    }
+#undef I4
+#undef LT
+}
+
 /* ------------------------------------------------------------- A.x ---- */
 /* v2rdm_solver.cc:2995-3050 (bpsdp_Au) -> d2.cc:314-594, spin.cc:276-508,
  * q2.cc:170-318, g2.cc:245-442 */
@@ -1382,7 +1555,11 @@ void v2o_Au(const v2o_problem *p, const double *u, double *A) {
         t1_like_visit(p, off, T2_AU, u, A, NULL, 1);
         off += 2L * p->trip_aab * p->trip_aab + 2L * p->trip_aaa * p->trip_aaa;
     }
-    if (p->d3) d3_visit(p, off, T2_AU, u, A);   /* v2rdm_solver.cc:3036-3038 */
+    if (p->d3) {   /* v2rdm_solver.cc:3036-3038 */
+        d3_visit(p, off, T2_AU, u, A);
+        off += d3_rows_count(p);
+    }
+    if (p->d4) d4_visit(p, off, T2_AU, u, A);   /* v2rdm_solver.cc:3040-3042 */
 }
 
 /* ----------------------------------------------------------- A^T.y ---- */
@@ -1737,5 +1914,9 @@ void v2o_ATu(const v2o_problem *p, const double *u, double *A) {
         t1_like_visit(p, off, T2_ATU, u, A, NULL, 1);
         off += 2L * p->trip_aab * p->trip_aab + 2L * p->trip_aaa * p->trip_aaa;
     }
-    if (p->d3) d3_visit(p, off, T2_ATU, u, A);   /* v2rdm_solver.cc:3094-3096 */
+    if (p->d3) {   /* v2rdm_solver.cc:3094-3096 */
+        d3_visit(p, off, T2_ATU, u, A);
+        off += d3_rows_count(p);
+    }
+    if (p->d4) d4_visit(p, off, T2_ATU, u, A);   /* v2rdm_solver.cc:3098-3100 */
 }

@@ -36,6 +36,7 @@ CASES = [
     ("ext3_dqg_q3_doublet", 3, 2, 1, "DQG+Q3", True, True, None),
     ("hub3_d_e3", 3, 1, 1, "D+E3", True, True, (1.0, 4.0)),
     ("ext3_d_f3_doublet", 3, 2, 1, "D+F3", True, True, None),
+    ("ext4_d_d4_quartet", 4, 4, 3, "D+D4", True, True, None),
 ]
 
 

@@ -18,7 +18,8 @@ def gpu_problem(kw):
                                   "ext4_dq_nosz", "ext4_dg_doublet", "ext5_dqg", "ext1_dqg",
                                   "hub3_dqgt2", "ext3_dqgt2_doublet", "hub4_dqgt1",
                                   "ext4_dqgt1t2_doublet", "hub4_dqg_d3", "ext3_d_d3_nosz_doublet",
-                                  "ext3_dqg_q3_doublet", "hub3_d_e3", "ext3_d_f3_doublet"])
+                                  "ext3_dqg_q3_doublet", "hub3_d_e3", "ext3_d_f3_doublet",
+                                  "ext4_d_d4_quartet"])
 def test_maps_bit_exact_golden(golden, cuda_device, name):
     import torch
     case = golden[name]

@@ -68,7 +68,7 @@ def test_header_symbols_exported():
                                   "ext4_dq_nosz", "ext4_dg_doublet", "ext1_dqg", "hub3_dqgt2",
                                   "ext3_dqgt2_doublet", "hub4_dqgt1", "ext4_dqgt1t2_doublet",
                                   "hub4_dqg_d3", "ext3_d_d3_nosz_doublet", "ext3_dqg_q3_doublet",
-                                  "hub3_d_e3", "ext3_d_f3_doublet"])
+                                  "hub3_d_e3", "ext3_d_f3_doublet", "ext4_d_d4_quartet"])
 def test_host_problem_matches_golden(golden, name):
     case = golden[name]
     kw = case_kwargs(case)
@@ -94,7 +94,8 @@ def test_layout_helper_matches_library():
                  (4, 2, 1, "DG", True), (3, 2, 1, "DQGT2", True), (4, 2, 2, "DQGT1", True),
                  (4, 2, 1, "DQGT1T2", True), (3, 1, 1, "DQGT", False), (4, 2, 2, "DQG+D3", True),
                  (3, 2, 1, "D+D3", False), (3, 2, 1, "DQG+Q3", True), (3, 1, 1, "DQGT1+D3+Q3", True),
-                 (3, 2, 1, "D+E3", True), (3, 2, 1, "DQGT1T2+Q3+E3+F3", True)]:
+                 (3, 2, 1, "D+E3", True), (3, 2, 1, "DQGT1T2+Q3+E3+F3", True), (5, 4, 3, "DQG+D4", True),
+                 (4, 2, 2, "DQGT1T2+D4", False)]:
         p = hb.V2RDMProblem(args[0], args[1], args[2], args[3], args[4])
         assert [d for _, d in hb.block_layout(*args)] == list(p.dims)
 
@@ -131,7 +132,8 @@ def test_config5_sizes_match_the_oracle():
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libv2rdm_ref.so")),
                     reason="oracle/_ref not built")
-@pytest.mark.parametrize("pos", ["DQGT1T2", "DQG+D3", "DQGT2+Q3", "DQG+E3", "DQGT1T2+D3+Q3+E3+F3"])
+@pytest.mark.parametrize("pos", ["DQGT1T2", "DQG+D3", "DQGT2+Q3", "DQG+E3", "DQGT1T2+D3+Q3+E3+F3",
+                                 "DQG+D4"])
 def test_triplet_families_bit_exact_against_reference_grid(pos):
     """T1 and T2 together (DQGT1T2), and D3 (CONSTRAIN_D3): sizes, b, c, both
     guesses and the packed A / A^T, against hilbert's compiled code, n = 1..3."""

@@ -22,7 +22,8 @@ def test_golden_cases_present(golden):
                                   "ext4_dq_nosz", "ext4_dg_doublet", "ext5_dqg", "ext1_dqg",
                                   "hub3_dqgt2", "ext3_dqgt2_doublet", "hub4_dqgt1",
                                   "ext4_dqgt1t2_doublet", "hub4_dqg_d3", "ext3_d_d3_nosz_doublet",
-                                  "ext3_dqg_q3_doublet", "hub3_d_e3", "ext3_d_f3_doublet"])
+                                  "ext3_dqg_q3_doublet", "hub3_d_e3", "ext3_d_f3_doublet",
+                                  "ext4_d_d4_quartet"])
 def test_oracle_matches_golden(golden, name):
     case = golden[name]
     kw = case_kwargs(case)
@@ -163,3 +164,22 @@ def test_q3_without_q2_and_g2_is_refused():
     blocks that do not exist, so the combination is refused."""
     with pytest.raises(ValueError):
         OracleProblem(3, 1, 1, "D+Q3", True, True, h=np.eye(3), g=np.zeros((3,) * 4))
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+def test_oracle_d4_bit_exact_against_reference_grid():
+    """CONSTRAIN_D4 (d4.cc) with every electron-count gate of its families
+    (n = 1..5, nalpha, nbeta = 0..4), and every family of the reference at
+    once; the reference's dual count includes the aabb family twice, and so
+    does the oracle's (empty trailing rows)."""
+    rng = np.random.default_rng(91)
+    for pos in ("D+D4", "DQGT1T2+Q3+E3+F3+D4"):
+        for n, na, nb, spin, sz in itertools.product([1, 2, 3, 4, 5], range(5), range(5), [0, 1], [0, 1]):
+            if na > n or nb > n or (pos != "D+D4" and (n > 4 or spin != sz)):
+                continue
+            kw = dict(h=rng.standard_normal((n, n)), g=rng.standard_normal((n,) * 4))
+            r = RefProblem(n, na, nb, pos, spin, sz, **kw)
+            o = OracleProblem(n, na, nb, pos, spin, sz, **kw)
+            assert (r.n_primal, r.n_dual) == (o.n_primal, o.n_dual) and list(r.dims) == list(o.dims)
+            x, y = rng.standard_normal(r.n_primal), rng.standard_normal(r.n_dual)
+            assert same(r.Au(x), o.Au(x)) and same(r.ATu(y), o.ATu(y))
