@@ -195,3 +195,25 @@ def test_active_active_hessian_block_and_step_follow_the_oracle(small_casscf):
     assert len(hist) == len(histo)
     assert all(abs(a[0] - b[0]) <= 1e-9 and a[3] == b[3] for a, b in zip(hist, histo))
     assert np.max(np.abs(U.numpy() - Uo)) <= 1e-9
+
+
+@needs_ref
+def test_casscf_macro_iterations_with_the_focas_step():
+    """casscf(..., orbital_step="focas") on the CPU with the oracle's active
+    solve (hilbert's compiled maps + the numpy BPSDP): the orbital step lowers
+    the energy the next SDP solve starts from."""
+    nc, na_ = 2, 4
+    h_mo, B_mo, *_ = ho.casscf_df_problem(nbf=8, naux=12, ncore=nc, nact=na_)
+
+    def solve_active(h_act, g_act):
+        r = RefProblem(na_, 2, 2, "DQG", True, True, h=h_act.numpy(), g=g_act.numpy())
+        x, _ = run_v2rdm(r, r.x0, SDPOptions(1e-6, 1e-6, 1e-9, 10000, 2000), 500)
+        d2p, d1p = r.pack_spatial_density(x)
+        return float(r.c @ x), torch.from_numpy(d2p), torch.from_numpy(d1p)
+
+    E, gn, h1, B1 = ho.casscf(torch.from_numpy(h_mo), torch.from_numpy(B_mo), nc, na_, solve_active,
+                              macro_iterations=2, orbital_step="focas")
+    assert E[1] < E[0] - 0.5
+    n = h_mo.shape[0]
+    # the rotated integrals stay those of an orthogonal transformation
+    assert abs(float(torch.linalg.eigvalsh(h1).sum()) - float(np.trace(h_mo))) <= 1e-9 * n
