@@ -155,3 +155,20 @@ def test_triplet_families_bit_exact_against_reference_grid(pos):
         assert np.array_equal(packed_apply(rp, ent, pal, x), r.Au(x))
         rp, ent, pal = operator(p, True)
         assert np.array_equal(packed_apply(rp, ent, pal, y), r.ATu(y))
+
+
+def test_positivity_bits_are_checked_at_the_abi():
+    """v2b_problem_create takes POSITIVITY in the low four bits and the
+    CONSTRAIN_D3 / _Q3 / _E3 / _F3 / _D4 flags above; anything else is
+    BAD_ARG, and every flag brings the D3 blocks with it."""
+    lib = _capi.load()
+    h = ctypes.c_void_p()
+    assert lib.v2b_problem_create(3, 1, 1, 3 | 512, 1, 1, 0, ctypes.byref(h)) == _capi.V2B_BAD_ARG
+    assert lib.v2b_problem_create(3, 1, 1, 7, 1, 1, 0, ctypes.byref(h)) == _capi.V2B_BAD_ARG
+    assert lib.v2b_problem_create(3, 1, 1, -1, 1, 1, 0, ctypes.byref(h)) == _capi.V2B_BAD_ARG
+    for flag, name in ((_capi.V2B_CONSTRAIN_Q3, "q3"), (_capi.V2B_CONSTRAIN_E3, "e3"),
+                       (_capi.V2B_CONSTRAIN_F3, "f3"), (_capi.V2B_CONSTRAIN_D4, "d4")):
+        assert lib.v2b_problem_create(4, 2, 2, 3 | flag, 1, 1, 0, ctypes.byref(h)) == _capi.V2B_OK
+        names = [b for b, _ in hb.block_layout(4, 2, 2, "DQG+" + name.upper(), True)]
+        assert "d3aaa" in names and any(b.startswith(name) for b in names)
+        lib.v2b_problem_destroy(h)
