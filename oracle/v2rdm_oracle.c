@@ -72,7 +72,7 @@ static void build_tables(v2o_problem *p) {
 #define D3_AAA(a, b, c) (p->ibas_aaa[((long)(a) * p->n + (b)) * p->n + (c)])
 #define D3_AAB(a, b, c) (p->ibas_aab[((long)(a) * p->n + (b)) * p->n + (c)])
 
-enum { T2_AU = 0, T2_ATU = 1, T2_GUESS = 2 };
+enum { MODE_AU = 0, MODE_ATU = 1, MODE_GUESS = 2 };
 static void t1_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
                      double *x);
 static void t1_like_visit(const v2o_problem *p, long off, int mode, const double *u, double *A,
@@ -633,8 +633,8 @@ void v2o_guess_hf(const v2o_problem *p, double *x) {
     for (int i = occ; i < n; i++) x[p->q1b + i * n + i] = 1.0;
     if (p->q2) q2_guess(p, x);
     if (p->g2) g2_guess(p, x);
-    if (p->t1) t1_visit(p, 0, T2_GUESS, NULL, NULL, x);   /* v2rdm_solver.cc:1817-1819 */
-    if (p->t2) t2_visit(p, 0, T2_GUESS, NULL, NULL, x);   /* v2rdm_solver.cc:1820-1822 */
+    if (p->t1) t1_visit(p, 0, MODE_GUESS, NULL, NULL, x);   /* v2rdm_solver.cc:1817-1819 */
+    if (p->t2) t2_visit(p, 0, MODE_GUESS, NULL, NULL, x);   /* v2rdm_solver.cc:1820-1822 */
 }
 
 /* ------------------------------------------------------------- T2 ---- */
@@ -649,89 +649,89 @@ void v2o_guess_hf(const v2o_problem *p, double *x) {
  *   6-9 T2bbb: bbb/bbb, bbb/baa, baa/bbb, baa/baa t2.cc:1604-1840
  * ("aaa" rows/cols are the aab triplets, "abb" / "baa" the aba triplets,
  * placed after them in the big blocks). */
-typedef struct { long col; double coef; } t2_term;
+typedef struct { long col; double coef; } map_term;
 
 #define T2_D2AA(a, b, c, d) (p->d2aa + (long)IAA(p, a, b) * p->gaa + IAA(p, c, d))
 #define T2_D2BB(a, b, c, d) (p->d2bb + (long)IAA(p, a, b) * p->gaa + IAA(p, c, d))
 #define T2_D2AB(a, b, c, d) (p->d2ab + (long)IAB(p, a, b) * p->gab + IAB(p, c, d))
 #define T2_D1A(a, b) (p->d1a + (long)(a) * p->n + (b))
 #define T2_D1B(a, b) (p->d1b + (long)(a) * p->n + (b))
-#define T2_ADD(c, v) do { t[nt].col = (c); t[nt].coef = (v); nt++; } while (0)
+#define ADD_TERM(c, v) do { t[nt].col = (c); t[nt].coef = (v); nt++; } while (0)
 
 /* sign of an aa geminal read as (a, b): -1 when a > b (the reference's s) */
 static double pair_sign(int a, int b) { return a > b ? -1.0 : 1.0; }
 
 /* terms of row (i, j, k) x column (l, m, q) of sub-block sb, at most 7 */
 static int t2_terms(const v2o_problem *p, int sb, int i, int j, int k, int l, int m, int q,
-                    t2_term *t) {
+                    map_term *t) {
     int nt = 0;
     switch (sb) {
     case 0:   /* T2aab */
     case 1: { /* T2bba: the same terms with alpha and beta exchanged */
         const int b = sb == 1;
-        if (k == q) T2_ADD(b ? T2_D2BB(i, j, l, m) : T2_D2AA(i, j, l, m), 1.0);
-        if (j == m && i == l) T2_ADD(b ? T2_D1A(q, k) : T2_D1B(q, k), 1.0);
-        if (j == l && i == m) T2_ADD(b ? T2_D1A(q, k) : T2_D1B(q, k), -1.0);
-        if (i == l) T2_ADD(b ? T2_D2AB(q, j, k, m) : T2_D2AB(j, q, m, k), -1.0);
-        if (j == l) T2_ADD(b ? T2_D2AB(q, i, k, m) : T2_D2AB(i, q, m, k), 1.0);
-        if (i == m) T2_ADD(b ? T2_D2AB(q, j, k, l) : T2_D2AB(j, q, l, k), 1.0);
-        if (j == m) T2_ADD(b ? T2_D2AB(q, i, k, l) : T2_D2AB(i, q, l, k), -1.0);
+        if (k == q) ADD_TERM(b ? T2_D2BB(i, j, l, m) : T2_D2AA(i, j, l, m), 1.0);
+        if (j == m && i == l) ADD_TERM(b ? T2_D1A(q, k) : T2_D1B(q, k), 1.0);
+        if (j == l && i == m) ADD_TERM(b ? T2_D1A(q, k) : T2_D1B(q, k), -1.0);
+        if (i == l) ADD_TERM(b ? T2_D2AB(q, j, k, m) : T2_D2AB(j, q, m, k), -1.0);
+        if (j == l) ADD_TERM(b ? T2_D2AB(q, i, k, m) : T2_D2AB(i, q, m, k), 1.0);
+        if (i == m) ADD_TERM(b ? T2_D2AB(q, j, k, l) : T2_D2AB(j, q, l, k), 1.0);
+        if (j == m) ADD_TERM(b ? T2_D2AB(q, i, k, l) : T2_D2AB(i, q, l, k), -1.0);
         break;
     }
     case 2:   /* aaa/aaa */
     case 6: { /* bbb/bbb */
         const int b = sb == 6;
-        if (k == q) T2_ADD(b ? T2_D2BB(i, j, l, m) : T2_D2AA(i, j, l, m), 1.0);
-        if (j == m && i == l) T2_ADD(b ? T2_D1B(q, k) : T2_D1A(q, k), 1.0);
-        if (j == l && i == m) T2_ADD(b ? T2_D1B(q, k) : T2_D1A(q, k), -1.0);
+        if (k == q) ADD_TERM(b ? T2_D2BB(i, j, l, m) : T2_D2AA(i, j, l, m), 1.0);
+        if (j == m && i == l) ADD_TERM(b ? T2_D1B(q, k) : T2_D1A(q, k), 1.0);
+        if (j == l && i == m) ADD_TERM(b ? T2_D1B(q, k) : T2_D1A(q, k), -1.0);
         if (i == l && q != j && k != m)
-            T2_ADD(b ? T2_D2BB(q, j, k, m) : T2_D2AA(q, j, k, m), -pair_sign(q, j) * pair_sign(k, m));
+            ADD_TERM(b ? T2_D2BB(q, j, k, m) : T2_D2AA(q, j, k, m), -pair_sign(q, j) * pair_sign(k, m));
         if (j == l && q != i && k != m)
-            T2_ADD(b ? T2_D2BB(q, i, k, m) : T2_D2AA(q, i, k, m), pair_sign(q, i) * pair_sign(k, m));
+            ADD_TERM(b ? T2_D2BB(q, i, k, m) : T2_D2AA(q, i, k, m), pair_sign(q, i) * pair_sign(k, m));
         if (i == m && q != j && k != l)
-            T2_ADD(b ? T2_D2BB(q, j, k, l) : T2_D2AA(q, j, k, l), pair_sign(q, j) * pair_sign(k, l));
+            ADD_TERM(b ? T2_D2BB(q, j, k, l) : T2_D2AA(q, j, k, l), pair_sign(q, j) * pair_sign(k, l));
         if (j == m && q != i && k != l)
-            T2_ADD(b ? T2_D2BB(q, i, k, l) : T2_D2AA(q, i, k, l), -pair_sign(q, i) * pair_sign(k, l));
+            ADD_TERM(b ? T2_D2BB(q, i, k, l) : T2_D2AA(q, i, k, l), -pair_sign(q, i) * pair_sign(k, l));
         break;
     }
     case 3:   /* aaa/abb */
-        if (i == l) T2_ADD(T2_D2AB(j, q, k, m), 1.0);
-        if (j == l) T2_ADD(T2_D2AB(i, q, k, m), -1.0);
+        if (i == l) ADD_TERM(T2_D2AB(j, q, k, m), 1.0);
+        if (j == l) ADD_TERM(T2_D2AB(i, q, k, m), -1.0);
         break;
     case 7:   /* bbb/baa */
-        if (i == l) T2_ADD(T2_D2AB(q, j, m, k), 1.0);
-        if (j == l) T2_ADD(T2_D2AB(q, i, m, k), -1.0);
+        if (i == l) ADD_TERM(T2_D2AB(q, j, m, k), 1.0);
+        if (j == l) ADD_TERM(T2_D2AB(q, i, m, k), -1.0);
         break;
     case 4:   /* abb/aaa */
-        if (i == l) T2_ADD(T2_D2AB(q, j, m, k), 1.0);
-        if (i == m) T2_ADD(T2_D2AB(q, j, l, k), -1.0);
+        if (i == l) ADD_TERM(T2_D2AB(q, j, m, k), 1.0);
+        if (i == m) ADD_TERM(T2_D2AB(q, j, l, k), -1.0);
         break;
     case 8:   /* baa/bbb */
-        if (i == l) T2_ADD(T2_D2AB(j, q, k, m), 1.0);
-        if (i == m) T2_ADD(T2_D2AB(j, q, k, l), -1.0);
+        if (i == l) ADD_TERM(T2_D2AB(j, q, k, m), 1.0);
+        if (i == m) ADD_TERM(T2_D2AB(j, q, k, l), -1.0);
         break;
     case 5:   /* abb/abb */
-        if (k == q) T2_ADD(T2_D2AB(i, j, l, m), 1.0);
-        if (j == m && i == l) T2_ADD(T2_D1B(q, k), 1.0);
-        if (i == l && q != j && k != m) T2_ADD(T2_D2BB(q, j, k, m), -pair_sign(q, j) * pair_sign(k, m));
-        if (j == m) T2_ADD(T2_D2AB(i, q, l, k), -1.0);
+        if (k == q) ADD_TERM(T2_D2AB(i, j, l, m), 1.0);
+        if (j == m && i == l) ADD_TERM(T2_D1B(q, k), 1.0);
+        if (i == l && q != j && k != m) ADD_TERM(T2_D2BB(q, j, k, m), -pair_sign(q, j) * pair_sign(k, m));
+        if (j == m) ADD_TERM(T2_D2AB(i, q, l, k), -1.0);
         break;
     case 9:   /* baa/baa */
-        if (k == q) T2_ADD(T2_D2AB(j, i, m, l), 1.0);
-        if (j == m && i == l) T2_ADD(T2_D1A(q, k), 1.0);
-        if (i == l && q != j && k != m) T2_ADD(T2_D2AA(q, j, k, m), -pair_sign(q, j) * pair_sign(k, m));
-        if (j == m) T2_ADD(T2_D2AB(q, i, k, l), -1.0);
+        if (k == q) ADD_TERM(T2_D2AB(j, i, m, l), 1.0);
+        if (j == m && i == l) ADD_TERM(T2_D1A(q, k), 1.0);
+        if (i == l && q != j && k != m) ADD_TERM(T2_D2AA(q, j, k, m), -pair_sign(q, j) * pair_sign(k, m));
+        if (j == m) ADD_TERM(T2_D2AB(q, i, k, l), -1.0);
         break;
     }
     return nt;
 }
 
 /* Visit every T2 row in the reference's order, dual rows from off.
- *  T2_AU:    A[row] = -u[t2] + terms                       (t2.cc:1236-1843)
- *  T2_ATU:   A[t2] -= u[row], A[col] += coef u[row]         (t2.cc:3376-3966,
+ *  MODE_AU:    A[row] = -u[t2] + terms                       (t2.cc:1236-1843)
+ *  MODE_ATU:   A[t2] -= u[row], A[col] += coef u[row]         (t2.cc:3376-3966,
  *            the scatter of the same terms in the same order)
- *  T2_GUESS: u[t2] = 0 + terms, zero on aaa/abb             (t2.cc:1845-2452) */
-typedef int (*big_terms_fn)(const v2o_problem *, int, int, int, int, int, int, int, t2_term *);
+ *  MODE_GUESS: u[t2] = 0 + terms, zero on aaa/abb             (t2.cc:1845-2452) */
+typedef int (*big_terms_fn)(const v2o_problem *, int, int, int, int, int, int, int, map_term *);
 
 /* the T2 block layout (aab, bba, then the aab+aba blocks), rows led by
  * -X(r, c) for X in lead = {aab, bba, aaa, bbb} */
@@ -753,13 +753,13 @@ static void big_visit(const v2o_problem *p, long off, int mode, const double *u,
             for (long c = 0; c < nc; c++) {
                 const int l = cb[3 * c], m = cb[3 * c + 1], q = cb[3 * c + 2];
                 const long id = (r0 + r) * width + (c0 + c);
-                t2_term t[8];
+                map_term t[8];
                 const int nt = terms(p, sb, i, j, k, l, m, q, t);
-                if (mode == T2_AU) {
+                if (mode == MODE_AU) {
                     double dum = -u[prim[blk] + id];
                     for (int e = 0; e < nt; e++) dum += t[e].coef * u[t[e].col];
                     A[dual[blk] + id] = dum;
-                } else if (mode == T2_ATU) {
+                } else if (mode == MODE_ATU) {
                     const double dum = u[dual[blk] + id];
                     A[prim[blk] + id] -= dum;
                     for (int e = 0; e < nt; e++) A[t[e].col] += t[e].coef * dum;
@@ -785,7 +785,7 @@ static void t2_visit(const v2o_problem *p, long off, int mode, const double *u, 
  * column's: (i j n | l m k)) with a sign, then d_kn times a D2 element.
  * Sub-blocks as for T2. */
 static int e3_terms(const v2o_problem *p, int sb, int i, int j, int k, int l, int m, int q,
-                    t2_term *t) {
+                    map_term *t) {
     int nt = 0;
     const long ta = p->trip_aab, t3 = p->trip_aaa;
 #define E3_AB(base, a, b, c, d, e, f) ((base) + (long)D3_AAB(a, b, c) * ta + D3_AAB(d, e, f))
@@ -794,8 +794,8 @@ static int e3_terms(const v2o_problem *p, int sb, int i, int j, int k, int l, in
     case 0:
     case 1: {
         const int b = sb == 1;
-        T2_ADD(E3_AB(b ? p->d3bba : p->d3aab, i, j, q, l, m, k), -1.0);
-        if (k == q) T2_ADD(b ? T2_D2BB(i, j, l, m) : T2_D2AA(i, j, l, m), 1.0);
+        ADD_TERM(E3_AB(b ? p->d3bba : p->d3aab, i, j, q, l, m, k), -1.0);
+        if (k == q) ADD_TERM(b ? T2_D2BB(i, j, l, m) : T2_D2AA(i, j, l, m), 1.0);
         break;
     }
     case 2:
@@ -803,33 +803,33 @@ static int e3_terms(const v2o_problem *p, int sb, int i, int j, int k, int l, in
         const int b = sb == 6;
         if (i != q && j != q && l != k && m != k) {
             const double sg = ((i < q && q < j) ? -1.0 : 1.0) * ((l < k && k < m) ? -1.0 : 1.0);
-            T2_ADD(E3_AA3(b ? p->d3bbb : p->d3aaa, i, j, q, l, m, k), -sg);
+            ADD_TERM(E3_AA3(b ? p->d3bbb : p->d3aaa, i, j, q, l, m, k), -sg);
         }
-        if (k == q) T2_ADD(b ? T2_D2BB(i, j, l, m) : T2_D2AA(i, j, l, m), 1.0);
+        if (k == q) ADD_TERM(b ? T2_D2BB(i, j, l, m) : T2_D2AA(i, j, l, m), 1.0);
         break;
     }
     case 3:
-        if (i != j && l != k) T2_ADD(E3_AB(p->d3aab, i, j, q, l, k, m), l > k ? -1.0 : 1.0);
+        if (i != j && l != k) ADD_TERM(E3_AB(p->d3aab, i, j, q, l, k, m), l > k ? -1.0 : 1.0);
         break;
     case 7:
         if (i != j && l != k)
-            T2_ADD(E3_AB(p->d3bba, i, j, q, l, k, m), (i > j ? -1.0 : 1.0) * (l > k ? -1.0 : 1.0));
+            ADD_TERM(E3_AB(p->d3bba, i, j, q, l, k, m), (i > j ? -1.0 : 1.0) * (l > k ? -1.0 : 1.0));
         break;
     case 4:
-        if (i != q && l != m) T2_ADD(E3_AB(p->d3aab, i, q, j, l, m, k), i > q ? -1.0 : 1.0);
+        if (i != q && l != m) ADD_TERM(E3_AB(p->d3aab, i, q, j, l, m, k), i > q ? -1.0 : 1.0);
         break;
     case 8:
         if (i != q && l != m)
-            T2_ADD(E3_AB(p->d3bba, i, q, j, l, m, k), (i > q ? -1.0 : 1.0) * (l > m ? -1.0 : 1.0));
+            ADD_TERM(E3_AB(p->d3bba, i, q, j, l, m, k), (i > q ? -1.0 : 1.0) * (l > m ? -1.0 : 1.0));
         break;
     case 5:
     case 9: {
         const int b = sb == 9;
         if (j != q && m != k) {
             const double sg = (j > q ? -1.0 : 1.0) * (m > k ? -1.0 : 1.0);
-            T2_ADD(E3_AB(b ? p->d3aab : p->d3bba, j, q, i, m, k, l), -sg);
+            ADD_TERM(E3_AB(b ? p->d3aab : p->d3bba, j, q, i, m, k, l), -sg);
         }
-        if (k == q) T2_ADD(b ? T2_D2AB(j, i, m, l) : T2_D2AB(i, j, l, m), 1.0);
+        if (k == q) ADD_TERM(b ? T2_D2AB(j, i, m, l) : T2_D2AB(i, j, l, m), 1.0);
         break;
     }
     }
@@ -849,8 +849,8 @@ static void e3_visit(const v2o_problem *p, long off, int mode, const double *u, 
  * then E3's D3 element with the opposite sign, then T2's terms without the
  * d_kn D2 term that E3 carries (T2 = E3 + F3), all in the reference's order. */
 static int f3_terms(const v2o_problem *p, int sb, int i, int j, int k, int l, int m, int q,
-                    t2_term *t) {
-    t2_term e[8], w[8];
+                    map_term *t) {
+    map_term e[8], w[8];
     const int ne = e3_terms(p, sb, i, j, k, l, m, q, e);
     const int nw = t2_terms(p, sb, i, j, k, l, m, q, w);
     int nt = 0;
@@ -883,21 +883,21 @@ static void f3_visit(const v2o_problem *p, long off, int mode, const double *u, 
 #define T1_G2H(base, r, c) ((base) + (long)(r) * p->gab + (c))
 
 static int t1_terms(const v2o_problem *p, int sb, int i, int j, int k, int l, int m, int q,
-                    t2_term *t) {
+                    map_term *t) {
     int nt = 0;
     if (sb < 2) {   /* aab, bba */
         const int b = sb == 1;
         const long q2 = b ? p->q2bb : p->q2aa, g2 = b ? p->g2ab : p->g2ba;
-        if (k == q) T2_ADD(q2 + (long)IAA(p, i, j) * p->gaa + IAA(p, l, m), 1.0);
+        if (k == q) ADD_TERM(q2 + (long)IAA(p, i, j) * p->gaa + IAA(p, l, m), 1.0);
         if (b) {
-            if (j == l) T2_ADD(T2_D2AB(q, m, k, i), -1.0);
-            if (l == i) T2_ADD(T2_D2AB(q, m, k, j), 1.0);
+            if (j == l) ADD_TERM(T2_D2AB(q, m, k, i), -1.0);
+            if (l == i) ADD_TERM(T2_D2AB(q, m, k, j), 1.0);
         } else {
-            if (j == l) T2_ADD(T2_D2AB(m, q, i, k), -1.0);
-            if (l == i) T2_ADD(T2_D2AB(m, q, j, k), 1.0);
+            if (j == l) ADD_TERM(T2_D2AB(m, q, i, k), -1.0);
+            if (l == i) ADD_TERM(T2_D2AB(m, q, j, k), 1.0);
         }
-        if (j == m) T2_ADD(T1_G2H(g2, IAB(p, q, i), IAB(p, k, l)), -1.0);
-        if (i == m) T2_ADD(T1_G2H(g2, IAB(p, q, j), IAB(p, k, l)), 1.0);
+        if (j == m) ADD_TERM(T1_G2H(g2, IAB(p, q, i), IAB(p, k, l)), -1.0);
+        if (i == m) ADD_TERM(T1_G2H(g2, IAB(p, q, j), IAB(p, k, l)), 1.0);
         return nt;
     }
     /* aaa, bbb */
@@ -905,23 +905,23 @@ static int t1_terms(const v2o_problem *p, int sb, int i, int j, int k, int l, in
     const long q2 = b ? p->q2bb : p->q2aa, d2 = b ? p->d2bb : p->d2aa, d1 = b ? p->d1b : p->d1a;
     const int sh = b ? p->gab : 0;
 #define T1_AA(base, a, bb, c, d) ((base) + (long)IAA(p, a, bb) * p->gaa + IAA(p, c, d))
-    if (k == q) T2_ADD(T1_AA(q2, i, j, l, m), 1.0);
-    if (j == q) T2_ADD(T1_AA(q2, i, k, l, m), -1.0);
-    if (i == q) T2_ADD(T1_AA(q2, j, k, l, m), 1.0);
-    if (l == k) T2_ADD(T1_AA(d2, q, m, j, i), 1.0);
-    if (j == l) T2_ADD(T1_AA(d2, q, m, k, i), -1.0);
-    if (l == i) T2_ADD(T1_AA(d2, q, m, k, j), 1.0);
+    if (k == q) ADD_TERM(T1_AA(q2, i, j, l, m), 1.0);
+    if (j == q) ADD_TERM(T1_AA(q2, i, k, l, m), -1.0);
+    if (i == q) ADD_TERM(T1_AA(q2, j, k, l, m), 1.0);
+    if (l == k) ADD_TERM(T1_AA(d2, q, m, j, i), 1.0);
+    if (j == l) ADD_TERM(T1_AA(d2, q, m, k, i), -1.0);
+    if (l == i) ADD_TERM(T1_AA(d2, q, m, k, j), 1.0);
     if (k == m) {
-        if (j == l) T2_ADD(d1 + (long)q * p->n + i, -1.0);
-        T2_ADD(T1_G2S(IAB(p, q, i), IAB(p, j, l), sh), 1.0);
+        if (j == l) ADD_TERM(d1 + (long)q * p->n + i, -1.0);
+        ADD_TERM(T1_G2S(IAB(p, q, i), IAB(p, j, l), sh), 1.0);
     }
     if (j == m) {
-        if (k == l) T2_ADD(d1 + (long)q * p->n + i, 1.0);
-        T2_ADD(T1_G2S(IAB(p, q, i), IAB(p, k, l), sh), -1.0);
+        if (k == l) ADD_TERM(d1 + (long)q * p->n + i, 1.0);
+        ADD_TERM(T1_G2S(IAB(p, q, i), IAB(p, k, l), sh), -1.0);
     }
     if (i == m) {
-        if (k == l) T2_ADD(d1 + (long)q * p->n + j, -1.0);
-        T2_ADD(T1_G2S(IAB(p, q, j), IAB(p, k, l), sh), 1.0);
+        if (k == l) ADD_TERM(d1 + (long)q * p->n + j, -1.0);
+        ADD_TERM(T1_G2S(IAB(p, q, j), IAB(p, k, l), sh), 1.0);
     }
 #undef T1_AA
     return nt;
@@ -944,14 +944,14 @@ static void t1_like_visit(const v2o_problem *p, long off, int mode, const double
             for (long c = 0; c < nr; c++) {
                 const int l = tb[3 * c], m = tb[3 * c + 1], q = tb[3 * c + 2];
                 const long id = r * nr + c;
-                t2_term t[12];
+                map_term t[12];
                 const int nt = t1_terms(p, sb, i, j, k, l, m, q, t);
-                if (mode == T2_AU) {
+                if (mode == MODE_AU) {
                     double dum = -u[prim[sb] + id];
                     if (q3) dum -= u[prim2[sb] + id];
                     for (int e = 0; e < nt; e++) dum += t[e].coef * u[t[e].col];
                     A[dual[sb] + id] = dum;
-                } else if (mode == T2_ATU) {
+                } else if (mode == MODE_ATU) {
                     const double dum = u[dual[sb] + id];
                     A[prim[sb] + id] -= dum;
                     if (q3) A[prim2[sb] + id] -= dum;
@@ -993,7 +993,7 @@ typedef struct {
     double *A;
     long row;
     int nt;
-    t2_term t[64];
+    map_term t[64];
 } d3_row;
 
 static void d3_add(d3_row *r, long col, double coef) {
@@ -1003,7 +1003,7 @@ static void d3_add(d3_row *r, long col, double coef) {
 }
 
 static void d3_emit(d3_row *r) {
-    if (r->mode == T2_AU) {
+    if (r->mode == MODE_AU) {
         double dum = 0.0;
         for (int e = 0; e < r->nt; e++) dum += r->t[e].coef * r->u[r->t[e].col];
         r->A[r->row] = dum;
@@ -1533,33 +1533,33 @@ void v2o_Au(const v2o_problem *p, const double *u, double *A) {
         off += 4L * gab * gab;
     }
     if (p->t1) {   /* v2rdm_solver.cc:3015-3017 */
-        t1_visit(p, off, T2_AU, u, A, NULL);
+        t1_visit(p, off, MODE_AU, u, A, NULL);
         off += 2L * p->trip_aab * p->trip_aab + 2L * p->trip_aaa * p->trip_aaa;
     }
     if (p->t2) {   /* v2rdm_solver.cc:3019-3022 */
-        t2_visit(p, off, T2_AU, u, A, NULL);
+        t2_visit(p, off, MODE_AU, u, A, NULL);
         const long w = (long)p->trip_aab + p->trip_aba;
         off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
     }
     if (p->e3) {   /* v2rdm_solver.cc:3024-3026 */
-        e3_visit(p, off, T2_AU, u, A);
+        e3_visit(p, off, MODE_AU, u, A);
         const long w = (long)p->trip_aab + p->trip_aba;
         off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
     }
     if (p->f3) {   /* v2rdm_solver.cc:3028-3030 */
-        f3_visit(p, off, T2_AU, u, A);
+        f3_visit(p, off, MODE_AU, u, A);
         const long w = (long)p->trip_aab + p->trip_aba;
         off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
     }
     if (p->q3) {   /* v2rdm_solver.cc:3032-3034 */
-        t1_like_visit(p, off, T2_AU, u, A, NULL, 1);
+        t1_like_visit(p, off, MODE_AU, u, A, NULL, 1);
         off += 2L * p->trip_aab * p->trip_aab + 2L * p->trip_aaa * p->trip_aaa;
     }
     if (p->d3) {   /* v2rdm_solver.cc:3036-3038 */
-        d3_visit(p, off, T2_AU, u, A);
+        d3_visit(p, off, MODE_AU, u, A);
         off += d3_rows_count(p);
     }
-    if (p->d4) d4_visit(p, off, T2_AU, u, A);   /* v2rdm_solver.cc:3040-3042 */
+    if (p->d4) d4_visit(p, off, MODE_AU, u, A);   /* v2rdm_solver.cc:3040-3042 */
 }
 
 /* ----------------------------------------------------------- A^T.y ---- */
@@ -1892,31 +1892,31 @@ void v2o_ATu(const v2o_problem *p, const double *u, double *A) {
         off += 4L * gab * gab;
     }
     if (p->t1) {   /* v2rdm_solver.cc:3073-3075 */
-        t1_visit(p, off, T2_ATU, u, A, NULL);
+        t1_visit(p, off, MODE_ATU, u, A, NULL);
         off += 2L * p->trip_aab * p->trip_aab + 2L * p->trip_aaa * p->trip_aaa;
     }
     if (p->t2) {   /* v2rdm_solver.cc:3077-3080 */
-        t2_visit(p, off, T2_ATU, u, A, NULL);
+        t2_visit(p, off, MODE_ATU, u, A, NULL);
         const long w = (long)p->trip_aab + p->trip_aba;
         off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
     }
     if (p->e3) {   /* v2rdm_solver.cc:3082-3084 */
-        e3_visit(p, off, T2_ATU, u, A);
+        e3_visit(p, off, MODE_ATU, u, A);
         const long w = (long)p->trip_aab + p->trip_aba;
         off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
     }
     if (p->f3) {   /* v2rdm_solver.cc:3086-3088 */
-        f3_visit(p, off, T2_ATU, u, A);
+        f3_visit(p, off, MODE_ATU, u, A);
         const long w = (long)p->trip_aab + p->trip_aba;
         off += 2L * p->trip_aab * p->trip_aab + 2 * w * w;
     }
     if (p->q3) {   /* v2rdm_solver.cc:3090-3092 */
-        t1_like_visit(p, off, T2_ATU, u, A, NULL, 1);
+        t1_like_visit(p, off, MODE_ATU, u, A, NULL, 1);
         off += 2L * p->trip_aab * p->trip_aab + 2L * p->trip_aaa * p->trip_aaa;
     }
     if (p->d3) {   /* v2rdm_solver.cc:3094-3096 */
-        d3_visit(p, off, T2_ATU, u, A);
+        d3_visit(p, off, MODE_ATU, u, A);
         off += d3_rows_count(p);
     }
-    if (p->d4) d4_visit(p, off, T2_ATU, u, A);   /* v2rdm_solver.cc:3098-3100 */
+    if (p->d4) d4_visit(p, off, MODE_ATU, u, A);   /* v2rdm_solver.cc:3098-3100 */
 }
