@@ -172,3 +172,33 @@ def test_positivity_bits_are_checked_at_the_abi():
         names = [b for b, _ in hb.block_layout(4, 2, 2, "DQG+" + name.upper(), True)]
         assert "d3aaa" in names and any(b.startswith(name) for b in names)
         lib.v2b_problem_destroy(h)
+
+
+@pytest.mark.parametrize("pos,n,na,nb,spin,sz", [
+    ("DQGT1T2+D3+Q3+E3+F3+D4", 4, 3, 2, True, True), ("DQG+D4", 5, 4, 4, True, False),
+    ("D+E3+F3", 4, 2, 1, False, True), ("DQGT2+Q3", 3, 2, 2, True, True)])
+def test_packed_operators_are_adjoint(pos, n, na, nb, spin, sz):
+    """<A x, y> = <x, A^T y> for the packed A and A^T the library builds,
+    with every constraint family combination it supports."""
+    p = hb.V2RDMProblem(n, na, nb, pos, spin, sz)
+    rng = np.random.default_rng(n * 10 + na)
+    x, y = rng.standard_normal(p.n_primal), rng.standard_normal(p.n_dual)
+    rp, ent, pal = operator(p, False)
+    ax = packed_apply(rp, ent, pal, x)
+    rp, ent, pal = operator(p, True)
+    aty = packed_apply(rp, ent, pal, y)
+    lhs, rhs = float(ax @ y), float(x @ aty)
+    assert abs(lhs - rhs) <= 1e-10 * max(1.0, abs(lhs))
+
+
+def test_helper_options_select_the_constraint_families():
+    """hilbert's CONSTRAIN_D3 / _Q3 / _E3 / _F3 / _D4 options reach the problem
+    through v2RDMHelper, as set_constraints reads them."""
+    n = 4
+    h, g = np.eye(n), np.zeros((n,) * 4)
+    o = hb.Options({"POSITIVITY": "DQGT1", "CONSTRAIN_Q3": True, "CONSTRAIN_D4": True})
+    helper = hb.v2RDMHelper(2, 2, n, h, g, o)
+    want = [d for _, d in hb.block_layout(n, 2, 2, "DQGT1+Q3+D4", True)]
+    assert list(helper.problem.dims) == want
+    names = [b for b, _ in hb.block_layout(n, 2, 2, "DQGT1+Q3+D4", True)]
+    assert {"t1aaa", "q3aab", "d3bbb", "d4aabb"} <= set(names) and "e3aaa" not in names
