@@ -94,22 +94,30 @@ def solve_on_device(inst, options, device=None):
     """One instance through the device path from the RANDOM guess."""
     import torch
     dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
-    p, b, c = inst.problem()
-    try:
-        x = torch.from_numpy(p.guess("RANDOM")).to(dev)
-        st = p.solve_device(x, torch.from_numpy(b).to(dev), torch.from_numpy(c).to(dev), options)
-        energy = float(np.dot(c, x.cpu().numpy()))
-    finally:
-        p.close()
+    with torch.cuda.device(dev):
+        p, b, c = inst.problem()
+        try:
+            x = torch.from_numpy(p.guess("RANDOM")).to(dev)
+            st = p.solve_device(x, torch.from_numpy(b).to(dev), torch.from_numpy(c).to(dev), options)
+            energy = float(np.dot(c, x.cpu().numpy()))
+        finally:
+            p.close()
     return {"energy": energy, "converged": bool(st["converged"]), "oiter": int(st["oiter"]),
             "iiter": int(st["iiter"])}
 
 
-def solve_batch(instances, options=None, rank=0, world=1, group=None, solve=solve_on_device):
+def solve_batch(instances, options=None, rank=0, world=1, group=None, solve=solve_on_device,
+                concurrency=1):
     """Solve this rank's slice, then gather every rank's results on the host
     (torch.distributed.all_gather_object over `group`, which should be a
     gloo group when the default one is NCCL).  Returns the results of all
-    instances, ordered by index, each {"index", "rank", ...solve's dict}."""
+    instances, ordered by index, each {"index", "rank", ...solve's dict}.
+
+    concurrency > 1 solves that many of the slice's instances at a time from
+    host threads: every problem runs on its own CUDA stream and the library
+    calls release the GIL, so small instances can share the GPU.  A new
+    thread starts on CUDA device 0, so each worker first takes the caller's
+    current device."""
     if options is None:
         options = Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6, "MAXITER": 400000,
                            "MU_UPDATE_FREQUENCY": 500})
@@ -117,11 +125,23 @@ def solve_batch(instances, options=None, rank=0, world=1, group=None, solve=solv
     if len(by_index) != len(instances):
         raise ValueError("instance indices must be unique")
     mine = shard(instances, world)[rank]
-    results = []
-    for k in mine:
+
+    def one(k):
         r = dict(solve(by_index[k], options))
         r.update(index=k, rank=rank)
-        results.append(r)
+        return r
+
+    if concurrency > 1 and len(mine) > 1:
+        from concurrent.futures import ThreadPoolExecutor
+        init = None
+        import torch
+        if torch.cuda.is_available():
+            dev = torch.cuda.current_device()
+            init = lambda: torch.cuda.set_device(dev)   # noqa: E731
+        with ThreadPoolExecutor(max_workers=int(concurrency), initializer=init) as pool:
+            results = list(pool.map(one, mine))
+    else:
+        results = [one(k) for k in mine]
     if world > 1:
         import torch.distributed as dist
         gathered = [None] * world

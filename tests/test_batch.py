@@ -76,3 +76,19 @@ def test_two_gloo_ranks_gather_every_result(tmp_path):
     for k, rank in zip(r0[:, 0].astype(int), r0[:, 1].astype(int)):
         assert k in parts[rank]
     assert np.array_equal(r0[:, 2], [-float(i.index) - i.U for i in batch])
+
+
+def test_concurrent_slice_gives_the_same_results():
+    """concurrency > 1 runs a rank's instances from host threads; the results
+    and their order do not change."""
+    import threading
+    seen = set()
+
+    def solve(inst, options):
+        seen.add(threading.get_ident())
+        return _fake_solve(inst, options)
+
+    batch = hubbard_batch(count=12)
+    a = solve_batch(batch, solve=_fake_solve)
+    b = solve_batch(batch, solve=solve, concurrency=4)
+    assert a == b and [r["index"] for r in b] == list(range(12))
