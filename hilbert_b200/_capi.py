@@ -34,7 +34,7 @@ EXPORTS = (
     "v2b_bpsdp_create", "v2b_bpsdp_solve", "v2b_bpsdp_is_converged", "v2b_bpsdp_get_mu",
     "v2b_bpsdp_set_mu", "v2b_bpsdp_get_y", "v2b_bpsdp_get_z", "v2b_bpsdp_set_y",
     "v2b_bpsdp_set_z", "v2b_bpsdp_iiter_total", "v2b_bpsdp_oiter_total", "v2b_bpsdp_destroy",
-    "v2b_problem_create", "v2b_problem_destroy", "v2b_problem_n_primal", "v2b_problem_n_dual",
+    "v2b_problem_create", "v2b_doci_problem_create", "v2b_problem_destroy", "v2b_problem_n_primal", "v2b_problem_n_dual",
     "v2b_problem_n_blocks", "v2b_problem_block_dims", "v2b_problem_build_b",
     "v2b_problem_build_c_hubbard", "v2b_problem_build_c_external", "v2b_problem_guess",
     "v2b_problem_Au", "v2b_problem_ATu", "v2b_problem_project", "v2b_problem_project_warm",
@@ -101,6 +101,7 @@ def load(path=LIB_PATH):
         "v2b_bpsdp_oiter_total": (ctypes.c_long, [vp]),
         "v2b_bpsdp_destroy": (None, [vp]),
         "v2b_problem_create": (ctypes.c_int, [ctypes.c_int] * 7 + [ctypes.POINTER(vp)]),
+        "v2b_doci_problem_create": (ctypes.c_int, [ctypes.c_int] * 4 + [ctypes.POINTER(vp)]),
         "v2b_problem_destroy": (None, [vp]),
         "v2b_problem_n_primal": (ctypes.c_long, [vp]),
         "v2b_problem_n_dual": (ctypes.c_long, [vp]),

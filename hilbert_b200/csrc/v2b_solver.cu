@@ -1448,6 +1448,27 @@ int v2b_problem_create(int nmo, int nalpha, int nbeta, int positivity, int const
     });
 }
 
+int v2b_doci_problem_create(int nmo, int nalpha, int nbeta, int positivity, v2b_problem **out) {
+    return guarded([&] {
+        if (!out) throw std::invalid_argument("v2b_doci_problem_create: out is NULL");
+        if (positivity < 0 || (positivity & ~(15 | V2B_CONSTRAIN_D3)))
+            throw std::invalid_argument("v2b_doci_problem_create: DOCI takes POSITIVITY and CONSTRAIN_D3 only");
+        v2b::ProblemSpec spec;
+        spec.doci = true;
+        spec.nmo = nmo;
+        spec.nalpha = nalpha;
+        spec.nbeta = nbeta;
+        spec.positivity = positivity & 15;
+        spec.constrain_d3 = (positivity & V2B_CONSTRAIN_D3) != 0;
+        std::unique_ptr<v2b_problem> p(new v2b_problem());
+        p->prob = v2b::make_problem(spec);
+        p->hostA = v2b::build_A(p->prob);
+        p->hostAT = v2b::build_AT(p->prob);
+        *out = p.release();
+        return V2B_OK;
+    });
+}
+
 void v2b_problem_destroy(v2b_problem *p) { delete p; }
 long v2b_problem_n_primal(const v2b_problem *p) { return p ? p->prob.n_primal : -1; }
 long v2b_problem_n_dual(const v2b_problem *p) { return p ? p->prob.n_dual : -1; }
@@ -1662,6 +1683,7 @@ int v2b_problem_projection_profile(const v2b_problem *p, double *ms, long *n, in
 int v2b_problem_pack_dims(const v2b_problem *p, long *d2_size, long *d1_size) {
     return guarded([&] {
         if (!p || !d2_size || !d1_size) throw std::invalid_argument("pack_dims: NULL argument");
+        if (p->prob.spec.doci) throw std::invalid_argument("pack_dims: the v2RDM density packing, not DOCI's");
         const long g00 = (long)p->prob.n * (p->prob.n + 1) / 2;
         *d2_size = g00 * (g00 + 1) / 2;
         *d1_size = g00;
@@ -1672,6 +1694,8 @@ int v2b_problem_pack_spatial_density(v2b_problem *p, const double *d_x, double *
                                      void *stream) {
     return guarded([&] {
         if (!p || !d_x || !d_d2 || !d_d1) throw std::invalid_argument("pack_spatial_density: NULL argument");
+        if (p->prob.spec.doci)
+            throw std::invalid_argument("pack_spatial_density: the v2RDM density packing, not DOCI's");
         p->setup();
         const v2b::Problem &q = p->prob;
         if (!p->ibas_aa_dev) {

@@ -6,6 +6,7 @@
 // them.  A gather that sums each row left to right with separate multiply
 // and add roundings therefore reproduces the reference's A.x and A^T.y.
 #include "v2rdm_problem.h"
+#include "doci_problem.h"
 
 #include <cmath>
 #include <cstdlib>
@@ -16,6 +17,7 @@
 namespace v2b {
 
 Problem make_problem(const ProblemSpec &spec) {
+    if (spec.doci) return make_doci_problem(spec);
     if (spec.nmo < 1 || spec.nalpha < 0 || spec.nbeta < 0 || spec.nalpha > spec.nmo ||
         spec.nbeta > spec.nmo)
         throw std::invalid_argument("invalid orbital / electron counts");
@@ -242,6 +244,7 @@ Problem make_problem(const ProblemSpec &spec) {
 
 // ------------------------------------------------------------------ b, c, x
 void build_b(const Problem &p, double *b) {
+    if (p.spec.doci) return doci_build_b(p, b);
     const int n = p.n, gab = p.gab, gaa = p.gaa;
     const double na = p.spec.nalpha, nb = p.spec.nbeta;
     std::memset(b, 0, sizeof(double) * p.n_dual);
@@ -303,6 +306,7 @@ void fill_d1(const Problem &p, const double *hsym, double *c) {
 }  // namespace
 
 void build_c_hubbard(const Problem &p, double t, double U, double *c) {
+    if (p.spec.doci) throw std::invalid_argument("v2RDM-DOCI has no Hubbard Hamiltonian: pass h and g");
     const int n = p.n, gab = p.gab;
     std::memset(c, 0, sizeof(double) * p.n_primal);
     std::vector<double> h((size_t)n * n, 0.0);
@@ -319,6 +323,7 @@ void build_c_hubbard(const Problem &p, double t, double U, double *c) {
 }
 
 void build_c_external(const Problem &p, const double *h, const double *g, double *c) {
+    if (p.spec.doci) return doci_build_c_external(p, h, g, c);
     const int64_t n = p.n;
     const int gab = p.gab, gaa = p.gaa;
     std::memset(c, 0, sizeof(double) * p.n_primal);
@@ -868,6 +873,8 @@ void guess_random(const Problem &p, double *x) {
 }
 
 void guess_hf(const Problem &p, double *x) {
+    if (p.spec.doci)
+        throw std::invalid_argument("v2RDM-DOCI starts from the random guess (v2rdm_doci_solver.cc:1325-1336)");
     // v2rdm_solver.cc:1713-1823; the reference stores doccpi = nalpha for
     // Hubbard / external problems, so both spins fill nalpha orbitals.
     const int n = p.n, gab = p.gab, gaa = p.gaa, occ = p.spec.nalpha;
@@ -988,6 +995,15 @@ const double kSqrt2 = std::sqrt(2.0);
 // (rows the reference assembles as "first part + separately summed tail").
 template <class S>
 void visit_A(const Problem &p, S &s) {
+    if (p.spec.doci) {
+        doci_rows(p, [&](int64_t row, const DociTerm *t, int nt) {
+            for (int q = 0; q < nt; q++) {
+                if (t[q].tail) s.g(row, t[q].col, t[q].coef);
+                else s.t(row, t[q].col, t[q].coef);
+            }
+        });
+        return;
+    }
     const int n = p.n, gab = p.gab, gaa = p.gaa;
     const double na = p.spec.nalpha, nb = p.spec.nbeta;
     int64_t off = 0;
@@ -1335,6 +1351,12 @@ void visit_A(const Problem &p, S &s) {
 // contribution in the order hilbert's bpsdp_ATu scatters it.
 template <class S>
 void visit_AT(const Problem &p, S &s) {
+    if (p.spec.doci) {   // bpsdp_ATu scatters the rows in bpsdp_Au's order
+        doci_rows(p, [&](int64_t row, const DociTerm *t, int nt) {
+            for (int q = 0; q < nt; q++) s.t(t[q].col, row, t[q].coef);
+        });
+        return;
+    }
     const int n = p.n, gab = p.gab, gaa = p.gaa;
     const double na = p.spec.nalpha, nb = p.spec.nbeta;
     int64_t off = 0;

@@ -31,6 +31,13 @@ struct ProblemSpec {
     bool constrain_e3 = false;          // CONSTRAIN_E3, implies D3 (:4124-4127)
     bool constrain_f3 = false;          // CONSTRAIN_F3, implies D3 (:4128-4131)
     bool constrain_d4 = false;          // CONSTRAIN_D4, implies D3 (:4144-4149)
+    bool doci = false;                  // the v2RDM-DOCI program (src/v2rdm_doci)
+};
+
+// offsets of the v2RDM-DOCI primal blocks (v2rdm_doci_solver.cc:542-600)
+struct DociOffsets {
+    int64_t d2s2 = -1, d2s0 = -1, d1 = -1, q2s2 = -1, q2s0 = -1, g2s2 = -1, g2s0 = -1;
+    int64_t d3s3 = -1, d3s1 = -1, t1aaa = -1, t1aab = -1, t1s1 = -1, t2s1 = -1, t2 = -1;
 };
 
 // Packed sparse operator: entry = col (bits 0..26) | coef code (27..30) | group flag (31).
@@ -75,6 +82,7 @@ struct Problem {
     std::vector<int> ibas_aaaa, ibas_aaab, ibas_aabb;
     int64_t d2ab = -1, d2aa = -1, d2bb = -1, d200 = -1, d1a = -1, d1b = -1, q1a = -1, q1b = -1;
     int64_t q2ab = -1, q2aa = -1, q2bb = -1, g2ab = -1, g2ba = -1, g2aa = -1;
+    DociOffsets doci;                // spec.doci only
     int64_t n_primal = 0, n_dual = 0;
     std::vector<int> dims;           // PSD block sizes, in primal order
     std::vector<int64_t> block_off;  // offset of each block in x
@@ -92,7 +100,7 @@ void build_c_hubbard(const Problem &p, double t, double U, double *c);
 // external Hamiltonian: h[i*n+j], g[i*n^3+j*n^2+k*n+l] = (ij|kl)
 void build_c_external(const Problem &p, const double *h, const double *g, double *c);
 void guess_random(const Problem &p, double *x);
-void guess_hf(const Problem &p, double *x);
+void guess_hf(const Problem &p, double *x);   // v2RDM only (DOCI's guess is the random one)
 
 PackedOperator build_A(const Problem &p);    // rows = dual constraints
 PackedOperator build_AT(const Problem &p);   // rows = primal variables

@@ -105,6 +105,10 @@ class V2RDMProblem:
         check(lib.v2b_problem_create(int(nmo), int(nalpha), int(nbeta), code,
                                      int(bool(constrain_spin)), int(bool(constrain_sz)),
                                      int(bool(hubbard_multiplicity)), ctypes.byref(h)))
+        self._sizes(h, nmo, nalpha, nbeta)
+
+    def _sizes(self, h, nmo, nalpha, nbeta):
+        lib = self._lib
         self._h = h
         self.nmo, self.nalpha, self.nbeta = nmo, nalpha, nbeta
         self.n_primal = lib.v2b_problem_n_primal(h)
@@ -314,6 +318,25 @@ class V2RDMProblem:
 
     def stream_handle(self):
         return self._lib.v2b_problem_stream(self._h)
+
+
+class DOCIProblem(V2RDMProblem):
+    """One v2RDM-DOCI problem (hilbert's src/v2rdm_doci) on the same device
+    path: b, c from h and (ij|kl), the random guess, A.x, A^T.y and the
+    solves.  positivity is hilbert's POSITIVITY (D ... DQGT1T2; DQGT2 is D,
+    Q, G and T2), optionally "+D3" for CONSTRAIN_D3."""
+
+    def __init__(self, nmo, nalpha, nbeta, positivity="DQG"):
+        lib = _capi.load()
+        self._lib = lib
+        h = ctypes.c_void_p()
+        pos, *extras = positivity.upper().split("+")
+        if pos not in _capi.POSITIVITY or not set(extras) <= {"D3"}:
+            raise ValueError(f"DOCI POSITIVITY {positivity} is not one of "
+                             f"{sorted(_capi.POSITIVITY)}, optionally +D3")
+        code = _capi.POSITIVITY[pos] | (_capi.V2B_CONSTRAIN_D3 if extras else 0)
+        check(lib.v2b_doci_problem_create(int(nmo), int(nalpha), int(nbeta), code, ctypes.byref(h)))
+        self._sizes(h, nmo, nalpha, nbeta)
 
 
 class BPSDPSolver:

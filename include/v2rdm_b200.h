@@ -116,6 +116,16 @@ void v2b_bpsdp_destroy(v2b_bpsdp *s);
  * the Hubbard initialiser (v2rdm_solver.cc:862) over the external one (:983). */
 int v2b_problem_create(int nmo, int nalpha, int nbeta, int positivity, int constrain_spin,
                        int constrain_sz, int hubbard_multiplicity, v2b_problem **out);
+/* The v2RDM-DOCI program that v2RDM_DOCISolver::common_init sets up
+ * (src/v2rdm_doci/v2rdm_doci_solver.cc:427-700: POSITIVITY D ... DQGT1T2 and
+ * CONSTRAIN_D3, C1, no frozen or restricted orbitals), as a problem for the
+ * same v2b_problem_* calls: b (BuildConstraints, :1338-1507), c from h and
+ * (ij|kl) (RepackIntegrals, tei.cc:127-153), the random guess (:1325-1336),
+ * A.x and A^T.y (bpsdp_Au / bpsdp_ATu, :1509-1566) and the solves.
+ * positivity = V2B_POSITIVITY_* | V2B_CONSTRAIN_D3.  DOCI has no Hubbard c,
+ * no HF guess and not the v2RDM density packing: those calls return
+ * V2B_BAD_ARG. */
+int v2b_doci_problem_create(int nmo, int nalpha, int nbeta, int positivity, v2b_problem **out);
 void v2b_problem_destroy(v2b_problem *p);
 long v2b_problem_n_primal(const v2b_problem *p);
 long v2b_problem_n_dual(const v2b_problem *p);

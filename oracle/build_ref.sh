@@ -24,9 +24,12 @@ mkdir -p "$out"
 # the definition line at column 0, end: the first closing brace at column 0)
 # into a generated translation unit under _ref/.
 extract() {  # $1 = file, $2... = member function names
-  local f="$1"; shift
+  extract_class v2RDMSolver "$@"
+}
+extract_class() {  # $1 = class, $2 = file, $3... = member function names
+  local cls="$1" f="$2"; shift 2
   for name in "$@"; do
-    awk -v pat="v2RDMSolver::${name}\\\\(" '
+    awk -v pat="${cls}::${name}\\\\(" '
       !on && $0 ~ /^[A-Za-z]/ && $0 ~ pat { on = 1 }
       on { print }
       on && $0 ~ /^}/ { on = 0; print "" }
@@ -69,3 +72,43 @@ done
 "$CXX" -shared -Wl,--no-undefined -o "$out/libv2rdm_ref.so" "${objs[@]}" \
     "$out/v2rdm_solver_extract.o" "$out/ref_harness.o"
 echo "built $out/libv2rdm_ref.so"
+
+# v2RDM-DOCI: the map files of src/v2rdm_doci, plus BuildConstraints, Guess,
+# bpsdp_Au / bpsdp_ATu and SymmetryPair from v2rdm_doci_solver.cc, plus the
+# part of common_init that turns POSITIVITY / CONSTRAIN_D3 into sizes,
+# offsets and the block list (from "pick conditions" up to the convergence
+# thresholds), which reads nothing from the wavefunction.
+dsrc="$ref/src/v2rdm_doci"
+dgen="$out/doci_solver_extract.cc"
+{
+  echo '// generated by oracle/build_ref.sh from the reference tree; do not edit'
+  echo '#include <psi4/psi4-dec.h>'
+  echo '#include <psi4/libqt/qt.h>'
+  echo '#include "v2rdm_doci_solver.h"'
+  echo 'using namespace psi;'
+  echo 'namespace hilbert {'
+  extract_class v2RDM_DOCISolver "$dsrc/v2rdm_doci_solver.cc" SymmetryPair TotalSym \
+      BuildConstraints Guess bpsdp_Au bpsdp_ATu
+  echo 'void v2RDM_DOCISolver::common_init() {'
+  awk '/pick conditions\.  default is dqg/ { on = 1 }
+       /v2rdm sdp convergence thresholds/ { on = 0 }
+       on { print }' "$dsrc/v2rdm_doci_solver.cc"
+  echo '}'
+  echo '}'
+} > "$dgen"
+for name in SymmetryPair TotalSym BuildConstraints Guess bpsdp_Au bpsdp_ATu; do
+  grep -q "v2RDM_DOCISolver::${name}(" "$dgen" || { echo "build_ref.sh: could not extract DOCI ${name}" >&2; exit 3; }
+done
+grep -q "dimensions_.push_back" "$dgen" || { echo "build_ref.sh: could not extract the DOCI sizing" >&2; exit 3; }
+DFLAGS=(-std=c++17 -O2 -fPIC -ffp-contract=off -w
+        -I"$here/ref_shim" -I"$dsrc" -I"$ref/src")
+dobjs=()
+for u in basis d2 q2 g2 d3 t1 t2 tei; do
+  "$CXX" "${DFLAGS[@]}" -c "$dsrc/$u.cc" -o "$out/doci_$u.o"
+  dobjs+=("$out/doci_$u.o")
+done
+"$CXX" "${DFLAGS[@]}" -c "$dgen" -o "$out/doci_solver_extract.o"
+"$CXX" "${DFLAGS[@]}" -c "$here/doci_ref_harness.cc" -o "$out/doci_ref_harness.o"
+"$CXX" -shared -Wl,--no-undefined -o "$out/libdoci_ref.so" "${dobjs[@]}" \
+    "$out/doci_solver_extract.o" "$out/doci_ref_harness.o"
+echo "built $out/libdoci_ref.so"

@@ -140,6 +140,8 @@ class Wavefunction {
     int nirrep_ = 1;
     int nmo_ = 0;
     int nso_ = 0;
+    int nalpha_ = 0;   // Psi4's Wavefunction members; v2RDMSolver declares its own
+    int nbeta_ = 0;
     long memory_ = 0;
     double energy_ = 0.0;
     double efzc_ = 0.0;

@@ -1,0 +1,186 @@
+"""v2RDM-DOCI (hilbert's src/v2rdm_doci) on the CPU: the oracle against the
+reference's compiled code and its golden fixture, and the product library's
+host-side problem (sizes, b, c, guess, packed A and A^T) against both."""
+import itertools
+import os
+import types
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+import hilbert_b200 as hb
+from hilbert_b200 import _capi
+from oracle.doci import DociOracle, DociRef, ref_available, symmetric_integrals
+from test_host_problem import operator, packed_apply
+
+GOLDEN = os.path.join(ROOT, "tests", "golden", "doci_maps.npz")
+POSITIVITIES = ["D", "DQ", "DG", "DQG", "DQGT1", "DQGT2", "DQGT1T2"]
+needs_ref = pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+
+
+def golden_cases():
+    with np.load(GOLDEN) as z:
+        names = sorted({k.split("/")[0] for k in z.files})
+        return {name: {k.split("/")[1]: z[k] for k in z.files if k.startswith(name + "/")}
+                for name in names}
+
+
+def d3_scaled_rows(n, positivity):
+    """Dual rows of the seniority-3 D3 condition (d3.cc:131-145), the one
+    family whose A.x the packed rows round differently (a partial sum
+    scaled by 1/6 as a whole)."""
+    pos, *extras = positivity.split("+")
+    if "D3" not in extras:
+        return np.zeros(0, np.int64)
+    pairs = n * (n - 1) // 2
+    start = 3 + 3 * n + n * n
+    if pos in ("DQ", "DQG", "DQGT1", "DQGT2", "DQGT1T2"):
+        start += pairs + n * n
+    if pos in ("DG", "DQG", "DQGT1", "DQGT2", "DQGT1T2"):
+        start += 4 * pairs + n * n
+    return np.arange(start, start + n * (n - 1))
+
+
+def assert_Au_matches(got, want, n, positivity, x):
+    """Bit-exact except the scaled D3 rows, which hold to a few ulps of their
+    terms (6(n-2) + 1 of them, each |1/6 x| or |(N/2 - 2) x|)."""
+    rows = d3_scaled_rows(n, positivity)
+    other = np.setdiff1d(np.arange(len(want)), rows)
+    assert np.array_equal(got[other], want[other])
+    if len(rows):
+        bound = 8 * n * np.finfo(float).eps * (1.0 + n) * np.abs(x).max()
+        assert np.max(np.abs(got[rows] - want[rows])) <= bound
+
+
+def product(n, na, nb, positivity):
+    return hb.DOCIProblem(n, na, nb, positivity)
+
+
+# ---------------------------------------------------------------- oracle pins
+def test_doci_oracle_matches_golden():
+    """The C restatement against the fixture made from hilbert's compiled DOCI code."""
+    for name, case in golden_cases().items():
+        n, na, nb = (int(v) for v in case["meta"])
+        pos = str(case["positivity"])
+        o = DociOracle(n, na, nb, pos)
+        assert np.array_equal(o.dims, case["dims"]), name
+        assert np.array_equal(o.b(), case["b"]), name
+        assert np.array_equal(o.c(case["h"], case["g"]), case["c"]), name
+        assert np.array_equal(o.guess(), case["x0"]), name
+        assert np.array_equal(o.Au(case["x"]), case["Ax"]), name
+        assert np.array_equal(o.ATu(case["y"]), case["ATy"]), name
+
+
+@needs_ref
+def test_doci_oracle_matches_reference_grid():
+    """Every POSITIVITY with and without D3, n = 2..5, open and closed shells."""
+    rng = np.random.default_rng(7)
+    for pos, d3, n in itertools.product(POSITIVITIES, ["", "+D3"], [2, 3, 4, 5]):
+        for na, nb in [(n // 2, n // 2), (min(n, n // 2 + 1), n // 2), (1, 1)]:
+            h, g = symmetric_integrals(rng, n)
+            r = DociRef(n, na, nb, pos + d3, h=h, g=g)
+            o = DociOracle(n, na, nb, pos + d3)
+            assert (o.n_primal, o.n_dual) == (r.n_primal, r.n_dual)
+            assert np.array_equal(o.dims, r.dims)
+            assert np.array_equal(o.b(), r.b) and np.array_equal(o.guess(), r.x0)
+            assert np.array_equal(o.c(h, g), r.c)
+            x, y = rng.standard_normal(r.n_primal), rng.standard_normal(r.n_dual)
+            assert np.array_equal(o.Au(x), r.Au(x)) and np.array_equal(o.ATu(y), r.ATu(y))
+
+
+# ------------------------------------------------------- product host problem
+def test_doci_host_problem_matches_golden():
+    for name, case in golden_cases().items():
+        n, na, nb = (int(v) for v in case["meta"])
+        pos = str(case["positivity"])
+        p = product(n, na, nb, pos)
+        assert list(p.dims) == list(case["dims"]), name
+        assert np.array_equal(p.b(), case["b"]), name
+        assert np.array_equal(p.c_external(case["h"], case["g"]), case["c"]), name
+        assert np.array_equal(p.guess("RANDOM"), case["x0"]), name
+        rp, ent, pal = operator(p, False)
+        assert_Au_matches(packed_apply(rp, ent, pal, case["x"]), case["Ax"], n, pos, case["x"])
+        rp, ent, pal = operator(p, True)
+        assert np.array_equal(packed_apply(rp, ent, pal, case["y"]), case["ATy"]), name
+        p.close()
+
+
+@pytest.mark.parametrize("pos", POSITIVITIES + ["DQG+D3", "DQGT1T2+D3"])
+def test_doci_host_problem_matches_oracle(pos):
+    rng = np.random.default_rng(11)
+    for n in (2, 3, 4, 6):
+        na = nb = n // 2
+        h, g = symmetric_integrals(rng, n)
+        o, p = DociOracle(n, na, nb, pos), product(n, na, nb, pos)
+        assert (p.n_primal, p.n_dual) == (o.n_primal, o.n_dual) and list(p.dims) == list(o.dims)
+        assert np.array_equal(p.b(), o.b()) and np.array_equal(p.c_external(h, g), o.c(h, g))
+        assert np.array_equal(p.guess("RANDOM"), o.guess())
+        x, y = rng.standard_normal(o.n_primal), rng.standard_normal(o.n_dual)
+        rp, ent, pal = operator(p, False)
+        assert len(pal) <= 16
+        assert_Au_matches(packed_apply(rp, ent, pal, x), o.Au(x), n, pos, x)
+        rp, ent, pal = operator(p, True)
+        assert np.array_equal(packed_apply(rp, ent, pal, y), o.ATu(y))
+        p.close()
+
+
+@pytest.mark.parametrize("pos", ["DQGT1T2+D3", "DQG"])
+def test_doci_packed_operators_are_adjoint(pos):
+    rng = np.random.default_rng(3)
+    p = product(5, 2, 2, pos)
+    x, y = rng.standard_normal(p.n_primal), rng.standard_normal(p.n_dual)
+    rp, ent, pal = operator(p, False)
+    ax = packed_apply(rp, ent, pal, x)
+    rp, ent, pal = operator(p, True)
+    aty = packed_apply(rp, ent, pal, y)
+    assert abs(ax @ y - x @ aty) <= 1e-12 * max(1.0, abs(ax @ y))
+
+
+def test_doci_refusals():
+    """What DOCI does not have is an error, not a silent v2RDM answer."""
+    with pytest.raises(ValueError):
+        hb.DOCIProblem(4, 2, 2, "DQG+E3")
+    lib = _capi.load()
+    import ctypes
+    h = ctypes.c_void_p()
+    for code in (3 | _capi.V2B_CONSTRAIN_Q3, 3 | _capi.V2B_CONSTRAIN_D4, 7, -1):
+        assert lib.v2b_doci_problem_create(4, 2, 2, code, ctypes.byref(h)) == _capi.V2B_BAD_ARG
+    assert lib.v2b_doci_problem_create(1, 1, 1, 3 | _capi.V2B_CONSTRAIN_D3, ctypes.byref(h)) == _capi.V2B_BAD_ARG
+    p = product(4, 2, 2, "DQG")
+    with pytest.raises(_capi.V2BError):
+        p.guess("HF")
+    with pytest.raises(_capi.V2BError):
+        p.c_hubbard(1.0, 4.0)
+    d2, d1 = ctypes.c_long(), ctypes.c_long()
+    assert lib.v2b_problem_pack_dims(p._h, ctypes.byref(d2), ctypes.byref(d1)) == _capi.V2B_BAD_ARG
+    p.close()
+
+
+# --------------------------------------------------------------- oracle solve
+def pair_hamiltonian(h, g):
+    """One electron pair in seniority zero: <pp'|H|qq'> = d_pq (2 h_pp + (pp|pp)) + (1 - d_pq) (pq|pq)."""
+    n = h.shape[0]
+    H = np.array([[g[p, q, p, q] for q in range(n)] for p in range(n)])
+    H[np.diag_indices(n)] += 2.0 * np.diag(h)
+    return H
+
+
+def oracle_solve(o, h, g, r_conv=1e-7, e_conv=1e-7, maxiter=20000):
+    from oracle.bpsdp import SDPOptions, run_v2rdm
+    prob = types.SimpleNamespace(n_primal=o.n_primal, n_dual=o.n_dual, b=o.b(), c=o.c(h, g),
+                                 dims=[int(d) for d in o.dims], Au=o.Au, ATu=o.ATu)
+    opts = SDPOptions(sdp_objective_convergence=e_conv, sdp_error_convergence=r_conv,
+                      cg_convergence=1e-10, cg_maxiter=10000, maxiter=maxiter)
+    x, solver = run_v2rdm(prob, o.guess(), opts, mu_update_frequency=500)
+    return float(prob.c @ x), solver
+
+
+def test_doci_one_pair_is_exact():
+    """For one electron pair the D condition alone is exact: the energy is the
+    lowest eigenvalue of the seniority-zero pair Hamiltonian."""
+    rng = np.random.default_rng(2)
+    h, g = symmetric_integrals(rng, 4)
+    e, solver = oracle_solve(DociOracle(4, 1, 1, "D"), h, g)
+    assert solver.is_converged()
+    assert abs(e - np.linalg.eigvalsh(pair_hamiltonian(h, g))[0]) < 1e-6
