@@ -169,3 +169,24 @@ def symmetric_integrals(rng, n):
     g = g + g.transpose(0, 1, 3, 2)
     g = g + g.transpose(2, 3, 0, 1)
     return h + h.T, g
+
+
+def seniority_zero_ci(h, g, npair):
+    """Exact DOCI energy: the lowest eigenvalue of the Hamiltonian in the
+    basis of closed-shell pair determinants (each orbital empty or doubly
+    occupied).  <I|H|I> = sum_i (2 h_ii + (ii|ii)) + sum_{i<j} (4 (ii|jj) - 2 (ij|ij))
+    over the pairs of I; moving one pair i -> a couples I and J by (ia|ia)."""
+    import itertools
+    n = h.shape[0]
+    dets = list(itertools.combinations(range(n), npair))
+    index = {d: k for k, d in enumerate(dets)}
+    H = np.zeros((len(dets), len(dets)))
+    for k, d in enumerate(dets):
+        occ = set(d)
+        H[k, k] = (sum(2.0 * h[i, i] + g[i, i, i, i] for i in d)
+                   + sum(4.0 * g[i, i, j, j] - 2.0 * g[i, j, i, j] for i, j in itertools.combinations(d, 2)))
+        for i in d:
+            for a in range(n):
+                if a not in occ:
+                    H[index[tuple(sorted((occ - {i}) | {a}))], k] = g[i, a, i, a]
+    return float(np.linalg.eigvalsh(H)[0])

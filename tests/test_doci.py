@@ -11,7 +11,7 @@ import pytest
 from conftest import ROOT
 import hilbert_b200 as hb
 from hilbert_b200 import _capi
-from oracle.doci import DociOracle, DociRef, ref_available, symmetric_integrals
+from oracle.doci import DociOracle, DociRef, ref_available, seniority_zero_ci, symmetric_integrals
 from test_host_problem import operator, packed_apply
 
 GOLDEN = os.path.join(ROOT, "tests", "golden", "doci_maps.npz")
@@ -183,4 +183,28 @@ def test_doci_one_pair_is_exact():
     h, g = symmetric_integrals(rng, 4)
     e, solver = oracle_solve(DociOracle(4, 1, 1, "D"), h, g)
     assert solver.is_converged()
-    assert abs(e - np.linalg.eigvalsh(pair_hamiltonian(h, g))[0]) < 1e-6
+    exact = np.linalg.eigvalsh(pair_hamiltonian(h, g))[0]
+    assert abs(exact - seniority_zero_ci(h, g, 1)) < 1e-12
+    assert abs(e - exact) < 1e-6
+
+
+def df_integrals(n, naux=12, seed=5):
+    """h with a spread diagonal, (ij|kl) = sum_Q B_ij^Q B_kl^Q (positive semidefinite)."""
+    rng = np.random.default_rng(seed)
+    h = 0.1 * rng.standard_normal((n, n))
+    h = h + h.T + np.diag(np.linspace(-2.0, 1.0, n))
+    B = 0.3 * rng.standard_normal((n, n, naux))
+    B = B + B.transpose(1, 0, 2)
+    return h, np.einsum("ijq,klq->ijkl", B, B)
+
+
+def test_doci_relaxations_bound_exact_doci():
+    """Each set of conditions is a relaxation of seniority-zero CI, and adding
+    Q and G tightens it: E(D) <= E(DQG) <= E(DOCI)."""
+    h, g = df_integrals(4)
+    exact = seniority_zero_ci(h, g, 2)
+    e_d, s_d = oracle_solve(DociOracle(4, 2, 2, "D"), h, g)
+    e_dqg, s_dqg = oracle_solve(DociOracle(4, 2, 2, "DQG"), h, g)
+    assert s_d.is_converged() and s_dqg.is_converged()
+    assert e_d <= e_dqg + 1e-6 and e_dqg <= exact + 1e-6
+    assert exact - e_dqg < 0.5   # DQG recovers most of the gap left by D (2.85 Eh here)

@@ -1,0 +1,63 @@
+"""v2RDM-DOCI on the B200: the device maps against the fixture made from
+hilbert's compiled DOCI code, and device solves against the exact one-pair
+answer and the numpy oracle (|dE| <= 1e-6)."""
+import numpy as np
+import pytest
+
+import hilbert_b200 as hb
+from oracle.doci import DociOracle, seniority_zero_ci, symmetric_integrals
+from test_doci import assert_Au_matches, df_integrals, golden_cases, oracle_solve, pair_hamiltonian
+
+pytestmark = pytest.mark.gpu
+
+E_TOL = 1e-6
+
+
+@pytest.mark.parametrize("name", sorted(golden_cases()))
+def test_doci_device_maps_golden(cuda_device, name):
+    import torch
+    case = golden_cases()[name]
+    n, na, nb = (int(v) for v in case["meta"])
+    pos = str(case["positivity"])
+    p = hb.DOCIProblem(n, na, nb, pos)
+    x = torch.from_numpy(case["x"]).to(cuda_device)
+    y = torch.from_numpy(case["y"]).to(cuda_device)
+    assert_Au_matches(p.Au(x).cpu().numpy(), case["Ax"], n, pos, case["x"])
+    assert np.array_equal(p.ATu(y).cpu().numpy(), case["ATy"])
+    p.close()
+
+
+def device_solve(p, h, g, r=1e-7, e=1e-7):
+    import torch
+    dev = torch.device("cuda", 0)
+    b, c = p.b(), p.c_external(h, g)
+    x = torch.from_numpy(p.guess("RANDOM")).to(dev)
+    opts = hb.Options({"R_CONVERGENCE": r, "E_CONVERGENCE": e, "MAXITER": 200000,
+                       "MU_UPDATE_FREQUENCY": 500})
+    st = p.solve_device(x, torch.from_numpy(b).to(dev), torch.from_numpy(c).to(dev), opts)
+    return float(c @ x.cpu().numpy()), st
+
+
+def test_doci_device_one_pair_is_exact(cuda_device):
+    rng = np.random.default_rng(2)
+    h, g = symmetric_integrals(rng, 4)
+    p = hb.DOCIProblem(4, 1, 1, "D")
+    e, st = device_solve(p, h, g)
+    p.close()
+    assert st["converged"]
+    assert abs(e - np.linalg.eigvalsh(pair_hamiltonian(h, g))[0]) <= E_TOL
+
+
+@pytest.mark.parametrize("pos", ["DQG", "DQGT1T2+D3"])
+def test_doci_device_solve_matches_oracle(cuda_device, pos):
+    """Six orbitals, three pairs, seeded density-fitted integrals."""
+    n = 6
+    h, g = df_integrals(n)
+    p = hb.DOCIProblem(n, 3, 3, pos)
+    e, st = device_solve(p, h, g)
+    p.close()
+    assert st["converged"]
+    eo, so = oracle_solve(DociOracle(n, 3, 3, pos), h, g)
+    assert so.is_converged()
+    assert abs(e - eo) <= E_TOL
+    assert e <= seniority_zero_ci(h, g, 3) + E_TOL
