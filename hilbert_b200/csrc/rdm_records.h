@@ -1,0 +1,27 @@
+// Density-matrix records of hilbert's RDM writers (see rdm_records.cpp).
+#pragma once
+
+#include "v2rdm_problem.h"
+
+namespace v2b {
+
+// struct tpdm / struct opdm, src/v2rdm_casscf/v2rdm_solver.h:53-65
+struct TpdmRecord {
+    int i, j, k, l;
+    double value;
+};
+struct OpdmRecord {
+    int i, j;
+    double value;
+};
+
+struct RdmCounts {
+    int64_t d2aa, d2bb, d2ab, d2, d1a, d1b;
+};
+
+RdmCounts rdm_counts(const Problem &p);
+// x is the host primal vector; any output may be null
+void rdm_records(const Problem &p, const double *x, TpdmRecord *d2aa, TpdmRecord *d2bb,
+                 TpdmRecord *d2ab, TpdmRecord *d2, OpdmRecord *d1a, OpdmRecord *d1b);
+
+}  // namespace v2b

@@ -28,6 +28,7 @@
 #include "v2b_refine.cuh"
 #include "v2rdm_b200.h"
 #include "v2rdm_problem.h"
+#include "rdm_records.h"
 
 namespace {
 
@@ -1677,6 +1678,28 @@ int v2b_problem_projection_profile(const v2b_problem *p, double *ms, long *n, in
             ms[k] = p->plan.ph_ms[k];
             n[k] = p->plan.ph_n[k];
         }
+        return V2B_OK;
+    });
+}
+int v2b_problem_rdm_counts(const v2b_problem *p, long *counts) {
+    return guarded([&] {
+        if (!p || !counts) throw std::invalid_argument("rdm_counts: NULL argument");
+        const v2b::RdmCounts c = v2b::rdm_counts(p->prob);
+        const long v[6] = {(long)c.d2aa, (long)c.d2bb, (long)c.d2ab, (long)c.d2, (long)c.d1a, (long)c.d1b};
+        std::copy(v, v + 6, counts);
+        return V2B_OK;
+    });
+}
+int v2b_problem_rdm_records(const v2b_problem *p, const double *x, v2b_tpdm_record *d2aa,
+                            v2b_tpdm_record *d2bb, v2b_tpdm_record *d2ab, v2b_tpdm_record *d2,
+                            v2b_opdm_record *d1a, v2b_opdm_record *d1b) {
+    static_assert(sizeof(v2b_tpdm_record) == sizeof(v2b::TpdmRecord), "record layout");
+    static_assert(sizeof(v2b_opdm_record) == sizeof(v2b::OpdmRecord), "record layout");
+    return guarded([&] {
+        if (!p || !x) throw std::invalid_argument("rdm_records: NULL argument");
+        v2b::rdm_records(p->prob, x, (v2b::TpdmRecord *)d2aa, (v2b::TpdmRecord *)d2bb,
+                         (v2b::TpdmRecord *)d2ab, (v2b::TpdmRecord *)d2, (v2b::OpdmRecord *)d1a,
+                         (v2b::OpdmRecord *)d1b);
         return V2B_OK;
     });
 }

@@ -289,6 +289,65 @@ class V2RDMProblem:
             out.append(nnz.value)
         return tuple(out)
 
+    # the records of hilbert's density-matrix writers (struct tpdm / struct opdm)
+    TPDM_RECORD = np.dtype([("i", np.int32), ("j", np.int32), ("k", np.int32), ("l", np.int32),
+                            ("value", np.float64)])
+    OPDM_RECORD = np.dtype([("i", np.int32), ("j", np.int32), ("value", np.float64)])
+    RDM_FILES = ("D2aa", "D2bb", "D2ab", "D2", "D1a", "D1b")
+
+    @staticmethod
+    def read_rdm_files(path):
+        """{file: {entry: bytes}} from write_rdm_files."""
+        out = {}
+        with np.load(path) as z:
+            for k in z.files:
+                name, key = k.split("/", 1)
+                out.setdefault(name, {})[key] = z[k].tobytes()
+        return out
+
+    def rdm_records(self, x):
+        """{file: records} as WriteTPDM, WriteTPDMSpinFree and WriteOPDM emit
+        them (write_tpdm.cc:40-519, write_opdm.cc:40-114) for the host or
+        device primal vector x: D2aa, D2bb, D2ab, the spin-free D2, D1a, D1b."""
+        xh = np.ascontiguousarray(x.detach().cpu().numpy() if hasattr(x, "detach") else x,
+                                  dtype=np.float64)
+        if xh.shape != (self.n_primal,):
+            raise ValueError(f"x must hold {self.n_primal} values")
+        counts = np.zeros(6, np.int64)
+        check(self._lib.v2b_problem_rdm_counts(self._h, counts.ctypes.data))
+        out = {name: np.zeros(int(cnt), self.TPDM_RECORD if name.startswith("D2") else self.OPDM_RECORD)
+               for name, cnt in zip(self.RDM_FILES, counts)}
+        check(self._lib.v2b_problem_rdm_records(self._h, xh.ctypes.data,
+                                                *[out[name].ctypes.data for name in self.RDM_FILES]))
+        return out
+
+    def rdm_entries(self, x):
+        """{file: {entry: bytes}}: every entry hilbert's writers put in their
+        PSIO files, byte for byte (the records when there are any, "length",
+        and for the D2 files "NUMBER ACTIVE ORBITALS", "ACTIVE ORBITALS" and
+        "NUMBER INACTIVE ORBITALS"; write_tpdm.cc:226-262,
+        write_opdm.cc:108-113)."""
+        recs = self.rdm_records(x)
+        n = int(self.nmo)
+        out = {}
+        for name, r in recs.items():
+            # an entry exists once something is written to it
+            e = {name: r.tobytes()} if len(r) else {}
+            e["length"] = np.int64(len(r)).tobytes()
+            if name.startswith("D2"):
+                e["NUMBER ACTIVE ORBITALS"] = np.int32(n).tobytes()
+                e["ACTIVE ORBITALS"] = np.arange(n, dtype=np.int32).tobytes()
+                e["NUMBER INACTIVE ORBITALS"] = np.int32(0).tobytes()
+            out[name] = e
+        return out
+
+    def write_rdm_files(self, path, x):
+        """Writes rdm_entries(x) to one .npz archive, one array per entry,
+        named "<file>/<entry>" (the PSIO container itself is Psi4's)."""
+        arrays = {f"{name}/{key}": np.frombuffer(val, np.uint8)
+                  for name, ent in self.rdm_entries(x).items() for key, val in ent.items()}
+        np.savez(path, **arrays)
+
     def pack_spatial_density(self, x):
         """hilbert's PackSpatialDensity of a device primal vector x (float64 CUDA
         tensor): (packed spin-summed active D2, packed D1), on the current stream"""

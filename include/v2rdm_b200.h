@@ -231,6 +231,28 @@ int v2b_problem_pack_dims(const v2b_problem *p, long *d2_size, long *d1_size);
 int v2b_problem_pack_spatial_density(v2b_problem *p, const double *d_x, double *d_d2, double *d_d1,
                                      void *stream);
 
+/* The density-matrix records hilbert writes after a solve, from the host
+ * primal vector x: the same records, order and values as WriteTPDM
+ * (src/v2rdm_casscf/write_tpdm.cc:40-310: files D2aa, D2bb, D2ab),
+ * WriteTPDMSpinFree (:312-519: file D2) and WriteOPDM (write_opdm.cc:40-114:
+ * files D1a, D1b), for the C1 active space (orbital numbers are active
+ * indices; no core records).  The record layouts are the reference's struct
+ * tpdm and struct opdm (v2rdm_solver.h:53-65).  counts[6] receives the
+ * record counts in the order D2aa, D2bb, D2ab, D2, D1a, D1b; any output
+ * array may be NULL.  v2RDM problems only. */
+typedef struct {
+    int i, j, k, l;
+    double value;
+} v2b_tpdm_record;
+typedef struct {
+    int i, j;
+    double value;
+} v2b_opdm_record;
+int v2b_problem_rdm_counts(const v2b_problem *p, long *counts);
+int v2b_problem_rdm_records(const v2b_problem *p, const double *x, v2b_tpdm_record *d2aa,
+                            v2b_tpdm_record *d2bb, v2b_tpdm_record *d2ab, v2b_tpdm_record *d2,
+                            v2b_opdm_record *d1a, v2b_opdm_record *d1b);
+
 /* ---- 3. allocation-free projection ------------------------------------------ */
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -48,12 +48,13 @@ gen="$out/v2rdm_solver_extract.cc"
       determine_n_primal determine_n_dual set_primal_offsets BuildConstraints \
       Guess bpsdp_Au bpsdp_ATu PackSpatialDensity
   extract "$src/oei.cc" GetOEI_external GetOEI_hubbard
+  extract "$src/write_tpdm.cc" WriteTPDM WriteTPDMSpinFree
   echo '}'
 } > "$gen"
 
 for name in SymmetryPair TotalSym set_constraints determine_n_primal determine_n_dual \
             set_primal_offsets BuildConstraints Guess bpsdp_Au bpsdp_ATu PackSpatialDensity \
-            GetOEI_external GetOEI_hubbard; do
+            GetOEI_external GetOEI_hubbard WriteTPDM WriteTPDMSpinFree; do
   grep -q "v2RDMSolver::${name}(" "$gen" || { echo "build_ref.sh: could not extract ${name}" >&2; exit 3; }
 done
 
@@ -61,7 +62,7 @@ done
 CXX="${CXX:-g++}"
 FLAGS=(-std=c++17 -O2 -fPIC -ffp-contract=off -w
        -I"$here/ref_shim" -I"$src" -I"$ref/src")
-units=(basis d2 spin q2 g2 t1 t2 d3 d4 e3 f3 q3 tei)
+units=(basis d2 spin q2 g2 t1 t2 d3 d4 e3 f3 q3 tei write_opdm)
 objs=()
 for u in "${units[@]}"; do
   "$CXX" "${FLAGS[@]}" -c "$src/$u.cc" -o "$out/$u.o"

@@ -251,6 +251,36 @@ class RefProblem:
             raise RuntimeError(self._lib.v2b_ref_last_error().decode())
         return d2, d1
 
+    # PSIO units and entries of hilbert's RDM writers (misc/hilbert_psifiles.h:33-42)
+    RDM_UNITS = {"D2aa": 270, "D2ab": 271, "D2bb": 272, "D1a": 277, "D1b": 278, "D2": 279}
+    TPDM = np.dtype([("i", np.int32), ("j", np.int32), ("k", np.int32), ("l", np.int32),
+                     ("value", np.float64)])
+    OPDM = np.dtype([("i", np.int32), ("j", np.int32), ("value", np.float64)])
+
+    def write_rdms(self, x):
+        """Runs the reference's WriteTPDM, WriteTPDMSpinFree and WriteOPDM on
+        x and returns what they wrote: {file: records} and {file: {entry: bytes}}"""
+        lib = self._lib
+        lib.v2b_ref_write_rdms.argtypes = [ctypes.c_void_p, _dp]
+        lib.v2b_ref_psio_entry.restype = ctypes.c_long
+        lib.v2b_ref_psio_entry.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p]
+        if lib.v2b_ref_write_rdms(self._p, np.ascontiguousarray(x, np.float64)):
+            raise RuntimeError(lib.v2b_ref_last_error().decode())
+        records, entries = {}, {}
+        for name, unit in self.RDM_UNITS.items():
+            entries[name] = {}
+            for key in (name, "length", "NUMBER ACTIVE ORBITALS", "ACTIVE ORBITALS",
+                        "NUMBER INACTIVE ORBITALS", "INACTIVE ORBITALS"):
+                size = lib.v2b_ref_psio_entry(unit, key.encode(), None)
+                if size < 0:
+                    continue
+                buf = ctypes.create_string_buffer(max(size, 1))
+                lib.v2b_ref_psio_entry(unit, key.encode(), buf)
+                entries[name][key] = buf.raw[:size]
+            raw = entries[name].get(name, b"")
+            records[name] = np.frombuffer(raw, self.TPDM if name.startswith("D2") else self.OPDM).copy()
+        return records, entries
+
     def ATu(self, y):
         out = np.zeros(self.n_primal)
         if self._lib.v2b_ref_ATu(self._p, out, np.ascontiguousarray(y, np.float64)):

@@ -134,6 +134,14 @@ class RefProblem : public v2RDMSolver {
         std::memcpy(d2, d2_act_spatial_sym_, sizeof(double) * d2_act_spatial_dim_);
         std::memcpy(d1, d1_act_spatial_sym_, sizeof(double) * d1_act_spatial_dim_);
     }
+    // write_tpdm.cc:40-519 and write_opdm.cc:40-114 on a given primal vector,
+    // into the in-memory PSIO stand-in
+    void write_rdms(const double *xin) {
+        std::memcpy(x->pointer(), xin, sizeof(double) * n_primal_);
+        WriteTPDM();
+        WriteTPDMSpinFree();
+        WriteOPDM();
+    }
     long d2_dim() const { return d2_act_spatial_dim_; }
     long d1_dim() const { return d1_act_spatial_dim_; }
     double efzc() const { return efzc_; }
@@ -285,6 +293,21 @@ void v2b_ref_triplets(void *p, int *aaa, int *aab, int *aba) {
 long v2b_ref_pack_dims(void *p, long *d1n) {
     *d1n = static_cast<RefProblem *>(p)->d1_dim();
     return static_cast<RefProblem *>(p)->d2_dim();
+}
+/* runs the reference's RDM writers on x; their files stay in the PSIO
+   stand-in until the next call */
+int v2b_ref_write_rdms(void *p, const double *x) {
+    try {
+        static_cast<RefProblem *>(p)->write_rdms(x);
+        return 0;
+    } catch (const std::exception &e) { g_last_error = e.what(); return 1; }
+}
+/* size of one written PSIO entry, -1 if absent; copy it into out (may be NULL) */
+long v2b_ref_psio_entry(int unit, const char *key, char *out) {
+    auto it = psi::psio_store().find({unit, key});
+    if (it == psi::psio_store().end()) return -1;
+    if (out) std::memcpy(out, it->second.data(), it->second.size());
+    return (long)it->second.size();
 }
 int v2b_ref_pack_spatial(void *p, const double *x, double *d2, double *d1) {
     try {

@@ -172,6 +172,50 @@ inline void C_DSCAL(size_t n, double a, double *x, int incx) {
     for (size_t i = 0; i < n; i++) x[i * incx] *= a;
 }
 
+/* PSIO: files are kept in memory, one byte string per (unit, entry), so the
+   oracle can read back what the reference's writers emit.  The store is
+   process-wide (psio_store()); open(PSIO_OPEN_NEW) empties the unit. */
+struct psio_address {
+    size_t page = 0, offset = 0;
+};
+static const psio_address PSIO_ZERO = {0, 0};
+enum { PSIO_OPEN_NEW = 0, PSIO_OPEN_OLD = 1 };
+typedef std::map<std::pair<int, std::string>, std::string> PsioStore;
+inline PsioStore &psio_store() {
+    static PsioStore store;
+    return store;
+}
+class PSIO {
+  public:
+    void open(int unit, int mode) {
+        if (mode != PSIO_OPEN_NEW) return;
+        PsioStore &s = psio_store();
+        for (auto it = s.begin(); it != s.end();)
+            it = it->first.first == unit ? s.erase(it) : std::next(it);
+    }
+    void close(int, int) {}
+    bool exists(int unit) {
+        for (auto &kv : psio_store())
+            if (kv.first.first == unit) return true;
+        return false;
+    }
+    void write(int unit, const char *key, char *buf, size_t size, psio_address start, psio_address *end) {
+        std::string &e = psio_store()[{unit, key}];
+        if (e.size() < start.offset + size) e.resize(start.offset + size);
+        std::memcpy(&e[start.offset], buf, size);
+        if (end) *end = psio_address{0, start.offset + size};
+    }
+    void write_entry(int unit, const char *key, char *buf, size_t size) {
+        write(unit, key, buf, size, PSIO_ZERO, nullptr);
+    }
+    void read(int unit, const char *key, char *buf, size_t size, psio_address start, psio_address *end) {
+        const std::string &e = psio_store().at({unit, key});
+        std::memcpy(buf, e.data() + start.offset, size);
+        if (end) *end = psio_address{0, start.offset + size};
+    }
+    void read_entry(int unit, const char *key, char *buf, size_t size) { read(unit, key, buf, size, PSIO_ZERO, nullptr); }
+};
+
 }  // namespace psi
 
 #endif

@@ -1,0 +1,73 @@
+"""The density-matrix records hilbert writes after a solve (WriteTPDM,
+WriteTPDMSpinFree, WriteOPDM), from the product library against what the
+reference's own compiled writers emit into the PSIO stand-in."""
+import itertools
+import os
+
+import numpy as np
+import pytest
+
+import hilbert_b200 as hb
+from oracle.maps import ref_available
+
+pytestmark = pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+
+
+def cases():
+    for n, na, nb in itertools.product([1, 2, 3, 4], [0, 1, 2, 3], [0, 1, 2]):
+        if na <= n and nb <= n:
+            yield n, na, nb
+
+
+def test_rdm_entries_match_the_reference_writers():
+    """Every record and every metadata entry, byte for byte."""
+    from oracle.maps import RefProblem
+    rng = np.random.default_rng(17)
+    for n, na, nb in cases():
+        r = RefProblem(n, na, nb, "DQG", True, True, h=rng.standard_normal((n, n)),
+                       g=rng.standard_normal((n,) * 4))
+        x = rng.standard_normal(r.n_primal)
+        _, ref_entries = r.write_rdms(x)
+        p = hb.V2RDMProblem(n, na, nb, "DQG")
+        mine = p.rdm_entries(x)
+        assert set(mine) == set(ref_entries)
+        for name, entries in ref_entries.items():
+            assert set(mine[name]) == set(entries) - {"INACTIVE ORBITALS"}, name
+            for key, val in entries.items():
+                if key != "INACTIVE ORBITALS":   # empty without core orbitals
+                    assert mine[name][key] == val, (n, na, nb, name, key)
+        p.close()
+
+
+def test_spin_free_sign_follows_the_reference():
+    """WriteTPDMSpinFree signs the aa and bb terms -1 when either pair is
+    reversed (write_tpdm.cc:349-351), so an element with both pairs reversed
+    differs from the spin sum of the D2aa/D2bb records."""
+    p = hb.V2RDMProblem(3, 1, 1, "D")
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(p.n_primal)
+    rec = p.rdm_records(x)
+    d2, aa, bb, ab = rec["D2"], rec["D2aa"], rec["D2bb"], rec["D2ab"]
+    key = lambda r: (int(r["i"]), int(r["j"]), int(r["k"]), int(r["l"]))
+    vab = {key(r): r["value"] for r in ab}
+    vaa = {key(r): r["value"] for r in aa}
+    vbb = {key(r): r["value"] for r in bb}
+    for r in d2:
+        i, j, k, l = key(r)
+        if i == j or k == l:
+            continue
+        sum_spin = vab[(i, j, k, l)] + vab[(j, i, l, k)] + vaa[(i, j, k, l)] + vbb[(i, j, k, l)]
+        if i > j and k > l:
+            assert r["value"] != pytest.approx(sum_spin)
+        else:
+            assert r["value"] == pytest.approx(sum_spin, abs=1e-12)
+
+
+def test_rdm_files_round_trip(tmp_path):
+    p = hb.V2RDMProblem(3, 2, 1, "DQG")
+    x = np.random.default_rng(2).standard_normal(p.n_primal)
+    path = os.path.join(tmp_path, "rdms.npz")
+    p.write_rdm_files(path, x)
+    assert hb.V2RDMProblem.read_rdm_files(path) == p.rdm_entries(x)
+    with pytest.raises(hb.V2BError):
+        hb.DOCIProblem(3, 1, 1, "DQG").rdm_records(np.zeros(hb.DOCIProblem(3, 1, 1, "DQG").n_primal))
