@@ -45,7 +45,7 @@ EXPORTS = (
     "v2b_problem_projection_counts", "v2b_problem_refine_counts", "v2b_problem_set_projection_mode", "v2b_problem_pack_dims", "v2b_problem_projection_profile",
     "v2b_problem_cg_profile",
     "v2b_problem_pack_spatial_density", "v2b_project_block_noalloc",
-    "v2b_problem_rdm_counts", "v2b_problem_rdm_records",
+    "v2b_problem_rdm_counts", "v2b_problem_rdm_records", "v2b_problem_set_state",
 )
 
 
@@ -133,6 +133,7 @@ def load(path=LIB_PATH):
         "v2b_problem_set_projection_mode": (ctypes.c_int, [vp, ctypes.c_int]),
         "v2b_problem_pack_dims": (ctypes.c_int, [vp, lp, lp]),
         "v2b_problem_rdm_counts": (ctypes.c_int, [vp, vp]),
+        "v2b_problem_set_state": (ctypes.c_int, [vp, ctypes.c_double, dp, dp]),
         "v2b_problem_rdm_records": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, vp, vp]),
         "v2b_problem_projection_profile": (ctypes.c_int, [vp, dp, lp, ctypes.c_int]),
         "v2b_problem_cg_profile": (ctypes.c_int, [vp, dp, ctypes.c_int]),

@@ -1078,6 +1078,9 @@ struct v2b_problem {
     // host operator tables, built once at creation
     v2b::PackedOperator hostA, hostAT;
     bool on_device = false;
+    // a restart state (v2b_problem_set_state) that the next solve starts from
+    bool resume = false;
+    std::vector<double> resume_y, resume_z;
 
     // device resources are created on first device use, so that the host-side
     // problem (sizes, b, c, guesses, operator tables) needs no GPU
@@ -1214,11 +1217,20 @@ struct v2b_problem {
                      void *data, long *oiter_out, long *iiter_out, double *energy) {
         if (muf < 1) throw std::invalid_argument("mu_update_frequency must be >= 1");
         const int64_t np = prob.n_primal, nd = prob.n_dual;
-        mu = 0.1;
         ensure_plan();
         plan.reset();
-        V2B_CK(cudaMemsetAsync(y, 0, nd * 8, stream));
-        V2B_CK(cudaMemsetAsync(z, 0, np * 8, stream));
+        if (resume) {   // mu was set with the state
+            V2B_CK(cudaMemcpyAsync(y, resume_y.data(), nd * 8, cudaMemcpyHostToDevice, stream));
+            V2B_CK(cudaMemcpyAsync(z, resume_z.data(), np * 8, cudaMemcpyHostToDevice, stream));
+            V2B_CK(cudaStreamSynchronize(stream));
+            resume = false;
+            std::vector<double>().swap(resume_y);
+            std::vector<double>().swap(resume_z);
+        } else {
+            mu = 0.1;
+            V2B_CK(cudaMemsetAsync(y, 0, nd * 8, stream));
+            V2B_CK(cudaMemsetAsync(z, 0, np * 8, stream));
+        }
         V2B_CK(cudaMemsetAsync(status, 0, 8, stream));
         v2b::spmv_A2_kernel<<<grid_for(nd, v2b::kSpmvThreads), v2b::kSpmvThreads, 0, stream>>>(
             A.rp, A.ent, nd, x, c, z, Ax, Acz, A.pal);
@@ -1589,6 +1601,17 @@ int v2b_problem_get_y(const v2b_problem *p, double *y) {
         if (!p || !y) throw std::invalid_argument("get_y: NULL argument");
         if (!p->on_device) throw std::invalid_argument("get_y: no device solve has run");
         V2B_CK(cudaMemcpy(y, p->y, p->prob.n_dual * 8, cudaMemcpyDeviceToHost));
+        return V2B_OK;
+    });
+}
+int v2b_problem_set_state(v2b_problem *p, double mu, const double *y, const double *z) {
+    return guarded([&] {
+        if (!p || !y || !z) throw std::invalid_argument("set_state: NULL argument");
+        if (!(mu > 0.0) || !std::isfinite(mu)) throw std::invalid_argument("set_state: mu must be positive");
+        p->resume_y.assign(y, y + p->prob.n_dual);
+        p->resume_z.assign(z, z + p->prob.n_primal);
+        p->mu = mu;
+        p->resume = true;
         return V2B_OK;
     });
 }

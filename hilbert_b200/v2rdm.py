@@ -233,6 +233,17 @@ class V2RDMProblem:
         check(self._lib.v2b_problem_get_y(self._h, _dptr(out)))
         return out
 
+    def get_mu(self):
+        return self._lib.v2b_problem_get_mu(self._h)
+
+    def set_state(self, mu, y, z):
+        """The next solve starts from mu, y and z (a restart from a checkpoint)."""
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        z = np.ascontiguousarray(z, dtype=np.float64)
+        if y.shape != (self.n_dual,) or z.shape != (self.n_primal,):
+            raise ValueError(f"y must hold {self.n_dual} values and z {self.n_primal}")
+        check(self._lib.v2b_problem_set_state(self._h, float(mu), _dptr(y), _dptr(z)))
+
     def get_z(self):
         out = np.zeros(self.n_primal)
         check(self._lib.v2b_problem_get_z(self._h, _dptr(out)))

@@ -174,6 +174,13 @@ int v2b_problem_solve_device(v2b_problem *p, double *d_x, const double *d_b, con
 int v2b_problem_get_y(const v2b_problem *p, double *y);
 int v2b_problem_get_z(const v2b_problem *p, double *z);
 double v2b_problem_get_mu(const v2b_problem *p);
+/* Restart from a checkpoint (ReadFromCheckpointFile,
+ * src/v2rdm_casscf/checkpoint.cc:90-124: MU, DUAL 1 = y, DUAL 2 = z; PRIMAL
+ * is the solve's own x argument): the next v2b_problem_solve or
+ * v2b_problem_solve_device starts from mu > 0, y (n_dual) and z (n_primal)
+ * instead of mu = 0.1 and y = z = 0.  Host arrays, copied here; one solve
+ * uses them. */
+int v2b_problem_set_state(v2b_problem *p, double mu, const double *y, const double *z);
 /* The packed constraint operator the device maps read: A (transposed = 0,
  * rows = dual constraints) or A^T (transposed = 1, rows = primal elements).
  * Entry bits 0..26 hold the column, 27..30 an index into the palette of
