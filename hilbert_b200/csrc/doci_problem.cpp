@@ -1,6 +1,7 @@
 // v2RDM-DOCI sizes, b and c (see doci_problem.h for the rows of A).
 #include "doci_problem.h"
 
+#include <algorithm>
 #include <cstring>
 #include <stdexcept>
 
@@ -75,7 +76,50 @@ Problem make_doci_problem(const ProblemSpec &spec) {
     p.n_dual = d;
     if (p.n_primal > (int64_t)kColMask || p.n_dual > (int64_t)kColMask)
         throw std::invalid_argument("problem too large for 27-bit packed column indices");
+    // the ab / aa geminal tables: DOCI's BuildBasis numbers them with the same
+    // loops as the v2RDM basis (src/v2rdm_doci/basis.cc:425-535)
+    ProblemSpec t;
+    t.nmo = (int)n;
+    t.positivity = POS_D;
+    const Problem tab = make_problem(t);
+    p.gab = tab.gab;
+    p.gaa = tab.gaa;
+    p.bas_ab = tab.bas_ab;
+    p.ibas_ab = tab.ibas_ab;
+    p.bas_aa = tab.bas_aa;
+    p.ibas_aa = tab.ibas_aa;
     return p;
+}
+
+int64_t doci_v2rdm_layout_size(const Problem &p) {
+    return (int64_t)p.gab * p.gab + 2 * (int64_t)p.gaa * p.gaa + 2 * (int64_t)p.n * p.n;
+}
+
+void doci_v2rdm_layout(const Problem &p, const double *x, double *out) {
+    // v2rdm_doci_solver.cc:1570-1597 builds D2aa (= D2bb) and D2ab from the
+    // seniority blocks; D1 is diagonal, the same for both spins (:1693-1700)
+    const int64_t n = p.n, gab = p.gab, gaa = p.gaa;
+    const int64_t ab = 0, aa = gab * gab, bb = aa + gaa * gaa, d1a = bb + gaa * gaa, d1b = d1a + n * n;
+    const DociOffsets &o = p.doci;
+    std::memset(out, 0, sizeof(double) * doci_v2rdm_layout_size(p));
+    for (int64_t g = 0; g < gaa; g++) {
+        // the reference's aa pair (i, j) has i > j (basis.cc:520-526)
+        const int64_t i = std::max(p.bas_aa[2 * g], p.bas_aa[2 * g + 1]);
+        const int64_t j = std::min(p.bas_aa[2 * g], p.bas_aa[2 * g + 1]);
+        out[aa + g * gaa + g] = x[o.d2s2 + i * n + j];
+        out[bb + g * gaa + g] = x[o.d2s2 + i * n + j];
+    }
+    for (int64_t g = 0; g < gab; g++) {
+        const int64_t i = p.bas_ab[2 * g], j = p.bas_ab[2 * g + 1];
+        if (i != j) out[ab + g * gab + g] = x[o.d2s2 + i * n + j];
+    }
+    for (int64_t i = 0; i < n; i++)
+        for (int64_t j = 0; j < n; j++)
+            out[ab + (int64_t)p.iab((int)i, (int)i) * gab + p.iab((int)j, (int)j)] = x[o.d2s0 + i * n + j];
+    for (int64_t i = 0; i < n; i++) {
+        out[d1a + i * n + i] = x[o.d1 + i];
+        out[d1b + i * n + i] = x[o.d1 + i];
+    }
 }
 
 void doci_build_b(const Problem &p, double *b) {

@@ -20,6 +20,10 @@ namespace v2b {
 Problem make_doci_problem(const ProblemSpec &spec);
 void doci_build_b(const Problem &p, double *b);
 void doci_build_c_external(const Problem &p, const double *h, const double *g, double *c);
+// x in the v2RDM layout (D2ab gab^2, D2aa gaa^2, D2bb gaa^2, D1a n^2, D1b n^2)
+// that hilbert's DOCI PackSpatialDensity builds before packing
+int64_t doci_v2rdm_layout_size(const Problem &p);
+void doci_v2rdm_layout(const Problem &p, const double *x, double *out);
 
 struct DociTerm {
     int64_t col;

@@ -29,6 +29,7 @@
 #include "v2rdm_b200.h"
 #include "v2rdm_problem.h"
 #include "rdm_records.h"
+#include "doci_problem.h"
 
 namespace {
 
@@ -1014,6 +1015,7 @@ struct v2b_problem {
     unsigned int *stats_counter = nullptr;
     v2b::GridBarrier *bar = nullptr;
     int *ibas_aa_dev = nullptr;   // n x n aa geminal numbers, for the density packing
+    double *pack_layout = nullptr;   // DOCI: x in the v2RDM layout, for the density packing
     int *status = nullptr;   // [0] fatal device status, [1] projection sweeps exhausted
     double *h_readback = nullptr;   // pinned: stats[4], cg_out[2], status[2]
     int cg_grid = 0;
@@ -1065,6 +1067,7 @@ struct v2b_problem {
                           stats_partials})
             cudaFree(p);
         if (cg_phase) cudaFree(cg_phase);
+        if (pack_layout) cudaFree(pack_layout);
         cudaFree(stats_counter);
         cudaFree(bar);
         cudaFree(ibas_aa_dev);
@@ -1704,6 +1707,18 @@ int v2b_problem_projection_profile(const v2b_problem *p, double *ms, long *n, in
         return V2B_OK;
     });
 }
+int v2b_doci_v2rdm_layout(const v2b_problem *p, const double *x, double *out, long *size) {
+    return guarded([&] {
+        if (!p || !size) throw std::invalid_argument("doci_v2rdm_layout: NULL argument");
+        if (!p->prob.spec.doci) throw std::invalid_argument("doci_v2rdm_layout: not a DOCI problem");
+        *size = (long)v2b::doci_v2rdm_layout_size(p->prob);
+        if (out) {
+            if (!x) throw std::invalid_argument("doci_v2rdm_layout: NULL x");
+            v2b::doci_v2rdm_layout(p->prob, x, out);
+        }
+        return V2B_OK;
+    });
+}
 int v2b_problem_rdm_counts(const v2b_problem *p, long *counts) {
     return guarded([&] {
         if (!p || !counts) throw std::invalid_argument("rdm_counts: NULL argument");
@@ -1729,7 +1744,6 @@ int v2b_problem_rdm_records(const v2b_problem *p, const double *x, v2b_tpdm_reco
 int v2b_problem_pack_dims(const v2b_problem *p, long *d2_size, long *d1_size) {
     return guarded([&] {
         if (!p || !d2_size || !d1_size) throw std::invalid_argument("pack_dims: NULL argument");
-        if (p->prob.spec.doci) throw std::invalid_argument("pack_dims: the v2RDM density packing, not DOCI's");
         const long g00 = (long)p->prob.n * (p->prob.n + 1) / 2;
         *d2_size = g00 * (g00 + 1) / 2;
         *d1_size = g00;
@@ -1740,8 +1754,6 @@ int v2b_problem_pack_spatial_density(v2b_problem *p, const double *d_x, double *
                                      void *stream) {
     return guarded([&] {
         if (!p || !d_x || !d_d2 || !d_d1) throw std::invalid_argument("pack_spatial_density: NULL argument");
-        if (p->prob.spec.doci)
-            throw std::invalid_argument("pack_spatial_density: the v2RDM density packing, not DOCI's");
         p->setup();
         const v2b::Problem &q = p->prob;
         if (!p->ibas_aa_dev) {
@@ -1753,6 +1765,25 @@ int v2b_problem_pack_spatial_density(v2b_problem *p, const double *d_x, double *
         a.n = q.n;
         a.d2ab = q.d2ab; a.d2aa = q.d2aa; a.d2bb = q.d2bb; a.d1a = q.d1a; a.d1b = q.d1b;
         a.ibas_aa = p->ibas_aa_dev;
+        if (q.spec.doci) {
+            // hilbert's DOCI packing (v2rdm_doci_solver.cc:1568-1703) is the
+            // v2RDM packing of D2ab, D2aa = D2bb and D1a = D1b expanded from
+            // the seniority blocks; D2s2, D2s0 and D1 lead the primal vector
+            const int64_t n = q.n, lead = 2 * n * n + n, size = v2b::doci_v2rdm_layout_size(q);
+            if (q.doci.d2s2 != 0 || q.doci.d2s0 != n * n || q.doci.d1 != 2 * n * n)
+                throw std::logic_error("DOCI block layout");
+            std::vector<double> blocks(lead), layout(size);
+            V2B_CK(cudaMemcpyAsync(blocks.data(), d_x, lead * 8, cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+            V2B_CK(cudaStreamSynchronize((cudaStream_t)stream));
+            v2b::doci_v2rdm_layout(q, blocks.data(), layout.data());
+            if (!p->pack_layout) p->pack_layout = dalloc<double>(size);
+            V2B_CK(cudaMemcpyAsync(p->pack_layout, layout.data(), size * 8, cudaMemcpyHostToDevice,
+                                   (cudaStream_t)stream));
+            V2B_CK(cudaStreamSynchronize((cudaStream_t)stream));   // layout is a host temporary
+            const int64_t gab2 = (int64_t)q.gab * q.gab, gaa2 = (int64_t)q.gaa * q.gaa;
+            a.d2ab = 0; a.d2aa = gab2; a.d2bb = gab2 + gaa2; a.d1a = gab2 + 2 * gaa2; a.d1b = a.d1a + n * n;
+            d_x = p->pack_layout;
+        }
         const int64_t g00 = (int64_t)q.n * (q.n + 1) / 2, total = g00 * (g00 + 1) / 2 + g00;
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 148 * 8));
         v2b::pack_spatial_density_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(d_x, a, d_d2, d_d1);

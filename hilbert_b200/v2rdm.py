@@ -408,6 +408,24 @@ class DOCIProblem(V2RDMProblem):
         check(lib.v2b_doci_problem_create(int(nmo), int(nalpha), int(nbeta), code, ctypes.byref(h)))
         self._sizes(h, nmo, nalpha, nbeta)
 
+    def v2rdm_layout(self, x):
+        """{"d2ab", "d2aa", "d2bb", "d1a", "d1b"}: the spin blocks of a DOCI
+        solution as hilbert's DOCI PackSpatialDensity builds them
+        (v2rdm_doci_solver.cc:1570-1597), flat, geminals numbered as in
+        V2RDMProblem."""
+        xh = np.ascontiguousarray(x.detach().cpu().numpy() if hasattr(x, "detach") else x,
+                                  dtype=np.float64)
+        if xh.shape != (self.n_primal,):
+            raise ValueError(f"x must hold {self.n_primal} values")
+        size = ctypes.c_long()
+        check(self._lib.v2b_doci_v2rdm_layout(self._h, None, None, ctypes.byref(size)))
+        out = np.zeros(size.value)
+        check(self._lib.v2b_doci_v2rdm_layout(self._h, xh.ctypes.data, out.ctypes.data, ctypes.byref(size)))
+        n = int(self.nmo)
+        gab, gaa = n * n, n * (n - 1) // 2
+        cuts = np.cumsum([gab * gab, gaa * gaa, gaa * gaa, n * n])
+        return dict(zip(("d2ab", "d2aa", "d2bb", "d1a", "d1b"), np.split(out, cuts)))
+
 
 class BPSDPSolver:
     """libsdp::BPSDPSolver with host callbacks (evaluate_Au / evaluate_ATu)."""

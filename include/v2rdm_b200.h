@@ -123,9 +123,17 @@ int v2b_problem_create(int nmo, int nalpha, int nbeta, int positivity, int const
  * (ij|kl) (RepackIntegrals, tei.cc:127-153), the random guess (:1325-1336),
  * A.x and A^T.y (bpsdp_Au / bpsdp_ATu, :1509-1566) and the solves.
  * positivity = V2B_POSITIVITY_* | V2B_CONSTRAIN_D3.  DOCI has no Hubbard c,
- * no HF guess and not the v2RDM density packing: those calls return
- * V2B_BAD_ARG. */
+ * no HF guess and no v2RDM RDM records: those calls return V2B_BAD_ARG.
+ * v2b_problem_pack_spatial_density packs a DOCI solution as hilbert's DOCI
+ * PackSpatialDensity does (v2rdm_doci_solver.cc:1568-1703). */
 int v2b_doci_problem_create(int nmo, int nalpha, int nbeta, int positivity, v2b_problem **out);
+/* A DOCI primal vector (host) in the v2RDM spin-block layout that hilbert's
+ * DOCI PackSpatialDensity builds first (v2rdm_doci_solver.cc:1570-1597):
+ * D2ab (gab^2, gab = nmo^2), D2aa and D2bb (gaa^2 each, gaa = nmo(nmo-1)/2,
+ * D2bb = D2aa), D1a and D1b (nmo^2 each, diagonal), geminals numbered as
+ * v2b_problem_create numbers them.  *size receives the length; out may be
+ * NULL to ask for it. */
+int v2b_doci_v2rdm_layout(const v2b_problem *p, const double *x, double *out, long *size);
 void v2b_problem_destroy(v2b_problem *p);
 long v2b_problem_n_primal(const v2b_problem *p);
 long v2b_problem_n_dual(const v2b_problem *p);

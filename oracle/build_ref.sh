@@ -89,7 +89,7 @@ dgen="$out/doci_solver_extract.cc"
   echo 'using namespace psi;'
   echo 'namespace hilbert {'
   extract_class v2RDM_DOCISolver "$dsrc/v2rdm_doci_solver.cc" SymmetryPair TotalSym \
-      BuildConstraints Guess bpsdp_Au bpsdp_ATu
+      BuildConstraints Guess bpsdp_Au bpsdp_ATu PackSpatialDensity
   echo 'void v2RDM_DOCISolver::common_init() {'
   awk '/pick conditions\.  default is dqg/ { on = 1 }
        /v2rdm sdp convergence thresholds/ { on = 0 }
@@ -97,7 +97,7 @@ dgen="$out/doci_solver_extract.cc"
   echo '}'
   echo '}'
 } > "$dgen"
-for name in SymmetryPair TotalSym BuildConstraints Guess bpsdp_Au bpsdp_ATu; do
+for name in SymmetryPair TotalSym BuildConstraints Guess bpsdp_Au bpsdp_ATu PackSpatialDensity; do
   grep -q "v2RDM_DOCISolver::${name}(" "$dgen" || { echo "build_ref.sh: could not extract DOCI ${name}" >&2; exit 3; }
 done
 grep -q "dimensions_.push_back" "$dgen" || { echo "build_ref.sh: could not extract the DOCI sizing" >&2; exit 3; }

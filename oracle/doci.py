@@ -67,6 +67,9 @@ def _lib(kind):
             lib.doci_ref_last_error.restype = ctypes.c_char_p
             for f in ("get_b", "get_c", "get_x"):
                 getattr(lib, "doci_ref_" + f).argtypes = [ctypes.c_void_p, _dp]
+            lib.doci_ref_pack_dims.restype = ctypes.c_long
+            lib.doci_ref_pack_dims.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long)]
+            lib.doci_ref_pack_spatial.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
         _libs[kind] = lib
     return _libs[kind]
 
@@ -159,6 +162,19 @@ class DociRef(_Base):
         if hh is not None:
             self.c = np.zeros(self.n_primal)
             lib.doci_ref_get_c(self._h, self.c)
+
+
+def _ref_pack(self, x):
+    """hilbert's DOCI PackSpatialDensity (v2rdm_doci_solver.cc:1568-1703) of x:
+    the packed spin-summed active D2 and D1"""
+    d1n = ctypes.c_long()
+    d2n = self._lib.doci_ref_pack_dims(self._h, ctypes.byref(d1n))
+    d2, d1 = np.zeros(d2n), np.zeros(d1n.value)
+    self._lib.doci_ref_pack_spatial(self._h, np.ascontiguousarray(x, np.float64), d2, d1)
+    return d2, d1
+
+
+DociRef.pack_spatial_density = _ref_pack
 
 
 def symmetric_integrals(rng, n):

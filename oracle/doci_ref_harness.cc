@@ -72,6 +72,7 @@ class RefDoci : private OptionHolder, public v2RDM_DOCISolver {
         amopi_[0] = nmo;
         amo_ = nmo;
         nfrzc_ = nfrzv_ = nrstc_ = nrstv_ = 0;
+        d2_act_spatial_sym_ = d1_act_spatial_sym_ = nullptr;
         epsilon_a_ = std::make_shared<Vector>(nmopi_);
         epsilon_b_ = std::make_shared<Vector>(nmopi_);
 
@@ -105,6 +106,23 @@ class RefDoci : private OptionHolder, public v2RDM_DOCISolver {
         c->zero();
         RepackIntegrals();
     }
+
+    /* PackSpatialDensity (v2rdm_doci_solver.cc:1568-1703) on a given x, with
+       the buffers GetIntegrals would allocate (tei.cc:74-94) */
+    void pack(const double *xin, double *d2, double *d1) {
+        std::memcpy(x->pointer(), xin, sizeof(double) * dimx_);
+        d2_act_spatial_dim_ = gems_00[0] * (gems_00[0] + 1) / 2;
+        d1_act_spatial_dim_ = amo_ * (amo_ + 1) / 2;
+        free(d2_act_spatial_sym_);
+        free(d1_act_spatial_sym_);
+        d2_act_spatial_sym_ = (double *)calloc(d2_act_spatial_dim_, sizeof(double));
+        d1_act_spatial_sym_ = (double *)calloc(d1_act_spatial_dim_, sizeof(double));
+        PackSpatialDensity();
+        std::memcpy(d2, d2_act_spatial_sym_, sizeof(double) * d2_act_spatial_dim_);
+        std::memcpy(d1, d1_act_spatial_sym_, sizeof(double) * d1_act_spatial_dim_);
+    }
+    long d2_dim() const { return (long)gems_00[0] * (gems_00[0] + 1) / 2; }
+    long d1_dim() const { return (long)amo_ * (amo_ + 1) / 2; }
 
     static Options &set(Options &o, const char *positivity, bool d3) {
         o.set_str("POSITIVITY", positivity);
@@ -185,6 +203,11 @@ void doci_ref_Au(void *p, const double *x, double *out) {
     std::vector<double> u(x, x + r->n_primal());
     r->bpsdp_Au(out, u.data());
 }
+long doci_ref_pack_dims(void *p, long *d1n) {
+    *d1n = ((RefDoci *)p)->d1_dim();
+    return ((RefDoci *)p)->d2_dim();
+}
+void doci_ref_pack_spatial(void *p, const double *x, double *d2, double *d1) { ((RefDoci *)p)->pack(x, d2, d1); }
 void doci_ref_ATu(void *p, const double *y, double *out) {
     RefDoci *r = (RefDoci *)p;
     std::vector<double> u(y, y + r->n_dual());

@@ -4,7 +4,8 @@ code.
 Requires oracle/_ref/libdoci_ref.so (oracle/build_ref.sh, which compiles the
 reference's src/v2rdm_doci sources in place).  Each case stores seeded
 integrals and inputs with the reference's outputs: block dims, b, c, the
-random guess, A.x and A^T.y.  Run from the repository root:
+random guess, A.x, A^T.y and the packed densities of PackSpatialDensity.
+Run from the repository root:
 
     python tests/golden/make_doci_golden.py
 """
@@ -45,6 +46,8 @@ def main():
                     f"{name}/dims": r.dims, f"{name}/h": h, f"{name}/g": g,
                     f"{name}/b": r.b, f"{name}/c": r.c, f"{name}/x0": r.x0,
                     f"{name}/x": x, f"{name}/Ax": r.Au(x), f"{name}/y": y, f"{name}/ATy": r.ATu(y)})
+        pd2, pd1 = r.pack_spatial_density(x)   # PackSpatialDensity of the same x
+        out.update({f"{name}/pd2": pd2, f"{name}/pd1": pd1})
         r.close()
     path = os.path.join(ROOT, "tests", "golden", "doci_maps.npz")
     np.savez_compressed(path, **out)

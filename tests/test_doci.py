@@ -152,9 +152,35 @@ def test_doci_refusals():
         p.guess("HF")
     with pytest.raises(_capi.V2BError):
         p.c_hubbard(1.0, 4.0)
-    d2, d1 = ctypes.c_long(), ctypes.c_long()
-    assert lib.v2b_problem_pack_dims(p._h, ctypes.byref(d2), ctypes.byref(d1)) == _capi.V2B_BAD_ARG
+    with pytest.raises(_capi.V2BError):
+        p.rdm_records(np.zeros(p.n_primal))
     p.close()
+
+
+def test_doci_layout_packs_like_the_reference():
+    """The DOCI spin blocks of v2rdm_layout, packed by hilbert's own v2RDM
+    PackSpatialDensity, give what hilbert's DOCI PackSpatialDensity gives
+    (the device packing of DOCI runs the v2RDM kernel on that layout)."""
+    if not (ref_available() and os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libv2rdm_ref.so"))):
+        pytest.skip("oracle/_ref not built")
+    from oracle.maps import RefProblem
+    rng = np.random.default_rng(23)
+    for n, pos in itertools.product([1, 2, 3, 4, 5], ["D", "DQG", "DQGT1T2+D3"]):
+        if n < 2 and pos.endswith("D3"):
+            continue
+        na = max(1, n // 2)
+        d = DociRef(n, na, na, pos)
+        x = rng.standard_normal(d.n_primal)
+        want_d2, want_d1 = d.pack_spatial_density(x)
+        p = product(n, na, na, pos)
+        layout = p.v2rdm_layout(x)
+        r = RefProblem(n, na, na, "D", False, True, h=np.zeros((n, n)), g=np.zeros((n,) * 4))
+        full = np.zeros(r.n_primal)
+        for block, v in layout.items():
+            full[r.offsets[block]:r.offsets[block] + len(v)] = v
+        got_d2, got_d1 = r.pack_spatial_density(full)
+        assert np.array_equal(got_d2, want_d2) and np.array_equal(got_d1, want_d1), (n, pos)
+        p.close()
 
 
 # --------------------------------------------------------------- oracle solve

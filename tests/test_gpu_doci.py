@@ -24,6 +24,8 @@ def test_doci_device_maps_golden(cuda_device, name):
     y = torch.from_numpy(case["y"]).to(cuda_device)
     assert_Au_matches(p.Au(x).cpu().numpy(), case["Ax"], n, pos, case["x"])
     assert np.array_equal(p.ATu(y).cpu().numpy(), case["ATy"])
+    d2, d1 = p.pack_spatial_density(x)
+    assert np.array_equal(d2.cpu().numpy(), case["pd2"]) and np.array_equal(d1.cpu().numpy(), case["pd1"])
     p.close()
 
 

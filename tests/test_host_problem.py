@@ -56,7 +56,7 @@ def product_problem(kw):
 
 def test_header_symbols_exported():
     header = open(os.path.join(ROOT, "include", "v2rdm_b200.h")).read()
-    declared = set(re.findall(r"\b(v2b_[A-Za-z_]+)\s*\(", header))
+    declared = set(re.findall(r"\b(v2b_[A-Za-z0-9_]+)\s*\(", header))
     declared -= {"v2b_sdp_callback", "v2b_sdp_monitor"}
     lib = _capi.load()
     for name in declared:
