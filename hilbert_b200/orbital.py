@@ -422,3 +422,40 @@ def casscf(h, B, ncore, nact, solve_active, macro_iterations=8, active_active=Fa
         h = U.T @ h @ U
         B = U.T @ B @ U
     return energies, gnorms, h, B
+
+
+def doci_solve_active(nmo, nalpha, nbeta, positivity="DQG", options=None):
+    """The active solve of v2RDM-DOCI on the device, for casscf: builds the
+    DOCI problem once, and for each (h, g) solves it from the random guess
+    (v2rdm_doci_solver.cc:1058-1137) and packs its densities as hilbert's
+    DOCI PackSpatialDensity does (:1568-1703)."""
+    from . import v2rdm
+    p = v2rdm.DOCIProblem(nmo, nalpha, nbeta, positivity)
+    opts = options or v2rdm.Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6,
+                                     "MAXITER": 100000, "MU_UPDATE_FREQUENCY": 500})
+
+    def solve(h_act, g_act):
+        dev = h_act.device
+        b = torch.from_numpy(p.b()).to(dev)
+        c = torch.from_numpy(p.c_external(h_act.cpu().numpy(), g_act.cpu().numpy())).to(dev)
+        x = torch.from_numpy(p.guess("RANDOM")).to(dev)
+        st = p.solve_device(x, b, c, opts)
+        if not st["converged"]:
+            raise RuntimeError("v2RDM-DOCI solve did not converge")
+        d2p, d1p = p.pack_spatial_density(x)
+        return float(c @ x), d2p, d1p
+
+    solve.problem = p
+    return solve
+
+
+def doci_casscf(h, B, nalpha, nbeta, solve_active=None, positivity="DQG", macro_iterations=8):
+    """Orbital-optimised v2RDM-DOCI: every orbital is active (no core, no
+    virtuals) and active-active rotations are on, as hilbert's DOCI
+    RotateOrbitals sets focas up (v2rdm_doci_solver.cc:997-1019, 1705-1766).
+    solve_active defaults to the device DOCI solve (doci_solve_active)."""
+    nmo = h.shape[0]
+    if solve_active is None:
+        solve_active = doci_solve_active(nmo, nalpha, nbeta, positivity)
+    return casscf(h, B, 0, nmo, solve_active, macro_iterations=macro_iterations, active_active=True,
+                  orbital_step="focas")

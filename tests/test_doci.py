@@ -234,3 +234,32 @@ def test_doci_relaxations_bound_exact_doci():
     assert s_d.is_converged() and s_dqg.is_converged()
     assert e_d <= e_dqg + 1e-6 and e_dqg <= exact + 1e-6
     assert exact - e_dqg < 0.5   # DQG recovers most of the gap left by D (2.85 Eh here)
+
+
+@needs_ref
+def test_doci_orbital_optimisation_with_the_focas_step():
+    """doci_casscf on the CPU with the oracle's DOCI solve and hilbert's
+    compiled DOCI packing: all orbitals active, active-active rotations on.
+    The energy falls and the orbital gradient shrinks."""
+    import torch
+    import hilbert_b200.orbital as ho
+    from oracle.bpsdp import SDPOptions, run_v2rdm
+    n, npair = 4, 2
+    h_mo, B_mo, *_ = ho.casscf_df_problem(nbf=n, naux=10, ncore=0, nact=n)
+
+    def solve_active(h_act, g_act):
+        h, g = h_act.numpy(), g_act.numpy()
+        o = DociOracle(n, npair, npair, "DQG")
+        prob = types.SimpleNamespace(n_primal=o.n_primal, n_dual=o.n_dual, b=o.b(), c=o.c(h, g),
+                                     dims=[int(d) for d in o.dims], Au=o.Au, ATu=o.ATu)
+        x, solver = run_v2rdm(prob, o.guess(), SDPOptions(1e-7, 1e-7, 1e-10, 10000, 20000), 500)
+        assert solver.is_converged()
+        e = float(prob.c @ x)
+        assert e <= seniority_zero_ci(h, g, npair) + 1e-6
+        d2p, d1p = DociRef(n, npair, npair, "DQG").pack_spatial_density(x)
+        return e, torch.from_numpy(d2p), torch.from_numpy(d1p)
+
+    E, gn, _, _ = ho.doci_casscf(torch.from_numpy(h_mo), torch.from_numpy(B_mo), npair, npair,
+                                 solve_active=solve_active, macro_iterations=2)
+    assert E[1] < E[0] - 1.0
+    assert gn[1] < 0.1 * gn[0]

@@ -63,3 +63,17 @@ def test_doci_device_solve_matches_oracle(cuda_device, pos):
     assert so.is_converged()
     assert abs(e - eo) <= E_TOL
     assert e <= seniority_zero_ci(h, g, 3) + E_TOL
+
+
+def test_doci_casscf_on_the_device(cuda_device):
+    """doci_casscf with the device DOCI solve and packing follows the CPU
+    chain (oracle solve, hilbert's compiled DOCI packing) of test_doci."""
+    import torch
+    import hilbert_b200.orbital as ho
+    n, npair = 4, 2
+    h_mo, B_mo, *_ = ho.casscf_df_problem(nbf=n, naux=10, ncore=0, nact=n)
+    E, gn, _, _ = ho.doci_casscf(torch.from_numpy(h_mo).to(cuda_device), torch.from_numpy(B_mo).to(cuda_device),
+                                 npair, npair, macro_iterations=3)
+    assert all(b <= a + 1e-6 for a, b in zip(E, E[1:]))
+    assert abs(E[0] - (-28.3102401)) <= 1e-5 and abs(E[2] - (-33.5748761)) <= 1e-4
+    assert gn[2] < 0.01 * gn[0]
