@@ -5,8 +5,8 @@ for sm_100a, C++ host orchestration; entry points in include/v2rdm_b200.h).
 This package mirrors hilbert's Python-facing interface on top of it.
 """
 from ._capi import LIB_PATH, V2BError, load  # noqa: F401
-from .v2rdm import (BPSDPSolver, DOCIProblem, Options, V2RDMProblem, block_layout,  # noqa: F401
+from .v2rdm import (BatchProblem, BPSDPSolver, DOCIProblem, Options, V2RDMProblem, block_layout,  # noqa: F401
                     block_offsets, v2RDMHelper)
 
-__all__ = ["BPSDPSolver", "DOCIProblem", "Options", "V2RDMProblem", "v2RDMHelper", "block_layout",
+__all__ = ["BatchProblem", "BPSDPSolver", "DOCIProblem", "Options", "V2RDMProblem", "v2RDMHelper", "block_layout",
            "block_offsets", "load", "LIB_PATH", "V2BError"]

@@ -17,7 +17,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .v2rdm import Options, V2RDMProblem, block_layout
+from .v2rdm import BatchProblem, Options, V2RDMProblem, block_layout
 
 
 @dataclass(frozen=True)
@@ -104,6 +104,56 @@ def solve_on_device(inst, options, device=None):
             p.close()
     return {"energy": energy, "converged": bool(st["converged"]), "oiter": int(st["oiter"]),
             "iiter": int(st["iiter"])}
+
+
+def launch_groups(problems, capacity=16):
+    """Indices of problems grouped for BatchProblem, in order: a group grows
+    while the union of its parts' A and A^T palettes each stays within
+    `capacity` coefficients."""
+    groups, pal_a, pal_at = [], set(), set()
+    for k, p in enumerate(problems):
+        a, at = p.palette(False), p.palette(True)
+        if groups and len(pal_a | a) <= capacity and len(pal_at | at) <= capacity:
+            groups[-1].append(k)
+            pal_a |= a
+            pal_at |= at
+        else:
+            groups.append([k])
+            pal_a, pal_at = set(a), set(at)
+    return groups
+
+
+def solve_in_one_launch(instances, options=None, device=None):
+    """This rank's instances solved together, one BatchProblem per palette
+    group: every device launch of the iteration covers all of a group's
+    instances.  Each instance starts from its own random guess; the results
+    are those of solve_on_device, per instance, in input order, plus the
+    group's shared outer and CG iteration counts."""
+    import torch
+    if options is None:
+        options = Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6, "MAXITER": 400000,
+                           "MU_UPDATE_FREQUENCY": 500})
+    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    built = [inst.problem() for inst in instances]
+    results = [None] * len(instances)
+    with torch.cuda.device(dev):
+        for group in launch_groups([p for p, _, _ in built]):
+            parts = [built[k] for k in group]
+            batch = BatchProblem([p for p, _, _ in parts])
+            try:
+                x = torch.from_numpy(np.concatenate([p.guess("RANDOM") for p, _, _ in parts])).to(dev)
+                b = torch.from_numpy(np.concatenate([b for _, b, _ in parts])).to(dev)
+                c = np.concatenate([c for _, _, c in parts])
+                st = batch.solve_device(x, b, torch.from_numpy(c).to(dev), options)
+                for k, xk, (_, _, ck) in zip(group, batch.split(x), parts):
+                    results[k] = {"energy": float(np.dot(ck, xk)), "converged": bool(st["converged"]),
+                                  "oiter": int(st["oiter"]), "iiter": int(st["iiter"]),
+                                  "group": len(group)}
+            finally:
+                batch.close()
+    for p, _, _ in built:
+        p.close()
+    return results
 
 
 def solve_batch(instances, options=None, rank=0, world=1, group=None, solve=solve_on_device,

@@ -15,6 +15,7 @@ namespace v2b {
 namespace {
 void check(const Problem &p) {
     if (p.spec.doci) throw std::invalid_argument("the v2RDM density records, not DOCI's");
+    if (p.spec.batch_parts) throw std::invalid_argument("density records of a batch: ask each part");
 }
 }  // namespace
 

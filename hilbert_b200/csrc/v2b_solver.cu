@@ -1485,6 +1485,33 @@ int v2b_doci_problem_create(int nmo, int nalpha, int nbeta, int positivity, v2b_
     });
 }
 
+int v2b_problem_palette(const v2b_problem *p, int transposed, double *out, int *count) {
+    return guarded([&] {
+        if (!p || !count) throw std::invalid_argument("palette: NULL argument");
+        const std::vector<double> &pal = transposed ? p->hostAT.palette : p->hostA.palette;
+        *count = (int)pal.size();
+        if (out) std::copy(pal.begin(), pal.end(), out);
+        return V2B_OK;
+    });
+}
+int v2b_batch_problem_create(const v2b_problem *const *parts, int count, v2b_problem **out) {
+    return guarded([&] {
+        if (!out || !parts || count < 1) throw std::invalid_argument("v2b_batch_problem_create: bad argument");
+        std::vector<const v2b::Problem *> probs;
+        std::vector<const v2b::PackedOperator *> A, AT;
+        for (int k = 0; k < count; k++) {
+            if (!parts[k]) throw std::invalid_argument("v2b_batch_problem_create: NULL part");
+            probs.push_back(&parts[k]->prob);
+            A.push_back(&parts[k]->hostA);
+            AT.push_back(&parts[k]->hostAT);
+        }
+        std::unique_ptr<v2b_problem> p(new v2b_problem());
+        v2b::make_batch(probs, A, AT, p->prob, p->hostA, p->hostAT);
+        *out = p.release();
+        return V2B_OK;
+    });
+}
+
 void v2b_problem_destroy(v2b_problem *p) { delete p; }
 long v2b_problem_n_primal(const v2b_problem *p) { return p ? p->prob.n_primal : -1; }
 long v2b_problem_n_dual(const v2b_problem *p) { return p ? p->prob.n_dual : -1; }
@@ -1744,6 +1771,7 @@ int v2b_problem_rdm_records(const v2b_problem *p, const double *x, v2b_tpdm_reco
 int v2b_problem_pack_dims(const v2b_problem *p, long *d2_size, long *d1_size) {
     return guarded([&] {
         if (!p || !d2_size || !d1_size) throw std::invalid_argument("pack_dims: NULL argument");
+        if (p->prob.spec.batch_parts) throw std::invalid_argument("pack_dims: pack each part of a batch");
         const long g00 = (long)p->prob.n * (p->prob.n + 1) / 2;
         *d2_size = g00 * (g00 + 1) / 2;
         *d1_size = g00;
@@ -1754,6 +1782,7 @@ int v2b_problem_pack_spatial_density(v2b_problem *p, const double *d_x, double *
                                      void *stream) {
     return guarded([&] {
         if (!p || !d_x || !d_d2 || !d_d1) throw std::invalid_argument("pack_spatial_density: NULL argument");
+        if (p->prob.spec.batch_parts) throw std::invalid_argument("pack_spatial_density: pack each part of a batch");
         p->setup();
         const v2b::Problem &q = p->prob;
         if (!p->ibas_aa_dev) {

@@ -244,6 +244,7 @@ Problem make_problem(const ProblemSpec &spec) {
 
 // ------------------------------------------------------------------ b, c, x
 void build_b(const Problem &p, double *b) {
+    if (p.spec.batch_parts) throw std::invalid_argument("a batch's b is its parts' b, concatenated");
     if (p.spec.doci) return doci_build_b(p, b);
     const int n = p.n, gab = p.gab, gaa = p.gaa;
     const double na = p.spec.nalpha, nb = p.spec.nbeta;
@@ -306,6 +307,7 @@ void fill_d1(const Problem &p, const double *hsym, double *c) {
 }  // namespace
 
 void build_c_hubbard(const Problem &p, double t, double U, double *c) {
+    if (p.spec.batch_parts) throw std::invalid_argument("a batch's c is its parts' c, concatenated");
     if (p.spec.doci) throw std::invalid_argument("v2RDM-DOCI has no Hubbard Hamiltonian: pass h and g");
     const int n = p.n, gab = p.gab;
     std::memset(c, 0, sizeof(double) * p.n_primal);
@@ -323,6 +325,7 @@ void build_c_hubbard(const Problem &p, double t, double U, double *c) {
 }
 
 void build_c_external(const Problem &p, const double *h, const double *g, double *c) {
+    if (p.spec.batch_parts) throw std::invalid_argument("a batch's c is its parts' c, concatenated");
     if (p.spec.doci) return doci_build_c_external(p, h, g, c);
     const int64_t n = p.n;
     const int gab = p.gab, gaa = p.gaa;
@@ -867,12 +870,14 @@ void t2_rows(const Problem &p, int64_t off, F &&f, bool f3 = false) {
 }  // namespace
 
 void guess_random(const Problem &p, double *x) {
+    if (p.spec.batch_parts) throw std::invalid_argument("a batch's guess is its parts' guesses, concatenated");
     // v2rdm_solver.cc:1799-1806 (C library rand() seeded with 0)
     srand(0);
     for (int64_t i = 0; i < p.n_primal; i++) x[i] = ((double)rand() / RAND_MAX - 1.0) * 2.0;
 }
 
 void guess_hf(const Problem &p, double *x) {
+    if (p.spec.batch_parts) throw std::invalid_argument("a batch's guess is its parts' guesses, concatenated");
     if (p.spec.doci)
         throw std::invalid_argument("v2RDM-DOCI starts from the random guess (v2rdm_doci_solver.cc:1325-1336)");
     // v2rdm_solver.cc:1713-1823; the reference stores doccpi = nalpha for

@@ -32,6 +32,7 @@ struct ProblemSpec {
     bool constrain_f3 = false;          // CONSTRAIN_F3, implies D3 (:4128-4131)
     bool constrain_d4 = false;          // CONSTRAIN_D4, implies D3 (:4144-4149)
     bool doci = false;                  // the v2RDM-DOCI program (src/v2rdm_doci)
+    int batch_parts = 0;                // > 0: independent problems along the diagonal
 };
 
 // offsets of the v2RDM-DOCI primal blocks (v2rdm_doci_solver.cc:542-600)
@@ -104,5 +105,14 @@ void guess_hf(const Problem &p, double *x);   // v2RDM only (DOCI's guess is the
 
 PackedOperator build_A(const Problem &p);    // rows = dual constraints
 PackedOperator build_AT(const Problem &p);   // rows = primal variables
+
+// Independent problems as one: x, b, c, y concatenated in order, the PSD
+// blocks concatenated, A block diagonal (each part's packed rows with its
+// columns shifted and its coefficient codes mapped into one palette).
+// Throws std::invalid_argument when the parts' coefficients do not fit one
+// 16-entry palette or the columns 27 bits.
+void make_batch(const std::vector<const Problem *> &parts, const std::vector<const PackedOperator *> &A,
+                const std::vector<const PackedOperator *> &AT, Problem &out, PackedOperator &outA,
+                PackedOperator &outAT);
 
 }  // namespace v2b

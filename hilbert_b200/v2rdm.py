@@ -123,6 +123,15 @@ class V2RDMProblem:
             self._lib.v2b_problem_destroy(self._h)
             self._h = None
 
+    def palette(self, transposed=False):
+        """The distinct coefficients of A (or A^T), as bit patterns: parts
+        whose palettes together hold at most 16 can share one BatchProblem."""
+        count = ctypes.c_int()
+        check(self._lib.v2b_problem_palette(self._h, int(transposed), None, ctypes.byref(count)))
+        out = np.zeros(count.value)
+        check(self._lib.v2b_problem_palette(self._h, int(transposed), out.ctypes.data, ctypes.byref(count)))
+        return set(out.view(np.uint64).tolist())
+
     def __del__(self):
         try:
             self.close()
@@ -425,6 +434,30 @@ class DOCIProblem(V2RDMProblem):
         gab, gaa = n * n, n * (n - 1) // 2
         cuts = np.cumsum([gab * gab, gaa * gaa, gaa * gaa, n * n])
         return dict(zip(("d2ab", "d2aa", "d2bb", "d1a", "d1b"), np.split(out, cuts)))
+
+
+class BatchProblem(V2RDMProblem):
+    """Independent problems (V2RDMProblem / DOCIProblem parts) solved as one
+    block-diagonal problem, every device launch covering all of them.  x, b,
+    c and y are the parts' vectors concatenated in order (``split`` cuts a
+    vector back into parts).  The parts may be closed afterwards."""
+
+    def __init__(self, parts):
+        lib = _capi.load()
+        self._lib = lib
+        parts = list(parts)
+        handles = (ctypes.c_void_p * len(parts))(*[p._h.value if hasattr(p._h, "value") else p._h
+                                                   for p in parts])
+        h = ctypes.c_void_p()
+        check(lib.v2b_batch_problem_create(handles, len(parts), ctypes.byref(h)))
+        self._sizes(h, None, None, None)
+        self.primal_cuts = np.cumsum([p.n_primal for p in parts])[:-1]
+        self.dual_cuts = np.cumsum([p.n_dual for p in parts])[:-1]
+
+    def split(self, v, dual=False):
+        """The parts' pieces of a batch vector (host array or tensor)."""
+        v = v.detach().cpu().numpy() if hasattr(v, "detach") else np.asarray(v)
+        return np.split(v, self.dual_cuts if dual else self.primal_cuts)
 
 
 class BPSDPSolver:

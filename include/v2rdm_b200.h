@@ -134,6 +134,22 @@ int v2b_doci_problem_create(int nmo, int nalpha, int nbeta, int positivity, v2b_
  * v2b_problem_create numbers them.  *size receives the length; out may be
  * NULL to ask for it. */
 int v2b_doci_v2rdm_layout(const v2b_problem *p, const double *x, double *out, long *size);
+/* Independent problems (count >= 1, each from v2b_problem_create or
+ * v2b_doci_problem_create) as one problem whose every device launch covers
+ * them all: x, b, c and y are the parts' vectors concatenated in order, the
+ * PSD blocks the parts' blocks in order, and A is block diagonal.  The joint
+ * boundary-point SDP separates into the parts, so a solve converges to the
+ * parts' own optima side by side (the penalty mu, the CG scalars and the
+ * convergence test are shared).  No counterpart in the reference, which
+ * solves one problem per call.  V2B_BAD_ARG when the parts' coefficients do
+ * not fit one 16-entry palette.  The parts may be destroyed afterwards.
+ * build_b, build_c_*, guess, the density packing and the RDM records are
+ * the parts' own: they return V2B_BAD_ARG on a batch. */
+int v2b_batch_problem_create(const v2b_problem *const *parts, int count, v2b_problem **out);
+/* The distinct coefficients of A (transposed = 0) or A^T (1), at most 16:
+ * *count receives how many; out (may be NULL) the values.  Parts whose
+ * palettes together hold at most 16 values can share one batch. */
+int v2b_problem_palette(const v2b_problem *p, int transposed, double *out, int *count);
 void v2b_problem_destroy(v2b_problem *p);
 long v2b_problem_n_primal(const v2b_problem *p);
 long v2b_problem_n_dual(const v2b_problem *p);
