@@ -11,6 +11,15 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+    config.addinivalue_line("markers", "first_device_run: a device path not yet run on a GPU")
+
+
+def pytest_collection_modifyitems(config, items):
+    """Tests of device paths that have not run on a GPU yet go after the
+    others (stable order otherwise), so that under -x a failure there cannot
+    stop them; test_zz_no_alloc stays last."""
+    items.sort(key=lambda item: (item.module.__name__.startswith("test_zz"),
+                                 item.get_closest_marker("first_device_run") is not None))
 
 
 @pytest.fixture(scope="session")

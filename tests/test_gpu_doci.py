@@ -8,7 +8,7 @@ import hilbert_b200 as hb
 from oracle.doci import DociOracle, seniority_zero_ci, symmetric_integrals
 from test_doci import assert_Au_matches, df_integrals, golden_cases, oracle_solve, pair_hamiltonian
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.first_device_run]
 
 E_TOL = 1e-6
 
