@@ -328,7 +328,8 @@ class V2RDMProblem:
     def rdm_records(self, x):
         """{file: records} as WriteTPDM, WriteTPDMSpinFree and WriteOPDM emit
         them (write_tpdm.cc:40-519, write_opdm.cc:40-114) for the host or
-        device primal vector x: D2aa, D2bb, D2ab, the spin-free D2, D1a, D1b."""
+        device primal vector x: D2aa, D2bb, D2ab, the spin-free D2, D1a, D1b
+        (for DOCI, what its WriteTPDM writes: D2aa, D2bb, D2ab)."""
         xh = np.ascontiguousarray(x.detach().cpu().numpy() if hasattr(x, "detach") else x,
                                   dtype=np.float64)
         if xh.shape != (self.n_primal,):
@@ -336,9 +337,10 @@ class V2RDMProblem:
         counts = np.zeros(6, np.int64)
         check(self._lib.v2b_problem_rdm_counts(self._h, counts.ctypes.data))
         out = {name: np.zeros(int(cnt), self.TPDM_RECORD if name.startswith("D2") else self.OPDM_RECORD)
-               for name, cnt in zip(self.RDM_FILES, counts)}
-        check(self._lib.v2b_problem_rdm_records(self._h, xh.ctypes.data,
-                                                *[out[name].ctypes.data for name in self.RDM_FILES]))
+               for name, cnt in zip(self.RDM_FILES, counts) if cnt >= 0}   # -1: not written
+        check(self._lib.v2b_problem_rdm_records(
+            self._h, xh.ctypes.data, *[out[name].ctypes.data if name in out else None
+                                       for name in self.RDM_FILES]))
         return out
 
     def rdm_entries(self, x):

@@ -122,8 +122,8 @@ int v2b_problem_create(int nmo, int nalpha, int nbeta, int positivity, int const
  * same v2b_problem_* calls: b (BuildConstraints, :1338-1507), c from h and
  * (ij|kl) (RepackIntegrals, tei.cc:127-153), the random guess (:1325-1336),
  * A.x and A^T.y (bpsdp_Au / bpsdp_ATu, :1509-1566) and the solves.
- * positivity = V2B_POSITIVITY_* | V2B_CONSTRAIN_D3.  DOCI has no Hubbard c,
- * no HF guess and no v2RDM RDM records: those calls return V2B_BAD_ARG.
+ * positivity = V2B_POSITIVITY_* | V2B_CONSTRAIN_D3.  DOCI has no Hubbard c
+ * and no HF guess: those calls return V2B_BAD_ARG.
  * v2b_problem_pack_spatial_density packs a DOCI solution as hilbert's DOCI
  * PackSpatialDensity does (v2rdm_doci_solver.cc:1568-1703). */
 int v2b_doci_problem_create(int nmo, int nalpha, int nbeta, int positivity, v2b_problem **out);
@@ -269,8 +269,10 @@ int v2b_problem_pack_spatial_density(v2b_problem *p, const double *d_x, double *
  * files D1a, D1b), for the C1 active space (orbital numbers are active
  * indices; no core records).  The record layouts are the reference's struct
  * tpdm and struct opdm (v2rdm_solver.h:53-65).  counts[6] receives the
- * record counts in the order D2aa, D2bb, D2ab, D2, D1a, D1b; any output
- * array may be NULL.  v2RDM problems only. */
+ * record counts in the order D2aa, D2bb, D2ab, D2, D1a, D1b, -1 for a file
+ * the problem's writers do not write: a DOCI problem gives what v2RDM-DOCI's
+ * WriteTPDM writes (src/v2rdm_doci/write_tpdm.cc:47-176: D2aa, D2bb, D2ab
+ * only).  Any output array may be NULL. */
 typedef struct {
     int i, j, k, l;
     double value;

@@ -104,7 +104,7 @@ grep -q "dimensions_.push_back" "$dgen" || { echo "build_ref.sh: could not extra
 DFLAGS=(-std=c++17 -O2 -fPIC -ffp-contract=off -w
         -I"$here/ref_shim" -I"$dsrc" -I"$ref/src")
 dobjs=()
-for u in basis d2 q2 g2 d3 t1 t2 tei; do
+for u in basis d2 q2 g2 d3 t1 t2 tei write_tpdm; do
   "$CXX" "${DFLAGS[@]}" -c "$dsrc/$u.cc" -o "$out/doci_$u.o"
   dobjs+=("$out/doci_$u.o")
 done

@@ -177,6 +177,31 @@ def _ref_pack(self, x):
 DociRef.pack_spatial_density = _ref_pack
 
 
+def _ref_write_tpdm(self, x):
+    """Runs the reference DOCI WriteTPDM on x; {file: {entry: bytes}} for the
+    D2aa (unit 270), D2ab (271) and D2bb (272) files it writes."""
+    lib = self._lib
+    lib.doci_ref_write_tpdm.argtypes = [ctypes.c_void_p, _dp]
+    lib.doci_ref_psio_entry.restype = ctypes.c_long
+    lib.doci_ref_psio_entry.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p]
+    lib.doci_ref_write_tpdm(self._h, np.ascontiguousarray(x, np.float64))
+    out = {}
+    for name, unit in (("D2aa", 270), ("D2ab", 271), ("D2bb", 272)):
+        out[name] = {}
+        for key in (name, "length", "NUMBER ACTIVE ORBITALS", "ACTIVE ORBITALS",
+                    "NUMBER INACTIVE ORBITALS", "INACTIVE ORBITALS"):
+            size = lib.doci_ref_psio_entry(unit, key.encode(), None)
+            if size < 0:
+                continue
+            buf = ctypes.create_string_buffer(max(size, 1))
+            lib.doci_ref_psio_entry(unit, key.encode(), buf)
+            out[name][key] = buf.raw[:size]
+    return out
+
+
+DociRef.write_tpdm = _ref_write_tpdm
+
+
 def symmetric_integrals(rng, n):
     """Random real h and (ij|kl) with the 8-fold symmetry of real orbitals."""
     h = rng.standard_normal((n, n))

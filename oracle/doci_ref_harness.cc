@@ -13,7 +13,7 @@
  * Everything else runs the reference's own compiled functions: the sizing,
  * offsets and block list (the POSITIVITY part of common_init, extracted by
  * build_ref.sh), BuildBasis, BuildConstraints, Guess, RepackIntegrals (c),
- * bpsdp_Au and bpsdp_ATu.
+ * bpsdp_Au, bpsdp_ATu, PackSpatialDensity and WriteTPDM.
  */
 #include <cstring>
 #include <string>
@@ -109,17 +109,27 @@ class RefDoci : private OptionHolder, public v2RDM_DOCISolver {
 
     /* PackSpatialDensity (v2rdm_doci_solver.cc:1568-1703) on a given x, with
        the buffers GetIntegrals would allocate (tei.cc:74-94) */
-    void pack(const double *xin, double *d2, double *d1) {
-        std::memcpy(x->pointer(), xin, sizeof(double) * dimx_);
+    void alloc_packing() {
         d2_act_spatial_dim_ = gems_00[0] * (gems_00[0] + 1) / 2;
         d1_act_spatial_dim_ = amo_ * (amo_ + 1) / 2;
         free(d2_act_spatial_sym_);
         free(d1_act_spatial_sym_);
         d2_act_spatial_sym_ = (double *)calloc(d2_act_spatial_dim_, sizeof(double));
         d1_act_spatial_sym_ = (double *)calloc(d1_act_spatial_dim_, sizeof(double));
+    }
+    void pack(const double *xin, double *d2, double *d1) {
+        std::memcpy(x->pointer(), xin, sizeof(double) * dimx_);
+        alloc_packing();
         PackSpatialDensity();
         std::memcpy(d2, d2_act_spatial_sym_, sizeof(double) * d2_act_spatial_dim_);
         std::memcpy(d1, d1_act_spatial_sym_, sizeof(double) * d1_act_spatial_dim_);
+    }
+    /* WriteTPDM (src/v2rdm_doci/write_tpdm.cc:47-176) on a given x, into the
+       in-memory PSIO stand-in */
+    void write_tpdm(const double *xin) {
+        std::memcpy(x->pointer(), xin, sizeof(double) * dimx_);
+        alloc_packing();
+        WriteTPDM();
     }
     long d2_dim() const { return (long)gems_00[0] * (gems_00[0] + 1) / 2; }
     long d1_dim() const { return (long)amo_ * (amo_ + 1) / 2; }
@@ -208,6 +218,14 @@ long doci_ref_pack_dims(void *p, long *d1n) {
     return ((RefDoci *)p)->d2_dim();
 }
 void doci_ref_pack_spatial(void *p, const double *x, double *d2, double *d1) { ((RefDoci *)p)->pack(x, d2, d1); }
+void doci_ref_write_tpdm(void *p, const double *x) { ((RefDoci *)p)->write_tpdm(x); }
+/* size of one written PSIO entry, -1 if absent; copy it into out (may be NULL) */
+long doci_ref_psio_entry(int unit, const char *key, char *out) {
+    auto it = psi::psio_store().find({unit, key});
+    if (it == psi::psio_store().end()) return -1;
+    if (out) std::memcpy(out, it->second.data(), it->second.size());
+    return (long)it->second.size();
+}
 void doci_ref_ATu(void *p, const double *y, double *out) {
     RefDoci *r = (RefDoci *)p;
     std::vector<double> u(y, y + r->n_dual());

@@ -152,8 +152,6 @@ def test_doci_refusals():
         p.guess("HF")
     with pytest.raises(_capi.V2BError):
         p.c_hubbard(1.0, 4.0)
-    with pytest.raises(_capi.V2BError):
-        p.rdm_records(np.zeros(p.n_primal))
     p.close()
 
 
@@ -263,3 +261,23 @@ def test_doci_orbital_optimisation_with_the_focas_step():
                                  solve_active=solve_active, macro_iterations=2)
     assert E[1] < E[0] - 1.0
     assert gn[1] < 0.1 * gn[0]
+
+
+@needs_ref
+def test_doci_rdm_entries_match_the_reference_writer():
+    """What v2RDM-DOCI's WriteTPDM writes (D2aa, D2bb, D2ab and their
+    metadata), byte for byte; DOCI writes no spin-free D2 and no 1-RDM files."""
+    rng = np.random.default_rng(29)
+    for n, pos in itertools.product([1, 2, 3, 4, 5], ["D", "DQG+D3"]):
+        if n < 2 and pos.endswith("D3"):
+            continue
+        na = max(1, n // 2)
+        r = DociRef(n, na, na, pos)
+        x = rng.standard_normal(r.n_primal)
+        want = r.write_tpdm(x)
+        p = product(n, na, na, pos)
+        got = p.rdm_entries(x)
+        assert set(got) == {"D2aa", "D2bb", "D2ab"}
+        for name, entries in want.items():
+            assert got[name] == entries, (n, pos, name)
+        p.close()
