@@ -604,6 +604,72 @@ class v2RDMHelper:
         return d1a + d1b
 
 
+class v2RDM_DOCIHelper:
+    """hilbert.v2RDM_DOCIHelper (src/python_api/python_helpers.cc:99-101, 339-352).
+
+    hilbert builds it from a Psi4 wavefunction; here
+    ``v2RDM_DOCIHelper(nalpha, nbeta, nmo, h, g, options)`` takes what the
+    solver reads from one: the electron counts and the integrals h and
+    g = (ij|kl) of the nmo orbitals.  POSITIVITY and CONSTRAIN_D3 choose the
+    conditions (v2rdm_doci_solver.cc:427-494).  With OPTIMIZE_ORBITALS and the
+    density-fitting factors ``B`` (naux x nmo x nmo, g = sum_Q B^Q B^Q) the
+    orbitals are optimised as well (orbital.doci_casscf); otherwise they stay
+    fixed."""
+
+    def __init__(self, nalpha, nbeta, nmo, h, g, options, B=None):
+        self.options = options if isinstance(options, Options) else Options(options)
+        o = self.options
+        pos = o.get("POSITIVITY") + ("+D3" if o.get("CONSTRAIN_D3") else "")
+        self.problem = DOCIProblem(nmo, nalpha, nbeta, pos)
+        self.h = np.ascontiguousarray(h, dtype=np.float64).reshape(nmo, nmo)
+        self.B = None if B is None else np.ascontiguousarray(B, dtype=np.float64)
+        if g is None:
+            if self.B is None:
+                raise ValueError("give g = (ij|kl) or the density-fitting factors B")
+            g = np.einsum("Qij,Qkl->ijkl", self.B, self.B)
+        self.c = self.problem.c_external(self.h, np.ascontiguousarray(g, dtype=np.float64))
+        self.b = self.problem.b()
+        self.x = None
+        self.stats = None
+        self.variables = {}
+
+    def _sdp_options(self):
+        # DOCI calls solve(ORBOPT_FREQUENCY) until converged, updating mu
+        # after each call (v2rdm_doci_solver.cc:1113-1137)
+        o = Options({k: v for k, v in self.options._v.items()})
+        o.set("MU_UPDATE_FREQUENCY", int(self.options.get("ORBOPT_FREQUENCY")))
+        return o
+
+    def compute_energy(self, monitor=None, macro_iterations=8):
+        """The DOCI energy; with orbital optimisation, after macro_iterations
+        SDP solves and orbital steps."""
+        p = self.problem
+        if self.options.get("OPTIMIZE_ORBITALS") and self.B is not None:
+            import torch
+            from . import orbital
+            dev = torch.device("cuda", torch.cuda.current_device())
+            solve = orbital.doci_solve_active(p.nmo, p.nalpha, p.nbeta,
+                                              self.options.get("POSITIVITY")
+                                              + ("+D3" if self.options.get("CONSTRAIN_D3") else ""),
+                                              self._sdp_options())
+            energies, gnorms, _, _ = orbital.doci_casscf(
+                torch.from_numpy(self.h).to(dev), torch.from_numpy(self.B).to(dev), p.nalpha, p.nbeta,
+                solve_active=solve, macro_iterations=macro_iterations)
+            solve.problem.close()
+            self.stats = {"energies": energies, "orbital_gradients": gnorms}
+            e = energies[-1]
+        else:
+            self.x, self.stats = p.solve(p.guess("RANDOM"), self.b, self.c, self._sdp_options(), monitor)
+            e = float(self.c @ self.x)
+            n = p.nmo
+            # natural-orbital occupations 2 D1(i) (v2rdm_doci_solver.cc:1148-1153)
+            self.occupations = 2.0 * self.x[2 * n * n:2 * n * n + n]
+        # enuc = efzc = 0 for given integrals (v2rdm_doci_solver.cc:1157-1158)
+        self.variables["CURRENT ENERGY"] = e
+        self.variables["v2RDM-DOCI TOTAL ENERGY"] = e
+        return e
+
+
 def block_layout(nmo, nalpha, nbeta, positivity="DQG", constrain_spin=True):
     """[(name, dim)] in the primal order of set_primal_offsets (v2rdm_solver.cc:3729-4079)."""
     n = int(nmo)

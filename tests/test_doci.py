@@ -281,3 +281,26 @@ def test_doci_rdm_entries_match_the_reference_writer():
         for name, entries in want.items():
             assert got[name] == entries, (n, pos, name)
         p.close()
+
+
+def test_doci_helper_builds_the_problem_its_options_name():
+    """v2RDM_DOCIHelper: POSITIVITY / CONSTRAIN_D3 pick the conditions, c from
+    h and (ij|kl) or from the DF factors, ORBOPT_FREQUENCY sets the mu period;
+    without a GPU compute_energy fails loudly."""
+    rng = np.random.default_rng(8)
+    n = 4
+    h, g = symmetric_integrals(rng, n)
+    helper = hb.v2RDM_DOCIHelper(2, 2, n, h, g, {"POSITIVITY": "DQG", "CONSTRAIN_D3": True,
+                                                 "ORBOPT_FREQUENCY": 250})
+    o = DociOracle(n, 2, 2, "DQG+D3")
+    assert helper.problem.n_primal == o.n_primal
+    assert np.array_equal(helper.b, o.b()) and np.array_equal(helper.c, o.c(h, g))
+    assert helper._sdp_options().get("MU_UPDATE_FREQUENCY") == 250
+    B = 0.3 * rng.standard_normal((6, n, n))
+    B = B + B.transpose(0, 2, 1)
+    from_b = hb.v2RDM_DOCIHelper(2, 2, n, h, None, {"POSITIVITY": "DQ"}, B=B)
+    assert np.allclose(from_b.c, DociOracle(n, 2, 2, "DQ").c(h, np.einsum("Qij,Qkl->ijkl", B, B)))
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        with pytest.raises(_capi.V2BError):
+            helper.compute_energy()

@@ -77,3 +77,22 @@ def test_doci_casscf_on_the_device(cuda_device):
     assert all(b <= a + 1e-6 for a, b in zip(E, E[1:]))
     assert abs(E[0] - (-28.3102401)) <= 1e-5 and abs(E[2] - (-33.5748761)) <= 1e-4
     assert gn[2] < 0.01 * gn[0]
+
+
+def test_doci_helper_energy(cuda_device):
+    """v2RDM_DOCIHelper with fixed orbitals gives the oracle's DOCI energy;
+    with the DF factors and OPTIMIZE_ORBITALS the energy falls below it."""
+    import hilbert_b200.orbital as ho
+    n, npair = 4, 2
+    h_mo, B_mo, *_ = ho.casscf_df_problem(nbf=n, naux=10, ncore=0, nact=n)
+    g = np.einsum("Qij,Qkl->ijkl", B_mo, B_mo)
+    opts = {"POSITIVITY": "DQG", "OPTIMIZE_ORBITALS": False, "R_CONVERGENCE": 1e-7,
+            "E_CONVERGENCE": 1e-7, "MAXITER": 200000}
+    helper = hb.v2RDM_DOCIHelper(npair, npair, n, h_mo, g, opts)
+    e = helper.compute_energy()
+    eo, so = oracle_solve(DociOracle(n, npair, npair, "DQG"), h_mo, g)
+    assert so.is_converged() and abs(e - eo) <= E_TOL
+    assert helper.variables["v2RDM-DOCI TOTAL ENERGY"] == e
+    assert abs(helper.occupations.sum() - 2 * npair) <= 1e-5
+    opt = hb.v2RDM_DOCIHelper(npair, npair, n, h_mo, None, dict(opts, OPTIMIZE_ORBITALS=True), B=B_mo)
+    assert opt.compute_energy(macro_iterations=3) < e - 1.0
