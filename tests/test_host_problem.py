@@ -202,3 +202,27 @@ def test_helper_options_select_the_constraint_families():
     assert list(helper.problem.dims) == want
     names = [b for b, _ in hb.block_layout(n, 2, 2, "DQGT1+Q3+D4", True)]
     assert {"t1aaa", "q3aab", "d3bbb", "d4aabb"} <= set(names) and "e3aaa" not in names
+
+
+def test_new_entry_points_refuse_bad_arguments():
+    """NULL handles, wrong problem kinds and bad values give V2B_BAD_ARG."""
+    lib = _capi.load()
+    bad = _capi.V2B_BAD_ARG
+    out = ctypes.c_void_p()
+    counts = np.zeros(6, np.int64)
+    size = ctypes.c_long()
+    n = ctypes.c_int()
+    assert lib.v2b_batch_problem_create(None, 1, ctypes.byref(out)) == bad
+    assert lib.v2b_batch_problem_create((ctypes.c_void_p * 1)(None), 1, ctypes.byref(out)) == bad
+    assert lib.v2b_problem_rdm_counts(None, counts.ctypes.data) == bad
+    assert lib.v2b_problem_palette(None, 0, None, ctypes.byref(n)) == bad
+    assert lib.v2b_doci_v2rdm_layout(None, None, None, ctypes.byref(size)) == bad
+    p = hb.V2RDMProblem(3, 1, 1, "DQG")
+    assert lib.v2b_doci_v2rdm_layout(p._h, None, None, ctypes.byref(size)) == bad   # not DOCI
+    y, z = np.zeros(p.n_dual), np.zeros(p.n_primal)
+    dp = ctypes.POINTER(ctypes.c_double)
+    for mu in (0.0, -1.0, float("nan"), float("inf")):
+        assert lib.v2b_problem_set_state(p._h, mu, y.ctypes.data_as(dp), z.ctypes.data_as(dp)) == bad
+    assert lib.v2b_problem_set_state(p._h, 0.5, None, z.ctypes.data_as(dp)) == bad
+    assert lib.v2b_problem_rdm_records(p._h, None, None, None, None, None, None, None) == bad
+    p.close()
