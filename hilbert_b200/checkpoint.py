@@ -4,7 +4,9 @@ The file holds the entries hilbert's WriteCheckpointFile writes
 (src/v2rdm_casscf/checkpoint.cc:48-88), with the same names and contents:
 "MU" (the penalty after the last solve), "PRIMAL" (x), "DUAL 1" (y),
 "DUAL 2" (z) and, for an orbital-optimised run, "MO TO MO' TRANSFORMATION
-MATRIX" and "SO TO MO TRANSFORMATION MATRIX".  The container is one .npz
+MATRIX" and "SO TO MO TRANSFORMATION MATRIX".  v2RDM-DOCI writes the same
+entries (src/v2rdm_doci/checkpoint.cc:48-86), so a DOCIProblem restarts the
+same way.  The container is one .npz
 archive (the reference's is a Psi4 PSIO file).  A restart is
 ReadFromCheckpointFile (checkpoint.cc:90-124): mu, y and z seed the next
 solve, and x is its starting point.

@@ -36,3 +36,13 @@ def test_restart_checks_sizes_and_mu(tmp_path):
     with pytest.raises(hb.V2BError):
         p.set_state(0.0, np.zeros(p.n_dual), np.zeros(p.n_primal))
     p.close()
+
+
+def test_doci_restart_uses_the_same_entries(tmp_path):
+    p = hb.DOCIProblem(4, 2, 2, "DQG")
+    path = os.path.join(tmp_path, "doci.ck.npz")
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(p.n_primal)
+    ck.save_checkpoint(path, 2.5, x, rng.standard_normal(p.n_dual), rng.standard_normal(p.n_primal))
+    assert np.array_equal(ck.restart(p, path), x) and p.get_mu() == 2.5
+    p.close()
