@@ -226,3 +226,29 @@ def test_new_entry_points_refuse_bad_arguments():
     assert lib.v2b_problem_set_state(p._h, 0.5, None, z.ctypes.data_as(dp)) == bad
     assert lib.v2b_problem_rdm_records(p._h, None, None, None, None, None, None, None) == bad
     p.close()
+
+
+@pytest.mark.parametrize("kind,n,pos", [("doci", 20, "DQGT1T2+D3"), ("v2rdm", 8, "DQGT1T2+D3+Q3+E3+F3+D4"),
+                                        ("v2rdm", 20, "DQG")])
+def test_packed_A_and_AT_are_exact_transposes(kind, n, pos):
+    """At sizes beyond the reference grid: the (row, column, coefficient)
+    triples of A^T, duplicates summed, are exactly those of A transposed
+    (both emitters visit the same terms)."""
+    import scipy.sparse as sp
+
+    def csr(rp, ent, pal, shape):
+        rows = np.repeat(np.arange(len(rp) - 1), np.diff(rp))
+        m = sp.coo_matrix((pal[(ent >> 27) & 15], (rows, (ent & ((1 << 27) - 1)).astype(np.int64))),
+                          shape=shape).tocsr()
+        m.sum_duplicates()
+        m.eliminate_zeros()
+        return m
+
+    p = (hb.DOCIProblem(n, n // 2, n // 2, pos) if kind == "doci"
+         else hb.V2RDMProblem(n, n // 2, n // 2, pos))
+    A = csr(*operator(p, False), (p.n_dual, p.n_primal))
+    AT = csr(*operator(p, True), (p.n_primal, p.n_dual))
+    diff = A.T.tocsr() - AT
+    diff.eliminate_zeros()
+    assert diff.nnz == 0
+    p.close()
