@@ -94,4 +94,29 @@ void rdm_records(const Problem &p, const double *x, TpdmRecord *d2aa, TpdmRecord
     records(p, x, Blocks{p.d2ab, p.d2aa, p.d2bb, p.d1a, p.d1b}, d2aa, d2bb, d2ab, d2, d1a, d1b);
 }
 
+void iwl_records(const Problem &p, const double *x, TpdmRecord *aa, TpdmRecord *ab, TpdmRecord *bb) {
+    // WriteTPDM_IWL (src/v2rdm_casscf/write_tpdm_iwl.cc:45-205): the calls it
+    // makes to IWL::write_value, labels in (i, k, j, l) order for the element
+    // D2(ij, kl); aa and bb scaled by 1/4; no core orbitals, so no core calls
+    check(p);
+    if (p.spec.doci) throw std::invalid_argument("the IWL 2-RDM of v2RDM problems");
+    const int gab = p.gab, gaa = p.gaa;
+    int64_t caa = 0, cab = 0;
+    for (int ij = 0; ij < gab; ij++) {
+        const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
+        for (int kl = 0; kl < gab; kl++) {
+            const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
+            if (ab) ab[cab] = TpdmRecord{i, k, j, l, x[p.d2ab + (int64_t)ij * gab + kl]};
+            cab++;
+            if (i != j && k != l) {
+                const int64_t e = (int64_t)p.iaa(i, j) * gaa + p.iaa(k, l);
+                const double s = 0.25 * (double)((i < j ? 1 : -1) * (k < l ? 1 : -1));
+                if (aa) aa[caa] = TpdmRecord{i, k, j, l, s * x[p.d2aa + e]};
+                if (bb) bb[caa] = TpdmRecord{i, k, j, l, s * x[p.d2bb + e]};
+                caa++;
+            }
+        }
+    }
+}
+
 }  // namespace v2b

@@ -24,4 +24,8 @@ RdmCounts rdm_counts(const Problem &p);
 void rdm_records(const Problem &p, const double *x, TpdmRecord *d2aa, TpdmRecord *d2bb,
                  TpdmRecord *d2ab, TpdmRecord *d2, OpdmRecord *d1a, OpdmRecord *d1b);
 
+// the IWL::write_value calls of WriteTPDM_IWL (v2RDM problems), as records
+// (i, j, k, l) = its labels; counts are rdm_counts' d2aa (aa, bb) and d2ab
+void iwl_records(const Problem &p, const double *x, TpdmRecord *aa, TpdmRecord *ab, TpdmRecord *bb);
+
 }  // namespace v2b

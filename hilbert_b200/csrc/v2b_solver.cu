@@ -1768,6 +1768,15 @@ int v2b_problem_rdm_records(const v2b_problem *p, const double *x, v2b_tpdm_reco
         return V2B_OK;
     });
 }
+int v2b_problem_tpdm_iwl_records(const v2b_problem *p, const double *x, v2b_tpdm_record *d2aa,
+                                 v2b_tpdm_record *d2ab, v2b_tpdm_record *d2bb) {
+    return guarded([&] {
+        if (!p || !x) throw std::invalid_argument("tpdm_iwl_records: NULL argument");
+        v2b::iwl_records(p->prob, x, (v2b::TpdmRecord *)d2aa, (v2b::TpdmRecord *)d2ab,
+                         (v2b::TpdmRecord *)d2bb);
+        return V2B_OK;
+    });
+}
 int v2b_problem_pack_dims(const v2b_problem *p, long *d2_size, long *d1_size) {
     return guarded([&] {
         if (!p || !d2_size || !d1_size) throw std::invalid_argument("pack_dims: NULL argument");

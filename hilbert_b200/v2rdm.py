@@ -343,6 +343,23 @@ class V2RDMProblem:
                                        for name in self.RDM_FILES]))
         return out
 
+    def tpdm_iwl_records(self, x):
+        """{"D2aa", "D2ab", "D2bb"}: the IWL::write_value calls of WriteTPDM_IWL
+        (write_tpdm_iwl.cc:45-205) as records, fields i, j, k, l holding the
+        labels (i, k, j, l) of D2(ij, kl)."""
+        xh = np.ascontiguousarray(x.detach().cpu().numpy() if hasattr(x, "detach") else x,
+                                  dtype=np.float64)
+        if xh.shape != (self.n_primal,):
+            raise ValueError(f"x must hold {self.n_primal} values")
+        counts = np.zeros(6, np.int64)
+        check(self._lib.v2b_problem_rdm_counts(self._h, counts.ctypes.data))
+        out = {"D2aa": np.zeros(int(counts[0]), self.TPDM_RECORD),
+               "D2ab": np.zeros(int(counts[2]), self.TPDM_RECORD),
+               "D2bb": np.zeros(int(counts[0]), self.TPDM_RECORD)}
+        check(self._lib.v2b_problem_tpdm_iwl_records(self._h, xh.ctypes.data, out["D2aa"].ctypes.data,
+                                                     out["D2ab"].ctypes.data, out["D2bb"].ctypes.data))
+        return out
+
     def rdm_entries(self, x):
         """{file: {entry: bytes}}: every entry hilbert's writers put in their
         PSIO files, byte for byte (the records when there are any, "length",

@@ -285,6 +285,14 @@ int v2b_problem_rdm_counts(const v2b_problem *p, long *counts);
 int v2b_problem_rdm_records(const v2b_problem *p, const double *x, v2b_tpdm_record *d2aa,
                             v2b_tpdm_record *d2bb, v2b_tpdm_record *d2ab, v2b_tpdm_record *d2,
                             v2b_opdm_record *d1a, v2b_opdm_record *d1b);
+/* The 2-RDM as WriteTPDM_IWL hands it to Psi4's IWL writer for gradients
+ * (src/v2rdm_casscf/write_tpdm_iwl.cc:45-205): one record per write_value
+ * call, in call order, labels (i, k, j, l) for the element D2(ij, kl), aa and
+ * bb values scaled by 1/4 (record counts: counts[0] and counts[2] of
+ * v2b_problem_rdm_counts).  The IWL files store only values above their
+ * cutoff, 1e-14; that filtering is the IWL writer's.  v2RDM problems only. */
+int v2b_problem_tpdm_iwl_records(const v2b_problem *p, const double *x, v2b_tpdm_record *d2aa,
+                                 v2b_tpdm_record *d2ab, v2b_tpdm_record *d2bb);
 
 /* ---- 3. allocation-free projection ------------------------------------------ */
 

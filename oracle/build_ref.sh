@@ -49,12 +49,13 @@ gen="$out/v2rdm_solver_extract.cc"
       Guess bpsdp_Au bpsdp_ATu PackSpatialDensity
   extract "$src/oei.cc" GetOEI_external GetOEI_hubbard
   extract "$src/write_tpdm.cc" WriteTPDM WriteTPDMSpinFree
+  extract "$src/write_tpdm_iwl.cc" WriteTPDM_IWL
   echo '}'
 } > "$gen"
 
 for name in SymmetryPair TotalSym set_constraints determine_n_primal determine_n_dual \
             set_primal_offsets BuildConstraints Guess bpsdp_Au bpsdp_ATu PackSpatialDensity \
-            GetOEI_external GetOEI_hubbard WriteTPDM WriteTPDMSpinFree; do
+            GetOEI_external GetOEI_hubbard WriteTPDM WriteTPDMSpinFree WriteTPDM_IWL; do
   grep -q "v2RDMSolver::${name}(" "$gen" || { echo "build_ref.sh: could not extract ${name}" >&2; exit 3; }
 done
 

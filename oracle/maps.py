@@ -281,6 +281,21 @@ class RefProblem:
             records[name] = np.frombuffer(raw, self.TPDM if name.startswith("D2") else self.OPDM).copy()
         return records, entries
 
+    def iwl_records(self):
+        """After write_rdms: the reference IWL writer's write_value calls per
+        file, {"D2aa", "D2ab", "D2bb"}: (labels (n, 4), values (n,)), and the
+        files' cutoff."""
+        lib = self._lib
+        lib.v2b_ref_iwl_records.restype = ctypes.c_long
+        lib.v2b_ref_iwl_records.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p]
+        out, cutoff = {}, ctypes.c_double()
+        for name, spin in (("D2aa", b"aa"), ("D2ab", b"ab"), ("D2bb", b"bb")):
+            count = lib.v2b_ref_iwl_records(spin, None, None)
+            buf = np.zeros((max(count, 0), 5))
+            lib.v2b_ref_iwl_records(spin, buf.ctypes.data, ctypes.byref(cutoff))
+            out[name] = (buf[:, :4].astype(np.int64), buf[:, 4].copy())
+        return out, cutoff.value
+
     def ATu(self, y):
         out = np.zeros(self.n_primal)
         if self._lib.v2b_ref_ATu(self._p, out, np.ascontiguousarray(y, np.float64)):

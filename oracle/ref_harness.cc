@@ -141,6 +141,7 @@ class RefProblem : public v2RDMSolver {
         WriteTPDM();
         WriteTPDMSpinFree();
         WriteOPDM();
+        WriteTPDM_IWL();   // write_tpdm_iwl.cc:45-205, into the IWL stand-in
     }
     long d2_dim() const { return d2_act_spatial_dim_; }
     long d1_dim() const { return d1_act_spatial_dim_; }
@@ -301,6 +302,22 @@ int v2b_ref_write_rdms(void *p, const double *x) {
         static_cast<RefProblem *>(p)->write_rdms(x);
         return 0;
     } catch (const std::exception &e) { g_last_error = e.what(); return 1; }
+}
+/* the write_value calls of the IWL writer on one file ("aa", "ab", "bb"):
+   their count, copied into out (5 doubles each: p, q, r, s, value) if not
+   NULL; *cutoff receives the file's cutoff */
+long v2b_ref_iwl_records(const char *spin, double *out, double *cutoff) {
+    const int unit = spin[1] == 'b' ? (spin[0] == 'a' ? PSIF_MO_AB_TPDM : PSIF_MO_BB_TPDM) : PSIF_MO_AA_TPDM;
+    auto it = psi::iwl_store().find(unit);
+    if (it == psi::iwl_store().end()) return -1;
+    if (cutoff) *cutoff = it->second.cutoff;
+    const auto &rec = it->second.records;
+    if (out)
+        for (size_t k = 0; k < rec.size(); k++) {
+            out[5 * k] = rec[k].p; out[5 * k + 1] = rec[k].q; out[5 * k + 2] = rec[k].r;
+            out[5 * k + 3] = rec[k].s; out[5 * k + 4] = rec[k].value;
+        }
+    return (long)rec.size();
 }
 /* size of one written PSIO entry, -1 if absent; copy it into out (may be NULL) */
 long v2b_ref_psio_entry(int unit, const char *key, char *out) {

@@ -216,6 +216,44 @@ class PSIO {
     void read_entry(int unit, const char *key, char *buf, size_t size) { read(unit, key, buf, size, PSIO_ZERO, nullptr); }
 };
 
+/* IWL: every write_value call is recorded, per unit, in call order, with the
+   cutoff the file was opened with; the harness reads the records back.
+   Psi4's own buffers and its cutoff test are not restated here. */
+struct IwlRecord {
+    int p, q, r, s;
+    double value;
+};
+struct IwlFile {
+    double cutoff = 0.0;
+    std::vector<IwlRecord> records;
+};
+inline std::map<int, IwlFile> &iwl_store() {
+    static std::map<int, IwlFile> store;
+    return store;
+}
+class IWL {
+  public:
+    IWL(PSIO *, int unit, double cutoff, int, int) : unit_(unit) {
+        iwl_store()[unit] = IwlFile();
+        iwl_store()[unit].cutoff = cutoff;
+    }
+    void write_value(int p, int q, int r, int s, double value, int, const std::string &, int) {
+        iwl_store()[unit_].records.push_back(IwlRecord{p, q, r, s, value});
+    }
+    void flush(int) {}
+    void set_keep_flag(int) {}
+    void close() {}
+  private:
+    int unit_;
+};
+
 }  // namespace psi
+
+/* stand-in unit numbers for the MO-basis 2-RDM files the IWL writer opens */
+#ifndef PSIF_MO_AA_TPDM
+#define PSIF_MO_AA_TPDM 9001
+#define PSIF_MO_AB_TPDM 9002
+#define PSIF_MO_BB_TPDM 9003
+#endif
 
 #endif

@@ -71,3 +71,23 @@ def test_rdm_files_round_trip(tmp_path):
     assert hb.V2RDMProblem.read_rdm_files(path) == p.rdm_entries(x)
     d = hb.DOCIProblem(3, 1, 1, "DQG")   # DOCI writes the three spin blocks only
     assert set(d.rdm_records(np.zeros(d.n_primal))) == {"D2aa", "D2bb", "D2ab"}
+
+
+def test_iwl_records_match_the_reference_iwl_writer():
+    """WriteTPDM_IWL's write_value calls, in order: labels and values."""
+    from oracle.maps import RefProblem
+    rng = np.random.default_rng(19)
+    for n, na, nb in cases():
+        r = RefProblem(n, na, nb, "DQG", True, True, h=rng.standard_normal((n, n)),
+                       g=rng.standard_normal((n,) * 4))
+        x = rng.standard_normal(r.n_primal)
+        r.write_rdms(x)
+        want, cutoff = r.iwl_records()
+        assert cutoff == 1e-14
+        p = hb.V2RDMProblem(n, na, nb, "DQG")
+        got = p.tpdm_iwl_records(x)
+        for name, (labels, values) in want.items():
+            g = got[name]
+            assert np.array_equal(np.stack([g["i"], g["j"], g["k"], g["l"]], axis=1), labels), (n, name)
+            assert np.array_equal(g["value"], values), (n, na, nb, name)
+        p.close()
