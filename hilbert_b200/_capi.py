@@ -134,13 +134,13 @@ def load(path=LIB_PATH):
         "v2b_problem_refine_counts": (ctypes.c_int, [vp, lp, ctypes.c_int]),
         "v2b_problem_set_projection_mode": (ctypes.c_int, [vp, ctypes.c_int]),
         "v2b_problem_pack_dims": (ctypes.c_int, [vp, lp, lp]),
-        "v2b_problem_rdm_counts": (ctypes.c_int, [vp, vp]),
+        "v2b_problem_rdm_counts": (ctypes.c_int, [vp, ctypes.c_int, vp]),
         "v2b_problem_set_state": (ctypes.c_int, [vp, ctypes.c_double, dp, dp]),
         "v2b_doci_v2rdm_layout": (ctypes.c_int, [vp, vp, vp, lp]),
         "v2b_batch_problem_create": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(vp)]),
         "v2b_problem_palette": (ctypes.c_int, [vp, ctypes.c_int, vp, ip]),
-        "v2b_problem_tpdm_iwl_records": (ctypes.c_int, [vp, vp, vp, vp, vp]),
-        "v2b_problem_rdm_records": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, vp, vp]),
+        "v2b_problem_tpdm_iwl_records": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp, vp]),
+        "v2b_problem_rdm_records": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp, vp, vp, vp, vp]),
         "v2b_problem_projection_profile": (ctypes.c_int, [vp, dp, lp, ctypes.c_int]),
         "v2b_problem_cg_profile": (ctypes.c_int, [vp, dp, ctypes.c_int]),
         "v2b_problem_pack_spatial_density": (ctypes.c_int, [vp, vp, vp, vp, vp]),

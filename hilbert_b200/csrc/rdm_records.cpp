@@ -4,10 +4,11 @@
 //   WriteTPDM          src/v2rdm_casscf/write_tpdm.cc:40-310   (D2aa, D2bb, D2ab)
 //   WriteTPDMSpinFree  src/v2rdm_casscf/write_tpdm.cc:312-519  (D2)
 //   WriteOPDM          src/v2rdm_casscf/write_opdm.cc:40-114   (D1a, D1b)
-// for the C1 active space (no frozen or restricted core, so the core
-// records of those functions are empty; orbital numbers are active indices),
-// and as v2RDM-DOCI's WriteTPDM (src/v2rdm_doci/write_tpdm.cc:47-176) for a
-// DOCI problem.
+//   WriteTPDM_IWL      src/v2rdm_casscf/write_tpdm_iwl.cc:45-205 (IWL labels)
+// for C1 with ncore doubly occupied (restricted) orbitals numbered 0 ..
+// ncore-1 ahead of the active ones (active orbital i is ncore + i); and as
+// v2RDM-DOCI's WriteTPDM (src/v2rdm_doci/write_tpdm.cc:47-176) for a DOCI
+// problem (no core).
 #include "rdm_records.h"
 
 #include <stdexcept>
@@ -18,33 +19,44 @@
 namespace v2b {
 
 namespace {
-void check(const Problem &p) {
+void check(const Problem &p, int ncore) {
     if (p.spec.batch_parts) throw std::invalid_argument("density records of a batch: ask each part");
+    if (ncore < 0) throw std::invalid_argument("ncore must be >= 0");
+    if (p.spec.doci && ncore) throw std::invalid_argument("v2RDM-DOCI writes no core records");
 }
 
 struct Blocks {   // where the spin blocks sit in the vector the records read
     int64_t d2ab, d2aa, d2bb, d1a, d1b;
 };
 
-void records(const Problem &p, const double *x, const Blocks &o, TpdmRecord *d2aa, TpdmRecord *d2bb,
-             TpdmRecord *d2ab, TpdmRecord *d2, OpdmRecord *d1a, OpdmRecord *d1b) {
-    const int n = p.n, gab = p.gab, gaa = p.gaa;
-    int64_t caa = 0, cab = 0, csf = 0;
+// a record sink that counts when given no array
+struct Out {
+    TpdmRecord *r;
+    int64_t n = 0;
+    void put(int i, int j, int k, int l, double v) {
+        if (r) r[n] = TpdmRecord{i, j, k, l, v};
+        n++;
+    }
+};
+
+void records(const Problem &p, const double *x, const Blocks &o, int ncore, TpdmRecord *d2aa,
+             TpdmRecord *d2bb, TpdmRecord *d2ab, TpdmRecord *d2, OpdmRecord *d1a, OpdmRecord *d1b) {
+    const int n = p.n, gab = p.gab, gaa = p.gaa, c0 = ncore;
+    Out aa{d2aa}, bb{d2bb}, ab{d2ab}, sf{d2};
+    // active-active (write_tpdm.cc:55-108, 320-372)
     for (int ij = 0; ij < gab; ij++) {
         const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
         for (int kl = 0; kl < gab; kl++) {
             const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
             const double vab = x[o.d2ab + (int64_t)ij * gab + kl];
-            if (d2ab) d2ab[cab] = TpdmRecord{i, j, k, l, vab};
-            cab++;
-            if (i != j && k != l) {   // write_tpdm.cc:86-105: signed by the order of both pairs
+            ab.put(c0 + i, c0 + j, c0 + k, c0 + l, vab);
+            if (i != j && k != l) {   // signed by the order of both pairs
                 const int64_t e = (int64_t)p.iaa(i, j) * gaa + p.iaa(k, l);
                 const double s = (double)((i < j ? 1 : -1) * (k < l ? 1 : -1));
-                if (d2aa) d2aa[caa] = TpdmRecord{i, j, k, l, s * x[o.d2aa + e]};
-                if (d2bb) d2bb[caa] = TpdmRecord{i, j, k, l, s * x[o.d2bb + e]};
-                caa++;
+                aa.put(c0 + i, c0 + j, c0 + k, c0 + l, s * x[o.d2aa + e]);
+                bb.put(c0 + i, c0 + j, c0 + k, c0 + l, s * x[o.d2bb + e]);
             }
-            if (d2) {   // write_tpdm.cc:320-372
+            if (d2) {
                 double v = 0.0;
                 v += vab;
                 v += x[o.d2ab + (int64_t)p.iab(j, i) * gab + p.iab(l, k)];
@@ -56,31 +68,74 @@ void records(const Problem &p, const double *x, const Blocks &o, TpdmRecord *d2a
                     v += sg * x[o.d2aa + e];
                     v += sg * x[o.d2bb + e];
                 }
-                d2[csf] = TpdmRecord{i, j, k, l, v};
+                sf.put(c0 + i, c0 + j, c0 + k, c0 + l, v);
+            } else {
+                sf.n++;
             }
-            csf++;
         }
     }
+    // core-core (write_tpdm.cc:110-147, 374-405)
+    for (int i = 0; i < c0; i++)
+        for (int j = 0; j < c0; j++) {
+            ab.put(i, j, i, j, 1.0);
+            if (i != j) {
+                aa.put(i, j, i, j, 1.0);
+                bb.put(i, j, i, j, 1.0);
+                aa.put(i, j, j, i, -1.0);
+                bb.put(i, j, j, i, -1.0);
+            }
+            sf.put(i, j, i, j, i != j ? 2.0 + 2.0 : 2.0);
+            if (i != j) sf.put(i, j, j, i, -2.0);
+        }
+    // core-active, from D1 (write_tpdm.cc:149-224, 407-462)
+    for (int i = 0; i < c0; i++)
+        for (int j = 0; j < n; j++)
+            for (int l = 0; l < n; l++) {
+                const int jf = c0 + j, lf = c0 + l;
+                const double va = x[o.d1a + (int64_t)j * n + l], vb = x[o.d1b + (int64_t)j * n + l];
+                aa.put(i, jf, i, lf, va);
+                bb.put(i, jf, i, lf, vb);
+                aa.put(i, jf, lf, i, -va);
+                bb.put(i, jf, lf, i, -vb);
+                aa.put(jf, i, lf, i, va);
+                bb.put(jf, i, lf, i, vb);
+                aa.put(jf, i, i, lf, -va);
+                bb.put(jf, i, i, lf, -vb);
+                ab.put(i, jf, i, lf, vb);    // valab: the beta D1
+                ab.put(jf, i, lf, i, va);    // valba: the alpha D1
+                const double sum = va + vb + vb + va, neg = -va - vb;
+                sf.put(i, jf, i, lf, sum);
+                sf.put(i, jf, lf, i, neg);
+                sf.put(jf, i, lf, i, sum);
+                sf.put(jf, i, i, lf, neg);
+            }
+    // D1 (write_opdm.cc:50-106): active, then core
     int64_t c1 = 0;
     for (int i = 0; i < n; i++)
         for (int j = 0; j < n; j++, c1++) {
-            if (d1a) d1a[c1] = OpdmRecord{i, j, x[o.d1a + (int64_t)i * n + j]};
-            if (d1b) d1b[c1] = OpdmRecord{i, j, x[o.d1b + (int64_t)i * n + j]};
+            if (d1a) d1a[c1] = OpdmRecord{c0 + i, c0 + j, x[o.d1a + (int64_t)i * n + j]};
+            if (d1b) d1b[c1] = OpdmRecord{c0 + i, c0 + j, x[o.d1b + (int64_t)i * n + j]};
         }
+    for (int i = 0; i < c0; i++, c1++) {
+        if (d1a) d1a[c1] = OpdmRecord{i, i, 1.0};
+        if (d1b) d1b[c1] = OpdmRecord{i, i, 1.0};
+    }
 }
 }  // namespace
 
-RdmCounts rdm_counts(const Problem &p) {
-    check(p);
-    const int64_t n = p.n, gab = p.gab, same = n * (n - 1) * n * (n - 1);
+RdmCounts rdm_counts(const Problem &p, int ncore) {
+    check(p, ncore);
+    const int64_t n = p.n, gab = p.gab, c = ncore, same = n * (n - 1) * n * (n - 1);
     if (p.spec.doci)   // src/v2rdm_doci/write_tpdm.cc writes the three spin blocks only
         return RdmCounts{same, same, gab * gab, -1, -1, -1};
-    return RdmCounts{same, same, gab * gab, gab * gab, n * n, n * n};
+    const int64_t aa = same + 2 * c * (c - 1) + 4 * c * n * n;
+    return RdmCounts{aa, aa, gab * gab + c * c + 2 * c * n * n, gab * gab + c * c + c * (c - 1) + 4 * c * n * n,
+                     n * n + c, n * n + c};
 }
 
-void rdm_records(const Problem &p, const double *x, TpdmRecord *d2aa, TpdmRecord *d2bb,
+void rdm_records(const Problem &p, const double *x, int ncore, TpdmRecord *d2aa, TpdmRecord *d2bb,
                  TpdmRecord *d2ab, TpdmRecord *d2, OpdmRecord *d1a, OpdmRecord *d1b) {
-    check(p);
+    check(p, ncore);
     if (p.spec.doci) {
         // DOCI's WriteTPDM (src/v2rdm_doci/write_tpdm.cc:47-176) writes the
         // spin blocks its PackSpatialDensity expands, D2bb from D2aa
@@ -88,35 +143,60 @@ void rdm_records(const Problem &p, const double *x, TpdmRecord *d2aa, TpdmRecord
         doci_v2rdm_layout(p, x, layout.data());
         const int64_t gab2 = (int64_t)p.gab * p.gab, gaa2 = (int64_t)p.gaa * p.gaa, nn = (int64_t)p.n * p.n;
         const Blocks o{0, gab2, gab2 + gaa2, gab2 + 2 * gaa2, gab2 + 2 * gaa2 + nn};
-        records(p, layout.data(), o, d2aa, d2bb, d2ab, nullptr, nullptr, nullptr);
+        records(p, layout.data(), o, 0, d2aa, d2bb, d2ab, nullptr, nullptr, nullptr);
         return;
     }
-    records(p, x, Blocks{p.d2ab, p.d2aa, p.d2bb, p.d1a, p.d1b}, d2aa, d2bb, d2ab, d2, d1a, d1b);
+    records(p, x, Blocks{p.d2ab, p.d2aa, p.d2bb, p.d1a, p.d1b}, ncore, d2aa, d2bb, d2ab, d2, d1a, d1b);
 }
 
-void iwl_records(const Problem &p, const double *x, TpdmRecord *aa, TpdmRecord *ab, TpdmRecord *bb) {
+void iwl_records(const Problem &p, const double *x, int ncore, TpdmRecord *aa_out, TpdmRecord *ab_out,
+                 TpdmRecord *bb_out) {
     // WriteTPDM_IWL (src/v2rdm_casscf/write_tpdm_iwl.cc:45-205): the calls it
-    // makes to IWL::write_value, labels in (i, k, j, l) order for the element
-    // D2(ij, kl); aa and bb scaled by 1/4; no core orbitals, so no core calls
-    check(p);
+    // makes to IWL::write_value, labels (i, k, j, l) for the element D2(ij, kl),
+    // aa and bb values scaled by 1/4
+    check(p, ncore);
     if (p.spec.doci) throw std::invalid_argument("the IWL 2-RDM of v2RDM problems");
-    const int gab = p.gab, gaa = p.gaa;
-    int64_t caa = 0, cab = 0;
+    const int n = p.n, gab = p.gab, gaa = p.gaa, c0 = ncore;
+    Out aa{aa_out}, ab{ab_out}, bb{bb_out};
     for (int ij = 0; ij < gab; ij++) {
         const int i = p.bas_ab[2 * ij], j = p.bas_ab[2 * ij + 1];
         for (int kl = 0; kl < gab; kl++) {
             const int k = p.bas_ab[2 * kl], l = p.bas_ab[2 * kl + 1];
-            if (ab) ab[cab] = TpdmRecord{i, k, j, l, x[p.d2ab + (int64_t)ij * gab + kl]};
-            cab++;
+            ab.put(c0 + i, c0 + k, c0 + j, c0 + l, x[p.d2ab + (int64_t)ij * gab + kl]);
             if (i != j && k != l) {
                 const int64_t e = (int64_t)p.iaa(i, j) * gaa + p.iaa(k, l);
                 const double s = 0.25 * (double)((i < j ? 1 : -1) * (k < l ? 1 : -1));
-                if (aa) aa[caa] = TpdmRecord{i, k, j, l, s * x[p.d2aa + e]};
-                if (bb) bb[caa] = TpdmRecord{i, k, j, l, s * x[p.d2bb + e]};
-                caa++;
+                aa.put(c0 + i, c0 + k, c0 + j, c0 + l, s * x[p.d2aa + e]);
+                bb.put(c0 + i, c0 + k, c0 + j, c0 + l, s * x[p.d2bb + e]);
             }
         }
     }
+    for (int i = 0; i < c0; i++)   // core-core (:84-107)
+        for (int j = 0; j < c0; j++) {
+            ab.put(i, i, j, j, 1.0);
+            if (i != j) {
+                aa.put(i, i, j, j, 0.25);
+                bb.put(i, i, j, j, 0.25);
+                aa.put(i, j, j, i, -0.25);
+                bb.put(i, j, j, i, -0.25);
+            }
+        }
+    for (int i = 0; i < c0; i++)   // core-active, from D1 (:109-190)
+        for (int j = 0; j < n; j++)
+            for (int l = 0; l < n; l++) {
+                const int jf = c0 + j, lf = c0 + l;
+                const double va = 0.25 * x[p.d1a + (int64_t)j * n + l], vb = 0.25 * x[p.d1b + (int64_t)j * n + l];
+                aa.put(i, i, jf, lf, va);
+                bb.put(i, i, jf, lf, vb);
+                aa.put(i, lf, jf, i, -va);
+                bb.put(i, lf, jf, i, -vb);
+                aa.put(jf, lf, i, i, va);
+                bb.put(jf, lf, i, i, vb);
+                aa.put(jf, i, i, lf, -va);
+                bb.put(jf, i, i, lf, -vb);
+                ab.put(i, i, jf, lf, x[p.d1b + (int64_t)j * n + l]);
+                ab.put(jf, lf, i, i, x[p.d1a + (int64_t)j * n + l]);
+            }
 }
 
 }  // namespace v2b

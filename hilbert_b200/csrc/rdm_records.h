@@ -19,13 +19,15 @@ struct RdmCounts {
     int64_t d2aa, d2bb, d2ab, d2, d1a, d1b;
 };
 
-RdmCounts rdm_counts(const Problem &p);
-// x is the host primal vector; any output may be null
-void rdm_records(const Problem &p, const double *x, TpdmRecord *d2aa, TpdmRecord *d2bb,
+// ncore doubly occupied orbitals come first (0 .. ncore-1), active orbital
+// i is ncore + i; x is the host primal vector; any output may be null
+RdmCounts rdm_counts(const Problem &p, int ncore);
+void rdm_records(const Problem &p, const double *x, int ncore, TpdmRecord *d2aa, TpdmRecord *d2bb,
                  TpdmRecord *d2ab, TpdmRecord *d2, OpdmRecord *d1a, OpdmRecord *d1b);
 
 // the IWL::write_value calls of WriteTPDM_IWL (v2RDM problems), as records
 // (i, j, k, l) = its labels; counts are rdm_counts' d2aa (aa, bb) and d2ab
-void iwl_records(const Problem &p, const double *x, TpdmRecord *aa, TpdmRecord *ab, TpdmRecord *bb);
+void iwl_records(const Problem &p, const double *x, int ncore, TpdmRecord *aa, TpdmRecord *ab,
+                 TpdmRecord *bb);
 
 }  // namespace v2b

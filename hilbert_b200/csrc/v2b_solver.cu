@@ -1746,33 +1746,33 @@ int v2b_doci_v2rdm_layout(const v2b_problem *p, const double *x, double *out, lo
         return V2B_OK;
     });
 }
-int v2b_problem_rdm_counts(const v2b_problem *p, long *counts) {
+int v2b_problem_rdm_counts(const v2b_problem *p, int ncore, long *counts) {
     return guarded([&] {
         if (!p || !counts) throw std::invalid_argument("rdm_counts: NULL argument");
-        const v2b::RdmCounts c = v2b::rdm_counts(p->prob);
+        const v2b::RdmCounts c = v2b::rdm_counts(p->prob, ncore);
         const long v[6] = {(long)c.d2aa, (long)c.d2bb, (long)c.d2ab, (long)c.d2, (long)c.d1a, (long)c.d1b};
         std::copy(v, v + 6, counts);
         return V2B_OK;
     });
 }
-int v2b_problem_rdm_records(const v2b_problem *p, const double *x, v2b_tpdm_record *d2aa,
+int v2b_problem_rdm_records(const v2b_problem *p, int ncore, const double *x, v2b_tpdm_record *d2aa,
                             v2b_tpdm_record *d2bb, v2b_tpdm_record *d2ab, v2b_tpdm_record *d2,
                             v2b_opdm_record *d1a, v2b_opdm_record *d1b) {
     static_assert(sizeof(v2b_tpdm_record) == sizeof(v2b::TpdmRecord), "record layout");
     static_assert(sizeof(v2b_opdm_record) == sizeof(v2b::OpdmRecord), "record layout");
     return guarded([&] {
         if (!p || !x) throw std::invalid_argument("rdm_records: NULL argument");
-        v2b::rdm_records(p->prob, x, (v2b::TpdmRecord *)d2aa, (v2b::TpdmRecord *)d2bb,
+        v2b::rdm_records(p->prob, x, ncore, (v2b::TpdmRecord *)d2aa, (v2b::TpdmRecord *)d2bb,
                          (v2b::TpdmRecord *)d2ab, (v2b::TpdmRecord *)d2, (v2b::OpdmRecord *)d1a,
                          (v2b::OpdmRecord *)d1b);
         return V2B_OK;
     });
 }
-int v2b_problem_tpdm_iwl_records(const v2b_problem *p, const double *x, v2b_tpdm_record *d2aa,
+int v2b_problem_tpdm_iwl_records(const v2b_problem *p, int ncore, const double *x, v2b_tpdm_record *d2aa,
                                  v2b_tpdm_record *d2ab, v2b_tpdm_record *d2bb) {
     return guarded([&] {
         if (!p || !x) throw std::invalid_argument("tpdm_iwl_records: NULL argument");
-        v2b::iwl_records(p->prob, x, (v2b::TpdmRecord *)d2aa, (v2b::TpdmRecord *)d2ab,
+        v2b::iwl_records(p->prob, x, ncore, (v2b::TpdmRecord *)d2aa, (v2b::TpdmRecord *)d2ab,
                          (v2b::TpdmRecord *)d2bb);
         return V2B_OK;
     });

@@ -325,49 +325,51 @@ class V2RDMProblem:
                 out.setdefault(name, {})[key] = z[k].tobytes()
         return out
 
-    def rdm_records(self, x):
+    def rdm_records(self, x, ncore=0):
         """{file: records} as WriteTPDM, WriteTPDMSpinFree and WriteOPDM emit
         them (write_tpdm.cc:40-519, write_opdm.cc:40-114) for the host or
         device primal vector x: D2aa, D2bb, D2ab, the spin-free D2, D1a, D1b
-        (for DOCI, what its WriteTPDM writes: D2aa, D2bb, D2ab)."""
+        (for DOCI, what its WriteTPDM writes: D2aa, D2bb, D2ab).  ncore
+        doubly occupied orbitals are numbered first, with their core-core and
+        core-active records."""
         xh = np.ascontiguousarray(x.detach().cpu().numpy() if hasattr(x, "detach") else x,
                                   dtype=np.float64)
         if xh.shape != (self.n_primal,):
             raise ValueError(f"x must hold {self.n_primal} values")
         counts = np.zeros(6, np.int64)
-        check(self._lib.v2b_problem_rdm_counts(self._h, counts.ctypes.data))
+        check(self._lib.v2b_problem_rdm_counts(self._h, int(ncore), counts.ctypes.data))
         out = {name: np.zeros(int(cnt), self.TPDM_RECORD if name.startswith("D2") else self.OPDM_RECORD)
                for name, cnt in zip(self.RDM_FILES, counts) if cnt >= 0}   # -1: not written
         check(self._lib.v2b_problem_rdm_records(
-            self._h, xh.ctypes.data, *[out[name].ctypes.data if name in out else None
+            self._h, int(ncore), xh.ctypes.data, *[out[name].ctypes.data if name in out else None
                                        for name in self.RDM_FILES]))
         return out
 
-    def tpdm_iwl_records(self, x):
+    def tpdm_iwl_records(self, x, ncore=0):
         """{"D2aa", "D2ab", "D2bb"}: the IWL::write_value calls of WriteTPDM_IWL
         (write_tpdm_iwl.cc:45-205) as records, fields i, j, k, l holding the
-        labels (i, k, j, l) of D2(ij, kl)."""
+        labels (i, k, j, l) of D2(ij, kl); ncore as in rdm_records."""
         xh = np.ascontiguousarray(x.detach().cpu().numpy() if hasattr(x, "detach") else x,
                                   dtype=np.float64)
         if xh.shape != (self.n_primal,):
             raise ValueError(f"x must hold {self.n_primal} values")
         counts = np.zeros(6, np.int64)
-        check(self._lib.v2b_problem_rdm_counts(self._h, counts.ctypes.data))
+        check(self._lib.v2b_problem_rdm_counts(self._h, int(ncore), counts.ctypes.data))
         out = {"D2aa": np.zeros(int(counts[0]), self.TPDM_RECORD),
                "D2ab": np.zeros(int(counts[2]), self.TPDM_RECORD),
                "D2bb": np.zeros(int(counts[0]), self.TPDM_RECORD)}
-        check(self._lib.v2b_problem_tpdm_iwl_records(self._h, xh.ctypes.data, out["D2aa"].ctypes.data,
+        check(self._lib.v2b_problem_tpdm_iwl_records(self._h, int(ncore), xh.ctypes.data, out["D2aa"].ctypes.data,
                                                      out["D2ab"].ctypes.data, out["D2bb"].ctypes.data))
         return out
 
-    def rdm_entries(self, x):
+    def rdm_entries(self, x, ncore=0):
         """{file: {entry: bytes}}: every entry hilbert's writers put in their
         PSIO files, byte for byte (the records when there are any, "length",
-        and for the D2 files "NUMBER ACTIVE ORBITALS", "ACTIVE ORBITALS" and
-        "NUMBER INACTIVE ORBITALS"; write_tpdm.cc:226-262,
-        write_opdm.cc:108-113)."""
-        recs = self.rdm_records(x)
-        n = int(self.nmo)
+        and for the D2 files "NUMBER ACTIVE ORBITALS", "ACTIVE ORBITALS",
+        "NUMBER INACTIVE ORBITALS" and, with core orbitals, "INACTIVE
+        ORBITALS"; write_tpdm.cc:226-262, write_opdm.cc:108-113)."""
+        recs = self.rdm_records(x, ncore)
+        n, c = int(self.nmo), int(ncore)
         out = {}
         for name, r in recs.items():
             # an entry exists once something is written to it
@@ -375,16 +377,18 @@ class V2RDMProblem:
             e["length"] = np.int64(len(r)).tobytes()
             if name.startswith("D2"):
                 e["NUMBER ACTIVE ORBITALS"] = np.int32(n).tobytes()
-                e["ACTIVE ORBITALS"] = np.arange(n, dtype=np.int32).tobytes()
-                e["NUMBER INACTIVE ORBITALS"] = np.int32(0).tobytes()
+                e["ACTIVE ORBITALS"] = np.arange(c, c + n, dtype=np.int32).tobytes()
+                e["NUMBER INACTIVE ORBITALS"] = np.int32(c).tobytes()
+                if c:
+                    e["INACTIVE ORBITALS"] = np.arange(c, dtype=np.int32).tobytes()
             out[name] = e
         return out
 
-    def write_rdm_files(self, path, x):
-        """Writes rdm_entries(x) to one .npz archive, one array per entry,
-        named "<file>/<entry>" (the PSIO container itself is Psi4's)."""
+    def write_rdm_files(self, path, x, ncore=0):
+        """Writes rdm_entries(x, ncore) to one .npz archive, one array per
+        entry, named "<file>/<entry>" (the PSIO container itself is Psi4's)."""
         arrays = {f"{name}/{key}": np.frombuffer(val, np.uint8)
-                  for name, ent in self.rdm_entries(x).items() for key, val in ent.items()}
+                  for name, ent in self.rdm_entries(x, ncore).items() for key, val in ent.items()}
         np.savez(path, **arrays)
 
     def pack_spatial_density(self, x):

@@ -266,8 +266,9 @@ int v2b_problem_pack_spatial_density(v2b_problem *p, const double *d_x, double *
  * primal vector x: the same records, order and values as WriteTPDM
  * (src/v2rdm_casscf/write_tpdm.cc:40-310: files D2aa, D2bb, D2ab),
  * WriteTPDMSpinFree (:312-519: file D2) and WriteOPDM (write_opdm.cc:40-114:
- * files D1a, D1b), for the C1 active space (orbital numbers are active
- * indices; no core records).  The record layouts are the reference's struct
+ * files D1a, D1b), for C1 with ncore >= 0 doubly occupied (restricted)
+ * orbitals numbered 0 .. ncore-1 ahead of the active ones (active orbital i
+ * is ncore + i), including the writers' core-core and core-active records.  The record layouts are the reference's struct
  * tpdm and struct opdm (v2rdm_solver.h:53-65).  counts[6] receives the
  * record counts in the order D2aa, D2bb, D2ab, D2, D1a, D1b, -1 for a file
  * the problem's writers do not write: a DOCI problem gives what v2RDM-DOCI's
@@ -281,17 +282,17 @@ typedef struct {
     int i, j;
     double value;
 } v2b_opdm_record;
-int v2b_problem_rdm_counts(const v2b_problem *p, long *counts);
-int v2b_problem_rdm_records(const v2b_problem *p, const double *x, v2b_tpdm_record *d2aa,
+int v2b_problem_rdm_counts(const v2b_problem *p, int ncore, long *counts);
+int v2b_problem_rdm_records(const v2b_problem *p, int ncore, const double *x, v2b_tpdm_record *d2aa,
                             v2b_tpdm_record *d2bb, v2b_tpdm_record *d2ab, v2b_tpdm_record *d2,
                             v2b_opdm_record *d1a, v2b_opdm_record *d1b);
 /* The 2-RDM as WriteTPDM_IWL hands it to Psi4's IWL writer for gradients
  * (src/v2rdm_casscf/write_tpdm_iwl.cc:45-205): one record per write_value
  * call, in call order, labels (i, k, j, l) for the element D2(ij, kl), aa and
- * bb values scaled by 1/4 (record counts: counts[0] and counts[2] of
- * v2b_problem_rdm_counts).  The IWL files store only values above their
+ * bb values scaled by 1/4, core orbitals as in v2b_problem_rdm_records
+ * (record counts: counts[0] and counts[2] of v2b_problem_rdm_counts).  The IWL files store only values above their
  * cutoff, 1e-14; that filtering is the IWL writer's.  v2RDM problems only. */
-int v2b_problem_tpdm_iwl_records(const v2b_problem *p, const double *x, v2b_tpdm_record *d2aa,
+int v2b_problem_tpdm_iwl_records(const v2b_problem *p, int ncore, const double *x, v2b_tpdm_record *d2aa,
                                  v2b_tpdm_record *d2ab, v2b_tpdm_record *d2bb);
 
 /* ---- 3. allocation-free projection ------------------------------------------ */

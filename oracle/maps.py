@@ -257,14 +257,16 @@ class RefProblem:
                      ("value", np.float64)])
     OPDM = np.dtype([("i", np.int32), ("j", np.int32), ("value", np.float64)])
 
-    def write_rdms(self, x):
-        """Runs the reference's WriteTPDM, WriteTPDMSpinFree and WriteOPDM on
-        x and returns what they wrote: {file: records} and {file: {entry: bytes}}"""
+    def write_rdms(self, x, ncore=0):
+        """Runs the reference's WriteTPDM, WriteTPDMSpinFree, WriteOPDM and
+        WriteTPDM_IWL on x, with ncore restricted doubly occupied orbitals
+        numbered first, and returns what the PSIO writers wrote: {file:
+        records} and {file: {entry: bytes}} (iwl_records has the rest)"""
         lib = self._lib
-        lib.v2b_ref_write_rdms.argtypes = [ctypes.c_void_p, _dp]
+        lib.v2b_ref_write_rdms.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int]
         lib.v2b_ref_psio_entry.restype = ctypes.c_long
         lib.v2b_ref_psio_entry.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p]
-        if lib.v2b_ref_write_rdms(self._p, np.ascontiguousarray(x, np.float64)):
+        if lib.v2b_ref_write_rdms(self._p, np.ascontiguousarray(x, np.float64), int(ncore)):
             raise RuntimeError(lib.v2b_ref_last_error().decode())
         records, entries = {}, {}
         for name, unit in self.RDM_UNITS.items():

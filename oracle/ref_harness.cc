@@ -136,12 +136,25 @@ class RefProblem : public v2RDMSolver {
     }
     // write_tpdm.cc:40-519 and write_opdm.cc:40-114 on a given primal vector,
     // into the in-memory PSIO stand-in
-    void write_rdms(const double *xin) {
+    // the writers on a given x; with ncore > 0 they see the C1 orbital
+    // numbering build_mapping_arrays gives restricted doubly occupied
+    // orbitals (basis.cc:100-111, 415-424): core 0 .. ncore-1, active i at ncore + i
+    void write_rdms(const double *xin, int ncore) {
         std::memcpy(x->pointer(), xin, sizeof(double) * n_primal_);
+        const int saved_rst = rstcpi_[0], saved_nrst = nrstc_, saved_off = pitzer_offset_full[0];
+        std::vector<int> saved_full(full_basis, full_basis + amo_);
+        rstcpi_[0] = ncore;
+        nrstc_ = ncore;
+        pitzer_offset_full[0] = 0;
+        for (int i = 0; i < amo_; i++) full_basis[i] = ncore + i;
         WriteTPDM();
         WriteTPDMSpinFree();
         WriteOPDM();
         WriteTPDM_IWL();   // write_tpdm_iwl.cc:45-205, into the IWL stand-in
+        rstcpi_[0] = saved_rst;
+        nrstc_ = saved_nrst;
+        pitzer_offset_full[0] = saved_off;
+        std::copy(saved_full.begin(), saved_full.end(), full_basis);
     }
     long d2_dim() const { return d2_act_spatial_dim_; }
     long d1_dim() const { return d1_act_spatial_dim_; }
@@ -297,9 +310,9 @@ long v2b_ref_pack_dims(void *p, long *d1n) {
 }
 /* runs the reference's RDM writers on x; their files stay in the PSIO
    stand-in until the next call */
-int v2b_ref_write_rdms(void *p, const double *x) {
+int v2b_ref_write_rdms(void *p, const double *x, int ncore) {
     try {
-        static_cast<RefProblem *>(p)->write_rdms(x);
+        static_cast<RefProblem *>(p)->write_rdms(x, ncore);
         return 0;
     } catch (const std::exception &e) { g_last_error = e.what(); return 1; }
 }

@@ -214,7 +214,7 @@ def test_new_entry_points_refuse_bad_arguments():
     n = ctypes.c_int()
     assert lib.v2b_batch_problem_create(None, 1, ctypes.byref(out)) == bad
     assert lib.v2b_batch_problem_create((ctypes.c_void_p * 1)(None), 1, ctypes.byref(out)) == bad
-    assert lib.v2b_problem_rdm_counts(None, counts.ctypes.data) == bad
+    assert lib.v2b_problem_rdm_counts(None, 0, counts.ctypes.data) == bad
     assert lib.v2b_problem_palette(None, 0, None, ctypes.byref(n)) == bad
     assert lib.v2b_doci_v2rdm_layout(None, None, None, ctypes.byref(size)) == bad
     p = hb.V2RDMProblem(3, 1, 1, "DQG")
@@ -224,7 +224,8 @@ def test_new_entry_points_refuse_bad_arguments():
     for mu in (0.0, -1.0, float("nan"), float("inf")):
         assert lib.v2b_problem_set_state(p._h, mu, y.ctypes.data_as(dp), z.ctypes.data_as(dp)) == bad
     assert lib.v2b_problem_set_state(p._h, 0.5, None, z.ctypes.data_as(dp)) == bad
-    assert lib.v2b_problem_rdm_records(p._h, None, None, None, None, None, None, None) == bad
+    assert lib.v2b_problem_rdm_records(p._h, 0, None, None, None, None, None, None, None) == bad
+    assert lib.v2b_problem_rdm_counts(p._h, -1, counts.ctypes.data) == bad
     p.close()
 
 

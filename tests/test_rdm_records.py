@@ -19,23 +19,24 @@ def cases():
             yield n, na, nb
 
 
-def test_rdm_entries_match_the_reference_writers():
-    """Every record and every metadata entry, byte for byte."""
+@pytest.mark.parametrize("ncore", [0, 1, 3])
+def test_rdm_entries_match_the_reference_writers(ncore):
+    """Every record and every metadata entry, byte for byte, with and without
+    restricted doubly occupied orbitals."""
     from oracle.maps import RefProblem
-    rng = np.random.default_rng(17)
+    rng = np.random.default_rng(17 + ncore)
     for n, na, nb in cases():
         r = RefProblem(n, na, nb, "DQG", True, True, h=rng.standard_normal((n, n)),
                        g=rng.standard_normal((n,) * 4))
         x = rng.standard_normal(r.n_primal)
-        _, ref_entries = r.write_rdms(x)
+        _, ref_entries = r.write_rdms(x, ncore)
         p = hb.V2RDMProblem(n, na, nb, "DQG")
-        mine = p.rdm_entries(x)
+        mine = p.rdm_entries(x, ncore)
         assert set(mine) == set(ref_entries)
         for name, entries in ref_entries.items():
-            assert set(mine[name]) == set(entries) - {"INACTIVE ORBITALS"}, name
+            assert set(mine[name]) == set(entries), (ncore, name)
             for key, val in entries.items():
-                if key != "INACTIVE ORBITALS":   # empty without core orbitals
-                    assert mine[name][key] == val, (n, na, nb, name, key)
+                assert mine[name][key] == val, (n, na, nb, ncore, name, key)
         p.close()
 
 
@@ -73,19 +74,20 @@ def test_rdm_files_round_trip(tmp_path):
     assert set(d.rdm_records(np.zeros(d.n_primal))) == {"D2aa", "D2bb", "D2ab"}
 
 
-def test_iwl_records_match_the_reference_iwl_writer():
+@pytest.mark.parametrize("ncore", [0, 2])
+def test_iwl_records_match_the_reference_iwl_writer(ncore):
     """WriteTPDM_IWL's write_value calls, in order: labels and values."""
     from oracle.maps import RefProblem
-    rng = np.random.default_rng(19)
+    rng = np.random.default_rng(19 + ncore)
     for n, na, nb in cases():
         r = RefProblem(n, na, nb, "DQG", True, True, h=rng.standard_normal((n, n)),
                        g=rng.standard_normal((n,) * 4))
         x = rng.standard_normal(r.n_primal)
-        r.write_rdms(x)
+        r.write_rdms(x, ncore)
         want, cutoff = r.iwl_records()
         assert cutoff == 1e-14
         p = hb.V2RDMProblem(n, na, nb, "DQG")
-        got = p.tpdm_iwl_records(x)
+        got = p.tpdm_iwl_records(x, ncore)
         for name, (labels, values) in want.items():
             g = got[name]
             assert np.array_equal(np.stack([g["i"], g["j"], g["k"], g["l"]], axis=1), labels), (n, name)
