@@ -459,3 +459,23 @@ def doci_casscf(h, B, nalpha, nbeta, solve_active=None, positivity="DQG", macro_
         solve_active = doci_solve_active(nmo, nalpha, nbeta, positivity)
     return casscf(h, B, 0, nmo, solve_active, macro_iterations=macro_iterations, active_active=True,
                   orbital_step="focas")
+
+
+def eri_factors(g, rel_tol=1e-12):
+    """Exact factors of 4-index integrals for the DF orbital code:
+    g[p, q, r, s] = (pq|rs) = sum_Q B[Q, p, q] B[Q, r, s].  (pq|rs) over the
+    pairs (pq) is a symmetric positive semidefinite matrix for real orbitals;
+    its eigenvectors with eigenvalues above rel_tol * the largest give B.
+    This lets the focas step of the density-fitted path run on the
+    integrals of hilbert's non-DF path (SCF_TYPE PK, 4-index integrals)."""
+    g = torch.as_tensor(g)
+    n = g.shape[0]
+    M = g.reshape(n * n, n * n)
+    M = 0.5 * (M + M.T)
+    w, V = torch.linalg.eigh(M)
+    top = float(w.max()) if w.numel() else 0.0
+    if float(w.min()) < -max(rel_tol * top, 1e-12) * 1e3:
+        raise ValueError("the integrals are not positive semidefinite over orbital pairs")
+    keep = w > rel_tol * top
+    B = (V[:, keep] * torch.sqrt(w[keep])).T.reshape(-1, n, n)
+    return B

@@ -634,8 +634,8 @@ class v2RDM_DOCIHelper:
     g = (ij|kl) of the nmo orbitals.  POSITIVITY and CONSTRAIN_D3 choose the
     conditions (v2rdm_doci_solver.cc:427-494).  With OPTIMIZE_ORBITALS and the
     density-fitting factors ``B`` (naux x nmo x nmo, g = sum_Q B^Q B^Q) the
-    orbitals are optimised as well (orbital.doci_casscf); otherwise they stay
-    fixed."""
+    orbitals are optimised as well (orbital.doci_casscf); given g alone, its
+    exact factors (orbital.eri_factors) serve as B."""
 
     def __init__(self, nalpha, nbeta, nmo, h, g, options, B=None):
         self.options = options if isinstance(options, Options) else Options(options)
@@ -648,7 +648,8 @@ class v2RDM_DOCIHelper:
             if self.B is None:
                 raise ValueError("give g = (ij|kl) or the density-fitting factors B")
             g = np.einsum("Qij,Qkl->ijkl", self.B, self.B)
-        self.c = self.problem.c_external(self.h, np.ascontiguousarray(g, dtype=np.float64))
+        self._g = np.ascontiguousarray(g, dtype=np.float64)
+        self.c = self.problem.c_external(self.h, self._g)
         self.b = self.problem.b()
         self.x = None
         self.stats = None
@@ -665,6 +666,13 @@ class v2RDM_DOCIHelper:
         """The DOCI energy; with orbital optimisation, after macro_iterations
         SDP solves and orbital steps."""
         p = self.problem
+        if self.options.get("OPTIMIZE_ORBITALS"):
+            import torch
+            if not torch.cuda.is_available():
+                raise _capi.V2BError(_capi.V2B_NO_DEVICE, "v2RDM-DOCI orbital optimisation needs a CUDA device")
+        if self.options.get("OPTIMIZE_ORBITALS") and self.B is None and self._g is not None:
+            from . import orbital
+            self.B = orbital.eri_factors(self._g).numpy()
         if self.options.get("OPTIMIZE_ORBITALS") and self.B is not None:
             import torch
             from . import orbital

@@ -96,3 +96,16 @@ def test_doci_helper_energy(cuda_device):
     assert abs(helper.occupations.sum() - 2 * npair) <= 1e-5
     opt = hb.v2RDM_DOCIHelper(npair, npair, n, h_mo, None, dict(opts, OPTIMIZE_ORBITALS=True), B=B_mo)
     assert opt.compute_energy(macro_iterations=3) < e - 1.0
+
+
+def test_doci_helper_optimises_orbitals_from_4_index_integrals(cuda_device):
+    """Given (ij|kl) alone, the helper factors it exactly and optimises the
+    orbitals: the same energies as from the DF factors themselves."""
+    import hilbert_b200.orbital as ho
+    n, npair = 4, 2
+    h_mo, B_mo, *_ = ho.casscf_df_problem(nbf=n, naux=10, ncore=0, nact=n)
+    g = np.einsum("Qij,Qkl->ijkl", B_mo, B_mo)
+    opts = {"POSITIVITY": "DQG", "OPTIMIZE_ORBITALS": True}
+    e_g = hb.v2RDM_DOCIHelper(npair, npair, n, h_mo, g, opts).compute_energy(macro_iterations=2)
+    e_b = hb.v2RDM_DOCIHelper(npair, npair, n, h_mo, None, opts, B=B_mo).compute_energy(macro_iterations=2)
+    assert abs(e_g - e_b) <= 1e-5

@@ -217,3 +217,27 @@ def test_casscf_macro_iterations_with_the_focas_step():
     n = h_mo.shape[0]
     # the rotated integrals stay those of an orthogonal transformation
     assert abs(float(torch.linalg.eigvalsh(h1).sum()) - float(np.trace(h_mo))) <= 1e-9 * n
+
+
+def test_eri_factors_reproduce_4_index_integrals():
+    """Factors of (pq|rs) give back the integrals, and the DF orbital energy
+    on them equals the energy on the original factors."""
+    rng = np.random.default_rng(12)
+    n, naux = 5, 9
+    B = rng.standard_normal((naux, n, n))
+    B = torch.from_numpy(0.5 * (B + B.transpose(0, 2, 1)))
+    g = torch.einsum("Qpq,Qrs->pqrs", B, B)
+    F = ho.eri_factors(g)
+    assert F.shape[0] <= n * (n + 1) // 2
+    assert torch.allclose(torch.einsum("Qpq,Qrs->pqrs", F, F), g, atol=1e-11)
+    h = torch.from_numpy(rng.standard_normal((n, n)))
+    h = h + h.T
+    D = torch.eye(n, dtype=torch.float64)
+    G = torch.einsum("pq,rs->pqrs", D, D).reshape(n * n, n * n)
+    K = torch.zeros((n, n), dtype=torch.float64)
+    K[0, 1], K[1, 0] = 0.3, -0.3
+    e1 = ho.rotated_energy(K, h, B, D, G)
+    e2 = ho.rotated_energy(K, h, F, D, G)
+    assert abs(float(e1 - e2)) < 1e-10
+    with pytest.raises(ValueError):
+        ho.eri_factors(-g)
