@@ -44,6 +44,12 @@ DEFAULTS = {
     "ORBOPT_MAXITER": 10,           # :168
     "ORBOPT_GRADIENT_CONVERGENCE": 1e-4,   # :153
     "ORBOPT_ENERGY_CONVERGENCE": 1e-8,     # :156
+    "TPDM_WRITE_FULL": False,       # :103
+    "WRITE_CHECKPOINT_FILE": False,  # :208
+    "OPDM_WRITE_FULL": False,       # :286
+    "TPDM_WRITE_SPIN_FREE": False,  # :289
+    "TPDM_WRITE": False,            # :292
+    "DERTYPE": "NONE",              # Psi4's global derivative option
 }
 
 
@@ -612,7 +618,40 @@ class v2RDMHelper:
         # enuc = efzc = 0 for Hubbard / external Hamiltonians (v2rdm_solver.cc:851-853, 972-974)
         self.variables["CURRENT ENERGY"] = e
         self.variables["v2RDM TOTAL ENERGY"] = e
+        self.files = self.written_files()
         return e
+
+    def written_files(self):
+        """The files hilbert's compute_energy writes after the solve under the
+        write options (v2rdm_solver.cc:1474-1516), {file: {entry: bytes}}:
+        TPDM_WRITE (WriteActiveTPDM, write_tpdm.cc:521-602: the active records
+        and "length"), TPDM_WRITE_FULL (WriteTPDM), TPDM_WRITE_SPIN_FREE,
+        OPDM_WRITE_FULL; with DERTYPE FIRST or WRITE_CHECKPOINT_FILE the
+        checkpoint ("CHECKPOINT", entries as in hilbert_b200.checkpoint), and
+        with DERTYPE FIRST the IWL 2-RDM records ("IWL"; the orbital
+        Lagrangian that hilbert also builds then is not)."""
+        o, p, x = self.options, self.problem, self.x
+        out = {}
+        entries = p.rdm_entries(x)
+        if o.get("TPDM_WRITE"):
+            n = int(p.nmo)
+            counts = {"D2aa": n * (n - 1) * n * (n - 1), "D2bb": n * (n - 1) * n * (n - 1), "D2ab": n ** 4}
+            for name, cnt in counts.items():   # the leading active-active records
+                rec = np.frombuffer(entries[name].get(name, b""), self.problem.TPDM_RECORD)[:cnt]
+                out[name] = ({name: rec.tobytes()} if cnt else {}) | {"length": np.int64(cnt).tobytes()}
+        if o.get("TPDM_WRITE_FULL"):
+            out.update({k: entries[k] for k in ("D2aa", "D2bb", "D2ab")})
+        if o.get("TPDM_WRITE_SPIN_FREE"):
+            out["D2"] = entries["D2"]
+        if o.get("OPDM_WRITE_FULL"):
+            out.update({k: entries[k] for k in ("D1a", "D1b")})
+        first = str(o.get("DERTYPE")).upper() == "FIRST"
+        if first or o.get("WRITE_CHECKPOINT_FILE"):
+            out["CHECKPOINT"] = {"MU": np.float64(p.get_mu()).tobytes(), "PRIMAL": x.tobytes(),
+                                 "DUAL 1": p.get_y().tobytes(), "DUAL 2": p.get_z().tobytes()}
+        if first:
+            out["IWL"] = p.tpdm_iwl_records(x)
+        return out
 
     def get_opdm(self):
         """Spin-summed active 1-RDM D1a + D1b (python_api.cc:374-394, C1 active block)."""

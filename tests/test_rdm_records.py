@@ -93,3 +93,23 @@ def test_iwl_records_match_the_reference_iwl_writer(ncore):
             assert np.array_equal(np.stack([g["i"], g["j"], g["k"], g["l"]], axis=1), labels), (n, name)
             assert np.array_equal(g["value"], values), (n, na, nb, name)
         p.close()
+
+
+def test_helper_write_options_select_the_reference_files():
+    """v2RDMHelper.written_files follows hilbert's write options: TPDM_WRITE is
+    WriteActiveTPDM (the leading active records, "length" only)."""
+    from oracle.maps import RefProblem
+    n = 3
+    rng = np.random.default_rng(6)
+    h, g = rng.standard_normal((n, n)), rng.standard_normal((n,) * 4)
+    helper = hb.v2RDMHelper(2, 1, n, h.ravel(), g.ravel(),
+                            {"TPDM_WRITE": True, "OPDM_WRITE_FULL": True, "TPDM_WRITE_SPIN_FREE": True})
+    helper.x = rng.standard_normal(helper.problem.n_primal)   # stands in for a solved x
+    files = helper.written_files()
+    assert set(files) == {"D2aa", "D2bb", "D2ab", "D2", "D1a", "D1b"}
+    r = RefProblem(n, 2, 1, "DQG", True, True, h=h, g=g)
+    _, full = r.write_rdms(helper.x, 0)
+    for name in ("D2aa", "D2bb", "D2ab"):
+        assert set(files[name]) <= {name, "length"}
+        assert files[name].get(name, b"") == full[name].get(name, b"")   # no core: active = full
+    assert files["D2"] == full["D2"] and files["D1a"] == full["D1a"]
