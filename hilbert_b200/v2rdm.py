@@ -632,6 +632,10 @@ class v2RDMHelper:
         Lagrangian that hilbert also builds then is not)."""
         o, p, x = self.options, self.problem, self.x
         out = {}
+        first = str(o.get("DERTYPE")).upper() == "FIRST"
+        if not (first or any(o.get(k) for k in ("TPDM_WRITE", "TPDM_WRITE_FULL", "TPDM_WRITE_SPIN_FREE",
+                                                "OPDM_WRITE_FULL", "WRITE_CHECKPOINT_FILE"))):
+            return out
         entries = p.rdm_entries(x)
         if o.get("TPDM_WRITE"):
             n = int(p.nmo)
@@ -645,7 +649,6 @@ class v2RDMHelper:
             out["D2"] = entries["D2"]
         if o.get("OPDM_WRITE_FULL"):
             out.update({k: entries[k] for k in ("D1a", "D1b")})
-        first = str(o.get("DERTYPE")).upper() == "FIRST"
         if first or o.get("WRITE_CHECKPOINT_FILE"):
             out["CHECKPOINT"] = {"MU": np.float64(p.get_mu()).tobytes(), "PRIMAL": x.tobytes(),
                                  "DUAL 1": p.get_y().tobytes(), "DUAL 2": p.get_z().tobytes()}
