@@ -49,3 +49,18 @@ def test_restart_reaches_the_uninterrupted_energy(cuda_device, tmp_path):
     # the restart continues rather than starting over
     assert st_rest["oiter"] < st_full["oiter"]
     q.close()
+
+
+def test_helper_writes_the_checkpoint_entries(cuda_device):
+    """WRITE_CHECKPOINT_FILE: the helper leaves MU, PRIMAL, DUAL 1 and DUAL 2
+    of its solve (v2rdm_solver.cc:1514-1516)."""
+    opts = {"HUBBARD_HAMILTONIAN": True, "N_HUBBARD_SITES": 4, "N_HUBBARD_SPINS": 4, "HUBBARD_U": 4.0,
+            "R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6, "MAXITER": 100000, "MU_UPDATE_FREQUENCY": 500,
+            "WRITE_CHECKPOINT_FILE": True}
+    helper = hb.v2RDMHelper(None, opts)
+    helper.compute_energy()
+    ck_entries = helper.files["CHECKPOINT"]
+    assert set(ck_entries) == {"MU", "PRIMAL", "DUAL 1", "DUAL 2"}
+    assert np.frombuffer(ck_entries["PRIMAL"], np.float64).tolist() == helper.x.tolist()
+    assert np.frombuffer(ck_entries["MU"], np.float64)[0] == helper.problem.get_mu()
+    assert len(np.frombuffer(ck_entries["DUAL 1"], np.float64)) == helper.problem.n_dual
