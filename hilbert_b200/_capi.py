@@ -47,7 +47,7 @@ EXPORTS = (
     "v2b_problem_pack_spatial_density", "v2b_project_block_noalloc",
     "v2b_problem_rdm_counts", "v2b_problem_rdm_records", "v2b_problem_set_state",
     "v2b_doci_v2rdm_layout", "v2b_batch_problem_create", "v2b_problem_palette",
-    "v2b_problem_tpdm_iwl_records",
+    "v2b_problem_tpdm_iwl_records", "v2b_problem_d3_counts", "v2b_problem_d3_records",
 )
 
 
@@ -140,6 +140,8 @@ def load(path=LIB_PATH):
         "v2b_batch_problem_create": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(vp)]),
         "v2b_problem_palette": (ctypes.c_int, [vp, ctypes.c_int, vp, ip]),
         "v2b_problem_tpdm_iwl_records": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp, vp]),
+        "v2b_problem_d3_counts": (ctypes.c_int, [vp, vp]),
+        "v2b_problem_d3_records": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp, vp, vp]),
         "v2b_problem_rdm_records": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp, vp, vp, vp, vp]),
         "v2b_problem_projection_profile": (ctypes.c_int, [vp, dp, lp, ctypes.c_int]),
         "v2b_problem_cg_profile": (ctypes.c_int, [vp, dp, ctypes.c_int]),

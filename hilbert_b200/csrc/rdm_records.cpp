@@ -5,6 +5,7 @@
 //   WriteTPDMSpinFree  src/v2rdm_casscf/write_tpdm.cc:312-519  (D2)
 //   WriteOPDM          src/v2rdm_casscf/write_opdm.cc:40-114   (D1a, D1b)
 //   WriteTPDM_IWL      src/v2rdm_casscf/write_tpdm_iwl.cc:45-205 (IWL labels)
+//   WriteActive3PDM    src/v2rdm_casscf/write_3pdm.cc:50-206   (D3aaa, D3aab, D3bba, D3bbb)
 // for C1 with ncore doubly occupied (restricted) orbitals numbered 0 ..
 // ncore-1 ahead of the active ones (active orbital i is ncore + i); and as
 // v2RDM-DOCI's WriteTPDM (src/v2rdm_doci/write_tpdm.cc:47-176) for a DOCI
@@ -196,6 +197,70 @@ void iwl_records(const Problem &p, const double *x, int ncore, TpdmRecord *aa_ou
                 bb.put(jf, i, i, lf, -vb);
                 ab.put(i, i, jf, lf, x[p.d1b + (int64_t)j * n + l]);
                 ab.put(jf, lf, i, i, x[p.d1a + (int64_t)j * n + l]);
+            }
+}
+
+void d3_counts(const Problem &p, int64_t *counts) {
+    check(p, 0);
+    if (p.spec.doci || !p.d3) throw std::invalid_argument("3-RDM records need the v2RDM D3 blocks (CONSTRAIN_D3)");
+    const int64_t n = p.n, distinct = n * (n - 1) * (n - 2), pair_first = n * n * (n - 1);
+    counts[0] = distinct * distinct;
+    counts[1] = pair_first * pair_first;
+}
+
+void d3_records(const Problem &p, const double *x, int ncore, Dm3Record *aaa, Dm3Record *aab,
+                Dm3Record *bba, Dm3Record *bbb) {
+    // every ordered triple (i, j, k) in the aba order, i n^2 + j n + k
+    // (basis.cc:640-727); the sign is the parity of the order within the
+    // alpha pair (aab) or the whole triple (aaa)
+    int64_t counts[2];
+    d3_counts(p, counts);
+    if (ncore < 0) throw std::invalid_argument("ncore must be >= 0");
+    const int n = p.n, c0 = ncore;
+    const int64_t taab = p.trip_aab, taaa = p.trip_aaa;
+    auto put = [](Dm3Record *r, int64_t k, int a, int b, int c, int d, int e, int f, double v) {
+        if (r) r[k] = Dm3Record{a, b, c, d, e, f, v};
+    };
+    int64_t q = 0;
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++)
+            for (int k = 0; k < n; k++) {
+                if (i == j) continue;
+                const int64_t ijk = p.ibas_aab[((int64_t)i * n + j) * n + k];
+                for (int l = 0; l < n; l++)
+                    for (int m = 0; m < n; m++)
+                        for (int o = 0; o < n; o++) {
+                            if (l == m) continue;
+                            const int64_t lmo = p.ibas_aab[((int64_t)l * n + m) * n + o];
+                            const int s = (i > j ? -1 : 1) * (l > m ? -1 : 1);
+                            put(aab, q, c0 + i, c0 + j, c0 + k, c0 + l, c0 + m, c0 + o, s * x[p.d3aab + ijk * taab + lmo]);
+                            put(bba, q, c0 + i, c0 + j, c0 + k, c0 + l, c0 + m, c0 + o, s * x[p.d3bba + ijk * taab + lmo]);
+                            q++;
+                        }
+            }
+    auto parity = [](int a, int b, int c) {
+        int s = 1;
+        if (a > b) s = -s;
+        if (a > c) s = -s;
+        if (b > c) s = -s;
+        return s;
+    };
+    q = 0;
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++)
+            for (int k = 0; k < n; k++) {
+                if (i == j || i == k || j == k) continue;
+                const int64_t ijk = p.ibas_aaa[((int64_t)i * n + j) * n + k];
+                for (int l = 0; l < n; l++)
+                    for (int m = 0; m < n; m++)
+                        for (int o = 0; o < n; o++) {
+                            if (l == m || l == o || m == o) continue;
+                            const int64_t lmo = p.ibas_aaa[((int64_t)l * n + m) * n + o];
+                            const int s = parity(i, j, k) * parity(l, m, o);
+                            put(aaa, q, c0 + i, c0 + j, c0 + k, c0 + l, c0 + m, c0 + o, s * x[p.d3aaa + ijk * taaa + lmo]);
+                            put(bbb, q, c0 + i, c0 + j, c0 + k, c0 + l, c0 + m, c0 + o, s * x[p.d3bbb + ijk * taaa + lmo]);
+                            q++;
+                        }
             }
 }
 

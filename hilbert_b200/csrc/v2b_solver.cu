@@ -1777,6 +1777,26 @@ int v2b_problem_tpdm_iwl_records(const v2b_problem *p, int ncore, const double *
         return V2B_OK;
     });
 }
+int v2b_problem_d3_counts(const v2b_problem *p, long *counts) {
+    return guarded([&] {
+        if (!p || !counts) throw std::invalid_argument("d3_counts: NULL argument");
+        int64_t c[2];
+        v2b::d3_counts(p->prob, c);
+        counts[0] = (long)c[0];
+        counts[1] = (long)c[1];
+        return V2B_OK;
+    });
+}
+int v2b_problem_d3_records(const v2b_problem *p, int ncore, const double *x, v2b_dm3_record *d3aaa,
+                           v2b_dm3_record *d3aab, v2b_dm3_record *d3bba, v2b_dm3_record *d3bbb) {
+    static_assert(sizeof(v2b_dm3_record) == sizeof(v2b::Dm3Record), "record layout");
+    return guarded([&] {
+        if (!p || !x) throw std::invalid_argument("d3_records: NULL argument");
+        v2b::d3_records(p->prob, x, ncore, (v2b::Dm3Record *)d3aaa, (v2b::Dm3Record *)d3aab,
+                        (v2b::Dm3Record *)d3bba, (v2b::Dm3Record *)d3bbb);
+        return V2B_OK;
+    });
+}
 int v2b_problem_pack_dims(const v2b_problem *p, long *d2_size, long *d1_size) {
     return guarded([&] {
         if (!p || !d2_size || !d1_size) throw std::invalid_argument("pack_dims: NULL argument");

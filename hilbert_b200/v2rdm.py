@@ -49,6 +49,7 @@ DEFAULTS = {
     "OPDM_WRITE_FULL": False,       # :286
     "TPDM_WRITE_SPIN_FREE": False,  # :289
     "TPDM_WRITE": False,            # :292
+    "3PDM_WRITE": False,            # :295
     "DERTYPE": "NONE",              # Psi4's global derivative option
 }
 
@@ -368,6 +369,26 @@ class V2RDMProblem:
                                                      out["D2ab"].ctypes.data, out["D2bb"].ctypes.data))
         return out
 
+    DM3_RECORD = np.dtype([("i", np.int32), ("j", np.int32), ("k", np.int32), ("l", np.int32),
+                           ("m", np.int32), ("n", np.int32), ("value", np.float64)])
+
+    def d3_entries(self, x, ncore=0):
+        """{"D3aaa", "D3aab", "D3bba", "D3bbb"}: {entry: bytes} as
+        WriteActive3PDM writes them (write_3pdm.cc:50-206): the records when
+        there are any, then "length"."""
+        xh = np.ascontiguousarray(x.detach().cpu().numpy() if hasattr(x, "detach") else x,
+                                  dtype=np.float64)
+        if xh.shape != (self.n_primal,):
+            raise ValueError(f"x must hold {self.n_primal} values")
+        counts = np.zeros(2, np.int64)
+        check(self._lib.v2b_problem_d3_counts(self._h, counts.ctypes.data))
+        rec = {name: np.zeros(int(counts[0 if name in ("D3aaa", "D3bbb") else 1]), self.DM3_RECORD)
+               for name in ("D3aaa", "D3aab", "D3bba", "D3bbb")}
+        check(self._lib.v2b_problem_d3_records(self._h, int(ncore), xh.ctypes.data,
+                                               *[rec[k].ctypes.data for k in ("D3aaa", "D3aab", "D3bba", "D3bbb")]))
+        return {name: ({name: r.tobytes()} if len(r) else {}) | {"length": np.int64(len(r)).tobytes()}
+                for name, r in rec.items()}
+
     def rdm_entries(self, x, ncore=0):
         """{file: {entry: bytes}}: every entry hilbert's writers put in their
         PSIO files, byte for byte (the records when there are any, "length",
@@ -626,7 +647,8 @@ class v2RDMHelper:
         write options (v2rdm_solver.cc:1474-1516), {file: {entry: bytes}}:
         TPDM_WRITE (WriteActiveTPDM, write_tpdm.cc:521-602: the active records
         and "length"), TPDM_WRITE_FULL (WriteTPDM), TPDM_WRITE_SPIN_FREE,
-        OPDM_WRITE_FULL; with DERTYPE FIRST or WRITE_CHECKPOINT_FILE the
+        OPDM_WRITE_FULL, 3PDM_WRITE with CONSTRAIN_D3 (WriteActive3PDM,
+        write_3pdm.cc:50-206); with DERTYPE FIRST or WRITE_CHECKPOINT_FILE the
         checkpoint ("CHECKPOINT", entries as in hilbert_b200.checkpoint), and
         with DERTYPE FIRST the IWL 2-RDM records ("IWL"; the orbital
         Lagrangian that hilbert also builds then is not)."""
@@ -634,7 +656,7 @@ class v2RDMHelper:
         out = {}
         first = str(o.get("DERTYPE")).upper() == "FIRST"
         if not (first or any(o.get(k) for k in ("TPDM_WRITE", "TPDM_WRITE_FULL", "TPDM_WRITE_SPIN_FREE",
-                                                "OPDM_WRITE_FULL", "WRITE_CHECKPOINT_FILE"))):
+                                                "OPDM_WRITE_FULL", "WRITE_CHECKPOINT_FILE", "3PDM_WRITE"))):
             return out
         entries = p.rdm_entries(x)
         if o.get("TPDM_WRITE"):
@@ -649,6 +671,8 @@ class v2RDMHelper:
             out["D2"] = entries["D2"]
         if o.get("OPDM_WRITE_FULL"):
             out.update({k: entries[k] for k in ("D1a", "D1b")})
+        if o.get("3PDM_WRITE") and o.get("CONSTRAIN_D3"):
+            out.update(p.d3_entries(x))
         if first or o.get("WRITE_CHECKPOINT_FILE"):
             out["CHECKPOINT"] = {"MU": np.float64(p.get_mu()).tobytes(), "PRIMAL": x.tobytes(),
                                  "DUAL 1": p.get_y().tobytes(), "DUAL 2": p.get_z().tobytes()}

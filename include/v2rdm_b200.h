@@ -294,6 +294,18 @@ int v2b_problem_rdm_records(const v2b_problem *p, int ncore, const double *x, v2
  * cutoff, 1e-14; that filtering is the IWL writer's.  v2RDM problems only. */
 int v2b_problem_tpdm_iwl_records(const v2b_problem *p, int ncore, const double *x, v2b_tpdm_record *d2aa,
                                  v2b_tpdm_record *d2ab, v2b_tpdm_record *d2bb);
+/* The 3-RDM records of WriteActive3PDM (src/v2rdm_casscf/write_3pdm.cc:50-206;
+ * 3PDM_WRITE with CONSTRAIN_D3), files D3aaa, D3aab, D3bba, D3bbb, layout
+ * struct dm3 (:39-47), orbitals numbered as in v2b_problem_rdm_records.
+ * counts[0]: records in D3aaa and in D3bbb; counts[1]: in D3aab and D3bba.
+ * Problems with the D3 blocks only. */
+typedef struct {
+    int i, j, k, l, m, n;
+    double value;
+} v2b_dm3_record;
+int v2b_problem_d3_counts(const v2b_problem *p, long *counts);
+int v2b_problem_d3_records(const v2b_problem *p, int ncore, const double *x, v2b_dm3_record *d3aaa,
+                           v2b_dm3_record *d3aab, v2b_dm3_record *d3bba, v2b_dm3_record *d3bbb);
 
 /* ---- 3. allocation-free projection ------------------------------------------ */
 

@@ -63,7 +63,7 @@ done
 CXX="${CXX:-g++}"
 FLAGS=(-std=c++17 -O2 -fPIC -ffp-contract=off -w
        -I"$here/ref_shim" -I"$src" -I"$ref/src")
-units=(basis d2 spin q2 g2 t1 t2 d3 d4 e3 f3 q3 tei write_opdm)
+units=(basis d2 spin q2 g2 t1 t2 d3 d4 e3 f3 q3 tei write_opdm write_3pdm)
 objs=()
 for u in "${units[@]}"; do
   "$CXX" "${FLAGS[@]}" -c "$src/$u.cc" -o "$out/$u.o"

@@ -252,10 +252,13 @@ class RefProblem:
         return d2, d1
 
     # PSIO units and entries of hilbert's RDM writers (misc/hilbert_psifiles.h:33-42)
-    RDM_UNITS = {"D2aa": 270, "D2ab": 271, "D2bb": 272, "D1a": 277, "D1b": 278, "D2": 279}
+    RDM_UNITS = {"D2aa": 270, "D2ab": 271, "D2bb": 272, "D1a": 277, "D1b": 278, "D2": 279,
+                 "D3aaa": 273, "D3aab": 274, "D3bba": 275, "D3bbb": 276}
     TPDM = np.dtype([("i", np.int32), ("j", np.int32), ("k", np.int32), ("l", np.int32),
                      ("value", np.float64)])
     OPDM = np.dtype([("i", np.int32), ("j", np.int32), ("value", np.float64)])
+    DM3 = np.dtype([("i", np.int32), ("j", np.int32), ("k", np.int32), ("l", np.int32),
+                    ("m", np.int32), ("n", np.int32), ("value", np.float64)])
 
     def write_rdms(self, x, ncore=0):
         """Runs the reference's WriteTPDM, WriteTPDMSpinFree, WriteOPDM and
@@ -279,8 +282,12 @@ class RefProblem:
                 buf = ctypes.create_string_buffer(max(size, 1))
                 lib.v2b_ref_psio_entry(unit, key.encode(), buf)
                 entries[name][key] = buf.raw[:size]
+            if not entries[name]:   # a file this problem's writers do not write
+                del entries[name]
+                continue
             raw = entries[name].get(name, b"")
-            records[name] = np.frombuffer(raw, self.TPDM if name.startswith("D2") else self.OPDM).copy()
+            dt = self.TPDM if name.startswith("D2") else self.DM3 if name.startswith("D3") else self.OPDM
+            records[name] = np.frombuffer(raw, dt).copy()
         return records, entries
 
     def iwl_records(self):

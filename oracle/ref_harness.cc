@@ -151,6 +151,7 @@ class RefProblem : public v2RDMSolver {
         WriteTPDMSpinFree();
         WriteOPDM();
         WriteTPDM_IWL();   // write_tpdm_iwl.cc:45-205, into the IWL stand-in
+        if (constrain_d3_) WriteActive3PDM();   // write_3pdm.cc:50-206
         rstcpi_[0] = saved_rst;
         nrstc_ = saved_nrst;
         pitzer_offset_full[0] = saved_off;

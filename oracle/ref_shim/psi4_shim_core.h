@@ -168,6 +168,11 @@ inline double C_DDOT(size_t n, double *x, int incx, double *y, int incy) {
     for (size_t i = 0; i < n; i++) s += x[i * incx] * y[i * incy];
     return s;
 }
+inline double C_DNRM2(size_t n, double *x, int incx) {
+    double s = 0.0;
+    for (size_t i = 0; i < n; i++) s += x[i * incx] * x[i * incx];
+    return std::sqrt(s);
+}
 inline void C_DSCAL(size_t n, double a, double *x, int incx) {
     for (size_t i = 0; i < n; i++) x[i * incx] *= a;
 }

@@ -113,3 +113,22 @@ def test_helper_write_options_select_the_reference_files():
         assert set(files[name]) <= {name, "length"}
         assert files[name].get(name, b"") == full[name].get(name, b"")   # no core: active = full
     assert files["D2"] == full["D2"] and files["D1a"] == full["D1a"]
+
+
+@pytest.mark.parametrize("ncore", [0, 2])
+def test_d3_entries_match_the_reference_3pdm_writer(ncore):
+    """WriteActive3PDM's D3aaa, D3aab, D3bba and D3bbb files, byte for byte."""
+    from oracle.maps import RefProblem
+    rng = np.random.default_rng(41 + ncore)
+    for n, na, nb in [(3, 2, 1), (4, 2, 2), (4, 3, 1), (2, 1, 1), (5, 2, 2)]:
+        r = RefProblem(n, na, nb, "DQG+D3", True, True, h=rng.standard_normal((n, n)),
+                       g=rng.standard_normal((n,) * 4))
+        x = rng.standard_normal(r.n_primal)
+        _, ref_entries = r.write_rdms(x, ncore)
+        p = hb.V2RDMProblem(n, na, nb, "DQG+D3")
+        mine = p.d3_entries(x, ncore)
+        for name, entries in mine.items():
+            assert entries == ref_entries[name], (n, na, nb, ncore, name)
+        p.close()
+    with pytest.raises(hb.V2BError):
+        hb.V2RDMProblem(3, 1, 1, "DQG").d3_entries(np.zeros(hb.V2RDMProblem(3, 1, 1, "DQG").n_primal))
