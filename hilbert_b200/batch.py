@@ -157,7 +157,7 @@ def solve_in_one_launch(instances, options=None, device=None):
 
 
 def solve_batch(instances, options=None, rank=0, world=1, group=None, solve=solve_on_device,
-                concurrency=1):
+                concurrency=1, one_launch=False, solve_slice=solve_in_one_launch):
     """Solve this rank's slice, then gather every rank's results on the host
     (torch.distributed.all_gather_object over `group`, which should be a
     gloo group when the default one is NCCL).  Returns the results of all
@@ -167,7 +167,11 @@ def solve_batch(instances, options=None, rank=0, world=1, group=None, solve=solv
     host threads: every problem runs on its own CUDA stream and the library
     calls release the GIL, so small instances can share the GPU.  A new
     thread starts on CUDA device 0, so each worker first takes the caller's
-    current device."""
+    current device.
+
+    one_launch=True solves the whole slice together instead, with
+    solve_slice(instances, options) (default solve_in_one_launch: one
+    block-diagonal problem per palette group, every launch covering them)."""
     if options is None:
         options = Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6, "MAXITER": 400000,
                            "MU_UPDATE_FREQUENCY": 500})
@@ -181,7 +185,14 @@ def solve_batch(instances, options=None, rank=0, world=1, group=None, solve=solv
         r.update(index=k, rank=rank)
         return r
 
-    if concurrency > 1 and len(mine) > 1:
+    if one_launch:
+        results = []
+        if mine:
+            for k, r in zip(mine, solve_slice([by_index[k] for k in mine], options)):
+                r = dict(r)
+                r.update(index=k, rank=rank)
+                results.append(r)
+    elif concurrency > 1 and len(mine) > 1:
         from concurrent.futures import ThreadPoolExecutor
         init = None
         import torch

@@ -50,24 +50,26 @@ def _fake_solve(inst, options):
             "iiter": inst.electrons}
 
 
-def _rank_main(rank, world, port, out_dir):
+def _rank_main(rank, world, port, out_dir, one_launch=False):
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        res = solve_batch(hubbard_batch(), rank=rank, world=world, solve=_fake_solve)
+        res = solve_batch(hubbard_batch(), rank=rank, world=world, solve=_fake_solve,
+                          one_launch=one_launch, solve_slice=_fake_slice)
         np.save(os.path.join(out_dir, f"rank{rank}.npy"),
                 np.array([(r["index"], r["rank"], r["energy"], r["oiter"]) for r in res]))
     finally:
         dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_gather_every_result(tmp_path):
+@pytest.mark.parametrize("one_launch", [False, True])
+def test_two_gloo_ranks_gather_every_result(tmp_path, one_launch):
     torch = pytest.importorskip("torch")
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         port = s.getsockname()[1]
-    torch.multiprocessing.spawn(_rank_main, args=(2, port, str(tmp_path)), nprocs=2, join=True)
+    torch.multiprocessing.spawn(_rank_main, args=(2, port, str(tmp_path), one_launch), nprocs=2, join=True)
     r0, r1 = (np.load(tmp_path / f"rank{k}.npy") for k in (0, 1))
     assert np.array_equal(r0, r1)
     batch = hubbard_batch()
@@ -92,3 +94,22 @@ def test_concurrent_slice_gives_the_same_results():
     a = solve_batch(batch, solve=_fake_solve)
     b = solve_batch(batch, solve=solve, concurrency=4)
     assert a == b and [r["index"] for r in b] == list(range(12))
+
+
+
+def _fake_slice(insts, options):
+    return [_fake_solve(i, options) for i in insts]
+
+
+def test_one_launch_slice_gives_the_same_results():
+    """one_launch=True hands the rank's whole slice to one slice solver and
+    keeps the per-instance results and their order."""
+    calls = []
+
+    def solve_slice(insts, options):
+        calls.append(len(insts))
+        return _fake_slice(insts, options)
+
+    batch = hubbard_batch(count=12)
+    assert solve_batch(batch, one_launch=True, solve_slice=solve_slice) == solve_batch(batch, solve=_fake_solve)
+    assert calls == [12]
