@@ -1,5 +1,5 @@
-"""torch.ops.v2rdm.{Au, ATu, solve}: the device maps and the device solve as
-PyTorch operators on CUDA float64 tensors.
+"""torch.ops.v2rdm.{Au, ATu, solve, doci_Au, doci_ATu}: the device maps and
+the device solve as PyTorch operators on CUDA float64 tensors.
 
 A problem is named by the arguments hilbert builds its tables from (nmo,
 nalpha, nbeta, POSITIVITY, CONSTRAIN_SPIN, CONSTRAIN_SZ and the Hubbard
@@ -14,7 +14,7 @@ import threading
 
 import torch
 
-from .v2rdm import Options, V2RDMProblem
+from .v2rdm import DOCIProblem, Options, V2RDMProblem
 
 _lock = threading.Lock()
 _problems = {}
@@ -31,6 +31,18 @@ def problem(nmo, nalpha, nbeta, positivity="DQG", constrain_spin=True, constrain
         if p is None:
             p = V2RDMProblem(key[0], key[1], key[2], key[3], key[4], key[5],
                              hubbard_multiplicity=key[6])
+            _problems[key] = p
+    return p
+
+
+def doci_problem(nmo, nalpha, nbeta, positivity="DQG", device=None):
+    """The cached DOCIProblem for these arguments on this CUDA device."""
+    dev = torch.cuda.current_device() if device is None else int(device)
+    key = ("doci", int(nmo), int(nalpha), int(nbeta), str(positivity), dev)
+    with _lock:
+        p = _problems.get(key)
+        if p is None:
+            p = DOCIProblem(key[1], key[2], key[3], key[4])
             _problems[key] = p
     return p
 
@@ -109,6 +121,38 @@ def _(x0, b, c, *args):
     return torch.empty_like(x0)
 
 
+@torch.library.custom_op("v2rdm::doci_Au", mutates_args=(), device_types="cuda")
+def doci_Au(x: torch.Tensor, nmo: int, nalpha: int, nbeta: int, positivity: str) -> torch.Tensor:
+    """A x of v2RDM-DOCI: hilbert's DOCI bpsdp_Au (v2rdm_doci_solver.cc:1509-1537)"""
+    with torch.cuda.device(x.device):
+        return doci_problem(nmo, nalpha, nbeta, positivity, x.device.index).Au(x.contiguous())
+
+
+@torch.library.custom_op("v2rdm::doci_ATu", mutates_args=(), device_types="cuda")
+def doci_ATu(y: torch.Tensor, nmo: int, nalpha: int, nbeta: int, positivity: str) -> torch.Tensor:
+    """A^T y of v2RDM-DOCI: hilbert's DOCI bpsdp_ATu (v2rdm_doci_solver.cc:1539-1566)"""
+    with torch.cuda.device(y.device):
+        return doci_problem(nmo, nalpha, nbeta, positivity, y.device.index).ATu(y.contiguous())
+
+
+def _doci_sizes(nmo, nalpha, nbeta, positivity):
+    p = DOCIProblem(nmo, nalpha, nbeta, positivity)   # host tables only
+    try:
+        return p.n_primal, p.n_dual
+    finally:
+        p.close()
+
+
+@doci_Au.register_fake
+def _(x, nmo, nalpha, nbeta, positivity):
+    return x.new_empty(_doci_sizes(nmo, nalpha, nbeta, positivity)[1])
+
+
+@doci_ATu.register_fake
+def _(y, nmo, nalpha, nbeta, positivity):
+    return y.new_empty(_doci_sizes(nmo, nalpha, nbeta, positivity)[0])
+
+
 def _setup(ctx, inputs, output):
     ctx.spec = inputs[1:]
 
@@ -123,3 +167,15 @@ def _ATu_backward(ctx, grad):
 
 Au.register_autograd(_Au_backward, setup_context=_setup)
 ATu.register_autograd(_ATu_backward, setup_context=_setup)
+
+
+def _doci_Au_backward(ctx, grad):
+    return (torch.ops.v2rdm.doci_ATu(grad.contiguous(), *ctx.spec),) + (None,) * len(ctx.spec)
+
+
+def _doci_ATu_backward(ctx, grad):
+    return (torch.ops.v2rdm.doci_Au(grad.contiguous(), *ctx.spec),) + (None,) * len(ctx.spec)
+
+
+doci_Au.register_autograd(_doci_Au_backward, setup_context=_setup)
+doci_ATu.register_autograd(_doci_ATu_backward, setup_context=_setup)

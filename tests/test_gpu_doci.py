@@ -109,3 +109,20 @@ def test_doci_helper_optimises_orbitals_from_4_index_integrals(cuda_device):
     e_g = hb.v2RDM_DOCIHelper(npair, npair, n, h_mo, g, opts).compute_energy(macro_iterations=2)
     e_b = hb.v2RDM_DOCIHelper(npair, npair, n, h_mo, None, opts, B=B_mo).compute_energy(macro_iterations=2)
     assert abs(e_g - e_b) <= 1e-5
+
+
+def test_doci_torch_ops_and_their_adjoint(cuda_device):
+    """torch.ops.v2rdm.doci_Au equals the device map, and autograd through it
+    gives doci_ATu (d<A x, w>/dx = A^T w)."""
+    import torch
+    import hilbert_b200.torch_ops  # noqa: F401  (registers the operators)
+    spec = (4, 2, 2, "DQG+D3")
+    p = hb.DOCIProblem(*spec)
+    rng = np.random.default_rng(9)
+    x = torch.from_numpy(rng.standard_normal(p.n_primal)).to(cuda_device).requires_grad_(True)
+    w = torch.from_numpy(rng.standard_normal(p.n_dual)).to(cuda_device)
+    ax = torch.ops.v2rdm.doci_Au(x, *spec)
+    assert torch.equal(ax.detach(), p.Au(x.detach()))
+    (ax * w).sum().backward()
+    assert torch.equal(x.grad, p.ATu(w))
+    p.close()

@@ -39,3 +39,13 @@ def test_clear_releases_cached_problems():
     torch_ops._problems[("test",)] = p
     torch_ops.clear()
     assert not torch_ops._problems and p._h is None
+
+
+def test_doci_operators_shapes_and_no_cpu_fallback():
+    p = hb.DOCIProblem(4, 2, 2, "DQG+D3")
+    x = torch.empty(p.n_primal, dtype=torch.float64, device="meta")
+    y = torch.empty(p.n_dual, dtype=torch.float64, device="meta")
+    assert torch.ops.v2rdm.doci_Au(x, 4, 2, 2, "DQG+D3").shape == (p.n_dual,)
+    assert torch.ops.v2rdm.doci_ATu(y, 4, 2, 2, "DQG+D3").shape == (p.n_primal,)
+    with pytest.raises((NotImplementedError, RuntimeError)):
+        torch.ops.v2rdm.doci_Au(torch.zeros(p.n_primal, dtype=torch.float64), 4, 2, 2, "DQG+D3")
