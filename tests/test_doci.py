@@ -304,3 +304,22 @@ def test_doci_helper_builds_the_problem_its_options_name():
     if not torch.cuda.is_available():
         with pytest.raises(_capi.V2BError):
             helper.compute_energy()
+
+
+@needs_ref
+def test_doci_one_orbital_edge_cases():
+    """n = 1 (no pairs: Q2s2, G2s2 and the T2 3x3 blocks are empty), zero and
+    one pair, against the reference; the oracle and the product agree."""
+    rng = np.random.default_rng(13)
+    for pos, na in itertools.product(["D", "DQ", "DG", "DQG", "DQGT2"], [0, 1]):
+        h, g = symmetric_integrals(rng, 1)
+        r = DociRef(1, na, na, pos, h=h, g=g)
+        o, p = DociOracle(1, na, na, pos), product(1, na, na, pos)
+        assert list(p.dims) == list(r.dims) and np.array_equal(o.dims, r.dims)
+        assert np.array_equal(p.b(), r.b) and np.array_equal(o.b(), r.b)
+        assert np.array_equal(p.c_external(h, g), r.c) and np.array_equal(o.c(h, g), r.c)
+        x, y = rng.standard_normal(r.n_primal), rng.standard_normal(r.n_dual)
+        assert np.array_equal(packed_apply(*operator(p, False), x), r.Au(x))
+        assert np.array_equal(packed_apply(*operator(p, True), y), r.ATu(y))
+        assert np.array_equal(o.Au(x), r.Au(x)) and np.array_equal(o.ATu(y), r.ATu(y))
+        p.close()
