@@ -586,6 +586,13 @@ class BPSDPSolver:
         return self._lib.v2b_bpsdp_oiter_total(self._h)
 
 
+def _check_sdp_solver(options):
+    # SDP_SOLVER (plugin.cc:246): hilbert offers libsdp's BPSDP and RRSDP
+    # (v2rdm_solver.cc:424-447); only the boundary-point method is built here
+    if str(options.get("SDP_SOLVER")).upper() != "BPSDP":
+        raise NotImplementedError(f"SDP_SOLVER {options.get('SDP_SOLVER')}: only BPSDP is on the device path")
+
+
 class v2RDMHelper:
     """hilbert.v2RDMHelper (src/python_api/python_helpers.cc:104-113, 357-371).
 
@@ -616,6 +623,7 @@ class v2RDMHelper:
         else:
             raise TypeError("v2RDMHelper(nalpha, nbeta, nmo, h, g, options) or v2RDMHelper(ref_wfn, options)")
         o = self.options
+        _check_sdp_solver(o)
         pos = (o.get("POSITIVITY") + ("+D3" if o.get("CONSTRAIN_D3") else "")
                + ("+Q3" if o.get("CONSTRAIN_Q3") else "") + ("+E3" if o.get("CONSTRAIN_E3") else "")
                + ("+F3" if o.get("CONSTRAIN_F3") else "") + ("+D4" if o.get("CONSTRAIN_D4") else ""))
@@ -706,6 +714,7 @@ class v2RDM_DOCIHelper:
     def __init__(self, nalpha, nbeta, nmo, h, g, options, B=None):
         self.options = options if isinstance(options, Options) else Options(options)
         o = self.options
+        _check_sdp_solver(o)
         pos = o.get("POSITIVITY") + ("+D3" if o.get("CONSTRAIN_D3") else "")
         self.problem = DOCIProblem(nmo, nalpha, nbeta, pos)
         self.h = np.ascontiguousarray(h, dtype=np.float64).reshape(nmo, nmo)

@@ -253,3 +253,15 @@ def test_packed_A_and_AT_are_exact_transposes(kind, n, pos):
     diff.eliminate_zeros()
     assert diff.nnz == 0
     p.close()
+
+
+def test_helpers_refuse_other_sdp_solvers():
+    """SDP_SOLVER RRSDP is hilbert's other libsdp solver; it is not built, so
+    asking for it is an error, not a BPSDP solve."""
+    n = 2
+    h, g = np.eye(n), np.zeros((n,) * 4)
+    with pytest.raises(NotImplementedError):
+        hb.v2RDMHelper(1, 1, n, h.ravel(), g.ravel(), {"SDP_SOLVER": "RRSDP"})
+    with pytest.raises(NotImplementedError):
+        hb.v2RDM_DOCIHelper(1, 1, n, h, g, {"SDP_SOLVER": "RRSDP"})
+    hb.v2RDMHelper(1, 1, n, h.ravel(), g.ravel(), {"SDP_SOLVER": "BPSDP"})
