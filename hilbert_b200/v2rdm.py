@@ -50,6 +50,7 @@ DEFAULTS = {
     "TPDM_WRITE_SPIN_FREE": False,  # :289
     "TPDM_WRITE": False,            # :292
     "3PDM_WRITE": False,            # :295
+    "RESTART_FROM_CHECKPOINT_FILE": "",   # :185
     "DERTYPE": "NONE",              # Psi4's global derivative option
 }
 
@@ -624,6 +625,11 @@ class v2RDMHelper:
             raise TypeError("v2RDMHelper(nalpha, nbeta, nmo, h, g, options) or v2RDMHelper(ref_wfn, options)")
         o = self.options
         _check_sdp_solver(o)
+        if o.get("RESTART_FROM_CHECKPOINT_FILE"):
+            # v2rdm_solver.cc:958-959, 1081-1082
+            kind = "Hubbard" if self._hubbard else "external"
+            raise ValueError(f"RESTART_FROM_CHECKPOINT_FILE is incompatible with {kind} Hamiltonian "
+                             "(restart a problem with hilbert_b200.checkpoint.restart)")
         pos = (o.get("POSITIVITY") + ("+D3" if o.get("CONSTRAIN_D3") else "")
                + ("+Q3" if o.get("CONSTRAIN_Q3") else "") + ("+E3" if o.get("CONSTRAIN_E3") else "")
                + ("+F3" if o.get("CONSTRAIN_F3") else "") + ("+D4" if o.get("CONSTRAIN_D4") else ""))

@@ -265,3 +265,12 @@ def test_helpers_refuse_other_sdp_solvers():
     with pytest.raises(NotImplementedError):
         hb.v2RDM_DOCIHelper(1, 1, n, h, g, {"SDP_SOLVER": "RRSDP"})
     hb.v2RDMHelper(1, 1, n, h.ravel(), g.ravel(), {"SDP_SOLVER": "BPSDP"})
+
+
+def test_helper_refuses_restart_files_as_the_reference_does():
+    """RESTART_FROM_CHECKPOINT_FILE is an error for Hubbard and external
+    Hamiltonians in hilbert (v2rdm_solver.cc:958-959, 1081-1082)."""
+    with pytest.raises(ValueError, match="Hubbard"):
+        hb.v2RDMHelper(None, {"HUBBARD_HAMILTONIAN": True, "RESTART_FROM_CHECKPOINT_FILE": "ck"})
+    with pytest.raises(ValueError, match="external"):
+        hb.v2RDMHelper(1, 1, 2, np.eye(2).ravel(), np.zeros(16), {"RESTART_FROM_CHECKPOINT_FILE": "ck"})
