@@ -51,6 +51,7 @@ DEFAULTS = {
     "TPDM_WRITE": False,            # :292
     "3PDM_WRITE": False,            # :295
     "RESTART_FROM_CHECKPOINT_FILE": "",   # :185
+    "GPC_CONSTRAINTS": "NONE",      # :223
     "DERTYPE": "NONE",              # Psi4's global derivative option
 }
 
@@ -587,11 +588,14 @@ class BPSDPSolver:
         return self._lib.v2b_bpsdp_oiter_total(self._h)
 
 
-def _check_sdp_solver(options):
+def _check_unbuilt_options(options):
     # SDP_SOLVER (plugin.cc:246): hilbert offers libsdp's BPSDP and RRSDP
     # (v2rdm_solver.cc:424-447); only the boundary-point method is built here
     if str(options.get("SDP_SOLVER")).upper() != "BPSDP":
         raise NotImplementedError(f"SDP_SOLVER {options.get('SDP_SOLVER')}: only BPSDP is on the device path")
+    # the generalized Pauli constraints (generalized_pauli*.cc) are not built
+    if str(options.get("GPC_CONSTRAINTS")).upper() != "NONE":
+        raise NotImplementedError(f"GPC_CONSTRAINTS {options.get('GPC_CONSTRAINTS')}: not on the device path")
 
 
 class v2RDMHelper:
@@ -624,7 +628,7 @@ class v2RDMHelper:
         else:
             raise TypeError("v2RDMHelper(nalpha, nbeta, nmo, h, g, options) or v2RDMHelper(ref_wfn, options)")
         o = self.options
-        _check_sdp_solver(o)
+        _check_unbuilt_options(o)
         if o.get("RESTART_FROM_CHECKPOINT_FILE"):
             # v2rdm_solver.cc:958-959, 1081-1082
             kind = "Hubbard" if self._hubbard else "external"
@@ -720,7 +724,7 @@ class v2RDM_DOCIHelper:
     def __init__(self, nalpha, nbeta, nmo, h, g, options, B=None):
         self.options = options if isinstance(options, Options) else Options(options)
         o = self.options
-        _check_sdp_solver(o)
+        _check_unbuilt_options(o)
         pos = o.get("POSITIVITY") + ("+D3" if o.get("CONSTRAIN_D3") else "")
         self.problem = DOCIProblem(nmo, nalpha, nbeta, pos)
         self.h = np.ascontiguousarray(h, dtype=np.float64).reshape(nmo, nmo)

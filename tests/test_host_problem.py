@@ -264,7 +264,9 @@ def test_helpers_refuse_other_sdp_solvers():
         hb.v2RDMHelper(1, 1, n, h.ravel(), g.ravel(), {"SDP_SOLVER": "RRSDP"})
     with pytest.raises(NotImplementedError):
         hb.v2RDM_DOCIHelper(1, 1, n, h, g, {"SDP_SOLVER": "RRSDP"})
-    hb.v2RDMHelper(1, 1, n, h.ravel(), g.ravel(), {"SDP_SOLVER": "BPSDP"})
+    with pytest.raises(NotImplementedError):
+        hb.v2RDMHelper(1, 1, n, h.ravel(), g.ravel(), {"GPC_CONSTRAINTS": "1RDM"})
+    hb.v2RDMHelper(1, 1, n, h.ravel(), g.ravel(), {"SDP_SOLVER": "BPSDP", "GPC_CONSTRAINTS": "NONE"})
 
 
 def test_helper_refuses_restart_files_as_the_reference_does():
