@@ -649,10 +649,20 @@ class v2RDMHelper:
         self.stats = None
         self.variables = {}
 
+    def _sdp_options(self):
+        # hilbert's solve(maxiter) length, and so the mu period, is
+        # ORBOPT_FREQUENCY whenever OPTIMIZE_ORBITALS is set, even for the
+        # Hubbard and external Hamiltonians that skip the orbital step
+        # (v2rdm_solver.cc:1298, 1342)
+        o = Options({k: v for k, v in self.options._v.items()})
+        if o.get("OPTIMIZE_ORBITALS"):
+            o.set("MU_UPDATE_FREQUENCY", int(o.get("ORBOPT_FREQUENCY")))
+        return o
+
     def compute_energy(self, monitor=None):
         p = self.problem
         x0 = p.guess(self.options.get("TPDM_GUESS"))
-        self.x, self.stats = p.solve(x0, self.b, self.c, self.options, monitor)
+        self.x, self.stats = p.solve(x0, self.b, self.c, self._sdp_options(), monitor)
         e = float(self.c @ self.x)
         # enuc = efzc = 0 for Hubbard / external Hamiltonians (v2rdm_solver.cc:851-853, 972-974)
         self.variables["CURRENT ENERGY"] = e

@@ -276,3 +276,14 @@ def test_helper_refuses_restart_files_as_the_reference_does():
         hb.v2RDMHelper(None, {"HUBBARD_HAMILTONIAN": True, "RESTART_FROM_CHECKPOINT_FILE": "ck"})
     with pytest.raises(ValueError, match="external"):
         hb.v2RDMHelper(1, 1, 2, np.eye(2).ravel(), np.zeros(16), {"RESTART_FROM_CHECKPOINT_FILE": "ck"})
+
+
+def test_helper_mu_period_follows_the_reference():
+    """hilbert solves in calls of ORBOPT_FREQUENCY iterations when
+    OPTIMIZE_ORBITALS is set (its default), of MU_UPDATE_FREQUENCY otherwise
+    (v2rdm_solver.cc:1298)."""
+    h, g = np.eye(2).ravel(), np.zeros(16)
+    default = hb.v2RDMHelper(1, 1, 2, h, g, {})
+    assert default._sdp_options().get("MU_UPDATE_FREQUENCY") == 500   # ORBOPT_FREQUENCY
+    fixed = hb.v2RDMHelper(1, 1, 2, h, g, {"OPTIMIZE_ORBITALS": False, "MU_UPDATE_FREQUENCY": 700})
+    assert fixed._sdp_options().get("MU_UPDATE_FREQUENCY") == 700
