@@ -650,14 +650,10 @@ class v2RDMHelper:
         self.variables = {}
 
     def _sdp_options(self):
-        # hilbert's solve(maxiter) length, and so the mu period, is
-        # ORBOPT_FREQUENCY whenever OPTIMIZE_ORBITALS is set, even for the
-        # Hubbard and external Hamiltonians that skip the orbital step
-        # (v2rdm_solver.cc:1298, 1342)
-        o = Options({k: v for k, v in self.options._v.items()})
-        if o.get("OPTIMIZE_ORBITALS"):
-            o.set("MU_UPDATE_FREQUENCY", int(o.get("ORBOPT_FREQUENCY")))
-        return o
+        # hilbert solves in calls of MU_UPDATE_FREQUENCY iterations for the
+        # Hubbard and external Hamiltonians, whatever OPTIMIZE_ORBITALS says
+        # (v2rdm_solver.cc:1298-1301)
+        return self.options
 
     def compute_energy(self, monitor=None):
         p = self.problem

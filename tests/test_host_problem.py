@@ -279,11 +279,13 @@ def test_helper_refuses_restart_files_as_the_reference_does():
 
 
 def test_helper_mu_period_follows_the_reference():
-    """hilbert solves in calls of ORBOPT_FREQUENCY iterations when
-    OPTIMIZE_ORBITALS is set (its default), of MU_UPDATE_FREQUENCY otherwise
-    (v2rdm_solver.cc:1298)."""
+    """For Hubbard and external Hamiltonians hilbert solves in calls of
+    MU_UPDATE_FREQUENCY iterations even when OPTIMIZE_ORBITALS asks for
+    ORBOPT_FREQUENCY (v2rdm_solver.cc:1298-1301); v2RDM-DOCI always uses
+    ORBOPT_FREQUENCY (v2rdm_doci_solver.cc:1116)."""
     h, g = np.eye(2).ravel(), np.zeros(16)
-    default = hb.v2RDMHelper(1, 1, 2, h, g, {})
-    assert default._sdp_options().get("MU_UPDATE_FREQUENCY") == 500   # ORBOPT_FREQUENCY
-    fixed = hb.v2RDMHelper(1, 1, 2, h, g, {"OPTIMIZE_ORBITALS": False, "MU_UPDATE_FREQUENCY": 700})
-    assert fixed._sdp_options().get("MU_UPDATE_FREQUENCY") == 700
+    for orbopt in (True, False):
+        helper = hb.v2RDMHelper(1, 1, 2, h, g, {"OPTIMIZE_ORBITALS": orbopt, "MU_UPDATE_FREQUENCY": 700})
+        assert helper._sdp_options().get("MU_UPDATE_FREQUENCY") == 700
+    doci = hb.v2RDM_DOCIHelper(1, 1, 2, np.eye(2), np.zeros((2,) * 4), {"MU_UPDATE_FREQUENCY": 700})
+    assert doci._sdp_options().get("MU_UPDATE_FREQUENCY") == 500
