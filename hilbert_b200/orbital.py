@@ -393,14 +393,18 @@ def active_space(h, B, ncore, nact):
 
 
 def casscf(h, B, ncore, nact, solve_active, macro_iterations=8, active_active=False,
-           orbital_step="lbfgs"):
+           orbital_step="lbfgs", g_conv=None, e_conv=None):
     """v2RDM-CASSCF macro-iterations: solve the active-space v2RDM in the
     current orbitals (solve_active(h_act, g_act) -> (E_active, packed d2,
     packed d1) on the same device as h), optimise the orbitals at those
     densities, rotate h and B, repeat.  orbital_step: "lbfgs"
     (optimize_orbitals) or "focas" (optimize_orbitals_focas with focas's
-    defaults).  Returns the energies after each SDP
-    solve and the orbital-gradient norms at each orbital step."""
+    defaults).  With g_conv and e_conv (ORBOPT_GRADIENT_CONVERGENCE and
+    ORBOPT_ENERGY_CONVERGENCE) it stops early, as hilbert's loop does, once
+    the orbital gradient at the solved densities is below g_conv and the
+    energy moved less than e_conv since the last solve.  Returns the
+    energies after each SDP solve and the orbital-gradient norms at each
+    orbital step."""
     if orbital_step not in ("lbfgs", "focas"):
         raise ValueError(f"orbital_step: {orbital_step!r}")
     nmo = h.shape[0]
@@ -421,6 +425,9 @@ def casscf(h, B, ncore, nact, solve_active, macro_iterations=8, active_active=Fa
             gnorms.append(gn)
         h = U.T @ h @ U
         B = U.T @ B @ U
+        if (g_conv is not None and e_conv is not None and len(energies) > 1
+                and gnorms[-1] < g_conv and abs(energies[-1] - energies[-2]) < e_conv):
+            break
     return energies, gnorms, h, B
 
 
@@ -449,7 +456,8 @@ def doci_solve_active(nmo, nalpha, nbeta, positivity="DQG", options=None):
     return solve
 
 
-def doci_casscf(h, B, nalpha, nbeta, solve_active=None, positivity="DQG", macro_iterations=8):
+def doci_casscf(h, B, nalpha, nbeta, solve_active=None, positivity="DQG", macro_iterations=8,
+                g_conv=None, e_conv=None):
     """Orbital-optimised v2RDM-DOCI: every orbital is active (no core, no
     virtuals) and active-active rotations are on, as hilbert's DOCI
     RotateOrbitals sets focas up (v2rdm_doci_solver.cc:997-1019, 1705-1766).
@@ -458,7 +466,7 @@ def doci_casscf(h, B, nalpha, nbeta, solve_active=None, positivity="DQG", macro_
     if solve_active is None:
         solve_active = doci_solve_active(nmo, nalpha, nbeta, positivity)
     return casscf(h, B, 0, nmo, solve_active, macro_iterations=macro_iterations, active_active=True,
-                  orbital_step="focas")
+                  orbital_step="focas", g_conv=g_conv, e_conv=e_conv)
 
 
 def eri_factors(g, rel_tol=1e-12):

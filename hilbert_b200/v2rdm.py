@@ -754,8 +754,10 @@ class v2RDM_DOCIHelper:
         return o
 
     def compute_energy(self, monitor=None, macro_iterations=8):
-        """The DOCI energy; with orbital optimisation, after macro_iterations
-        SDP solves and orbital steps."""
+        """The DOCI energy; with orbital optimisation, after at most
+        macro_iterations SDP solves and orbital steps, fewer once the orbital
+        gradient and the energy change pass ORBOPT_GRADIENT_CONVERGENCE and
+        ORBOPT_ENERGY_CONVERGENCE."""
         p = self.problem
         if self.options.get("OPTIMIZE_ORBITALS"):
             import torch
@@ -774,7 +776,9 @@ class v2RDM_DOCIHelper:
                                               self._sdp_options())
             energies, gnorms, _, _ = orbital.doci_casscf(
                 torch.from_numpy(self.h).to(dev), torch.from_numpy(self.B).to(dev), p.nalpha, p.nbeta,
-                solve_active=solve, macro_iterations=macro_iterations)
+                solve_active=solve, macro_iterations=macro_iterations,
+                g_conv=float(self.options.get("ORBOPT_GRADIENT_CONVERGENCE")),
+                e_conv=float(self.options.get("ORBOPT_ENERGY_CONVERGENCE")))
             solve.problem.close()
             self.stats = {"energies": energies, "orbital_gradients": gnorms}
             e = energies[-1]

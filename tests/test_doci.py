@@ -258,9 +258,11 @@ def test_doci_orbital_optimisation_with_the_focas_step():
         return e, torch.from_numpy(d2p), torch.from_numpy(d1p)
 
     E, gn, _, _ = ho.doci_casscf(torch.from_numpy(h_mo), torch.from_numpy(B_mo), npair, npair,
-                                 solve_active=solve_active, macro_iterations=2)
+                                 solve_active=solve_active, macro_iterations=5, g_conv=1.0, e_conv=10.0)
     assert E[1] < E[0] - 1.0
     assert gn[1] < 0.1 * gn[0]
+    # the thresholds stop the loop after the second solve (|g| 0.58 < 1, |dE| 5.3 < 10)
+    assert len(E) == 2
 
 
 @needs_ref

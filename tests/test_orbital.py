@@ -241,3 +241,4 @@ def test_eri_factors_reproduce_4_index_integrals():
     assert abs(float(e1 - e2)) < 1e-10
     with pytest.raises(ValueError):
         ho.eri_factors(-g)
+
