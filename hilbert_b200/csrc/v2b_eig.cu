@@ -12,6 +12,9 @@
 // Every gemm launch covers all blocks of the problem: the grid is the list of
 // 64 x 64 output tiles of every block.
 #include "v2b_eig.cuh"
+#include "v2b_kernels.cuh"
+
+#include <mutex>
 
 #include <algorithm>
 
@@ -215,23 +218,36 @@ template <bool TA, bool TB, int EPI>
 static cudaError_t launch_variant(int ntiles, cudaStream_t s, GEMM_ARGS, int *sched) {
     auto kern = gemm_tiles_kernel<TA, TB, EPI>;
     // opt in to the pipeline's shared memory and size the persistent grid,
-    // once per variant (thread-safe static initialisation)
+    // once per variant, device and context (function attributes are per
+    // device and do not survive a cudaDeviceReset)
     struct Cfg {
-        cudaError_t err = cudaSuccess;
-        int slots = 1;
+        unsigned long long ctx = 0;
+        int slots = 0;
     };
-    static const Cfg cfg = [kern] {
-        Cfg c;
-        int dev = 0, sms = 0, occ = 0;
-        c.err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
-        if (c.err == cudaSuccess) c.err = cudaGetDevice(&dev);
-        if (c.err == cudaSuccess) c.err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (c.err == cudaSuccess)
-            c.err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kGemmThreads, kGemmSmem);
-        c.slots = std::max(1, sms * occ);
-        return c;
-    }();
-    if (cfg.err != cudaSuccess) return cfg.err;
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static Cfg cache[kMaxDevices];
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    Cfg cfg;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        const unsigned long long ctx = current_context_id();
+        if (cache[dev].slots == 0 || cache[dev].ctx != ctx) {
+            int sms = 0, occ = 0;
+            err = raise_dynamic_smem((const void *)kern, kGemmSmem);
+            if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (err == cudaSuccess)
+                err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kGemmThreads, kGemmSmem);
+            if (err != cudaSuccess) return err;
+            // the context id is read after the calls above, which create the context if needed
+            cache[dev].ctx = current_context_id();
+            cache[dev].slots = std::max(1, sms * occ);
+        }
+        cfg = cache[dev];
+    }
     const int grid = sched ? std::min(ntiles, cfg.slots) : ntiles;
     kern<<<grid, kGemmThreads, kGemmSmem, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate,
                                                orth, ntiles, sched);

@@ -9,6 +9,10 @@
 //                        middle factor of U+ and the refined eigenvectors
 #include "v2b_kernels.cuh"
 
+#include <cuda.h>
+
+#include <mutex>
+
 namespace v2b {
 
 __global__ void spmv_kernel(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ent,
@@ -541,6 +545,39 @@ __global__ void half_residual_kernel(const double *__restrict__ G, double *__res
     const int64_t off = boff[blockIdx.x];
     for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x)
         H[off + e] = 0.5 * (((e / n == e % n) ? 1.0 : 0.0) - G[off + e]);
+}
+
+cudaError_t raise_dynamic_smem(const void *func, int bytes) {
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, func);
+    if (e == cudaSuccess && fa.maxDynamicSharedSizeBytes < bytes)
+        e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
+}
+
+unsigned long long current_context_id() {
+    // driver entry points through the runtime: no link-time libcuda dependency
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static const std::pair<GetCurrent, GetId> fn = [] {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+            qa != cudaDriverEntryPointSuccess)
+            a = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+            qb != cudaDriverEntryPointSuccess)
+            b = nullptr;
+        return std::make_pair((GetCurrent)a, (GetId)b);
+    }();
+    if (!fn.first || !fn.second) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (fn.first(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (fn.second(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
 }
 
 }  // namespace v2b

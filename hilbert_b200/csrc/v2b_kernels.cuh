@@ -83,6 +83,15 @@ __global__ void identity_blocks_kernel(double *__restrict__ Vt, const int64_t *_
 __global__ void half_residual_kernel(const double *__restrict__ G, double *__restrict__ H,
                                      const int64_t *__restrict__ boff, const int *__restrict__ bdim);
 
+// Raise func's dynamic shared-memory limit on the current device to at least
+// bytes, under one process-wide lock; never lowers it, because several
+// problems (and the allocation-free entry point) share the attribute.
+cudaError_t raise_dynamic_smem(const void *func, int bytes);
+// Unique id of the current CUDA context, 0 when there is none.  A new
+// context (after cudaDeviceReset) gets a new id, so per-device caches of
+// symbol addresses and function attributes can tell that they are stale.
+unsigned long long current_context_id();
+
 inline size_t jacobi_smem_bytes(int n) {
     const int np = n + (n & 1);
     return (size_t)np * np * sizeof(double) + (size_t)(np / 2) * (sizeof(double2) + 2 * sizeof(int));

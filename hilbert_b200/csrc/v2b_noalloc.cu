@@ -6,19 +6,21 @@
 // or a latency-bound loop where an allocation (which can synchronise the
 // device) is not acceptable.  v2b_project_block_noalloc serves them: it runs
 // the same kernels as the library's projection (symmetrize_kernel,
-// jacobi_warm_kernel from V = I, the batched GEMM tiles) but takes every
-// scratch buffer from one file-scope __device__ array instead of cudaMalloc.
+// jacobi_warm_kernel from V = I with the library's 30-sweep limit, the
+// batched GEMM tiles) but takes every scratch buffer from one file-scope
+// __device__ array instead of cudaMalloc.
 //
 // The array holds up to kNoAllocMaxDim = 128 rows: its size is fixed at
-// build time (about 3.7 MB) and every GPU that loads the library keeps it
-// until the process exits.  All calls share it and it keeps the contents of
-// the last call; the entry point clears what must start at zero on every
-// call.  Calls that overlap on the GPU (different streams, threads or
-// processes sharing a context) race on the array and must be serialised by
-// the caller.  The first call on a device, with that device current, looks up
-// the array's device address with cudaGetSymbolAddress (the host-side name of
-// the array is only a stand-in, never a device address); make that first call
-// before any stream capture.
+// build time (about 4.4 MB) and every GPU that loads the library keeps it
+// until the process exits.  All calls in a process share it and it keeps the
+// contents of the last call; the entry point clears what must start at zero
+// on every call.  Calls that overlap on the GPU (different streams or host
+// threads) race on the array and must be serialised by the caller.  The
+// first call on a device, with that device current, looks up the array's
+// device address with cudaGetSymbolAddress (the host-side name of the array
+// is only a stand-in, never a device address) and caches it with the
+// context's id; a call in a new context (after cudaDeviceReset) looks it up
+// again.  Make the first call on each device before any stream capture.
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -33,7 +35,7 @@
 namespace v2b {
 
 constexpr int kNoAllocMaxDim = 128;
-constexpr int kNoAllocSweeps = 24;
+constexpr int kNoAllocSweeps = 30;   // the library projection's Jacobi sweep limit
 constexpr int kNoAllocPairs = kNoAllocMaxDim / 2;
 constexpr int64_t kNoAllocMat = (int64_t)kNoAllocMaxDim * kNoAllocMaxDim;   // doubles per matrix
 // rotation record + per-step counts (in double2 units), as jacobi_warm_kernel lays them out
@@ -78,6 +80,7 @@ namespace {
 std::mutex g_noalloc_mu;
 constexpr int kMaxDevices = 64;
 unsigned char *g_noalloc_base[kMaxDevices] = {};
+unsigned long long g_noalloc_ctx[kMaxDevices] = {};   // context the address belongs to
 
 int fail(int code, const std::string &msg) {
     v2b::set_last_error(msg);   // read back through v2b_last_error()
@@ -106,7 +109,8 @@ extern "C" int v2b_project_block_noalloc(const double *d_U, int n, double mu, do
     unsigned char *base = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_base[dev]) {
+        const unsigned long long ctx = current_context_id();
+        if (!g_noalloc_base[dev] || g_noalloc_ctx[dev] != ctx) {
             // host code sees only a stand-in for the array: ask the runtime for
             // its address on this device
             void *p = nullptr;
@@ -114,18 +118,15 @@ extern "C" int v2b_project_block_noalloc(const double *d_U, int n, double mu, do
             if (e != cudaSuccess)
                 return fail(V2B_CUDA_ERROR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
             g_noalloc_base[dev] = (unsigned char *)p;
+            g_noalloc_ctx[dev] = current_context_id();   // the lookup created the context if needed
         }
         base = g_noalloc_base[dev];
-        // the Jacobi kernel's shared-memory limit is shared with the rest of the
-        // library: raise it when this block needs more, never lower it
-        cudaFuncAttributes fa;
-        e = cudaFuncGetAttributes(&fa, jacobi_warm_kernel);
-        if (e == cudaSuccess && fa.maxDynamicSharedSizeBytes < (int)jacobi_smem_bytes(n))
-            e = cudaFuncSetAttribute(jacobi_warm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)jacobi_smem_bytes(n));
-        if (e != cudaSuccess)
-            return fail(V2B_CUDA_ERROR, std::string("shared-memory attribute: ") + cudaGetErrorString(e));
     }
+    // the Jacobi kernel's shared-memory limit is shared with the rest of the
+    // library: raise it when this block needs more, never lower it
+    e = raise_dynamic_smem((const void *)jacobi_warm_kernel, (int)jacobi_smem_bytes(n));
+    if (e != cudaSuccess)
+        return fail(V2B_CUDA_ERROR, std::string("shared-memory attribute: ") + cudaGetErrorString(e));
     NoAllocLayout *L = section<NoAllocLayout>(base, 0);
     double *Us = section<double>(base, offsetof(NoAllocLayout, Us));
     double *W = section<double>(base, offsetof(NoAllocLayout, W));

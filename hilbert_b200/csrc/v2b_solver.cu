@@ -70,6 +70,26 @@ T *dalloc(size_t n) {
     return (T *)p;
 }
 
+// first index of a non-finite value in v[0..n), or -1 (host arrays)
+int64_t first_nonfinite(const double *v, int64_t n) {
+    for (int64_t i = 0; i < n; i++)
+        if (!std::isfinite(v[i])) return i;
+    return -1;
+}
+
+// lowest index of a non-finite value in each of up to three device vectors
+__global__ void nonfinite_kernel(const double *__restrict__ a, int64_t na, const double *__restrict__ b,
+                                 int64_t nb, const double *__restrict__ c, int64_t nc,
+                                 unsigned long long *first) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na + nb + nc; i += stride) {
+        const int which = i < na ? 0 : (i < na + nb ? 1 : 2);
+        const int64_t k = i - (which > 0 ? na : 0) - (which > 1 ? nb : 0);
+        const double v = which == 0 ? a[k] : (which == 1 ? b[k] : c[k]);
+        if (!isfinite(v)) atomicMin(first + which, (unsigned long long)k);
+    }
+}
+
 void ensure_device() {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
@@ -356,8 +376,7 @@ struct ProjectPlan {
         if (ntiles) V2B_CK(cudaMemcpy(tiles, tl.data(), ntiles * sizeof(int4), cudaMemcpyHostToDevice));
         if (nsmall) rot = dalloc<double2>(ro);
         if (smem)
-            V2B_CK(cudaFuncSetAttribute(v2b::jacobi_warm_kernel,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            V2B_CK(v2b::raise_dynamic_smem((const void *)v2b::jacobi_warm_kernel, (int)smem));
         if (nbig) {
             rec_b = dalloc<double2>(rb);
             norm_b = dalloc<double>((size_t)nbig * v2b::kBigCluster);
@@ -395,17 +414,13 @@ struct ProjectPlan {
         V2B_CK(cudaMemcpy(rowbase, rb_host.data(), nblk * 4, cudaMemcpyHostToDevice));
         classify_smem = (size_t)maxn * sizeof(double);
         if (classify_smem > 48 * 1024)
-            V2B_CK(cudaFuncSetAttribute(v2b::refine_classify_kernel,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)classify_smem));
+            V2B_CK(v2b::raise_dynamic_smem((const void *)v2b::refine_classify_kernel, (int)classify_smem));
         const int kc = v2b::kRefineSmallCluster;
-        V2B_CK(cudaFuncSetAttribute(v2b::cluster_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(2 * kc * (kc + 1) * sizeof(double))));
-        V2B_CK(cudaFuncSetAttribute(v2b::bj_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(3 * kc * (kc + 1) * sizeof(double))));
+        V2B_CK(v2b::raise_dynamic_smem((const void *)v2b::cluster_eig_kernel, (int)(2 * kc * (kc + 1) * sizeof(double))));
+        V2B_CK(v2b::raise_dynamic_smem((const void *)v2b::bj_apply_kernel, (int)(3 * kc * (kc + 1) * sizeof(double))));
         // clusters of kRefineSmallCluster+1 .. kJacobiMaxDim rows use jacobi_warm_kernel
         mid_smem = v2b::jacobi_smem_bytes(v2b::kJacobiMaxDim);
-        V2B_CK(cudaFuncSetAttribute(v2b::jacobi_warm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)std::max(smem, mid_smem)));
+        V2B_CK(v2b::raise_dynamic_smem((const void *)v2b::jacobi_warm_kernel, (int)std::max(smem, mid_smem)));
         build_block_jacobi();
         V2B_CK(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
         fresh = true;
@@ -1072,6 +1087,7 @@ struct v2b_problem {
         cudaFree(bar);
         cudaFree(ibas_aa_dev);
         cudaFree(status);
+        if (nonfinite) cudaFree(nonfinite);
         if (h_readback) cudaFreeHost(h_readback);
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
@@ -1083,6 +1099,14 @@ struct v2b_problem {
     bool on_device = false;
     // a restart state (v2b_problem_set_state) that the next solve starts from
     bool resume = false;
+    // v2b_problem_continue: the next solve keeps mu, y, z and the projection's
+    // bases of the last device solve (libsdp's state across solve() calls)
+    bool keep_state = false;
+    bool solved = false;   // a device solve has run (its state can be continued)
+    // polls of a CG grid-barrier wait before it gives up (a few seconds of 32 ns sleeps)
+    static constexpr long long kDefaultWaitLimit = 40000000LL;
+    long long wait_limit = kDefaultWaitLimit;
+    unsigned long long *nonfinite = nullptr;   // nonfinite_kernel's three results
     std::vector<double> resume_y, resume_z;
 
     // device resources are created on first device use, so that the host-side
@@ -1154,7 +1178,7 @@ struct v2b_problem {
         P.Ax = Ax; P.Acz = Acz; P.b = b; P.mu = mu;
         P.y = y; P.r = r; P.p0 = p0; P.p1 = p1; P.t = t; P.q = q;
         P.partials = partials; P.bar = bar; P.status = status;
-        P.spin_limit = 40000000LL;   // a few seconds of 32 ns polls
+        P.spin_limit = wait_limit;
         P.tol = tol; P.maxit = maxit; P.out = cg_out;
         P.phase_ns = profiling ? cg_phase : nullptr;
         void *args[] = {&P};
@@ -1216,13 +1240,36 @@ struct v2b_problem {
         out[4] = h_readback[3];
     }
 
+    // x, b, c on the device must be finite: a NaN there would only surface
+    // after a whole iteration, inside the projection
+    void check_inputs_finite() {
+        if (!nonfinite) nonfinite = dalloc<unsigned long long>(3);
+        V2B_CK(cudaMemsetAsync(nonfinite, 0xff, 3 * sizeof(unsigned long long), stream));
+        const int64_t tot = 2 * prob.n_primal + prob.n_dual;
+        nonfinite_kernel<<<grid_for(tot, 256), 256, 0, stream>>>(x, prob.n_primal, b, prob.n_dual, c,
+                                                                  prob.n_primal, nonfinite);
+        V2B_CK(cudaGetLastError());
+        launches++;
+        unsigned long long first[3];
+        V2B_CK(cudaMemcpyAsync(first, nonfinite, sizeof first, cudaMemcpyDeviceToHost, stream));
+        V2B_CK(cudaStreamSynchronize(stream));
+        const char *names[3] = {"x", "b", "c"};
+        for (int k = 0; k < 3; k++)
+            if (first[k] != ~0ull)
+                throw Failure(V2B_NAN, std::string("non-finite value in ") + names[k] + " at index " +
+                                           std::to_string(first[k]));
+    }
+
     int solve_device(const v2b_sdp_options &o, int muf, v2b_sdp_monitor monitor, int print_level,
                      void *data, long *oiter_out, long *iiter_out, double *energy) {
         if (muf < 1) throw std::invalid_argument("mu_update_frequency must be >= 1");
+        check_inputs_finite();
         const int64_t np = prob.n_primal, nd = prob.n_dual;
         ensure_plan();
-        plan.reset();
-        if (resume) {   // mu was set with the state
+        if (keep_state) {   // continue where the last device solve stopped
+            keep_state = false;
+        } else if (resume) {   // mu was set with the state
+            plan.reset();
             V2B_CK(cudaMemcpyAsync(y, resume_y.data(), nd * 8, cudaMemcpyHostToDevice, stream));
             V2B_CK(cudaMemcpyAsync(z, resume_z.data(), np * 8, cudaMemcpyHostToDevice, stream));
             V2B_CK(cudaStreamSynchronize(stream));
@@ -1230,6 +1277,7 @@ struct v2b_problem {
             std::vector<double>().swap(resume_y);
             std::vector<double>().swap(resume_z);
         } else {
+            plan.reset();
             mu = 0.1;
             V2B_CK(cudaMemsetAsync(y, 0, nd * 8, stream));
             V2B_CK(cudaMemsetAsync(z, 0, np * 8, stream));
@@ -1257,6 +1305,7 @@ struct v2b_problem {
             }
             if (!converged && res[2] > 0.0) mu = mu * res[1] / res[2];
         }
+        solved = true;
         if (oiter_out) *oiter_out = oiter;
         if (iiter_out) *iiter_out = iiter;
         if (energy) *energy = res[3];
@@ -1614,6 +1663,15 @@ int v2b_problem_solve(v2b_problem *p, double *x, const double *b, const double *
                       double *energy) {
     return guarded([&] {
         if (!p || !x || !b || !c || !options) throw std::invalid_argument("solve: NULL argument");
+        const double *in[3] = {x, b, c};
+        const int64_t len[3] = {p->prob.n_primal, p->prob.n_dual, p->prob.n_primal};
+        const char *names[3] = {"x", "b", "c"};
+        for (int k = 0; k < 3; k++) {
+            const int64_t i = first_nonfinite(in[k], len[k]);
+            if (i >= 0)
+                throw Failure(V2B_NAN, std::string("non-finite value in ") + names[k] + " at index " +
+                                           std::to_string(i));
+        }
         p->setup();
         const int64_t np = p->prob.n_primal, nd = p->prob.n_dual;
         V2B_CK(cudaMemcpyAsync(p->x, x, np * 8, cudaMemcpyHostToDevice, p->stream));
@@ -1642,6 +1700,25 @@ int v2b_problem_set_state(v2b_problem *p, double mu, const double *y, const doub
         p->resume_z.assign(z, z + p->prob.n_primal);
         p->mu = mu;
         p->resume = true;
+        p->keep_state = false;
+        return V2B_OK;
+    });
+}
+int v2b_problem_set_wait_limit(v2b_problem *p, long long polls) {
+    return guarded([&] {
+        if (!p || polls < 0) throw std::invalid_argument("set_wait_limit: bad argument");
+        p->wait_limit = polls ? polls : v2b_problem::kDefaultWaitLimit;
+        return V2B_OK;
+    });
+}
+int v2b_problem_continue(v2b_problem *p) {
+    return guarded([&] {
+        if (!p) throw std::invalid_argument("continue: NULL argument");
+        if (!p->on_device || !p->solved) throw std::invalid_argument("continue: no device solve has run");
+        p->resume = false;
+        std::vector<double>().swap(p->resume_y);
+        std::vector<double>().swap(p->resume_z);
+        p->keep_state = true;
         return V2B_OK;
     });
 }

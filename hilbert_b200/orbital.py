@@ -392,72 +392,145 @@ def active_space(h, B, ncore, nact):
     return e_core, Fi[act, act], g
 
 
-def casscf(h, B, ncore, nact, solve_active, macro_iterations=8, active_active=False,
-           orbital_step="lbfgs", g_conv=None, e_conv=None):
-    """v2RDM-CASSCF macro-iterations: solve the active-space v2RDM in the
-    current orbitals (solve_active(h_act, g_act) -> (E_active, packed d2,
-    packed d1) on the same device as h), optimise the orbitals at those
-    densities, rotate h and B, repeat.  orbital_step: "lbfgs"
-    (optimize_orbitals) or "focas" (optimize_orbitals_focas with focas's
-    defaults).  With g_conv and e_conv (ORBOPT_GRADIENT_CONVERGENCE and
-    ORBOPT_ENERGY_CONVERGENCE) it stops early, as hilbert's loop does, once
-    the orbital gradient at the solved densities is below g_conv and the
-    energy moved less than e_conv since the last solve.  Returns the
-    energies after each SDP solve and the orbital-gradient norms at each
-    orbital step."""
+def casscf(h, B, ncore, nact, solve_active, macro_iterations=None, active_active=False,
+           orbital_step="lbfgs", g_conv=None, e_conv=None, info=None, orbopt_maxiter=10):
+    """v2RDM-CASSCF macro-iterations in hilbert's order (v2rdm_solver.cc:1330-1361,
+    v2rdm_doci_solver.cc:1111-1137): an SDP solve in the current orbitals, an
+    orbital step at its densities, the rotation of h and B, repeated until
+    the SDP has converged and the orbital step has met its thresholds.
+
+    solve_active(h_act, g_act) -> (E_active, packed d2, packed d1[, converged])
+    on the same device as h: either a full solve (three values, or
+    converged True) or, as hilbert runs it, one call of ORBOPT_FREQUENCY
+    iterations that continues from the previous call's state (active_solver
+    with a frequency).  A solve_active whose ``exhausted`` attribute turns
+    true has spent its MAXITER budget and ends the loop.
+
+    orbital_step: "lbfgs" (optimize_orbitals) or "focas"
+    (optimize_orbitals_focas with focas's defaults).  The orbital step has
+    converged (orbopt_converged_, v2rdm_doci_solver.cc:1753-1762) when its
+    total energy change is below e_conv and its final gradient norm below
+    g_conv (ORBOPT_ENERGY_CONVERGENCE, ORBOPT_GRADIENT_CONVERGENCE); without
+    g_conv and e_conv it never counts as converged.  macro_iterations (None:
+    no cap) bounds the rounds of solve and orbital step.  The focas step runs
+    at most orbopt_maxiter iterations (ORBOPT_MAXITER) with g_conv and e_conv
+    as its own thresholds (focas's defaults 1e-4 and 1e-8 when not given).
+
+    Returns the energies after each SDP solve, the orbital-gradient norms at
+    each orbital step (at the solved densities, before the step), and h, B in
+    the final orbitals.  ``info`` (a dict, optional) receives sdp_converged,
+    orbitals_converged, rounds and final_energy (the energy at the last
+    densities in the final orbitals, where hilbert reports it)."""
     if orbital_step not in ("lbfgs", "focas"):
         raise ValueError(f"orbital_step: {orbital_step!r}")
+    if macro_iterations is None and (g_conv is None or e_conv is None):
+        raise ValueError("give macro_iterations, or g_conv and e_conv to stop on")
     nmo = h.shape[0]
     nvirt = nmo - ncore - nact
     pairs = rotation_pairs(ncore, nact, nvirt, active_active)
     energies, gnorms = [], []
-    for _ in range(macro_iterations):
+    sdp_conv = orb_conv = False
+    e_final = None
+    rounds = 0
+    while macro_iterations is None or rounds < macro_iterations:
         e_core, h_act, g_act = active_space(h, B, ncore, nact)
-        e_act, d2p, d1p = solve_active(h_act, g_act)
+        res = solve_active(h_act, g_act)
+        e_act, d2p, d1p = res[:3]
+        sdp_conv = bool(res[3]) if len(res) > 3 else True
         energies.append(e_core + e_act)
         Da, Ga = unpack_densities(d2p, d1p, nact)
         if orbital_step == "focas":
-            U, _, hist = optimize_orbitals_focas(h, B, Da, Ga, ncore, nact, active_active=active_active)
-            gnorms.append(hist[0][2])
+            U, e_final, hist = optimize_orbitals_focas(
+                h, B, Da, Ga, ncore, nact, maxiter=orbopt_maxiter,
+                g_conv=1e-4 if g_conv is None else g_conv, e_conv=1e-8 if e_conv is None else e_conv,
+                active_active=active_active)
+            g_first, g_last = hist[0][2], hist[-1][2]
         else:
             D, G = full_densities(Da, Ga, ncore, nvirt)
-            U, _, gn, _ = optimize_orbitals(h, B, D, G, pairs)
-            gnorms.append(gn)
+            U, e_final, g_first, g_last = optimize_orbitals(h, B, D, G, pairs)
+        gnorms.append(g_first)
         h = U.T @ h @ U
         B = U.T @ B @ U
-        if (g_conv is not None and e_conv is not None and len(energies) > 1
-                and gnorms[-1] < g_conv and abs(energies[-1] - energies[-2]) < e_conv):
+        rounds += 1
+        orb_conv = (g_conv is not None and e_conv is not None
+                    and abs(e_final - energies[-1]) < e_conv and abs(g_last) < g_conv)
+        if (sdp_conv and orb_conv) or getattr(solve_active, "exhausted", False):
             break
+    if info is not None:
+        info.update(sdp_converged=sdp_conv, orbitals_converged=orb_conv, rounds=rounds,
+                    final_energy=e_final)
     return energies, gnorms, h, B
 
 
-def doci_solve_active(nmo, nalpha, nbeta, positivity="DQG", options=None):
-    """The active solve of v2RDM-DOCI on the device, for casscf: builds the
-    DOCI problem once, and for each (h, g) solves it from the random guess
-    (v2rdm_doci_solver.cc:1058-1137) and packs its densities as hilbert's
-    DOCI PackSpatialDensity does (:1568-1703)."""
+def active_solver(p, options, frequency=None):
+    """The active-space SDP solve on the device for casscf, from a problem p
+    (v2rdm.V2RDMProblem or DOCIProblem) and its Options.
+
+    frequency None: every call solves from the reference's random guess to
+    convergence within MAXITER outer iterations and raises if it does not
+    converge.  frequency k (ORBOPT_FREQUENCY): hilbert's schedule.  The first
+    call starts from the random guess; every later call continues from the
+    x, y, z and mu the previous call left, as libsdp's solver keeps them
+    between solve() calls, for at most k outer iterations with mu updated
+    after them (sdp_->solve(..., ORBOPT_FREQUENCY, ...),
+    v2rdm_doci_solver.cc:1113).  MAXITER bounds the outer iterations of all
+    calls together (hilbert hands it to libsdp as SDPOptions.maxiter,
+    v2rdm_solver.cc:430); once it is spent without convergence the closure's
+    ``exhausted`` attribute turns true.  A call returns (c.x, packed d2,
+    packed d1, converged); x is packed as hilbert's PackSpatialDensity."""
     from . import v2rdm
-    p = v2rdm.DOCIProblem(nmo, nalpha, nbeta, positivity)
-    opts = options or v2rdm.Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6,
-                                     "MAXITER": 100000, "MU_UPDATE_FREQUENCY": 500})
+    state = {"x": None, "oiter": 0, "iiter": 0}
+    maxiter = int(options.get("MAXITER"))
 
     def solve(h_act, g_act):
         dev = h_act.device
         b = torch.from_numpy(p.b()).to(dev)
         c = torch.from_numpy(p.c_external(h_act.cpu().numpy(), g_act.cpu().numpy())).to(dev)
-        x = torch.from_numpy(p.guess("RANDOM")).to(dev)
-        st = p.solve_device(x, b, c, opts)
-        if not st["converged"]:
-            raise RuntimeError("v2RDM-DOCI solve did not converge")
+        if frequency is None:
+            x = torch.from_numpy(p.guess("RANDOM")).to(dev)
+            st = p.solve_device(x, b, c, options)
+            if not st["converged"]:
+                raise RuntimeError(f"the SDP did not converge in MAXITER = {maxiter} iterations")
+        else:
+            if state["x"] is None:
+                state["x"] = torch.from_numpy(p.guess("RANDOM")).to(dev)
+            else:
+                p.continue_state()
+            x = state["x"]
+            k = max(1, min(int(frequency), maxiter - state["oiter"]))
+            o = v2rdm.Options(dict(options._v))
+            o.set("MAXITER", k)
+            o.set("MU_UPDATE_FREQUENCY", k)
+            st = p.solve_device(x, b, c, o)
+            solve.exhausted = (not st["converged"]) and state["oiter"] + st["oiter"] >= maxiter
+        state["oiter"] += st["oiter"]
+        state["iiter"] += st["iiter"]
+        solve.oiter, solve.iiter = state["oiter"], state["iiter"]
         d2p, d1p = p.pack_spatial_density(x)
-        return float(c @ x), d2p, d1p
+        return float(c @ x), d2p, d1p, st["converged"]
 
     solve.problem = p
+    solve.exhausted = False
+    solve.oiter = solve.iiter = 0
     return solve
 
 
-def doci_casscf(h, B, nalpha, nbeta, solve_active=None, positivity="DQG", macro_iterations=8,
-                g_conv=None, e_conv=None):
+def doci_solve_active(nmo, nalpha, nbeta, positivity="DQG", options=None, frequency=None):
+    """The active solve of v2RDM-DOCI on the device for casscf: the DOCI
+    problem built once (v2rdm_doci_solver.cc:427-700), solved by
+    active_solver (each call to convergence, or hilbert's calls of
+    ORBOPT_FREQUENCY iterations with the state carried over,
+    :1111-1137), its densities packed as hilbert's DOCI
+    PackSpatialDensity does (:1568-1703)."""
+    from . import v2rdm
+    p = v2rdm.DOCIProblem(nmo, nalpha, nbeta, positivity)
+    opts = options or v2rdm.Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6,
+                                     "MAXITER": 100000, "MU_UPDATE_FREQUENCY": 500})
+    return active_solver(p, opts, frequency)
+
+
+def doci_casscf(h, B, nalpha, nbeta, solve_active=None, positivity="DQG", macro_iterations=None,
+                g_conv=None, e_conv=None, info=None, orbopt_maxiter=10):
     """Orbital-optimised v2RDM-DOCI: every orbital is active (no core, no
     virtuals) and active-active rotations are on, as hilbert's DOCI
     RotateOrbitals sets focas up (v2rdm_doci_solver.cc:997-1019, 1705-1766).
@@ -466,7 +539,8 @@ def doci_casscf(h, B, nalpha, nbeta, solve_active=None, positivity="DQG", macro_
     if solve_active is None:
         solve_active = doci_solve_active(nmo, nalpha, nbeta, positivity)
     return casscf(h, B, 0, nmo, solve_active, macro_iterations=macro_iterations, active_active=True,
-                  orbital_step="focas", g_conv=g_conv, e_conv=e_conv)
+                  orbital_step="focas", g_conv=g_conv, e_conv=e_conv, info=info,
+                  orbopt_maxiter=orbopt_maxiter)
 
 
 def eri_factors(g, rel_tol=1e-12):

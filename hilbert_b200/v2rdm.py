@@ -262,6 +262,17 @@ class V2RDMProblem:
             raise ValueError(f"y must hold {self.n_dual} values and z {self.n_primal}")
         check(self._lib.v2b_problem_set_state(self._h, float(mu), _dptr(y), _dptr(z)))
 
+    def set_wait_limit(self, polls=0):
+        """Polls of a CG grid-barrier wait before the solve gives up with
+        V2B_DEVICE_TIMEOUT (0: the default, seconds)."""
+        check(self._lib.v2b_problem_set_wait_limit(self._h, int(polls)))
+
+    def continue_state(self):
+        """The next solve continues from the penalty, dual variables and
+        eigenvector bases the last device solve left, as libsdp's solver
+        keeps them between solve() calls (v2rdm_solver.cc:1330-1361)."""
+        check(self._lib.v2b_problem_continue(self._h))
+
     def get_z(self):
         out = np.zeros(self.n_primal)
         check(self._lib.v2b_problem_get_z(self._h, _dptr(out)))
@@ -753,35 +764,43 @@ class v2RDM_DOCIHelper:
         o.set("MU_UPDATE_FREQUENCY", int(self.options.get("ORBOPT_FREQUENCY")))
         return o
 
-    def compute_energy(self, monitor=None, macro_iterations=8):
-        """The DOCI energy; with orbital optimisation, after at most
-        macro_iterations SDP solves and orbital steps, fewer once the orbital
-        gradient and the energy change pass ORBOPT_GRADIENT_CONVERGENCE and
-        ORBOPT_ENERGY_CONVERGENCE."""
+    def compute_energy(self, monitor=None, macro_iterations=None):
+        """The DOCI energy.  With OPTIMIZE_ORBITALS it runs hilbert's loop
+        (v2rdm_doci_solver.cc:1111-1137): solve() calls of ORBOPT_FREQUENCY
+        SDP iterations that carry x, y, z and mu over, each followed by a
+        focas orbital step (ORBOPT_MAXITER iterations at most), until the SDP
+        has converged and the orbital step met ORBOPT_GRADIENT_CONVERGENCE and
+        ORBOPT_ENERGY_CONVERGENCE.  MAXITER bounds the SDP iterations of all
+        calls together; macro_iterations (None: no cap) the rounds.  The
+        energy is c.x in the final orbitals, where hilbert takes it (:1142).
+        stats["converged"] is False when a cap ended the loop first."""
         p = self.problem
-        if self.options.get("OPTIMIZE_ORBITALS"):
+        o = self.options
+        if o.get("OPTIMIZE_ORBITALS"):
             import torch
             if not torch.cuda.is_available():
                 raise _capi.V2BError(_capi.V2B_NO_DEVICE, "v2RDM-DOCI orbital optimisation needs a CUDA device")
-        if self.options.get("OPTIMIZE_ORBITALS") and self.B is None and self._g is not None:
+        if o.get("OPTIMIZE_ORBITALS") and self.B is None and self._g is not None:
             from . import orbital
             self.B = orbital.eri_factors(self._g).numpy()
-        if self.options.get("OPTIMIZE_ORBITALS") and self.B is not None:
+        if o.get("OPTIMIZE_ORBITALS") and self.B is not None:
             import torch
             from . import orbital
             dev = torch.device("cuda", torch.cuda.current_device())
-            solve = orbital.doci_solve_active(p.nmo, p.nalpha, p.nbeta,
-                                              self.options.get("POSITIVITY")
-                                              + ("+D3" if self.options.get("CONSTRAIN_D3") else ""),
-                                              self._sdp_options())
+            solve = orbital.active_solver(p, o, frequency=int(o.get("ORBOPT_FREQUENCY")))
+            info = {}
             energies, gnorms, _, _ = orbital.doci_casscf(
                 torch.from_numpy(self.h).to(dev), torch.from_numpy(self.B).to(dev), p.nalpha, p.nbeta,
                 solve_active=solve, macro_iterations=macro_iterations,
-                g_conv=float(self.options.get("ORBOPT_GRADIENT_CONVERGENCE")),
-                e_conv=float(self.options.get("ORBOPT_ENERGY_CONVERGENCE")))
-            solve.problem.close()
-            self.stats = {"energies": energies, "orbital_gradients": gnorms}
-            e = energies[-1]
+                g_conv=float(o.get("ORBOPT_GRADIENT_CONVERGENCE")),
+                e_conv=float(o.get("ORBOPT_ENERGY_CONVERGENCE")), info=info,
+                orbopt_maxiter=int(o.get("ORBOPT_MAXITER")))
+            converged = info["sdp_converged"] and info["orbitals_converged"]
+            self.stats = {"energies": energies, "orbital_gradients": gnorms, "converged": converged,
+                          "sdp_converged": info["sdp_converged"],
+                          "orbitals_converged": info["orbitals_converged"], "rounds": info["rounds"],
+                          "oiter": solve.oiter, "iiter": solve.iiter}
+            e = info["final_energy"]
         else:
             self.x, self.stats = p.solve(p.guess("RANDOM"), self.b, self.c, self._sdp_options(), monitor)
             e = float(self.c @ self.x)

@@ -205,6 +205,26 @@ double v2b_problem_get_mu(const v2b_problem *p);
  * instead of mu = 0.1 and y = z = 0.  Host arrays, copied here; one solve
  * uses them. */
 int v2b_problem_set_state(v2b_problem *p, double mu, const double *y, const double *z);
+/* No counterpart in the reference (its solver has no device waits).  The
+ * conjugate-gradient kernel is one persistent launch whose blocks meet at
+ * grid barriers; each wait polls at most `polls` times (32 ns sleeps between
+ * polls) before it records V2B_DEVICE_TIMEOUT, every block leaves at its next
+ * barrier and the solve returns that status.  0 restores the default of 40
+ * million polls (seconds).  The device solve also checks x, b and c for
+ * non-finite values before its first iteration and returns V2B_NAN, naming
+ * the vector and index, without iterating (v2b_problem_solve checks the host
+ * arrays before any device work). */
+int v2b_problem_set_wait_limit(v2b_problem *p, long long polls);
+/* libsdp's solver keeps mu, y and z from one solve() call to the next, and
+ * hilbert's orbital-optimising loops rely on it: solve(ORBOPT_FREQUENCY),
+ * rotate the orbitals (new c), solve again from where the SDP stopped
+ * (src/v2rdm_casscf/v2rdm_solver.cc:1330-1361,
+ * src/v2rdm_doci/v2rdm_doci_solver.cc:1111-1137).  A device solve starts
+ * from mu = 0.1 and y = z = 0 unless this is called before it: then the next
+ * v2b_problem_solve or v2b_problem_solve_device continues from the mu, y, z
+ * and eigenvector bases that the last device solve of p left (x is the
+ * solve's own argument).  V2B_BAD_ARG before the first device solve. */
+int v2b_problem_continue(v2b_problem *p);
 /* The packed constraint operator the device maps read: A (transposed = 0,
  * rows = dual constraints) or A^T (transposed = 1, rows = primal elements).
  * Entry bits 0..26 hold the column, 27..30 an index into the palette of
@@ -314,12 +334,13 @@ int v2b_problem_d3_records(const v2b_problem *p, int ncore, const double *x, v2b
  * device synchronisation of an allocation is not acceptable there): projects
  * ONE n x n block d_U (row-major, device memory) like v2b_problem_project,
  * writing d_x = U+ / mu and d_z = U+ - sym(U), on the given cudaStream_t.
- * n <= 128: all scratch is a fixed file-scope device array (about 3.7 MB,
+ * n <= 128: all scratch is a fixed file-scope device array (about 4.4 MB,
  * held by every GPU that loads the library until exit); larger n returns
  * V2B_BAD_ARG.  Allocates nothing.  Every call reuses the same array, so calls
  * that overlap on the GPU race and must be serialised by the caller.  The
- * first call on a device looks the array up with cudaGetSymbolAddress; make
- * it before any stream capture. */
+ * first call on a device looks the array up with cudaGetSymbolAddress (a
+ * call in a new context, after cudaDeviceReset, looks it up again); make it
+ * before any stream capture. */
 int v2b_project_block_noalloc(const double *d_U, int n, double mu, double *d_x, double *d_z,
                               void *stream);
 

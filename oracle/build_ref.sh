@@ -59,9 +59,21 @@ for name in SymmetryPair TotalSym set_constraints determine_n_primal determine_n
   grep -q "v2RDMSolver::${name}(" "$gen" || { echo "build_ref.sh: could not extract ${name}" >&2; exit 3; }
 done
 
-# -ffp-contract=off keeps a*b+c as two roundings, as in a plain x86-64 build
+# -ffp-contract=off keeps a*b+c as two roundings, as in a plain x86-64 build.
+# -fopenmp: the reference parallelises its maps with OpenMP (q2.cc, g2.cc,
+# t2.cc, ...); every output element is still written by one thread in the
+# reference's order, so results stay bit-identical.  x86-64-v3 (AVX2, FMA)
+# rather than -march=native: the library is built here and also runs on the
+# GPU host, whose CPU model may differ.
 CXX="${CXX:-g++}"
-FLAGS=(-std=c++17 -O2 -fPIC -ffp-contract=off -w
+# some images wrap g++ without the path to libgomp.spec: point -B at it
+OMPB=()
+if ! echo 'int main(){return 0;}' | "$CXX" -x c++ -fopenmp - -o /dev/null 2>/dev/null; then
+  spec="$(ls /usr/lib/gcc/x86_64-linux-gnu/*/libgomp.spec 2>/dev/null | tail -1)"
+  [ -n "$spec" ] || { echo "build_ref.sh: $CXX cannot build OpenMP code" >&2; exit 4; }
+  OMPB=(-B"$(dirname "$spec")/")
+fi
+FLAGS=(-std=c++17 -O3 -march=x86-64-v3 -fopenmp "${OMPB[@]}" -fPIC -ffp-contract=off -w
        -I"$here/ref_shim" -I"$src" -I"$ref/src")
 units=(basis d2 spin q2 g2 t1 t2 d3 d4 e3 f3 q3 tei write_opdm write_3pdm)
 objs=()
@@ -71,7 +83,7 @@ for u in "${units[@]}"; do
 done
 "$CXX" "${FLAGS[@]}" -c "$gen" -o "$out/v2rdm_solver_extract.o"
 "$CXX" "${FLAGS[@]}" -c "$here/ref_harness.cc" -o "$out/ref_harness.o"
-"$CXX" -shared -Wl,--no-undefined -o "$out/libv2rdm_ref.so" "${objs[@]}" \
+"$CXX" -shared -fopenmp "${OMPB[@]}" -Wl,--no-undefined -o "$out/libv2rdm_ref.so" "${objs[@]}" \
     "$out/v2rdm_solver_extract.o" "$out/ref_harness.o"
 echo "built $out/libv2rdm_ref.so"
 
@@ -102,7 +114,7 @@ for name in SymmetryPair TotalSym BuildConstraints Guess bpsdp_Au bpsdp_ATu Pack
   grep -q "v2RDM_DOCISolver::${name}(" "$dgen" || { echo "build_ref.sh: could not extract DOCI ${name}" >&2; exit 3; }
 done
 grep -q "dimensions_.push_back" "$dgen" || { echo "build_ref.sh: could not extract the DOCI sizing" >&2; exit 3; }
-DFLAGS=(-std=c++17 -O2 -fPIC -ffp-contract=off -w
+DFLAGS=(-std=c++17 -O3 -march=x86-64-v3 -fopenmp "${OMPB[@]}" -fPIC -ffp-contract=off -w
         -I"$here/ref_shim" -I"$dsrc" -I"$ref/src")
 dobjs=()
 for u in basis d2 q2 g2 d3 t1 t2 tei write_tpdm; do
@@ -111,6 +123,6 @@ for u in basis d2 q2 g2 d3 t1 t2 tei write_tpdm; do
 done
 "$CXX" "${DFLAGS[@]}" -c "$dgen" -o "$out/doci_solver_extract.o"
 "$CXX" "${DFLAGS[@]}" -c "$here/doci_ref_harness.cc" -o "$out/doci_ref_harness.o"
-"$CXX" -shared -Wl,--no-undefined -o "$out/libdoci_ref.so" "${dobjs[@]}" \
+"$CXX" -shared -fopenmp "${OMPB[@]}" -Wl,--no-undefined -o "$out/libdoci_ref.so" "${dobjs[@]}" \
     "$out/doci_solver_extract.o" "$out/doci_ref_harness.o"
 echo "built $out/libdoci_ref.so"

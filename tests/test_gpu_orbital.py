@@ -89,3 +89,26 @@ def test_df_casscf_macro_iterations(cuda_device):
         assert b_ <= a + 1e-6
     assert E[-1] < E[0] - 1e-2
     assert gn[-1] < 0.1 * gn[0]
+
+
+def test_df_casscf_on_hilbert_schedule(cuda_device):
+    """v2RDM-CASSCF (config 2: nbf 40, naux 160, 5 core + (10e, 10o)) on
+    hilbert's schedule: solve(ORBOPT_FREQUENCY = 500) calls on the device
+    that carry x, y, z and mu over while the orbitals change between them
+    (v2rdm_solver.cc:1330-1361).  After a few rounds the SDP state is still
+    the one solve's (the iteration count only grows by the calls), the
+    energy has fallen below the first round's, and the orbital gradient has
+    shrunk."""
+    import torch
+    nc, na_ = 5, 10
+    h_mo, B_mo, *_ = ho.casscf_df_problem(40, 160, nc, na_)
+    p = hb.V2RDMProblem(na_, 5, 5)
+    opts = hb.Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6, "MAXITER": 100000})
+    solve = ho.active_solver(p, opts, frequency=500)
+    info = {}
+    E, gn, _, _ = ho.casscf(torch.from_numpy(h_mo).to(cuda_device), torch.from_numpy(B_mo).to(cuda_device),
+                            nc, na_, solve, macro_iterations=6, info=info)
+    assert info["rounds"] == 6 and solve.oiter <= 6 * 500
+    assert not solve.exhausted
+    assert E[-1] < E[0] - 1e-2
+    assert gn[-1] < 0.1 * gn[0]
