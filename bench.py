@@ -49,19 +49,23 @@ WORKLOADS = {
                      hubbard=(1.0, 4.0), hubbard_multiplicity=True,
                      r_conv=1e-6, e_conv=1e-6, cg_conv=1e-9, muf=500, maxiter=400000),
 }
-# (outer, CG) iterations of the FP64 solve to convergence; the reference arm
-# scales its per-iteration sample by them.
-#  hubbard8: the CPU oracle run (C restatement maps + numpy boundary-point
-#    loop): energy -4.9364448537582035 at eps_p 9.83e-7, eps_d 1.00e-6.
-#  df20: the FP64 device solve (one outer iteration of the CPU path takes
-#    seconds here, so a CPU solve to convergence takes hours; the device path
-#    reproduces the CPU oracle's iteration counts on the Hubbard rings).
-FP64_ITERS = {"hubbard8": (13801, 503997), "df20": (4080, 183147)}
-# FP64 energies the device result is compared with:
-#  hubbard8: the CPU oracle; df20: the FP64 device solve that diagonalises
-#  every block by selective Jacobi each iteration (no warm refinement).
-FP64_ENERGY = {"hubbard8": (-4.9364448537582035, "cpu oracle"),
-               "df20": (-103.6150114064154, "fp64 device solve, Jacobi every iteration")}
+# FP64 reference of each workload: the CPU oracle's converged solve, hilbert's
+# compiled maps (oracle/_ref) driven by the numpy boundary-point restatement
+# (oracle/bpsdp.py), generated by tests/golden/make_fp64_energies.py into
+# tests/golden/fp64_<workload>.json.  Its outer / CG iteration counts scale
+# the reference arm's per-iteration sample; its energy is what |dE| is taken
+# against.
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def fp64_reference(workload):
+    """{"energy", "outer_iterations", "cg_iterations", "wall_s", ...} of the
+    CPU oracle's FP64 solve, or None when its fixture is absent."""
+    path = os.path.join(GOLDEN, f"fp64_{workload}.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f)
 
 
 def hamiltonian(w):
@@ -82,7 +86,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="df20", choices=sorted(WORKLOADS))
-    ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-sample-seconds", type=float, default=60.0,
+                    help="seconds of CPU work sampled for the CPU baseline (the reference arm "
+                         "divides a few minutes among its steps)")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the solve on the plain FP64 path (selective Jacobi on every block "
                          "every iteration) that a 1-GPU run times for comparison")
@@ -190,12 +196,16 @@ def max_over_ranks(v, world):
 
 
 def cpu_threads():
+    """(OpenMP threads of the compiled maps, BLAS threads of numpy's LAPACK)"""
+    omp = int(os.environ.get("OMP_NUM_THREADS", "0") or 0) or (os.cpu_count() or 1)
+    blas = 1
     try:
         from threadpoolctl import threadpool_info
         n = [i.get("num_threads", 1) for i in threadpool_info() if i.get("user_api") == "blas"]
-        return max(n) if n else 1
+        blas = max(n) if n else 1
     except Exception:
-        return os.cpu_count() or 1
+        pass
+    return omp, blas
 
 
 def cpu_sample(w, seconds):
@@ -249,30 +259,92 @@ def cpu_sample(w, seconds):
     return t_cg, t_outer, kind, reps
 
 
+def config_of(args, w):
+    """The workload description both arms print (the same keys and values)."""
+    kind_h = "hubbard" if w["hamiltonian"] == "hubbard" else "external"
+    return {"workload": args.workload, "nmo": w["nmo"], "nalpha": w["nalpha"], "nbeta": w["nbeta"],
+            "positivity": w["positivity"],
+            "hamiltonian": ({"hubbard_t_U": list(w["hubbard"])} if kind_h == "hubbard"
+                            else {"synthetic_df": w["df"]}),
+            "r_convergence": w["r_conv"], "e_convergence": w["e_conv"], "cg_convergence": w["cg_conv"],
+            "mu_update_frequency": w["muf"], "tpdm_guess": "RANDOM",
+            "parallelism": "replicas" if args.gpus > 1 else "single",
+            "l2": "flushed between steps (256 MiB write)"}
+
+
+def cpu_baseline(w, ref, seconds, steps=1):
+    """The CPU path timed on a bounded sample, scaled to the FP64 solve's
+    iteration counts (the CPU oracle's own solve, ref)."""
+    omp, blas = cpu_threads()
+    vals = []
+    for _ in range(steps):
+        t_cg, t_out, kind, reps = cpu_sample(w, seconds)
+        vals.append(t_cg * ref["cg_iterations"] + t_out * ref["outer_iterations"])
+    return {"value": statistics.mean(vals), "unit": "s", "cores": omp, "kind": kind,
+            "openmp_threads_maps": omp, "blas_threads": blas,
+            "sample": f"{reps[0]} CG iterations ({t_cg * 1e3:.2f} ms each) and {reps[1]} outer-iteration "
+                      f"bodies ({t_out * 1e3:.2f} ms each) timed on the host per step, scaled to the "
+                      f"{ref['cg_iterations']} CG + {ref['outer_iterations']} outer iterations of the CPU "
+                      f"oracle's FP64 solve to convergence",
+            "measured_full_solve": {"wall_s": ref.get("wall_s"), "omp_threads": ref.get("omp_threads"),
+                                    "where": "the build container's host cores (generator run)"}}
+
+
 def run_reference(args, w):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    oiter, iiter = FP64_ITERS.get(args.workload, (None, None))
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    ref = fp64_reference(args.workload)
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": f"no FP64 CPU solve fixture for {args.workload}"}))
+        return
+    # each step a bounded sample; the whole run stays within a few minutes
+    per_step = max(2.0, min(args.cpu_sample_seconds, 180.0 / max(1, args.warmup + args.steps)))
     vals = []
+    cb = None
     for k in range(args.warmup + args.steps):
-        t_cg, t_out, kind, reps = cpu_sample(w, max(2.0, args.cpu_sample_seconds / 3))
+        b = cpu_baseline(w, ref, per_step)
         if k >= args.warmup:
-            vals.append(t_cg * iiter + t_out * oiter if oiter else None)
-    total = statistics.mean(vals) if oiter else None
+            vals.append(b["value"])
+            cb = b
+    total = max(vals)
+    cb["value"] = total
     line = {"impl": "reference", "metric": METRIC, "value": total, "unit": "s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, **{k: v for k, v in w.items()},
-                       "fp64_outer_iterations": oiter, "fp64_cg_iterations": iiter,
-                       "parallelism": "replicas"},
-            "cpu_baseline": {"value": total, "unit": "s", "cores": cpu_threads(), "kind": kind,
-                             "sample": f"per step: {reps[0]} CG iterations ({t_cg*1e3:.2f} ms each) and "
-                                       f"{reps[1]} outer-iteration bodies ({t_out*1e3:.2f} ms each) timed, "
-                                       f"scaled to {iiter} CG + {oiter} outer iterations to convergence"},
+            "config": config_of(args, w),
+            "cpu_baseline": cb,
             "e2e": {"value": total, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def cusolver_projection_ms(p, dev, reps=5):
+    """Reference point for the plain FP64 path: one projection of the
+    problem's blocks by cuSOLVER's syevd (torch.linalg.eigh, the blocks of
+    each size batched) and U+ = V max(L, 0) V^T, ms per call."""
+    import torch
+    dims = [int(d) for d in p.dims]
+    by = {}
+    for d in dims:
+        by[d] = by.get(d, 0) + 1
+    mats = {d: torch.randn(k, d, d, dtype=torch.float64, device=dev) for d, k in by.items()}
+    mats = {d: 0.5 * (m + m.transpose(1, 2)) for d, m in mats.items()}
+
+    def once():
+        for m in mats.values():
+            lam, V = torch.linalg.eigh(m)
+            _ = (V * lam.clamp(min=0.0).unsqueeze(1)) @ V.transpose(1, 2)
+
+    once()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        once()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
 
 
 def run_b200(args, w):
@@ -298,21 +370,23 @@ def run_b200(args, w):
     dx0 = torch.from_numpy(x0).to(dev)
     dx = torch.empty_like(dx0)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    ref = fp64_reference(args.workload)
 
-    def one(profile=False):
+    def one():
         dx.copy_(dx0)
         flush.fill_(1.0)
         torch.cuda.synchronize()
         barrier(world)
-        st = p.solve_device(dx, db, dc, opts)
-        return st
+        return p.solve_device(dx, db, dc, opts)
 
     clk = ClockSampler(local).start()   # started before the warm-up: no fork in the timed region
     for _ in range(args.warmup):
         one()
     times, stats = [], None
     launches0 = p.kernel_launches()
-    p.set_profiling(True)
+    # kernel-class CUDA events only (level 1) in the timed steps: they give
+    # the CG kernel's launch time for the roofline at negligible cost
+    p.set_profiling(1)
     with clk:
         for _ in range(args.steps):
             dx.copy_(dx0)
@@ -328,10 +402,8 @@ def run_b200(args, w):
             torch.cuda.synchronize()
             times.append(ev0.elapsed_time(ev1) / 1e3)
     prof = p.profile()
-    phases = {"cg_kernel": {k: round(v, 1) for k, v in p.cg_profile().items()},
-              "projection": {k: [round(v[0], 1), v[1]] for k, v in p.projection_profile().items()}}
-    p.set_profiling(False)
     launches = p.kernel_launches() - launches0
+    p.set_profiling(0)
     t = max_over_ranks(max(times), world)
     energy = float(c @ dx.cpu().numpy())
 
@@ -346,11 +418,22 @@ def run_b200(args, w):
         e2e_times.append(time.perf_counter() - t0)
     te2e = max_over_ranks(max(e2e_times), world)
 
+    # one more solve with the phase timers on (level 2), outside the timed steps
+    phases = None
+    if world == 1:
+        p.set_profiling(2)
+        one()
+        phases = {"cg_kernel": {k: round(v, 1) for k, v in p.cg_profile().items()},
+                  "projection": {k: [round(v[0], 1), v[1]] for k, v in p.projection_profile().items()},
+                  "kernel_classes_ms": {k: round(v[0], 1) for k, v in p.profile().items()}}
+        p.set_profiling(0)
+
     # the plain FP64 path on the same problem (1 GPU only): every block fully
     # diagonalised by selective Jacobi every iteration, as libsdp does with LAPACK
     plain = None
     if world == 1 and not args.no_plain:
         p.set_projection_mode("jacobi")
+        p.set_profiling(1)
         dx.copy_(dx0)
         flush.fill_(1.0)
         torch.cuda.synchronize()
@@ -360,15 +443,24 @@ def run_b200(args, w):
         st_plain = p.solve_device(dx, db, dc, opts)
         ev1.record()
         torch.cuda.synchronize()
+        pprof = p.profile()
+        p.set_profiling(0)
         e_plain = float(c @ dx.cpu().numpy())
         p.set_projection_mode("refine")
-        plain = {"seconds": ev0.elapsed_time(ev1) / 1e3, "energy": e_plain,
+        sec = ev0.elapsed_time(ev1) / 1e3
+        cus = cusolver_projection_ms(p, dev)
+        proj_ms, proj_n = pprof["projection"]
+        plain = {"seconds": sec, "energy": e_plain,
                  "outer_iterations": st_plain["oiter"], "cg_iterations": st_plain["iiter"],
-                 "converged": st_plain["converged"]}
+                 "converged": st_plain["converged"],
+                 "projection_ms_per_call": proj_ms / max(proj_n, 1),
+                 "cusolver_syevd_projection_ms_per_call": cus,
+                 "seconds_with_cusolver_projection_estimate":
+                     sec - proj_ms / 1e3 + st_plain["oiter"] * cus / 1e3}
 
     # roofline: cg_kernel, the largest single kernel (the projection is a
     # sequence of GEMM-tile, test and Jacobi kernels; its FLOP rate is reported
-    # beside it)
+    # beside it).  Its launch time comes from the timed steps' CUDA events.
     oiter, iiter = stats["oiter"], stats["iiter"]
     npr, ndu = p.n_primal, p.n_dual
     nnz_a, nnz_t = p.operator_nnz()
@@ -380,15 +472,17 @@ def run_b200(args, w):
     hbm = peaks.get("hbm_gbs", 6650.0)
     ms_cg, n_cg = prof["cg_kernel"]
     m = iiter / max(oiter, 1)   # CG iterations per launch (one launch per outer iteration)
-    per_iter = 8.0 * (2 * npr + 7 * ndu) + 4.0 * (nnz_a + nnz_t + npr + ndu)
-    bytes_launch = (m + 1) * per_iter   # + the initial residual, one A^T and one A pass
+    # algorithmic bytes: vectors only (index tables excluded), per CG iteration
+    # one A and one A^T (read / write x and y once each) and ~5 CG vector streams
+    per_iter = 8.0 * (2 * npr + 7 * ndu)
+    bytes_launch = (m + 1) * per_iter   # + the initial residual's A^T and A pass
     ach = bytes_launch / (ms_cg / n_cg / 1e3) / 1e9
     roof = {"kernel": "cg_kernel", "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
             "frac": ach / hbm, "traffic": None,
-            "algorithmic_bytes": "per CG iteration 8 (2 n_p + 7 n_d) vector bytes + 4 (nnz(A) + "
-                                 "nnz(A^T) + n_p + n_d) operator-table bytes; (m + 1) iterations "
-                                 f"per launch, m = {m:.1f}",
-            "peak_source": ("MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s")}
+            "algorithmic_bytes": "per CG iteration 8 (2 n_p + 7 n_d) vector bytes (index tables "
+                                 f"excluded); (m + 1) iterations per launch, m = {m:.1f}",
+            "peak_source": ("MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s") + " (of measured)",
+            "launch_ms": ms_cg / max(n_cg, 1)}
     ms_pj, n_pj = prof["projection"]
     flops = sum((16.0 / 3.0) * float(d) ** 3 for d in p.dims)
     roof["projection"] = {"ms_per_call": ms_pj / max(n_pj, 1),
@@ -398,43 +492,33 @@ def run_b200(args, w):
                                   "counted as for LAPACK), FP64; no FP64 peak is measured"}
     tot = sum(x[0] for x in prof.values())
     roof["kernel_ms_share"] = {k: round(v[0] / tot, 4) for k, v in prof.items()}
-    # ms per part of the timed solve: the CG kernel's phases barrier to barrier
-    # (its own clock), the projection's phases as [ms, launches or calls]
     roof["phases_ms"] = phases
 
     cpu = None
-    if rank == 0 and world == 1 and args.cpu_sample_seconds > 0:
-        t_cg, t_out, kind, reps = cpu_sample(w, args.cpu_sample_seconds)
-        cpu = {"value": t_cg * iiter + t_out * oiter, "unit": "s", "cores": cpu_threads(),
-               "kind": kind,
-               "sample": f"{reps[0]} CG iterations ({t_cg*1e3:.2f} ms each) and {reps[1]} "
-                         f"outer-iteration bodies ({t_out*1e3:.2f} ms each) timed on the host, "
-                         f"scaled to the {iiter} CG + {oiter} outer iterations of the device solve"}
+    if rank == 0 and world == 1 and args.cpu_sample_seconds > 0 and ref is not None:
+        cpu = cpu_baseline(w, ref, args.cpu_sample_seconds)
     clocks = clk.summary()
     if rank == 0:
+        cfg = config_of(args, w)
+        fp64_e = ref["energy"] if ref else None
+        cfg.update({"n_primal": npr, "n_dual": ndu, "block_dims": sorted(set(int(d) for d in p.dims)),
+                    "outer_iterations": oiter, "cg_iterations": iiter,
+                    "energy": energy, "converged": stats["converged"],
+                    "fp64_energy": fp64_e,
+                    "fp64_energy_source": ("CPU oracle FP64 solve (hilbert's compiled maps + numpy "
+                                           "boundary-point restatement), tests/golden/fp64_"
+                                           f"{args.workload}.json") if ref else None,
+                    "fp64_outer_iterations": ref["outer_iterations"] if ref else None,
+                    "abs_dE_vs_fp64": abs(energy - fp64_e) if ref else None,
+                    "plain_fp64_path": plain,
+                    "speedup_vs_plain_fp64": (plain["seconds"] / t) if plain else None,
+                    "abs_dE_vs_plain_fp64": abs(energy - plain["energy"]) if plain else None,
+                    "projection_refine_counts": p.refine_counts(),
+                    "max_outer_cap": args.max_outer or None})
         line = {"metric": METRIC, "value": t, "unit": "s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": args.workload, "nmo": w["nmo"], "nalpha": w["nalpha"],
-                           "nbeta": w["nbeta"], "positivity": w["positivity"],
-                           "hamiltonian": ({"hubbard_t_U": list(w["hubbard"])} if kind_h == "hubbard"
-                                           else {"synthetic_df": w["df"]}),
-                           "r_convergence": w["r_conv"],
-                           "e_convergence": w["e_conv"], "cg_convergence": w["cg_conv"],
-                           "mu_update_frequency": w["muf"], "n_primal": npr, "n_dual": ndu,
-                           "block_dims": sorted(set(int(d) for d in p.dims)),
-                           "parallelism": "replicas" if world > 1 else "single",
-                           "l2": "flushed between steps (256 MiB write)",
-                           "outer_iterations": oiter, "cg_iterations": iiter,
-                           "energy": energy, "converged": stats["converged"],
-                           "fp64_energy": FP64_ENERGY[args.workload][0],
-                           "fp64_energy_source": FP64_ENERGY[args.workload][1],
-                           "abs_dE_vs_fp64": abs(energy - FP64_ENERGY[args.workload][0]),
-                           "plain_fp64_path": plain,
-                           "speedup_vs_plain_fp64": (plain["seconds"] / t) if plain else None,
-                           "abs_dE_vs_plain_fp64": abs(energy - plain["energy"]) if plain else None,
-                           "projection_refine_counts": p.refine_counts(),
-                           "max_outer_cap": args.max_outer or None},
+                "config": cfg,
                 "e2e": {"value": te2e, "unit": "s", "h2d_bytes_per_step": 8 * (2 * npr + ndu),
                         "d2h_bytes_per_step": 8 * npr},
                 "gpu_launches": int(launches),

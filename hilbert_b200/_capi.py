@@ -46,7 +46,7 @@ EXPORTS = (
     "v2b_problem_cg_profile",
     "v2b_problem_pack_spatial_density", "v2b_project_block_noalloc",
     "v2b_problem_rdm_counts", "v2b_problem_rdm_records", "v2b_problem_set_state", "v2b_problem_continue",
-    "v2b_problem_set_wait_limit",
+    "v2b_problem_set_wait_limit", "v2b_df_transform", "v2b_df_transform_adjoint",
     "v2b_doci_v2rdm_layout", "v2b_batch_problem_create", "v2b_problem_palette",
     "v2b_problem_tpdm_iwl_records", "v2b_problem_d3_counts", "v2b_problem_d3_records",
 )
@@ -139,6 +139,8 @@ def load(path=LIB_PATH):
         "v2b_problem_set_state": (ctypes.c_int, [vp, ctypes.c_double, dp, dp]),
         "v2b_problem_continue": (ctypes.c_int, [vp]),
         "v2b_problem_set_wait_limit": (ctypes.c_int, [vp, ctypes.c_longlong]),
+        "v2b_df_transform": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, ctypes.c_int, vp]),
+        "v2b_df_transform_adjoint": (ctypes.c_int, [vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, vp]),
         "v2b_doci_v2rdm_layout": (ctypes.c_int, [vp, vp, vp, lp]),
         "v2b_batch_problem_create": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(vp)]),
         "v2b_problem_palette": (ctypes.c_int, [vp, ctypes.c_int, vp, ip]),

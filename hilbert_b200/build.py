@@ -15,9 +15,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libv2rdm_b200.so")
 SOURCES = ["v2rdm_problem.cpp", "doci_problem.cpp", "rdm_records.cpp", "batch_problem.cpp", "v2b_kernels.cu", "v2b_eig.cu", "v2b_bigjacobi.cu", "v2b_refine.cu",
-           "v2b_orbital.cu", "v2b_solver.cu", "v2b_noalloc.cu"]
+           "v2b_orbital.cu", "v2b_transform.cu", "v2b_solver.cu", "v2b_noalloc.cu"]
 HEADERS = ["v2rdm_problem.h", "doci_problem.h", "rdm_records.h", "v2b_kernels.cuh", "v2b_device.cuh", "v2b_eig.cuh", "v2b_bigjacobi.cuh",
-           "v2b_refine.cuh", "v2b_orbital.cuh"]
+           "v2b_refine.cuh", "v2b_orbital.cuh", "v2b_transform.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -43,7 +43,8 @@ struct CgParams {
     const double *Ax, *Acz, *b;     // rhs = Acz + mu (b - Ax)
     double mu;
     double *y, *r, *p0, *p1, *t, *q;
-    double *partials;               // >= 2 * gridDim.x (r.r partials, then p.q partials)
+    double2 *rp0, *rp1;             // cg_fused_kernel: (r, p) pairs, double-buffered
+    double *partials;               // >= 4 * gridDim.x (r.r partials, then p.q [, r.q, q.q] partials)
     GridBarrier *bar;
     int *status;
     long long spin_limit;
@@ -66,6 +67,7 @@ __global__ void spmv_AT_U_kernel(const uint32_t *__restrict__ rp,
                                  const double *__restrict__ c, double mu,
                                  double *__restrict__ ATy, double *__restrict__ U, Palette pal);
 __global__ void cg_kernel(CgParams P);
+__global__ void cg_fused_kernel(CgParams P);
 __global__ void stats_kernel(const double *__restrict__ Ax, const double *__restrict__ b,
                              const double *__restrict__ ATy, const double *__restrict__ z,
                              const double *__restrict__ c, const double *__restrict__ x,

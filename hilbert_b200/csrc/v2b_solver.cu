@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -1026,6 +1027,10 @@ struct v2b_problem {
     double *x = nullptr, *b = nullptr, *c = nullptr, *y = nullptr, *z = nullptr;
     double *Ax = nullptr, *Acz = nullptr, *ATy = nullptr, *U = nullptr;
     double *r = nullptr, *p0 = nullptr, *p1 = nullptr, *t = nullptr, *q = nullptr;
+    double2 *rpbuf = nullptr;   // cg_fused_kernel's two (r, p) pair buffers
+    // conjugate-gradient kernel: 1 fused (cg_fused_kernel, two grid barriers
+    // per iteration), 0 classic (cg_kernel, three)
+    int cg_variant = 1;
     double *partials = nullptr, *cg_out = nullptr, *stats = nullptr, *stats_partials = nullptr;
     unsigned int *stats_counter = nullptr;
     v2b::GridBarrier *bar = nullptr;
@@ -1048,6 +1053,7 @@ struct v2b_problem {
     // CG phases, summed by the kernel's own clock: initial residual, A^T p, A t, update
     static constexpr int kCgPhases = 4;
     unsigned long long *cg_phase = nullptr;
+    bool phases = false;   // profiling level 2
     void mark(int cls, int edge) {
         if (profiling) V2B_CK(cudaEventRecord(ev[2 * cls + edge], stream));
     }
@@ -1061,14 +1067,18 @@ struct v2b_problem {
             prof_n[k] += 1;
         }
     }
-    void set_profiling(bool on) {
+    // level 0 off; 1 CUDA events around each kernel class; 2 also the
+    // projection's phases and the CG kernel's own phase clock
+    void set_profiling(int level) {
+        const bool on = level > 0;
         if (on && !ev[0])
             for (auto &e : ev) V2B_CK(cudaEventCreate(&e));
-        if (on && !cg_phase) cg_phase = dalloc<unsigned long long>(kCgPhases);
+        if (level > 1 && !cg_phase) cg_phase = dalloc<unsigned long long>(kCgPhases);
         if (cg_phase) V2B_CK(cudaMemset(cg_phase, 0, kCgPhases * sizeof(unsigned long long)));
         profiling = on;
+        phases = level > 1;
         for (int k = 0; k < kClasses; k++) { prof_ms[k] = 0.0; prof_n[k] = 0; }
-        plan.prof = on;
+        plan.prof = level > 1;
         plan.pev_used = 0;
         for (int k = 0; k < ProjectPlan::kPhases; k++) { plan.ph_ms[k] = 0.0; plan.ph_n[k] = 0; }
     }
@@ -1088,6 +1098,7 @@ struct v2b_problem {
         cudaFree(ibas_aa_dev);
         cudaFree(status);
         if (nonfinite) cudaFree(nonfinite);
+        if (rpbuf) cudaFree(rpbuf);
         if (h_readback) cudaFreeHost(h_readback);
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
@@ -1122,16 +1133,18 @@ struct v2b_problem {
         ATy = dalloc<double>(np); U = dalloc<double>(np); t = dalloc<double>(np);
         b = dalloc<double>(nd); y = dalloc<double>(nd); Ax = dalloc<double>(nd);
         Acz = dalloc<double>(nd); r = dalloc<double>(nd); p0 = dalloc<double>(nd);
-        p1 = dalloc<double>(nd); q = dalloc<double>(nd);
+        p1 = dalloc<double>(nd); q = dalloc<double>(nd); rpbuf = dalloc<double2>(2 * (size_t)nd);
+        if (const char *v = std::getenv("V2B_CG_VARIANT")) cg_variant = std::atoi(v) == 0 ? 0 : 1;
         int per_sm = 0;
-        V2B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v2b::cg_kernel,
-                                                             v2b::kCgThreads, 0));
+        V2B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, cg_variant ? (const void *)v2b::cg_fused_kernel : (const void *)v2b::cg_kernel,
+            v2b::kCgThreads, 0));
         if (per_sm < 1) throw Failure(V2B_INTERNAL, "cg_kernel cannot be resident");
         // small problems: fewer CTAs make the grid barrier cheaper
         const int64_t rows = std::max(prob.n_primal, prob.n_dual);
         const int64_t want = (rows + (int64_t)v2b::kCgThreads - 1) / (int64_t)v2b::kCgThreads;
         cg_grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sm_count() * per_sm));
-        partials = dalloc<double>(2 * (size_t)cg_grid);
+        partials = dalloc<double>(4 * (size_t)cg_grid);
         stats_partials = dalloc<double>(4 * v2b::kStatsBlocks);
         cg_out = dalloc<double>(2);
         stats = dalloc<double>(4);
@@ -1177,13 +1190,15 @@ struct v2b_problem {
         P.np = prob.n_primal; P.nd = prob.n_dual;
         P.Ax = Ax; P.Acz = Acz; P.b = b; P.mu = mu;
         P.y = y; P.r = r; P.p0 = p0; P.p1 = p1; P.t = t; P.q = q;
+        P.rp0 = rpbuf; P.rp1 = rpbuf + prob.n_dual;
         P.partials = partials; P.bar = bar; P.status = status;
         P.spin_limit = wait_limit;
         P.tol = tol; P.maxit = maxit; P.out = cg_out;
-        P.phase_ns = profiling ? cg_phase : nullptr;
+        P.phase_ns = (profiling && phases) ? cg_phase : nullptr;
         void *args[] = {&P};
-        V2B_CK(cudaLaunchCooperativeKernel((const void *)v2b::cg_kernel, dim3(cg_grid),
-                                           dim3(v2b::kCgThreads), args, 0, stream));
+        V2B_CK(cudaLaunchCooperativeKernel(
+            cg_variant ? (const void *)v2b::cg_fused_kernel : (const void *)v2b::cg_kernel, dim3(cg_grid),
+            dim3(v2b::kCgThreads), args, 0, stream));
         launches++;
     }
 
@@ -1754,7 +1769,7 @@ int v2b_problem_set_profiling(v2b_problem *p, int on) {
     return guarded([&] {
         if (!p) throw std::invalid_argument("set_profiling: NULL problem");
         p->setup();
-        p->set_profiling(on != 0);
+        p->set_profiling(on < 0 ? 0 : on);
         return V2B_OK;
     });
 }

@@ -75,15 +75,62 @@ def full_densities(D_act, G_act, ncore, nvirt=0):
     return D, G
 
 
+def _dptr(t):
+    import ctypes
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def df_transform(U, B):
+    """B'_Q = U^T B_Q U for every Q of B (count x n x n): focas's DF integral
+    transform (orbopt_integraltransform_cpu.cc:235-261).  CUDA tensors run
+    the library's FP64 tensor-core kernel (v2b_df_transform); CPU tensors
+    evaluate the same products in torch."""
+    if not U.is_cuda:
+        return U.T @ B @ U
+    from . import _capi
+    lib = _capi.load()
+    n, count = U.shape[0], B.shape[0]
+    U = U.contiguous()
+    B = B.contiguous()
+    out = torch.empty_like(B)
+    _capi.check(lib.v2b_df_transform(_dptr(U), _dptr(B), _dptr(out), n, count,
+                                     _dptr_stream(U.device)))
+    return out
+
+
+def df_transform_adjoint(U, B, M):
+    """sum_Q (B_Q U M_Q^T + B_Q^T U M_Q): the U-gradient of
+    sum_Q <M_Q, U^T B_Q U>.  CUDA tensors run v2b_df_transform_adjoint."""
+    if not U.is_cuda:
+        return (B @ U @ M.transpose(1, 2)).sum(0) + (B.transpose(1, 2) @ U @ M).sum(0)
+    from . import _capi
+    lib = _capi.load()
+    n, count = U.shape[0], B.shape[0]
+    U, B, M = U.contiguous(), B.contiguous(), M.contiguous()
+    dU = torch.empty_like(U)
+    work = torch.empty_like(B)
+    _capi.check(lib.v2b_df_transform_adjoint(_dptr(U), _dptr(B), _dptr(M), _dptr(dU), _dptr(work), n,
+                                             count, _dptr_stream(U.device)))
+    return dU
+
+
+def _dptr_stream(device):
+    import ctypes
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
 class RotatedEnergy(torch.autograd.Function):
-    """E(kappa) for U = exp(kappa); backward by the hand-written adjoint."""
+    """E(kappa) for U = exp(kappa); backward by the hand-written adjoint.
+    The integral transforms h' = U^T h U, B'_Q = U^T B_Q U and their adjoint
+    run in the library's kernels for CUDA tensors (df_transform,
+    df_transform_adjoint); the 2-RDM contraction b' Gm is a plain GEMM."""
 
     @staticmethod
     def forward(ctx, kappa, h, B, D, Gm):
         n = h.shape[0]
         U = torch.linalg.matrix_exp(kappa)
-        hp = U.T @ h @ U
-        Bp = U.T @ B @ U                      # (naux, n, n), one GEMM pair per Q
+        hp = df_transform(U, h.unsqueeze(0))[0]
+        Bp = df_transform(U, B)               # (naux, n, n), one matrix per CTA
         b = Bp.reshape(B.shape[0], n * n)
         Gb = b @ Gm                           # rows: (Gm b'_Q)^T, Gm symmetric
         E = (hp * D).sum() + 0.5 * (Gb * b).sum()
@@ -95,8 +142,8 @@ class RotatedEnergy(torch.autograd.Function):
         kappa, h, B, D, U, Gb = ctx.saved_tensors
         n = h.shape[0]
         M = Gb.reshape(B.shape[0], n, n)      # dE/dB'^Q
-        dU = h @ U @ D.T + h.T @ U @ D
-        dU = dU + (B @ U @ M.transpose(1, 2)).sum(0) + (B.transpose(1, 2) @ U @ M).sum(0)
+        dU = df_transform_adjoint(U, h.unsqueeze(0), D.unsqueeze(0))   # h U D^T + h^T U D
+        dU = dU + df_transform_adjoint(U, B, M)
         Z = torch.zeros((2 * n, 2 * n), dtype=kappa.dtype, device=kappa.device)
         Z[:n, :n] = kappa.T
         Z[n:, n:] = kappa.T
@@ -325,8 +372,8 @@ def optimize_orbitals_focas(h, B, Da, Ga, ncore, nact, maxiter=10, g_conv=1e-4, 
     def rotate(k):
         nonlocal h, B, Utot
         U = torch.linalg.matrix_exp(_pair_kappa(k, pairs, nmo))
-        h = U.T @ h @ U
-        B = U.T @ B @ U
+        h = df_transform(U, h.unsqueeze(0))[0]
+        B = df_transform(U, B)
         Utot = Utot @ U
 
     def energy():
@@ -449,8 +496,8 @@ def casscf(h, B, ncore, nact, solve_active, macro_iterations=None, active_active
             D, G = full_densities(Da, Ga, ncore, nvirt)
             U, e_final, g_first, g_last = optimize_orbitals(h, B, D, G, pairs)
         gnorms.append(g_first)
-        h = U.T @ h @ U
-        B = U.T @ B @ U
+        h = df_transform(U, h.unsqueeze(0))[0]
+        B = df_transform(U, B)
         rounds += 1
         orb_conv = (g_conv is not None and e_conv is not None
                     and abs(e_final - energies[-1]) < e_conv and abs(g_last) < g_conv)

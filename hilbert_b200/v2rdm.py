@@ -285,7 +285,9 @@ class V2RDMProblem:
                       "stats_kernel")
 
     def set_profiling(self, on=True):
-        check(self._lib.v2b_problem_set_profiling(self._h, int(bool(on))))
+        """on: False/0 off, True/1 CUDA events per kernel class, 2 also the
+        CG and projection phases."""
+        check(self._lib.v2b_problem_set_profiling(self._h, int(on)))
 
     def profile(self):
         """{kernel: (total_ms, launches)} from CUDA events on the library's stream"""

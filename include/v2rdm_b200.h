@@ -238,16 +238,20 @@ int v2b_problem_operator(const v2b_problem *p, int transposed, uint32_t *row_ptr
 long v2b_problem_kernel_launches(const v2b_problem *p);
 /* CUDA-event timing of each kernel class of the device iteration, recorded on
  * the library's stream: 0 cg_kernel, 1 spmv_AT_U_kernel, 2 jacobi_project_kernel,
- * 3 spmv_A2_kernel, 4 stats_kernel.  set_profiling resets the totals. */
+ * 3 spmv_A2_kernel, 4 stats_kernel.  set_profiling resets the totals; on =
+ * 0 off, 1 the kernel classes only, 2 also the phases below (the CG kernel's
+ * phase clock and the projection's per-phase events cost some time). */
 int v2b_problem_set_profiling(v2b_problem *p, int on);
-/* with profiling on: CUDA-event time of the projection's phases, the first
+/* with profiling level 2: CUDA-event time of the projection's phases, the first
  * count of: [0] GEMM tiles, [1] acceptance test, [2] clusters + Newton step,
  * [3] block-Jacobi sweeps, [4] Jacobi kernels (no reference counterpart) */
 int v2b_problem_projection_profile(const v2b_problem *p, double *ms, long *n, int count);
-/* with profiling on: milliseconds of the CG kernel's phases, barrier to
+/* with profiling level 2: milliseconds of the CG kernel's phases, barrier to
  * barrier on the kernel's own clock, the first count of: [0] initial
- * residual, [1] A^T p and the new direction, [2] A t and p.q, [3] the r
- * update and r.r (no reference counterpart) */
+ * residual, [1] the update of y, r, p fused with the A^T gather of the new
+ * direction, [2] A t and its dot products, [3] 0 (a separate update pass of
+ * the classic three-barrier kernel, selected by V2B_CG_VARIANT=0 in the
+ * environment) (no reference counterpart) */
 int v2b_problem_cg_profile(const v2b_problem *p, double *ms, int count);
 int v2b_problem_profile(const v2b_problem *p, double *ms /* [5] */, long *launches /* [5] */);
 /* the cudaStream_t the device solve runs on (after the first device call) */
@@ -326,6 +330,21 @@ typedef struct {
 int v2b_problem_d3_counts(const v2b_problem *p, long *counts);
 int v2b_problem_d3_records(const v2b_problem *p, int ncore, const double *x, v2b_dm3_record *d3aaa,
                            v2b_dm3_record *d3aab, v2b_dm3_record *d3bba, v2b_dm3_record *d3bbb);
+
+/* ---- 2c. the orbital step's integral transform -------------------------------- */
+
+/* focas's density-fitted integral transform (OrbitalOptimizer::TransformTei_Q,
+ * src/focas/C_files/orbopt_integraltransform_cpu.cc:235-261, and
+ * TransformOei, :263-285, for count = 1): d_Bp[Q] = U^T d_B[Q] U for
+ * Q = 0 .. count-1, n x n row-major matrices in device memory, on FP64
+ * tensor cores, one matrix per CTA.  n <= 80, else V2B_BAD_ARG. */
+int v2b_df_transform(const double *d_U, const double *d_B, double *d_Bp, int n, int count, void *stream);
+/* No counterpart in the reference (focas has no derivative with respect to
+ * U).  The adjoint of the transform: d_dU = sum_Q (B_Q U M_Q^T + B_Q^T U M_Q),
+ * the gradient of sum_Q <M_Q, U^T B_Q U> with respect to U, summed over Q in
+ * order.  d_work: count * n * n doubles of scratch.  n <= 80. */
+int v2b_df_transform_adjoint(const double *d_U, const double *d_B, const double *d_M, double *d_dU,
+                             double *d_work, int n, int count, void *stream);
 
 /* ---- 3. allocation-free projection ------------------------------------------ */
 

@@ -1,6 +1,11 @@
 import os
 import sys
 
+# The oracle's compiled reference maps use OpenMP; the test problems are
+# small, and a parallel region per map loop across every core of a large
+# host costs more than it saves.  Set before any library loads libgomp.
+os.environ.setdefault("OMP_NUM_THREADS", "4")
+
 import numpy as np
 import pytest
 

@@ -112,3 +112,30 @@ def test_df_casscf_on_hilbert_schedule(cuda_device):
     assert not solve.exhausted
     assert E[-1] < E[0] - 1e-2
     assert gn[-1] < 0.1 * gn[0]
+
+
+@pytest.mark.parametrize("n,count", [(40, 160), (13, 7), (80, 3), (1, 2)])
+def test_df_transform_kernels_match_torch(cuda_device, n, count):
+    """The library's FP64 tensor-core transform B'_Q = U^T B_Q U and its
+    adjoint sum_Q (B_Q U M_Q^T + B_Q^T U M_Q) against torch's FP64 GEMMs, to
+    1e-13 relative (the products differ only in summation order)."""
+    import torch
+    g = torch.Generator().manual_seed(n * 1000 + count)
+    U = torch.linalg.qr(torch.randn(n, n, generator=g, dtype=torch.float64))[0].to(cuda_device)
+    B = torch.randn(count, n, n, generator=g, dtype=torch.float64).to(cuda_device)
+    M = torch.randn(count, n, n, generator=g, dtype=torch.float64).to(cuda_device)
+    Bp = ho.df_transform(U, B)
+    ref = U.T @ B @ U
+    assert torch.allclose(Bp, ref, rtol=0, atol=1e-13 * float(ref.abs().max()))
+    dU = ho.df_transform_adjoint(U, B, M)
+    ref = (B @ U @ M.transpose(1, 2)).sum(0) + (B.transpose(1, 2) @ U @ M).sum(0)
+    assert torch.allclose(dU, ref, rtol=0, atol=1e-13 * float(ref.abs().max()) * count)
+
+
+def test_df_transform_rejects_too_many_orbitals(cuda_device):
+    import torch
+    from hilbert_b200 import _capi
+    U = torch.eye(81, dtype=torch.float64, device=cuda_device)
+    with pytest.raises(_capi.V2BError) as e:
+        ho.df_transform(U, U.unsqueeze(0))
+    assert e.value.code == _capi.V2B_BAD_ARG and "at most 80" in str(e.value)

@@ -155,7 +155,7 @@ def test_profiling_timers_leave_the_solve_unchanged(cuda_device):
     opts = hb.Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6, "MAXITER": 60,
                        "MU_UPDATE_FREQUENCY": 20})
     runs = []
-    for on in (False, True):
+    for on in (0, 2):
         p = hb.V2RDMProblem(6, 3, 3, hubbard_multiplicity=True)
         p.set_profiling(on)
         x, st = p.solve(p.guess("RANDOM"), p.b(), p.c_hubbard(1.0, 4.0), opts)
@@ -165,7 +165,8 @@ def test_profiling_timers_leave_the_solve_unchanged(cuda_device):
     classes, cg, phases = p.profile(), p.cg_profile(), p.projection_profile()
     assert classes["cg_kernel"][1] == 60
     assert all(v >= 0.0 for v in cg.values())
-    assert cg["transpose_gather"] > 0.0 and cg["gather_dot"] > 0.0 and cg["update"] > 0.0
+    # the fused CG kernel applies the update inside its transpose-gather pass
+    assert cg["transpose_gather"] > 0.0 and cg["gather_dot"] > 0.0 and cg["update"] >= 0.0
     # barrier-to-barrier phases lie inside the kernels' event-timed span
     assert sum(cg.values()) <= 1.05 * classes["cg_kernel"][0] + 0.5
     assert phases["gemm"][1] > 0
