@@ -48,6 +48,9 @@ WORKLOADS = {
     "hubbard8": dict(nmo=8, nalpha=4, nbeta=4, positivity="DQG", hamiltonian="hubbard",
                      hubbard=(1.0, 4.0), hubbard_multiplicity=True,
                      r_conv=1e-6, e_conv=1e-6, cg_conv=1e-9, muf=500, maxiter=400000),
+    # config 3: 64 independent DQG rings (L 6..14, N in {L-2, L, L+2}, U/t ~ U[1, 8], seed 3)
+    "batch64": dict(kind="batch", count=64, seed=3, positivity="DQG", r_conv=1e-6, e_conv=1e-6,
+                    cg_conv=1e-9, muf=500, maxiter=400000, concurrency=16),
 }
 # FP64 reference of each workload: the CPU oracle's converged solve, hilbert's
 # compiled maps (oracle/_ref) driven by the numpy boundary-point restatement
@@ -529,11 +532,109 @@ def run_b200(args, w):
         dist.destroy_process_group()
 
 
+def run_batch(args, w):
+    """Config 3: the 64-ring batch on one GPU.  Every instance keeps its own
+    problem, stream, penalty and convergence test (its result is the one it
+    gets alone); `concurrency` host threads drive the instances at once, so
+    the GPU runs many small solves side by side.  ``value``: inputs already
+    in device memory; ``e2e``: host arrays through the public solve().  Both
+    are device-synchronised wall clocks around the whole batch (the work
+    spans many streams).  The four smallest instances are also timed one at a
+    time and four at once, beside it."""
+    import numpy as np
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+
+    import hilbert_b200 as hb
+    from hilbert_b200.batch import hubbard_batch
+    world, rank, local = dist_setup()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    opts = hb.Options({"R_CONVERGENCE": w["r_conv"], "E_CONVERGENCE": w["e_conv"],
+                       "CG_CONVERGENCE": w["cg_conv"], "MAXITER": args.max_outer or w["maxiter"],
+                       "MU_UPDATE_FREQUENCY": w["muf"]})
+    insts = hubbard_batch(count=w["count"], seed=w["seed"], positivity=w["positivity"])
+    built = [i.problem() for i in insts]
+    x0 = [p.guess("RANDOM") for p, _, _ in built]
+    dev_in = [(torch.from_numpy(b).to(dev), torch.from_numpy(c).to(dev)) for _, b, c in built]
+
+    def init():
+        torch.cuda.set_device(dev)
+
+    def device_one(k):
+        p = built[k][0]
+        x = torch.from_numpy(x0[k]).to(dev)
+        st = p.solve_device(x, dev_in[k][0], dev_in[k][1], opts)
+        return float(built[k][2] @ x.cpu().numpy()), st
+
+    def host_one(k):
+        p, b, c = built[k]
+        xh, st = p.solve(x0[k], b, c, opts)
+        return float(c @ xh), st
+
+    def timed(fn, idx, workers):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=workers, initializer=init) as pool:
+            out = list(pool.map(fn, idx))
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, out
+
+    order = sorted(range(len(insts)), key=lambda k: -insts[k].cost())   # longest first
+    k_conc = int(w["concurrency"])
+    small = order[-4:]
+    for _ in range(args.warmup):   # warm-up: the four smallest instances at once
+        timed(device_one, small, 4)
+    launches0 = sum(p.kernel_launches() for p, _, _ in built)
+    times, res = [], None
+    for _ in range(args.steps):
+        t, res = timed(device_one, order, k_conc)
+        times.append(t)
+    launches = sum(p.kernel_launches() for p, _, _ in built) - launches0
+    t = max(times)
+    te2e, res_h = timed(host_one, order, k_conc)
+    # the same four instances one at a time and at once (the smallest four,
+    # to keep the sequential leg short)
+    t_seq4, _ = timed(device_one, small, 1)
+    t_conc4, _ = timed(device_one, small, 4)
+    energies = {k: e for k, (e, _) in zip(order, res)}
+    energies_h = {k: e for k, (e, _) in zip(order, res_h)}
+    conv = sum(bool(st["converged"]) for _, st in res)
+    if rank == 0:
+        cfg = {"workload": args.workload, "instances": len(insts), "seed": w["seed"],
+               "positivity": w["positivity"], "sites": [i.sites for i in insts],
+               "electrons": [i.electrons for i in insts], "U_over_t": [round(i.U, 4) for i in insts],
+               "r_convergence": w["r_conv"], "e_convergence": w["e_conv"], "cg_convergence": w["cg_conv"],
+               "mu_update_frequency": w["muf"], "concurrency": k_conc, "converged": conv,
+               "outer_iterations_max": max(int(st["oiter"]) for _, st in res),
+               "max_abs_dE_device_vs_host_arrays": max(abs(energies[k] - energies_h[k]) for k in energies),
+               "smallest4_sequential_s": t_seq4, "smallest4_concurrent_s": t_conc4,
+               "smallest4_speedup": t_seq4 / t_conc4,
+               "parallelism": "single", "timing": "device-synchronised wall clock (many streams)"}
+        line = {"metric": METRIC, "value": t, "unit": "s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": cfg,
+                "e2e": {"value": te2e, "unit": "s",
+                        "h2d_bytes_per_step": int(sum(8 * (2 * p.n_primal + p.n_dual) for p, _, _ in built)),
+                        "d2h_bytes_per_step": int(sum(8 * p.n_primal for p, _, _ in built))},
+                "gpu_launches": int(launches), "roofline": None, "cpu_baseline": None}
+        print(json.dumps(line), flush=True)
+    for p, _, _ in built:
+        p.close()
+
+
 def main():
     args = parse()
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
+        if w.get("kind") == "batch":
+            print(json.dumps({"impl": "reference", "unavailable": "the batch workload has no CPU arm; "
+                                                                 "time its instances as hubbard rings"}))
+            return
         run_reference(args, w)
+    elif w.get("kind") == "batch":
+        run_batch(args, w)
     else:
         run_b200(args, w)
 

@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kCgThreads, 3) cg_kernel(CgParams P) {
     };
 
     // r = rhs - A A^T y
-    for (int64_t sl = gwarp; sl < P.st.nslices; sl += nwarps) {
+    for (int64_t sl = P.st.split[gwarp], se = P.st.split[gwarp + 1]; sl < se; sl++) {
         uint32_t row;
         const double v = sell_row<false>(P.st, sl, lane, P.y, nullptr, 0.0, palT, row);
         if (row != 0xffffffffu) P.t[row] = v;
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(kCgThreads, 3) cg_kernel(CgParams P) {
     }
     if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
     double loc = 0.0;
-    for (int64_t sl = gwarp; sl < P.sa.nslices; sl += nwarps) {
+    for (int64_t sl = P.sa.split[gwarp], se = P.sa.split[gwarp + 1]; sl < se; sl++) {
         uint32_t row;
         const double av = sell_row<false>(P.sa, sl, lane, P.t, nullptr, 0.0, palA, row);
         if (row != 0xffffffffu) {
@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(kCgThreads, 3) cg_kernel(CgParams P) {
     double *pnew = P.p0;
     bool done = !(sqrt(rs) >= P.tol);
     while (!done && it < P.maxit) {
-        for (int64_t sl = gwarp; sl < P.st.nslices; sl += nwarps) {
+        for (int64_t sl = P.st.split[gwarp], se = P.st.split[gwarp + 1]; sl < se; sl++) {
             uint32_t row;
             const double v = sell_row<true>(P.st, sl, lane, P.r, pold, beta, palT, row);
             if (row != 0xffffffffu) P.t[row] = v;
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(kCgThreads, 3) cg_kernel(CgParams P) {
                 loc += pnew[j] * q;
             }
         }
-        for (int64_t sl = gwarp; sl < P.sa.nslices; sl += nwarps) {
+        for (int64_t sl = P.sa.split[gwarp], se = P.sa.split[gwarp + 1]; sl < se; sl++) {
             uint32_t row;
             const double q = sell_row<false>(P.sa, sl, lane, P.t, nullptr, 0.0, palA, row);
             if (row != 0xffffffffu) {
@@ -266,218 +266,6 @@ __global__ void __launch_bounds__(kCgThreads, 3) cg_kernel(CgParams P) {
         double *tmp = (pnew == P.p0) ? P.p1 : P.p0;
         pold = pnew;
         pnew = tmp;
-    }
-    if (gtid == 0) {
-        P.out[0] = (double)it;
-        P.out[1] = sqrt(rs);
-    }
-}
-
-// ----------------------------------------------------------- fused CG
-// The Aᵀ gather of a direction p' = r' + beta p with r' = r - alpha q,
-// formed per operand from the pair (r, p) and q exactly as the owner of
-// that row forms it (same operations, same rounding), so the gathered
-// operand equals the stored one bit for bit.
-__device__ __forceinline__ double fused_dir(double2 rp, double q, double alpha, double beta) {
-    const double rn = __dsub_rn(rp.x, __dmul_rn(alpha, q));
-    return __dadd_rn(rn, __dmul_rn(beta, rp.y));
-}
-
-__device__ __forceinline__ double sell_row_fused(const SellOp &S, int64_t sl, int lane,
-                                                 const double2 *__restrict__ rp, const double *__restrict__ q,
-                                                 double alpha, double beta, const double *pal, uint32_t &row) {
-    const int64_t pos = sl * 32 + lane;
-    row = __ldcs(S.perm + pos);
-    const int len = __ldcs(S.len + pos);
-    const uint32_t base = __ldcs(S.off + sl) + lane;
-    double acc0 = 0.0, acc1 = 0.0;
-    bool grp = false;
-#pragma unroll 4
-    for (int k = 0; k < len; k++) {
-        const uint32_t w = __ldcs(S.ent + base + 32u * k);
-        const uint32_t c = w & kDevColMask;
-        const double v = __dmul_rn(pal[(w >> 27) & 15u], fused_dir(__ldg(rp + c), __ldg(q + c), alpha, beta));
-        grp = grp || (w >> 31);
-        if (grp) acc1 = __dadd_rn(acc1, v);
-        else acc0 = __dadd_rn(acc0, v);
-    }
-    return grp ? __dadd_rn(acc0, acc1) : acc0;
-}
-
-__device__ __forceinline__ double warp_row_fused(const uint32_t *__restrict__ ent, uint32_t b, uint32_t e,
-                                                 const double2 *__restrict__ rp, const double *__restrict__ q,
-                                                 double alpha, double beta, const double *pal, int lane) {
-    double acc = 0.0;
-    for (uint32_t k = b + lane; k < e; k += 32) {
-        const uint32_t w = __ldg(ent + k);
-        const uint32_t c = w & kDevColMask;
-        acc += pal[(w >> 27) & 15u] * fused_dir(__ldg(rp + c), __ldg(q + c), alpha, beta);
-    }
-    return warp_sum(acc);
-}
-
-// Solves (A A^T) y = rhs like cg_kernel (the same conjugate-gradient
-// iterates), with two grid barriers per iteration instead of three.  The
-// update of an iteration (y += alpha p, r -= alpha q, p = r + beta p) is
-// not a pass of its own: it is applied in the next pass, where every owner
-// of a dual row updates its row while the A^T gather forms the same new
-// direction on the fly from (r, p) and q.  The exact r.r of the updated r is
-// summed in that pass; beta, needed before it is known, comes from the dots
-// of the previous pass, r.r - 2 alpha r.q + alpha^2 q.q (the same quantity
-// in exact arithmetic; its rounding error relative to r.r is of the order of
-// the machine epsilon times the per-iteration reduction of r.r).
-//   A   owners: r' = r - alpha q, y += alpha p, p' = r' + beta p, partial r'.r'
-//       gather: t = A^T p'
-//   --- barrier: stop when ||r'|| < tol
-//   B   q = A t; partial p'.q, r'.q, q.q  (by the lane that formed q_j)
-//   --- barrier: alpha = r'.r' / p'.q, beta = (r'.r' - 2 alpha r'.q + alpha^2 q.q) / r'.r'
-// (r, p) pairs are double-buffered: owners write the next pair while other
-// warps still gather the current one.
-__global__ void __launch_bounds__(kCgThreads, 3) cg_fused_kernel(CgParams P) {
-    __shared__ double palA[16], palT[16];
-    __shared__ double red[32];
-    __shared__ double bcast;
-    __shared__ int flag;
-    if (threadIdx.x < 16) {
-        palA[threadIdx.x] = P.palA.v[threadIdx.x];
-        palT[threadIdx.x] = P.palT.v[threadIdx.x];
-    }
-    __syncthreads();
-    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    const int nb = gridDim.x;
-    const int lane = threadIdx.x & 31;
-    const int64_t gwarp = gtid >> 5, nwarps = stride >> 5;
-    const bool timed = P.phase_ns != nullptr && gtid == 0;
-    unsigned long long tmark = timed ? global_ns() : 0ull;
-    auto lap = [&](int k) {
-        if (timed) {
-            const unsigned long long now = global_ns();
-            P.phase_ns[k] += now - tmark;
-            tmark = now;
-        }
-    };
-    double *const y = P.y, *const q = P.q, *const t = P.t;
-    double2 *cur = P.rp0, *nxt = P.rp1;
-    double *const part_rs = P.partials, *const part_d = P.partials + nb;   // [nb], [3 nb]
-
-    // r = rhs - A A^T y; the pair (r, 0) and q = 0 enter the first pass with alpha = beta = 0
-    for (int64_t sl = gwarp; sl < P.st.nslices; sl += nwarps) {
-        uint32_t row;
-        const double v = sell_row<false>(P.st, sl, lane, y, nullptr, 0.0, palT, row);
-        if (row != 0xffffffffu) t[row] = v;
-    }
-    for (int64_t w = gwarp; w < P.n_long_t; w += nwarps) {
-        const int64_t i = __ldg(P.long_t + w);
-        const double v = warp_row(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), y, nullptr, 0.0,
-                                  palT, lane);
-        if (lane == 0) t[i] = v;
-    }
-    if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
-    double loc = 0.0;
-    auto init_row = [&](int64_t j, double av) {
-        const double v = P.Acz[j] + P.mu * (P.b[j] - P.Ax[j]) - av;
-        cur[j] = make_double2(v, 0.0);
-        q[j] = 0.0;
-        loc += v * v;
-    };
-    for (int64_t sl = gwarp; sl < P.sa.nslices; sl += nwarps) {
-        uint32_t row;
-        const double av = sell_row<false>(P.sa, sl, lane, t, nullptr, 0.0, palA, row);
-        if (row != 0xffffffffu) init_row(row, av);
-    }
-    for (int64_t w = gwarp; w < P.n_long_a; w += nwarps) {
-        const int64_t j = __ldg(P.long_a + w);
-        const double av = warp_row(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), t, nullptr, 0.0,
-                                   palA, lane);
-        if (lane == 0) init_row(j, av);
-    }
-    double sb = block_sum(loc, red);
-    if (threadIdx.x == 0) part_rs[blockIdx.x] = sb;
-    if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
-    lap(0);
-    double rs = sum_partials(part_rs, nb, &bcast);
-
-    int it = 0;
-    double alpha = 0.0, beta = 0.0;
-    bool done = !(sqrt(rs) >= P.tol);
-    while (!done) {
-        // A: apply the pending update and gather the new direction
-        loc = 0.0;
-        for (int64_t j = gtid; j < P.nd; j += stride) {
-            const double2 v = cur[j];
-            const double qj = q[j];
-            const double rn = __dsub_rn(v.x, __dmul_rn(alpha, qj));
-            y[j] += alpha * v.y;
-            const double pn = __dadd_rn(rn, __dmul_rn(beta, v.y));
-            nxt[j] = make_double2(rn, pn);
-            loc += rn * rn;
-        }
-        for (int64_t sl = gwarp; sl < P.st.nslices; sl += nwarps) {
-            uint32_t row;
-            const double v = sell_row_fused(P.st, sl, lane, cur, q, alpha, beta, palT, row);
-            if (row != 0xffffffffu) t[row] = v;
-        }
-        for (int64_t w = gwarp; w < P.n_long_t; w += nwarps) {
-            const int64_t i = __ldg(P.long_t + w);
-            const double v = warp_row_fused(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), cur, q, alpha,
-                                            beta, palT, lane);
-            if (lane == 0) t[i] = v;
-        }
-        sb = block_sum(loc, red);
-        if (threadIdx.x == 0) part_rs[blockIdx.x] = sb;
-        if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
-        lap(1);
-        const double rs_new = sum_partials(part_rs, nb, &bcast);
-        if (it > 0) {
-            if (!(rs_new == rs_new)) {   // NaN
-                if (gtid == 0) atomicExch(P.status, kStatusNan);
-                rs = rs_new;
-                break;
-            }
-            rs = rs_new;
-            if (sqrt(rs) < P.tol) break;
-        }
-        if (it >= P.maxit) break;
-
-        // B: q = A t and the dots of the new pair with it
-        double lpq = 0.0, lrq = 0.0, lqq = 0.0;
-        auto dot_row = [&](int64_t j, double qv) {
-            q[j] = qv;
-            const double2 v = nxt[j];
-            lpq += v.y * qv;
-            lrq += v.x * qv;
-            lqq += qv * qv;
-        };
-        for (int64_t w = gwarp; w < P.n_long_a; w += nwarps) {
-            const int64_t j = __ldg(P.long_a + w);
-            const double qv = warp_row(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), t, nullptr, 0.0,
-                                       palA, lane);
-            if (lane == 0) dot_row(j, qv);
-        }
-        for (int64_t sl = gwarp; sl < P.sa.nslices; sl += nwarps) {
-            uint32_t row;
-            const double qv = sell_row<false>(P.sa, sl, lane, t, nullptr, 0.0, palA, row);
-            if (row != 0xffffffffu) dot_row(row, qv);
-        }
-        sb = block_sum(lpq, red);
-        if (threadIdx.x == 0) part_d[blockIdx.x] = sb;
-        sb = block_sum(lrq, red);
-        if (threadIdx.x == 0) part_d[nb + blockIdx.x] = sb;
-        sb = block_sum(lqq, red);
-        if (threadIdx.x == 0) part_d[2 * nb + blockIdx.x] = sb;
-        if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
-        lap(2);
-        const double pq = sum_partials(part_d, nb, &bcast);
-        const double rq = sum_partials(part_d + nb, nb, &bcast);
-        const double qq = sum_partials(part_d + 2 * nb, nb, &bcast);
-        if (!(pq > 0.0)) break;   // range of A A^T exhausted (or non-finite)
-        alpha = rs / pq;
-        beta = (rs - 2.0 * alpha * rq + alpha * alpha * qq) / rs;
-        it++;
-        double2 *tmp = cur;
-        cur = nxt;
-        nxt = tmp;
     }
     if (gtid == 0) {
         P.out[0] = (double)it;

@@ -23,6 +23,7 @@ struct SellOp {
     const uint32_t *ent, *perm, *off;
     const uint8_t *len;
     int64_t nslices;
+    const uint32_t *split;   // CG warp w takes slices split[w] .. split[w + 1] - 1
 };
 constexpr int kJacobiThreads = 512;
 constexpr int kJacobiMaxDim = 160;     // np*np doubles + rotations must fit in 227 KB
@@ -43,8 +44,7 @@ struct CgParams {
     const double *Ax, *Acz, *b;     // rhs = Acz + mu (b - Ax)
     double mu;
     double *y, *r, *p0, *p1, *t, *q;
-    double2 *rp0, *rp1;             // cg_fused_kernel: (r, p) pairs, double-buffered
-    double *partials;               // >= 4 * gridDim.x (r.r partials, then p.q [, r.q, q.q] partials)
+    double *partials;               // >= 2 * gridDim.x (r.r partials, then p.q partials)
     GridBarrier *bar;
     int *status;
     long long spin_limit;
@@ -67,7 +67,6 @@ __global__ void spmv_AT_U_kernel(const uint32_t *__restrict__ rp,
                                  const double *__restrict__ c, double mu,
                                  double *__restrict__ ATy, double *__restrict__ U, Palette pal);
 __global__ void cg_kernel(CgParams P);
-__global__ void cg_fused_kernel(CgParams P);
 __global__ void stats_kernel(const double *__restrict__ Ax, const double *__restrict__ b,
                              const double *__restrict__ ATy, const double *__restrict__ z,
                              const double *__restrict__ c, const double *__restrict__ x,

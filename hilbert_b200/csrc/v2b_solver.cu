@@ -107,6 +107,8 @@ struct DeviceOp {
     uint32_t *sell_ent = nullptr, *sell_perm = nullptr, *sell_off = nullptr;
     uint8_t *sell_len = nullptr;
     int64_t nslices = 0;
+    std::vector<uint32_t> host_off;   // slice offsets (entries), for the work split
+    uint32_t *sell_split = nullptr;   // per CG warp: its first slice (nwarps + 1 entries)
 
     void upload(const v2b::PackedOperator &op) {
         nrows = op.nrows;
@@ -162,6 +164,7 @@ struct DeviceOp {
         }
         nslices = (int64_t)off.size();
         off.push_back((uint32_t)e.size());
+        host_off = off;
         sell_ent = dalloc<uint32_t>(e.size());
         sell_perm = dalloc<uint32_t>(perm.size());
         sell_len = dalloc<uint8_t>(len.size());
@@ -173,6 +176,45 @@ struct DeviceOp {
         }
         V2B_CK(cudaMemcpy(sell_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice));
     }
+    // Contiguous runs of slices, one per CG warp, of about equal work: a
+    // slice costs its stored entries (32 x its width) plus a fixed share for
+    // its row indices and the write of its results; the long rows, which
+    // warps take round-robin (row k: warp k mod nwarps), count toward their
+    // warp's share.  Round-robin slices gave warps unequal work, which every
+    // grid barrier then waited for.
+    void split_slices(int64_t nwarps, const v2b::PackedOperator &op) {
+        const double fixed = 32.0 * 3.0;
+        std::vector<double> extra(nwarps, 0.0);
+        int64_t k = 0;
+        double total = 0.0;
+        for (int64_t r = 0; r < op.nrows; r++) {
+            const uint32_t L = op.row_ptr[r + 1] - op.row_ptr[r];
+            if (L <= v2b::kCgLongRow) continue;
+            const double c = 32.0 * (double)((L + 31) / 32) + fixed;
+            extra[k % nwarps] += c;
+            total += c;
+            k++;
+        }
+        for (int64_t s = 0; s < nslices; s++) total += (double)(host_off[s + 1] - host_off[s]) + fixed;
+        const double avg = total / (double)nwarps;
+        std::vector<uint32_t> first(nwarps + 1, (uint32_t)nslices);
+        int64_t s = 0;
+        for (int64_t w = 0; w < nwarps; w++) {
+            first[w] = (uint32_t)s;
+            const double budget = avg - extra[w];
+            double acc = 0.0;
+            while (s < nslices) {
+                const double c = (double)(host_off[s + 1] - host_off[s]) + fixed;
+                if (w + 1 < nwarps && acc + 0.5 * c > budget) break;
+                acc += c;
+                s++;
+            }
+        }
+        first[nwarps] = (uint32_t)nslices;
+        if (sell_split) cudaFree(sell_split);
+        sell_split = dalloc<uint32_t>(first.size());
+        V2B_CK(cudaMemcpy(sell_split, first.data(), first.size() * 4, cudaMemcpyHostToDevice));
+    }
     v2b::SellOp sell() const {
         v2b::SellOp s;
         s.ent = sell_ent;
@@ -180,12 +222,14 @@ struct DeviceOp {
         s.off = sell_off;
         s.len = sell_len;
         s.nslices = nslices;
+        s.split = sell_split;
         return s;
     }
     void release() {
         for (void *p : {(void *)rp, (void *)ent, (void *)long_rows, (void *)sell_ent, (void *)sell_perm,
-                        (void *)sell_off, (void *)sell_len})
+                        (void *)sell_off, (void *)sell_len, (void *)sell_split})
             cudaFree(p);
+        sell_split = nullptr;
         rp = ent = sell_ent = sell_perm = sell_off = nullptr;
         sell_len = nullptr;
         long_rows = nullptr;
@@ -1027,10 +1071,6 @@ struct v2b_problem {
     double *x = nullptr, *b = nullptr, *c = nullptr, *y = nullptr, *z = nullptr;
     double *Ax = nullptr, *Acz = nullptr, *ATy = nullptr, *U = nullptr;
     double *r = nullptr, *p0 = nullptr, *p1 = nullptr, *t = nullptr, *q = nullptr;
-    double2 *rpbuf = nullptr;   // cg_fused_kernel's two (r, p) pair buffers
-    // conjugate-gradient kernel: 1 fused (cg_fused_kernel, two grid barriers
-    // per iteration), 0 classic (cg_kernel, three)
-    int cg_variant = 1;
     double *partials = nullptr, *cg_out = nullptr, *stats = nullptr, *stats_partials = nullptr;
     unsigned int *stats_counter = nullptr;
     v2b::GridBarrier *bar = nullptr;
@@ -1098,7 +1138,6 @@ struct v2b_problem {
         cudaFree(ibas_aa_dev);
         cudaFree(status);
         if (nonfinite) cudaFree(nonfinite);
-        if (rpbuf) cudaFree(rpbuf);
         if (h_readback) cudaFreeHost(h_readback);
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
@@ -1133,18 +1172,18 @@ struct v2b_problem {
         ATy = dalloc<double>(np); U = dalloc<double>(np); t = dalloc<double>(np);
         b = dalloc<double>(nd); y = dalloc<double>(nd); Ax = dalloc<double>(nd);
         Acz = dalloc<double>(nd); r = dalloc<double>(nd); p0 = dalloc<double>(nd);
-        p1 = dalloc<double>(nd); q = dalloc<double>(nd); rpbuf = dalloc<double2>(2 * (size_t)nd);
-        if (const char *v = std::getenv("V2B_CG_VARIANT")) cg_variant = std::atoi(v) == 0 ? 0 : 1;
+        p1 = dalloc<double>(nd); q = dalloc<double>(nd);
         int per_sm = 0;
-        V2B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, cg_variant ? (const void *)v2b::cg_fused_kernel : (const void *)v2b::cg_kernel,
-            v2b::kCgThreads, 0));
+        V2B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v2b::cg_kernel,
+                                                             v2b::kCgThreads, 0));
         if (per_sm < 1) throw Failure(V2B_INTERNAL, "cg_kernel cannot be resident");
         // small problems: fewer CTAs make the grid barrier cheaper
         const int64_t rows = std::max(prob.n_primal, prob.n_dual);
         const int64_t want = (rows + (int64_t)v2b::kCgThreads - 1) / (int64_t)v2b::kCgThreads;
         cg_grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sm_count() * per_sm));
-        partials = dalloc<double>(4 * (size_t)cg_grid);
+        A.split_slices((int64_t)cg_grid * (v2b::kCgThreads / 32), hostA);
+        AT.split_slices((int64_t)cg_grid * (v2b::kCgThreads / 32), hostAT);
+        partials = dalloc<double>(2 * (size_t)cg_grid);
         stats_partials = dalloc<double>(4 * v2b::kStatsBlocks);
         cg_out = dalloc<double>(2);
         stats = dalloc<double>(4);
@@ -1190,15 +1229,13 @@ struct v2b_problem {
         P.np = prob.n_primal; P.nd = prob.n_dual;
         P.Ax = Ax; P.Acz = Acz; P.b = b; P.mu = mu;
         P.y = y; P.r = r; P.p0 = p0; P.p1 = p1; P.t = t; P.q = q;
-        P.rp0 = rpbuf; P.rp1 = rpbuf + prob.n_dual;
         P.partials = partials; P.bar = bar; P.status = status;
         P.spin_limit = wait_limit;
         P.tol = tol; P.maxit = maxit; P.out = cg_out;
         P.phase_ns = (profiling && phases) ? cg_phase : nullptr;
         void *args[] = {&P};
-        V2B_CK(cudaLaunchCooperativeKernel(
-            cg_variant ? (const void *)v2b::cg_fused_kernel : (const void *)v2b::cg_kernel, dim3(cg_grid),
-            dim3(v2b::kCgThreads), args, 0, stream));
+        V2B_CK(cudaLaunchCooperativeKernel((const void *)v2b::cg_kernel, dim3(cg_grid),
+                                           dim3(v2b::kCgThreads), args, 0, stream));
         launches++;
     }
 

@@ -158,17 +158,18 @@ def rotated_energy(kappa, h, B, D, G):
 
 
 def rotation_pairs(ncore, nact, nvirt, active_active=False):
-    """Non-redundant rotation pairs (p, q), p > q, in focas's order: by the
-    classes of (p, q) (virtual-core, virtual-active, active-core, then optional
-    active-active), then p, then q."""
+    """Non-redundant rotation pairs (p, q), p > q, in focas's order
+    (Determine_GradIndMap, src/focas/C_files/orbopt_gradient.cc:151-186): by
+    the class of p (active, then virtual), then the class of q (core, then
+    active; active-active pairs only with active_active), then p, then q."""
     core = range(ncore)
     act = range(ncore, ncore + nact)
     virt = range(ncore + nact, ncore + nact + nvirt)
-    pairs = [(p, q) for p in virt for q in core]
-    pairs += [(p, q) for p in virt for q in act]
-    pairs += [(p, q) for p in act for q in core]
+    pairs = [(p, q) for p in act for q in core]
     if active_active:
         pairs += [(p, q) for p in act for q in act if q < p]
+    pairs += [(p, q) for p in virt for q in core]
+    pairs += [(p, q) for p in virt for q in act]
     return pairs
 
 
@@ -313,21 +314,61 @@ def diagonal_hessian(h, B, Da, Ga, ncore, nact, active_active=False):
     H_ad = (2.0 * (2.0 * (Fd[a][:, None] - Fd[c][None, :]) + Dtt[:, None] * Fid[c][None, :]
                    - (Qtt + Ztt)[:, None])
             + 2.0 * coul[:, c] + 4.0 * (tupp - ttpp) + 4.0 * exch[:, c] + 12.0 * (tptp - uptp))
-    parts = [H_ed.reshape(-1), H_ea.reshape(-1), H_ad.reshape(-1)]
+    parts = [H_ad.reshape(-1)]
     if active_active:
-        X = torch.einsum("tuvw,Qvw->Qtu", Ga, Ba)                 # sum_rs G_turs B^Q_rs
-        Bt, Xt = torch.diagonal(Ba, dim1=1, dim2=2), torch.diagonal(X, dim1=1, dim2=2)
-        tt_uu = torch.einsum("Qt,Qu->tu", Bt, Xt)                 # sum_rs (tt|rs) G_uurs
-        coul = tt_uu + tt_uu.T - 2.0 * (Ba * X).sum(0)
-        Y = torch.einsum("Qtr,urs,Qts->tu", Ba, torch.diagonal(Ga, dim1=0, dim2=2).permute(2, 0, 1), Ba)
-        W = torch.einsum("Qur,Qts,urts->tu", Ba, Ba, Ga)          # sum_rs (ur|ts) G_urts
         Fia = Fi[a, a]
-        H_aa = (2.0 * (Dtt[:, None] * torch.diagonal(Fia)[None, :] + Dtt[None, :] * torch.diagonal(Fia)[:, None]
-                       - (Qtt + Ztt)[:, None] - (Qtt + Ztt)[None, :] - 2.0 * Da * Fia)
-                + coul + 2.0 * (Y + Y.T - 2.0 * W))
+        H_aa = 2.0 * (Dtt[:, None] * torch.diagonal(Fia)[None, :] + Dtt[None, :] * torch.diagonal(Fia)[:, None]
+                      - (Qtt + Ztt)[:, None] - (Qtt + Ztt)[None, :] - 2.0 * Da * Fia)
+        H_aa = H_aa + _focas_aa_two_electron(B, Ga, nact)
         t_idx, u_idx = torch.tril_indices(nact, nact, offset=-1, device=h.device)
         parts.append(H_aa[t_idx, u_idx])
+    parts += [H_ed.reshape(-1), H_ea.reshape(-1)]   # focas's order (Determine_GradIndMap)
     return torch.cat(parts)
+
+
+def _focas_aa_two_electron(B, Ga, nact):
+    """The two-electron part of focas's active-active diagonal Hessian as the
+    compiled ComputeH_diag_aa computes it (orbopt_hessian.cc:465-827).  Its
+    comment names Shepard's Eq. B27 sums over four-index integrals (tu|rs),
+    which the routine forms by DGEMM into a scratch array, but its sums read
+    the three-index array tei at those scratch positions instead
+    (tei[ttrs_int], tei[uurs_int], tei[turs_int] in the Coulomb part,
+    tei[trts_int], tei[urus_int], tei[urts_int] in the exchange part).  With
+    L(i, j) the packed index of an active pair (i, j) (i >= j: i (i + 1) / 2
+    + j), m = nact (nact + 1) / 2 and T(x, y) = tei[y m + x], tei being the
+    factors Q-major over the packed lower triangle of all orbitals
+    (tei.cc:281-283) in the current orbitals, it adds for t > u
+      sum_rs [T(L_rs, L_tt) G_uurs + T(L_rs, L_uu) G_ttrs - 2 T(L_rs, L_tu) G_turs]
+      + 2 sum_rs [T(L_tr, L_ts) G_urus + T(L_ur, L_us) G_trts - 2 T(L_ur, L_ts) G_urts],
+    which this function reproduces (the compiled values to 1e-15).  Raises
+    when those positions would run past the array, where the reference reads
+    out of bounds."""
+    n = B.shape[1]
+    m = nact * (nact + 1) // 2
+    tri = torch.tril_indices(n, n, device=B.device)
+    tei = B[:, tri[0], tri[1]].reshape(-1)
+    if m * m > tei.numel():
+        raise ValueError(f"focas's active-active Hessian reads {m * m} elements of a three-index array "
+                         f"of {tei.numel()} (naux too small for {nact} active orbitals)")
+    T = tei[:m * m].reshape(m, m)          # T[y, x] = tei[y m + x]
+    i = torch.arange(nact, device=B.device)
+    hi, lo = torch.maximum(i[:, None], i[None, :]), torch.minimum(i[:, None], i[None, :])
+    L = hi * (hi + 1) // 2 + lo            # L[i, j], packed active pair index
+    G = Ga
+    d = torch.diagonal(L)                  # L_tt
+    # Coulomb: C[t, r, s] = T(L_rs, L_tt); Tu[t, u, r, s] = T(L_rs, L_tu)
+    C = T[d][:, L]
+    Tu = T[L][:, :, L]
+    Guu = torch.diagonal(G, dim1=0, dim2=1).permute(2, 0, 1)   # Guu[u, r, s] = G_uurs
+    coul = (torch.einsum("trs,urs->tu", C, Guu) + torch.einsum("urs,trs->tu", C, Guu)
+            - 2.0 * torch.einsum("turs,turs->tu", Tu, G))
+    # exchange: T(L_tr, L_ts) = T[L_ts, L_tr]; T(L_ur, L_ts) = T[L_ts, L_ur]
+    X = T[L[:, None, :], L[:, :, None]]    # X[t, r, s] = T[L_ts, L_tr]
+    Y = T[L[:, None, None, :], L[None, :, :, None]]   # Y[t, u, r, s] = T[L_ts, L_ur]
+    Gxr = torch.einsum("urus->urs", G)     # G_urus as [u, r, s]
+    exch = (torch.einsum("trs,urs->tu", X, Gxr) + torch.einsum("urs,trs->tu", X, Gxr)
+            - 2.0 * torch.einsum("turs,urts->tu", Y, G))
+    return coul + 2.0 * exch
 
 
 def _pair_kappa(theta, pairs, n):

@@ -126,3 +126,33 @@ done
 "$CXX" -shared -fopenmp "${OMPB[@]}" -Wl,--no-undefined -o "$out/libdoci_ref.so" "${dobjs[@]}" \
     "$out/doci_solver_extract.o" "$out/doci_ref_harness.o"
 echo "built $out/libdoci_ref.so"
+
+# focas's C++ orbital optimizer (the DF path v2RDM-CASSCF calls,
+# src/focas/C_files/*.cc), compiled from the reference sources.  Its class
+# header is copied into _ref/focas/ with two lines added -- a constructor
+# that takes the orbital spaces directly (the real one reads them from a
+# Psi4 wavefunction) and a friend harness -- and the C_files are copied
+# beside it so that their "../orbital_optimizer.h" finds that copy.
+# BLAS / LAPACK: numpy's ILP64 OpenBLAS (hilbert's misc/blas.h passes 64-bit
+# integers), reached through the forwarding wrappers in focas_harness.cc.
+fsrc="$ref/src/focas"
+fout="$out/focas"
+mkdir -p "$fout/C_files"
+awk '/^class OrbitalOptimizer \{/ { print "struct FocasHarnessSetup;"; print "struct FocasHarness;"; print; print "  friend struct FocasHarness;"; next }
+     /OrbitalOptimizer\(std::shared_ptr<Wavefunction> reference_wavefunction, Options & options\);/ { print; print "    explicit OrbitalOptimizer(const FocasHarnessSetup &setup);"; next }
+     { print }' "$fsrc/orbital_optimizer.h" > "$fout/orbital_optimizer.h"
+grep -q "FocasHarnessSetup &setup" "$fout/orbital_optimizer.h" || { echo "build_ref.sh: could not patch orbital_optimizer.h" >&2; exit 3; }
+cp "$fsrc"/C_files/*.cc "$fout/C_files/"
+openblas="$(ls "$(python3 -c 'import numpy, os; print(os.path.dirname(numpy.__file__))')".libs/libscipy_openblas64_*.so 2>/dev/null | head -1)"
+[ -n "$openblas" ] || { echo "build_ref.sh: numpy's OpenBLAS not found" >&2; exit 4; }
+FFLAGS=(-std=c++17 -O2 -fPIC -ffp-contract=off -w -I"$here/ref_shim" -I"$fout" -I"$ref/src")
+fobjs=()
+for f in "$fout"/C_files/*.cc; do
+  o="$fout/$(basename "$f" .cc).o"
+  "$CXX" "${FFLAGS[@]}" -c "$f" -o "$o"
+  fobjs+=("$o")
+done
+"$CXX" "${FFLAGS[@]}" -c "$here/focas_harness.cc" -o "$fout/focas_harness.o"
+"$CXX" -shared -Wl,--no-undefined -o "$out/libfocas_ref.so" "${fobjs[@]}" "$fout/focas_harness.o" \
+    "$openblas" -Wl,-rpath,"$(dirname "$openblas")"
+echo "built $out/libfocas_ref.so"

@@ -234,6 +234,21 @@ def focas_diagonal_hessian(h, B, d2p, d1p, ncore, nact, active_active=False):
             e = eri[T, i, T, i] - sum(D_act[t, u] * eri[act[u], i, T, i] for u in range(nact))
             H[(T, i)] = v + c + 4.0 * d + x + 12.0 * e
     if active_active:
+        # ComputeH_diag_aa's sums read the three-index array tei (Q-major
+        # over the packed lower triangle of all orbitals) at the positions of
+        # its four-index scratch array (orbopt_hessian.cc:640-642, 731-733,
+        # 797-799): tei[y m + x] with x, y packed active-pair indices and
+        # m = nact (nact + 1) / 2, restated as read
+        m = nact * (nact + 1) // 2
+        iu = np.tril_indices(B.shape[1])
+        tei = np.ascontiguousarray(B[:, iu[0], iu[1]]).reshape(-1)
+
+        def L(i, j):
+            return i * (i + 1) // 2 + j if i >= j else j * (j + 1) // 2 + i
+
+        def T3(x, y):
+            return tei[y * m + x]
+
         A = act
         for t in range(nact):
             for u in range(t):
@@ -245,10 +260,10 @@ def focas_diagonal_hessian(h, B, d2p, d1p, ncore, nact, active_active=False):
                 for r in range(nact):
                     for q in range(nact):
                         R, S = A[r], A[q]
-                        c += (eri[T, T, R, S] * P(u, u, r, q) + eri[Uo, Uo, R, S] * P(t, t, r, q)
-                              - 2.0 * eri[T, Uo, R, S] * P(t, u, r, q))
-                        x += (eri[T, R, T, S] * P(u, r, u, q) + eri[Uo, R, Uo, S] * P(t, r, t, q)
-                              - 2.0 * eri[Uo, R, T, S] * P(u, r, t, q))
+                        c += (T3(L(r, q), L(t, t)) * P(u, u, r, q) + T3(L(r, q), L(u, u)) * P(t, t, r, q)
+                              - 2.0 * T3(L(r, q), L(t, u)) * P(t, u, r, q))
+                        x += (T3(L(t, r), L(t, q)) * P(u, r, u, q) + T3(L(u, r), L(u, q)) * P(t, r, t, q)
+                              - 2.0 * T3(L(u, r), L(t, q)) * P(u, r, t, q))
                 H[(T, Uo)] = v + c + 2.0 * x
     return H
 
@@ -283,15 +298,16 @@ def focas_gradient(h, B, D_act, G_act, ncore, nact, active_active=False):
 
 
 def rotation_pairs(ncore, nact, nvirt, active_active=False):
-    """focas's rotation order (Grad_IndMap, orbopt_gradient.cc:147-183):
-    virtual-core, virtual-active, active-core, then active-active (t > u)."""
+    """focas's rotation order (Determine_GradIndMap, orbopt_gradient.cc:151-186):
+    active-core, active-active (t > u, with active-active rotations),
+    virtual-core, virtual-active; then p, then q."""
     core = range(ncore)
     act = range(ncore, ncore + nact)
     virt = range(ncore + nact, ncore + nact + nvirt)
-    pairs = ([(p, q) for p in virt for q in core] + [(p, q) for p in virt for q in act]
-             + [(p, q) for p in act for q in core])
+    pairs = [(p, q) for p in act for q in core]
     if active_active:
         pairs += [(p, q) for p in act for q in act if q < p]
+    pairs += [(p, q) for p in virt for q in core] + [(p, q) for p in virt for q in act]
     return pairs
 
 

@@ -156,6 +156,12 @@ typedef std::shared_ptr<Wavefunction> SharedWavefunction;
 
 struct iwlbuf { int dummy; };
 
+/* LAPACK's dsyevd with Psi4's libqt calling convention (the matrix as
+ * LAPACK sees it: eigenvectors come back as contiguous columns); defined by
+ * the focas harness, which links LAPACK */
+int C_DSYEVD(char jobz, char uplo, int n, double *a, int lda, double *w, double *work, int lwork,
+             int *iwork, int liwork);
+
 /* BLAS level-1 helpers used by the maps (plain loops: no FMA contraction) */
 inline void C_DCOPY(size_t n, double *x, int incx, double *y, int incy) {
     for (size_t i = 0; i < n; i++) y[i * incy] = x[i * incx];

@@ -282,7 +282,7 @@ def test_doci_orbital_optimisation_on_hilbert_schedule():
     assert info["sdp_converged"] and info["orbitals_converged"]
     assert info["rounds"] < 40
     assert E[1] < E[0] - 1.0
-    assert abs(info["final_energy"] - (-33.57490907)) <= 1e-6
+    assert abs(info["final_energy"] - (-33.57490517)) <= 1e-6
     assert gn[-1] < 1e-3 and gn[-1] < 1e-3 * gn[0]
 
 
