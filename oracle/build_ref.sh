@@ -1,5 +1,6 @@
 #!/usr/bin/env bash
-# Build recipe for oracle/_ref/libv2rdm_ref.so: hilbert's OWN constraint-map,
+# Build recipe for oracle/_ref/ (libv2rdm_ref.so, libdoci_ref.so, libfocas_ref.so):
+# hilbert's OWN constraint-map,
 # index-table, sizing, b/c and guess code compiled where it lies in the
 # reference tree, against the test-only Psi4 stand-ins in oracle/ref_shim/.
 #
