@@ -48,6 +48,11 @@ WORKLOADS = {
     "hubbard8": dict(nmo=8, nalpha=4, nbeta=4, positivity="DQG", hamiltonian="hubbard",
                      hubbard=(1.0, 4.0), hubbard_multiplicity=True,
                      r_conv=1e-6, e_conv=1e-6, cg_conv=1e-9, muf=500, maxiter=400000),
+    # config 5: the 4 x 4 periodic Hubbard lattice, 16 electrons, U/t = 8, DQG+T2
+    # (80.4 M primal variables, T2 blocks of 1,920 and 6,016 rows)
+    "hubbard4x4": dict(nmo=16, nalpha=8, nbeta=8, positivity="DQGT2", hamiltonian="hubbard2d",
+                       hubbard2d=dict(lx=4, ly=4, t=1.0, U=8.0), hubbard_multiplicity=False,
+                       r_conv=1e-6, e_conv=1e-6, cg_conv=1e-9, muf=500, maxiter=400000),
     # config 3: 64 independent DQG rings (L 6..14, N in {L-2, L, L+2}, U/t ~ U[1, 8], seed 3)
     "batch64": dict(kind="batch", count=64, seed=3, positivity="DQG", r_conv=1e-6, e_conv=1e-6,
                     cg_conv=1e-9, muf=500, maxiter=400000, concurrency=16),
@@ -75,6 +80,9 @@ def hamiltonian(w):
     """('hubbard', (t, U)) or ('external', (h, g)) for a workload"""
     if w["hamiltonian"] == "hubbard":
         return "hubbard", w["hubbard"]
+    if w["hamiltonian"] == "hubbard2d":
+        from hilbert_b200.synthetic import hubbard_2d
+        return "external", hubbard_2d(**w["hubbard2d"])
     from hilbert_b200.synthetic import df_hamiltonian
     return "external", df_hamiltonian(**w["df"])
 
@@ -268,6 +276,7 @@ def config_of(args, w):
     return {"workload": args.workload, "nmo": w["nmo"], "nalpha": w["nalpha"], "nbeta": w["nbeta"],
             "positivity": w["positivity"],
             "hamiltonian": ({"hubbard_t_U": list(w["hubbard"])} if kind_h == "hubbard"
+                            else {"hubbard_2d": w["hubbard2d"]} if "hubbard2d" in w
                             else {"synthetic_df": w["df"]}),
             "r_convergence": w["r_conv"], "e_convergence": w["e_conv"], "cg_convergence": w["cg_conv"],
             "mu_update_frequency": w["muf"], "tpdm_guess": "RANDOM",

@@ -190,18 +190,22 @@ __global__ void __launch_bounds__(kGemmThreads, 3)
                     const int c = c0 + wn + j * 8 + 2 * fk + h;
                     if (c >= n) continue;
                     const double v = acc[i][j][h];
-                    const int64_t e = off + (int64_t)r * n + c;
-                    if (EPI == kEpiStore) {
-                        C[e] = v;
-                    } else if (EPI == kEpiAdd) {
-                        C[e] = Cin[e] + v;
-                    } else if (EPI == kEpiNS) {   // v = (Vt Vt^T)[r][c]
-                        const double id = (r == c) ? 1.0 : 0.0;
-                        C[e] = 1.5 * id - 0.5 * v;
-                        dev = fmax(dev, fabs(v - id));
-                    } else {   // kEpiProject: v = U+
-                        xo[e] = v * inv_mu;
-                        zo[e] = v - Us[e];
+                    // t.w: an off-diagonal tile of a symmetric product, stored
+                    // at (r, c) and at its mirror image (c, r)
+                    for (int m = 0; m <= t.w; m++) {
+                        const int64_t e = m ? off + (int64_t)c * n + r : off + (int64_t)r * n + c;
+                        if (EPI == kEpiStore) {
+                            C[e] = v;
+                        } else if (EPI == kEpiAdd) {
+                            C[e] = Cin[e] + v;
+                        } else if (EPI == kEpiNS) {   // v = (Vt Vt^T)[r][c]
+                            const double id = (r == c) ? 1.0 : 0.0;
+                            C[e] = 1.5 * id - 0.5 * v;
+                            dev = fmax(dev, fabs(v - id));
+                        } else {   // kEpiProject: v = U+
+                            xo[e] = v * inv_mu;
+                            zo[e] = v - Us[e];
+                        }
                     }
                 }
         }

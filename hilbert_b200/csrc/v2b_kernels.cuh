@@ -67,6 +67,10 @@ __global__ void spmv_AT_U_kernel(const uint32_t *__restrict__ rp,
                                  const double *__restrict__ c, double mu,
                                  double *__restrict__ ATy, double *__restrict__ U, Palette pal);
 __global__ void cg_kernel(CgParams P);
+// the CG starting point of the next outer iteration from the last dual
+// solutions (order 0: y itself, 1: 2y - y1, 2: 3y - 3y1 + y2); y1, y2 shift
+__global__ void extrapolate_y_kernel(double *__restrict__ y, double *__restrict__ y1,
+                                     double *__restrict__ y2, int64_t n, int order);
 __global__ void stats_kernel(const double *__restrict__ Ax, const double *__restrict__ b,
                              const double *__restrict__ ATy, const double *__restrict__ z,
                              const double *__restrict__ c, const double *__restrict__ x,

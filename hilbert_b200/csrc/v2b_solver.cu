@@ -180,8 +180,10 @@ struct DeviceOp {
     // slice costs its stored entries (32 x its width) plus a fixed share for
     // its row indices and the write of its results; the long rows, which
     // warps take round-robin (row k: warp k mod nwarps), count toward their
-    // warp's share.  Round-robin slices gave warps unequal work, which every
-    // grid barrier then waited for.
+    // warp's share.  Warp w's run ends where the cumulative slice work comes
+    // nearest to (w + 1) x the average less the long-row work of warps 0..w
+    // (cumulative targets: the rounding of one warp does not carry into the
+    // next).
     void split_slices(int64_t nwarps, const v2b::PackedOperator &op) {
         const double fixed = 32.0 * 3.0;
         std::vector<double> extra(nwarps, 0.0);
@@ -195,20 +197,19 @@ struct DeviceOp {
             total += c;
             k++;
         }
-        for (int64_t s = 0; s < nslices; s++) total += (double)(host_off[s + 1] - host_off[s]) + fixed;
+        std::vector<double> cum(nslices + 1, 0.0);
+        for (int64_t s = 0; s < nslices; s++) cum[s + 1] = cum[s] + (double)(host_off[s + 1] - host_off[s]) + fixed;
+        total += cum[nslices];
         const double avg = total / (double)nwarps;
-        std::vector<uint32_t> first(nwarps + 1, (uint32_t)nslices);
-        int64_t s = 0;
+        std::vector<uint32_t> first(nwarps + 1, 0);
+        double ce = 0.0;
         for (int64_t w = 0; w < nwarps; w++) {
-            first[w] = (uint32_t)s;
-            const double budget = avg - extra[w];
-            double acc = 0.0;
-            while (s < nslices) {
-                const double c = (double)(host_off[s + 1] - host_off[s]) + fixed;
-                if (w + 1 < nwarps && acc + 0.5 * c > budget) break;
-                acc += c;
-                s++;
-            }
+            ce += extra[w];
+            const double target = (double)(w + 1) * avg - ce;
+            int64_t s = std::lower_bound(cum.begin(), cum.end(), target) - cum.begin();
+            if (s > 0 && s <= nslices && target - cum[s - 1] < cum[s] - target) s--;
+            s = std::min<int64_t>(std::max<int64_t>(s, first[w]), nslices);
+            first[w + 1] = (uint32_t)s;
         }
         first[nwarps] = (uint32_t)nslices;
         if (sell_split) cudaFree(sell_split);
@@ -263,6 +264,11 @@ struct ProjectPlan {
     int *bdim = nullptr, *counters = nullptr;
     int4 *tiles = nullptr;
     int ntiles = 0;
+    // the upper tiles (row tile <= column tile) of every block, w = 1 on the
+    // off-diagonal ones: for products that are symmetric, whose kernel then
+    // stores each off-diagonal tile and its mirror image
+    int4 *stiles = nullptr;
+    int nstiles = 0;
     int *gemm_sched = nullptr;   // persistent-grid tile counter of the GEMM launches
     double2 *rot = nullptr;
     double *Vt = nullptr, *Vt2 = nullptr, *Us = nullptr, *W = nullptr, *T = nullptr, *P = nullptr;
@@ -408,6 +414,12 @@ struct ProjectPlan {
         // longest K first: the persistent GEMM grid takes tiles in this order
         std::stable_sort(tl.begin(), tl.end(), [&](const int4 &a, const int4 &b) { return d[a.x] > d[b.x]; });
         ntiles = (int)tl.size();
+        std::vector<int4> stl;
+        for (const int4 &t : tl)
+            if (t.y <= t.z) stl.push_back(make_int4(t.x, t.y, t.z, t.y < t.z ? 1 : 0));
+        nstiles = (int)stl.size();
+        stiles = dalloc<int4>(std::max(nstiles, 1));
+        if (nstiles) V2B_CK(cudaMemcpy(stiles, stl.data(), nstiles * sizeof(int4), cudaMemcpyHostToDevice));
         boff = dalloc<int64_t>(nblk);
         gemm_sched = dalloc<int>(2);
         V2B_CK(cudaMemset(gemm_sched, 0, 2 * sizeof(int)));
@@ -478,7 +490,7 @@ struct ProjectPlan {
         if (staged) cudaEventDestroy(staged);
         staged = nullptr;
         staged_pending = false;
-        for (void *q : {(void *)boff, (void *)rot_off, (void *)bdim, (void *)counters, (void *)tiles,
+        for (void *q : {(void *)boff, (void *)rot_off, (void *)bdim, (void *)counters, (void *)tiles, (void *)stiles,
                         (void *)gemm_sched, (void *)rot, (void *)Vt, (void *)Vt2, (void *)Us, (void *)W, (void *)T,
                         (void *)P, (void *)rec_b, (void *)norm_b, (void *)sub_boff, (void *)sub_roff,
                         (void *)sub_bdim, (void *)bstate, (void *)orth, (void *)bnorm, (void *)norm_part,
@@ -493,12 +505,14 @@ struct ProjectPlan {
         built = false;
     }
 
+    // sym: the product is symmetric (Vt W with W = Us Vt^T, Vt^T P Vt, Vt Vt^T):
+    // the upper tiles are computed and mirrored
     void gemm(v2b::GemmVariant v, const double *A, const double *B, double *C, const double *Cin,
               double inv_mu, double *x, double *z, cudaStream_t s, long &launches,
-              const int *only_work = nullptr) {
+              const int *only_work = nullptr, bool sym = false) {
         ph_begin(0, s);
-        V2B_CK(v2b::launch_gemm_tiles(v, ntiles, s, A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, x, z,
-                                      only_work, orth, gemm_sched));
+        V2B_CK(v2b::launch_gemm_tiles(v, sym ? nstiles : ntiles, s, A, B, C, sym ? stiles : tiles, boff, bdim,
+                                      Cin, Us, inv_mu, x, z, only_work, orth, gemm_sched));
         ph_end(s);
         launches++;
     }
@@ -876,7 +890,7 @@ struct ProjectPlan {
                 for (int b = 0; b < nblk; b++) nw = nw || st[b] == kStWork;
                 if (nw) {
                     gemm(kGemmNTStore, Us, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
-                    gemm(kGemmNNStore, Vt, W, T, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
+                    gemm(kGemmNNStore, Vt, W, T, nullptr, 0.0, nullptr, nullptr, s, launches, bstate, true);
                 }
             }
             ++stamp;
@@ -958,7 +972,7 @@ struct ProjectPlan {
                 launches++;
                 V2B_CK(cudaMemsetAsync(orth, 0, nblk * sizeof(unsigned long long), s));
                 gemm(kGemmNNStore, W, Vt, Vt2, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
-                gemm(kGemmNTNewtonSchulz, Vt2, Vt2, W, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
+                gemm(kGemmNTNewtonSchulz, Vt2, Vt2, W, nullptr, 0.0, nullptr, nullptr, s, launches, bstate, true);
                 gemm(kGemmNNStore, W, Vt2, Vt, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
             }
         }
@@ -1019,7 +1033,7 @@ struct ProjectPlan {
             launches++;
             fresh = false;
         } else if (++calls, ++since_reset % kReorthEvery == 0) {
-            gemm(kGemmNTStore, Vt, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches);
+            gemm(kGemmNTStore, Vt, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches, nullptr, true);
             half_residual_kernel<<<nblk, 256, 0, s>>>(W, T, boff, bdim);
             V2B_CK(cudaGetLastError());
             launches++;
@@ -1030,7 +1044,7 @@ struct ProjectPlan {
         V2B_CK(cudaGetLastError());
         launches++;
         gemm(kGemmNTStore, Us, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches);
-        gemm(kGemmNNStore, Vt, W, T, nullptr, 0.0, nullptr, nullptr, s, launches);
+        gemm(kGemmNNStore, Vt, W, T, nullptr, 0.0, nullptr, nullptr, s, launches, nullptr, true);
         std::vector<int> st(nblk);
         for (int b = 0; b < nblk; b++)
             st[b] = dims[b] == 0 ? kStDone
@@ -1045,7 +1059,7 @@ struct ProjectPlan {
         V2B_CK(cudaEventRecord(staged, s));
         staged_pending = true;
         gemm(kGemmTNStore, Vt, P, W, nullptr, 0.0, nullptr, nullptr, s, launches);
-        gemm(kGemmNNProject, W, Vt, nullptr, nullptr, 1.0 / mu, x, z, s, launches);
+        gemm(kGemmNNProject, W, Vt, nullptr, nullptr, 1.0 / mu, x, z, s, launches, nullptr, true);
     }
 };
 
@@ -1071,6 +1085,7 @@ struct v2b_problem {
     double *x = nullptr, *b = nullptr, *c = nullptr, *y = nullptr, *z = nullptr;
     double *Ax = nullptr, *Acz = nullptr, *ATy = nullptr, *U = nullptr;
     double *r = nullptr, *p0 = nullptr, *p1 = nullptr, *t = nullptr, *q = nullptr;
+    double *y1 = nullptr, *y2 = nullptr;   // the last two dual solutions, for the CG start
     double *partials = nullptr, *cg_out = nullptr, *stats = nullptr, *stats_partials = nullptr;
     unsigned int *stats_counter = nullptr;
     v2b::GridBarrier *bar = nullptr;
@@ -1128,7 +1143,7 @@ struct v2b_problem {
         A.release();
         AT.release();
         plan.release();
-        for (double *p : {x, b, c, y, z, Ax, Acz, ATy, U, r, p0, p1, t, q, partials, cg_out, stats,
+        for (double *p : {x, b, c, y, z, Ax, Acz, ATy, U, r, p0, p1, t, q, y1, y2, partials, cg_out, stats,
                           stats_partials})
             cudaFree(p);
         if (cg_phase) cudaFree(cg_phase);
@@ -1173,6 +1188,7 @@ struct v2b_problem {
         b = dalloc<double>(nd); y = dalloc<double>(nd); Ax = dalloc<double>(nd);
         Acz = dalloc<double>(nd); r = dalloc<double>(nd); p0 = dalloc<double>(nd);
         p1 = dalloc<double>(nd); q = dalloc<double>(nd);
+        y1 = dalloc<double>(nd); y2 = dalloc<double>(nd);
         int per_sm = 0;
         V2B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v2b::cg_kernel,
                                                              v2b::kCgThreads, 0));
@@ -1240,9 +1256,12 @@ struct v2b_problem {
     }
 
     // one boundary-point iteration; returns {iters, eps_p, eps_d, E_p, E_d}
-    void iterate(const v2b_sdp_options &o, double out[5]) {
+    void iterate(const v2b_sdp_options &o, double out[5], int order) {
         const int64_t np = prob.n_primal, nd = prob.n_dual;
         mark(0, 0);
+        v2b::extrapolate_y_kernel<<<grid_for(nd, 256), 256, 0, stream>>>(y, y1, y2, nd, order);
+        V2B_CK(cudaGetLastError());
+        launches++;
         launch_cg(o.cg_convergence, o.cg_maxiter);
         mark(0, 1);
         mark(1, 0);
@@ -1346,7 +1365,9 @@ struct v2b_problem {
             const long budget = std::min<long>(muf, o.maxiter - oiter);
             for (long k = 0; k < budget; k++) {
                 cur_oiter = oiter;
-                iterate(o, res);
+                // mu is fixed inside this block: extrapolate the CG start through
+                // the block's previous solutions (none at its first iteration)
+                iterate(o, res, (int)std::min<long>(k, 2));
                 const int it = (int)res[0];
                 if (monitor) monitor(print_level, (int)oiter, it, res[3], res[4], mu, res[1], res[2], data);
                 oiter++;

@@ -23,3 +23,22 @@ def df_hamiltonian(n=20, naux=400, seed_b=4, seed_h=5):
     Bm = B.reshape(naux, n * n)
     g = (Bm.T @ Bm).reshape(n, n, n, n)
     return h, g
+
+
+def hubbard_2d(lx=4, ly=4, t=1.0, U=8.0):
+    """(h, g) of the periodic lx x ly Hubbard lattice for the external-
+    Hamiltonian path (hilbert's own Hubbard path is the 1D ring only):
+    h_ij = -t for the lattice neighbours of site i = x + lx y (left, right,
+    up, down with wrap-around, each pair once), g_pppp = U, (pq|rs) order."""
+    n = lx * ly
+    h = np.zeros((n, n))
+    for y in range(ly):
+        for x in range(lx):
+            i = x + lx * y
+            for j in ((x + 1) % lx + lx * y, x + lx * ((y + 1) % ly)):
+                if j != i:
+                    h[i, j] = h[j, i] = -t
+    g = np.zeros((n, n, n, n))
+    for p in range(n):
+        g[p, p, p, p] = U
+    return h, g

@@ -83,9 +83,18 @@ def project_blocks(U, dims, mu):
 
 
 class BPSDPSolver:
-    """libsdp::BPSDPSolver-shaped driver: state (mu, y, z) persists across solve() calls."""
+    """libsdp::BPSDPSolver-shaped driver: state (mu, y, z) persists across solve() calls.
 
-    def __init__(self, n_primal, n_dual, options=None):
+    cg_start: "last" starts each CG from the last y; "extrapolate" from the
+    polynomial extrapolation through the last solutions of the same solve()
+    call (2y - y1 after one, 3y - 3y1 + y2 after two), as the device solve
+    does.  Either start reaches the same CG tolerance: only the number of CG
+    iterations changes."""
+
+    def __init__(self, n_primal, n_dual, options=None, cg_start="last"):
+        if cg_start not in ("last", "extrapolate"):
+            raise ValueError(f"cg_start: {cg_start!r}")
+        self.cg_start = cg_start
         self.n_primal = int(n_primal)
         self.n_dual = int(n_dual)
         self.options = options or SDPOptions()
@@ -110,9 +119,16 @@ class BPSDPSolver:
     def solve(self, x, b, c, dims, maxiter, Au, ATu, monitor=None):
         o = self.options
         AAT = lambda v: Au(ATu(v))
-        for _ in range(int(maxiter)):
+        hist = []
+        for k in range(int(maxiter)):
             rhs = Au(c - self.z) + self.mu * (b - Au(x))
-            self.y, iiter = cg_solve(AAT, rhs, self.y, o.cg_convergence, o.cg_maxiter)
+            y0 = self.y
+            if self.cg_start == "extrapolate" and k >= 2:
+                y0 = 3.0 * (self.y - hist[-1]) + hist[-2]
+            elif self.cg_start == "extrapolate" and k == 1:
+                y0 = 2.0 * self.y - hist[-1]
+            hist = (hist + [self.y])[-2:]
+            self.y, iiter = cg_solve(AAT, rhs, y0, o.cg_convergence, o.cg_maxiter)
             ATy = ATu(self.y)
             U = self.mu * x + ATy - c
             xn, self.z = project_blocks(U, dims, self.mu)

@@ -20,7 +20,8 @@ iteration state (x, y, z, mu, counters) after every solve() call and resumes
 from it.  Run from the repository root:
 
     OMP_NUM_THREADS=8 python tests/golden/make_fp64_energies.py hubbard8
-    OMP_NUM_THREADS=8 python tests/golden/make_fp64_energies.py df20 --state /tmp/df20.npz
+    OMP_NUM_THREADS=8 python tests/golden/make_fp64_energies.py df20 --state /tmp/df20.npz \
+        --cg-start extrapolate
 """
 import argparse
 import json
@@ -56,11 +57,14 @@ def main():
     ap.add_argument("workload", choices=sorted(WORKLOADS))
     ap.add_argument("--state", default=None, help="checkpoint file for a resumable run")
     ap.add_argument("--max-outer", type=int, default=400000)
+    ap.add_argument("--cg-start", choices=("last", "extrapolate"), default="last",
+                    help="CG starting point (oracle/bpsdp.py): the last y, or the extrapolation "
+                         "through the last solutions, which the device solve uses")
     a = ap.parse_args()
     w = WORKLOADS[a.workload]
     P = problem(w)
     opts = SDPOptions(1e-6, 1e-6, 1e-9, 10000, a.max_outer)
-    s = BPSDPSolver(P.n_primal, P.n_dual, opts)
+    s = BPSDPSolver(P.n_primal, P.n_dual, opts, cg_start=a.cg_start)
     x = P.x0.copy()
     wall = 0.0
     if a.state and os.path.exists(a.state):
@@ -86,6 +90,7 @@ def main():
            "options": {"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6, "CG_CONVERGENCE": 1e-9,
                        "MU_UPDATE_FREQUENCY": MUF, "TPDM_GUESS": "RANDOM"},
            "maps": "hilbert's compiled maps (oracle/_ref)", "solver": "oracle/bpsdp.py",
+           "cg_start": a.cg_start,
            "omp_threads": int(os.environ.get("OMP_NUM_THREADS", "0") or 0), "wall_s": round(wall, 1)}
     path = os.path.join(ROOT, "tests", "golden", f"fp64_{a.workload}.json")
     with open(path, "w") as f:
