@@ -24,15 +24,22 @@ namespace cg = cooperative_groups;
 
 namespace v2b {
 
-__global__ void __cluster_dims__(kBigCluster, 1, 1) __launch_bounds__(kBigThreads)
-    jacobi_big_kernel(BigJacobiArgs a) {
+// The body, for T stored as R: double (jacobi_big_kernel, in place in a.T)
+// or float (jacobi_big32_kernel: T32 is the working copy, filled from a.T).
+// Rotation parameters are computed in double from the stored elements and
+// recorded as double pairs (exactly orthogonal to double rounding), so the
+// replay keeps the rows of Vt orthonormal whatever R is; the two-sided
+// updates of T run in R.
+template <typename R>
+__device__ __forceinline__ void jacobi_big_body(const BigJacobiArgs &a, R *Tall) {
     cg::cluster_group cl = cg::this_cluster();
     const int blk = blockIdx.x / kBigCluster;
     const int rank = (int)cl.block_rank();
     const int n = a.bdim[blk];
     if (n <= 0) return;   // uniform over the cluster
     const int np = n + (n & 1), m = np / 2, nsteps = np - 1;
-    double *T = a.T + a.boff[blk];
+    R *T = Tall + a.boff[blk];
+    const double *T0 = a.T + a.boff[blk];
     double *P = a.P + a.boff[blk];
     double *Vt = a.Vt + a.boff[blk];
     double2 *rec = a.rot + a.roff[blk];                          // sweeps x steps x m
@@ -52,14 +59,15 @@ __global__ void __cluster_dims__(kBigCluster, 1, 1) __launch_bounds__(kBigThread
     double fro = 0.0;
     for (int i = r0 + warp; i < r1; i += nwarp) {
         for (int j = i + 1 + lane; j < n; j += 32) {
-            const double v = 0.5 * (T[(int64_t)i * n + j] + T[(int64_t)j * n + i]);
+            const R v = (R)(0.5 * (T0[(int64_t)i * n + j] + T0[(int64_t)j * n + i]));
             T[(int64_t)i * n + j] = v;
             T[(int64_t)j * n + i] = v;
-            fro += 2.0 * v * v;
+            fro += 2.0 * (double)v * (double)v;
         }
         if (lane == 0) {
-            const double d = T[(int64_t)i * n + i];
-            fro += d * d;
+            const R d = (R)T0[(int64_t)i * n + i];
+            T[(int64_t)i * n + i] = d;
+            fro += (double)d * (double)d;
         }
     }
     for (int64_t r = ctid; r < (int64_t)a.max_sweeps * (nsteps + 1); r += cstride) scount[r] = 0;
@@ -83,8 +91,9 @@ __global__ void __cluster_dims__(kBigCluster, 1, 1) __launch_bounds__(kBigThread
                 rr_pair(st, (int)k, np, p, q);
                 double c = 1.0, s = 0.0;
                 if (q < n) {
-                    const double apq = __ldcg(T + (int64_t)p * n + q);
-                    const double app = __ldcg(T + (int64_t)p * n + p), aqq = __ldcg(T + (int64_t)q * n + q);
+                    const double apq = (double)__ldcg(T + (int64_t)p * n + q);
+                    const double app = (double)__ldcg(T + (int64_t)p * n + p);
+                    const double aqq = (double)__ldcg(T + (int64_t)q * n + q);
                     if (fabs(apq) > atol && apq * apq > gtol * fabs(aqq - app)) {
                         const double tau = (aqq - app) / (2.0 * apq);
                         const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + hypot(1.0, tau));
@@ -122,19 +131,20 @@ __global__ void __cluster_dims__(kBigCluster, 1, 1) __launch_bounds__(kBigThread
                 rr_pair(st, Pk, np, pP, qP);
                 rr_pair(st, Qk, np, pQ, qQ);
                 const bool qPin = qP < n, qQin = qQ < n;   // n odd: index n is padding
-                const double b11 = __ldcg(T + (int64_t)pP * n + pQ);
-                const double b12 = qQin ? __ldcg(T + (int64_t)pP * n + qQ) : 0.0;
-                const double b21 = qPin ? __ldcg(T + (int64_t)qP * n + pQ) : 0.0;
-                const double b22 = (qPin && qQin) ? __ldcg(T + (int64_t)qP * n + qQ) : 0.0;
-                const double m11 = b11 * cq.x - b12 * cq.y, m12 = b11 * cq.y + b12 * cq.x;
-                const double m21 = b21 * cq.x - b22 * cq.y, m22 = b21 * cq.y + b22 * cq.x;
-                const double n11 = cp.x * m11 - cp.y * m21, n12 = cp.x * m12 - cp.y * m22;
-                const double n21 = cp.y * m11 + cp.x * m21, n22 = cp.y * m12 + cp.x * m22;
+                const R cqx = (R)cq.x, cqy = (R)cq.y, cpx = (R)cp.x, cpy = (R)cp.y;
+                const R b11 = __ldcg(T + (int64_t)pP * n + pQ);
+                const R b12 = qQin ? __ldcg(T + (int64_t)pP * n + qQ) : (R)0;
+                const R b21 = qPin ? __ldcg(T + (int64_t)qP * n + pQ) : (R)0;
+                const R b22 = (qPin && qQin) ? __ldcg(T + (int64_t)qP * n + qQ) : (R)0;
+                const R m11 = b11 * cqx - b12 * cqy, m12 = b11 * cqy + b12 * cqx;
+                const R m21 = b21 * cqx - b22 * cqy, m22 = b21 * cqy + b22 * cqx;
+                const R n11 = cpx * m11 - cpy * m21, n12 = cpx * m12 - cpy * m22;
+                const R n21 = cpy * m11 + cpx * m21, n22 = cpy * m12 + cpx * m22;
                 if (Pk == Qk) {
                     T[(int64_t)pP * n + pP] = n11;
                     T[(int64_t)qP * n + qP] = n22;
-                    T[(int64_t)pP * n + qP] = 0.0;
-                    T[(int64_t)qP * n + pP] = 0.0;
+                    T[(int64_t)pP * n + qP] = (R)0;
+                    T[(int64_t)qP * n + pP] = (R)0;
                 } else {
                     T[(int64_t)pP * n + pQ] = n11; T[(int64_t)pQ * n + pP] = n11;
                     if (qQin) { T[(int64_t)pP * n + qQ] = n12; T[(int64_t)qQ * n + pP] = n12; }
@@ -157,15 +167,15 @@ __global__ void __cluster_dims__(kBigCluster, 1, 1) __launch_bounds__(kBigThread
     // middle factor P of U+ = V P V^T
     for (int64_t e = ctid; e < (int64_t)n * n; e += cstride) {
         const int i = (int)(e / n), j = (int)(e % n);
-        const double li = __ldcg(T + (int64_t)i * n + i);
+        const double li = (double)__ldcg(T + (int64_t)i * n + i);
         double pv;
         if (i == j) {
             pv = fmax(li, 0.0);
         } else {
-            const double lj = __ldcg(T + (int64_t)j * n + j);
+            const double lj = (double)__ldcg(T + (int64_t)j * n + j);
             const double pi = fmax(li, 0.0), pj = fmax(lj, 0.0);
             const double gam = (li != lj) ? (pi - pj) / (li - lj) : (li > 0.0 ? 1.0 : 0.0);
-            pv = gam * __ldcg(T + e);
+            pv = gam * (double)__ldcg(T + e);
         }
         P[e] = pv;
     }
@@ -199,6 +209,16 @@ __global__ void __cluster_dims__(kBigCluster, 1, 1) __launch_bounds__(kBigThread
             cl.sync();
         }
     }
+}
+
+__global__ void __cluster_dims__(kBigCluster, 1, 1) __launch_bounds__(kBigThreads)
+    jacobi_big_kernel(BigJacobiArgs a) {
+    jacobi_big_body<double>(a, a.T);
+}
+
+__global__ void __cluster_dims__(kBigCluster, 1, 1) __launch_bounds__(kBigThreads)
+    jacobi_big32_kernel(BigJacobiArgs a, float *T32) {
+    jacobi_big_body<float>(a, T32);
 }
 
 }  // namespace v2b

@@ -33,5 +33,9 @@ inline int64_t big_record_slots(int n, int max_sweeps) {
 }
 
 __global__ void jacobi_big_kernel(BigJacobiArgs a);
+// the same selective Jacobi with T held in FP32 (T32: a working copy laid
+// out like a.T, filled from a.T's symmetric part); the rotations and the
+// replay onto Vt stay FP64, P is written from the FP32 result
+__global__ void jacobi_big32_kernel(BigJacobiArgs a, float *T32);
 
 }  // namespace v2b

@@ -13,6 +13,7 @@ constexpr int kStWork = 0;     // refinement passes continue
 constexpr int kStDone = 1;     // T passed the acceptance test; P written
 constexpr int kStJacobi = 2;   // handed to the selective Jacobi kernels
 constexpr int kStBlockJacobi = 3;   // block-Jacobi sweeps over pairs of row groups
+constexpr int kStFp32 = 4;     // mixed mode: an FP32 eigensolve, then FP64 Rayleigh-Ritz + Newton
 
 constexpr int kBJGroup = 32;           // rows per block-Jacobi group (pairs: 64-row subproblems)
 constexpr int kBJMaxSweeps = 24;

@@ -282,6 +282,8 @@ struct ProjectPlan {
     // Jacobi block lists of one call (subsets), device copies and pinned staging
     int64_t *sub_boff = nullptr, *sub_roff = nullptr;
     int *sub_bdim = nullptr;
+    int64_t *sub32_boff = nullptr, *sub32_roff = nullptr;   // mode 2's FP32 eigensolve list
+    int *sub32_bdim = nullptr;
     int64_t *h_sub = nullptr;   // pinned: 3 x nblk int64 (boff, roff, bdim) for small then big
     // refinement state
     int *bstate = nullptr, *h_bstate_up = nullptr;   // device / pinned staging
@@ -369,7 +371,16 @@ struct ProjectPlan {
     }
     bool fresh = true;
     bool built = false;
-    int mode = 0;   // 0: warm refinement, 1: selective Jacobi on every block, every call
+    // 0: warm refinement; 1: selective Jacobi on every block, every call;
+    // 2: warm refinement where the blocks above kJacobiMaxDim rows that
+    //    would change to block-Jacobi sweeps take an FP32 selective Jacobi
+    //    eigensolve instead, followed by the FP64 Rayleigh-Ritz step
+    //    (T recomputed in the new basis) and the FP64 acceptance test and
+    //    Newton passes; block-Jacobi only if that fails
+    int mode = 0;
+    float *T32 = nullptr;          // mode 2: FP32 working copy of T (total elements)
+    long fp32_solves = 0;          // blocks given the FP32 eigensolve
+    static constexpr double kFp32AbsTol = 3e-6, kFp32GapTol = 3e-5;
     long calls = 0, since_reset = 0;
     double abs_tol = 1e-14, gap_tol = 1e-13;
 
@@ -441,6 +452,9 @@ struct ProjectPlan {
         sub_boff = dalloc<int64_t>(nblk);
         sub_roff = dalloc<int64_t>(nblk);
         sub_bdim = dalloc<int>(nblk);
+        sub32_boff = dalloc<int64_t>(nblk);
+        sub32_roff = dalloc<int64_t>(nblk);
+        sub32_bdim = dalloc<int>(nblk);
         V2B_CK(cudaMallocHost(&h_sub, std::max(nblk, 1) * 3 * sizeof(int64_t)));
         // refinement
         bstate = dalloc<int>(nblk);
@@ -497,8 +511,10 @@ struct ProjectPlan {
                         (void *)cls_counts, (void *)done_stamp, (void *)Vsave,
                         (void *)Tsave, (void *)arena, (void *)crec, (void *)cnorm, (void *)Tc,
                         (void *)Pc, (void *)bj_dev, (void *)bj_on,
-                        (void *)rowbase, (void *)lam, (void *)Qt})
+                        (void *)rowbase, (void *)lam, (void *)Qt, (void *)sub32_boff, (void *)sub32_roff,
+                        (void *)sub32_bdim, (void *)T32})
             cudaFree(q);
+        T32 = nullptr;
         for (void *q : {(void *)h_sub, (void *)h_bstate_up, (void *)h_state, (void *)h_edges,
                         (void *)h_arena, (void *)h_bjon})
             if (q) cudaFreeHost(q);
@@ -859,7 +875,7 @@ struct ProjectPlan {
     void refine(std::vector<int> &st, cudaStream_t s, long &launches) {
         using namespace v2b;
         bool any = false;
-        for (int b = 0; b < nblk; b++) any = any || st[b] == kStWork || st[b] == kStBlockJacobi;
+        for (int b = 0; b < nblk; b++) any = any || st[b] == kStWork || st[b] == kStBlockJacobi || st[b] == kStFp32;
         if (!any) return;
         V2B_CK(cudaMemsetAsync(orth, 0, nblk * sizeof(unsigned long long), s));
         V2B_CK(cudaMemcpyAsync(Vsave, Vt, total * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -880,9 +896,10 @@ struct ProjectPlan {
             V2B_CK(cudaMemsetAsync(orth + b, 0, sizeof(unsigned long long), s));
             changed[b] = 0;
         };
+        std::vector<char> fp32_done(nblk, 0);
         auto to_block_jacobi = [&](int b) {
             restore(b);
-            st[b] = kStBlockJacobi;
+            st[b] = (mode == 2 && !fp32_done[b] && dims[b] > kJacobiMaxDim) ? kStFp32 : kStBlockJacobi;
         };
         for (int pass = 0;; pass++) {
             if (pass > 0) {   // T of the blocks that took a Newton step (bstate == kStWork)
@@ -953,8 +970,24 @@ struct ProjectPlan {
                     jblk.push_back(b);
                 }
             }
-            if (nwork == 0 && nbj == 0) break;
+            int nfp = 0;
+            for (int b = 0; b < nblk; b++) nfp += st[b] == kStFp32;
+            if (nwork == 0 && nbj == 0 && nfp == 0) break;
             upload_states(s, st);
+            if (nfp) {
+                // FP32 eigensolve; the next pass recomputes T in the new basis
+                // (the FP64 Rayleigh-Ritz step) and tests / polishes it in FP64
+                ph_begin(3, s);
+                fp32_solve(st, s, launches);
+                ph_end(s);
+                for (int b = 0; b < nblk; b++)
+                    if (st[b] == kStFp32) {
+                        st[b] = kStWork;
+                        fp32_done[b] = 1;
+                        changed[b] = 1;
+                        newton[b] = 0;
+                    }
+            }
             if (nbj) {
                 ph_begin(3, s);
                 block_jacobi_sweep(st, s, launches);
@@ -975,8 +1008,41 @@ struct ProjectPlan {
                 gemm(kGemmNTNewtonSchulz, Vt2, Vt2, W, nullptr, 0.0, nullptr, nullptr, s, launches, bstate, true);
                 gemm(kGemmNNStore, W, Vt2, Vt, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
             }
+            if (nfp) upload_states(s, st);   // the solved blocks are Newton-mode blocks from the next pass on
         }
         upload_states(s, st);
+    }
+
+    // mode 2: FP32 selective Jacobi (jacobi_big32_kernel) on the blocks in
+    // state kStFp32, each warm-started from the call's basis: T is read from
+    // the FP64 T, the rotations are replayed onto Vt in FP64
+    void fp32_solve(const std::vector<int> &st, cudaStream_t s, long &launches) {
+        using namespace v2b;
+        std::vector<int64_t> hb, hr;
+        std::vector<int> hd;
+        for (int b = 0; b < nblk; b++)
+            if (st[b] == kStFp32) {
+                hb.push_back(h_off[b]);
+                hr.push_back(h_roff_big[b]);
+                hd.push_back(dims[b]);
+            }
+        const int nb = (int)hb.size();
+        if (nb == 0) return;
+        if (!T32) T32 = dalloc<float>(total);
+        V2B_CK(cudaMemcpyAsync(sub32_boff, hb.data(), nb * 8, cudaMemcpyHostToDevice, s));
+        V2B_CK(cudaMemcpyAsync(sub32_roff, hr.data(), nb * 8, cudaMemcpyHostToDevice, s));
+        V2B_CK(cudaMemcpyAsync(sub32_bdim, hd.data(), nb * 4, cudaMemcpyHostToDevice, s));
+        BigJacobiArgs a;
+        a.T = T; a.P = P; a.Vt = Vt; a.boff = sub32_boff; a.bdim = sub32_bdim;
+        a.rot = rec_b; a.roff = sub32_roff; a.max_sweeps = kBigSweeps; a.norm_part = norm_b;
+        a.abs_tol = kFp32AbsTol; a.gap_tol = kFp32GapTol; a.counters = counters + 2;
+        const size_t alist_bytes = (size_t)((max_big + 1) / 2 + 1) * sizeof(int);
+        jacobi_big32_kernel<<<nb * kBigCluster, kBigThreads, alist_bytes, s>>>(a, T32);
+        V2B_CK(cudaGetLastError());
+        // the copied lists stay valid until the kernel has read them
+        V2B_CK(cudaStreamSynchronize(s));
+        launches++;
+        fp32_solves += nb;
     }
 
     // selective Jacobi on the blocks in state kStJacobi
@@ -1049,7 +1115,8 @@ struct ProjectPlan {
         for (int b = 0; b < nblk; b++)
             st[b] = dims[b] == 0 ? kStDone
                     : (mode == 1 || dims[b] < kRefineMinDim) ? kStJacobi
-                    : (cold ? kStBlockJacobi : kStWork);
+                    : !cold ? kStWork
+                    : (mode == 2 && dims[b] > kJacobiMaxDim) ? kStFp32 : kStBlockJacobi;
         if (staged_pending) V2B_CK(cudaEventSynchronize(staged));
         upload_states(s, st);
         refine(st, s, launches);
@@ -1869,7 +1936,7 @@ int v2b_problem_cg_profile(const v2b_problem *p, double *ms, int count) {
 
 int v2b_problem_set_projection_mode(v2b_problem *p, int mode) {
     return guarded([&] {
-        if (!p || mode < 0 || mode > 1) throw std::invalid_argument("set_projection_mode: bad argument");
+        if (!p || mode < 0 || mode > 2) throw std::invalid_argument("set_projection_mode: bad argument");
         p->plan.mode = mode;
         return V2B_OK;
     });
@@ -2004,9 +2071,10 @@ int v2b_problem_refine_counts(const v2b_problem *p, long *counts, int n) {
     return guarded([&] {
         if (!p || !counts || n < 0) throw std::invalid_argument("refine_counts: bad argument");
         const ProjectPlan &q = p->plan;
-        const long v[8] = {q.refine_accepted, q.refine_jacobi, q.refine_passes, q.refine_clusters,
-                           q.refine_large_clusters, q.fb_edges, q.fb_passes, q.refine_bj_sweeps};
-        for (int i = 0; i < n && i < 8; i++) counts[i] = v[i];
+        const long v[9] = {q.refine_accepted, q.refine_jacobi, q.refine_passes, q.refine_clusters,
+                           q.refine_large_clusters, q.fb_edges, q.fb_passes, q.refine_bj_sweeps,
+                           q.fp32_solves};
+        for (int i = 0; i < n && i < 9; i++) counts[i] = v[i];
         return V2B_OK;
     });
 }

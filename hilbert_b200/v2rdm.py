@@ -447,12 +447,15 @@ class V2RDMProblem:
         return d2, d1
 
     def set_projection_mode(self, mode):
-        """"refine" (default: warm refinement) or "jacobi" (selective Jacobi on
-        every block every iteration: the plain FP64 path)"""
-        check(self._lib.v2b_problem_set_projection_mode(self._h, {"refine": 0, "jacobi": 1}[mode]))
+        """"refine" (default: warm refinement), "jacobi" (selective Jacobi on
+        every block every iteration: the plain FP64 path) or "mixed" (warm
+        refinement whose large blocks take an FP32 eigensolve, an FP64
+        Rayleigh-Ritz step and FP64 Newton passes where refine would take
+        block-Jacobi sweeps)"""
+        check(self._lib.v2b_problem_set_projection_mode(self._h, {"refine": 0, "jacobi": 1, "mixed": 2}[mode]))
 
     REFINE_COUNTS = ("accepted", "jacobi", "passes", "clusters", "large_clusters",
-                     "fallback_edges", "fallback_passes", "block_jacobi_sweeps")
+                     "fallback_edges", "fallback_passes", "block_jacobi_sweeps", "fp32_eigensolves")
 
     def refine_counts(self):
         """counts of the warm eigen-refinement, keyed by REFINE_COUNTS"""

@@ -265,12 +265,18 @@ int v2b_problem_projection_counts(const v2b_problem *p, long *calls, long *rotat
  * call), [3] clusters diagonalised exactly, [4] blocks that changed to
  * block-Jacobi sweeps for a cluster above 64 rows, [5] ... for too many
  * non-separable pairs, [6] blocks handed to the Jacobi kernels after their
- * passes or sweeps ran out, [7] block-Jacobi sweeps run. */
+ * passes or sweeps ran out, [7] block-Jacobi sweeps run, [8] FP32
+ * eigensolves of blocks (projection mode 2). */
 int v2b_problem_refine_counts(const v2b_problem *p, long *counts, int n);
 /* No counterpart in the reference.  Projection method of the device solve:
  * 0 (default) warm refinement with block-Jacobi and Jacobi fallbacks; 1 the
  * plain path, selective Jacobi on every block in every iteration (the
- * per-iteration full eigendecomposition libsdp performs, in FP64). */
+ * per-iteration full eigendecomposition libsdp performs, in FP64); 2 mixed
+ * precision: warm refinement in which a block above 160 rows that would
+ * change to block-Jacobi sweeps first takes an FP32 selective Jacobi
+ * eigensolve (FP32 storage and updates, FP64 rotations), then an FP64
+ * Rayleigh-Ritz step (T recomputed in the new basis) and the FP64
+ * acceptance test and Newton passes. */
 int v2b_problem_set_projection_mode(v2b_problem *p, int mode);
 
 /* ---- 2b. densities for the orbital optimiser --------------------------------- */

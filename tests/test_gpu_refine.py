@@ -80,3 +80,30 @@ def test_cold_projection_resets_warm_basis(cuda_device):
         assert np.max(np.abs(x.cpu().numpy() - xr)) <= TOL * scale
         assert np.max(np.abs(z.cpu().numpy() - zr)) <= TOL * scale
         U = U + 1e-5 * rng.standard_normal(p.n_primal)
+
+
+def test_mixed_precision_projection_mode_matches_fp64(cuda_device):
+    """Projection mode "mixed": blocks above 160 rows that would take
+    block-Jacobi sweeps get an FP32 eigensolve, then the FP64 Rayleigh-Ritz
+    step and Newton passes.  On a (10e, 10o) DF problem (G2aa block of 200
+    rows) the solve converges to the FP64 (mode "refine") energy within
+    1e-6 Eh, and the FP32 eigensolve did run."""
+    import torch
+    from hilbert_b200.synthetic import df_hamiltonian
+    p = hb.V2RDMProblem(10, 5, 5, "DQG")
+    assert max(p.dims) > 160
+    b = torch.from_numpy(p.b()).to(cuda_device)
+    c = torch.from_numpy(p.c_external(*df_hamiltonian(10, 400, 4, 5))).to(cuda_device)
+    x0 = p.guess("RANDOM")
+    opts = hb.Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6, "MAXITER": 200000,
+                       "MU_UPDATE_FREQUENCY": 500})
+    e = {}
+    for mode in ("refine", "mixed"):
+        p.set_projection_mode(mode)
+        x = torch.from_numpy(x0).to(cuda_device)
+        st = p.solve_device(x, b, c, opts)
+        assert st["converged"], mode
+        e[mode] = float(c @ x)
+    assert abs(e["mixed"] - e["refine"]) <= 1e-6
+    assert p.refine_counts()["fp32_eigensolves"] > 0
+    p.set_projection_mode("refine")
