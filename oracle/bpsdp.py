@@ -64,8 +64,18 @@ def cg_solve(apply, rhs, y, tol, maxiter):
     return y, it
 
 
-def project_blocks(U, dims, mu):
-    """Split U into U+ / mu (new x) and -U- (new z), block by block."""
+def project_blocks(U, dims, mu, precision="fp64"):
+    """Split U into U+ / mu (new x) and -U- (new z), block by block.
+
+    precision "fp64": LAPACK eigh in FP64.  "fp32rr": the eigenvectors from
+    an FP32 eigh, then one FP64 Rayleigh-Ritz step: V re-orthonormalised by
+    one Newton-Schulz step, T = V^T sym(U) V in FP64, and U+ = V (G o T) V^T
+    with G_pq = (f(t_pp) - f(t_qq)) / (t_pp - t_qq), f(t) = max(t, 0) (the
+    first-order Daleckii-Krein form, exact on the diagonal and for pairs of
+    the same sign).  The precision study of the mixed-precision projection
+    runs the whole iteration with it."""
+    if precision not in ("fp64", "fp32rr"):
+        raise ValueError(f"precision: {precision!r}")
     x = np.empty_like(U)
     z = np.empty_like(U)
     off = 0
@@ -73,11 +83,25 @@ def project_blocks(U, dims, mu):
         d = int(d)
         m = U[off:off + d * d].reshape(d, d)
         m = 0.5 * (m + m.T)
-        w, v = np.linalg.eigh(m)
-        wp = np.maximum(w, 0.0)
-        wn = np.minimum(w, 0.0)
-        x[off:off + d * d] = ((v * wp) @ v.T).ravel() / mu
-        z[off:off + d * d] = -((v * wn) @ v.T).ravel()
+        if precision == "fp64":
+            w, v = np.linalg.eigh(m)
+            x[off:off + d * d] = ((v * np.maximum(w, 0.0)) @ v.T).ravel() / mu
+            z[off:off + d * d] = -((v * np.minimum(w, 0.0)) @ v.T).ravel()
+            off += d * d
+            continue
+        else:
+            _, v32 = np.linalg.eigh(m.astype(np.float32))
+            v = v32.astype(np.float64)
+            v = v @ (1.5 * np.eye(d) - 0.5 * (v.T @ v))
+            t = v.T @ m @ v
+            dg = np.diag(t).copy()
+            fp = np.maximum(dg, 0.0)
+            num = fp[:, None] - fp[None, :]
+            den = dg[:, None] - dg[None, :]
+            g = np.where(den != 0.0, num / np.where(den == 0.0, 1.0, den), (dg[:, None] > 0.0) * 1.0)
+            up = v @ (g * t) @ v.T
+        x[off:off + d * d] = up.ravel() / mu
+        z[off:off + d * d] = (up - m).ravel()
         off += d * d
     return x, z
 
@@ -89,12 +113,13 @@ class BPSDPSolver:
     polynomial extrapolation through the last solutions of the same solve()
     call (2y - y1 after one, 3y - 3y1 + y2 after two), as the device solve
     does.  Either start reaches the same CG tolerance: only the number of CG
-    iterations changes."""
+    iterations changes.  precision: the projection's (project_blocks)."""
 
-    def __init__(self, n_primal, n_dual, options=None, cg_start="last"):
+    def __init__(self, n_primal, n_dual, options=None, cg_start="last", precision="fp64"):
         if cg_start not in ("last", "extrapolate"):
             raise ValueError(f"cg_start: {cg_start!r}")
         self.cg_start = cg_start
+        self.precision = precision
         self.n_primal = int(n_primal)
         self.n_dual = int(n_dual)
         self.options = options or SDPOptions()
@@ -131,7 +156,7 @@ class BPSDPSolver:
             self.y, iiter = cg_solve(AAT, rhs, y0, o.cg_convergence, o.cg_maxiter)
             ATy = ATu(self.y)
             U = self.mu * x + ATy - c
-            xn, self.z = project_blocks(U, dims, self.mu)
+            xn, self.z = project_blocks(U, dims, self.mu, self.precision)
             x[:] = xn
             self.primal_error = float(np.linalg.norm(Au(x) - b))
             self.dual_error = float(np.linalg.norm(ATy + self.z - c))

@@ -183,3 +183,15 @@ def test_oracle_d4_bit_exact_against_reference_grid():
             assert (r.n_primal, r.n_dual) == (o.n_primal, o.n_dual) and list(r.dims) == list(o.dims)
             x, y = rng.standard_normal(r.n_primal), rng.standard_normal(r.n_dual)
             assert same(r.Au(x), o.Au(x)) and same(r.ATu(y), o.ATu(y))
+
+
+def test_fp32_eigenvectors_with_an_fp64_rayleigh_ritz_step_keep_the_solve():
+    """The precision study of the mixed projection at n = 4 (a (4e, 4o)
+    synthetic DF problem): FP32 eigenvectors followed by one FP64
+    Rayleigh-Ritz step converge in the outer iterations of the FP64
+    projection (to 1%) and to its energy within 1e-7 Eh."""
+    from oracle.precision_study import run
+    a, b = run(4, "fp64"), run(4, "fp32rr")
+    assert a["converged"] and b["converged"]
+    assert abs(a["outer_iterations"] - b["outer_iterations"]) <= 0.01 * a["outer_iterations"]
+    assert abs(a["energy"] - b["energy"]) <= 1e-7
