@@ -871,7 +871,10 @@ struct ProjectPlan {
     // restarting from the call's saved basis and T (block-Jacobi keeps Vt
     // orthonormal by construction, the Newton steps only to the accepted
     // tolerance).  A block in block-Jacobi mode takes one sweep per pass, and
-    // after kBJMaxSweeps goes to the selective Jacobi kernels.
+    // after kBJMaxSweeps goes to the selective Jacobi kernels.  In the mixed
+    // mode a block above kJacobiMaxDim rows takes the FP32 eigensolve before
+    // block-Jacobi; from then on its clusters of every size take the cluster
+    // kernels, and a later restart begins from the FP32-solved basis.
     void refine(std::vector<int> &st, cudaStream_t s, long &launches) {
         using namespace v2b;
         bool any = false;
@@ -896,7 +899,11 @@ struct ProjectPlan {
             V2B_CK(cudaMemsetAsync(orth + b, 0, sizeof(unsigned long long), s));
             changed[b] = 0;
         };
-        std::vector<char> fp32_done(nblk, 0);
+        // fp32_done: the block took the FP32 eigensolve in this call; snap:
+        // its FP64 T in the new basis is computed at the top of the next
+        // pass, and the basis and T are then kept as the block's restart
+        // point in place of the call's saved ones
+        std::vector<char> fp32_done(nblk, 0), snap(nblk, 0);
         auto to_block_jacobi = [&](int b) {
             restore(b);
             st[b] = (mode == 2 && !fp32_done[b] && dims[b] > kJacobiMaxDim) ? kStFp32 : kStBlockJacobi;
@@ -908,6 +915,14 @@ struct ProjectPlan {
                 if (nw) {
                     gemm(kGemmNTStore, Us, Vt, W, nullptr, 0.0, nullptr, nullptr, s, launches, bstate);
                     gemm(kGemmNNStore, Vt, W, T, nullptr, 0.0, nullptr, nullptr, s, launches, bstate, true);
+                }
+                for (int b = 0; b < nblk; b++) {
+                    if (!snap[b]) continue;
+                    const size_t bytes = (size_t)dims[b] * dims[b] * sizeof(double);
+                    V2B_CK(cudaMemcpyAsync(Vsave + h_off[b], Vt + h_off[b], bytes, cudaMemcpyDeviceToDevice, s));
+                    V2B_CK(cudaMemcpyAsync(Tsave + h_off[b], T + h_off[b], bytes, cudaMemcpyDeviceToDevice, s));
+                    snap[b] = 0;
+                    changed[b] = 0;
                 }
             }
             ++stamp;
@@ -956,7 +971,9 @@ struct ProjectPlan {
                 clusters_of(b, cl);
                 size_t kmax = 0;
                 for (const auto &c : cl) kmax = std::max(kmax, c.size());
-                if ((int)kmax > kRefineSmallCluster) {
+                // after the FP32 eigensolve the clusters are those of an
+                // almost diagonal T: any size goes to the cluster kernels
+                if ((int)kmax > kRefineSmallCluster && !fp32_done[b]) {
                     refine_large_clusters++;
                     to_block_jacobi(b);
                     nbj++;
@@ -984,6 +1001,7 @@ struct ProjectPlan {
                     if (st[b] == kStFp32) {
                         st[b] = kStWork;
                         fp32_done[b] = 1;
+                        snap[b] = 1;
                         changed[b] = 1;
                         newton[b] = 0;
                     }
