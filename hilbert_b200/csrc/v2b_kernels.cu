@@ -72,16 +72,26 @@ __global__ void spmv_AT_U_kernel(const uint32_t *__restrict__ rp,
 // Long rows inside CG: one warp per row, lanes stride over the entries and the
 // partial sums meet in a shuffle tree (order differs from hilbert's left-to-
 // right sum; the bit-exact kernels above are the ones the map API uses).
+// The operand of entry column c: x[c], or with RBP the direction
+// r + beta p from the interleaved pair z[c] = (r_c, p_c), one 16-byte load.
+template <bool RBP>
+__device__ __forceinline__ double operand(const double *__restrict__ x, const double2 *__restrict__ z,
+                                          double beta, uint32_t c) {
+    if (RBP) {
+        const double2 v = __ldg(z + c);
+        return __dadd_rn(v.x, __dmul_rn(beta, v.y));
+    }
+    return __ldg(x + c);
+}
+
+template <bool RBP>
 __device__ __forceinline__ double warp_row(const uint32_t *__restrict__ ent, uint32_t b, uint32_t e,
-                                           const double *__restrict__ x, const double *__restrict__ p,
+                                           const double *__restrict__ x, const double2 *__restrict__ z,
                                            double beta, const double *pal, int lane) {
     double acc = 0.0;
     for (uint32_t k = b + lane; k < e; k += 32) {
         const uint32_t w = __ldg(ent + k);
-        const uint32_t c = w & kDevColMask;
-        double v = __ldg(x + c);
-        if (p) v = __dadd_rn(v, __dmul_rn(beta, __ldg(p + c)));
-        acc += pal[(w >> 27) & 15u] * v;
+        acc += pal[(w >> 27) & 15u] * operand<RBP>(x, z, beta, w & kDevColMask);
     }
     return warp_sum(acc);
 }
@@ -93,7 +103,7 @@ __device__ __forceinline__ double warp_row(const uint32_t *__restrict__ ent, uin
 // stay in L2.
 template <bool RBP>
 __device__ __forceinline__ double sell_row(const SellOp &S, int64_t sl, int lane,
-                                           const double *__restrict__ x, const double *__restrict__ p,
+                                           const double *__restrict__ x, const double2 *__restrict__ z,
                                            double beta, const double *pal, uint32_t &row) {
     const int64_t pos = sl * 32 + lane;
     row = __ldcs(S.perm + pos);
@@ -104,10 +114,7 @@ __device__ __forceinline__ double sell_row(const SellOp &S, int64_t sl, int lane
 #pragma unroll 4
     for (int k = 0; k < len; k++) {
         const uint32_t w = __ldcs(S.ent + base + 32u * k);
-        const uint32_t c = w & kDevColMask;
-        double xv = __ldg(x + c);
-        if (RBP) xv = __dadd_rn(xv, __dmul_rn(beta, __ldg(p + c)));
-        const double v = __dmul_rn(pal[(w >> 27) & 15u], xv);
+        const double v = __dmul_rn(pal[(w >> 27) & 15u], operand<RBP>(x, z, beta, w & kDevColMask));
         grp = grp || (w >> 31);
         if (grp) acc1 = __dadd_rn(acc1, v);
         else acc0 = __dadd_rn(acc0, v);
@@ -121,6 +128,9 @@ __device__ __forceinline__ double sell_row(const SellOp &S, int64_t sl, int lane
 //   1. t = A^T (r + beta p_old), p_new = r + beta p_old
 //   2. q = A t,  partial p_new.q
 //   3. y += alpha p_new, r -= alpha q, partial r.r
+// r and the direction p live interleaved, z[j] = (r_j, p_j), so the gather of
+// step 1 reads both with one 16-byte load; p_new goes to its own array pn in
+// step 1 (z is being gathered) and into z with the new r in step 3.
 // The p.q and r.r partials live in separate arrays: a block that has passed
 // barrier 2 writes its r.r partial while slower blocks may still be summing
 // the p.q partials.  Operator rows of up to kCgLongRow entries are applied
@@ -163,8 +173,8 @@ __global__ void __launch_bounds__(kCgThreads, 3) cg_kernel(CgParams P) {
     }
     for (int64_t w = gwarp; w < P.n_long_t; w += nwarps) {
         const int64_t i = __ldg(P.long_t + w);
-        const double v = warp_row(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), P.y, nullptr, 0.0,
-                                  palT, lane);
+        const double v = warp_row<false>(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), P.y, nullptr,
+                                         0.0, palT, lane);
         if (lane == 0) P.t[i] = v;
     }
     if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
@@ -174,17 +184,17 @@ __global__ void __launch_bounds__(kCgThreads, 3) cg_kernel(CgParams P) {
         const double av = sell_row<false>(P.sa, sl, lane, P.t, nullptr, 0.0, palA, row);
         if (row != 0xffffffffu) {
             const double v = P.Acz[row] + P.mu * (P.b[row] - P.Ax[row]) - av;
-            P.r[row] = v;
+            P.z[row] = make_double2(v, 0.0);   // first direction p = r (beta = 0)
             loc += v * v;
         }
     }
     for (int64_t w = gwarp; w < P.n_long_a; w += nwarps) {
         const int64_t j = __ldg(P.long_a + w);
-        const double av = warp_row(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), P.t, nullptr, 0.0,
-                                   palA, lane);
+        const double av = warp_row<false>(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), P.t, nullptr,
+                                          0.0, palA, lane);
         if (lane == 0) {
             const double v = P.Acz[j] + P.mu * (P.b[j] - P.Ax[j]) - av;
-            P.r[j] = v;
+            P.z[j] = make_double2(v, 0.0);
             loc += v * v;
         }
     }
@@ -196,31 +206,32 @@ __global__ void __launch_bounds__(kCgThreads, 3) cg_kernel(CgParams P) {
 
     int it = 0;
     double beta = 0.0;
-    const double *pold = P.r;   // first direction p = r (beta = 0)
-    double *pnew = P.p0;
+    double *pnew = P.pn;
     bool done = !(sqrt(rs) >= P.tol);
     while (!done && it < P.maxit) {
         for (int64_t sl = P.st.split[gwarp], se = P.st.split[gwarp + 1]; sl < se; sl++) {
             uint32_t row;
-            const double v = sell_row<true>(P.st, sl, lane, P.r, pold, beta, palT, row);
+            const double v = sell_row<true>(P.st, sl, lane, nullptr, P.z, beta, palT, row);
             if (row != 0xffffffffu) P.t[row] = v;
         }
         for (int64_t w = gwarp; w < P.n_long_t; w += nwarps) {
             const int64_t i = __ldg(P.long_t + w);
-            const double v = warp_row(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), P.r, pold,
-                                      beta, palT, lane);
+            const double v = warp_row<true>(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), nullptr, P.z,
+                                            beta, palT, lane);
             if (lane == 0) P.t[i] = v;
         }
-        for (int64_t j = gtid; j < P.nd; j += stride)
-            pnew[j] = __dadd_rn(P.r[j], __dmul_rn(beta, pold[j]));
+        for (int64_t j = gtid; j < P.nd; j += stride) {
+            const double2 v = P.z[j];
+            pnew[j] = __dadd_rn(v.x, __dmul_rn(beta, v.y));
+        }
         if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
         lap(1);
 
         loc = 0.0;
         for (int64_t w = gwarp; w < P.n_long_a; w += nwarps) {
             const int64_t j = __ldg(P.long_a + w);
-            const double q = warp_row(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), P.t, nullptr,
-                                      0.0, palA, lane);
+            const double q = warp_row<false>(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), P.t, nullptr,
+                                             0.0, palA, lane);
             if (lane == 0) {
                 P.q[j] = q;
                 loc += pnew[j] * q;
@@ -244,9 +255,10 @@ __global__ void __launch_bounds__(kCgThreads, 3) cg_kernel(CgParams P) {
 
         loc = 0.0;
         for (int64_t j = gtid; j < P.nd; j += stride) {
-            P.y[j] += alpha * pnew[j];
-            const double rv = P.r[j] - alpha * P.q[j];
-            P.r[j] = rv;
+            const double pv = pnew[j];
+            P.y[j] += alpha * pv;
+            const double rv = P.z[j].x - alpha * P.q[j];
+            P.z[j] = make_double2(rv, pv);
             loc += rv * rv;
         }
         s = block_sum(loc, red);
@@ -262,10 +274,6 @@ __global__ void __launch_bounds__(kCgThreads, 3) cg_kernel(CgParams P) {
         done = sqrt(rs_new) < P.tol;
         beta = rs_new / rs;
         rs = rs_new;
-        // the next direction is built from r and the current one
-        double *tmp = (pnew == P.p0) ? P.p1 : P.p0;
-        pold = pnew;
-        pnew = tmp;
     }
     if (gtid == 0) {
         P.out[0] = (double)it;

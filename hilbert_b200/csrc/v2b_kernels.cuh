@@ -43,7 +43,8 @@ struct CgParams {
     int64_t np, nd;
     const double *Ax, *Acz, *b;     // rhs = Acz + mu (b - Ax)
     double mu;
-    double *y, *r, *p0, *p1, *t, *q;
+    double *y, *pn, *t, *q;
+    double2 *z;                     // (r_j, p_j) interleaved; pn: the new direction
     double *partials;               // >= 2 * gridDim.x (r.r partials, then p.q partials)
     GridBarrier *bar;
     int *status;

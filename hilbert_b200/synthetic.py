@@ -42,3 +42,45 @@ def hubbard_2d(lx=4, ly=4, t=1.0, U=8.0):
     for p in range(n):
         g[p, p, p, p] = U
     return h, g
+
+
+def main(argv=None):
+    """One solve of a synthetic DF active space on cuda:0 through the public
+    API, printed as one JSON line: the small, bounded command that profilers
+    and quick checks run.
+
+        python -m hilbert_b200.synthetic --n 20 --naux 400 --max-outer 2
+    """
+    import argparse
+    import json
+
+    import torch
+
+    import hilbert_b200 as hb
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--n", type=int, default=20, help="active orbitals (n electrons, singlet)")
+    ap.add_argument("--naux", type=int, default=400)
+    ap.add_argument("--positivity", default="DQG")
+    ap.add_argument("--max-outer", type=int, default=2, help="MAXITER of the solve")
+    ap.add_argument("--projection", default="refine", choices=("refine", "jacobi", "mixed"))
+    a = ap.parse_args(argv)
+    if a.n % 2:
+        raise SystemExit("--n must be even (n electrons in n orbitals, singlet)")
+    dev = torch.device("cuda", 0)
+    p = hb.V2RDMProblem(a.n, a.n // 2, a.n // 2, a.positivity, True, True)
+    h, g = df_hamiltonian(n=a.n, naux=a.naux)
+    b, c, x0 = p.b(), p.c_external(h, g), p.guess("RANDOM")
+    p.set_projection_mode(a.projection)
+    opts = hb.Options({"R_CONVERGENCE": 1e-6, "E_CONVERGENCE": 1e-6, "CG_CONVERGENCE": 1e-9,
+                       "MAXITER": a.max_outer, "MU_UPDATE_FREQUENCY": 500})
+    x = torch.from_numpy(x0).to(dev)
+    st = p.solve_device(x, torch.from_numpy(b).to(dev), torch.from_numpy(c).to(dev), opts)
+    torch.cuda.synchronize()
+    print(json.dumps({"n": a.n, "naux": a.naux, "positivity": a.positivity, "n_primal": int(x0.size),
+                      "n_dual": int(b.size), "outer_iterations": st["oiter"], "cg_iterations": st["iiter"],
+                      "converged": st["converged"], "energy": float(c @ x.cpu().numpy()),
+                      "kernel_launches": p.kernel_launches()}))
+
+
+if __name__ == "__main__":
+    main()

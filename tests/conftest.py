@@ -16,15 +16,12 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
-    config.addinivalue_line("markers", "first_device_run: a device path not yet run on a GPU")
 
 
 def pytest_collection_modifyitems(config, items):
-    """Tests of device paths that have not run on a GPU yet go after the
-    others (stable order otherwise), so that under -x a failure there cannot
-    stop them; test_zz_no_alloc stays last."""
-    items.sort(key=lambda item: (item.module.__name__.startswith("test_zz"),
-                                 item.get_closest_marker("first_device_run") is not None))
+    """test_zz_no_alloc runs last (stable order otherwise): its entry point
+    holds a fixed device array, the other tests allocate freely."""
+    items.sort(key=lambda item: item.module.__name__.startswith("test_zz"))
 
 
 @pytest.fixture(scope="session")

@@ -6,7 +6,7 @@ import pytest
 from hilbert_b200.batch import RingInstance, solve_in_one_launch, solve_on_device
 from hilbert_b200.v2rdm import Options
 
-pytestmark = [pytest.mark.gpu, pytest.mark.first_device_run]
+pytestmark = pytest.mark.gpu
 
 
 def test_rings_in_one_launch_match_each_alone(cuda_device):

@@ -9,7 +9,7 @@ import pytest
 import hilbert_b200 as hb
 from hilbert_b200 import checkpoint as ck
 
-pytestmark = [pytest.mark.gpu, pytest.mark.first_device_run]
+pytestmark = pytest.mark.gpu
 
 
 def ring(n=6):

@@ -9,7 +9,7 @@ from oracle.doci import DociOracle, seniority_zero_ci, symmetric_integrals
 from test_doci import (assert_Au_matches, df_integrals, doci_schedule_energy, golden_cases, oracle_solve,
                        pair_hamiltonian)
 
-pytestmark = [pytest.mark.gpu, pytest.mark.first_device_run]
+pytestmark = pytest.mark.gpu
 
 E_TOL = 1e-6
 

@@ -14,16 +14,12 @@ def gpu_problem(kw):
                            kw["constrain_sz"], hubbard_multiplicity="hubbard" in kw)
 
 
-FIRST_RUN = pytest.mark.first_device_run   # the T1 and 3-/4-RDM families
-
-
 @pytest.mark.parametrize("name", ["hub2_dqg", "hub4_dqg", "hub4_d_nospin", "ext3_dqg_triplet",
                                   "ext4_dq_nosz", "ext4_dg_doublet", "ext5_dqg", "ext1_dqg",
-                                  "hub3_dqgt2", "ext3_dqgt2_doublet"]
-                         + [pytest.param(name, marks=FIRST_RUN) for name in (
-                             "hub4_dqgt1", "ext4_dqgt1t2_doublet", "hub4_dqg_d3",
-                             "ext3_d_d3_nosz_doublet", "ext3_dqg_q3_doublet", "hub3_d_e3",
-                             "ext3_d_f3_doublet", "ext4_d_d4_quartet")])
+                                  "hub3_dqgt2", "ext3_dqgt2_doublet", "hub4_dqgt1",
+                                  "ext4_dqgt1t2_doublet", "hub4_dqg_d3", "ext3_d_d3_nosz_doublet",
+                                  "ext3_dqg_q3_doublet", "hub3_d_e3", "ext3_d_f3_doublet",
+                                  "ext4_d_d4_quartet"])
 def test_maps_bit_exact_golden(golden, cuda_device, name):
     import torch
     case = golden[name]

@@ -169,3 +169,16 @@ def test_profiling_timers_leave_the_solve_unchanged(cuda_device):
     # barrier-to-barrier phases lie inside the kernels' event-timed span
     assert sum(cg.values()) <= 1.05 * classes["cg_kernel"][0] + 0.5
     assert phases["gemm"][1] > 0
+
+
+def test_synthetic_runner_prints_one_capped_solve(cuda_device, capsys):
+    """python -m hilbert_b200.synthetic: one solve of a small DF active
+    space, capped at MAXITER outer iterations, reported as one JSON line."""
+    import json
+
+    from hilbert_b200.synthetic import main
+    main(["--n", "4", "--naux", "30", "--max-outer", "3"])
+    out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert out["outer_iterations"] == 3 and not out["converged"]
+    assert out["cg_iterations"] > 0 and out["kernel_launches"] > 0
+    assert np.isfinite(out["energy"])
