@@ -37,6 +37,14 @@ namespace v2b {
 // CTAs an SM holds) and CTAs take tiles in list order, the tile list sorted
 // by block dimension (its K) descending: the longest tiles start first and
 // the short ones fill in behind them.  Without one, CTA i computes tile i.
+//
+// Split K: when a launch has fewer tiles than the grid has CTA slots, the
+// plan cuts the K range of the large blocks' tiles into S parts (tile word w:
+// bit 0 mirror, bits 4-7 the part s, bits 8-11 S, bits 12+ the output tile's
+// group; S <= kGemmMaxSplit).  Each part stores its 64 x 64 partial product
+// in the group's slot s of split_ws and counts itself in split_cnt[group]; the part that arrives
+// last sums the slots in the order s = 0 .. S-1 (the same bits whichever
+// part arrives last), re-arms the counter and runs the epilogue.
 constexpr int kGemmBK = 16;
 constexpr int kGemmStages = 3;
 constexpr int kGemmThreads = 128;
@@ -96,12 +104,13 @@ __global__ void __launch_bounds__(kGemmThreads, 3)
                       const double *__restrict__ Cin, const double *__restrict__ Us, double inv_mu,
                       double *__restrict__ xo, double *__restrict__ zo,
                       const int *__restrict__ bstate, unsigned long long *__restrict__ orth,
-                      int ntiles, int *__restrict__ sched) {
+                      int ntiles, int *__restrict__ sched, double *__restrict__ split_ws,
+                      int *__restrict__ split_cnt) {
     // op(A) rows are m-contiguous in memory when A is read transposed;
     // op(B) columns are m-contiguous when B is read as stored
     constexpr bool AK = TA, BKM = !TB;
     extern __shared__ double gsm[];
-    __shared__ int s_tile;
+    __shared__ int s_tile, s_last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
     const int fr = lane >> 2, fk = lane & 3;
@@ -139,13 +148,18 @@ __global__ void __launch_bounds__(kGemmThreads, 3)
 #pragma unroll
             for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-        const int nk = (n + kGemmBK - 1) / kGemmBK;
+        const int split = (t.w >> 8) & 15, part = (t.w >> 4) & 15;
+        const int nk_all = (n + kGemmBK - 1) / kGemmBK;
+        // this part's K chunks: kb .. kb + nk - 1
+        const int per = split > 1 ? (nk_all + split - 1) / split : nk_all;
+        const int kb = split > 1 ? min(part * per, nk_all) : 0;
+        const int nk = min(nk_all - kb, per);
 #pragma unroll
         for (int st = 0; st < kGemmStages - 1; st++) {
             if (st < nk) {
                 double *sa = gsm + st * 2 * kOpDoubles;
-                load_op<AK>(sa, Ab, n, r0, st * kGemmBK);
-                load_op<BKM>(sa + kOpDoubles, Bb, n, c0, st * kGemmBK);
+                load_op<AK>(sa, Ab, n, r0, (kb + st) * kGemmBK);
+                load_op<BKM>(sa + kOpDoubles, Bb, n, c0, (kb + st) * kGemmBK);
             }
             cp_async_commit();
         }
@@ -156,8 +170,8 @@ __global__ void __launch_bounds__(kGemmThreads, 3)
             const int kn = kt + kGemmStages - 1;
             if (kn < nk) {
                 double *sa = gsm + (kn % kGemmStages) * 2 * kOpDoubles;
-                load_op<AK>(sa, Ab, n, r0, kn * kGemmBK);
-                load_op<BKM>(sa + kOpDoubles, Bb, n, c0, kn * kGemmBK);
+                load_op<AK>(sa, Ab, n, r0, (kb + kn) * kGemmBK);
+                load_op<BKM>(sa + kOpDoubles, Bb, n, c0, (kb + kn) * kGemmBK);
             }
             cp_async_commit();
             const double *sa = gsm + (kt % kGemmStages) * 2 * kOpDoubles;
@@ -178,6 +192,37 @@ __global__ void __launch_bounds__(kGemmThreads, 3)
         cp_async_wait<0>();
         __syncthreads();   // the next tile's copies reuse the stages
 
+        if (split > 1) {
+            const unsigned group = (unsigned)t.w >> 12;
+            double *slot = split_ws + ((int64_t)group * kGemmMaxSplit + part) * (kGemmTile * kGemmTile);
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++)
+                        __stcg(slot + (wm + i * 8 + fr) * kGemmTile + wn + j * 8 + 2 * fk + h, acc[i][j][h]);
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0) s_last = atomicAdd(split_cnt + group, 1) == split - 1;
+            __syncthreads();
+            if (!s_last) continue;
+            __threadfence();
+            const double *slots = split_ws + (int64_t)group * kGemmMaxSplit * (kGemmTile * kGemmTile);
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int e = (wm + i * 8 + fr) * kGemmTile + wn + j * 8 + 2 * fk + h;
+                        double v = __ldcg(slots + e);
+                        for (int q = 1; q < split; q++) v += __ldcg(slots + q * (kGemmTile * kGemmTile) + e);
+                        acc[i][j][h] = v;
+                    }
+            if (threadIdx.x == 0) split_cnt[group] = 0;   // every part has arrived: re-arm
+        }
+
         double dev = 0.0;
 #pragma unroll
         for (int i = 0; i < 4; i++) {
@@ -192,7 +237,7 @@ __global__ void __launch_bounds__(kGemmThreads, 3)
                     const double v = acc[i][j][h];
                     // t.w: an off-diagonal tile of a symmetric product, stored
                     // at (r, c) and at its mirror image (c, r)
-                    for (int m = 0; m <= t.w; m++) {
+                    for (int m = 0; m <= (t.w & 1); m++) {
                         const int64_t e = m ? off + (int64_t)c * n + r : off + (int64_t)r * n + c;
                         if (EPI == kEpiStore) {
                             C[e] = v;
@@ -219,7 +264,8 @@ __global__ void __launch_bounds__(kGemmThreads, 3)
 }
 
 template <bool TA, bool TB, int EPI>
-static cudaError_t launch_variant(int ntiles, cudaStream_t s, GEMM_ARGS, int *sched) {
+static cudaError_t launch_variant(int ntiles, cudaStream_t s, GEMM_ARGS, int *sched, double *split_ws,
+                                  int *split_cnt) {
     auto kern = gemm_tiles_kernel<TA, TB, EPI>;
     // opt in to the pipeline's shared memory and size the persistent grid,
     // once per variant, device and context (function attributes are per
@@ -254,15 +300,28 @@ static cudaError_t launch_variant(int ntiles, cudaStream_t s, GEMM_ARGS, int *sc
     }
     const int grid = sched ? std::min(ntiles, cfg.slots) : ntiles;
     kern<<<grid, kGemmThreads, kGemmSmem, s>>>(A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate,
-                                               orth, ntiles, sched);
+                                               orth, ntiles, sched, split_ws, split_cnt);
     return cudaGetLastError();
 }
 
-cudaError_t launch_gemm_tiles(GemmVariant v, int ntiles, cudaStream_t s, GEMM_ARGS, int *sched) {
+cudaError_t gemm_slots(int *slots) {
+    int dev = 0, sms = 0, occ = 0;
+    const void *kern = (const void *)gemm_tiles_kernel<false, false, kEpiStore>;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = raise_dynamic_smem(kern, kGemmSmem);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kGemmThreads, kGemmSmem);
+    if (e == cudaSuccess) *slots = std::max(1, sms * occ);
+    return e;
+}
+
+cudaError_t launch_gemm_tiles(GemmVariant v, int ntiles, cudaStream_t s, GEMM_ARGS, int *sched, double *split_ws,
+                              int *split_cnt) {
     if (ntiles <= 0) return cudaSuccess;
 #define V2B_GEMM_CASE(NAME, TA, TB, EPI) \
     case NAME:                           \
-        return launch_variant<TA, TB, EPI>(ntiles, s, A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate, orth, sched);
+        return launch_variant<TA, TB, EPI>(ntiles, s, A, B, C, tiles, boff, bdim, Cin, Us, inv_mu, xo, zo, bstate, orth, \
+                                           sched, split_ws, split_cnt);
     switch (v) {
         V2B_GEMM_CASE(kGemmNTNewtonSchulz, false, true, kEpiNS)
         V2B_GEMM_CASE(kGemmNTStore, false, true, kEpiStore)

@@ -13,6 +13,7 @@ constexpr int kEpiAdd = 1;       // C = Cin + op(A) op(B)
 constexpr int kEpiProject = 2;   // x = (op(A) op(B)) / mu, z = op(A) op(B) - Us
 constexpr int kEpiNS = 3;        // C = 3/2 I - 1/2 op(A) op(B); orth[b] = max |op(A) op(B) - I|
 constexpr int kGemmTile = 64;
+constexpr int kGemmMaxSplit = 4;   // K parts of one output tile at most
 
 #define GEMM_ARGS                                                                           \
     const double *__restrict__ A, const double *__restrict__ B, double *__restrict__ C,     \
@@ -29,11 +30,16 @@ constexpr int kGemmTile = 64;
 // progress) are skipped.  sched: two ints, zero before the first launch, that
 // make the grid persistent (tiles taken in list order; the kernel leaves them
 // zero again); null launches one CTA per tile.  Launches that share a sched
-// pair must be ordered (one stream).
+// pair must be ordered (one stream).  Tiles split along K (tile word bits
+// 8-11 above 1) need split_ws (kGemmMaxSplit x 64 x 64 doubles per group) and split_cnt
+// (one int per group, zero before the first launch, left zero).
 enum GemmVariant { kGemmNTStore = 0, kGemmNNStore = 1, kGemmTNStore = 2, kGemmNNProject = 3,
                    kGemmNNAdd = 4, kGemmNTNewtonSchulz = 5 };
 cudaError_t launch_gemm_tiles(GemmVariant v, int ntiles, cudaStream_t s, GEMM_ARGS,
-                              int *sched = nullptr);
+                              int *sched = nullptr, double *split_ws = nullptr, int *split_cnt = nullptr);
+// CTA slots of the persistent GEMM grid on the current device (SMs x
+// resident CTAs)
+cudaError_t gemm_slots(int *slots);
 
 }  // namespace v2b
 

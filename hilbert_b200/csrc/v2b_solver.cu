@@ -269,6 +269,16 @@ struct ProjectPlan {
     // stores each off-diagonal tile and its mirror image
     int4 *stiles = nullptr;
     int nstiles = 0;
+    // both lists with the tiles of blocks of kSplitMinDim rows or more cut
+    // along K into up to kGemmMaxSplit parts, enough to fill the GEMM grid's
+    // CTA slots (gemm_tiles_kernel); the parts' partial products meet in
+    // split_ws, counted in split_cnt
+    static constexpr int kSplitMinDim = 256;
+    int4 *ktiles = nullptr, *kstiles = nullptr;
+    int nktiles = 0, nkstiles = 0;
+    double *split_ws = nullptr;
+    int *split_cnt = nullptr;
+    bool split_k = true;
     int *gemm_sched = nullptr;   // persistent-grid tile counter of the GEMM launches
     double2 *rot = nullptr;
     double *Vt = nullptr, *Vt2 = nullptr, *Us = nullptr, *W = nullptr, *T = nullptr, *P = nullptr;
@@ -431,6 +441,39 @@ struct ProjectPlan {
         nstiles = (int)stl.size();
         stiles = dalloc<int4>(std::max(nstiles, 1));
         if (nstiles) V2B_CK(cudaMemcpy(stiles, stl.data(), nstiles * sizeof(int4), cudaMemcpyHostToDevice));
+        {
+            int slots = 0;
+            V2B_CK(v2b::gemm_slots(&slots));
+            int ngroups = 0;
+            auto split_list = [&](const std::vector<int4> &L) {
+                const int nl = std::max<int>((int)L.size(), 1);
+                const int S = std::min(v2b::kGemmMaxSplit, (slots + nl - 1) / nl);
+                std::vector<int4> out;
+                int g = 0;
+                for (const int4 &t : L) {
+                    if (S < 2 || d[t.x] < kSplitMinDim || g >= (1 << 19)) {
+                        out.push_back(t);
+                        continue;
+                    }
+                    for (int q = 0; q < S; q++)
+                        out.push_back(make_int4(t.x, t.y, t.z, (t.w & 1) | (q << 4) | (S << 8) | (g << 12)));
+                    g++;
+                }
+                ngroups = std::max(ngroups, g);   // a launch uses one list: the lists share the groups
+                return out;
+            };
+            const std::vector<int4> kl = split_list(tl), ksl = split_list(stl);
+            nktiles = (int)kl.size();
+            nkstiles = (int)ksl.size();
+            ktiles = dalloc<int4>(std::max(nktiles, 1));
+            kstiles = dalloc<int4>(std::max(nkstiles, 1));
+            if (nktiles) V2B_CK(cudaMemcpy(ktiles, kl.data(), nktiles * sizeof(int4), cudaMemcpyHostToDevice));
+            if (nkstiles) V2B_CK(cudaMemcpy(kstiles, ksl.data(), nkstiles * sizeof(int4), cudaMemcpyHostToDevice));
+            split_ws = dalloc<double>((size_t)std::max(ngroups, 1) * v2b::kGemmMaxSplit * v2b::kGemmTile *
+                                      v2b::kGemmTile);
+            split_cnt = dalloc<int>(std::max(ngroups, 1));
+            V2B_CK(cudaMemset(split_cnt, 0, std::max(ngroups, 1) * sizeof(int)));
+        }
         boff = dalloc<int64_t>(nblk);
         gemm_sched = dalloc<int>(2);
         V2B_CK(cudaMemset(gemm_sched, 0, 2 * sizeof(int)));
@@ -505,7 +548,7 @@ struct ProjectPlan {
         staged = nullptr;
         staged_pending = false;
         for (void *q : {(void *)boff, (void *)rot_off, (void *)bdim, (void *)counters, (void *)tiles, (void *)stiles,
-                        (void *)gemm_sched, (void *)rot, (void *)Vt, (void *)Vt2, (void *)Us, (void *)W, (void *)T,
+                        (void *)ktiles, (void *)kstiles, (void *)split_ws, (void *)split_cnt, (void *)gemm_sched, (void *)rot, (void *)Vt, (void *)Vt2, (void *)Us, (void *)W, (void *)T,
                         (void *)P, (void *)rec_b, (void *)norm_b, (void *)sub_boff, (void *)sub_roff,
                         (void *)sub_bdim, (void *)bstate, (void *)orth, (void *)bnorm, (void *)norm_part,
                         (void *)cls_counts, (void *)done_stamp, (void *)Vsave,
@@ -527,8 +570,10 @@ struct ProjectPlan {
               double inv_mu, double *x, double *z, cudaStream_t s, long &launches,
               const int *only_work = nullptr, bool sym = false) {
         ph_begin(0, s);
-        V2B_CK(v2b::launch_gemm_tiles(v, sym ? nstiles : ntiles, s, A, B, C, sym ? stiles : tiles, boff, bdim,
-                                      Cin, Us, inv_mu, x, z, only_work, orth, gemm_sched));
+        const int nt = sym ? (split_k ? nkstiles : nstiles) : (split_k ? nktiles : ntiles);
+        const int4 *tl = sym ? (split_k ? kstiles : stiles) : (split_k ? ktiles : tiles);
+        V2B_CK(v2b::launch_gemm_tiles(v, nt, s, A, B, C, tl, boff, bdim, Cin, Us, inv_mu, x, z, only_work, orth,
+                                      gemm_sched, split_ws, split_cnt));
         ph_end(s);
         launches++;
     }
@@ -1956,6 +2001,14 @@ int v2b_problem_set_projection_mode(v2b_problem *p, int mode) {
     return guarded([&] {
         if (!p || mode < 0 || mode > 2) throw std::invalid_argument("set_projection_mode: bad argument");
         p->plan.mode = mode;
+        return V2B_OK;
+    });
+}
+
+int v2b_problem_set_gemm_split(v2b_problem *p, int on) {
+    return guarded([&] {
+        if (!p) throw std::invalid_argument("set_gemm_split: NULL problem");
+        p->plan.split_k = on != 0;
         return V2B_OK;
     });
 }

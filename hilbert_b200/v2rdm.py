@@ -454,6 +454,11 @@ class V2RDMProblem:
         block-Jacobi sweeps)"""
         check(self._lib.v2b_problem_set_projection_mode(self._h, {"refine": 0, "jacobi": 1, "mixed": 2}[mode]))
 
+    def set_gemm_split(self, on=True):
+        """the projection's GEMM tiles of large blocks cut along K when a
+        launch has fewer tiles than CTA slots (default), or each in one piece"""
+        check(self._lib.v2b_problem_set_gemm_split(self._h, int(bool(on))))
+
     REFINE_COUNTS = ("accepted", "jacobi", "passes", "clusters", "large_clusters",
                      "fallback_edges", "fallback_passes", "block_jacobi_sweeps", "fp32_eigensolves")
 

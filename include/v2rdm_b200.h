@@ -279,6 +279,13 @@ int v2b_problem_refine_counts(const v2b_problem *p, long *counts, int n);
  * acceptance test and Newton passes. */
 int v2b_problem_set_projection_mode(v2b_problem *p, int mode);
 
+/* The projection's FP64 GEMM launches cut the K range of large blocks' tiles
+ * into parts when a launch has fewer tiles than the GPU has CTA slots, and
+ * sum the parts in a fixed order (run-to-run identical).  on = 0 computes
+ * every tile in one piece.  Default on.  No reference counterpart: libsdp
+ * projects with LAPACK on the host. */
+int v2b_problem_set_gemm_split(v2b_problem *p, int on);
+
 /* ---- 2b. densities for the orbital optimiser --------------------------------- */
 
 /* PackSpatialDensity (v2rdm_solver.cc:3110-3219, C1): from a primal x on the

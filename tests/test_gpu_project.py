@@ -63,3 +63,26 @@ def test_large_block_repeated_projection(cuda_device):
         scale = max(1.0, np.linalg.norm(U2))
         assert np.max(np.abs(x.cpu().numpy() - xr)) <= TOL * scale
         assert np.max(np.abs(z.cpu().numpy() - zr)) <= TOL * scale
+
+
+def test_split_k_gemm_matches_lapack_and_repeats(cuda_device):
+    """The GEMM tiles of blocks of 256 rows or more cut along K (the 288-row
+    block of n = 12) and in one piece both match LAPACK; the split sums its
+    parts in a fixed order, so two projections give the same bits."""
+    import torch
+    p = hb.V2RDMProblem(12, 6, 6)
+    assert max(p.dims) >= 256
+    rng = np.random.default_rng(12)
+    U = rng.standard_normal(p.n_primal)
+    xr, zr = project_blocks(U, p.dims, 0.61)
+    scale = max(1.0, np.linalg.norm(U))
+    out = {}
+    for on in (True, False, True):
+        p.set_gemm_split(on)
+        x, z = p.project(torch.from_numpy(U).to(cuda_device), 0.61)
+        x, z = x.cpu().numpy(), z.cpu().numpy()
+        assert np.max(np.abs(x - xr)) <= TOL * scale, on
+        assert np.max(np.abs(z - zr)) <= TOL * scale, on
+        if on in out:
+            assert np.array_equal(out[on][0], x) and np.array_equal(out[on][1], z)
+        out[on] = (x, z)
