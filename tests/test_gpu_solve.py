@@ -148,6 +148,23 @@ def test_dqgt2_energy_between_dqg_and_fci(cuda_device):
     assert e["DQGT2"] <= hubbard_fci(4, 4, 1.0, 4.0) + E_TOL
 
 
+@pytest.mark.parametrize("extra", [("POSITIVITY", "DQGT1"), ("CONSTRAIN_D3", True)])
+def test_t1_and_d3_tighten_dqg_below_fci(cuda_device, extra):
+    """Device solves through the T1 and D3 maps (hilbert's t1.cc and d3.cc
+    families): each added condition keeps E(DQG) <= E <= E(FCI) on the
+    4-site ring at U/t = 4."""
+    o = hubbard_options(4, 4.0)
+    base = hb.v2RDMHelper(None, o)
+    e_dqg = base.compute_energy()
+    o = hubbard_options(4, 4.0)
+    o.set(*extra)
+    helper = hb.v2RDMHelper(None, o)
+    e = helper.compute_energy()
+    assert base.stats["converged"] and helper.stats["converged"]
+    assert e_dqg <= e + E_TOL
+    assert e <= hubbard_fci(4, 4, 1.0, 4.0) + E_TOL
+
+
 def test_profiling_timers_leave_the_solve_unchanged(cuda_device):
     """Kernel-class events, projection phases and the CG kernel's own phase
     clock: all populated, consistent with each other, and the solve with them
