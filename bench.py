@@ -414,6 +414,7 @@ def run_b200(args, w):
             torch.cuda.synchronize()
             times.append(ev0.elapsed_time(ev1) / 1e3)
     prof = p.profile()
+    split_choice = p.gemm_split_choice()
     launches = p.kernel_launches() - launches0
     p.set_profiling(0)
     t = max_over_ranks(max(times), world)
@@ -554,6 +555,7 @@ def run_b200(args, w):
                     "speedup_vs_plain_fp64": (plain["seconds"] / t) if plain else None,
                     "abs_dE_vs_plain_fp64": abs(energy - plain["energy"]) if plain else None,
                     "projection_refine_counts": p.refine_counts(),
+                    "gemm_split_autotuned": {"full_list": split_choice[0], "upper_list": split_choice[1]},
                     "max_outer_cap": args.max_outer or None})
         line = {"metric": METRIC, "value": t, "unit": "s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": False,

@@ -42,7 +42,7 @@ EXPORTS = (
     "v2b_problem_solve_device", "v2b_problem_get_y", "v2b_problem_get_z", "v2b_problem_get_mu",
     "v2b_problem_kernel_launches", "v2b_problem_operator_size", "v2b_problem_operator",
     "v2b_problem_set_profiling", "v2b_problem_profile", "v2b_problem_stream",
-    "v2b_problem_projection_counts", "v2b_problem_refine_counts", "v2b_problem_set_projection_mode", "v2b_problem_set_gemm_split", "v2b_problem_pack_dims", "v2b_problem_projection_profile",
+    "v2b_problem_projection_counts", "v2b_problem_refine_counts", "v2b_problem_set_projection_mode", "v2b_problem_set_gemm_split", "v2b_problem_gemm_split_choice", "v2b_problem_pack_dims", "v2b_problem_projection_profile",
     "v2b_problem_cg_profile",
     "v2b_problem_pack_spatial_density", "v2b_project_block_noalloc",
     "v2b_problem_rdm_counts", "v2b_problem_rdm_records", "v2b_problem_set_state", "v2b_problem_continue",
@@ -135,6 +135,7 @@ def load(path=LIB_PATH):
         "v2b_problem_refine_counts": (ctypes.c_int, [vp, lp, ctypes.c_int]),
         "v2b_problem_set_projection_mode": (ctypes.c_int, [vp, ctypes.c_int]),
         "v2b_problem_set_gemm_split": (ctypes.c_int, [vp, ctypes.c_int]),
+        "v2b_problem_gemm_split_choice": (ctypes.c_int, [vp, ip, ip]),
         "v2b_problem_pack_dims": (ctypes.c_int, [vp, lp, lp]),
         "v2b_problem_rdm_counts": (ctypes.c_int, [vp, ctypes.c_int, vp]),
         "v2b_problem_set_state": (ctypes.c_int, [vp, ctypes.c_double, dp, dp]),

@@ -270,15 +270,16 @@ struct ProjectPlan {
     int4 *stiles = nullptr;
     int nstiles = 0;
     // both lists with the tiles of blocks of kSplitMinDim rows or more cut
-    // along K into up to kGemmMaxSplit parts, enough to fill the GEMM grid's
-    // CTA slots (gemm_tiles_kernel); the parts' partial products meet in
-    // split_ws, counted in split_cnt
+    // along K into the number of parts the tuner found fastest
+    // (gemm_tiles_kernel); the parts' partial products meet in split_ws,
+    // counted in split_cnt
     static constexpr int kSplitMinDim = 256;
     int4 *ktiles = nullptr, *kstiles = nullptr;
     int nktiles = 0, nkstiles = 0;
     double *split_ws = nullptr;
     int *split_cnt = nullptr;
     bool split_k = true;
+    int split_full = 1, split_sym = 1;   // the tuner's choices
     int *gemm_sched = nullptr;   // persistent-grid tile counter of the GEMM launches
     double2 *rot = nullptr;
     double *Vt = nullptr, *Vt2 = nullptr, *Us = nullptr, *W = nullptr, *T = nullptr, *P = nullptr;
@@ -394,6 +395,96 @@ struct ProjectPlan {
     long calls = 0, since_reset = 0;
     double abs_tol = 1e-14, gap_tol = 1e-13;
 
+    // K-split tile list: the tiles of blocks of kSplitMinDim rows or more cut
+    // into S parts (tile word: bits 4-7 part, 8-11 S, 12+ group), the others
+    // as they are
+    static std::vector<int4> split_tiles(const std::vector<int> &d, const std::vector<int4> &L, int S,
+                                         int &groups) {
+        std::vector<int4> out;
+        groups = 0;
+        for (const int4 &t : L) {
+            if (S < 2 || d[t.x] < kSplitMinDim || groups >= (1 << 19)) {
+                out.push_back(t);
+                continue;
+            }
+            for (int q = 0; q < S; q++)
+                out.push_back(make_int4(t.x, t.y, t.z, (t.w & 1) | (q << 4) | (S << 8) | (groups << 12)));
+            groups++;
+        }
+        return out;
+    }
+
+    // The split autotuner: for the full and the symmetric tile list, the part
+    // count S in {1, 2, kGemmMaxSplit} whose GEMM launch over every block is
+    // fastest on this GPU (CUDA events, one warm-up and three timed launches
+    // each, on the zeroed work arrays, when the plan is built).  The launches
+    // are the per-iteration products W = Us Vt^T (full list) and
+    // T = Vt W (symmetric list).
+    void tune_split(const std::vector<int> &d, const std::vector<int4> &tl, const std::vector<int4> &stl) {
+        using namespace v2b;
+        int groups = 0;
+        split_tiles(d, tl, 2, groups);
+        split_ws = dalloc<double>((size_t)std::max(groups, 1) * kGemmMaxSplit * kGemmTile * kGemmTile);
+        split_cnt = dalloc<int>(std::max(groups, 1));
+        V2B_CK(cudaMemset(split_cnt, 0, std::max(groups, 1) * sizeof(int)));
+        for (double *b : {Vt, Us, W, T}) V2B_CK(cudaMemset(b, 0, total * sizeof(double)));
+        // the uploads and fills above ran on the legacy stream, the timed
+        // launches run on a non-blocking one
+        V2B_CK(cudaDeviceSynchronize());
+        cudaStream_t s = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        V2B_CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        V2B_CK(cudaEventCreate(&e0));
+        V2B_CK(cudaEventCreate(&e1));
+        int4 *buf = dalloc<int4>(std::max<size_t>(1, (size_t)kGemmMaxSplit * std::max(tl.size(), stl.size())));
+        auto pick = [&](const std::vector<int4> &L, bool sym, int &n_out) {
+            int best_s = 1;
+            float best = 0.0f;
+            for (int S : {1, 2, kGemmMaxSplit}) {
+                int g = 0;
+                const std::vector<int4> k = split_tiles(d, L, S, g);
+                if (k.empty()) break;
+                V2B_CK(cudaMemcpy(buf, k.data(), k.size() * sizeof(int4), cudaMemcpyHostToDevice));
+                float ms = 0.0f;
+                for (int rep = 0; rep < 4; rep++) {
+                    if (rep == 1) V2B_CK(cudaEventRecord(e0, s));
+                    if (sym)
+                        V2B_CK(launch_gemm_tiles(kGemmNNStore, (int)k.size(), s, Vt, W, T, buf, boff, bdim, nullptr,
+                                                 Us, 0.0, nullptr, nullptr, nullptr, orth, gemm_sched, split_ws,
+                                                 split_cnt));
+                    else
+                        V2B_CK(launch_gemm_tiles(kGemmNTStore, (int)k.size(), s, Us, Vt, W, buf, boff, bdim, nullptr,
+                                                 Us, 0.0, nullptr, nullptr, nullptr, orth, gemm_sched, split_ws,
+                                                 split_cnt));
+                }
+                V2B_CK(cudaEventRecord(e1, s));
+                V2B_CK(cudaEventSynchronize(e1));
+                V2B_CK(cudaEventElapsedTime(&ms, e0, e1));
+                if (S == 1 || ms < best) {
+                    best = ms;
+                    best_s = S;
+                }
+            }
+            int g = 0;
+            const std::vector<int4> k = split_tiles(d, L, best_s, g);
+            n_out = (int)k.size();
+            int4 *dev = dalloc<int4>(std::max(n_out, 1));
+            if (n_out) V2B_CK(cudaMemcpy(dev, k.data(), n_out * sizeof(int4), cudaMemcpyHostToDevice));
+            return std::make_pair(dev, best_s);
+        };
+        auto full = pick(tl, false, nktiles);
+        auto upper = pick(stl, true, nkstiles);
+        ktiles = full.first;
+        kstiles = upper.first;
+        split_full = full.second;
+        split_sym = upper.second;
+        V2B_CK(cudaDeviceSynchronize());   // the chosen lists' uploads complete before any launch
+        cudaFree(buf);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaStreamDestroy(s);
+    }
+
     void build(const std::vector<int> &d) {
         dims = d;
         nblk = (int)d.size();
@@ -441,39 +532,6 @@ struct ProjectPlan {
         nstiles = (int)stl.size();
         stiles = dalloc<int4>(std::max(nstiles, 1));
         if (nstiles) V2B_CK(cudaMemcpy(stiles, stl.data(), nstiles * sizeof(int4), cudaMemcpyHostToDevice));
-        {
-            int slots = 0;
-            V2B_CK(v2b::gemm_slots(&slots));
-            int ngroups = 0;
-            auto split_list = [&](const std::vector<int4> &L) {
-                const int nl = std::max<int>((int)L.size(), 1);
-                const int S = std::min(v2b::kGemmMaxSplit, (slots + nl - 1) / nl);
-                std::vector<int4> out;
-                int g = 0;
-                for (const int4 &t : L) {
-                    if (S < 2 || d[t.x] < kSplitMinDim || g >= (1 << 19)) {
-                        out.push_back(t);
-                        continue;
-                    }
-                    for (int q = 0; q < S; q++)
-                        out.push_back(make_int4(t.x, t.y, t.z, (t.w & 1) | (q << 4) | (S << 8) | (g << 12)));
-                    g++;
-                }
-                ngroups = std::max(ngroups, g);   // a launch uses one list: the lists share the groups
-                return out;
-            };
-            const std::vector<int4> kl = split_list(tl), ksl = split_list(stl);
-            nktiles = (int)kl.size();
-            nkstiles = (int)ksl.size();
-            ktiles = dalloc<int4>(std::max(nktiles, 1));
-            kstiles = dalloc<int4>(std::max(nkstiles, 1));
-            if (nktiles) V2B_CK(cudaMemcpy(ktiles, kl.data(), nktiles * sizeof(int4), cudaMemcpyHostToDevice));
-            if (nkstiles) V2B_CK(cudaMemcpy(kstiles, ksl.data(), nkstiles * sizeof(int4), cudaMemcpyHostToDevice));
-            split_ws = dalloc<double>((size_t)std::max(ngroups, 1) * v2b::kGemmMaxSplit * v2b::kGemmTile *
-                                      v2b::kGemmTile);
-            split_cnt = dalloc<int>(std::max(ngroups, 1));
-            V2B_CK(cudaMemset(split_cnt, 0, std::max(ngroups, 1) * sizeof(int)));
-        }
         boff = dalloc<int64_t>(nblk);
         gemm_sched = dalloc<int>(2);
         V2B_CK(cudaMemset(gemm_sched, 0, 2 * sizeof(int)));
@@ -485,6 +543,7 @@ struct ProjectPlan {
         V2B_CK(cudaMemcpy(bdim, d.data(), nblk * 4, cudaMemcpyHostToDevice));
         V2B_CK(cudaMemset(counters, 0, 16));
         if (ntiles) V2B_CK(cudaMemcpy(tiles, tl.data(), ntiles * sizeof(int4), cudaMemcpyHostToDevice));
+        tune_split(d, tl, stl);
         if (nsmall) rot = dalloc<double2>(ro);
         if (smem)
             V2B_CK(v2b::raise_dynamic_smem((const void *)v2b::jacobi_warm_kernel, (int)smem));
@@ -2009,6 +2068,15 @@ int v2b_problem_set_gemm_split(v2b_problem *p, int on) {
     return guarded([&] {
         if (!p) throw std::invalid_argument("set_gemm_split: NULL problem");
         p->plan.split_k = on != 0;
+        return V2B_OK;
+    });
+}
+
+int v2b_problem_gemm_split_choice(const v2b_problem *p, int *full, int *upper) {
+    return guarded([&] {
+        if (!p || !full || !upper) throw std::invalid_argument("gemm_split_choice: NULL argument");
+        *full = p->plan.built ? p->plan.split_full : 0;
+        *upper = p->plan.built ? p->plan.split_sym : 0;
         return V2B_OK;
     });
 }

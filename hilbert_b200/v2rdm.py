@@ -459,6 +459,13 @@ class V2RDMProblem:
         launch has fewer tiles than CTA slots (default), or each in one piece"""
         check(self._lib.v2b_problem_set_gemm_split(self._h, int(bool(on))))
 
+    def gemm_split_choice(self):
+        """(S for the full tile list, S for the upper-tile list) chosen by the
+        split autotuner when the projection plan was built; (0, 0) before"""
+        full, upper = ctypes.c_int(), ctypes.c_int()
+        check(self._lib.v2b_problem_gemm_split_choice(self._h, ctypes.byref(full), ctypes.byref(upper)))
+        return full.value, upper.value
+
     REFINE_COUNTS = ("accepted", "jacobi", "passes", "clusters", "large_clusters",
                      "fallback_edges", "fallback_passes", "block_jacobi_sweeps", "fp32_eigensolves")
 

@@ -280,11 +280,17 @@ int v2b_problem_refine_counts(const v2b_problem *p, long *counts, int n);
 int v2b_problem_set_projection_mode(v2b_problem *p, int mode);
 
 /* The projection's FP64 GEMM launches cut the K range of large blocks' tiles
- * into parts when a launch has fewer tiles than the GPU has CTA slots, and
- * sum the parts in a fixed order (run-to-run identical).  on = 0 computes
- * every tile in one piece.  Default on.  No reference counterpart: libsdp
+ * into parts (the count chosen by a timed autotuner when the plan is
+ * built), and sum the parts in a fixed order (run-to-run identical).  on = 0
+ * computes every tile in one piece.  Default on.  No reference counterpart: libsdp
  * projects with LAPACK on the host. */
 int v2b_problem_set_gemm_split(v2b_problem *p, int on);
+/* The part counts S the split autotuner chose when the projection plan was
+ * built (the first projection): for the full tile list (W = Us Vt^T) and for
+ * the upper-tile list of the symmetric products (T = Vt W, U+ = Vt^T P Vt).
+ * Each is the fastest of S = 1, 2, 4 in timed launches over every block on
+ * this GPU; 0 before the plan exists. */
+int v2b_problem_gemm_split_choice(const v2b_problem *p, int *full, int *upper);
 
 /* ---- 2b. densities for the orbital optimiser --------------------------------- */
 

@@ -67,8 +67,9 @@ def test_large_block_repeated_projection(cuda_device):
 
 def test_split_k_gemm_matches_lapack_and_repeats(cuda_device):
     """The GEMM tiles of blocks of 256 rows or more cut along K (the 288-row
-    block of n = 12) and in one piece both match LAPACK; the split sums its
-    parts in a fixed order, so two projections give the same bits."""
+    block of n = 12; the part count is the autotuner's) and in one piece both
+    match LAPACK; the split sums its parts in a fixed order, so two
+    projections give the same bits."""
     import torch
     p = hb.V2RDMProblem(12, 6, 6)
     assert max(p.dims) >= 256
@@ -86,3 +87,5 @@ def test_split_k_gemm_matches_lapack_and_repeats(cuda_device):
         if on in out:
             assert np.array_equal(out[on][0], x) and np.array_equal(out[on][1], z)
         out[on] = (x, z)
+    full, upper = p.gemm_split_choice()   # the autotuner's part counts
+    assert full in (1, 2, 4) and upper in (1, 2, 4)
