@@ -72,26 +72,16 @@ __global__ void spmv_AT_U_kernel(const uint32_t *__restrict__ rp,
 // Long rows inside CG: one warp per row, lanes stride over the entries and the
 // partial sums meet in a shuffle tree (order differs from hilbert's left-to-
 // right sum; the bit-exact kernels above are the ones the map API uses).
-// The operand of entry column c: x[c], or with RBP the direction
-// r + beta p from the interleaved pair z[c] = (r_c, p_c), one 16-byte load.
-template <bool RBP>
-__device__ __forceinline__ double operand(const double *__restrict__ x, const double2 *__restrict__ z,
-                                          double beta, uint32_t c) {
-    if (RBP) {
-        const double2 v = __ldg(z + c);
-        return __dadd_rn(v.x, __dmul_rn(beta, v.y));
-    }
-    return __ldg(x + c);
-}
-
-template <bool RBP>
 __device__ __forceinline__ double warp_row(const uint32_t *__restrict__ ent, uint32_t b, uint32_t e,
-                                           const double *__restrict__ x, const double2 *__restrict__ z,
+                                           const double *__restrict__ x, const double *__restrict__ p,
                                            double beta, const double *pal, int lane) {
     double acc = 0.0;
     for (uint32_t k = b + lane; k < e; k += 32) {
         const uint32_t w = __ldg(ent + k);
-        acc += pal[(w >> 27) & 15u] * operand<RBP>(x, z, beta, w & kDevColMask);
+        const uint32_t c = w & kDevColMask;
+        double v = __ldg(x + c);
+        if (p) v = __dadd_rn(v, __dmul_rn(beta, __ldg(p + c)));
+        acc += pal[(w >> 27) & 15u] * v;
     }
     return warp_sum(acc);
 }
@@ -103,7 +93,7 @@ __device__ __forceinline__ double warp_row(const uint32_t *__restrict__ ent, uin
 // stay in L2.
 template <bool RBP>
 __device__ __forceinline__ double sell_row(const SellOp &S, int64_t sl, int lane,
-                                           const double *__restrict__ x, const double2 *__restrict__ z,
+                                           const double *__restrict__ x, const double *__restrict__ p,
                                            double beta, const double *pal, uint32_t &row) {
     const int64_t pos = sl * 32 + lane;
     row = __ldcs(S.perm + pos);
@@ -114,7 +104,10 @@ __device__ __forceinline__ double sell_row(const SellOp &S, int64_t sl, int lane
 #pragma unroll 4
     for (int k = 0; k < len; k++) {
         const uint32_t w = __ldcs(S.ent + base + 32u * k);
-        const double v = __dmul_rn(pal[(w >> 27) & 15u], operand<RBP>(x, z, beta, w & kDevColMask));
+        const uint32_t c = w & kDevColMask;
+        double xv = __ldg(x + c);
+        if (RBP) xv = __dadd_rn(xv, __dmul_rn(beta, __ldg(p + c)));
+        const double v = __dmul_rn(pal[(w >> 27) & 15u], xv);
         grp = grp || (w >> 31);
         if (grp) acc1 = __dadd_rn(acc1, v);
         else acc0 = __dadd_rn(acc0, v);
@@ -124,18 +117,20 @@ __device__ __forceinline__ double sell_row(const SellOp &S, int64_t sl, int lane
 
 // ------------------------------------------------------------------ CG
 // Solves (A A^T) y = rhs with rhs = A(c - z) + mu (b - A x), warm-started from
-// y.  Three grid barriers per iteration:
-//   1. t = A^T (r + beta p_old), p_new = r + beta p_old
-//   2. q = A t,  partial p_new.q
-//   3. y += alpha p_new, r -= alpha q, partial r.r
-// r and the direction p live interleaved, z[j] = (r_j, p_j), so the gather of
-// step 1 reads both with one 16-byte load; p_new goes to its own array pn in
-// step 1 (z is being gathered) and into z with the new r in step 3.
-// The p.q and r.r partials live in separate arrays: a block that has passed
-// barrier 2 writes its r.r partial while slower blocks may still be summing
-// the p.q partials.  Operator rows of up to kCgLongRow entries are applied
+// y, in the form CG takes on normal equations: with t = A^T p the step
+// length's denominator p.(A A^T p) is ||t||^2, which the pass that forms t
+// sums as it goes, so the update of y and r joins the pass that forms A t.
+// Two grid barriers per iteration:
+//   1. p_new = r + beta p_old, t = A^T p_new, partial ||t||^2
+//      -> alpha = r.r / ||t||^2
+//   2. per row j of A: q_j = (A t)_j, y_j += alpha p_new_j,
+//      r_j -= alpha q_j, partial r.r  -> beta, convergence
+// The t.t and r.r partials live in separate arrays: a block that has passed
+// one barrier writes its next partial while slower blocks may still be
+// summing the other.  Operator rows of up to kCgLongRow entries are applied
 // from the sliced-ELL copies (one warp per 32-row slice), longer rows by a
-// warp each from the CSR tables.
+// warp each from the CSR tables; every row of A is in exactly one of the
+// two, so the row update of pass 2 covers every dual index once.
 // 3 CTAs per SM: the gathers are latency-bound and gain more from resident
 // warps than from registers (2 CTAs per SM measured 10-15% slower)
 __global__ void __launch_bounds__(kCgThreads, 3) cg_kernel(CgParams P) {
@@ -143,22 +138,24 @@ __global__ void __launch_bounds__(kCgThreads, 3) cg_kernel(CgParams P) {
     __shared__ double red[32];
     __shared__ double bcast;
     __shared__ int flag;
+    __shared__ unsigned long long tmark;   // phase clock (CTA 0, thread 0)
     if (threadIdx.x < 16) {
         palA[threadIdx.x] = P.palA.v[threadIdx.x];
         palT[threadIdx.x] = P.palT.v[threadIdx.x];
     }
     __syncthreads();
-    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    // 32-bit thread indices (a grid holds far fewer than 2^31 threads);
+    // the kernel runs at the 40-register limit of 3 CTAs per SM
+    const unsigned gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned stride = gridDim.x * blockDim.x;
     const int nb = gridDim.x;
 
     const int lane = threadIdx.x & 31;
-    const int64_t gwarp = gtid >> 5, nwarps = stride >> 5;
+    const unsigned gwarp = gtid >> 5, nwarps = stride >> 5;
     // optional phase clock: CTA 0 adds the time from barrier to barrier
-    const bool timed = P.phase_ns != nullptr && gtid == 0;
-    unsigned long long tmark = timed ? global_ns() : 0ull;
+    if (gtid == 0) tmark = global_ns();
     auto lap = [&](int k) {
-        if (timed) {
+        if (P.phase_ns != nullptr && gtid == 0) {
             const unsigned long long now = global_ns();
             P.phase_ns[k] += now - tmark;
             tmark = now;
@@ -173,8 +170,8 @@ __global__ void __launch_bounds__(kCgThreads, 3) cg_kernel(CgParams P) {
     }
     for (int64_t w = gwarp; w < P.n_long_t; w += nwarps) {
         const int64_t i = __ldg(P.long_t + w);
-        const double v = warp_row<false>(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), P.y, nullptr,
-                                         0.0, palT, lane);
+        const double v = warp_row(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), P.y, nullptr, 0.0,
+                                  palT, lane);
         if (lane == 0) P.t[i] = v;
     }
     if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
@@ -184,88 +181,91 @@ __global__ void __launch_bounds__(kCgThreads, 3) cg_kernel(CgParams P) {
         const double av = sell_row<false>(P.sa, sl, lane, P.t, nullptr, 0.0, palA, row);
         if (row != 0xffffffffu) {
             const double v = P.Acz[row] + P.mu * (P.b[row] - P.Ax[row]) - av;
-            P.z[row] = make_double2(v, 0.0);   // first direction p = r (beta = 0)
+            P.r[row] = v;
             loc += v * v;
         }
     }
     for (int64_t w = gwarp; w < P.n_long_a; w += nwarps) {
         const int64_t j = __ldg(P.long_a + w);
-        const double av = warp_row<false>(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), P.t, nullptr,
-                                          0.0, palA, lane);
+        const double av = warp_row(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), P.t, nullptr, 0.0,
+                                   palA, lane);
         if (lane == 0) {
             const double v = P.Acz[j] + P.mu * (P.b[j] - P.Ax[j]) - av;
-            P.z[j] = make_double2(v, 0.0);
+            P.r[j] = v;
             loc += v * v;
         }
     }
     double s = block_sum(loc, red);
-    if (threadIdx.x == 0) P.partials[blockIdx.x] = s;
+    if (threadIdx.x == 0) P.partials[nb + blockIdx.x] = s;
     if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
     lap(0);
-    double rs = sum_partials(P.partials, nb, &bcast);
+    double rs = sum_partials(P.partials + nb, nb, &bcast);
 
     int it = 0;
     double beta = 0.0;
-    double *pnew = P.pn;
+    // p_old is r on the first iteration (beta = 0), then p0 and p1 alternate
+    // as p_new and p_old
     bool done = !(sqrt(rs) >= P.tol);
     while (!done && it < P.maxit) {
+        // pass 1: t = A^T (r + beta p_old), ||t||^2; p_new = r + beta p_old
+        const double *pold = it == 0 ? P.r : ((it & 1) ? P.p0 : P.p1);
+        double *pnew = (it & 1) ? P.p1 : P.p0;
+        loc = 0.0;
         for (int64_t sl = P.st.split[gwarp], se = P.st.split[gwarp + 1]; sl < se; sl++) {
             uint32_t row;
-            const double v = sell_row<true>(P.st, sl, lane, nullptr, P.z, beta, palT, row);
-            if (row != 0xffffffffu) P.t[row] = v;
+            const double v = sell_row<true>(P.st, sl, lane, P.r, pold, beta, palT, row);
+            if (row != 0xffffffffu) {
+                P.t[row] = v;
+                loc += v * v;
+            }
         }
         for (int64_t w = gwarp; w < P.n_long_t; w += nwarps) {
             const int64_t i = __ldg(P.long_t + w);
-            const double v = warp_row<true>(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), nullptr, P.z,
-                                            beta, palT, lane);
-            if (lane == 0) P.t[i] = v;
+            const double v = warp_row(P.t_ent, __ldg(P.t_rp + i), __ldg(P.t_rp + i + 1), P.r, pold,
+                                      beta, palT, lane);
+            if (lane == 0) {
+                P.t[i] = v;
+                loc += v * v;
+            }
         }
-        for (int64_t j = gtid; j < P.nd; j += stride) {
-            const double2 v = P.z[j];
-            pnew[j] = __dadd_rn(v.x, __dmul_rn(beta, v.y));
-        }
+        for (int64_t j = gtid; j < P.nd; j += stride)
+            pnew[j] = __dadd_rn(P.r[j], __dmul_rn(beta, pold[j]));
+        s = block_sum(loc, red);
+        if (threadIdx.x == 0) P.partials[blockIdx.x] = s;
         if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
         lap(1);
+        const double tt = sum_partials(P.partials, nb, &bcast);
+        if (!(tt > 0.0)) break;   // range of A A^T exhausted (or non-finite)
+        const double alpha = rs / tt;
 
+        // pass 2: q = A t row by row, y += alpha p_new, r -= alpha q, r.r
         loc = 0.0;
         for (int64_t w = gwarp; w < P.n_long_a; w += nwarps) {
             const int64_t j = __ldg(P.long_a + w);
-            const double q = warp_row<false>(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), P.t, nullptr,
-                                             0.0, palA, lane);
+            const double q = warp_row(P.a_ent, __ldg(P.a_rp + j), __ldg(P.a_rp + j + 1), P.t, nullptr,
+                                      0.0, palA, lane);
             if (lane == 0) {
-                P.q[j] = q;
-                loc += pnew[j] * q;
+                P.y[j] += alpha * pnew[j];
+                const double rv = P.r[j] - alpha * q;
+                P.r[j] = rv;
+                loc += rv * rv;
             }
         }
         for (int64_t sl = P.sa.split[gwarp], se = P.sa.split[gwarp + 1]; sl < se; sl++) {
             uint32_t row;
             const double q = sell_row<false>(P.sa, sl, lane, P.t, nullptr, 0.0, palA, row);
             if (row != 0xffffffffu) {
-                P.q[row] = q;
-                loc += pnew[row] * q;
+                P.y[row] += alpha * pnew[row];
+                const double rv = P.r[row] - alpha * q;
+                P.r[row] = rv;
+                loc += rv * rv;
             }
         }
         s = block_sum(loc, red);
         if (threadIdx.x == 0) P.partials[nb + blockIdx.x] = s;
         if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
         lap(2);
-        const double pq = sum_partials(P.partials + nb, nb, &bcast);
-        if (!(pq > 0.0)) break;   // range of A A^T exhausted (or non-finite)
-        const double alpha = rs / pq;
-
-        loc = 0.0;
-        for (int64_t j = gtid; j < P.nd; j += stride) {
-            const double pv = pnew[j];
-            P.y[j] += alpha * pv;
-            const double rv = P.z[j].x - alpha * P.q[j];
-            P.z[j] = make_double2(rv, pv);
-            loc += rv * rv;
-        }
-        s = block_sum(loc, red);
-        if (threadIdx.x == 0) P.partials[blockIdx.x] = s;
-        if (!grid_sync(P.bar, P.status, P.spin_limit, &flag)) return;
-        lap(3);
-        const double rs_new = sum_partials(P.partials, nb, &bcast);
+        const double rs_new = sum_partials(P.partials + nb, nb, &bcast);
         it++;
         if (!(rs_new == rs_new)) {   // NaN
             if (gtid == 0) atomicExch(P.status, kStatusNan);

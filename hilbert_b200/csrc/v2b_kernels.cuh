@@ -43,16 +43,16 @@ struct CgParams {
     int64_t np, nd;
     const double *Ax, *Acz, *b;     // rhs = Acz + mu (b - Ax)
     double mu;
-    double *y, *pn, *t, *q;
-    double2 *z;                     // (r_j, p_j) interleaved; pn: the new direction
-    double *partials;               // >= 2 * gridDim.x (r.r partials, then p.q partials)
+    double *y, *r, *p0, *p1, *t;
+    double *partials;               // >= 2 * gridDim.x (t.t partials, then r.r partials)
     GridBarrier *bar;
     int *status;
     long long spin_limit;
     double tol;
     int maxit;
     double *out;                    // out[0] = iterations, out[1] = final ||r||
-    unsigned long long *phase_ns;   // null, or 4 sums of ns: initial residual, A^T p, A t, update
+    unsigned long long *phase_ns;   // null, or 4 sums of ns: initial residual, pass 1 (A^T p),
+                                    // pass 2 (A t and the update), and a slot left at zero
 };
 
 __global__ void spmv_kernel(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ent,

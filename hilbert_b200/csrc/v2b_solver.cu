@@ -1273,7 +1273,7 @@ struct v2b_problem {
     cudaStream_t stream = nullptr;
     double *x = nullptr, *b = nullptr, *c = nullptr, *y = nullptr, *z = nullptr;
     double *Ax = nullptr, *Acz = nullptr, *ATy = nullptr, *U = nullptr;
-    double *rp = nullptr, *pn = nullptr, *t = nullptr, *q = nullptr;   // rp: CG (r, p) pairs
+    double *r = nullptr, *p0 = nullptr, *p1 = nullptr, *t = nullptr;
     double *y1 = nullptr, *y2 = nullptr;   // the last two dual solutions, for the CG start
     double *partials = nullptr, *cg_out = nullptr, *stats = nullptr, *stats_partials = nullptr;
     unsigned int *stats_counter = nullptr;
@@ -1332,7 +1332,7 @@ struct v2b_problem {
         A.release();
         AT.release();
         plan.release();
-        for (double *p : {x, b, c, y, z, Ax, Acz, ATy, U, rp, pn, t, q, y1, y2, partials, cg_out, stats,
+        for (double *p : {x, b, c, y, z, Ax, Acz, ATy, U, r, p0, p1, t, y1, y2, partials, cg_out, stats,
                           stats_partials})
             cudaFree(p);
         if (cg_phase) cudaFree(cg_phase);
@@ -1375,8 +1375,8 @@ struct v2b_problem {
         x = dalloc<double>(np); c = dalloc<double>(np); z = dalloc<double>(np);
         ATy = dalloc<double>(np); U = dalloc<double>(np); t = dalloc<double>(np);
         b = dalloc<double>(nd); y = dalloc<double>(nd); Ax = dalloc<double>(nd);
-        Acz = dalloc<double>(nd); rp = dalloc<double>(2 * nd); pn = dalloc<double>(nd);
-        q = dalloc<double>(nd);
+        Acz = dalloc<double>(nd); r = dalloc<double>(nd); p0 = dalloc<double>(nd);
+        p1 = dalloc<double>(nd);
         y1 = dalloc<double>(nd); y2 = dalloc<double>(nd);
         int per_sm = 0;
         V2B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v2b::cg_kernel,
@@ -1433,7 +1433,7 @@ struct v2b_problem {
         P.palA = A.pal; P.palT = AT.pal;
         P.np = prob.n_primal; P.nd = prob.n_dual;
         P.Ax = Ax; P.Acz = Acz; P.b = b; P.mu = mu;
-        P.y = y; P.z = reinterpret_cast<double2 *>(rp); P.pn = pn; P.t = t; P.q = q;
+        P.y = y; P.r = r; P.p0 = p0; P.p1 = p1; P.t = t;
         P.partials = partials; P.bar = bar; P.status = status;
         P.spin_limit = wait_limit;
         P.tol = tol; P.maxit = maxit; P.out = cg_out;

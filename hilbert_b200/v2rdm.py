@@ -305,7 +305,9 @@ class V2RDMProblem:
         check(self._lib.v2b_problem_projection_profile(self._h, ms, n, k))
         return {name: (ms[i], n[i]) for i, name in enumerate(self.PROJECTION_PHASES)}
 
-    CG_PHASES = ("initial_residual", "transpose_gather", "gather_dot", "update")
+    # pass 1: t = A^T (r + beta p) and ||t||^2; pass 2: A t with the y, r
+    # update and r.r
+    CG_PHASES = ("initial_residual", "transpose_gather", "gather_update")
 
     def cg_profile(self):
         """{phase: total_ms} of the CG kernel, barrier to barrier, with profiling on"""

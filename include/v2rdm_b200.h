@@ -248,8 +248,8 @@ int v2b_problem_set_profiling(v2b_problem *p, int on);
 int v2b_problem_projection_profile(const v2b_problem *p, double *ms, long *n, int count);
 /* with profiling level 2: milliseconds of the CG kernel's phases, barrier to
  * barrier on the kernel's own clock, the first count of: [0] initial
- * residual, [1] A^T p and the new direction, [2] A t and p.q, [3] the r
- * update and r.r (no reference counterpart) */
+ * residual, [1] the new direction p, t = A^T p and ||t||^2, [2] A t with the
+ * y and r update and r.r, [3] zero (no reference counterpart) */
 int v2b_problem_cg_profile(const v2b_problem *p, double *ms, int count);
 int v2b_problem_profile(const v2b_problem *p, double *ms /* [5] */, long *launches /* [5] */);
 /* the cudaStream_t the device solve runs on (after the first device call) */
