@@ -148,21 +148,42 @@ def test_dqgt2_energy_between_dqg_and_fci(cuda_device):
     assert e["DQGT2"] <= hubbard_fci(4, 4, 1.0, 4.0) + E_TOL
 
 
-@pytest.mark.parametrize("extra", [("POSITIVITY", "DQGT1"), ("CONSTRAIN_D3", True)])
-def test_t1_and_d3_tighten_dqg_below_fci(cuda_device, extra):
-    """Device solves through the T1 and D3 maps (hilbert's t1.cc and d3.cc
-    families): each added condition keeps E(DQG) <= E <= E(FCI) on the
-    4-site ring at U/t = 4."""
-    o = hubbard_options(4, 4.0)
-    base = hb.v2RDMHelper(None, o)
-    e_dqg = base.compute_energy()
-    o = hubbard_options(4, 4.0)
-    o.set(*extra)
-    helper = hb.v2RDMHelper(None, o)
-    e = helper.compute_energy()
-    assert base.stats["converged"] and helper.stats["converged"]
-    assert e_dqg <= e + E_TOL
-    assert e <= hubbard_fci(4, 4, 1.0, 4.0) + E_TOL
+def test_t1_tightens_dqg_below_fci(cuda_device):
+    """A device solve through the T1 maps (hilbert's t1.cc family) keeps
+    E(DQG) <= E(DQGT1) <= E(FCI) on the 4-site ring at U/t = 4."""
+    e = {}
+    for pos in ("DQG", "DQGT1"):
+        o = hubbard_options(4, 4.0)
+        o.set("POSITIVITY", pos)
+        helper = hb.v2RDMHelper(None, o)
+        e[pos] = helper.compute_energy()
+        assert helper.stats["converged"], pos
+    assert e["DQG"] <= e["DQGT1"] + E_TOL
+    assert e["DQGT1"] <= hubbard_fci(4, 4, 1.0, 4.0) + E_TOL
+
+
+def test_d3_trajectory_matches_oracle_on_reference_maps(cuda_device):
+    """60 boundary-point iterations with the D3 condition (DQG+D3, 4-site
+    ring) follow the numpy oracle driven by hilbert's own compiled maps
+    (d3.cc through oracle/_ref).  (On the device a DQG+D3 solve of this
+    ring did not reach 1e-6 within 100,000 outer iterations; the oracle
+    after 3,000 stood at eps_p = 2e-5: the check is on the trajectory.)"""
+    from oracle.bpsdp import BPSDPSolver
+    from oracle.maps import RefProblem, ref_available
+    if not ref_available():
+        pytest.skip("oracle/_ref not built")
+    n = 4
+    r = RefProblem(n, 2, 2, "DQG+D3", True, True, hubbard=(1.0, 4.0))
+    so = BPSDPSolver(r.n_primal, r.n_dual, SDPOptions(1e-12, 1e-12, 1e-9, 10000, 60))
+    xo = r.x0.copy()
+    so.solve(xo, r.b, r.c, r.dims, 60, r.Au, r.ATu)
+    p = hb.V2RDMProblem(n, 2, 2, "DQG+D3", hubbard_multiplicity=True)
+    opts = hb.Options({"R_CONVERGENCE": 1e-12, "E_CONVERGENCE": 1e-12, "MAXITER": 60,
+                       "MU_UPDATE_FREQUENCY": 100})
+    xg, st = p.solve(r.x0, r.b, r.c, opts)
+    assert st["oiter"] == 60
+    assert np.max(np.abs(xg - xo)) <= 1e-6
+    assert abs(float(r.c @ xg) - float(r.c @ xo)) <= 1e-7
 
 
 def test_profiling_timers_leave_the_solve_unchanged(cuda_device):
