@@ -76,6 +76,24 @@ def fp64_reference(workload):
         return json.load(f)
 
 
+# Outer and CG iteration counts of the device's own FP64 solve of each
+# workload to convergence (default path, B200): what the CPU arm's sampled
+# per-iteration costs are scaled by when the CPU oracle's full solve is not
+# available as a fixture.
+DEVICE_COUNTS = {"df20": {"outer_iterations": 4101, "cg_iterations": 127159}}
+
+
+def iteration_counts(workload):
+    """(counts, source): the CPU oracle's FP64 solve when its fixture exists,
+    else the device solve's counts, else (None, None)."""
+    ref = fp64_reference(workload)
+    if ref is not None:
+        return ref, "the CPU oracle's FP64 solve to convergence"
+    if workload in DEVICE_COUNTS:
+        return dict(DEVICE_COUNTS[workload]), "the device's FP64 solve to convergence (B200, default path)"
+    return None, None
+
+
 def hamiltonian(w):
     """('hubbard', (t, U)) or ('external', (h, g)) for a workload"""
     if w["hamiltonian"] == "hubbard":
@@ -284,9 +302,9 @@ def config_of(args, w):
             "l2": "flushed between steps (256 MiB write)"}
 
 
-def cpu_baseline(w, ref, seconds, steps=1):
-    """The CPU path timed on a bounded sample, scaled to the FP64 solve's
-    iteration counts (the CPU oracle's own solve, ref)."""
+def cpu_baseline(w, ref, seconds, steps=1, source="the CPU oracle's FP64 solve to convergence"):
+    """The CPU path timed on a bounded sample, scaled to the iteration counts
+    of an FP64 solve to convergence (ref; source says whose)."""
     omp, blas = cpu_threads()
     vals = []
     for _ in range(steps):
@@ -296,8 +314,7 @@ def cpu_baseline(w, ref, seconds, steps=1):
             "openmp_threads_maps": omp, "blas_threads": blas,
             "sample": f"{reps[0]} CG iterations ({t_cg * 1e3:.2f} ms each) and {reps[1]} outer-iteration "
                       f"bodies ({t_out * 1e3:.2f} ms each) timed on the host per step, scaled to the "
-                      f"{ref['cg_iterations']} CG + {ref['outer_iterations']} outer iterations of the CPU "
-                      f"oracle's FP64 solve to convergence",
+                      f"{ref['cg_iterations']} CG + {ref['outer_iterations']} outer iterations of {source}",
             "measured_full_solve": {"wall_s": ref.get("wall_s"), "omp_threads": ref.get("omp_threads"),
                                     "where": "the build container's host cores (generator run)"}}
 
@@ -307,16 +324,17 @@ def run_reference(args, w):
     if rank != 0:
         return
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
-    ref = fp64_reference(args.workload)
+    ref, source = iteration_counts(args.workload)
     if ref is None:
-        print(json.dumps({"impl": "reference", "unavailable": f"no FP64 CPU solve fixture for {args.workload}"}))
+        print(json.dumps({"impl": "reference", "unavailable": f"no converged FP64 solve of {args.workload} "
+                                                             "to scale the CPU sample by"}))
         return
     # each step a bounded sample; the whole run stays within a few minutes
     per_step = max(2.0, min(args.cpu_sample_seconds, 180.0 / max(1, args.warmup + args.steps)))
     vals = []
     cb = None
     for k in range(args.warmup + args.steps):
-        b = cpu_baseline(w, ref, per_step)
+        b = cpu_baseline(w, ref, per_step, source=source)
         if k >= args.warmup:
             vals.append(b["value"])
             cb = b
@@ -535,8 +553,12 @@ def run_b200(args, w):
     roof["phases_ms"] = phases
 
     cpu = None
-    if rank == 0 and world == 1 and args.cpu_sample_seconds > 0 and ref is not None:
-        cpu = cpu_baseline(w, ref, args.cpu_sample_seconds)
+    counts, source = iteration_counts(args.workload)
+    if counts is None and stats is not None and stats["converged"]:
+        counts = {"outer_iterations": int(stats["oiter"]), "cg_iterations": int(stats["iiter"])}
+        source = "this run's device solve to convergence"
+    if rank == 0 and world == 1 and args.cpu_sample_seconds > 0 and counts is not None:
+        cpu = cpu_baseline(w, counts, args.cpu_sample_seconds, source=source)
     clocks = clk.summary()
     if rank == 0:
         cfg = config_of(args, w)
