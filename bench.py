@@ -81,6 +81,13 @@ def fp64_reference(workload):
 # per-iteration costs are scaled by when the CPU oracle's full solve is not
 # available as a fixture.
 DEVICE_COUNTS = {"df20": {"outer_iterations": 4101, "cg_iterations": 127159}}
+# DRAM bytes the CG kernel moves per CG iteration (dram__bytes_read.sum +
+# dram__bytes_write.sum from one ncu capture of a whole launch: 9.56 + 4.70 GB
+# over 142 iterations and the initial residual, on the same df20 problem;
+# `python -m hilbert_b200.synthetic --n 20 --naux 400 --max-outer 1`).  The
+# bench's launches run the same passes over the same vectors, so their traffic
+# is this figure times their iterations.
+CG_DRAM_BYTES_PER_ITERATION = {"df20": 14.26e9 / 143}
 
 
 def iteration_counts(workload):
@@ -536,10 +543,16 @@ def run_b200(args, w):
     bytes_launch = (m + 1) * per_iter   # + the initial residual's A^T and A pass
     ach = bytes_launch / (ms_cg / n_cg / 1e3) / 1e9
     roof = {"kernel": "cg_kernel", "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-            "frac": ach / hbm, "traffic": None,
+            "frac": ach / hbm,
+            "traffic": (CG_DRAM_BYTES_PER_ITERATION[args.workload] * (m + 1)
+                        if args.workload in CG_DRAM_BYTES_PER_ITERATION else None),
+            "traffic_source": ("ncu DRAM bytes per CG iteration of one captured launch on the same "
+                               "problem, times (m + 1)" if args.workload in CG_DRAM_BYTES_PER_ITERATION
+                               else None),
             "algorithmic_bytes": "per CG iteration 8 (2 n_p + 7 n_d) vector bytes (index tables "
                                  f"excluded); (m + 1) iterations per launch, m = {m:.1f}",
-            "peak_source": ("MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s") + " (of measured)",
+            "peak_source": ("MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks
+                            else "fallback 6650 GB/s (of fallback)"),
             "launch_ms": ms_cg / max(n_cg, 1)}
     ms_pj, n_pj = prof["projection"]
     flops = sum((16.0 / 3.0) * float(d) ** 3 for d in p.dims)
