@@ -165,9 +165,10 @@ def test_t1_tightens_dqg_below_fci(cuda_device):
 def test_d3_trajectory_matches_oracle_on_reference_maps(cuda_device):
     """60 boundary-point iterations with the D3 condition (DQG+D3, 4-site
     ring) follow the numpy oracle driven by hilbert's own compiled maps
-    (d3.cc through oracle/_ref).  (On the device a DQG+D3 solve of this
-    ring did not reach 1e-6 within 100,000 outer iterations; the oracle
-    after 3,000 stood at eps_p = 2e-5: the check is on the trajectory.)"""
+    (d3.cc through oracle/_ref).  (A DQG+D3 solve of this ring does not
+    reach 1e-6 within 100,000 outer iterations, on the device as in the
+    oracle, which stands at eps_p = eps_d = 1.3e-6 there: the check is on
+    the trajectory.)"""
     from oracle.bpsdp import BPSDPSolver
     from oracle.maps import RefProblem, ref_available
     if not ref_available():
