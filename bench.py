@@ -236,6 +236,7 @@ def cpu_threads():
     omp = int(os.environ.get("OMP_NUM_THREADS", "0") or 0) or (os.cpu_count() or 1)
     blas = 1
     try:
+        import numpy  # noqa: F401  (loads the BLAS the query below looks for)
         from threadpoolctl import threadpool_info
         n = [i.get("num_threads", 1) for i in threadpool_info() if i.get("user_api") == "blas"]
         blas = max(n) if n else 1
