@@ -39,8 +39,12 @@ class SDPOptions:
         self.maxiter = maxiter
 
 
-def cg_solve(apply, rhs, y, tol, maxiter):
-    """Plain conjugate gradients on the SPD-on-range operator A A^T (warm start y)."""
+def cg_solve(apply, rhs, y, tol, maxiter, split=None):
+    """Plain conjugate gradients on the SPD-on-range operator A A^T (warm start y).
+
+    split = (ATu, Au): the step length's denominator p.(A A^T p) is taken as
+    ||A^T p||^2, equal in exact arithmetic (the form CG takes on normal
+    equations, which the device kernel uses)."""
     r = rhs - apply(y)
     p = r.copy()
     rs = float(r @ r)
@@ -48,8 +52,13 @@ def cg_solve(apply, rhs, y, tol, maxiter):
     if np.sqrt(rs) < tol:
         return y, 0
     while it < maxiter:
-        Ap = apply(p)
-        pAp = float(p @ Ap)
+        if split is None:
+            Ap = apply(p)
+            pAp = float(p @ Ap)
+        else:
+            t = split[0](p)
+            Ap = split[1](t)
+            pAp = float(t @ t)
         if pAp <= 0.0:
             break
         alpha = rs / pAp
@@ -113,12 +122,17 @@ class BPSDPSolver:
     polynomial extrapolation through the last solutions of the same solve()
     call (2y - y1 after one, 3y - 3y1 + y2 after two), as the device solve
     does.  Either start reaches the same CG tolerance: only the number of CG
-    iterations changes.  precision: the projection's (project_blocks)."""
+    iterations changes.  precision: the projection's (project_blocks).
+    cg_step: "pq" takes the CG step length as r.r / p.(A A^T p), "normal" as
+    r.r / ||A^T p||^2 (the device's form; cg_solve)."""
 
-    def __init__(self, n_primal, n_dual, options=None, cg_start="last", precision="fp64"):
+    def __init__(self, n_primal, n_dual, options=None, cg_start="last", precision="fp64", cg_step="pq"):
         if cg_start not in ("last", "extrapolate"):
             raise ValueError(f"cg_start: {cg_start!r}")
+        if cg_step not in ("pq", "normal"):
+            raise ValueError(f"cg_step: {cg_step!r}")
         self.cg_start = cg_start
+        self.cg_step = cg_step
         self.precision = precision
         self.n_primal = int(n_primal)
         self.n_dual = int(n_dual)
@@ -153,7 +167,8 @@ class BPSDPSolver:
             elif self.cg_start == "extrapolate" and k == 1:
                 y0 = 2.0 * self.y - hist[-1]
             hist = (hist + [self.y])[-2:]
-            self.y, iiter = cg_solve(AAT, rhs, y0, o.cg_convergence, o.cg_maxiter)
+            self.y, iiter = cg_solve(AAT, rhs, y0, o.cg_convergence, o.cg_maxiter,
+                                     split=(ATu, Au) if self.cg_step == "normal" else None)
             ATy = ATu(self.y)
             U = self.mu * x + ATy - c
             xn, self.z = project_blocks(U, dims, self.mu, self.precision)

@@ -195,3 +195,25 @@ def test_fp32_eigenvectors_with_an_fp64_rayleigh_ritz_step_keep_the_solve():
     assert a["converged"] and b["converged"]
     assert abs(a["outer_iterations"] - b["outer_iterations"]) <= 0.01 * a["outer_iterations"]
     assert abs(a["energy"] - b["energy"]) <= 1e-7
+
+
+def test_normal_equations_cg_step_keeps_the_solve():
+    """The device CG's step length r.r / ||A^T p||^2 (with its extrapolated
+    start) against the p.(A A^T p) form on a (4e, 4o) synthetic DF problem:
+    the same solution within 1e-8 Eh, in outer iterations within 1%."""
+    from hilbert_b200.synthetic import df_hamiltonian
+    from oracle.bpsdp import BPSDPSolver, SDPOptions
+    h, g = df_hamiltonian(4, 400, 4, 5)
+    o = OracleProblem(4, 2, 2, "DQG", True, True, h=h, g=g)
+    out = {}
+    for step in ("pq", "normal"):
+        s = BPSDPSolver(o.n_primal, o.n_dual, SDPOptions(1e-6, 1e-6, 1e-9, 10000, 200000),
+                        cg_start="extrapolate", cg_step=step)
+        x = o.guess("random")
+        while not s.is_converged() and s.oiter_total() < 200000:
+            s.solve(x, o.b, o.c, [int(d) for d in o.dims], 500, o.Au, o.ATu)
+        assert s.is_converged()
+        out[step] = (float(o.c @ x), s.oiter_total(), s.iiter_total())
+    (ea, na, _), (eb, nb, _) = out["pq"], out["normal"]
+    assert abs(ea - eb) <= 1e-8
+    assert abs(na - nb) <= 0.01 * na
