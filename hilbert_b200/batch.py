@@ -212,10 +212,12 @@ def solve_batch(instances, options=None, rank=0, world=1, group=None, solve=solv
 
 
 def main(argv=None):
-    """python -m hilbert_b200.batch [--count 64] [--mode one-launch|sequential|both]
+    """python -m hilbert_b200.batch [--count 64] [--mode one-launch|sequential|both] [--maxiter N]
     Solves the seeded ring batch on this process's GPU and prints one JSON
     line: wall time per mode (CUDA-synchronised, problem set-up included),
-    instances converged, and the largest energy difference between the modes."""
+    instances converged, outer iterations, and the largest energy difference
+    between the modes.  --maxiter caps the outer iterations of every solve
+    (hilbert's MAXITER) for a bounded run."""
     import argparse
     import json
     import time
@@ -226,13 +228,15 @@ def main(argv=None):
     ap.add_argument("--count", type=int, default=64)
     ap.add_argument("--mode", choices=("one-launch", "sequential", "both"), default="both")
     ap.add_argument("--r-convergence", type=float, default=1e-6)
+    ap.add_argument("--maxiter", type=int, default=400000)
     args = ap.parse_args(argv)
     if not torch.cuda.is_available():
         raise SystemExit("hilbert_b200.batch: needs a CUDA device")
     insts = hubbard_batch(count=args.count)
     opts = Options({"R_CONVERGENCE": args.r_convergence, "E_CONVERGENCE": args.r_convergence,
-                    "MAXITER": 400000, "MU_UPDATE_FREQUENCY": 500})
-    out = {"workload": f"{args.count} Hubbard rings (L 6-14, seed 3), DQG", "r_convergence": args.r_convergence}
+                    "MAXITER": args.maxiter, "MU_UPDATE_FREQUENCY": 500})
+    out = {"workload": f"{args.count} Hubbard rings (L 6-14, seed 3), DQG", "r_convergence": args.r_convergence,
+           "maxiter": args.maxiter}
     energies = {}
     for mode in (("one-launch", "sequential") if args.mode == "both" else (args.mode,)):
         torch.cuda.synchronize()
@@ -244,6 +248,7 @@ def main(argv=None):
         torch.cuda.synchronize()
         out[f"{mode}_s"] = round(time.perf_counter() - t0, 3)
         out[f"{mode}_converged"] = sum(r["converged"] for r in res)
+        out[f"{mode}_outer_iterations_max"] = max(int(r["oiter"]) for r in res)
         energies[mode] = np.array([r["energy"] for r in res])
     if len(energies) == 2:
         out["max_abs_dE"] = float(np.max(np.abs(energies["one-launch"] - energies["sequential"])))
