@@ -24,6 +24,12 @@ Multi-GPU: replicas only.  Each rank solves its own copy of the workload;
 the reported time is the max over ranks; nothing crosses NVLink in the data
 path.
 
+``roofline`` is the CG kernel's: algorithmic bytes 8 (2 n_p + 7 n_d) per CG
+iteration over its CUDA-event launch time, against the measured HBM copy
+bandwidth; ``traffic`` is the kernel's DRAM bytes per iteration from one ncu
+capture on the same problem (CG_DRAM_BYTES_PER_ITERATION) times the launch's
+iterations.
+
 ``--impl reference`` times the reference's own CPU implementation of the path
 (hilbert's compiled constraint maps from oracle/_ref, else the C restatement,
 driven by the numpy boundary-point restatement), each step a bounded sample
