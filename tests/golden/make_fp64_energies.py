@@ -15,9 +15,10 @@ Workloads (the same definitions as bench.py):
   hubbard8  1D periodic Hubbard ring, 8 sites, 8 electrons, t = 1, U = 4
   df20      (20e, 20o) synthetic density-fitted integrals (naux 400, seeds 4, 5)
 
-The df20 solve takes hours on a few host cores.  --state PATH saves the
-iteration state (x, y, z, mu, counters) after every solve() call and resumes
-from it.  Run from the repository root:
+The df20 solve takes hours (5.4 h on 7 threads for the committed fixture,
+with the extrapolated CG start).  --state PATH saves the iteration state
+(x, y, z, mu, counters) after every solve() call and resumes from it.  Run
+from the repository root:
 
     OMP_NUM_THREADS=8 python tests/golden/make_fp64_energies.py hubbard8
     OMP_NUM_THREADS=8 python tests/golden/make_fp64_energies.py df20 --state /tmp/df20.npz \
