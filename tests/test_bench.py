@@ -46,3 +46,21 @@ def test_cg_traffic_scales_with_iterations():
     per = bench.CG_DRAM_BYTES_PER_ITERATION["df20"]
     # one ncu capture: 14.26 GB over 142 CG iterations and the initial residual
     assert abs(per * 143 - 14.26e9) < 1e6
+
+
+def test_fp64_fixtures_describe_the_bench_problems():
+    """Each committed CPU-oracle fixture is a converged solve of the problem
+    its workload names: the same primal and dual sizes as the oracle builds
+    for it, and errors below the thresholds it was run at."""
+    from oracle.maps import OracleProblem
+    for name in ("hubbard8", "df20"):
+        ref = bench.fp64_reference(name)
+        if ref is None:
+            continue
+        w = bench.WORKLOADS[name]
+        kind, ham = bench.hamiltonian(w)
+        kw = dict(hubbard=ham) if kind == "hubbard" else dict(h=ham[0], g=ham[1])
+        o = OracleProblem(w["nmo"], w["nalpha"], w["nbeta"], w["positivity"], True, True, **kw)
+        assert (ref["n_primal"], ref["n_dual"]) == (o.n_primal, o.n_dual), name
+        assert ref["converged"] and ref["eps_p"] < 1e-6 and ref["eps_d"] < 1e-6, name
+        assert abs(ref["energy"] - ref["dual_energy"]) < 1e-6, name
