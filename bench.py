@@ -251,6 +251,9 @@ def cpu_threads():
     return omp, blas
 
 
+_CPU_PROBLEMS = {}
+
+
 def cpu_sample(w, seconds):
     """Time the CPU path on a bounded sample.
 
@@ -265,12 +268,16 @@ def cpu_sample(w, seconds):
     from oracle import maps
     from oracle.bpsdp import project_blocks
     kind = "reference" if maps.ref_available() else "port"
-    P = maps.RefProblem if kind == "reference" else maps.OracleProblem
-    kind_h, ham = hamiltonian(w)
-    kw = dict(hubbard=ham) if kind_h == "hubbard" else dict(h=ham[0], g=ham[1])
-    prob = P(w["nmo"], w["nalpha"], w["nbeta"], w["positivity"], True, True, **kw)
-    o = maps.OracleProblem(w["nmo"], w["nalpha"], w["nbeta"], w["positivity"], True, True, **kw)
-    x = o.guess("random")
+    key = (id(w), kind)
+    if key not in _CPU_PROBLEMS:   # built once per workload: the steps time the iteration only
+        P = maps.RefProblem if kind == "reference" else maps.OracleProblem
+        kind_h, ham = hamiltonian(w)
+        kw = dict(hubbard=ham) if kind_h == "hubbard" else dict(h=ham[0], g=ham[1])
+        prob = P(w["nmo"], w["nalpha"], w["nbeta"], w["positivity"], True, True, **kw)
+        o = maps.OracleProblem(w["nmo"], w["nalpha"], w["nbeta"], w["positivity"], True, True, **kw)
+        _CPU_PROBLEMS[key] = (prob, o.guess("random"))
+    prob, x = _CPU_PROBLEMS[key]
+    x = x.copy()
     z = np.zeros(prob.n_primal)
     y = np.random.default_rng(0).standard_normal(prob.n_dual)
     r = y.copy()
